@@ -1,0 +1,123 @@
+/*
+ * xpu_b200.h
+ *
+ * C ABI of the B200-native GpuScan / GpuJoin / GpuPreAgg executor.
+ *
+ * PG-Strom's GPU service (src/gpu_service.c) receives three XpuCommands from
+ * PostgreSQL backends and, for each XpuTaskExec, launches kern_gpujoin_main
+ * (src/cuda_gpujoin.cu:1050).  This library is the drop-in replacement for
+ * everything below that socket: the service keeps its protocol handling and
+ * calls these entry points instead of cuLaunchKernel.  All structs crossing
+ * the boundary are the reference's own wire formats (pgstrom_abi.h); no
+ * C++ or torch type appears here.
+ *
+ * Conventions (kept from the reference):
+ *   - a non-zero return value is one of ERRCODE_* ('E', 'F', 'd', 'f') and
+ *     *err is filled like kern_errorbuf in gpuClientELog;
+ *   - the session blob and inner buffer are copied by the callee
+ *     (gpu_service.c:3363-3371); kds_src belongs to the caller;
+ *   - one session may be used from several threads; calls on the same
+ *     session are serialised internally.
+ */
+#ifndef XPU_B200_H
+#define XPU_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#include "pgstrom_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct xpuB200Device  xpuB200Device;
+typedef struct xpuB200Session xpuB200Session;
+
+/*
+ * Attach GPU 'cuda_dindex' and reserve bookkeeping for up to hbm_budget
+ * bytes of device memory (0 = 90% of free memory).
+ * Replaces gpuservSetupGpuContext / gpuservSetupGpuModule
+ * (gpu_service.c:6463, :6231-6319).  No runtime compilation: the kernels
+ * are built into this library for sm_100a.
+ */
+int  xpuB200Init(int cuda_dindex, uint64_t hbm_budget,
+                 xpuB200Device **p_dev, kern_errorbuf *err);
+void xpuB200Shutdown(xpuB200Device *dev);
+
+/*
+ * Open a query session: validate and translate the session bytecode,
+ * upload the inner relations of a GpuJoin (kmrels may be NULL) and build
+ * their device hash indexes, and allocate the GROUP BY final buffer.
+ * Replaces gpuservHandleOpenSession (gpu_service.c:3320-3410) together
+ * with __setupGpuQueryJoinInnerBuffer (:2198-2354) and the kds_final
+ * allocation of getGpuQueryBuffer (:2357-2412).
+ */
+int  xpuB200OpenSession(xpuB200Device *dev,
+                        const kern_session_info *session, uint64_t session_sz,
+                        const kern_multirels *kmrels, uint64_t kmrels_sz,
+                        xpuB200Session **p_sess, kern_errorbuf *err);
+
+/*
+ * Execute one chunk (KDS_FORMAT_BLOCK heap pages, KDS_FORMAT_ARROW, or
+ * KDS_FORMAT_ROW).  kds_src is a host pointer unless kds_src_on_device is
+ * non-zero, in which case it is a device pointer on this GPU.  Statistics
+ * (nitems_raw / nitems_in / nitems_out / stats[]) are written to *results
+ * when results is not NULL; results->num_rels must give the capacity of
+ * results->stats[].  Pre-aggregated groups stay on the device until
+ * xpuB200Final.
+ * Replaces gpuservHandleGpuTaskExec / __gpuservLaunchGpuTaskExecKernel
+ * (gpu_service.c:4006-4290, :3760-4003).
+ */
+int  xpuB200ExecTask(xpuB200Session *sess,
+                     const kern_data_store *kds_src, int kds_src_on_device,
+                     kern_exec_results *results, kern_errorbuf *err);
+
+/*
+ * Materialise the final buffer in the reference's KDS_FORMAT_HASH layout
+ * (kern_hashitem tuples with kagg_state__* partial states), as read by
+ * pgstromScanNextTuple (executor.c:861-883) and finalised by aggfuncs.c.
+ * If buf_sz is smaller than the result, nothing is copied, *p_required is
+ * set and ERRCODE_SUSPEND_NO_SPACE is returned.
+ * Replaces gpuservHandleGpuTaskFinal (gpu_service.c:5685-5882).
+ */
+int  xpuB200Final(xpuB200Session *sess, void *kds_final_buf, uint64_t buf_sz,
+                  uint64_t *p_required, kern_exec_results *results,
+                  kern_errorbuf *err);
+
+void xpuB200CloseSession(xpuB200Session *sess);
+
+/*
+ * Whole-command entry point for a service loop: handles the three command
+ * tags gpuservGpuWorkerMain dispatches (gpu_service.c:5951-5964):
+ *   XpuCommandTag__OpenSession  -> *p_sess is created (kmrels may be NULL)
+ *   XpuCommandTag__XpuTaskExec  -> kds_src at xcmd->u.task.kds_src_offset
+ *   XpuCommandTag__XpuTaskFinal -> resp carries results + kds_final
+ * The response (XpuCommandTag__Success / __Error) is written into resp
+ * (capacity resp_sz bytes); returns 0 or an ERRCODE_*.
+ */
+int  xpuB200HandleCommand(xpuB200Device *dev, xpuB200Session **p_sess,
+                          const XpuCommand *xcmd,
+                          const kern_multirels *kmrels, uint64_t kmrels_sz,
+                          XpuCommand *resp, uint64_t resp_sz);
+
+/* Device memory helpers for callers that keep chunks resident in HBM. */
+int  xpuB200DeviceAlloc(xpuB200Device *dev, uint64_t sz, void **p_dptr);
+int  xpuB200DeviceFree(xpuB200Device *dev, void *dptr);
+int  xpuB200CopyToDevice(xpuB200Device *dev, void *dptr, const void *src, uint64_t sz);
+
+/*
+ * Time one ExecTask over a device-resident chunk 'niters' times with CUDA
+ * events on the session's stream (no host synchronisation inside the timed
+ * region other than at its end); returns the average kernel milliseconds
+ * in *p_msec.  Used by the benchmark to report the kernel roofline.
+ */
+int  xpuB200TimeExecTask(xpuB200Session *sess, const kern_data_store *kds_src_dev,
+                         int niters, double *p_msec, kern_errorbuf *err);
+
+/* Diagnostics: translated plan summary and host-side hash self test. */
+int  xpuB200SessionInfo(xpuB200Session *sess, char *buf, uint64_t buf_sz);
+uint32_t xpuB200HashBytes(const void *data, uint32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif  /* XPU_B200_H */

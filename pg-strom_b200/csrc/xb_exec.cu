@@ -1,0 +1,1945 @@
+/*
+ * xb_exec.cu
+ *
+ * B200 (sm_100a) kernels of the scan / hash-join / pre-aggregation path and
+ * the C ABI declared in include/xpu_b200.h.
+ *
+ * Kernels:
+ *   xb_build_inner   decodes the inner relation (KDS_FORMAT_HASH, built on
+ *                    the host by gpu_join.c:2129-2164) into SoA register
+ *                    images and an open-addressing (hash,row) index;
+ *   xb_exec_kernel   persistent executor: warps claim heap pages (or Arrow /
+ *                    row groups), decode tuples, run scan quals, probe the
+ *                    joins depth-first and update the GROUP BY tables.  Heap
+ *                    pages of the next claim are prefetched into L2 by the
+ *                    TMA engine (cp.async.bulk.prefetch.L2) while the current
+ *                    ones are decoded;
+ *   xb_final_*       materialise kds_final in the reference layout.
+ *
+ * Reference counterparts: kern_gpujoin_main (cuda_gpujoin.cu:1050-1279),
+ * __gpuscan_load_source_block/_arrow/_row (cuda_gpuscan.cu:405-727),
+ * execGpuJoinHashJoin (cuda_gpujoin.cu:304-494), execGpuPreAggGroupBy and
+ * friends (cuda_gpupreagg.cu:1112-2326), __writeOutOneTuplePreAgg
+ * (cuda_gpupreagg.cu:18-223).
+ */
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+#include <mutex>
+#include <vector>
+#include <string>
+#include <cstring>
+#include <cstdio>
+#include <cstdlib>
+#include <cstdarg>
+#include "xb_plan.h"
+#include "xb_device.cuh"
+#include "xb_compile.h"
+#include "xpu_b200.h"
+
+#define XB_BLOCK        256
+#define XB_WARPS        (XB_BLOCK / 32)
+#define XB_CLAIM        4           /* heap pages claimed per warp at a time */
+#define XB_ROWS_UNIT    1024        /* rows per unit for ARROW / ROW chunks */
+#define XB_PROBE_LIMIT  4096        /* max probes in the global group table */
+
+/* ================================================================
+ * memory-order helpers (generic addresses: shared or global)
+ * ================================================================ */
+__device__ __forceinline__ uint32_t xb_ld_acquire(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void xb_st_release(uint32_t *p, uint32_t v)
+{
+    asm volatile("st.release.gpu.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+/* L2 prefetch of a contiguous range by the TMA engine (sm_90+) */
+__device__ __forceinline__ void xb_prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
+}
+
+/* ================================================================
+ * partial-aggregate state arithmetic
+ * ================================================================ */
+__device__ __forceinline__ void xb_atomic_add_i128(uint64_t *p, xb_i128 v)
+{
+    uint64_t lo = (uint64_t)v;
+    uint64_t hi = (uint64_t)((unsigned __int128)v >> 64);
+    uint64_t old = atomicAdd((unsigned long long *)&p[0], (unsigned long long)lo);
+    if (old + lo < old)
+        hi += 1;
+    if (hi)
+        atomicAdd((unsigned long long *)&p[1], (unsigned long long)hi);
+}
+
+/* compensated atomic sum: hi accumulates the rounded sum, lo the exact
+ * rounding error of each addition (TwoSum on the value atomicAdd saw) */
+__device__ __forceinline__ void xb_atomic_add_f64c(double *hi, double *lo, double x)
+{
+    double old = atomicAdd(hi, x);
+    double s = __dadd_rn(old, x);
+    double bp = __dsub_rn(s, old);
+    double e = __dadd_rn(__dsub_rn(old, __dsub_rn(s, bp)), __dsub_rn(x, bp));
+    if (e != 0.0)
+        atomicAdd(lo, e);
+}
+
+__device__ __forceinline__ double xb_reg_f64(uint64_t v, int rk)
+{
+    return rk == XB_RK_FLT ? __longlong_as_double(v) : (double)(int64_t)v;
+}
+
+__device__ __noinline__ void xb_init_states(const xb_plan *plan, char *e)
+{
+    for (uint32_t i = 0; i < plan->naggs; i++) {
+        const xb_agg &a = plan->aggs[i];
+        if (a.state_sz == 0)
+            continue;
+        uint64_t *s = (uint64_t *)(e + a.state_off);
+        for (uint32_t k = 0; k < a.state_sz / 8; k++)
+            s[k] = 0;
+        switch (a.action) {
+        case KAGG_ACTION__PMIN_INT32:
+        case KAGG_ACTION__PMIN_INT64:
+        case KAGG_ACTION__PMIN_FP64:
+            s[0] = (uint64_t)INT64_MAX;
+            break;
+        case KAGG_ACTION__PMAX_INT32:
+        case KAGG_ACTION__PMAX_INT64:
+        case KAGG_ACTION__PMAX_FP64:
+            s[0] = (uint64_t)INT64_MIN;
+            break;
+        default:
+            break;
+        }
+    }
+}
+
+/* __updateOneTupleGroupBy + __update_groupby__* (cuda_gpupreagg.cu:1196-1605) */
+__device__ __noinline__ void xb_update_states(const xb_plan *plan, char *e, const XbRegs &R,
+                                 uint32_t lane, xb_status *st)
+{
+    for (uint32_t i = 0; i < plan->naggs; i++) {
+        const xb_agg &a = plan->aggs[i];
+        if (a.state_sz == 0)
+            continue;
+        if (a.filter >= 0 && (RISNULL(R, a.filter) || RVAL(R, a.filter) == 0))
+            continue;
+        char *s = e + a.state_off;
+        bool n0 = a.arg0 < 0 ? true : (RISNULL(R, a.arg0) != 0);
+        uint64_t v0 = a.arg0 < 0 ? 0 : RVAL(R, a.arg0);
+        int rk0 = a.arg0 < 0 ? 0 : plan->rk[a.arg0];
+        switch (a.action) {
+        case KAGG_ACTION__NROWS_ANY:
+            atomicAdd((unsigned long long *)s, 1ULL);
+            break;
+        case KAGG_ACTION__NROWS_COND:
+            if (!n0) atomicAdd((unsigned long long *)s, 1ULL);
+            break;
+        case KAGG_ACTION__PMIN_INT32:
+        case KAGG_ACTION__PMIN_INT64:
+            if (!n0) { atomicOr((unsigned int *)(s + 8), 1u); atomicMin((long long *)s, (long long)v0); }
+            break;
+        case KAGG_ACTION__PMAX_INT32:
+        case KAGG_ACTION__PMAX_INT64:
+            if (!n0) { atomicOr((unsigned int *)(s + 8), 1u); atomicMax((long long *)s, (long long)v0); }
+            break;
+        case KAGG_ACTION__PMIN_FP64:
+            if (!n0) {
+                atomicOr((unsigned int *)(s + 8), 1u);
+                atomicMin((long long *)s, (long long)xb_f64_ordered(xb_reg_f64(v0, rk0)));
+            }
+            break;
+        case KAGG_ACTION__PMAX_FP64:
+            if (!n0) {
+                atomicOr((unsigned int *)(s + 8), 1u);
+                atomicMax((long long *)s, (long long)xb_f64_ordered(xb_reg_f64(v0, rk0)));
+            }
+            break;
+        case KAGG_ACTION__PSUM_INT:
+        case KAGG_ACTION__PAVG_INT:
+            if (!n0) {
+                atomicAdd((unsigned long long *)s, 1ULL);
+                atomicAdd((unsigned long long *)(s + 8), (unsigned long long)v0);
+            }
+            break;
+        case KAGG_ACTION__PSUM_INT64:
+        case KAGG_ACTION__PAVG_INT64:
+            if (!n0) {
+                atomicAdd((unsigned long long *)s, 1ULL);
+                xb_atomic_add_i128((uint64_t *)(s + 8), (xb_i128)(int64_t)v0);
+            }
+            break;
+        case KAGG_ACTION__PSUM_FP:
+        case KAGG_ACTION__PAVG_FP:
+            if (!n0) {
+                atomicAdd((unsigned long long *)s, 1ULL);
+                xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), xb_reg_f64(v0, rk0));
+            }
+            break;
+        case KAGG_ACTION__PSUM_NUMERIC:
+        case KAGG_ACTION__PAVG_NUMERIC:
+            if (!n0) {
+                uint8_t kind; int16_t w; xb_i128 v;
+                if (xb_numeric_decode((const uint8_t *)v0, &kind, &w, &v)) {
+                    XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
+                } else if (kind == XB_NUM_VALID) {
+                    atomicAdd((unsigned long long *)s, 1ULL);
+                    xb_atomic_add_i128((uint64_t *)(s + 8), xb_numeric_rescale(a.weight, w, v));
+                } else {
+                    uint32_t special = kind == XB_NUM_PINF ? PAGG_NUMERIC_ATTRS__PINF
+                                     : kind == XB_NUM_NINF ? PAGG_NUMERIC_ATTRS__NINF
+                                     : PAGG_NUMERIC_ATTRS__NAN;
+                    atomicOr((unsigned int *)(s + 24), special);
+                }
+            }
+            break;
+        case KAGG_ACTION__STDDEV:
+            if (!n0) {
+                double x = xb_reg_f64(v0, rk0);
+                atomicAdd((unsigned long long *)s, 1ULL);
+                xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
+                xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
+            }
+            break;
+        case KAGG_ACTION__COVAR: {
+            bool n1 = RISNULL(R, a.arg1) != 0;
+            if (!n0 && !n1) {
+                double x = xb_reg_f64(v0, rk0);
+                double y = xb_reg_f64(RVAL(R, a.arg1), plan->rk[a.arg1]);
+                atomicAdd((unsigned long long *)s, 1ULL);
+                xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
+                xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
+                xb_atomic_add_f64c((double *)(s + 40), (double *)(s + 48), y);
+                xb_atomic_add_f64c((double *)(s + 56), (double *)(s + 64), y * y);
+                xb_atomic_add_f64c((double *)(s + 72), (double *)(s + 80), x * y);
+            }
+            break;
+        }
+        default:
+            break;
+        }
+    }
+}
+
+/* merge a shared-memory group entry's states into a global entry */
+__device__ __noinline__ void xb_merge_states(const xb_plan *plan, char *dst, const char *src)
+{
+    for (uint32_t i = 0; i < plan->naggs; i++) {
+        const xb_agg &a = plan->aggs[i];
+        if (a.state_sz == 0)
+            continue;
+        char *d = dst + a.state_off;
+        const char *s = src + a.state_off;
+        const uint64_t *su = (const uint64_t *)s;
+        switch (a.action) {
+        case KAGG_ACTION__NROWS_ANY:
+        case KAGG_ACTION__NROWS_COND:
+            if (su[0]) atomicAdd((unsigned long long *)d, su[0]);
+            break;
+        case KAGG_ACTION__PMIN_INT32:
+        case KAGG_ACTION__PMIN_INT64:
+        case KAGG_ACTION__PMIN_FP64:
+            if (*(const uint32_t *)(s + 8)) {
+                atomicOr((unsigned int *)(d + 8), 1u);
+                atomicMin((long long *)d, (long long)su[0]);
+            }
+            break;
+        case KAGG_ACTION__PMAX_INT32:
+        case KAGG_ACTION__PMAX_INT64:
+        case KAGG_ACTION__PMAX_FP64:
+            if (*(const uint32_t *)(s + 8)) {
+                atomicOr((unsigned int *)(d + 8), 1u);
+                atomicMax((long long *)d, (long long)su[0]);
+            }
+            break;
+        case KAGG_ACTION__PSUM_INT:
+        case KAGG_ACTION__PAVG_INT:
+            if (su[0]) {
+                atomicAdd((unsigned long long *)d, su[0]);
+                atomicAdd((unsigned long long *)(d + 8), su[1]);
+            }
+            break;
+        case KAGG_ACTION__PSUM_INT64:
+        case KAGG_ACTION__PAVG_INT64:
+        case KAGG_ACTION__PSUM_NUMERIC:
+        case KAGG_ACTION__PAVG_NUMERIC:
+            if (su[0]) {
+                atomicAdd((unsigned long long *)d, su[0]);
+                xb_atomic_add_i128((uint64_t *)(d + 8),
+                                   (xb_i128)(((unsigned __int128)su[2] << 64) | su[1]));
+            }
+            if (a.state_sz >= 32 && *(const uint32_t *)(s + 24))
+                atomicOr((unsigned int *)(d + 24), *(const uint32_t *)(s + 24));
+            break;
+        case KAGG_ACTION__PSUM_FP:
+        case KAGG_ACTION__PAVG_FP:
+        case KAGG_ACTION__STDDEV:
+        case KAGG_ACTION__COVAR:
+            if (su[0]) {
+                atomicAdd((unsigned long long *)d, su[0]);
+                for (uint32_t k = 8; k + 16 <= a.state_sz; k += 16) {
+                    xb_atomic_add_f64c((double *)(d + k), (double *)(d + k + 8),
+                                       *(const double *)(s + k));
+                    double lo = *(const double *)(s + k + 8);
+                    if (lo != 0.0)
+                        atomicAdd((double *)(d + k + 8), lo);
+                }
+            }
+            break;
+        default:
+            break;
+        }
+    }
+}
+
+/* ================================================================
+ * group keys
+ * ================================================================ */
+__device__ __forceinline__ uint32_t xb_numeric_varsize(const uint8_t *vl)
+{
+    if (vl[0] & 0x01)
+        return (vl[0] >> 1) & 0x7f;
+    return ((uint32_t)xb_fetch_le(vl, 4) >> 2) & 0x3fffffff;
+}
+
+/* key value of register 'reg' for this lane, as a key image */
+__device__ __forceinline__ void
+xb_key_from_regs(const xb_key &k, const XbRegs &R, uint32_t lane, xb_keyimg *img)
+{
+    img->isnull = RISNULL(R, k.reg);
+    img->val = RVAL(R, k.reg);
+    img->len = RAUX(R, k.reg);
+}
+
+__device__ __forceinline__ bool
+xb_key_equal(const xb_key &k, const xb_keyimg &x, const xb_keyimg &y)
+{
+    if (x.isnull || y.isnull)
+        return x.isnull && y.isnull;        /* NULLs group together */
+    if (k.rk == XB_RK_TEXT)
+        return x.len == y.len &&
+               xb_bytes_eq((const uint8_t *)x.val, (const uint8_t *)y.val, x.len);
+    if (k.rk == XB_RK_NUM) {
+        int err = 0;
+        return xb_numeric_cmp((const uint8_t *)x.val, (const uint8_t *)y.val, &err) == 0 && !err;
+    }
+    return x.val == y.val;
+}
+
+/* copy a key image into an entry; into the arena when 'gt' is given */
+__device__ __forceinline__ bool
+xb_key_store(const xb_key &k, const xb_keyimg &src, xb_keyimg *dst,
+             xb_gtable *gt, xb_status *st)
+{
+    *dst = src;
+    if (src.isnull || !gt)
+        return true;
+    if (k.rk == XB_RK_TEXT || k.rk == XB_RK_NUM) {
+        uint32_t nbytes = (k.rk == XB_RK_TEXT) ? src.len
+                                               : xb_numeric_varsize((const uint8_t *)src.val);
+        unsigned long long off = atomicAdd((unsigned long long *)&gt->arena_used,
+                                           (unsigned long long)((nbytes + 7) & ~7u));
+        if (off + nbytes > gt->arena_sz) {
+            XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_ARENA_FULL);
+            return false;
+        }
+        char *p = gt->arena + off;
+        const char *s = (const char *)src.val;
+        for (uint32_t i = 0; i < nbytes; i++)
+            p[i] = s[i];
+        dst->val = (uint64_t)p;
+    }
+    return true;
+}
+
+/*
+ * Find the group whose keys equal 'keys', or create it.  Works on the
+ * shared-memory table (gt == nullptr) and on the global table.  An entry
+ * is claimed EMPTY->BUSY by CAS, initialised, then published READY with a
+ * release store; readers wait (bounded) on BUSY entries.
+ * Returns nullptr when the table is full (*full) or on error.
+ */
+__device__ __noinline__ char *
+xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t hash,
+              const xb_keyimg *keys, xb_gtable *gt, xb_status *st, bool *full)
+{
+    const uint32_t gsz = plan->gent_size;
+    uint64_t pos = hash & cap_mask;
+    uint64_t limit = gt ? (cap_mask < XB_PROBE_LIMIT ? cap_mask : XB_PROBE_LIMIT) : cap_mask;
+    for (uint64_t probe = 0; probe <= limit; probe++) {
+        char *e = entries + pos * gsz;
+        xb_gent_head *h = (xb_gent_head *)e;
+        uint32_t s = xb_ld_acquire(&h->state);
+        if (s == XB_GSTATE_EMPTY) {
+            if (atomicCAS(&h->state, XB_GSTATE_EMPTY, XB_GSTATE_BUSY) == XB_GSTATE_EMPTY) {
+                h->hash = hash;
+                xb_keyimg *img = (xb_keyimg *)(e + plan->gent_keys_off);
+                bool ok = true;
+                for (uint32_t k = 0; k < plan->nkeys; k++)
+                    ok &= xb_key_store(plan->keys[k], keys[k], &img[k], gt, st);
+                xb_init_states(plan, e);
+                if (gt)
+                    atomicAdd((unsigned long long *)&gt->nused, 1ULL);
+                xb_st_release(&h->state, XB_GSTATE_READY);
+                return ok ? e : nullptr;
+            }
+            s = xb_ld_acquire(&h->state);
+        }
+        uint32_t spins = 0;
+        while (s == XB_GSTATE_BUSY) {
+            if (++spins > XB_WAIT_LIMIT) {
+                XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_WAIT_TIMEOUT);
+                return nullptr;
+            }
+            __nanosleep(20);
+            s = xb_ld_acquire(&h->state);
+        }
+        if (h->hash == hash) {
+            const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
+            bool eq = true;
+            for (uint32_t k = 0; k < plan->nkeys && eq; k++)
+                eq = xb_key_equal(plan->keys[k], img[k], keys[k]);
+            if (eq)
+                return e;
+        }
+        pos = (pos + 1) & cap_mask;
+    }
+    *full = true;
+    return nullptr;
+}
+
+/* ================================================================
+ * executor kernel
+ * ================================================================ */
+struct XbExecArgs {
+    const xb_plan  *plan;
+    const kern_data_store *kds;
+    uint32_t        nunits;
+    uint32_t        format;
+    uint32_t        sm_cap;         /* shared-memory group table entries (0: none) */
+    uint32_t        regs_bytes;     /* per-warp register file bytes */
+    xb_gtable      *gt;
+    xb_status      *st;
+};
+
+struct XbCounters {
+    unsigned long long raw, in, out;
+    unsigned long long depth[XB_MAX_DEPTH + 1];
+};
+
+struct XbCtx {
+    const xb_plan  *plan;
+    XbRegs          R;
+    char           *sm_entries;
+    uint32_t        sm_mask;
+    xb_gtable      *gt;
+    xb_status      *st;
+    XbCounters      cnt;
+    bool            failed;
+};
+
+__device__ __noinline__ void xb_groupby(XbCtx &c, uint32_t act)
+{
+    const xb_plan *plan = c.plan;
+    const uint32_t lane = xb_lane();
+    if (plan->gb_args.count && !xb_vm_run(plan->insns + plan->gb_args.start,
+                                         plan->gb_args.count, c.R, act, c.st)) {
+        c.failed = true;
+        return;
+    }
+    uint32_t hash = 0;
+    if (plan->has_groupby == 1) {
+        if (!xb_vm_run(plan->insns + plan->gb_keyhash.start,
+                       plan->gb_keyhash.count, c.R, act, c.st)) {
+            c.failed = true;
+            return;
+        }
+        hash = (uint32_t)RVAL(c.R, plan->gb_keyhash.result);
+    }
+    if ((act >> lane) & 1u) {
+        xb_keyimg keys[XB_MAX_KEYS];
+        for (uint32_t k = 0; k < plan->nkeys; k++)
+            xb_key_from_regs(plan->keys[k], c.R, lane, &keys[k]);
+        char *e = nullptr;
+        bool full = false;
+        if (c.sm_entries)
+            e = xb_group_find(plan, c.sm_entries, c.sm_mask, hash, keys, nullptr, c.st, &full);
+        if (!e) {
+            full = false;
+            e = xb_group_find(plan, c.gt->entries, c.gt->cap_mask, hash, keys, c.gt, c.st, &full);
+            if (!e && full) {
+                XB_RAISE(c.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+                atomicOr(&c.gt->overflow, 1u);
+            }
+        }
+        if (e)
+            xb_update_states(plan, e, c.R, lane, c.st);
+        else
+            c.failed = true;
+    }
+    /* keep the failure flag warp-uniform: later full-mask ballots rely on it */
+    c.failed = __any_sync(XB_FULL, c.failed);
+}
+
+/* load the inner row's pre-decoded registers for lanes in 'cand' */
+__device__ __forceinline__ void
+xb_load_inner(const xb_inner *in, XbRegs &R, uint32_t lane, uint32_t cand, uint32_t row)
+{
+    const bool mine = (cand >> lane) & 1u;
+    const uint32_t words = (in->nitems + 31) / 32;
+    for (uint32_t k = 0; k < in->nloads; k++) {
+        uint32_t reg = in->load[k].reg;
+        bool isnull = true;
+        if (mine) {
+            RVAL(R, reg) = __ldg((const unsigned long long *)&in->vals[(size_t)k * in->nitems + row]);
+            RAUX(R, reg) = __ldg(&in->auxs[(size_t)k * in->nitems + row]);
+            isnull = (__ldg(&in->nulls[(size_t)k * words + row / 32]) >> (row % 32)) & 1u;
+        }
+        xb_set_null(R, reg, isnull);
+    }
+}
+
+template <int D>
+__device__ __noinline__ void xb_join_depth(XbCtx &c, uint32_t act)
+{
+    const xb_plan *plan = c.plan;
+    if constexpr (D > XB_MAX_DEPTH) {
+        (void)plan; (void)act;
+        return;
+    } else {
+        if ((uint32_t)D > plan->nrels) {
+            c.cnt.out += __popc(act);
+            if (plan->has_groupby)
+                xb_groupby(c, act);
+            return;
+        }
+        const uint32_t lane = xb_lane();
+        const xb_inner *in = &plan->inner[D];
+        const xb_prog &hp = plan->hash_value[D];
+        if (!xb_vm_run(plan->insns + hp.start, hp.count, c.R, act, c.st)) {
+            c.failed = true;
+            return;
+        }
+        const uint32_t hash = (uint32_t)RVAL(c.R, hp.result);
+        uint64_t pos = hash & in->cap_mask;
+        bool live = ((act >> lane) & 1u) && in->nitems > 0;
+        for (;;) {
+            uint32_t row = 0;
+            bool got = false;
+            if (live) {
+                for (uint32_t probe = 0; probe <= in->cap_mask; probe++) {
+                    uint64_t ent = __ldg((const unsigned long long *)&in->index[pos]);
+                    pos = (pos + 1) & in->cap_mask;
+                    if (ent == 0) { live = false; break; }
+                    if ((uint32_t)(ent >> 32) == hash) {
+                        row = (uint32_t)ent - 1;
+                        got = true;
+                        if (in->unique_hash)
+                            live = false;
+                        break;
+                    }
+                }
+                if (!got) live = false;
+            }
+            const uint32_t cand = __ballot_sync(XB_FULL, got);
+            if (cand == 0)
+                break;
+            xb_load_inner(in, c.R, lane, cand, row);
+            uint32_t ok = cand;
+            const xb_prog &jp = plan->join_quals[D];
+            if (jp.count) {
+                if (!xb_vm_run(plan->insns + jp.start, jp.count, c.R, cand, c.st)) {
+                    c.failed = true;
+                    return;
+                }
+                bool pass = ((cand >> lane) & 1u) && !RISNULL(c.R, jp.result) &&
+                            RVAL(c.R, jp.result) != 0;
+                ok = __ballot_sync(XB_FULL, pass);
+            }
+            c.cnt.depth[D] += __popc(ok);
+            if (ok) {
+                xb_join_depth<D + 1>(c, ok);
+                if (c.failed)
+                    return;
+            }
+        }
+    }
+}
+
+/* scan quals + joins + group-by over one batch of 32 decoded rows */
+__device__ __forceinline__ void xb_process_batch(XbCtx &c, uint32_t loaded)
+{
+    const xb_plan *plan = c.plan;
+    const uint32_t lane = xb_lane();
+    uint32_t pass = loaded;
+    if (plan->scan_quals.count) {
+        if (!xb_vm_run(plan->insns + plan->scan_quals.start, plan->scan_quals.count,
+                       c.R, loaded, c.st)) {
+            c.failed = true;
+            return;
+        }
+        int r = plan->scan_quals.result;
+        bool ok = ((loaded >> lane) & 1u) && !RISNULL(c.R, r) && RVAL(c.R, r) != 0;
+        pass = __ballot_sync(XB_FULL, ok);
+    }
+    c.cnt.in += __popc(pass);
+    if (pass)
+        xb_join_depth<1>(c, pass);
+}
+
+/* write the NULL ballots of the depth-0 load registers */
+__device__ __forceinline__ void
+xb_publish_load_nulls(const xb_plan *plan, XbRegs &R, bool ok, uint32_t nullbits)
+{
+    for (uint32_t i = 0; i < plan->nload0; i++)
+        xb_set_null(R, plan->load0[i].reg, !ok || ((nullbits >> i) & 1u));
+}
+
+__device__ __noinline__ void
+xb_scan_heap_page(XbCtx &c, const kern_data_store *kds, const XbCol *cols, int kds_ncols,
+                  uint32_t block_id)
+{
+    const xb_plan *plan = c.plan;
+    const uint32_t lane = xb_lane();
+    const uint8_t *page = (const uint8_t *)kds + kds->block_offset + (size_t)block_id * PGSTROM_BLCKSZ;
+    const uint32_t pd_lower = *(const uint16_t *)(page + 12);
+    uint32_t nlp = 0;
+    if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ)
+        nlp = (pd_lower - SizeOfPageHeaderData) / sizeof(ItemIdData);
+    else if (pd_lower > PGSTROM_BLCKSZ) {
+        if (lane == 0) XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
+        c.failed = true;
+        return;
+    }
+    for (uint32_t base = 0; base < nlp; base += 32) {
+        const uint32_t idx = base + lane;
+        bool normal = false, ok = false;
+        uint32_t nullbits = 0;
+        if (idx < nlp) {
+            const uint32_t lp = ((const uint32_t *)(page + SizeOfPageHeaderData))[idx];
+            if (ITEMID_FLAGS(lp) == LP_NORMAL) {
+                const uint32_t off = ITEMID_OFF(lp), len = ITEMID_LEN(lp);
+                normal = true;
+                if (off >= SizeOfPageHeaderData && len >= SizeofHeapTupleHeader &&
+                    off + len <= PGSTROM_BLCKSZ) {
+                    const uint8_t *htup = page + off;
+                    const uint16_t infomask2 = *(const uint16_t *)(htup + 18);
+                    const uint16_t infomask = *(const uint16_t *)(htup + 20);
+                    const uint32_t t_hoff = htup[22];
+                    int natts = infomask2 & HEAP_NATTS_MASK;
+                    if (natts > kds_ncols) natts = kds_ncols;
+                    const uint8_t *nullmap = (infomask & HEAP_HASNULL) ? htup + SizeofHeapTupleHeader : nullptr;
+                    if (t_hoff >= SizeofHeapTupleHeader && t_hoff <= len &&
+                        (!nullmap || SizeofHeapTupleHeader + (natts + 7) / 8 <= t_hoff)) {
+                        ok = xb_decode_tuple(cols, natts, nullmap, htup + t_hoff, len - t_hoff,
+                                             plan->load0, plan->nload0,
+                                             c.R.val + lane, c.R.aux + lane, 32, false, &nullbits);
+                    }
+                    if (!ok) {
+                        XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+                    }
+                }
+            }
+        }
+        const uint32_t nrm = __ballot_sync(XB_FULL, normal);
+        c.cnt.raw += __popc(nrm);
+        if (__any_sync(XB_FULL, normal && !ok)) {
+            c.failed = true;
+            return;
+        }
+        xb_publish_load_nulls(plan, c.R, ok, nullbits);
+        const uint32_t loaded = __ballot_sync(XB_FULL, ok);
+        if (loaded)
+            xb_process_batch(c, loaded);
+        if (c.failed)
+            return;
+    }
+}
+
+/* Arrow column -> register (xpu_*_datum_arrow_read) */
+__device__ __forceinline__ bool
+xb_arrow_load(const kern_data_store *kds, const kern_colmeta *cm, uint32_t row, int ld,
+              uint64_t *val, uint32_t *aux, bool *isnull, xb_status *st)
+{
+    if (cm->virtual_offset != 0) {
+        if (cm->virtual_offset < 0) { *isnull = true; return true; }
+        *isnull = false;
+        return xb_load_datum(ld, (const uint8_t *)kds + cm->virtual_offset, val, aux);
+    }
+    if (cm->nullmap_offset) {
+        const uint8_t *nm = (const uint8_t *)kds + cm->nullmap_offset;
+        uint32_t b = row >> 3;
+        if (b >= cm->nullmap_length || !((nm[b] >> (row & 7)) & 1)) { *isnull = true; return true; }
+    }
+    const uint8_t *values = (const uint8_t *)kds + cm->values_offset;
+    const int tag = cm->attopts.tag;
+    *isnull = false;
+    *aux = 0;
+    switch (ld) {
+    case XB_LD_INT2: case XB_LD_INT4: case XB_LD_INT8: {
+        uint32_t w = ld == XB_LD_INT2 ? 2 : ld == XB_LD_INT4 ? 4 : 8;
+        if (tag != ArrowType__Int || cm->attopts.u.integer.bitWidth != w * 8) return false;
+        if ((uint64_t)w * (row + 1) > cm->values_length) { *isnull = true; return true; }
+        int64_t v = w == 2 ? (int64_t)((const int16_t *)values)[row]
+                  : w == 4 ? (int64_t)((const int32_t *)values)[row]
+                           : ((const int64_t *)values)[row];
+        *val = (uint64_t)v;
+        return true;
+    }
+    case XB_LD_FLT8:
+        if (tag != ArrowType__FloatingPoint || cm->attopts.u.floating_point.precision != ArrowPrecision__Double)
+            return false;
+        if (8ULL * (row + 1) > cm->values_length) { *isnull = true; return true; }
+        *val = ((const uint64_t *)values)[row];
+        return true;
+    case XB_LD_DATE:
+        if (tag != ArrowType__Date) return false;
+        if (cm->attopts.u.date.unit == ArrowDateUnit__Day) {
+            if (4ULL * (row + 1) > cm->values_length) { *isnull = true; return true; }
+            *val = (uint64_t)(int64_t)(int32_t)(((const uint32_t *)values)[row] - 10957u);
+        } else {
+            if (8ULL * (row + 1) > cm->values_length) { *isnull = true; return true; }
+            *val = (uint64_t)(int64_t)(int32_t)(((const uint64_t *)values)[row] / 86400000ULL - 10957ULL);
+        }
+        return true;
+    case XB_LD_BOOL:
+        if (tag != ArrowType__Bool) return false;
+        if ((row >> 3) >= cm->values_length) { *isnull = true; return true; }
+        *val = (values[row >> 3] >> (row & 7)) & 1;
+        return true;
+    case XB_LD_TEXT: {
+        if (tag != ArrowType__Utf8 && tag != ArrowType__Binary && tag != ArrowType__LargeUtf8) return false;
+        const uint8_t *extra = (const uint8_t *)kds + cm->extra_offset;
+        uint64_t s, e;
+        if (tag == ArrowType__LargeUtf8) {
+            if (8ULL * (row + 2) > cm->values_length + 8) { *isnull = true; return true; }
+            s = ((const uint64_t *)values)[row]; e = ((const uint64_t *)values)[row + 1];
+        } else {
+            if (4ULL * (row + 2) > cm->values_length + 4) { *isnull = true; return true; }
+            s = ((const uint32_t *)values)[row]; e = ((const uint32_t *)values)[row + 1];
+        }
+        if (s > e || e > cm->extra_length) { *isnull = true; return true; }
+        *val = (uint64_t)(extra + s);
+        *aux = (uint32_t)(e - s);
+        return true;
+    }
+    default:
+        return false;
+    }
+}
+
+__device__ __noinline__ void
+xb_scan_arrow_unit(XbCtx &c, const kern_data_store *kds, uint32_t unit)
+{
+    const xb_plan *plan = c.plan;
+    const uint32_t lane = xb_lane();
+    const uint32_t row0 = unit * XB_ROWS_UNIT;
+    for (uint32_t b = 0; b < XB_ROWS_UNIT; b += 32) {
+        if (row0 + b >= kds->nitems)
+            break;
+        const uint32_t row = row0 + b + lane;
+        const bool exists = row < kds->nitems;
+        bool ok = exists;
+        uint32_t nullbits = 0;
+        if (exists) {
+            for (uint32_t i = 0; i < plan->nload0; i++) {
+                const xb_load &ldd = plan->load0[i];
+                bool isnull = true;
+                if (ldd.resno <= (int)kds->ncols) {
+                    const kern_colmeta *cm = &kds->colmeta[ldd.resno - 1];
+                    if (!xb_arrow_load(kds, cm, row, ldd.ld, &RVAL(c.R, ldd.reg),
+                                       &RAUX(c.R, ldd.reg), &isnull, c.st)) {
+                        ok = false;
+                        XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_ARROW_TYPE);
+                        break;
+                    }
+                }
+                if (isnull) nullbits |= 1u << i;
+            }
+        }
+        c.cnt.raw += __popc(__ballot_sync(XB_FULL, exists));
+        if (__any_sync(XB_FULL, exists && !ok)) {
+            c.failed = true;
+            return;
+        }
+        xb_publish_load_nulls(plan, c.R, ok, nullbits);
+        const uint32_t loaded = __ballot_sync(XB_FULL, ok);
+        if (loaded)
+            xb_process_batch(c, loaded);
+        if (c.failed)
+            return;
+    }
+}
+
+__device__ __noinline__ void
+xb_scan_row_unit(XbCtx &c, const kern_data_store *kds, const XbCol *cols, uint32_t unit)
+{
+    const xb_plan *plan = c.plan;
+    const uint32_t lane = xb_lane();
+    const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
+    const uint32_t row0 = unit * XB_ROWS_UNIT;
+    for (uint32_t b = 0; b < XB_ROWS_UNIT; b += 32) {
+        if (row0 + b >= kds->nitems)
+            break;
+        const uint32_t row = row0 + b + lane;
+        bool exists = row < kds->nitems, ok = false;
+        uint32_t nullbits = 0;
+        if (exists) {
+            uint64_t off = rowindex[row];
+            if (off == 0) {
+                exists = false;
+            } else if (off <= kds->length) {
+                const uint8_t *t = (const uint8_t *)kds + kds->length - off;
+                const kern_tupitem *ti = (const kern_tupitem *)t;
+                uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
+                int natts = ti->t_infomask2 & HEAP_NATTS_MASK;
+                if (natts > (int)kds->ncols) natts = kds->ncols;
+                bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
+                if (!ti->has_xact_attrs && ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 &&
+                    pay <= ti->t_len && off >= ti->t_len &&
+                    (!hasnull || 15u + (natts + 7) / 8 <= pay))
+                    ok = xb_decode_tuple(cols, natts, (ti->t_infomask & HEAP_HASNULL) ? ti->t_bits : nullptr,
+                                         t + pay, ti->t_len - pay, plan->load0, plan->nload0,
+                                         c.R.val + lane, c.R.aux + lane, 32, false, &nullbits);
+            }
+            if (exists && !ok)
+                XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+        }
+        c.cnt.raw += __popc(__ballot_sync(XB_FULL, exists));
+        if (__any_sync(XB_FULL, exists && !ok)) {
+            c.failed = true;
+            return;
+        }
+        xb_publish_load_nulls(plan, c.R, ok, nullbits);
+        const uint32_t loaded = __ballot_sync(XB_FULL, ok);
+        if (loaded)
+            xb_process_batch(c, loaded);
+        if (c.failed)
+            return;
+    }
+}
+
+__global__ void __launch_bounds__(XB_BLOCK, 3)
+xb_exec_kernel(XbExecArgs args)
+{
+    extern __shared__ __align__(16) char smem[];
+    const xb_plan *plan = args.plan;
+    const kern_data_store *kds = args.kds;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = threadIdx.x >> 5;
+
+    XbCol *cols = (XbCol *)smem;
+    char *sm_entries = smem + sizeof(XbCol) * XB_MAX_COLS;
+    const size_t sm_bytes = (size_t)args.sm_cap * plan->gent_size;
+    char *regs_base = sm_entries + sm_bytes + (size_t)warp * args.regs_bytes;
+
+    const int kds_ncols = kds->ncols < XB_MAX_COLS ? (int)kds->ncols : XB_MAX_COLS;
+    for (int i = threadIdx.x; i < kds_ncols; i += blockDim.x) {
+        cols[i].attlen = kds->colmeta[i].attlen;
+        cols[i].attalign = kds->colmeta[i].attalign > 0 ? kds->colmeta[i].attalign : 1;
+        cols[i].attcacheoff = kds->colmeta[i].attcacheoff;
+    }
+    for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
+        ((uint32_t *)sm_entries)[i] = 0;
+    __syncthreads();
+
+    XbCtx c;
+    c.plan = plan;
+    c.R = xb_regs_setup(regs_base, plan->nregs);
+    c.sm_entries = args.sm_cap ? sm_entries : nullptr;
+    c.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
+    c.gt = args.gt;
+    c.st = args.st;
+    memset(&c.cnt, 0, sizeof(c.cnt));
+    c.failed = false;
+    for (uint32_t r = lane; r < plan->nregs; r += 32)
+        c.R.nullm[r] = XB_FULL;
+    __syncwarp();
+
+    if (args.format == KDS_FORMAT_BLOCK) {
+        const uint32_t stride = XB_CLAIM;
+        uint64_t claim = 0;
+        if (lane == 0)
+            claim = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
+        claim = __shfl_sync(XB_FULL, claim, 0);
+        while (claim < args.nunits && !c.failed) {
+            uint64_t next = 0;
+            if (lane == 0)
+                next = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
+            next = __shfl_sync(XB_FULL, next, 0);
+            /* pull the next claim's pages into L2 while these are decoded */
+            if (lane < stride && next + lane < args.nunits) {
+                const char *p = (const char *)kds + kds->block_offset + (next + lane) * (size_t)PGSTROM_BLCKSZ;
+                if ((((uintptr_t)p) & 15) == 0)
+                    xb_prefetch_l2(p, PGSTROM_BLCKSZ);
+            }
+            for (uint32_t k = 0; k < stride && claim + k < args.nunits && !c.failed; k++)
+                xb_scan_heap_page(c, kds, cols, kds_ncols, (uint32_t)(claim + k));
+            if (*(volatile uint32_t *)&args.st->errcode != 0)
+                break;
+            claim = next;
+        }
+    } else {
+        for (;;) {
+            uint64_t unit = 0;
+            if (lane == 0)
+                unit = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
+            unit = __shfl_sync(XB_FULL, unit, 0);
+            if (unit >= args.nunits || c.failed)
+                break;
+            if (args.format == KDS_FORMAT_ARROW)
+                xb_scan_arrow_unit(c, kds, (uint32_t)unit);
+            else
+                xb_scan_row_unit(c, kds, cols, (uint32_t)unit);
+            if (*(volatile uint32_t *)&args.st->errcode != 0)
+                break;
+        }
+    }
+
+    /* per-warp statistics */
+    if (lane == 0) {
+        atomicAdd((unsigned long long *)&args.st->nitems_raw, c.cnt.raw);
+        atomicAdd((unsigned long long *)&args.st->nitems_in, c.cnt.in);
+        atomicAdd((unsigned long long *)&args.st->nitems_out, c.cnt.out);
+        for (uint32_t d = 1; d <= plan->nrels && d <= XB_MAX_DEPTH; d++)
+            atomicAdd((unsigned long long *)&args.st->nitems_depth[d], c.cnt.depth[d]);
+    }
+    __syncthreads();
+
+    /* merge the shared-memory group table into the global table */
+    if (args.sm_cap) {
+        for (uint32_t i = threadIdx.x; i < args.sm_cap; i += blockDim.x) {
+            char *e = sm_entries + (size_t)i * plan->gent_size;
+            const xb_gent_head *h = (const xb_gent_head *)e;
+            if (h->state != XB_GSTATE_READY)
+                continue;
+            const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
+            bool full = false;
+            char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, h->hash,
+                                    img, args.gt, args.st, &full);
+            if (g)
+                xb_merge_states(plan, g, e);
+            else if (full) {
+                XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+                atomicOr(&args.gt->overflow, 1u);
+            }
+        }
+    }
+}
+
+/* ================================================================
+ * inner relation build
+ * ================================================================ */
+struct XbBuildArgs {
+    const kern_data_store *kds;     /* KDS_FORMAT_HASH inner buffer (device) */
+    xb_inner       *in;             /* device copy of the plan's inner descriptor */
+    xb_status      *st;
+};
+
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_build_inner(XbBuildArgs args)
+{
+    __shared__ XbCol cols[XB_MAX_COLS];
+    const kern_data_store *kds = args.kds;
+    xb_inner *in = args.in;
+    const int ncols = kds->ncols < XB_MAX_COLS ? (int)kds->ncols : XB_MAX_COLS;
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) {
+        cols[i].attlen = kds->colmeta[i].attlen;
+        cols[i].attalign = kds->colmeta[i].attalign > 0 ? kds->colmeta[i].attalign : 1;
+        cols[i].attcacheoff = kds->colmeta[i].attcacheoff;
+    }
+    __syncthreads();
+    const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
+    const uint32_t n = in->nitems;
+    const uint32_t words = (n + 31) / 32;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n;
+         row += gridDim.x * blockDim.x) {
+        uint64_t off = rowindex[row];
+        if (off == 0 || off > kds->length) {
+            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+            continue;
+        }
+        const kern_tupitem *ti = (const kern_tupitem *)((const char *)kds + kds->length - off);
+        uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
+        int natts = ti->t_infomask2 & HEAP_NATTS_MASK;
+        if (natts > ncols) natts = ncols;
+        uint32_t nullbits = 0;
+        bool ok = false;
+        const bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
+        if (ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 && pay <= ti->t_len && off >= ti->t_len &&
+            (!hasnull || 15u + (natts + 7) / 8 <= pay))
+            ok = xb_decode_tuple(cols, natts, (ti->t_infomask & HEAP_HASNULL) ? ti->t_bits : nullptr,
+                                 (const uint8_t *)ti + pay, ti->t_len - pay, in->load, in->nloads,
+                                 in->vals + row, in->auxs + row, n, true, &nullbits);
+        if (!ok) {
+            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+            continue;
+        }
+        for (uint32_t k = 0; k < in->nloads; k++) {
+            if ((nullbits >> k) & 1u)
+                atomicOr(&in->nulls[(size_t)k * words + row / 32], 1u << (row % 32));
+        }
+        /* index insert: (hash << 32) | (row + 1) */
+        const uint32_t hash = ti->hash;
+        const unsigned long long ent = ((unsigned long long)hash << 32) | (row + 1);
+        uint64_t pos = hash & in->cap_mask;
+        for (uint32_t probe = 0; probe <= in->cap_mask; probe++) {
+            unsigned long long old = atomicCAS((unsigned long long *)&in->index[pos], 0ULL, ent);
+            if (old == 0)
+                break;
+            if ((uint32_t)(old >> 32) == hash)
+                atomicExch(&in->unique_hash, 0u);
+            pos = (pos + 1) & in->cap_mask;
+        }
+    }
+}
+
+/* ================================================================
+ * Final: kds_final materialisation
+ * ================================================================ */
+struct XbFinalArgs {
+    const xb_plan  *plan;
+    xb_gtable      *gt;
+    uint64_t        cap;
+    uint64_t       *sizes;          /* per entry: item bytes (0 if empty) */
+    uint32_t       *flags;          /* per entry: 1 if ready */
+    uint64_t       *size_scan;
+    uint32_t       *flag_scan;
+    char           *kds_final;      /* device buffer (header already in place) */
+    uint64_t        items_base;     /* offset of the first item */
+    uint64_t        length;
+    uint32_t        nslots;
+};
+
+/* one partial-aggregate tuple (__writeOutOneTuplePreAgg layout); returns t_len */
+__device__ uint32_t
+xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint32_t rowid)
+{
+    const uint32_t nattrs = plan->naggs;
+    uint32_t t_hoff = (uint32_t)PGSTROM_MAXALIGN(15 + (nattrs + 7) / 8);
+    uint16_t infomask = HEAP_HASNULL;
+    char *base = (char *)ti;
+    if (ti) {
+        for (uint32_t i = 0; i < t_hoff; i++) base[i] = 0;
+        ti->t_infomask2 = (uint16_t)(nattrs & HEAP_NATTS_MASK);
+        ti->t_hoff = (uint8_t)(t_hoff + MINIMAL_TUPLE_OFFSET);
+        ti->hash = ((const xb_gent_head *)e)->hash;
+    }
+    const xb_keyimg *keys = (const xb_keyimg *)(e + plan->gent_keys_off);
+    for (uint32_t j = 0; j < nattrs; j++) {
+        const xb_agg &a = plan->aggs[j];
+        uint32_t t_next = (uint32_t)PGSTROM_TYPEALIGN(a.attalign, t_hoff);
+        if (ti)
+            for (uint32_t i = t_hoff; i < t_next; i++) base[i] = 0;
+        char *buf = ti ? base + t_next : nullptr;
+        uint32_t nbytes = 0;
+        const uint64_t *su = (const uint64_t *)(e + a.state_off);
+        switch (a.action) {
+        case KAGG_ACTION__VREF: {
+            if (a.key_index < 0) break;
+            const xb_key &k = plan->keys[a.key_index];
+            const xb_keyimg &img = keys[a.key_index];
+            if (img.isnull) break;
+            switch (k.ld) {
+            case XB_LD_BOOL: nbytes = 1; if (buf) buf[0] = (char)img.val; break;
+            case XB_LD_INT2: nbytes = 2; if (buf) *(int16_t *)buf = (int16_t)img.val; break;
+            case XB_LD_INT4:
+            case XB_LD_DATE: nbytes = 4; if (buf) *(int32_t *)buf = (int32_t)img.val; break;
+            case XB_LD_INT8:
+            case XB_LD_FLT8: nbytes = 8; if (buf) *(uint64_t *)buf = img.val; break;
+            case XB_LD_FLT4:
+                nbytes = 4;
+                if (buf) *(float *)buf = (float)__longlong_as_double(img.val);
+                break;
+            case XB_LD_TEXT:
+                nbytes = 4 + img.len;
+                if (buf) {
+                    *(uint32_t *)buf = nbytes << 2;
+                    for (uint32_t i = 0; i < img.len; i++) buf[4 + i] = ((const char *)img.val)[i];
+                }
+                infomask |= HEAP_HASVARWIDTH;
+                break;
+            case XB_LD_NUMERIC: {
+                const uint8_t *vl = (const uint8_t *)img.val;
+                nbytes = xb_numeric_varsize(vl);
+                if (buf) for (uint32_t i = 0; i < nbytes; i++) buf[i] = (char)vl[i];
+                infomask |= HEAP_HASVARWIDTH;
+                break;
+            }
+            }
+            break;
+        }
+        case KAGG_ACTION__NROWS_ANY:
+        case KAGG_ACTION__NROWS_COND:
+            nbytes = 8;
+            if (buf) *(uint64_t *)buf = su[0];
+            break;
+        case KAGG_ACTION__PMIN_INT32:
+        case KAGG_ACTION__PMIN_INT64:
+        case KAGG_ACTION__PMAX_INT32:
+        case KAGG_ACTION__PMAX_INT64: {
+            nbytes = sizeof(kagg_state__pminmax_int64_packed);
+            if (buf) {
+                kagg_state__pminmax_int64_packed *r = (kagg_state__pminmax_int64_packed *)buf;
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = *(const uint32_t *)(su + 1) ? PAGG_MINMAX_ATTRS__VALID : 0;
+                r->value = (int64_t)su[0];
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        case KAGG_ACTION__PMIN_FP64:
+        case KAGG_ACTION__PMAX_FP64: {
+            nbytes = sizeof(kagg_state__pminmax_fp64_packed);
+            if (buf) {
+                kagg_state__pminmax_fp64_packed *r = (kagg_state__pminmax_fp64_packed *)buf;
+                bool valid = *(const uint32_t *)(su + 1) != 0;
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = valid ? PAGG_MINMAX_ATTRS__VALID : 0;
+                r->value = valid ? xb_f64_from_ordered((int64_t)su[0])
+                                 : (a.action == KAGG_ACTION__PMIN_FP64 ? 1.7976931348623157e308
+                                                                        : -1.7976931348623157e308);
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        case KAGG_ACTION__PSUM_INT:
+        case KAGG_ACTION__PAVG_INT: {
+            nbytes = sizeof(kagg_state__psum_int_packed);
+            if (buf) {
+                kagg_state__psum_int_packed *r = (kagg_state__psum_int_packed *)buf;
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = 0;
+                r->nitems = (int64_t)su[0];
+                r->sum = (int64_t)su[1];
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        case KAGG_ACTION__PSUM_INT64:
+        case KAGG_ACTION__PAVG_INT64:
+        case KAGG_ACTION__PSUM_NUMERIC:
+        case KAGG_ACTION__PAVG_NUMERIC: {
+            nbytes = sizeof(kagg_state__psum_numeric_packed);
+            if (buf) {
+                kagg_state__psum_numeric_packed *r = (kagg_state__psum_numeric_packed *)buf;
+                bool is_num = (a.action == KAGG_ACTION__PSUM_NUMERIC || a.action == KAGG_ACTION__PAVG_NUMERIC);
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = is_num ? (((uint32_t)a.weight & PAGG_NUMERIC_ATTRS__WEIGHT) |
+                                     *(const uint32_t *)(su + 3)) : 0;
+                r->nitems = su[0];
+                r->sum.u64_lo = su[1];
+                r->sum.u64_hi = su[2];
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        case KAGG_ACTION__PSUM_FP:
+        case KAGG_ACTION__PAVG_FP: {
+            nbytes = sizeof(kagg_state__psum_fp_packed);
+            if (buf) {
+                kagg_state__psum_fp_packed *r = (kagg_state__psum_fp_packed *)buf;
+                const double *d = (const double *)su;
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = 0;
+                r->nitems = (int64_t)su[0];
+                r->sum = __dadd_rn(d[1], d[2]);
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        case KAGG_ACTION__STDDEV: {
+            nbytes = sizeof(kagg_state__stddev_packed);
+            if (buf) {
+                kagg_state__stddev_packed *r = (kagg_state__stddev_packed *)buf;
+                const double *d = (const double *)su;
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = 0;
+                r->nitems = (int64_t)su[0];
+                r->sum_x = __dadd_rn(d[1], d[2]);
+                r->sum_x2 = __dadd_rn(d[3], d[4]);
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        case KAGG_ACTION__COVAR: {
+            nbytes = sizeof(kagg_state__covar_packed);
+            if (buf) {
+                kagg_state__covar_packed *r = (kagg_state__covar_packed *)buf;
+                const double *d = (const double *)su;
+                r->vl_len_ = (int32_t)(nbytes << 2);
+                r->attrs = 0;
+                r->nitems = (int64_t)su[0];
+                r->sum_x = __dadd_rn(d[1], d[2]);
+                r->sum_xx = __dadd_rn(d[3], d[4]);
+                r->sum_y = __dadd_rn(d[5], d[6]);
+                r->sum_yy = __dadd_rn(d[7], d[8]);
+                r->sum_xy = __dadd_rn(d[9], d[10]);
+            }
+            infomask |= HEAP_HASVARWIDTH;
+            break;
+        }
+        default:
+            break;
+        }
+        if (ti && nbytes > 0)
+            ti->t_bits[j >> 3] |= (uint8_t)(1u << (j & 7));
+        t_hoff = t_next + nbytes;
+    }
+    t_hoff += ROWID_SIZE;
+    if (ti) {
+        ti->t_len = t_hoff;
+        ti->t_infomask = infomask;
+        *(uint32_t *)(base + t_hoff - ROWID_SIZE) = rowid;
+    }
+    return t_hoff;
+}
+
+__global__ void xb_final_sizes(XbFinalArgs args)
+{
+    const xb_plan *plan = args.plan;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < args.cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const char *e = args.gt->entries + i * plan->gent_size;
+        if (((const xb_gent_head *)e)->state == XB_GSTATE_READY) {
+            uint32_t t_len = xb_write_group_tuple(plan, e, nullptr, 0);
+            args.sizes[i] = PGSTROM_MAXALIGN(offsetof(kern_hashitem, t) + t_len);
+            args.flags[i] = 1;
+        } else {
+            args.sizes[i] = 0;
+            args.flags[i] = 0;
+        }
+    }
+}
+
+__global__ void xb_final_write(XbFinalArgs args)
+{
+    const xb_plan *plan = args.plan;
+    kern_data_store *kds = (kern_data_store *)args.kds_final;
+    uint64_t *hslots = (uint64_t *)(args.kds_final + KDS_HEAD_LENGTH(kds));
+    uint64_t *rowindex = hslots + args.nslots;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < args.cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (!args.flags[i])
+            continue;
+        const char *e = args.gt->entries + i * plan->gent_size;
+        const uint32_t rank = args.flag_scan[i];
+        const uint64_t item_off = args.items_base + args.size_scan[i];
+        kern_hashitem *hitem = (kern_hashitem *)(args.kds_final + item_off);
+        xb_write_group_tuple(plan, e, &hitem->t, rank);
+        rowindex[rank] = args.length - (item_off + offsetof(kern_hashitem, t));
+        const uint32_t hash = ((const xb_gent_head *)e)->hash;
+        unsigned long long mine = args.length - item_off;
+        unsigned long long prev = atomicExch((unsigned long long *)&hslots[hash % args.nslots], mine);
+        hitem->next = prev;
+    }
+}
+
+/* ================================================================
+ * host side
+ * ================================================================ */
+struct xpuB200Device {
+    int             dindex;
+    int             nsm;
+    uint64_t        hbm_budget;
+    cudaStream_t    stream;
+};
+
+struct xpuB200Session {
+    xpuB200Device  *dev;
+    std::mutex      lock;
+    std::vector<char> h_session;
+    char           *d_session = nullptr;
+    char           *d_kmrels = nullptr;
+    xb_plan        *h_plan = nullptr;
+    xb_plan        *d_plan = nullptr;
+    std::vector<void *> d_allocs;
+    xb_gtable       h_gt;
+    xb_gtable      *d_gt = nullptr;
+    xb_status      *d_status = nullptr;
+    xb_status      *h_status = nullptr;     /* pinned */
+    char           *d_src = nullptr;
+    uint64_t        d_src_cap = 0;
+    uint32_t        sm_cap = 0;
+    uint32_t        regs_bytes = 0;
+    size_t          smem_bytes = 0;
+    int             grid = 0;
+    uint64_t        total_raw = 0, total_in = 0, total_out = 0;
+    uint64_t        total_depth[XB_MAX_DEPTH + 1] = {0};
+    cudaEvent_t     ev0, ev1;
+};
+
+static const char *xb_msg_text(uint32_t id)
+{
+    switch (id) {
+    case XB_MSG_INT_RANGE:        return "integer value out of range";
+    case XB_MSG_DIV_ZERO:         return "division by zero";
+    case XB_MSG_FLT_RANGE:        return "float value out of range";
+    case XB_MSG_NUMERIC_RANGE:    return "numeric value is out of range";
+    case XB_MSG_NUMERIC_CORRUPT:  return "corrupted numeric datum";
+    case XB_MSG_VARLENA_EXTERNAL: return "external or compressed varlena is not supported";
+    case XB_MSG_BAD_TUPLE:        return "corrupted tuple or unsupported datum in the chunk";
+    case XB_MSG_GTABLE_FULL:      return "GpuPreAgg(GroupBy) - no space to write";
+    case XB_MSG_WAIT_TIMEOUT:     return "group entry wait timed out";
+    case XB_MSG_ARENA_FULL:       return "GpuPreAgg(GroupBy) - no space for variable-length keys";
+    case XB_MSG_BAD_PAGE:         return "corrupted heap page";
+    case XB_MSG_ARROW_TYPE:       return "Arrow column type does not match the device type";
+    default:                      return "device error";
+    }
+}
+
+static int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int line,
+                        const char *fmt, ...)
+{
+    if (err) {
+        memset(err, 0, sizeof(*err));
+        err->errcode = code;
+        err->lineno = line;
+        snprintf(err->filename, sizeof(err->filename), "%s", "xb_exec.cu");
+        snprintf(err->funcname, sizeof(err->funcname), "%s", func);
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(err->message, sizeof(err->message), fmt, ap);
+        va_end(ap);
+    }
+    return (int)code;
+}
+#define XB_ERR(err, code, ...) xb_set_error((err), (code), __func__, __LINE__, __VA_ARGS__)
+#define XB_CUDA(call, err) do {                                               \
+        cudaError_t __rc = (call);                                            \
+        if (__rc != cudaSuccess)                                              \
+            return XB_ERR((err), ERRCODE_DEVICE_FATAL, "%s: %s", #call,       \
+                          cudaGetErrorString(__rc));                          \
+    } while (0)
+
+static inline void xb_clear_error(kern_errorbuf *err)
+{
+    if (err) memset(err, 0, sizeof(*err));
+}
+
+extern "C" int
+xpuB200Init(int cuda_dindex, uint64_t hbm_budget, xpuB200Device **p_dev, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    int ndev = 0;
+    XB_CUDA(cudaGetDeviceCount(&ndev), err);
+    if (cuda_dindex < 0 || cuda_dindex >= ndev)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "GPU%d is not available (%d devices)", cuda_dindex, ndev);
+    XB_CUDA(cudaSetDevice(cuda_dindex), err);
+    cudaDeviceProp prop;
+    XB_CUDA(cudaGetDeviceProperties(&prop, cuda_dindex), err);
+    if (prop.major < 10)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "GPU%d is sm_%d%d; this build needs sm_100a",
+                      cuda_dindex, prop.major, prop.minor);
+    xpuB200Device *dev = new xpuB200Device();
+    dev->dindex = cuda_dindex;
+    dev->nsm = prop.multiProcessorCount;
+    if (hbm_budget == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        hbm_budget = (uint64_t)(fr * 0.9);
+    }
+    dev->hbm_budget = hbm_budget;
+    cudaError_t rc = cudaStreamCreateWithFlags(&dev->stream, cudaStreamNonBlocking);
+    if (rc != cudaSuccess) {
+        delete dev;
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cudaStreamCreate: %s", cudaGetErrorString(rc));
+    }
+    *p_dev = dev;
+    return 0;
+}
+
+extern "C" void
+xpuB200Shutdown(xpuB200Device *dev)
+{
+    if (!dev) return;
+    cudaSetDevice(dev->dindex);
+    cudaStreamSynchronize(dev->stream);
+    cudaStreamDestroy(dev->stream);
+    delete dev;
+}
+
+static void xb_session_free(xpuB200Session *s)
+{
+    cudaSetDevice(s->dev->dindex);
+    cudaStreamSynchronize(s->dev->stream);
+    for (void *p : s->d_allocs)
+        cudaFree(p);
+    if (s->d_src) cudaFree(s->d_src);
+    if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->h_plan) free(s->h_plan);
+    cudaEventDestroy(s->ev0);
+    cudaEventDestroy(s->ev1);
+    delete s;
+}
+
+static int xb_dalloc(xpuB200Session *s, size_t sz, void **p, kern_errorbuf *err)
+{
+    cudaError_t rc = cudaMalloc(p, sz < 256 ? 256 : sz);
+    if (rc != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cudaMalloc(%zu): %s", sz, cudaGetErrorString(rc));
+    }
+    s->d_allocs.push_back(*p);
+    return 0;
+}
+
+static uint64_t xb_next_pow2(uint64_t x)
+{
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+extern "C" int
+xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_t session_sz,
+                   const kern_multirels *kmrels, uint64_t kmrels_sz,
+                   xpuB200Session **p_sess, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    *p_sess = nullptr;
+    if (!dev || !session || session_sz < sizeof(kern_session_info))
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid OpenSession arguments");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    xpuB200Session *s = new xpuB200Session();
+    s->dev = dev;
+    cudaEventCreate(&s->ev0);
+    cudaEventCreate(&s->ev1);
+    int rc;
+    char msg[256];
+#define FAIL(...) do { rc = XB_ERR(err, __VA_ARGS__); xb_session_free(s); return rc; } while (0)
+#define DALLOC(sz, ptr) do { if ((rc = xb_dalloc(s, (sz), (void **)(ptr), err)) != 0) { xb_session_free(s); return rc; } } while (0)
+
+    s->h_session.assign((const char *)session, (const char *)session + session_sz);
+    DALLOC(session_sz, &s->d_session);
+    if (kmrels) {
+        if (kmrels_sz < offsetof(kern_multirels, chunks) ||
+            kmrels->num_inner_rels > XB_MAX_DEPTH ||
+            offsetof(kern_multirels, chunks) + sizeof(kmrels->chunks[0]) * kmrels->num_inner_rels > kmrels_sz)
+            FAIL(ERRCODE_DEVICE_ERROR, "kern_multirels is broken");
+    }
+    s->h_plan = (xb_plan *)calloc(1, sizeof(xb_plan));
+    if (xb_compile_session(session, session_sz, (uint64_t)s->d_session, kmrels,
+                           s->h_plan, msg, sizeof(msg)) != 0)
+        FAIL(ERRCODE_DEVICE_ERROR, "bytecode translation: %s", msg);
+    xb_plan *plan = s->h_plan;
+    cudaStream_t st = dev->stream;
+    if (cudaMemcpyAsync(s->d_session, session, session_sz, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        FAIL(ERRCODE_DEVICE_FATAL, "session upload failed");
+    DALLOC(sizeof(xb_status), &s->d_status);
+    if (cudaMallocHost((void **)&s->h_status, sizeof(xb_status)) != cudaSuccess)
+        FAIL(ERRCODE_DEVICE_FATAL, "cudaMallocHost failed");
+    cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st);
+
+    /* inner relations: upload and build indexes */
+    if (kmrels && plan->nrels > 0) {
+        DALLOC(kmrels_sz, &s->d_kmrels);
+        if (cudaMemcpyAsync(s->d_kmrels, kmrels, kmrels_sz, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            FAIL(ERRCODE_DEVICE_FATAL, "inner buffer upload failed");
+        for (uint32_t d = 1; d <= plan->nrels; d++) {
+            uint64_t koff = kmrels->chunks[d - 1].kds_offset;
+            if (koff == 0 || koff + sizeof(kern_data_store) > kmrels_sz)
+                FAIL(ERRCODE_DEVICE_ERROR, "inner KDS at depth %u is out of the buffer", d);
+            const kern_data_store *hk = (const kern_data_store *)((const char *)kmrels + koff);
+            if (hk->format != KDS_FORMAT_HASH || koff + hk->length > kmrels_sz ||
+                KDS_HEAD_LENGTH(hk) + sizeof(uint64_t) * ((uint64_t)hk->hash_nslots + hk->nitems) > hk->length)
+                FAIL(ERRCODE_DEVICE_ERROR, "inner KDS at depth %u is not a valid KDS_FORMAT_HASH", d);
+            xb_inner *in = &plan->inner[d];
+            in->nitems = hk->nitems;
+            uint64_t cap = xb_next_pow2((uint64_t)hk->nitems * 2 + 64);
+            in->cap_mask = (uint32_t)(cap - 1);
+            in->unique_hash = 1;
+            uint32_t n = hk->nitems > 0 ? hk->nitems : 1;
+            uint32_t words = (n + 31) / 32;
+            uint32_t nl = in->nloads > 0 ? in->nloads : 1;
+            DALLOC(cap * 8, &in->index);
+            DALLOC((size_t)nl * n * 8, &in->vals);
+            DALLOC((size_t)nl * n * 4, &in->auxs);
+            DALLOC((size_t)nl * words * 4, &in->nulls);
+            cudaMemsetAsync(in->index, 0, cap * 8, st);
+            cudaMemsetAsync(in->nulls, 0, (size_t)nl * words * 4, st);
+        }
+    }
+    /* group-by tables */
+    if (plan->has_groupby) {
+        double est = ((const kern_session_info *)s->h_session.data())->groupby_ngroups_estimation;
+        if (!(est >= 1.0)) est = 1.0;
+        if (plan->has_groupby == 2) est = 1.0;
+        uint64_t cap = xb_next_pow2((uint64_t)(est * 4) + 1024);
+        uint64_t max_cap = (dev->hbm_budget / 4) / plan->gent_size;
+        if (cap > max_cap) cap = xb_next_pow2(max_cap / 2 + 1);
+        uint64_t arena = plan->nkeys_text ? (64ULL << 20) + cap * 32 : 256;
+        s->h_gt.cap_mask = cap - 1;
+        s->h_gt.nused = 0;
+        s->h_gt.arena_sz = arena;
+        s->h_gt.arena_used = 0;
+        s->h_gt.overflow = 0;
+        DALLOC(cap * plan->gent_size, &s->h_gt.entries);
+        DALLOC(arena, &s->h_gt.arena);
+        cudaMemsetAsync(s->h_gt.entries, 0, cap * plan->gent_size, st);
+        DALLOC(sizeof(xb_gtable), &s->d_gt);
+        cudaMemcpyAsync(s->d_gt, &s->h_gt, sizeof(xb_gtable), cudaMemcpyHostToDevice, st);
+        /* shared-memory table for small group counts */
+        if (est <= 2048 && plan->gent_size <= 256) {
+            uint32_t smc = (uint32_t)xb_next_pow2((uint64_t)(est * 4) + 16);
+            if (smc < 32) smc = 32;
+            while ((size_t)smc * plan->gent_size > 48 * 1024 && smc > 32) smc >>= 1;
+            if ((size_t)smc * plan->gent_size <= 48 * 1024)
+                s->sm_cap = smc;
+        }
+    }
+    DALLOC(sizeof(xb_plan), &s->d_plan);
+    cudaMemcpyAsync(s->d_plan, plan, sizeof(xb_plan), cudaMemcpyHostToDevice, st);
+
+    /* build inner indexes on the device */
+    for (uint32_t d = 1; d <= plan->nrels; d++) {
+        XbBuildArgs ba;
+        ba.kds = (const kern_data_store *)(s->d_kmrels + kmrels->chunks[d - 1].kds_offset);
+        ba.in = &s->d_plan->inner[d];
+        ba.st = s->d_status;
+        uint32_t n = plan->inner[d].nitems;
+        int grid = (int)((n + XB_BLOCK - 1) / XB_BLOCK);
+        if (grid < 1) grid = 1;
+        if (grid > dev->nsm * 8) grid = dev->nsm * 8;
+        xb_build_inner<<<grid, XB_BLOCK, 0, st>>>(ba);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));
+    cudaMemcpy(s->h_status, s->d_status, sizeof(xb_status), cudaMemcpyDeviceToHost);
+    if (s->h_status->errcode)
+        FAIL(s->h_status->errcode, "inner relation build: %s", xb_msg_text(s->h_status->msg_id));
+    /* refresh the host copy of the inner descriptors (unique_hash) */
+    cudaMemcpy(s->h_plan, s->d_plan, sizeof(xb_plan), cudaMemcpyDeviceToHost);
+
+    /* launch geometry */
+    s->regs_bytes = (uint32_t)PGSTROM_TYPEALIGN(16, (size_t)plan->nregs * (32 * 8 + 32 * 4 + 4) + 4 * XB_MASK_STACK + 16);
+    s->smem_bytes = sizeof(XbCol) * XB_MAX_COLS + (size_t)s->sm_cap * plan->gent_size +
+                    (size_t)XB_WARPS * s->regs_bytes;
+    if (cudaFuncSetAttribute(xb_exec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)s->smem_bytes) != cudaSuccess)
+        FAIL(ERRCODE_DEVICE_FATAL, "dynamic shared memory of %zu bytes not available", s->smem_bytes);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_exec_kernel, XB_BLOCK, s->smem_bytes);
+    if (per_sm < 1)
+        FAIL(ERRCODE_DEVICE_FATAL, "executor kernel does not fit on an SM (%zu bytes smem)", s->smem_bytes);
+    s->grid = per_sm * dev->nsm;
+#undef FAIL
+#undef DALLOC
+    *p_sess = s;
+    return 0;
+}
+
+extern "C" void
+xpuB200CloseSession(xpuB200Session *sess)
+{
+    if (sess)
+        xb_session_free(sess);
+}
+
+static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
+                          const kern_data_store *h_kds_head, kern_errorbuf *err)
+{
+    XbExecArgs a;
+    a.plan = s->d_plan;
+    a.kds = d_kds;
+    a.format = (uint32_t)h_kds_head->format;
+    if (a.format == KDS_FORMAT_BLOCK)
+        a.nunits = h_kds_head->nitems;
+    else if (a.format == KDS_FORMAT_ARROW || a.format == KDS_FORMAT_ROW)
+        a.nunits = (h_kds_head->nitems + XB_ROWS_UNIT - 1) / XB_ROWS_UNIT;
+    else
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", h_kds_head->format);
+    a.sm_cap = s->sm_cap;
+    a.regs_bytes = s->regs_bytes;
+    a.gt = s->d_gt;
+    a.st = s->d_status;
+    int grid = s->grid;
+    uint32_t warps_needed = (a.format == KDS_FORMAT_BLOCK) ? (a.nunits + XB_CLAIM - 1) / XB_CLAIM : a.nunits;
+    if ((uint32_t)grid * XB_WARPS > warps_needed)
+        grid = (int)((warps_needed + XB_WARPS - 1) / XB_WARPS);
+    if (grid < 1) grid = 1;
+    xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, s->dev->stream>>>(a);
+    cudaError_t rc = cudaGetLastError();
+    if (rc != cudaSuccess)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "kernel launch: %s", cudaGetErrorString(rc));
+    return 0;
+}
+
+static int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
+{
+    if (kds->format == KDS_FORMAT_BLOCK) {
+        if ((uint64_t)kds->block_offset + (uint64_t)PGSTROM_BLCKSZ * kds->nitems > kds->length ||
+            kds->block_offset < KDS_HEAD_LENGTH(kds))
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "KDS_FORMAT_BLOCK chunk is broken");
+    } else if (kds->format == KDS_FORMAT_ARROW || kds->format == KDS_FORMAT_ROW) {
+        if (KDS_HEAD_LENGTH(kds) > kds->length)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "chunk header is broken");
+    } else {
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", kds->format);
+    }
+    if (kds->format == KDS_FORMAT_ARROW) {
+        for (uint32_t j = 0; j < kds->ncols && j < kds->nr_colmeta; j++) {
+            const kern_colmeta *cm = &kds->colmeta[j];
+            if (cm->virtual_offset != 0)
+                continue;
+            if (cm->nullmap_offset + cm->nullmap_length > kds->length ||
+                cm->values_offset + cm->values_length > kds->length ||
+                cm->extra_offset + cm->extra_length > kds->length)
+                return XB_ERR(err, ERRCODE_DEVICE_ERROR, "Arrow column %u is out of the chunk", j);
+        }
+    }
+    return 0;
+}
+
+static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_errorbuf *err)
+{
+    cudaStream_t st = s->dev->stream;
+    cudaMemcpyAsync(s->h_status, s->d_status, sizeof(xb_status), cudaMemcpyDeviceToHost, st);
+    cudaError_t rc = cudaStreamSynchronize(st);
+    if (rc != cudaSuccess)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "ExecTask: %s", cudaGetErrorString(rc));
+    const xb_status *hs = s->h_status;
+    if (hs->errcode)
+        return xb_set_error(err, hs->errcode, "xb_exec_kernel", hs->lineno, "%s", xb_msg_text(hs->msg_id));
+    s->total_raw += hs->nitems_raw;
+    s->total_in += hs->nitems_in;
+    s->total_out += hs->nitems_out;
+    for (uint32_t d = 1; d <= s->h_plan->nrels; d++)
+        s->total_depth[d] += hs->nitems_depth[d];
+    if (results) {
+        uint32_t cap = results->num_rels;
+        results->nitems_raw = (uint32_t)hs->nitems_raw;
+        results->nitems_in = (uint32_t)hs->nitems_in;
+        results->nitems_out = (uint32_t)hs->nitems_out;
+        results->num_rels = s->h_plan->nrels;
+        for (uint32_t d = 1; d <= s->h_plan->nrels && d <= cap; d++) {
+            results->stats[d - 1].nitems_roj = 0;
+            results->stats[d - 1].nitems_gist = 0;
+            results->stats[d - 1].nitems_out = (uint32_t)hs->nitems_depth[d];
+        }
+    }
+    return 0;
+}
+
+extern "C" int
+xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
+                kern_exec_results *results, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s || !kds_src)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid ExecTask arguments");
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    cudaStream_t st = s->dev->stream;
+    kern_data_store head;
+    const kern_data_store *d_kds;
+    std::vector<char> hbuf;
+    if (kds_src_on_device) {
+        XB_CUDA(cudaMemcpy(&head, kds_src, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+        uint64_t hl = KDS_HEAD_LENGTH(&head);
+        hbuf.resize(hl);
+        XB_CUDA(cudaMemcpy(hbuf.data(), kds_src, hl, cudaMemcpyDeviceToHost), err);
+        int rc = xb_check_kds((const kern_data_store *)hbuf.data(), err);
+        if (rc) return rc;
+        d_kds = kds_src;
+    } else {
+        int rc = xb_check_kds(kds_src, err);
+        if (rc) return rc;
+        head = *kds_src;
+        /* place the chunk so that heap pages start on a 16-byte boundary */
+        uint64_t shift = (kds_src->format == KDS_FORMAT_BLOCK) ? ((16 - (kds_src->block_offset & 15)) & 15) : 0;
+        uint64_t need = kds_src->length + shift + 64;
+        if (need > s->d_src_cap) {
+            if (s->d_src) cudaFree(s->d_src);
+            s->d_src = nullptr;
+            s->d_src_cap = 0;
+            XB_CUDA(cudaMalloc((void **)&s->d_src, need + (need >> 3)), err);
+            s->d_src_cap = need + (need >> 3);
+        }
+        XB_CUDA(cudaMemcpyAsync(s->d_src + shift, kds_src, kds_src->length, cudaMemcpyHostToDevice, st), err);
+        d_kds = (const kern_data_store *)(s->d_src + shift);
+    }
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+    int rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
+    if (rc) return rc;
+    return xb_finish_task(s, results, err);
+}
+
+extern "C" int
+xpuB200TimeExecTask(xpuB200Session *s, const kern_data_store *kds_src_dev, int niters,
+                    double *p_msec, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    cudaStream_t st = s->dev->stream;
+    kern_data_store head;
+    XB_CUDA(cudaMemcpy(&head, kds_src_dev, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+    std::vector<char> hbuf(KDS_HEAD_LENGTH(&head));
+    XB_CUDA(cudaMemcpy(hbuf.data(), kds_src_dev, hbuf.size(), cudaMemcpyDeviceToHost), err);
+    int rc = xb_check_kds((const kern_data_store *)hbuf.data(), err);
+    if (rc) return rc;
+    float total = 0.0f;
+    for (int i = 0; i < niters; i++) {
+        XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+        cudaEventRecord(s->ev0, st);
+        rc = xb_launch_exec(s, kds_src_dev, (const kern_data_store *)hbuf.data(), err);
+        if (rc) return rc;
+        cudaEventRecord(s->ev1, st);
+        rc = xb_finish_task(s, nullptr, err);
+        if (rc) return rc;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        total += ms;
+    }
+    *p_msec = niters > 0 ? total / niters : 0.0;
+    return 0;
+}
+
+extern "C" int
+xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *p_required,
+             kern_exec_results *results, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid Final arguments");
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    cudaStream_t st = s->dev->stream;
+    const xb_plan *plan = s->h_plan;
+    if (results) {
+        uint32_t cap = results->num_rels;
+        results->nitems_raw = (uint32_t)s->total_raw;
+        results->nitems_in = (uint32_t)s->total_in;
+        results->nitems_out = (uint32_t)s->total_out;
+        results->num_rels = plan->nrels;
+        for (uint32_t d = 1; d <= plan->nrels && d <= cap; d++)
+            results->stats[d - 1].nitems_out = (uint32_t)s->total_depth[d];
+        results->final_plan_task = true;
+    }
+    if (!plan->has_groupby) {
+        if (p_required) *p_required = 0;
+        return 0;
+    }
+    const kern_session_info *session = (const kern_session_info *)s->h_session.data();
+    const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
+    const uint64_t head_len = KDS_HEAD_LENGTH(fh);
+    const uint64_t cap = s->h_gt.cap_mask + 1;
+
+    uint64_t *d_sizes = nullptr, *d_size_scan = nullptr;
+    uint32_t *d_flags = nullptr, *d_flag_scan = nullptr;
+    char *d_out = nullptr;
+    void *d_temp = nullptr;
+    size_t temp1 = 0, temp2 = 0;
+    int rc = 0;
+    std::vector<void *> tmp;
+    auto alloc = [&](size_t sz, void **p) -> bool {
+        if (cudaMalloc(p, sz < 256 ? 256 : sz) != cudaSuccess) { cudaGetLastError(); return false; }
+        tmp.push_back(*p);
+        return true;
+    };
+    auto cleanup = [&]() { for (void *p : tmp) cudaFree(p); };
+    if (!alloc(cap * 8, (void **)&d_sizes) || !alloc(cap * 8, (void **)&d_size_scan) ||
+        !alloc(cap * 4, (void **)&d_flags) || !alloc(cap * 4, (void **)&d_flag_scan)) {
+        cleanup();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in Final");
+    }
+    XbFinalArgs fa;
+    memset(&fa, 0, sizeof(fa));
+    fa.plan = s->d_plan;
+    fa.gt = s->d_gt;
+    fa.cap = cap;
+    fa.sizes = d_sizes;
+    fa.flags = d_flags;
+    fa.size_scan = d_size_scan;
+    fa.flag_scan = d_flag_scan;
+    int grid = s->dev->nsm * 8;
+    /* the global table's entries pointer lives in h_gt */
+    xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
+    cub::DeviceScan::ExclusiveSum(nullptr, temp1, d_sizes, d_size_scan, (int64_t)cap, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, temp2, d_flags, d_flag_scan, (int64_t)cap, st);
+    if (!alloc(temp1 > temp2 ? temp1 : temp2, &d_temp)) {
+        cleanup();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in Final");
+    }
+    size_t tsz = temp1 > temp2 ? temp1 : temp2;
+    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_sizes, d_size_scan, (int64_t)cap, st);
+    tsz = temp1 > temp2 ? temp1 : temp2;
+    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_flags, d_flag_scan, (int64_t)cap, st);
+    uint64_t last_size = 0, last_scan = 0;
+    uint32_t last_flag = 0, last_fscan = 0;
+    cudaMemcpyAsync(&last_size, d_sizes + cap - 1, 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last_scan, d_size_scan + cap - 1, 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last_flag, d_flags + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last_fscan, d_flag_scan + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cleanup();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "Final: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    const uint64_t items = last_scan + last_size;
+    const uint64_t ngroups = (uint64_t)last_fscan + last_flag;
+    const uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(ngroups);
+    const uint64_t items_base = head_len + 8 * nslots + 8 * ngroups;
+    const uint64_t length = items_base + items;
+    if (p_required) *p_required = length;
+    if (results) {
+        results->final_nitems = (uint32_t)ngroups;
+        results->final_usage = items;
+        results->final_total = length;
+    }
+    if (!kds_final_buf || buf_sz < length) {
+        cleanup();
+        if (!kds_final_buf && buf_sz == 0)
+            return 0;           /* size query only */
+        return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE, "kds_final needs %llu bytes (buffer %llu)",
+                      (unsigned long long)length, (unsigned long long)buf_sz);
+    }
+    if (!alloc(length, (void **)&d_out)) {
+        cleanup();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for kds_final (%llu bytes)",
+                      (unsigned long long)length);
+    }
+    /* header: the session's kds_final definition with the actual sizes */
+    std::vector<char> head((const char *)fh, (const char *)fh + head_len);
+    kern_data_store *kh = (kern_data_store *)head.data();
+    kh->length = length;
+    kh->usage = items;
+    kh->nitems = (uint32_t)ngroups;
+    kh->format = KDS_FORMAT_HASH;
+    kh->hash_nslots = (uint32_t)nslots;
+    cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(d_out + head_len, 0, 8 * nslots + 8 * ngroups, st);
+    fa.kds_final = d_out;
+    fa.items_base = items_base;
+    fa.length = length;
+    fa.nslots = (uint32_t)nslots;
+    xb_final_write<<<grid, XB_BLOCK, 0, st>>>(fa);
+    cudaMemcpyAsync(kds_final_buf, d_out, length, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "Final: %s", cudaGetErrorString(cudaGetLastError()));
+    cleanup();
+    return rc;
+}
+
+extern "C" int
+xpuB200HandleCommand(xpuB200Device *dev, xpuB200Session **p_sess, const XpuCommand *xcmd,
+                     const kern_multirels *kmrels, uint64_t kmrels_sz,
+                     XpuCommand *resp, uint64_t resp_sz)
+{
+    kern_errorbuf ebuf;
+    int rc = 0;
+    if (!xcmd || xcmd->magic != XpuCommandMagicNumber || !resp ||
+        resp_sz < offsetof(XpuCommand, u) + sizeof(kern_errorbuf))
+        return ERRCODE_DEVICE_ERROR;
+    memset(resp, 0, offsetof(XpuCommand, u));
+    resp->magic = XpuCommandMagicNumber;
+    const uint64_t head = offsetof(XpuCommand, u);
+    switch (xcmd->tag) {
+    case XpuCommandTag__OpenSession:
+        rc = xpuB200OpenSession(dev, &xcmd->u.session, xcmd->length - head, kmrels, kmrels_sz,
+                                p_sess, &ebuf);
+        if (!rc) {
+            resp->tag = XpuCommandTag__Success;
+            resp->length = head;
+        }
+        break;
+    case XpuCommandTag__XpuTaskExec: {
+        const kern_data_store *kds = (const kern_data_store *)((const char *)xcmd + xcmd->u.task.kds_src_offset);
+        if (!*p_sess || xcmd->u.task.kds_src_offset == 0 ||
+            xcmd->u.task.kds_src_offset + sizeof(kern_data_store) > xcmd->length ||
+            xcmd->u.task.kds_src_offset + kds->length > xcmd->length) {
+            rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "malformed XpuTaskExec command");
+            break;
+        }
+        uint32_t nrels = (*p_sess)->h_plan->nrels;
+        uint64_t rsz = head + offsetof(kern_exec_results, stats) + sizeof(resp->u.results.stats[0]) * (nrels + 1);
+        if (resp_sz < rsz) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
+        memset(&resp->u.results, 0, rsz - head);
+        resp->u.results.num_rels = nrels;
+        rc = xpuB200ExecTask(*p_sess, kds, 0, &resp->u.results, &ebuf);
+        if (!rc) {
+            resp->tag = XpuCommandTag__Success;
+            resp->length = rsz;
+        }
+        break;
+    }
+    case XpuCommandTag__XpuTaskFinal: {
+        if (!*p_sess) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "XpuTaskFinal without a session"); break; }
+        uint32_t nrels = (*p_sess)->h_plan->nrels;
+        uint64_t rhead = head + PGSTROM_MAXALIGN(offsetof(kern_exec_results, stats) +
+                                                 sizeof(resp->u.results.stats[0]) * (nrels + 1));
+        if (resp_sz < rhead) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
+        memset(&resp->u.results, 0, rhead - head);
+        resp->u.results.num_rels = nrels;
+        uint64_t required = 0;
+        rc = xpuB200Final(*p_sess, (char *)resp + rhead, resp_sz - rhead, &required,
+                          &resp->u.results, &ebuf);
+        if (!rc) {
+            resp->tag = XpuCommandTag__Success;
+            resp->u.results.chunks_offset = (uint32_t)rhead;
+            resp->u.results.chunks_nitems = required > 0 ? 1 : 0;
+            resp->u.results.final_plan_task = true;
+            resp->length = rhead + required;
+        }
+        break;
+    }
+    default:
+        rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "unknown XpuCommand tag %u", xcmd->tag);
+        break;
+    }
+    if (rc) {
+        resp->tag = XpuCommandTag__Error;
+        resp->length = head + sizeof(kern_errorbuf);
+        memcpy(&resp->u.error, &ebuf, sizeof(kern_errorbuf));
+    }
+    return rc;
+}
+
+extern "C" int
+xpuB200DeviceAlloc(xpuB200Device *dev, uint64_t sz, void **p_dptr)
+{
+    cudaSetDevice(dev->dindex);
+    if (cudaMalloc(p_dptr, sz) != cudaSuccess) { cudaGetLastError(); return ERRCODE_DEVICE_FATAL; }
+    return 0;
+}
+
+extern "C" int
+xpuB200DeviceFree(xpuB200Device *dev, void *dptr)
+{
+    cudaSetDevice(dev->dindex);
+    return cudaFree(dptr) == cudaSuccess ? 0 : ERRCODE_DEVICE_FATAL;
+}
+
+extern "C" int
+xpuB200CopyToDevice(xpuB200Device *dev, void *dptr, const void *src, uint64_t sz)
+{
+    cudaSetDevice(dev->dindex);
+    return cudaMemcpy(dptr, src, sz, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : ERRCODE_DEVICE_FATAL;
+}
+
+extern "C" int
+xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
+{
+    if (!s || !buf) return ERRCODE_DEVICE_ERROR;
+    const xb_plan *p = s->h_plan;
+    snprintf(buf, buf_sz,
+             "{\"nregs\": %u, \"nslots\": %u, \"nrels\": %u, \"ninsns\": %u, \"has_groupby\": %u, "
+             "\"nkeys\": %u, \"naggs\": %u, \"gent_size\": %u, \"gtable_cap\": %llu, "
+             "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u]}",
+             p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
+             p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
+             s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash);
+    return 0;
+}
+
+extern "C" uint32_t
+xpuB200HashBytes(const void *data, uint32_t len)
+{
+    return xb_hash_bytes((const uint8_t *)data, len);
+}

@@ -1,0 +1,281 @@
+/*
+ * xb_plan.h
+ *
+ * The compiled form of one PG-Strom session, as executed by the B200
+ * kernels.  OpenSession translates the kern_session_info bytecode
+ * (LoadVars / ScanQuals / HashValue / JoinQuals / GroupBy*) into this
+ * structure once; every ExecTask then runs it without re-reading the
+ * kern_expression trees.
+ *
+ * Execution model (device):
+ *   - one warp processes 32 source rows at a time (one row per lane);
+ *   - every kvars slot of the session is a VM register; registers live in
+ *     shared memory as [reg][lane] 64-bit cells plus a 32-bit aux word and
+ *     a per-register NULL ballot, so the interpreter's instruction stream
+ *     is warp-uniform (no divergence on dispatch);
+ *   - expression trees become straight-line register programs (xb_insn);
+ *     AND/OR keep SQL 3-valued semantics and short-circuit by narrowing the
+ *     lane mask instead of branching;
+ *   - hash joins probe a rebuilt open-addressing index over the inner
+ *     KDS_FORMAT_HASH rows, whose referenced columns are pre-decoded into
+ *     SoA register images at OpenSession;
+ *   - GROUP BY updates a per-CTA shared-memory table, spilling to a global
+ *     open-addressing table in HBM; Final materialises kds_final in the
+ *     reference's KDS_FORMAT_HASH / kagg_state__* layout.
+ */
+#ifndef XB_PLAN_H
+#define XB_PLAN_H
+#include <stdint.h>
+#include "pgstrom_abi.h"
+
+#define XB_MAX_REGS         48      /* kvars slots + temporaries */
+#define XB_MAX_DEPTH        6       /* inner relations per session */
+#define XB_MAX_LOADS        32      /* LoadVars descriptors per depth */
+#define XB_MAX_KEYS         8       /* GROUP BY keys */
+#define XB_MAX_AGGS         32      /* partial aggregate columns */
+#define XB_MAX_INSNS        384     /* VM instructions per session */
+#define XB_MAX_COLS         64      /* source columns decoded per tuple */
+#define XB_MASK_STACK       8
+
+/* register kinds */
+#define XB_RK_INT       1   /* bool/int2/int4/int8/date/time/timestamp as int64 */
+#define XB_RK_FLT       2   /* float8 as IEEE754 double */
+#define XB_RK_TEXT      3   /* payload pointer + length (aux) */
+#define XB_RK_NUM       4   /* pointer to a numeric varlena */
+
+/* how a register is loaded from a tuple attribute */
+#define XB_LD_BOOL      1
+#define XB_LD_INT2      2
+#define XB_LD_INT4      3
+#define XB_LD_INT8      4
+#define XB_LD_FLT8      5
+#define XB_LD_FLT4      6
+#define XB_LD_DATE      7
+#define XB_LD_TEXT      8   /* text / varchar / bpchar / bytea */
+#define XB_LD_NUMERIC   9
+
+/* VM opcodes */
+#define XB_OP_END           0
+#define XB_OP_CONST         1   /* dst <- imm (kind); aux=1 -> NULL; text: aux=len */
+#define XB_OP_MOVE          2   /* dst <- a */
+#define XB_OP_CMP           3   /* dst <- a <sub> b, kind = operand kind */
+#define XB_OP_ARITH         4   /* dst <- a <sub> b, checked */
+#define XB_OP_CAST          5   /* dst <- cast(a), sub = cast kind */
+#define XB_OP_NOT           6
+#define XB_OP_NULLTEST      7   /* sub: 0=IS NULL, 1=IS NOT NULL */
+#define XB_OP_BOOLTEST      8   /* sub: 0..5 = IsTrue..IsNotUnknown */
+#define XB_OP_BOOL_INIT     9   /* dst <- TRUE (sub=0, AND) / FALSE (sub=1, OR) */
+#define XB_OP_AND_ACC       10  /* dst <- dst AND a (3-valued) */
+#define XB_OP_OR_ACC        11  /* dst <- dst OR a (3-valued) */
+#define XB_OP_MASK_PUSH     12
+#define XB_OP_MASK_NARROW   13  /* sub 0: drop lanes where a IS FALSE; 1: where a IS TRUE */
+#define XB_OP_MASK_POP      14
+#define XB_OP_HASH_INIT     15  /* dst <- 0xffffffff */
+#define XB_OP_HASH_ADD      16  /* dst <- merge(dst, hash(a)); skips NULL; sub = hash kind */
+#define XB_OP_HASH_FINI     17  /* dst <- dst ^ 0xffffffff */
+#define XB_OP_DISTINCT      18  /* dst <- a IS DISTINCT FROM b (kind) */
+
+/* XB_OP_CMP sub-ops */
+#define XB_CMP_EQ   0
+#define XB_CMP_NE   1
+#define XB_CMP_LT   2
+#define XB_CMP_LE   3
+#define XB_CMP_GT   4
+#define XB_CMP_GE   5
+
+/* XB_OP_ARITH sub-ops: low nibble = operator, high nibble = result width */
+#define XB_AR_ADD   0
+#define XB_AR_SUB   1
+#define XB_AR_MUL   2
+#define XB_AR_DIV   3
+#define XB_AR_W2    (1 << 4)
+#define XB_AR_W4    (2 << 4)
+#define XB_AR_W8    (3 << 4)
+
+/* XB_OP_CAST sub-ops */
+#define XB_CAST_I2I2    1   /* to int2 with range check */
+#define XB_CAST_I2I4    2
+#define XB_CAST_I2I8    3
+#define XB_CAST_I2F8    4
+#define XB_CAST_F82I2   5
+#define XB_CAST_F82I4   6
+#define XB_CAST_F82I8   7
+#define XB_CAST_I2BOOL  8
+
+/* XB_OP_HASH_ADD kinds: byte width of the hashed value, or special */
+#define XB_HK_W1    1
+#define XB_HK_W2    2
+#define XB_HK_W4    4
+#define XB_HK_W8    8
+#define XB_HK_TEXT  20
+#define XB_HK_NUM   21
+
+typedef struct xb_insn {
+    uint8_t     op;
+    uint8_t     dst;
+    uint8_t     a;
+    uint8_t     b;
+    uint8_t     sub;
+    uint8_t     kind;
+    uint16_t    aux;
+    int64_t     imm;
+} xb_insn;
+
+typedef struct xb_prog {
+    uint16_t    start;      /* first instruction in xb_plan.insns */
+    uint16_t    count;      /* 0 = no program */
+    int16_t     result;     /* register holding the result, or -1 */
+    uint16_t    __pad;
+} xb_prog;
+
+typedef struct xb_load {
+    int16_t     resno;      /* attribute number (1-based; <0 system column) */
+    uint8_t     reg;
+    uint8_t     ld;         /* XB_LD_* */
+} xb_load;
+
+/* a pre-decoded inner relation (one join depth) */
+typedef struct xb_inner {
+    uint32_t    nitems;
+    uint32_t    cap_mask;       /* index capacity - 1 (power of two) */
+    uint32_t    unique_hash;    /* 1 if all inner hash values differ */
+    uint32_t    nloads;
+    uint64_t   *index;          /* (hash << 32) | (row + 1); 0 = empty */
+    uint64_t   *vals;           /* [nloads][nitems] register images */
+    uint32_t   *auxs;           /* [nloads][nitems] */
+    uint32_t   *nulls;          /* [nloads][(nitems+31)/32] bit = NULL */
+    xb_load     load[XB_MAX_LOADS];
+} xb_inner;
+
+/* one partial-aggregate (or grouping key) column of the kds_final tuple */
+typedef struct xb_agg {
+    uint16_t    action;         /* KAGG_ACTION__* */
+    int16_t     arg0;           /* register, or -1 */
+    int16_t     arg1;
+    int16_t     filter;         /* register of FILTER clause, or -1 */
+    int32_t     typmod;
+    uint16_t    state_off;      /* byte offset of the state in a group entry */
+    uint16_t    state_sz;
+    int16_t     weight;         /* numeric: __numeric_typmod_weight(typmod) */
+    int16_t     key_index;      /* VREF: index into keys[], else -1 */
+    /* kds_final column attributes */
+    int16_t     attlen;
+    int8_t      attalign;
+    int8_t      __pad;
+} xb_agg;
+
+typedef struct xb_key {
+    uint8_t     reg;
+    uint8_t     rk;             /* XB_RK_* */
+    uint8_t     ld;             /* XB_LD_* of the key type (for write-out) */
+    uint8_t     hk;             /* XB_HK_* */
+    uint16_t    off;            /* offset of the key image in a group entry */
+    uint16_t    __pad;
+} xb_key;
+
+typedef struct xb_plan {
+    uint32_t    magic;
+    uint32_t    plan_sz;
+    uint32_t    nregs;
+    uint32_t    nslots;
+    uint32_t    nrels;
+    uint32_t    task_kind;      /* DEVTASK__* bits */
+    uint8_t     rk[XB_MAX_REGS];
+
+    /* depth 0: source tuples */
+    uint32_t    nload0;
+    int32_t     max_resno0;
+    xb_load     load0[XB_MAX_LOADS];
+    xb_prog     scan_quals;
+
+    /* depth 1..nrels: hash joins */
+    xb_prog     hash_value[XB_MAX_DEPTH + 1];
+    xb_prog     join_quals[XB_MAX_DEPTH + 1];
+    xb_inner    inner[XB_MAX_DEPTH + 1];
+
+    /* group-by */
+    uint32_t    has_groupby;    /* 1: GROUP BY keys, 2: no-group aggregation */
+    xb_prog     gb_args;        /* SaveExpr argument evaluation */
+    xb_prog     gb_keyhash;
+    uint32_t    nkeys;
+    xb_key      keys[XB_MAX_KEYS];
+    uint32_t    naggs;
+    xb_agg      aggs[XB_MAX_AGGS];
+    uint32_t    gent_size;      /* bytes of one group entry (multiple of 16) */
+    uint32_t    gent_keys_off;
+    uint32_t    nkeys_text;     /* number of text/numeric keys (arena use) */
+
+    /* VM code */
+    uint32_t    ninsns;
+    xb_insn     insns[XB_MAX_INSNS];
+} xb_plan;
+
+#define XB_PLAN_MAGIC   0x78623230U     /* 'xb20' */
+
+/* group entry header (global and shared-memory tables) */
+#define XB_GSTATE_EMPTY 0u
+#define XB_GSTATE_BUSY  1u
+#define XB_GSTATE_READY 2u
+typedef struct xb_gent_head {
+    uint32_t    hash;
+    uint32_t    state;
+} xb_gent_head;
+
+/* key image inside a group entry: 16 bytes per key */
+typedef struct xb_keyimg {
+    uint64_t    val;        /* int/float bits, or pointer to the key bytes */
+    uint32_t    len;        /* text length */
+    uint32_t    isnull;
+} xb_keyimg;
+
+/* per-launch task descriptor (device) */
+typedef struct xb_task {
+    const kern_data_store *kds_src;
+    uint32_t    nunits;         /* pages (BLOCK) or 32-row groups (ARROW/ROW) */
+    uint32_t    format;
+    uint32_t    nrows;          /* rows for ARROW/ROW */
+    uint32_t    block_offset;
+} xb_task;
+
+/* global group table */
+typedef struct xb_gtable {
+    uint64_t    cap_mask;
+    uint64_t    nused;          /* number of claimed entries */
+    char       *entries;        /* cap * gent_size bytes */
+    char       *arena;          /* text/numeric key bytes */
+    uint64_t    arena_sz;
+    uint64_t    arena_used;
+    uint32_t    overflow;       /* set when the table or arena ran out */
+    uint32_t    __pad;
+} xb_gtable;
+
+/* execution statistics and error state, one per launch (device) */
+typedef struct xb_status {
+    uint32_t    errcode;
+    int32_t     lineno;
+    uint32_t    msg_id;
+    uint32_t    __pad;
+    uint64_t    unit_cursor;    /* work distribution counter */
+    uint64_t    nitems_raw;
+    uint64_t    nitems_in;
+    uint64_t    nitems_out;
+    uint64_t    nitems_depth[XB_MAX_DEPTH + 1];
+} xb_status;
+
+/* error message ids reported by device code */
+#define XB_MSG_NONE             0
+#define XB_MSG_INT_RANGE        1
+#define XB_MSG_DIV_ZERO         2
+#define XB_MSG_FLT_RANGE        3
+#define XB_MSG_NUMERIC_RANGE    4
+#define XB_MSG_NUMERIC_CORRUPT  5
+#define XB_MSG_VARLENA_EXTERNAL 6
+#define XB_MSG_BAD_TUPLE        7
+#define XB_MSG_GTABLE_FULL      8
+#define XB_MSG_WAIT_TIMEOUT     9
+#define XB_MSG_ARENA_FULL       10
+#define XB_MSG_BAD_PAGE         11
+#define XB_MSG_ARROW_TYPE       12
+#define XB_MSG_NUMERIC_TYPE     13
+
+#endif  /* XB_PLAN_H */

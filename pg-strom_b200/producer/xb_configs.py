@@ -1,0 +1,155 @@
+"""
+Seeded synthetic workloads with the shapes, sizes and value distributions of
+the benchmark configurations (test and benchmark infrastructure).
+
+  scan_groupby     heap table (id int8, a int4 U[0,1000), b float8 N(0,1)
+                   with 5% NULL, c numeric(12,2) U[0,10000), g int4 U[0,64));
+                   WHERE a < 300 GROUP BY g -> count(*), sum(a), sum(c), avg(b)
+  join_groupby     fact(fk1, fk2, qty int4 U[1,50], price int8 U[100,1e6])
+                   with fk1 U[1,200000] into dim1(pk int4, region text: 25
+                   values of 8-16 bytes) and fk2 bounded-Zipf(s=1.1) over
+                   1..10000 into dim2(pk int4, flag int2 in 0..4);
+                   JOIN dim1, dim2 WHERE flag < 3 GROUP BY region ->
+                   sum(qty*price), count(*)
+
+Every generator also returns the expected per-group aggregates computed
+directly from the column arrays with numpy (independent of any page or
+bytecode decoding), so the oracle itself can be pinned against them.
+"""
+import numpy as np
+
+from xb_producer import (Table, Column, Var, Const, Func, Agg, SessionBuilder,
+                         encode_numeric_array, encode_text_array, encode_text_from_dict,
+                         hash_u32_array, hash_merge_array, kern_multirels, numeric_typmod)
+
+DEVKIND_GPU = 0x00000001
+DEVTASK_SCAN = 0x10000000
+DEVTASK_JOIN = 0x20000000
+DEVTASK_PREAGG = 0x40000000
+
+SEED_BASE = 0x5EED0000
+
+
+def rng_for(config, table):
+    return np.random.Generator(np.random.PCG64(SEED_BASE + config * 16 + table))
+
+
+def host_join_hash_int4(keys: np.ndarray) -> np.ndarray:
+    """get_tuple_hashvalue for one int4 key (gpu_join.c:1549-1584)."""
+    h = hash_merge_array(np.full(len(keys), 0xFFFFFFFF, dtype=np.uint32), hash_u32_array(keys, 4))
+    return h ^ np.uint32(0xFFFFFFFF)
+
+
+# ---------------------------------------------------------------------------
+def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300):
+    r = rng_for(seed_config, 0)
+    id_ = np.arange(nrows, dtype=np.int64)
+    a = r.integers(0, 1000, nrows, dtype=np.int32)
+    b = r.standard_normal(nrows)
+    bnull = r.random(nrows) < null_frac
+    c_unscaled = r.integers(0, 1_000_000, nrows, dtype=np.int64)
+    g = r.integers(0, 64, nrows, dtype=np.int32)
+    typmod_c = numeric_typmod(12, 2)
+    tbl = Table("t0", [
+        Column("id", "int8", values=id_),
+        Column("a", "int4", values=a),
+        Column("b", "float8", values=b, nulls=bnull),
+        Column("c", "numeric", typmod=typmod_c, values=encode_numeric_array(c_unscaled, 2)),
+        Column("g", "int4", values=g),
+    ], nrows)
+    va, vb, vc, vg = (Var(0, 2, "int4"), Var(0, 3, "float8"),
+                      Var(0, 4, "numeric", typmod_c), Var(0, 5, "int4"))
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    session = sb.build(
+        scan_quals=Func("int4lt", [va, Const("int4", a_limit)], "bool"),
+        groupby_keys=[vg],
+        aggs=[Agg("NROWS_ANY"),
+              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")),
+              Agg("PSUM_NUMERIC", vc, typmod_c),
+              Agg("PAVG_FP", vb)],
+        ngroups_estimate=64.0)
+    # expected partial states per group, straight from the arrays
+    m = a < a_limit
+    expect = {}
+    cnt = np.bincount(g[m], minlength=64)
+    suma = np.bincount(g[m], weights=None, minlength=64)
+    sa = np.zeros(64, dtype=np.int64)
+    np.add.at(sa, g[m], a[m].astype(np.int64))
+    sc = np.zeros(64, dtype=object)
+    sc[:] = 0
+    for k in range(64):
+        sc[k] = int(c_unscaled[m & (g == k)].sum())
+    mb = m & ~bnull
+    sb_ = np.zeros(64, dtype=np.float64)
+    np.add.at(sb_, g[mb], b[mb])                 # sequential, row order
+    nb = np.bincount(g[mb], minlength=64)
+    for k in range(64):
+        if cnt[k] == 0:
+            continue
+        expect[(k,)] = {"nrows": int(cnt[k]), "sum_a": (int(cnt[k]), int(sa[k])),
+                        "sum_c": (int(cnt[k]), sc[k], 2), "avg_b": (int(nb[k]), float(sb_[k]))}
+    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()),
+            "agg_names": ["nrows", "sum_a", "sum_c", "avg_b"], "nkeys": 1}
+    return tbl, session, None, expect, meta
+
+
+REGIONS = [("region_%02d" % i) + "abcdefg"[: (i * 3) % 8] for i in range(25)]
+
+
+def zipf_bounded(r, n, s, size):
+    """Bounded Zipf over 1..n with exponent s via its explicit CDF."""
+    w = 1.0 / np.arange(1, n + 1, dtype=np.float64) ** s
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    u = r.random(size)
+    return (np.searchsorted(cdf, u, side="right") + 1).astype(np.int32)
+
+
+def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3):
+    r1 = rng_for(seed_config, 1)
+    r2 = rng_for(seed_config, 2)
+    rf = rng_for(seed_config, 0)
+    # dimensions
+    pk1 = np.arange(1, ndim1 + 1, dtype=np.int32)
+    reg_code = r1.integers(0, len(REGIONS), ndim1)
+    dim1 = Table("dim1", [Column("pk", "int4", values=pk1),
+                          Column("region", "text", values=encode_text_from_dict(reg_code, REGIONS))], ndim1)
+    pk2 = np.arange(1, ndim2 + 1, dtype=np.int32)
+    flag = r2.integers(0, 5, ndim2, dtype=np.int16)
+    dim2 = Table("dim2", [Column("pk", "int4", values=pk2), Column("flag", "int2", values=flag)], ndim2)
+    # fact
+    fk1 = rf.integers(1, ndim1 + 1, nfact, dtype=np.int32)
+    fk2 = zipf_bounded(rf, ndim2, 1.1, nfact)
+    qty = rf.integers(1, 51, nfact, dtype=np.int32)
+    price = rf.integers(100, 1_000_001, nfact, dtype=np.int64)
+    fact = Table("fact", [Column("fk1", "int4", values=fk1), Column("fk2", "int4", values=fk2),
+                          Column("qty", "int4", values=qty), Column("price", "int8", values=price)], nfact)
+    kmrels = kern_multirels([dim1.hash_kds(host_join_hash_int4(pk1)),
+                             dim2.hash_kds(host_join_hash_int4(pk2))])
+    f_fk1, f_fk2, f_qty, f_price = (Var(0, 1, "int4"), Var(0, 2, "int4"),
+                                    Var(0, 3, "int4"), Var(0, 4, "int8"))
+    d1_pk, d1_region = Var(1, 1, "int4"), Var(1, 2, "text")
+    d2_pk, d2_flag = Var(2, 1, "int4"), Var(2, 2, "int2")
+    sb = SessionBuilder(2, DEVTASK_JOIN | DEVTASK_PREAGG | DEVKIND_GPU)
+    session = sb.build(
+        joins=[([f_fk1], [Func("int4eq", [f_fk1, d1_pk], "bool")], []),
+               ([f_fk2], [Func("int4eq", [f_fk2, d2_pk], "bool")],
+                [Func("int24lt", [d2_flag, Const("int4", flag_limit)], "bool")])],
+        groupby_keys=[d1_region],
+        aggs=[Agg("PSUM_INT64", Func("int48mul", [f_qty, f_price], "int8")),
+              Agg("NROWS_ANY")],
+        ngroups_estimate=25.0)
+    # expected
+    region_row = reg_code[fk1 - 1]
+    m = flag[fk2 - 1] < flag_limit
+    expect = {}
+    amount = qty.astype(np.int64) * price
+    for k in range(len(REGIONS)):
+        sel = m & (region_row == k)
+        n = int(sel.sum())
+        if n == 0:
+            continue
+        expect[(REGIONS[k].encode(),)] = {"sum_amount": (n, int(amount[sel].sum())), "nrows": n}
+    meta = {"nitems_raw": nfact, "nitems_in": nfact, "nitems_out": int(m.sum()),
+            "depth_out": [nfact, int(m.sum())], "agg_names": ["sum_amount", "nrows"], "nkeys": 1}
+    return fact, session, kmrels, expect, meta

@@ -1,0 +1,178 @@
+"""
+Python binding of the C ABI in include/xpu_b200.h (ctypes).
+
+The product is libxpu_b200.so; this module only marshals buffers for tests
+and the benchmark.  Loading fails loudly when the library is missing: there
+is no fallback implementation.
+"""
+import ctypes
+import os
+import struct
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxpu_b200.so")
+
+ERRCODE = {0: "SUCCESS", ord("E"): "DEVICE_ERROR", ord("F"): "DEVICE_FATAL",
+           ord("d"): "SUSPEND_NO_SPACE", ord("f"): "SUSPEND_FALLBACK"}
+
+
+class KernErrorbuf(ctypes.Structure):
+    _fields_ = [("errcode", ctypes.c_uint32), ("lineno", ctypes.c_int32),
+                ("filename", ctypes.c_char * 33), ("funcname", ctypes.c_char * 65),
+                ("message", ctypes.c_char * 201)]
+
+
+class XpuB200Error(RuntimeError):
+    def __init__(self, rc, ebuf):
+        self.errcode = rc
+        self.message = ebuf.message.decode(errors="replace")
+        super().__init__(f"[{ERRCODE.get(rc, rc)}] {ebuf.funcname.decode()}:{ebuf.lineno} {self.message}")
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with pg-strom_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        P, U64, I = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+        EB = ctypes.POINTER(KernErrorbuf)
+        L.xpuB200Init.argtypes = [I, U64, ctypes.POINTER(P), EB]
+        L.xpuB200Shutdown.argtypes = [P]
+        L.xpuB200OpenSession.argtypes = [P, P, U64, P, U64, ctypes.POINTER(P), EB]
+        L.xpuB200ExecTask.argtypes = [P, P, I, P, EB]
+        L.xpuB200Final.argtypes = [P, P, U64, ctypes.POINTER(U64), P, EB]
+        L.xpuB200CloseSession.argtypes = [P]
+        L.xpuB200HandleCommand.argtypes = [P, ctypes.POINTER(P), P, P, U64, P, U64]
+        L.xpuB200DeviceAlloc.argtypes = [P, U64, ctypes.POINTER(P)]
+        L.xpuB200DeviceFree.argtypes = [P, P]
+        L.xpuB200CopyToDevice.argtypes = [P, P, P, U64]
+        L.xpuB200TimeExecTask.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_double), EB]
+        L.xpuB200SessionInfo.argtypes = [P, ctypes.c_char_p, U64]
+        L.xpuB200HashBytes.argtypes = [P, ctypes.c_uint32]
+        L.xpuB200HashBytes.restype = ctypes.c_uint32
+        _LIB = L
+    return _LIB
+
+
+def _ptr(buf):
+    if isinstance(buf, np.ndarray):
+        return ctypes.c_void_p(buf.ctypes.data)
+    if isinstance(buf, (bytes, bytearray)):
+        return ctypes.cast(ctypes.c_char_p(bytes(buf)), ctypes.c_void_p)
+    raise TypeError(type(buf))
+
+
+def results_buffer(nrels):
+    return np.zeros(96 + 12 * (nrels + 1) + 16, dtype=np.uint8)
+
+
+def parse_results(buf):
+    b = bytes(buf)
+    nraw, nin, nout, nrels = struct.unpack_from("<IIII", b, 80)
+    stats = [struct.unpack_from("<III", b, 96 + 12 * i)[2] for i in range(nrels)]
+    final_nitems, = struct.unpack_from("<I", b, 24)
+    return {"nitems_raw": nraw, "nitems_in": nin, "nitems_out": nout, "num_rels": nrels,
+            "depth_out": stats, "final_nitems": final_nitems}
+
+
+class Device:
+    def __init__(self, dindex=0, hbm_budget=0):
+        self.h = ctypes.c_void_p()
+        e = KernErrorbuf()
+        rc = lib().xpuB200Init(dindex, hbm_budget, ctypes.byref(self.h), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+
+    def alloc(self, nbytes):
+        p = ctypes.c_void_p()
+        if lib().xpuB200DeviceAlloc(self.h, nbytes, ctypes.byref(p)):
+            raise MemoryError(f"device allocation of {nbytes} bytes failed")
+        return p.value
+
+    def free(self, dptr):
+        lib().xpuB200DeviceFree(self.h, ctypes.c_void_p(dptr))
+
+    def upload(self, arr: np.ndarray, align_pages=True):
+        """Copy a KDS chunk into device memory; heap pages land 16B aligned."""
+        shift = 0
+        if align_pages and arr.size > 48:
+            fmt = bytes(arr[24:25])
+            if fmt == b"b":
+                block_offset = int(np.frombuffer(arr[44:48].tobytes(), dtype=np.uint32)[0])
+                shift = (16 - (block_offset & 15)) & 15
+        base = self.alloc(arr.nbytes + 256)
+        if lib().xpuB200CopyToDevice(self.h, ctypes.c_void_p(base + shift), _ptr(arr), arr.nbytes):
+            raise RuntimeError("upload failed")
+        return base, base + shift
+
+    def close(self):
+        if self.h:
+            lib().xpuB200Shutdown(self.h)
+            self.h = ctypes.c_void_p()
+
+
+class Session:
+    def __init__(self, dev: Device, session: bytes, kmrels: np.ndarray = None, nrels=0):
+        self.dev = dev
+        self.nrels = nrels
+        self.h = ctypes.c_void_p()
+        self._session = np.frombuffer(session, dtype=np.uint8).copy()
+        self._kmrels = kmrels
+        e = KernErrorbuf()
+        rc = lib().xpuB200OpenSession(dev.h, _ptr(self._session), self._session.nbytes,
+                                      _ptr(kmrels) if kmrels is not None else None,
+                                      kmrels.nbytes if kmrels is not None else 0,
+                                      ctypes.byref(self.h), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+
+    def exec(self, kds, on_device=False):
+        res = results_buffer(self.nrels)
+        struct.pack_into("<I", res, 92, self.nrels)
+        e = KernErrorbuf()
+        p = ctypes.c_void_p(kds) if on_device else _ptr(kds)
+        rc = lib().xpuB200ExecTask(self.h, p, 1 if on_device else 0, _ptr(res), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return parse_results(res)
+
+    def time_exec(self, dptr, niters):
+        ms = ctypes.c_double()
+        e = KernErrorbuf()
+        rc = lib().xpuB200TimeExecTask(self.h, ctypes.c_void_p(dptr), niters, ctypes.byref(ms), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return ms.value
+
+    def final(self):
+        req = ctypes.c_uint64()
+        res = results_buffer(self.nrels)
+        struct.pack_into("<I", res, 92, self.nrels)
+        e = KernErrorbuf()
+        rc = lib().xpuB200Final(self.h, None, 0, ctypes.byref(req), _ptr(res), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        if req.value == 0:
+            return None, parse_results(res)
+        buf = np.zeros(req.value, dtype=np.uint8)
+        rc = lib().xpuB200Final(self.h, _ptr(buf), buf.nbytes, ctypes.byref(req), _ptr(res), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return buf, parse_results(res)
+
+    def info(self):
+        import json
+        b = ctypes.create_string_buffer(1024)
+        lib().xpuB200SessionInfo(self.h, b, 1024)
+        return json.loads(b.value.decode())
+
+    def close(self):
+        if self.h:
+            lib().xpuB200CloseSession(self.h)
+            self.h = ctypes.c_void_p()

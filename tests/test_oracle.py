@@ -1,0 +1,46 @@
+"""The oracle against ground truth computed directly from the generator's
+column arrays (no page or bytecode decoding on that side)."""
+import xb_configs as C
+import xb_final as F
+import xb_oracle as O
+
+
+def _want_c0(expect):
+    return {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
+
+
+def _want_c1(expect):
+    return {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+
+
+def test_oracle_scan_groupby():
+    tbl, sess, _, expect, meta = C.scan_groupby(nrows=150_000)
+    o = O.Oracle(sess)
+    for ch in tbl.block_chunks(pages_per_chunk=300):
+        o.exec(ch)
+    st = o.stats()
+    assert st["nitems_raw"] == meta["nitems_raw"] and st["nitems_in"] == meta["nitems_in"]
+    assert F.compare_groups(F.decode_kds_final(o.final(), sess), _want_c0(expect)) == []
+    o.close()
+
+
+def test_oracle_join_groupby():
+    fact, sess, km, expect, meta = C.join_groupby(nfact=200_000, ndim1=5000, ndim2=700)
+    o = O.Oracle(sess, km)
+    for ch in fact.block_chunks(pages_per_chunk=700):
+        o.exec(ch)
+    st = o.stats()
+    assert st["nitems_out"] == meta["nitems_out"]
+    assert st["depth_out"][:2] == meta["depth_out"]
+    assert F.compare_groups(F.decode_kds_final(o.final(), sess), _want_c1(expect)) == []
+    o.close()
+
+
+def test_oracle_all_filtered_out():
+    tbl, sess, _, expect, meta = C.scan_groupby(nrows=5000, a_limit=0)
+    o = O.Oracle(sess)
+    for ch in tbl.block_chunks():
+        o.exec(ch)
+    assert expect == {}
+    assert F.decode_kds_final(o.final(), sess) == {}
+    o.close()
