@@ -1,0 +1,90 @@
+"""Pins the oracle to PG-Strom's own code: hash_any, numeric decode and a
+full scan/join/group-by pass evaluated by the reference's host-compiled
+expression library over the same chunks and bytecode.  Skipped where
+oracle/_ref was not built (it needs the reference sources)."""
+import numpy as np
+import pytest
+
+import ref_pin
+import xb_configs as C
+import xb_final as F
+import xb_oracle as O
+import xb_producer as P
+
+pytestmark = pytest.mark.skipif(not ref_pin.available(), reason="oracle/_ref not built")
+
+
+def test_hash_any_matches_reference():
+    r = np.random.default_rng(11)
+    for n in list(range(0, 48)) + [100, 255, 1000]:
+        d = r.integers(0, 256, n, dtype=np.uint8).tobytes()
+        assert ref_pin.hash_any(d) == P.hash_any(d) == O.hash_bytes(d)
+
+
+def test_numeric_encoding_matches_reference():
+    r = np.random.default_rng(12)
+    vals = [0, 1, -1, 5, 10, 100, 9999, 10000, 123456, 999999, -999999, 1000000, 12300]
+    vals += list(r.integers(-10**9, 10**9, 200))
+    for scale in (0, 2, 4):
+        for v in vals:
+            got = ref_pin.numeric_decode(P.encode_numeric(int(v), scale))
+            assert got is not None
+            kind, w, iv = got
+            assert kind == 0
+            # value == v * 10^-scale
+            assert iv * 10 ** (scale - w if scale >= w else 0) == v * 10 ** (w - scale if w > scale else 0)
+        blob, offs = P.encode_numeric_array(np.array(vals[:50], dtype=np.int64) % 10**7, scale)
+        for i in range(50):
+            assert bytes(blob[offs[i]:offs[i + 1]]) == P.encode_numeric(int(vals[i] % 10**7), scale)
+
+
+def _ref_groups(res, aggs, keytypes):
+    out = {}
+    for g in res["groups"]:
+        keys = []
+        for hexv, tc in zip(g["keys"], keytypes):
+            if hexv is None:
+                keys.append(None)
+                continue
+            b = bytes.fromhex(hexv)
+            if tc == 11:
+                keys.append(b[4:])
+            else:
+                keys.append(int.from_bytes(b, "little", signed=True))
+        states = []
+        for st, (action, _, typmod) in zip(g["states"], [a for a in aggs if a[0] != 101]):
+            if action in (201, 202):
+                states.append(st)
+            elif action in (503, 603):
+                states.append((st[0], float(st[1])))
+            elif action in (504, 604):
+                w = (((typmod - 4) & 0x7FF) ^ 1024) - 1024 if typmod >= 0 else 15
+                states.append((st[0], int(st[1]), max(0, min(15, w))))
+            else:
+                states.append((st[0], int(st[1])))
+        out[tuple(keys)] = states
+    return out
+
+
+@pytest.mark.parametrize("which", ["scan", "join"])
+def test_oracle_matches_reference_functions(which):
+    if which == "scan":
+        tbl, sess, km, expect, meta = C.scan_groupby(nrows=60_000)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    else:
+        tbl, sess, km, expect, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    res = ref_pin.run(sess, chunks, km)
+    assert res["nitems_raw"] == meta["nitems_raw"]
+    assert res["nitems_in"] == meta["nitems_in"]
+    assert res["nitems_out"] == meta["nitems_out"]
+    aggs = F.session_aggs(sess)
+    stypes = F.slot_types(sess)
+    keytypes = [stypes[a0] for (act, a0, _) in aggs if act == 101]
+    ref = _ref_groups(res, aggs, keytypes)
+    o = O.Oracle(sess, km)
+    for ch in chunks:
+        o.exec(ch)
+    mine = F.decode_kds_final(o.final(), sess)
+    o.close()
+    assert F.compare_groups(mine, ref, rtol=0.0) == []
