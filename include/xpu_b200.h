@@ -99,6 +99,24 @@ int  xpuB200HandleCommand(xpuB200Device *dev, xpuB200Session **p_sess,
                           const kern_multirels *kmrels, uint64_t kmrels_sz,
                           XpuCommand *resp, uint64_t resp_sz);
 
+/*
+ * Prepared batches (the batched form of XpuTaskExec): many device-resident
+ * chunks of one session, validated once, executed by ONE persistent kernel
+ * launch whose warps claim work units (heap pages / 1024-row groups) from a
+ * device queue spanning all chunks.  The reference issues one
+ * kern_gpujoin_main launch plus a stream synchronisation per 64 MB chunk
+ * (gpu_service.c:3934-3948); a batch replaces those with a single launch.
+ * All chunks must share the session's column layout and KDS format.
+ */
+typedef struct xpuB200Batch xpuB200Batch;
+int  xpuB200BatchCreate(xpuB200Session *sess, const kern_data_store *const *kds_dev,
+                        uint32_t nchunks, xpuB200Batch **p_batch, kern_errorbuf *err);
+int  xpuB200BatchExec(xpuB200Batch *batch, kern_exec_results *results, kern_errorbuf *err);
+/* runs the batch niters times; average kernel milliseconds (CUDA events on
+ * the session stream) in *p_msec */
+int  xpuB200BatchTime(xpuB200Batch *batch, int niters, double *p_msec, kern_errorbuf *err);
+void xpuB200BatchDestroy(xpuB200Batch *batch);
+
 /* Device memory helpers for callers that keep chunks resident in HBM. */
 int  xpuB200DeviceAlloc(xpuB200Device *dev, uint64_t sz, void **p_dptr);
 int  xpuB200DeviceFree(xpuB200Device *dev, void *dptr);

@@ -30,6 +30,8 @@
 
 namespace {
 
+struct Sig { int op; uint8_t vmop; uint8_t sub; uint8_t kind; uint8_t nargs; };
+
 struct Compiler {
     const kern_session_info *session;
     size_t      session_sz;
@@ -241,6 +243,59 @@ struct Compiler {
         return r;
     }
 
+    /* true if evaluating kexp can neither raise an error nor dereference
+     * memory, so it may run on lanes whose earlier AND/OR argument already
+     * decided the result (no lane-mask narrowing needed) */
+    bool is_safe(const kern_expression *kexp, int depth = 0)
+    {
+        if (depth > 16)
+            return false;
+        switch (kexp->opcode) {
+        case FuncOpCode__ConstExpr:
+        case FuncOpCode__ParamExpr:
+        case FuncOpCode__VarExpr:
+            return true;
+        case FuncOpCode__NullTestExpr_IsNull:
+        case FuncOpCode__NullTestExpr_IsNotNull:
+        case FuncOpCode__BoolExpr_Not:
+        case FuncOpCode__BoolExpr_And:
+        case FuncOpCode__BoolExpr_Or:
+            break;
+        default: {
+            Sig s = {0, 0, 0, 0, 0};
+            if (!lookup(kexp->opcode, &s) || s.vmop != XB_OP_CMP ||
+                s.kind == XB_RK_TEXT || s.kind == XB_RK_NUM)
+                return false;
+            break;
+        }
+        }
+        const kern_expression *karg = first_arg(kexp);
+        for (uint32_t i = 0; i < kexp->nr_args; i++) {
+            if (!karg || !is_safe(karg, depth + 1))
+                return false;
+            if (i + 1 < kexp->nr_args)
+                karg = next_arg(kexp, karg);
+        }
+        return true;
+    }
+
+    /* fixed-width constant operand usable as an immediate */
+    bool const_imm(const kern_expression *kexp, int64_t *imm)
+    {
+        if (kexp->opcode != FuncOpCode__ConstExpr || kexp->u.c.const_isnull)
+            return false;
+        const char *addr = kexp->u.c.const_value;
+        const char *end = (const char *)kexp + kexp->len - sizeof(uint32_t);
+        switch (kexp->exptype) {
+        case TypeOpCode__int2: { int16_t v; if (end - addr < 2) return false; memcpy(&v, addr, 2); *imm = v; return true; }
+        case TypeOpCode__int4:
+        case TypeOpCode__date: { int32_t v; if (end - addr < 4) return false; memcpy(&v, addr, 4); *imm = v; return true; }
+        case TypeOpCode__int8:
+        case TypeOpCode__float8: { if (end - addr < 8) return false; memcpy(imm, addr, 8); return true; }
+        default: return false;
+        }
+    }
+
     /* ---- expression translation: returns the result register ---- */
     int expr(const kern_expression *kexp)
     {
@@ -278,8 +333,10 @@ struct Compiler {
                 return fail("malformed BoolExpr"), -1;
             int t = new_temp(XB_RK_INT);
             if (t < 0) return -1;
+            const bool masked = !is_safe(kexp);
             emit(XB_OP_BOOL_INIT, t, 0, 0, is_and ? 0 : 1);
-            emit(XB_OP_MASK_PUSH, 0);
+            if (masked)
+                emit(XB_OP_MASK_PUSH, 0);
             const kern_expression *karg = first_arg(kexp);
             for (uint32_t i = 0; i < kexp->nr_args; i++) {
                 if (!karg) return fail("BoolExpr argument %u is broken", i), -1;
@@ -289,11 +346,13 @@ struct Compiler {
                 if (r < 0) return -1;
                 emit(is_and ? XB_OP_AND_ACC : XB_OP_OR_ACC, t, r);
                 if (i + 1 < kexp->nr_args) {
-                    emit(XB_OP_MASK_NARROW, 0, r, 0, is_and ? 0 : 1);
+                    if (masked)
+                        emit(XB_OP_MASK_NARROW, 0, r, 0, is_and ? 0 : 1);
                     karg = next_arg(kexp, karg);
                 }
             }
-            emit(XB_OP_MASK_POP, 0);
+            if (masked)
+                emit(XB_OP_MASK_POP, 0);
             return t;
         }
         case FuncOpCode__BoolExpr_Not: {
@@ -346,6 +405,19 @@ struct Compiler {
             return slot;
         }
         case FuncOpCode__HashValue: {
+            if (kexp->nr_args == 1) {
+                const kern_expression *karg = first_arg(kexp);
+                int rk, ld, hk;
+                if (!karg) return fail("HashValue argument is broken"), -1;
+                if (!type_info(karg->exptype, &rk, &ld, &hk))
+                    return fail("HashValue on unsupported type %d", karg->exptype), -1;
+                int r = expr(karg);
+                if (r < 0) return -1;
+                int t1 = new_temp(XB_RK_INT);
+                if (t1 < 0) return -1;
+                emit(XB_OP_HASH1, t1, r, 0, hk, rk);
+                return t1;
+            }
             int t = new_temp(XB_RK_INT);
             if (t < 0) return -1;
             emit(XB_OP_HASH_INIT, t);
@@ -389,7 +461,6 @@ struct Compiler {
     int func(const kern_expression *kexp)
     {
         int op = kexp->opcode;
-        struct Sig { int op; uint8_t vmop; uint8_t sub; uint8_t kind; uint8_t nargs; };
         Sig s = {0, 0, 0, 0, 0};
         if (!lookup(op, &s))
             return fail("device function opcode %d is not supported", op), -1;
@@ -397,6 +468,18 @@ struct Compiler {
             return fail("opcode %d expects %d arguments", op, s.nargs), -1;
         int regs[2] = {0, 0};
         const kern_expression *karg = first_arg(kexp);
+        if (s.vmop == XB_OP_CMP && (s.kind == XB_RK_INT || s.kind == XB_RK_FLT) && s.nargs == 2 && karg) {
+            const kern_expression *k2 = next_arg(kexp, karg);
+            int64_t imm;
+            if (k2 && const_imm(k2, &imm)) {
+                int a = expr(karg);
+                if (a < 0) return -1;
+                int t = new_temp(XB_RK_INT);
+                if (t < 0) return -1;
+                emit(XB_OP_CMPI, t, a, 0, s.sub, s.kind, 0, imm);
+                return t;
+            }
+        }
         for (int i = 0; i < s.nargs; i++) {
             if (!karg) return fail("argument %d of opcode %d is broken", i, op), -1;
             regs[i] = expr(karg);
@@ -491,7 +574,6 @@ struct Compiler {
         int r = expr(kexp);
         if (r < 0)
             return false;
-        emit(XB_OP_END, 0);
         prog->count = (uint16_t)(plan->ninsns - prog->start);
         prog->result = (int16_t)r;
         if ((uint32_t)ntemps > plan->nregs)
@@ -510,10 +592,31 @@ struct Compiler {
         if (kexp->opcode != FuncOpCode__JoinQuals || kexp->exptype != TypeOpCode__bool)
             return fail("malformed JoinQuals");
         ntemps = plan->nslots;
+        if (kexp->nr_args == 1) {
+            const kern_expression *k1 = first_arg(kexp);
+            if (!k1 || k1->exptype != TypeOpCode__bool)
+                return fail("JoinQuals argument is broken");
+            int r = expr(k1);
+            if (r < 0) return false;
+            prog->count = (uint16_t)(plan->ninsns - prog->start);
+            prog->result = (int16_t)r;
+            if ((uint32_t)ntemps > plan->nregs)
+                plan->nregs = ntemps;
+            return err.empty();
+        }
+        bool masked = false;
+        {
+            const kern_expression *k = first_arg(kexp);
+            for (uint32_t i = 0; i < kexp->nr_args && k; i++) {
+                if (!is_safe(k)) masked = true;
+                if (i + 1 < kexp->nr_args) k = next_arg(kexp, k);
+            }
+        }
         int t = new_temp(XB_RK_INT);
         if (t < 0) return false;
         emit(XB_OP_BOOL_INIT, t, 0, 0, 0);
-        emit(XB_OP_MASK_PUSH, 0);
+        if (masked)
+            emit(XB_OP_MASK_PUSH, 0);
         const kern_expression *karg = first_arg(kexp);
         for (uint32_t i = 0; i < kexp->nr_args; i++) {
             if (!karg) return fail("JoinQuals argument %u is broken", i);
@@ -523,12 +626,13 @@ struct Compiler {
             if (r < 0) return false;
             emit(XB_OP_AND_ACC, t, r);
             if (i + 1 < kexp->nr_args) {
-                emit(XB_OP_MASK_NARROW, 0, r, 0, 0);
+                if (masked)
+                    emit(XB_OP_MASK_NARROW, 0, r, 0, 0);
                 karg = next_arg(kexp, karg);
             }
         }
-        emit(XB_OP_MASK_POP, 0);
-        emit(XB_OP_END, 0);
+        if (masked)
+            emit(XB_OP_MASK_POP, 0);
         prog->count = (uint16_t)(plan->ninsns - prog->start);
         prog->result = (int16_t)t;
         if ((uint32_t)ntemps > plan->nregs)
@@ -553,7 +657,6 @@ struct Compiler {
             if (i + 1 < kexp->nr_args)
                 karg = next_arg(kexp, karg);
         }
-        emit(XB_OP_END, 0);
         prog->count = (uint16_t)(plan->ninsns - prog->start);
         if ((uint32_t)ntemps > plan->nregs)
             plan->nregs = ntemps;

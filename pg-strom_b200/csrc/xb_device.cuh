@@ -52,13 +52,39 @@ __device__ __forceinline__ XbRegs xb_regs_setup(char *base, uint32_t nregs)
 #define RAUX(R, r)      ((R).aux[(r) * 32 + lane])
 #define RISNULL(R, r)   ((((R).nullm[r]) >> lane) & 1u)
 
-/* all lanes call this convergently; writes the NULL ballot of register r */
+/* all lanes call this convergently; writes the NULL ballot of register r.
+ * Every lane stores the same (warp-uniform) word, so each lane observes the
+ * new value on its next read without a warp barrier; the ballot itself
+ * orders this store after every lane's reads of the old value. */
 __device__ __forceinline__ void xb_set_null(XbRegs &R, int r, bool isnull)
 {
-    uint32_t m = __ballot_sync(XB_FULL, isnull);
-    if (xb_lane() == 0)
-        R.nullm[r] = m;
-    __syncwarp();
+    const uint32_t m = __ballot_sync(XB_FULL, isnull);
+    R.nullm[r] = m;
+}
+
+/* hash of a register value of the given hash kind (xpu_*_datum_hash) */
+__device__ __forceinline__ uint32_t
+xb_hash_reg(uint32_t hk, uint64_t x, uint32_t aux, bool act, bool *bad)
+{
+    switch (hk) {
+    case XB_HK_W1: return xb_hash_u32((uint32_t)x, 1);
+    case XB_HK_W2: return xb_hash_u32((uint32_t)x, 2);
+    case XB_HK_W4: return xb_hash_u32((uint32_t)x, 4);
+    case XB_HK_W8: return xb_hash_u64(x);
+    case XB_HK_TEXT:
+        return act ? xb_hash_bytes((const uint8_t *)x, aux) : 0;
+    case XB_HK_NUM:
+        if (act) {
+            uint8_t k; int16_t w; xb_i128 v;
+            if (xb_numeric_decode((const uint8_t *)x, &k, &w, &v)) {
+                *bad = true;
+                return 0;
+            }
+            return xb_hash_numeric(k, w, v);
+        }
+        return 0;
+    }
+    return 0;
 }
 
 /* ---------------------------------------------------------------
@@ -115,11 +141,15 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
 {
     const uint32_t lane = xb_lane();
     uint32_t active = active_in;
+    uint32_t mstack[XB_MASK_STACK];     /* per-thread copy of the lane-mask stack */
     int msp = 0;
     bool failed = false;
 
+    xb_insn next = count > 0 ? code[0] : xb_insn();
     for (uint32_t pc = 0; pc < count; pc++) {
-        const xb_insn in = code[pc];
+        const xb_insn in = next;
+        if (pc + 1 < count)
+            next = code[pc + 1];            /* overlap the fetch with this op */
         const bool act = ((active >> lane) & 1u) != 0;
         switch (in.op) {
         case XB_OP_END:
@@ -133,10 +163,47 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
         case XB_OP_MOVE:
             RVAL(R, in.dst) = RVAL(R, in.a);
             RAUX(R, in.dst) = RAUX(R, in.a);
-            __syncwarp();
-            if (lane == 0) R.nullm[in.dst] = R.nullm[in.a];
-            __syncwarp();
+            xb_set_null(R, in.dst, RISNULL(R, in.a));
             break;
+        case XB_OP_CMPI: {
+            const bool isnull = RISNULL(R, in.a);
+            bool res = false;
+            if (!isnull) {
+                const uint64_t x = RVAL(R, in.a);
+                int c;
+                if (in.kind == XB_RK_INT) {
+                    const int64_t a = (int64_t)x, b = in.imm;
+                    c = a < b ? -1 : (a > b ? 1 : 0);
+                } else {
+                    const double a = __longlong_as_double(x), b = __longlong_as_double(in.imm);
+                    const bool na = (a != a), nb = (b != b);
+                    c = na ? (nb ? 0 : 1) : (nb ? -1 : (a < b ? -1 : (a > b ? 1 : 0)));
+                }
+                switch (in.sub) {
+                case XB_CMP_EQ: res = (c == 0); break;
+                case XB_CMP_NE: res = (c != 0); break;
+                case XB_CMP_LT: res = (c < 0); break;
+                case XB_CMP_LE: res = (c <= 0); break;
+                case XB_CMP_GT: res = (c > 0); break;
+                default:        res = (c >= 0); break;
+                }
+            }
+            RVAL(R, in.dst) = res ? 1 : 0;
+            xb_set_null(R, in.dst, isnull);
+            break;
+        }
+        case XB_OP_HASH1: {
+            uint32_t h = 0xffffffffU;
+            if (!RISNULL(R, in.a)) {
+                bool bad = false;
+                const uint32_t hv = xb_hash_reg(in.sub, RVAL(R, in.a), RAUX(R, in.a), act, &bad);
+                if (bad) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT); failed = true; }
+                h = xb_hash_merge(h, hv);
+            }
+            RVAL(R, in.dst) = h ^ 0xffffffffU;
+            xb_set_null(R, in.dst, false);
+            break;
+        }
         case XB_OP_CMP: {
             bool isnull = RISNULL(R, in.a) || RISNULL(R, in.b);
             bool res = false;
@@ -313,10 +380,8 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
             break;
         }
         case XB_OP_MASK_PUSH:
-            if (msp < XB_MASK_STACK) {
-                if (lane == 0) R.mstack[msp] = active;
-                __syncwarp();
-            }
+            if (msp < XB_MASK_STACK)
+                mstack[msp] = active;
             msp++;
             break;
         case XB_OP_MASK_NARROW: {
@@ -329,10 +394,9 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
         case XB_OP_MASK_POP:
             msp--;
             if (msp >= 0 && msp < XB_MASK_STACK)
-                active = R.mstack[msp];
+                active = mstack[msp];
             else
                 active = active_in;
-            __syncwarp();
             break;
         case XB_OP_HASH_INIT:
             RVAL(R, in.dst) = 0xffffffffULL;
@@ -341,28 +405,9 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
         case XB_OP_HASH_ADD: {
             uint32_t h = (uint32_t)RVAL(R, in.dst);
             if (!RISNULL(R, in.a)) {
-                uint64_t x = RVAL(R, in.a);
-                uint32_t hv = 0;
-                switch (in.sub) {
-                case XB_HK_W1: hv = xb_hash_u32((uint32_t)x, 1); break;
-                case XB_HK_W2: hv = xb_hash_u32((uint32_t)x, 2); break;
-                case XB_HK_W4: hv = xb_hash_u32((uint32_t)x, 4); break;
-                case XB_HK_W8: hv = xb_hash_u64(x); break;
-                case XB_HK_TEXT:
-                    if (act) hv = xb_hash_bytes((const uint8_t *)x, RAUX(R, in.a));
-                    break;
-                case XB_HK_NUM:
-                    if (act) {
-                        uint8_t k; int16_t w; xb_i128 v;
-                        if (xb_numeric_decode((const uint8_t *)x, &k, &w, &v)) {
-                            XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
-                            failed = true;
-                        } else {
-                            hv = xb_hash_numeric(k, w, v);
-                        }
-                    }
-                    break;
-                }
+                bool bad = false;
+                const uint32_t hv = xb_hash_reg(in.sub, RVAL(R, in.a), RAUX(R, in.a), act, &bad);
+                if (bad) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT); failed = true; }
                 h = xb_hash_merge(h, hv);
             }
             RVAL(R, in.dst) = h;

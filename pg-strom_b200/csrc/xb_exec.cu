@@ -418,9 +418,10 @@ xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t ha
  * ================================================================ */
 struct XbExecArgs {
     const xb_plan  *plan;
-    const kern_data_store *kds;
-    uint32_t        nunits;
-    uint32_t        format;
+    const xb_task  *tasks;          /* work queue: chunks of this launch */
+    uint32_t        ntasks;
+    uint64_t        nunits;         /* total units over all tasks */
+    uint32_t        format;         /* common KDS format of the tasks */
     uint32_t        sm_cap;         /* shared-memory group table entries (0: none) */
     uint32_t        regs_bytes;     /* per-warp register file bytes */
     xb_gtable      *gt;
@@ -628,8 +629,8 @@ xb_scan_heap_page(XbCtx &c, const kern_data_store *kds, const XbCol *cols, int k
                 if (off >= SizeOfPageHeaderData && len >= SizeofHeapTupleHeader &&
                     off + len <= PGSTROM_BLCKSZ) {
                     const uint8_t *htup = page + off;
-                    const uint16_t infomask2 = *(const uint16_t *)(htup + 18);
-                    const uint16_t infomask = *(const uint16_t *)(htup + 20);
+                    const uint16_t infomask2 = (uint16_t)xb_fetch_le(htup + 18, 2);
+                    const uint16_t infomask = (uint16_t)xb_fetch_le(htup + 20, 2);
                     const uint32_t t_hoff = htup[22];
                     int natts = infomask2 & HEAP_NATTS_MASK;
                     if (natts > kds_ncols) natts = kds_ncols;
@@ -793,7 +794,7 @@ xb_scan_row_unit(XbCtx &c, const kern_data_store *kds, const XbCol *cols, uint32
             uint64_t off = rowindex[row];
             if (off == 0) {
                 exists = false;
-            } else if (off <= kds->length) {
+            } else if (off <= kds->length && ((kds->length - off) & 7) == 0) {
                 const uint8_t *t = (const uint8_t *)kds + kds->length - off;
                 const kern_tupitem *ti = (const kern_tupitem *)t;
                 uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
@@ -824,12 +825,25 @@ xb_scan_row_unit(XbCtx &c, const kern_data_store *kds, const XbCol *cols, uint32
     }
 }
 
+/* chunk owning global unit 'unit' (tasks are sorted by unit_base) */
+__device__ __forceinline__ uint32_t
+xb_find_task(const xb_task *tasks, uint32_t ntasks, uint64_t unit)
+{
+    uint32_t lo = 0, hi = ntasks;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (tasks[mid].unit_base <= unit) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(XB_BLOCK, 3)
 xb_exec_kernel(XbExecArgs args)
 {
     extern __shared__ __align__(16) char smem[];
     const xb_plan *plan = args.plan;
-    const kern_data_store *kds = args.kds;
+    /* all chunks of a launch share one column layout (checked by the host) */
+    const kern_data_store *kds0 = args.tasks[0].kds;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
 
@@ -838,11 +852,11 @@ xb_exec_kernel(XbExecArgs args)
     const size_t sm_bytes = (size_t)args.sm_cap * plan->gent_size;
     char *regs_base = sm_entries + sm_bytes + (size_t)warp * args.regs_bytes;
 
-    const int kds_ncols = kds->ncols < XB_MAX_COLS ? (int)kds->ncols : XB_MAX_COLS;
+    const int kds_ncols = kds0->ncols < XB_MAX_COLS ? (int)kds0->ncols : XB_MAX_COLS;
     for (int i = threadIdx.x; i < kds_ncols; i += blockDim.x) {
-        cols[i].attlen = kds->colmeta[i].attlen;
-        cols[i].attalign = kds->colmeta[i].attalign > 0 ? kds->colmeta[i].attalign : 1;
-        cols[i].attcacheoff = kds->colmeta[i].attcacheoff;
+        cols[i].attlen = kds0->colmeta[i].attlen;
+        cols[i].attalign = kds0->colmeta[i].attalign > 0 ? kds0->colmeta[i].attalign : 1;
+        cols[i].attcacheoff = kds0->colmeta[i].attcacheoff;
     }
     for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
         ((uint32_t *)sm_entries)[i] = 0;
@@ -872,14 +886,21 @@ xb_exec_kernel(XbExecArgs args)
             if (lane == 0)
                 next = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
             next = __shfl_sync(XB_FULL, next, 0);
-            /* pull the next claim's pages into L2 while these are decoded */
+            /* pull the next claim's pages into L2 (TMA bulk prefetch) while
+             * these are decoded */
             if (lane < stride && next + lane < args.nunits) {
-                const char *p = (const char *)kds + kds->block_offset + (next + lane) * (size_t)PGSTROM_BLCKSZ;
+                const uint64_t u = next + lane;
+                const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
+                const char *p = (const char *)t.kds + t.kds->block_offset +
+                                (u - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
                 if ((((uintptr_t)p) & 15) == 0)
                     xb_prefetch_l2(p, PGSTROM_BLCKSZ);
             }
-            for (uint32_t k = 0; k < stride && claim + k < args.nunits && !c.failed; k++)
-                xb_scan_heap_page(c, kds, cols, kds_ncols, (uint32_t)(claim + k));
+            for (uint32_t k = 0; k < stride && claim + k < args.nunits && !c.failed; k++) {
+                const uint64_t u = claim + k;
+                const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
+                xb_scan_heap_page(c, t.kds, cols, kds_ncols, (uint32_t)(u - t.unit_base));
+            }
             if (*(volatile uint32_t *)&args.st->errcode != 0)
                 break;
             claim = next;
@@ -892,10 +913,11 @@ xb_exec_kernel(XbExecArgs args)
             unit = __shfl_sync(XB_FULL, unit, 0);
             if (unit >= args.nunits || c.failed)
                 break;
+            const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, unit)];
             if (args.format == KDS_FORMAT_ARROW)
-                xb_scan_arrow_unit(c, kds, (uint32_t)unit);
+                xb_scan_arrow_unit(c, t.kds, (uint32_t)(unit - t.unit_base));
             else
-                xb_scan_row_unit(c, kds, cols, (uint32_t)unit);
+                xb_scan_row_unit(c, t.kds, cols, (uint32_t)(unit - t.unit_base));
             if (*(volatile uint32_t *)&args.st->errcode != 0)
                 break;
         }
@@ -960,7 +982,7 @@ xb_build_inner(XbBuildArgs args)
     for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n;
          row += gridDim.x * blockDim.x) {
         uint64_t off = rowindex[row];
-        if (off == 0 || off > kds->length) {
+        if (off == 0 || off > kds->length || ((kds->length - off) & 7) != 0) {
             XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
             continue;
         }
@@ -1016,7 +1038,18 @@ struct XbFinalArgs {
     uint32_t        nslots;
 };
 
-/* one partial-aggregate tuple (__writeOutOneTuplePreAgg layout); returns t_len */
+/* byte-wise store: kds_final columns follow the header's attalign, and the
+ * trailing row-id sits right after a variable-length key, so no store in a
+ * group tuple may assume natural alignment */
+__device__ __forceinline__ void xb_store(char *dst, const void *src, uint32_t n)
+{
+    const char *s = (const char *)src;
+    for (uint32_t i = 0; i < n; i++)
+        dst[i] = s[i];
+}
+
+/* one partial-aggregate tuple (__writeOutOneTuplePreAgg layout,
+ * cuda_gpupreagg.cu:18-223); returns t_len.  ti == nullptr only measures. */
 __device__ uint32_t
 xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint32_t rowid)
 {
@@ -1026,9 +1059,12 @@ xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint3
     char *base = (char *)ti;
     if (ti) {
         for (uint32_t i = 0; i < t_hoff; i++) base[i] = 0;
-        ti->t_infomask2 = (uint16_t)(nattrs & HEAP_NATTS_MASK);
-        ti->t_hoff = (uint8_t)(t_hoff + MINIMAL_TUPLE_OFFSET);
-        ti->hash = ((const xb_gent_head *)e)->hash;
+        const uint16_t im2 = (uint16_t)(nattrs & HEAP_NATTS_MASK);
+        const uint8_t hoff = (uint8_t)(t_hoff + MINIMAL_TUPLE_OFFSET);
+        const uint32_t hash = ((const xb_gent_head *)e)->hash;
+        xb_store(base + offsetof(kern_tupitem, hash), &hash, 4);
+        xb_store(base + offsetof(kern_tupitem, t_infomask2), &im2, 2);
+        xb_store(base + offsetof(kern_tupitem, t_hoff), &hoff, 1);
     }
     const xb_keyimg *keys = (const xb_keyimg *)(e + plan->gent_keys_off);
     for (uint32_t j = 0; j < nattrs; j++) {
@@ -1046,28 +1082,32 @@ xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint3
             const xb_keyimg &img = keys[a.key_index];
             if (img.isnull) break;
             switch (k.ld) {
-            case XB_LD_BOOL: nbytes = 1; if (buf) buf[0] = (char)img.val; break;
-            case XB_LD_INT2: nbytes = 2; if (buf) *(int16_t *)buf = (int16_t)img.val; break;
+            case XB_LD_BOOL: { uint8_t v = (uint8_t)img.val; nbytes = 1; if (buf) xb_store(buf, &v, 1); break; }
+            case XB_LD_INT2: { int16_t v = (int16_t)img.val; nbytes = 2; if (buf) xb_store(buf, &v, 2); break; }
             case XB_LD_INT4:
-            case XB_LD_DATE: nbytes = 4; if (buf) *(int32_t *)buf = (int32_t)img.val; break;
+            case XB_LD_DATE: { int32_t v = (int32_t)img.val; nbytes = 4; if (buf) xb_store(buf, &v, 4); break; }
             case XB_LD_INT8:
-            case XB_LD_FLT8: nbytes = 8; if (buf) *(uint64_t *)buf = img.val; break;
-            case XB_LD_FLT4:
+            case XB_LD_FLT8: { nbytes = 8; if (buf) xb_store(buf, &img.val, 8); break; }
+            case XB_LD_FLT4: {
+                float v = (float)__longlong_as_double(img.val);
                 nbytes = 4;
-                if (buf) *(float *)buf = (float)__longlong_as_double(img.val);
+                if (buf) xb_store(buf, &v, 4);
                 break;
-            case XB_LD_TEXT:
+            }
+            case XB_LD_TEXT: {
                 nbytes = 4 + img.len;
                 if (buf) {
-                    *(uint32_t *)buf = nbytes << 2;
-                    for (uint32_t i = 0; i < img.len; i++) buf[4 + i] = ((const char *)img.val)[i];
+                    const uint32_t hdr = nbytes << 2;           /* SET_VARSIZE */
+                    xb_store(buf, &hdr, 4);
+                    xb_store(buf + 4, (const void *)img.val, img.len);
                 }
                 infomask |= HEAP_HASVARWIDTH;
                 break;
+            }
             case XB_LD_NUMERIC: {
                 const uint8_t *vl = (const uint8_t *)img.val;
                 nbytes = xb_numeric_varsize(vl);
-                if (buf) for (uint32_t i = 0; i < nbytes; i++) buf[i] = (char)vl[i];
+                if (buf) xb_store(buf, vl, nbytes);
                 infomask |= HEAP_HASVARWIDTH;
                 break;
             }
@@ -1077,47 +1117,44 @@ xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint3
         case KAGG_ACTION__NROWS_ANY:
         case KAGG_ACTION__NROWS_COND:
             nbytes = 8;
-            if (buf) *(uint64_t *)buf = su[0];
+            if (buf) xb_store(buf, &su[0], 8);
             break;
         case KAGG_ACTION__PMIN_INT32:
         case KAGG_ACTION__PMIN_INT64:
         case KAGG_ACTION__PMAX_INT32:
         case KAGG_ACTION__PMAX_INT64: {
-            nbytes = sizeof(kagg_state__pminmax_int64_packed);
-            if (buf) {
-                kagg_state__pminmax_int64_packed *r = (kagg_state__pminmax_int64_packed *)buf;
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = *(const uint32_t *)(su + 1) ? PAGG_MINMAX_ATTRS__VALID : 0;
-                r->value = (int64_t)su[0];
-            }
+            kagg_state__pminmax_int64_packed r;
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = *(const uint32_t *)(su + 1) ? PAGG_MINMAX_ATTRS__VALID : 0;
+            r.value = (int64_t)su[0];
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
         case KAGG_ACTION__PMIN_FP64:
         case KAGG_ACTION__PMAX_FP64: {
-            nbytes = sizeof(kagg_state__pminmax_fp64_packed);
-            if (buf) {
-                kagg_state__pminmax_fp64_packed *r = (kagg_state__pminmax_fp64_packed *)buf;
-                bool valid = *(const uint32_t *)(su + 1) != 0;
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = valid ? PAGG_MINMAX_ATTRS__VALID : 0;
-                r->value = valid ? xb_f64_from_ordered((int64_t)su[0])
-                                 : (a.action == KAGG_ACTION__PMIN_FP64 ? 1.7976931348623157e308
-                                                                        : -1.7976931348623157e308);
-            }
+            kagg_state__pminmax_fp64_packed r;
+            const bool valid = *(const uint32_t *)(su + 1) != 0;
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = valid ? PAGG_MINMAX_ATTRS__VALID : 0;
+            r.value = valid ? xb_f64_from_ordered((int64_t)su[0])
+                            : (a.action == KAGG_ACTION__PMIN_FP64 ? 1.7976931348623157e308
+                                                                   : -1.7976931348623157e308);
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
         case KAGG_ACTION__PSUM_INT:
         case KAGG_ACTION__PAVG_INT: {
-            nbytes = sizeof(kagg_state__psum_int_packed);
-            if (buf) {
-                kagg_state__psum_int_packed *r = (kagg_state__psum_int_packed *)buf;
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = 0;
-                r->nitems = (int64_t)su[0];
-                r->sum = (int64_t)su[1];
-            }
+            kagg_state__psum_int_packed r;
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = 0;
+            r.nitems = (int64_t)su[0];
+            r.sum = (int64_t)su[1];
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
@@ -1125,62 +1162,58 @@ xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint3
         case KAGG_ACTION__PAVG_INT64:
         case KAGG_ACTION__PSUM_NUMERIC:
         case KAGG_ACTION__PAVG_NUMERIC: {
-            nbytes = sizeof(kagg_state__psum_numeric_packed);
-            if (buf) {
-                kagg_state__psum_numeric_packed *r = (kagg_state__psum_numeric_packed *)buf;
-                bool is_num = (a.action == KAGG_ACTION__PSUM_NUMERIC || a.action == KAGG_ACTION__PAVG_NUMERIC);
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = is_num ? (((uint32_t)a.weight & PAGG_NUMERIC_ATTRS__WEIGHT) |
-                                     *(const uint32_t *)(su + 3)) : 0;
-                r->nitems = su[0];
-                r->sum.u64_lo = su[1];
-                r->sum.u64_hi = su[2];
-            }
+            kagg_state__psum_numeric_packed r;
+            const bool is_num = (a.action == KAGG_ACTION__PSUM_NUMERIC || a.action == KAGG_ACTION__PAVG_NUMERIC);
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = is_num ? (((uint32_t)a.weight & PAGG_NUMERIC_ATTRS__WEIGHT) |
+                                *(const uint32_t *)(su + 3)) : 0;
+            r.nitems = su[0];
+            r.sum.u64_lo = su[1];
+            r.sum.u64_hi = su[2];
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
         case KAGG_ACTION__PSUM_FP:
         case KAGG_ACTION__PAVG_FP: {
-            nbytes = sizeof(kagg_state__psum_fp_packed);
-            if (buf) {
-                kagg_state__psum_fp_packed *r = (kagg_state__psum_fp_packed *)buf;
-                const double *d = (const double *)su;
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = 0;
-                r->nitems = (int64_t)su[0];
-                r->sum = __dadd_rn(d[1], d[2]);
-            }
+            kagg_state__psum_fp_packed r;
+            const double *d = (const double *)su;
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = 0;
+            r.nitems = (int64_t)su[0];
+            r.sum = __dadd_rn(d[1], d[2]);
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
         case KAGG_ACTION__STDDEV: {
-            nbytes = sizeof(kagg_state__stddev_packed);
-            if (buf) {
-                kagg_state__stddev_packed *r = (kagg_state__stddev_packed *)buf;
-                const double *d = (const double *)su;
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = 0;
-                r->nitems = (int64_t)su[0];
-                r->sum_x = __dadd_rn(d[1], d[2]);
-                r->sum_x2 = __dadd_rn(d[3], d[4]);
-            }
+            kagg_state__stddev_packed r;
+            const double *d = (const double *)su;
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = 0;
+            r.nitems = (int64_t)su[0];
+            r.sum_x = __dadd_rn(d[1], d[2]);
+            r.sum_x2 = __dadd_rn(d[3], d[4]);
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
         case KAGG_ACTION__COVAR: {
-            nbytes = sizeof(kagg_state__covar_packed);
-            if (buf) {
-                kagg_state__covar_packed *r = (kagg_state__covar_packed *)buf;
-                const double *d = (const double *)su;
-                r->vl_len_ = (int32_t)(nbytes << 2);
-                r->attrs = 0;
-                r->nitems = (int64_t)su[0];
-                r->sum_x = __dadd_rn(d[1], d[2]);
-                r->sum_xx = __dadd_rn(d[3], d[4]);
-                r->sum_y = __dadd_rn(d[5], d[6]);
-                r->sum_yy = __dadd_rn(d[7], d[8]);
-                r->sum_xy = __dadd_rn(d[9], d[10]);
-            }
+            kagg_state__covar_packed r;
+            const double *d = (const double *)su;
+            nbytes = sizeof(r);
+            r.vl_len_ = (int32_t)(nbytes << 2);
+            r.attrs = 0;
+            r.nitems = (int64_t)su[0];
+            r.sum_x = __dadd_rn(d[1], d[2]);
+            r.sum_xx = __dadd_rn(d[3], d[4]);
+            r.sum_y = __dadd_rn(d[5], d[6]);
+            r.sum_yy = __dadd_rn(d[7], d[8]);
+            r.sum_xy = __dadd_rn(d[9], d[10]);
+            if (buf) xb_store(buf, &r, nbytes);
             infomask |= HEAP_HASVARWIDTH;
             break;
         }
@@ -1188,14 +1221,14 @@ xb_write_group_tuple(const xb_plan *plan, const char *e, kern_tupitem *ti, uint3
             break;
         }
         if (ti && nbytes > 0)
-            ti->t_bits[j >> 3] |= (uint8_t)(1u << (j & 7));
+            base[offsetof(kern_tupitem, t_bits) + (j >> 3)] |= (char)(1u << (j & 7));
         t_hoff = t_next + nbytes;
     }
     t_hoff += ROWID_SIZE;
     if (ti) {
-        ti->t_len = t_hoff;
-        ti->t_infomask = infomask;
-        *(uint32_t *)(base + t_hoff - ROWID_SIZE) = rowid;
+        xb_store(base + offsetof(kern_tupitem, t_len), &t_hoff, 4);
+        xb_store(base + offsetof(kern_tupitem, t_infomask), &infomask, 2);
+        xb_store(base + t_hoff - ROWID_SIZE, &rowid, 4);        /* KERN_TUPITEM_SET_ROWID */
     }
     return t_hoff;
 }
@@ -1265,6 +1298,8 @@ struct xpuB200Session {
     xb_status      *h_status = nullptr;     /* pinned */
     char           *d_src = nullptr;
     uint64_t        d_src_cap = 0;
+    xb_task        *d_tasks = nullptr;      /* work queue of single-chunk launches */
+    uint32_t        d_tasks_cap = 0;
     uint32_t        sm_cap = 0;
     uint32_t        regs_bytes = 0;
     size_t          smem_bytes = 0;
@@ -1371,6 +1406,7 @@ static void xb_session_free(xpuB200Session *s)
     for (void *p : s->d_allocs)
         cudaFree(p);
     if (s->d_src) cudaFree(s->d_src);
+    if (s->d_tasks) cudaFree(s->d_tasks);
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->h_plan) free(s->h_plan);
     cudaEventDestroy(s->ev0);
@@ -1542,26 +1578,31 @@ xpuB200CloseSession(xpuB200Session *sess)
         xb_session_free(sess);
 }
 
-static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
-                          const kern_data_store *h_kds_head, kern_errorbuf *err)
+/* units of one chunk (pages, or 1024-row groups) */
+static uint32_t xb_chunk_units(const kern_data_store *head)
+{
+    if (head->format == KDS_FORMAT_BLOCK)
+        return head->nitems;
+    return (head->nitems + XB_ROWS_UNIT - 1) / XB_ROWS_UNIT;
+}
+
+/* launch the executor over a device-resident task table */
+static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
+                           uint64_t nunits, uint32_t format, kern_errorbuf *err)
 {
     XbExecArgs a;
     a.plan = s->d_plan;
-    a.kds = d_kds;
-    a.format = (uint32_t)h_kds_head->format;
-    if (a.format == KDS_FORMAT_BLOCK)
-        a.nunits = h_kds_head->nitems;
-    else if (a.format == KDS_FORMAT_ARROW || a.format == KDS_FORMAT_ROW)
-        a.nunits = (h_kds_head->nitems + XB_ROWS_UNIT - 1) / XB_ROWS_UNIT;
-    else
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", h_kds_head->format);
+    a.tasks = d_tasks;
+    a.ntasks = ntasks;
+    a.nunits = nunits;
+    a.format = format;
     a.sm_cap = s->sm_cap;
     a.regs_bytes = s->regs_bytes;
     a.gt = s->d_gt;
     a.st = s->d_status;
     int grid = s->grid;
-    uint32_t warps_needed = (a.format == KDS_FORMAT_BLOCK) ? (a.nunits + XB_CLAIM - 1) / XB_CLAIM : a.nunits;
-    if ((uint32_t)grid * XB_WARPS > warps_needed)
+    uint64_t warps_needed = (format == KDS_FORMAT_BLOCK) ? (nunits + XB_CLAIM - 1) / XB_CLAIM : nunits;
+    if ((uint64_t)grid * XB_WARPS > warps_needed)
         grid = (int)((warps_needed + XB_WARPS - 1) / XB_WARPS);
     if (grid < 1) grid = 1;
     xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, s->dev->stream>>>(a);
@@ -1569,6 +1610,26 @@ static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
     if (rc != cudaSuccess)
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "kernel launch: %s", cudaGetErrorString(rc));
     return 0;
+}
+
+/* single-chunk launch through the session's task buffer */
+static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
+                          const kern_data_store *h_kds_head, kern_errorbuf *err)
+{
+    if (h_kds_head->format != KDS_FORMAT_BLOCK && h_kds_head->format != KDS_FORMAT_ARROW &&
+        h_kds_head->format != KDS_FORMAT_ROW)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", h_kds_head->format);
+    if (!s->d_tasks) {
+        XB_CUDA(cudaMalloc((void **)&s->d_tasks, sizeof(xb_task) * 16), err);
+        s->d_tasks_cap = 16;
+    }
+    xb_task t;
+    t.kds = d_kds;
+    t.unit_base = 0;
+    t.nunits = xb_chunk_units(h_kds_head);
+    t.format = (uint32_t)h_kds_head->format;
+    XB_CUDA(cudaMemcpyAsync(s->d_tasks, &t, sizeof(t), cudaMemcpyHostToDevice, s->dev->stream), err);
+    return xb_launch_tasks(s, s->d_tasks, 1, t.nunits, t.format, err);
 }
 
 static int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
@@ -1592,6 +1653,9 @@ static int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
                 cm->values_offset + cm->values_length > kds->length ||
                 cm->extra_offset + cm->extra_length > kds->length)
                 return XB_ERR(err, ERRCODE_DEVICE_ERROR, "Arrow column %u is out of the chunk", j);
+            /* value arrays are read with their natural width */
+            if ((cm->values_offset & 7) != 0)
+                return XB_ERR(err, ERRCODE_DEVICE_ERROR, "Arrow column %u values are not 8-byte aligned", j);
         }
     }
     return 0;
@@ -1641,6 +1705,8 @@ xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_o
     const kern_data_store *d_kds;
     std::vector<char> hbuf;
     if (kds_src_on_device) {
+        if (((uintptr_t)kds_src & 7) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
         XB_CUDA(cudaMemcpy(&head, kds_src, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
         uint64_t hl = KDS_HEAD_LENGTH(&head);
         hbuf.resize(hl);
@@ -1680,6 +1746,8 @@ xpuB200TimeExecTask(xpuB200Session *s, const kern_data_store *kds_src_dev, int n
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
     cudaStream_t st = s->dev->stream;
     kern_data_store head;
+    if (((uintptr_t)kds_src_dev & 7) != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
     XB_CUDA(cudaMemcpy(&head, kds_src_dev, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
     std::vector<char> hbuf(KDS_HEAD_LENGTH(&head));
     XB_CUDA(cudaMemcpy(hbuf.data(), kds_src_dev, hbuf.size(), cudaMemcpyDeviceToHost), err);
@@ -1825,6 +1893,127 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
         rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "Final: %s", cudaGetErrorString(cudaGetLastError()));
     cleanup();
     return rc;
+}
+
+/* ----------------------------------------------------------------
+ * prepared batches: many device-resident chunks in one persistent launch
+ * ---------------------------------------------------------------- */
+struct xpuB200Batch {
+    xpuB200Session *sess;
+    xb_task        *d_tasks;
+    uint32_t        ntasks;
+    uint64_t        nunits;
+    uint32_t        format;
+    uint64_t        bytes;          /* sum of chunk lengths */
+    uint64_t        rows;           /* rows (ARROW/ROW) or pages (BLOCK) */
+};
+
+extern "C" int
+xpuB200BatchCreate(xpuB200Session *s, const kern_data_store *const *kds_dev, uint32_t nchunks,
+                   xpuB200Batch **p_batch, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    *p_batch = nullptr;
+    if (!s || !kds_dev || nchunks == 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid batch arguments");
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    std::vector<xb_task> tasks(nchunks);
+    std::vector<char> first_head;
+    uint64_t base = 0, bytes = 0, rows = 0;
+    uint32_t format = 0;
+    for (uint32_t i = 0; i < nchunks; i++) {
+        kern_data_store head;
+        if (((uintptr_t)kds_dev[i] & 7) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "chunk %u is not 8-byte aligned", i);
+        XB_CUDA(cudaMemcpy(&head, kds_dev[i], offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+        std::vector<char> hb(KDS_HEAD_LENGTH(&head));
+        XB_CUDA(cudaMemcpy(hb.data(), kds_dev[i], hb.size(), cudaMemcpyDeviceToHost), err);
+        const kern_data_store *h = (const kern_data_store *)hb.data();
+        int rc = xb_check_kds(h, err);
+        if (rc) return rc;
+        if (i == 0) {
+            first_head = hb;
+            format = (uint32_t)h->format;
+        } else {
+            /* one launch decodes every chunk with the same column layout */
+            const kern_data_store *f = (const kern_data_store *)first_head.data();
+            if ((uint32_t)h->format != format || h->ncols != f->ncols ||
+                (h->format != KDS_FORMAT_ARROW &&
+                 memcmp(h->colmeta, f->colmeta, sizeof(kern_colmeta) * h->ncols) != 0))
+                return XB_ERR(err, ERRCODE_DEVICE_ERROR, "chunk %u of the batch has another layout", i);
+        }
+        tasks[i].kds = kds_dev[i];
+        tasks[i].unit_base = base;
+        tasks[i].nunits = xb_chunk_units(h);
+        tasks[i].format = format;
+        base += tasks[i].nunits;
+        bytes += h->length;
+        rows += h->nitems;
+    }
+    xpuB200Batch *b = new xpuB200Batch();
+    b->sess = s;
+    b->ntasks = nchunks;
+    b->nunits = base;
+    b->format = format;
+    b->bytes = bytes;
+    b->rows = rows;
+    if (cudaMalloc((void **)&b->d_tasks, sizeof(xb_task) * nchunks) != cudaSuccess) {
+        delete b;
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for the batch");
+    }
+    cudaMemcpy(b->d_tasks, tasks.data(), sizeof(xb_task) * nchunks, cudaMemcpyHostToDevice);
+    *p_batch = b;
+    return 0;
+}
+
+extern "C" int
+xpuB200BatchExec(xpuB200Batch *b, kern_exec_results *results, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!b)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid batch");
+    xpuB200Session *s = b->sess;
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->dev->stream), err);
+    int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
+    if (rc) return rc;
+    return xb_finish_task(s, results, err);
+}
+
+extern "C" int
+xpuB200BatchTime(xpuB200Batch *b, int niters, double *p_msec, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    xpuB200Session *s = b->sess;
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    cudaStream_t st = s->dev->stream;
+    float total = 0.0f;
+    for (int i = 0; i < niters; i++) {
+        XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+        cudaEventRecord(s->ev0, st);
+        int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
+        if (rc) return rc;
+        cudaEventRecord(s->ev1, st);
+        rc = xb_finish_task(s, nullptr, err);
+        if (rc) return rc;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        total += ms;
+    }
+    *p_msec = niters > 0 ? total / niters : 0.0;
+    return 0;
+}
+
+extern "C" void
+xpuB200BatchDestroy(xpuB200Batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->sess->dev->dindex);
+    cudaFree(b->d_tasks);
+    delete b;
 }
 
 extern "C" int

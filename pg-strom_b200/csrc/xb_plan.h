@@ -74,6 +74,8 @@
 #define XB_OP_HASH_ADD      16  /* dst <- merge(dst, hash(a)); skips NULL; sub = hash kind */
 #define XB_OP_HASH_FINI     17  /* dst <- dst ^ 0xffffffff */
 #define XB_OP_DISTINCT      18  /* dst <- a IS DISTINCT FROM b (kind) */
+#define XB_OP_CMPI          19  /* dst <- a <sub> imm (kind INT or FLT), NULL if a NULL */
+#define XB_OP_HASH1         20  /* dst <- HashValue(a): init, add (sub = hash kind), final */
 
 /* XB_OP_CMP sub-ops */
 #define XB_CMP_EQ   0
@@ -228,13 +230,13 @@ typedef struct xb_keyimg {
     uint32_t    isnull;
 } xb_keyimg;
 
-/* per-launch task descriptor (device) */
+/* one chunk of a launch's work queue (device): units are heap pages for
+ * KDS_FORMAT_BLOCK and 1024-row groups for ARROW / ROW chunks */
 typedef struct xb_task {
-    const kern_data_store *kds_src;
-    uint32_t    nunits;         /* pages (BLOCK) or 32-row groups (ARROW/ROW) */
+    const kern_data_store *kds;
+    uint64_t    unit_base;      /* first global unit of this chunk */
+    uint32_t    nunits;
     uint32_t    format;
-    uint32_t    nrows;          /* rows for ARROW/ROW */
-    uint32_t    block_offset;
 } xb_task;
 
 /* global group table */

@@ -153,3 +153,77 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
     meta = {"nitems_raw": nfact, "nitems_in": nfact, "nitems_out": int(m.sum()),
             "depth_out": [nfact, int(m.sum())], "agg_names": ["sum_amount", "nrows"], "nkeys": 1}
     return fact, session, kmrels, expect, meta
+
+
+UNIX_TO_PG_DAYS = 10957                     # POSTGRES_EPOCH_JDATE - UNIX_EPOCH_JDATE
+
+
+def arrow_groupby(nrows=500_000_000, nkeys=10_000_000, seed_config=2, rows_per_chunk=2_500_000,
+                  with_expect=True):
+    """Arrow columnar high-cardinality pre-aggregation:
+    k int8 U over nkeys, v1 int4 U[-1e6,1e6], v2 float8 lognormal(0,1),
+    d Date32 U over 10 years from 2015-01-01, s dictionary text of 1000
+    values (unreferenced: its buffers are not loaded, as Arrow_Fdw loads
+    only referenced columns); WHERE d in [2018-01-01, 2020-01-01)
+    GROUP BY k -> count(*), sum(v1), min(v2), max(v2), sum(v2).
+    Returns (chunks, session, expect, meta)."""
+    r = rng_for(seed_config, 0)
+    d0 = 16436                                  # 2015-01-01 in Unix days
+    lo_day, hi_day = 17532, 18262               # 2018-01-01, 2020-01-01
+    typs = [("k", "int8"), ("v1", "int4"), ("v2", "float8"), ("d", "date"), ("s", "text")]
+    tbl = Table("t2", [Column(n, t) for n, t in typs], 0)
+    vk, vv1, vv2, vd = Var(0, 1, "int8"), Var(0, 2, "int4"), Var(0, 3, "float8"), Var(0, 4, "date")
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    from xb_producer import BoolOp
+    session = sb.build(
+        scan_quals=BoolOp("And", [Func("date_ge", [vd, Const("date", lo_day - UNIX_TO_PG_DAYS)], "bool"),
+                                  Func("date_lt", [vd, Const("date", hi_day - UNIX_TO_PG_DAYS)], "bool")]),
+        groupby_keys=[vk],
+        aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Func("int4_to_int8", [vv1], "int8")),
+              Agg("PMIN_FP64", vv2), Agg("PMAX_FP64", vv2), Agg("PSUM_FP", vv2)],
+        ngroups_estimate=float(min(nkeys, nrows)))
+    chunks = []
+    cols_all = {"k": [], "v1": [], "v2": [], "d": []}
+    done = 0
+    while done < nrows:
+        n = min(rows_per_chunk, nrows - done)
+        k = r.integers(0, nkeys, n, dtype=np.int64)
+        v1 = r.integers(-1_000_000, 1_000_001, n, dtype=np.int32)
+        v2 = r.lognormal(0.0, 1.0, n)
+        d = r.integers(d0, d0 + 3652, n, dtype=np.int32)
+        t = Table("t2", [Column(nm, ty) for nm, ty in typs], n)
+        chunks.append(t.arrow_kds({
+            "k": {"tag": 2, "bitwidth": 64, "values": k},
+            "v1": {"tag": 2, "bitwidth": 32, "values": v1},
+            "v2": {"tag": 3, "precision": 2, "values": v2},
+            "d": {"tag": 8, "unit": 0, "values": d},
+            "s": {"tag": 5},
+        }))
+        if with_expect:
+            for nm, arr in (("k", k), ("v1", v1), ("v2", v2), ("d", d)):
+                cols_all[nm].append(arr)
+        done += n
+    expect, meta = None, {"nitems_raw": nrows}
+    if with_expect:
+        k = np.concatenate(cols_all["k"]); v1 = np.concatenate(cols_all["v1"])
+        v2 = np.concatenate(cols_all["v2"]); d = np.concatenate(cols_all["d"])
+        m = (d >= lo_day) & (d < hi_day)
+        km, v1m, v2m = k[m], v1[m].astype(np.int64), v2[m]
+        order = np.argsort(km, kind="stable")     # stable: keeps row order per key
+        ks, v1s, v2s = km[order], v1m[order], v2m[order]
+        bounds = np.flatnonzero(np.diff(ks)) + 1
+        starts = np.concatenate([[0], bounds])
+        ends = np.concatenate([bounds, [len(ks)]])
+        expect = {}
+        for s_, e_ in zip(starts, ends):
+            if e_ <= s_:
+                continue
+            vals = v2s[s_:e_]
+            fsum = 0.0
+            for x in vals:                        # row-ordered FP64 sum
+                fsum += float(x)
+            cnt = int(e_ - s_)
+            expect[(int(ks[s_]),)] = [cnt, (cnt, int(v1s[s_:e_].sum())), (1, float(vals.min())),
+                                      (1, float(vals.max())), (cnt, fsum)]
+        meta.update({"nitems_in": int(m.sum()), "nitems_out": int(m.sum())})
+    return chunks, session, expect, meta

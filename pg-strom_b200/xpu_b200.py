@@ -53,6 +53,10 @@ def lib():
         L.xpuB200DeviceFree.argtypes = [P, P]
         L.xpuB200CopyToDevice.argtypes = [P, P, P, U64]
         L.xpuB200TimeExecTask.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_double), EB]
+        L.xpuB200BatchCreate.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(P), EB]
+        L.xpuB200BatchExec.argtypes = [P, P, EB]
+        L.xpuB200BatchTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
+        L.xpuB200BatchDestroy.argtypes = [P]
         L.xpuB200SessionInfo.argtypes = [P, ctypes.c_char_p, U64]
         L.xpuB200HashBytes.argtypes = [P, ctypes.c_uint32]
         L.xpuB200HashBytes.restype = ctypes.c_uint32
@@ -166,6 +170,9 @@ class Session:
             raise XpuB200Error(rc, e)
         return buf, parse_results(res)
 
+    def batch(self, dptrs):
+        return Batch(self, dptrs)
+
     def info(self):
         import json
         b = ctypes.create_string_buffer(1024)
@@ -175,4 +182,39 @@ class Session:
     def close(self):
         if self.h:
             lib().xpuB200CloseSession(self.h)
+            self.h = ctypes.c_void_p()
+
+
+class Batch:
+    """Many device-resident chunks executed by one persistent launch."""
+
+    def __init__(self, sess: Session, dptrs):
+        self.sess = sess
+        arr = (ctypes.c_void_p * len(dptrs))(*dptrs)
+        self.h = ctypes.c_void_p()
+        e = KernErrorbuf()
+        rc = lib().xpuB200BatchCreate(sess.h, arr, len(dptrs), ctypes.byref(self.h), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+
+    def exec(self):
+        res = results_buffer(self.sess.nrels)
+        struct.pack_into("<I", res, 92, self.sess.nrels)
+        e = KernErrorbuf()
+        rc = lib().xpuB200BatchExec(self.h, _ptr(res), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return parse_results(res)
+
+    def time(self, niters):
+        ms = ctypes.c_double()
+        e = KernErrorbuf()
+        rc = lib().xpuB200BatchTime(self.h, niters, ctypes.byref(ms), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return ms.value
+
+    def close(self):
+        if self.h:
+            lib().xpuB200BatchDestroy(self.h)
             self.h = ctypes.c_void_p()

@@ -88,3 +88,31 @@ def test_join_groupby_parity(device, nfact, nd1, nd2, ppc):
     assert F.compare_groups(got, truth) == []
     ofinal, ost = run_oracle(sess, chunks, km)
     assert F.compare_groups(got, F.decode_kds_final(ofinal, sess)) == []
+
+
+@pytest.mark.parametrize("nrows,nkeys,rpc", [(300_000, 20_000, 100_000), (2_000_000, 1_000_000, 700_000)])
+def test_arrow_groupby_parity(device, nrows, nkeys, rpc):
+    chunks, sess, expect, meta = C.arrow_groupby(nrows=nrows, nkeys=nkeys, rows_per_chunk=rpc)
+    final, st, res = run_gpu(device, sess, chunks)
+    assert st["nitems_raw"] == meta["nitems_raw"]
+    assert st["nitems_in"] == meta["nitems_in"]
+    got = F.decode_kds_final(final, sess)
+    assert F.compare_groups(got, expect) == []
+
+
+def test_batch_matches_single_chunk_path(device):
+    fact, sess, km, expect, meta = C.join_groupby(nfact=300_000, ndim1=20_000, ndim2=2_000)
+    chunks = fact.block_chunks(pages_per_chunk=300)
+    s = xpu_b200.Session(device, sess, km, 2)
+    ups = [device.upload(c) for c in chunks]
+    b = s.batch([p for _, p in ups])
+    r = b.exec()
+    assert r["nitems_raw"] == meta["nitems_raw"] and r["nitems_out"] == meta["nitems_out"]
+    assert r["depth_out"] == meta["depth_out"]
+    final, _ = s.final()
+    b.close()
+    s.close()
+    for base, _ in ups:
+        device.free(base)
+    truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+    assert F.compare_groups(F.decode_kds_final(final, sess), truth) == []
