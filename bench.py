@@ -73,24 +73,31 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x, world):
+def _reduce(x, world, op):
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(x, world):
+    """Step time of the job = the slowest rank's device time."""
+    import torch.distributed as dist
+    return _reduce(x, world, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, dist.ReduceOp.SUM if world > 1 else None)
+
+
+def shard_seed(rank):
+    """Weak scaling: every rank generates and owns a distinct fact shard."""
+    return 1 + 16 * rank
 
 
 class ClockSampler:
@@ -147,7 +154,7 @@ class ClockSampler:
 
 def build_workload(nrows, rank):
     import xb_configs as C
-    fact, sess, km, expect, meta = C.join_groupby(nfact=nrows, seed_config=1 + 16 * rank)
+    fact, sess, km, expect, meta = C.join_groupby(nfact=nrows, seed_config=shard_seed(rank))
     chunks = fact.block_chunks(pages_per_chunk=8190)
     return fact, sess, km, chunks, meta
 
@@ -163,19 +170,9 @@ def cpu_rows_per_sec(sess, km, chunks, seconds, threads):
     lock = threading.Lock()
     state = {"rows": 0, "next": 0}
     deadline = time.perf_counter() + seconds
-    rows_per_chunk = []
-    for ch in chunks:
-        nblk = int(np.frombuffer(ch[16:20].tobytes(), dtype=np.uint32)[0])
-        rows_per_chunk.append(None if nblk == 0 else nblk)
-
-    def chunk_rows(ch):
-        return None
 
     def worker():
-        if use_ref:
-            h = None
-        else:
-            o = O.Oracle(sess, km)
+        o = None if use_ref else O.Oracle(sess, km)
         while time.perf_counter() < deadline:
             with lock:
                 i = state["next"] % len(chunks)
@@ -190,7 +187,7 @@ def cpu_rows_per_sec(sess, km, chunks, seconds, threads):
                 n = o.stats()["nitems_raw"] - before
             with lock:
                 state["rows"] += n
-        if not use_ref:
+        if o is not None:
             o.close()
 
     t0 = time.perf_counter()

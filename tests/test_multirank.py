@@ -1,0 +1,73 @@
+"""The N>1 host logic of bench.py on CPU: two gloo ranks, each owning its
+own shard; the job time is the max over ranks, the row count the sum, and
+the per-rank shards are disjoint (distinct seeds).  Each rank runs the
+oracle on its shard and rank 0 checks the per-rank results add up to the
+union's."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q):
+    for sub in ("pg-strom_b200", os.path.join("pg-strom_b200", "producer"), "oracle", ""):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        import bench
+        import xb_configs as C
+        import xb_final as F
+        import xb_oracle as O
+        fact, sess, km, expect, meta = C.join_groupby(nfact=40_000, ndim1=2000, ndim2=300,
+                                                      seed_config=bench.shard_seed(rank))
+        o = O.Oracle(sess, km)
+        for ch in fact.block_chunks(pages_per_chunk=100):
+            o.exec(ch)
+        got = F.decode_kds_final(o.final(), sess)
+        o.close()
+        truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+        ok = F.compare_groups(got, truth) == []
+        t = bench.max_over_ranks(float(rank + 1), world)
+        n = bench.sum_over_ranks(1000.0, world)
+        objs = [None] * world
+        dist.all_gather_object(objs, (rank, ok, sorted(got.items())[:3]))
+        q.put((rank, ok, t, n, objs))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    for rank, ok, t, n, objs in res:
+        assert ok
+        assert t == 2.0          # max over ranks
+        assert n == 2000.0       # sum over ranks
+    # shards differ: the first groups' states are not identical across ranks
+    objs = res[0][4]
+    assert objs[0][2] != objs[1][2]
