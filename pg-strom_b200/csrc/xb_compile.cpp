@@ -25,6 +25,7 @@
 #include <cstring>
 #include <cstdarg>
 #include <string>
+#include <vector>
 #include "xb_plan.h"
 #include "xb_compile.h"
 
@@ -581,8 +582,9 @@ struct Compiler {
         return err.empty();
     }
 
-    /* JoinQuals: every argument must hold for an inner join */
-    bool join_program(const kern_expression *kexp, xb_prog *prog)
+    /* JoinQuals: every argument must hold for an inner join.  Argument
+     * 'skip' (if >= 0) is evaluated by the fused probe instead. */
+    bool join_program(const kern_expression *kexp, xb_prog *prog, int skip = -1)
     {
         prog->start = (uint16_t)plan->ninsns;
         prog->count = 0;
@@ -592,10 +594,24 @@ struct Compiler {
         if (kexp->opcode != FuncOpCode__JoinQuals || kexp->exptype != TypeOpCode__bool)
             return fail("malformed JoinQuals");
         ntemps = plan->nslots;
-        if (kexp->nr_args == 1) {
-            const kern_expression *k1 = first_arg(kexp);
-            if (!k1 || k1->exptype != TypeOpCode__bool)
-                return fail("JoinQuals argument is broken");
+        /* the arguments that remain for the VM */
+        std::vector<const kern_expression *> args;
+        {
+            const kern_expression *k = first_arg(kexp);
+            for (uint32_t i = 0; i < kexp->nr_args; i++) {
+                if (!k) return fail("JoinQuals argument %u is broken", i);
+                if (k->exptype != TypeOpCode__bool)
+                    return fail("JoinQuals argument is not bool");
+                if ((int)i != skip)
+                    args.push_back(k);
+                if (i + 1 < kexp->nr_args)
+                    k = next_arg(kexp, k);
+            }
+        }
+        if (args.empty())
+            return err.empty();         /* everything done by the fused probe */
+        if (args.size() == 1) {
+            const kern_expression *k1 = args[0];
             int r = expr(k1);
             if (r < 0) return false;
             prog->count = (uint16_t)(plan->ninsns - prog->start);
@@ -605,31 +621,19 @@ struct Compiler {
             return err.empty();
         }
         bool masked = false;
-        {
-            const kern_expression *k = first_arg(kexp);
-            for (uint32_t i = 0; i < kexp->nr_args && k; i++) {
-                if (!is_safe(k)) masked = true;
-                if (i + 1 < kexp->nr_args) k = next_arg(kexp, k);
-            }
-        }
+        for (const kern_expression *k : args)
+            if (!is_safe(k)) masked = true;
         int t = new_temp(XB_RK_INT);
         if (t < 0) return false;
         emit(XB_OP_BOOL_INIT, t, 0, 0, 0);
         if (masked)
             emit(XB_OP_MASK_PUSH, 0);
-        const kern_expression *karg = first_arg(kexp);
-        for (uint32_t i = 0; i < kexp->nr_args; i++) {
-            if (!karg) return fail("JoinQuals argument %u is broken", i);
-            if (karg->exptype != TypeOpCode__bool)
-                return fail("JoinQuals argument is not bool");
-            int r = expr(karg);
+        for (size_t i = 0; i < args.size(); i++) {
+            int r = expr(args[i]);
             if (r < 0) return false;
             emit(XB_OP_AND_ACC, t, r);
-            if (i + 1 < kexp->nr_args) {
-                if (masked)
-                    emit(XB_OP_MASK_NARROW, 0, r, 0, 0);
-                karg = next_arg(kexp, karg);
-            }
+            if (i + 1 < args.size() && masked)
+                emit(XB_OP_MASK_NARROW, 0, r, 0, 0);
         }
         if (masked)
             emit(XB_OP_MASK_POP, 0);
@@ -842,12 +846,121 @@ struct Compiler {
         plan->naggs = nattrs;
         plan->gent_size = (uint32_t)PGSTROM_TYPEALIGN(16, off);
 
-        /* programs: AggFuncs' SaveExpr arguments, then key hash */
+        /* programs: AggFuncs' SaveExpr arguments, then key hash, emitted
+         * back to back (the kernel runs them as one stream) */
         if (!save_program(kact, &plan->gb_args))
             return false;
         if (khash && !program(khash, &plan->gb_keyhash, false))
             return false;
+        if (khash && plan->gb_keyhash.start != plan->gb_args.start + plan->gb_args.count)
+            return fail("group-by programs are not contiguous");
         return true;
+    }
+
+    static bool is_int_eq(int op)
+    {
+        switch (op) {
+        case FuncOpCode__int2eq: case FuncOpCode__int24eq: case FuncOpCode__int28eq:
+        case FuncOpCode__int42eq: case FuncOpCode__int4eq: case FuncOpCode__int48eq:
+        case FuncOpCode__int82eq: case FuncOpCode__int84eq: case FuncOpCode__int8eq:
+        case FuncOpCode__date_eq:
+            return true;
+        }
+        return false;
+    }
+
+    /*
+     * Fused probe: HashValue(Var x) at this depth and a join qual
+     * "x = y" with y loaded from the inner relation at this depth.  The
+     * kernel then hashes x inline and compares y's pre-decoded column
+     * directly while walking the index; returns the index of the join qual
+     * it absorbs, or -1.
+     */
+    int detect_fused_probe(const kern_expression *kh, const kern_expression *kj, xb_inner *in)
+    {
+        in->fast_key = -1;
+        if (!kh || !kj || kh->nr_args != 1 || kj->opcode != FuncOpCode__JoinQuals)
+            return -1;
+        const kern_expression *hv = first_arg(kh);
+        if (!hv || hv->opcode != FuncOpCode__VarExpr)
+            return -1;
+        int rk, ld, hk;
+        if (!type_info(hv->exptype, &rk, &ld, &hk) || rk != XB_RK_INT)
+            return -1;
+        const int sx = hv->u.v.var_slot_id;
+        const kern_expression *q = first_arg(kj);
+        for (uint32_t i = 0; i < kj->nr_args && q; i++) {
+            if (is_int_eq(q->opcode) && q->nr_args == 2 && !(q->expflags & KEXP_FLAG__IS_PUSHED_DOWN)) {
+                const kern_expression *a = first_arg(q);
+                const kern_expression *b = a ? next_arg(q, a) : nullptr;
+                if (a && b && a->opcode == FuncOpCode__VarExpr && b->opcode == FuncOpCode__VarExpr) {
+                    int sa = a->u.v.var_slot_id, sb = b->u.v.var_slot_id;
+                    int sy = (sa == sx) ? sb : (sb == sx) ? sa : -1;
+                    for (uint32_t k = 0; sy >= 0 && k < in->nloads; k++) {
+                        if (in->load[k].reg == sy && plan->rk[sy] == XB_RK_INT) {
+                            const int kld = in->load[k].ld;
+                            in->fast_key = (int16_t)k;
+                            in->fast_outer = (uint8_t)sx;
+                            in->fast_hk = (uint8_t)hk;
+                            in->key32 = (kld == XB_LD_INT2 || kld == XB_LD_INT4 || kld == XB_LD_DATE) ? 1 : 0;
+                            return (int)i;
+                        }
+                    }
+                }
+            }
+            if (i + 1 < kj->nr_args)
+                q = next_arg(kj, q);
+        }
+        return -1;
+    }
+
+    /* registers read by instructions [start, start + count) */
+    void reads_of(const xb_prog &p, uint64_t *mask)
+    {
+        for (uint32_t i = p.start; i < (uint32_t)p.start + p.count; i++) {
+            const xb_insn &in = plan->insns[i];
+            switch (in.op) {
+            case XB_OP_CONST: case XB_OP_BOOL_INIT: case XB_OP_HASH_INIT:
+            case XB_OP_MASK_PUSH: case XB_OP_MASK_POP: case XB_OP_END:
+                break;
+            case XB_OP_CMP: case XB_OP_ARITH: case XB_OP_DISTINCT:
+                *mask |= (1ULL << in.a) | (1ULL << in.b);
+                break;
+            case XB_OP_AND_ACC: case XB_OP_OR_ACC: case XB_OP_HASH_ADD: case XB_OP_HASH_FINI:
+                *mask |= (1ULL << in.a) | (1ULL << in.dst);
+                break;
+            default:
+                *mask |= (1ULL << in.a);
+                break;
+            }
+        }
+    }
+
+    /* an inner load is live if its register is read after its join */
+    void compute_liveness()
+    {
+        uint64_t later = 0;     /* registers read by group-by and aggregates */
+        reads_of(plan->gb_args, &later);
+        reads_of(plan->gb_keyhash, &later);
+        for (uint32_t j = 0; j < plan->naggs; j++)
+            for (int16_t r : {plan->aggs[j].arg0, plan->aggs[j].arg1, plan->aggs[j].filter})
+                if (r >= 0) later |= 1ULL << r;
+        for (uint32_t k = 0; k < plan->nkeys; k++)
+            later |= 1ULL << plan->keys[k].reg;
+        for (int d = (int)plan->nrels; d >= 1; d--) {
+            xb_inner *in = &plan->inner[d];
+            uint64_t here = later;
+            reads_of(plan->join_quals[d], &here);
+            in->live = 0;
+            for (uint32_t k = 0; k < in->nloads; k++)
+                if (here & (1ULL << in->load[k].reg))
+                    in->live |= 1u << k;
+            /* registers read at this depth are needed from shallower depths */
+            reads_of(plan->join_quals[d], &later);
+            reads_of(plan->hash_value[d], &later);
+            if (in->fast_key >= 0)
+                later |= 1ULL << in->fast_outer;
+        }
     }
 
     bool run(const kern_multirels *kmrels)
@@ -925,11 +1038,14 @@ struct Compiler {
                 return false;
             const kern_expression *kj = packed_at(kjoin, d);
             if (!err.empty()) return false;
-            if (!join_program(kj, &plan->join_quals[d]))
+            int skip = detect_fused_probe(kh, kj, in);
+            if (!err.empty()) return false;
+            if (!join_program(kj, &plan->join_quals[d], skip))
                 return false;
         }
         if (!groupby())
             return false;
+        compute_liveness();
         if (plan->has_groupby == 0 && !(plan->task_kind & DEVTASK__PREAGG))
             return fail("scan/join without device projection or GROUP BY is not supported");
         return err.empty();

@@ -56,10 +56,28 @@ __device__ __forceinline__ XbRegs xb_regs_setup(char *base, uint32_t nregs)
  * Every lane stores the same (warp-uniform) word, so each lane observes the
  * new value on its next read without a warp barrier; the ballot itself
  * orders this store after every lane's reads of the old value. */
-__device__ __forceinline__ void xb_set_null(XbRegs &R, int r, bool isnull)
+__device__ __forceinline__ void xb_set_null(const XbRegs &R, int r, bool isnull)
 {
     const uint32_t m = __ballot_sync(XB_FULL, isnull);
     R.nullm[r] = m;
+}
+
+/* rare, register-hungry datum operations kept out of line so that the
+ * interpreter loop stays small */
+__device__ __noinline__ uint32_t xb_hash_text_ool(const uint8_t *p, uint32_t len)
+{
+    return xb_hash_bytes(p, len);
+}
+
+/* returns the hash, or sets *bad on a corrupt numeric */
+__device__ __noinline__ uint32_t xb_hash_numeric_ool(const uint8_t *vl, bool *bad)
+{
+    uint8_t k; int16_t w; xb_i128 v;
+    if (xb_numeric_decode(vl, &k, &w, &v)) {
+        *bad = true;
+        return 0;
+    }
+    return xb_hash_numeric(k, w, v);
 }
 
 /* hash of a register value of the given hash kind (xpu_*_datum_hash) */
@@ -72,17 +90,9 @@ xb_hash_reg(uint32_t hk, uint64_t x, uint32_t aux, bool act, bool *bad)
     case XB_HK_W4: return xb_hash_u32((uint32_t)x, 4);
     case XB_HK_W8: return xb_hash_u64(x);
     case XB_HK_TEXT:
-        return act ? xb_hash_bytes((const uint8_t *)x, aux) : 0;
+        return act ? xb_hash_text_ool((const uint8_t *)x, aux) : 0;
     case XB_HK_NUM:
-        if (act) {
-            uint8_t k; int16_t w; xb_i128 v;
-            if (xb_numeric_decode((const uint8_t *)x, &k, &w, &v)) {
-                *bad = true;
-                return 0;
-            }
-            return xb_hash_numeric(k, w, v);
-        }
-        return 0;
+        return act ? xb_hash_numeric_ool((const uint8_t *)x, bad) : 0;
     }
     return 0;
 }
@@ -102,15 +112,37 @@ __device__ __forceinline__ void xb_raise(xb_status *st, uint32_t code, uint32_t 
 /* ---------------------------------------------------------------
  * text helpers
  * --------------------------------------------------------------- */
+__device__ __noinline__ bool xb_bytes_eq_ool(const uint8_t *a, const uint8_t *b, uint32_t n);
+
+/* byte-string equality; within a 16-byte block the loads are independent
+ * (no early exit), so they are issued back to back instead of as a chain */
 __device__ __forceinline__ bool xb_bytes_eq(const uint8_t *a, const uint8_t *b, uint32_t n)
 {
-    for (uint32_t i = 0; i < n; i++)
-        if (a[i] != b[i])
+    if (a == b)
+        return true;
+    uint32_t i = 0;
+    for (; i + 16 <= n; i += 16) {
+        uint32_t diff = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < 16; k++)
+            diff |= (uint32_t)(a[i + k] ^ b[i + k]);
+        if (diff)
             return false;
-    return true;
+    }
+    uint32_t diff = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 15; k++)
+        if (i + k < n)
+            diff |= (uint32_t)(a[i + k] ^ b[i + k]);
+    return diff == 0;
 }
 
-__device__ __forceinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, int *err)
+__device__ __noinline__ bool xb_bytes_eq_ool(const uint8_t *a, const uint8_t *b, uint32_t n)
+{
+    return xb_bytes_eq(a, b, n);
+}
+
+__device__ __noinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, int *err)
 {
     uint8_t ka, kb; int16_t wa, wb; xb_i128 va, vb;
     if (xb_numeric_decode(a, &ka, &wa, &va) || xb_numeric_decode(b, &kb, &wb, &vb)) {
@@ -141,7 +173,7 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
 {
     const uint32_t lane = xb_lane();
     uint32_t active = active_in;
-    uint32_t mstack[XB_MASK_STACK];     /* per-thread copy of the lane-mask stack */
+    uint32_t ms0 = 0, ms1 = 0, ms2 = 0, ms3 = 0;   /* lane-mask stack (warp-uniform) */
     int msp = 0;
     bool failed = false;
 
@@ -220,7 +252,7 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
                 } else if (in.kind == XB_RK_TEXT) {
                     uint32_t la = RAUX(R, in.a), lb = RAUX(R, in.b);
                     if (act)
-                        c = (la == lb && xb_bytes_eq((const uint8_t *)x, (const uint8_t *)y, la)) ? 0 : 1;
+                        c = (la == lb && xb_bytes_eq_ool((const uint8_t *)x, (const uint8_t *)y, la)) ? 0 : 1;
                 } else if (in.kind == XB_RK_NUM) {
                     if (act) {
                         int err = 0;
@@ -248,29 +280,34 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
                 uint64_t x = RVAL(R, in.a), y = RVAL(R, in.b);
                 int opr = in.sub & 0x0f;
                 if (in.kind == XB_RK_INT) {
-                    int w = in.sub & 0xf0;
-                    int64_t a = (int64_t)x, b = (int64_t)y;
-                    __int128 r = 0;
+                    /* operands are int2/int4/int8 values sign-extended to 64 bits;
+                     * the result must fit the result type (xpu_basetype.cu:525-720) */
+                    const int w = in.sub & 0xf0;
+                    const int64_t a = (int64_t)x, b = (int64_t)y;
+                    int64_t r = 0;
                     bool bad = false;
-                    int64_t lo = (w == XB_AR_W2) ? -32768 : (w == XB_AR_W4) ? INT32_MIN : INT64_MIN;
-                    int64_t hi = (w == XB_AR_W2) ? 32767 : (w == XB_AR_W4) ? INT32_MAX : INT64_MAX;
-                    if (opr == XB_AR_ADD) r = (__int128)a + b;
-                    else if (opr == XB_AR_SUB) r = (__int128)a - b;
-                    else if (opr == XB_AR_MUL) r = (__int128)a * b;
-                    else {
-                        if (b == 0) {
-                            if (act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_DIV_ZERO); failed = true; }
-                            r = 0;
-                        } else if (b == -1) {
-                            r = -(__int128)a;
-                        } else {
-                            r = a / b;
-                        }
+                    if (opr == XB_AR_ADD) {
+                        r = (int64_t)((uint64_t)a + (uint64_t)b);
+                        bad = ((a ^ r) & (b ^ r)) < 0;
+                    } else if (opr == XB_AR_SUB) {
+                        r = (int64_t)((uint64_t)a - (uint64_t)b);
+                        bad = ((a ^ b) & (a ^ r)) < 0;
+                    } else if (opr == XB_AR_MUL) {
+                        r = (int64_t)((uint64_t)a * (uint64_t)b);
+                        const int64_t hi = __mul64hi(a, b);
+                        bad = hi != (r >> 63);
+                    } else if (b == 0) {
+                        if (act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_DIV_ZERO); failed = true; }
+                    } else if (b == -1) {
+                        bad = (a == INT64_MIN);
+                        r = (int64_t)(0 - (uint64_t)a);
+                    } else {
+                        r = a / b;
                     }
-                    if (r < lo || r > hi)
-                        bad = true;
+                    if (w == XB_AR_W2) bad |= (r < -32768 || r > 32767);
+                    else if (w == XB_AR_W4) bad |= (r < INT32_MIN || r > INT32_MAX);
                     if (bad && act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_INT_RANGE); failed = true; }
-                    out = (uint64_t)(int64_t)r;
+                    out = (uint64_t)r;
                 } else {
                     double a = __longlong_as_double(x), b = __longlong_as_double(y), r;
                     if (opr == XB_AR_ADD) r = a + b;
@@ -380,8 +417,13 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
             break;
         }
         case XB_OP_MASK_PUSH:
-            if (msp < XB_MASK_STACK)
-                mstack[msp] = active;
+            switch (msp) {
+            case 0: ms0 = active; break;
+            case 1: ms1 = active; break;
+            case 2: ms2 = active; break;
+            case 3: ms3 = active; break;
+            default: break;                     /* deeper: restored to active_in */
+            }
             msp++;
             break;
         case XB_OP_MASK_NARROW: {
@@ -393,10 +435,13 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
         }
         case XB_OP_MASK_POP:
             msp--;
-            if (msp >= 0 && msp < XB_MASK_STACK)
-                active = mstack[msp];
-            else
-                active = active_in;
+            switch (msp) {
+            case 0: active = ms0; break;
+            case 1: active = ms1; break;
+            case 2: active = ms2; break;
+            case 3: active = ms3; break;
+            default: active = active_in; break;
+            }
             break;
         case XB_OP_HASH_INIT:
             RVAL(R, in.dst) = 0xffffffffULL;

@@ -417,7 +417,8 @@ xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t ha
  * executor kernel
  * ================================================================ */
 struct XbExecArgs {
-    const xb_plan  *plan;
+    const xb_plan  *plan;           /* device copy (copied into shared memory) */
+    uint32_t        plan_bytes;     /* bytes of the plan copy: header + used code */
     const xb_task  *tasks;          /* work queue: chunks of this launch */
     uint32_t        ntasks;
     uint64_t        nunits;         /* total units over all tasks */
@@ -428,40 +429,50 @@ struct XbExecArgs {
     xb_status      *st;
 };
 
-struct XbCounters {
+/* per-warp mutable state, in shared memory */
+struct XbWarpState {
     unsigned long long raw, in, out;
     unsigned long long depth[XB_MAX_DEPTH + 1];
+    uint32_t failed;
+    uint32_t __pad;
 };
 
+/* everything a warp needs, passed by value (registers) */
 struct XbCtx {
-    const xb_plan  *plan;
+    const xb_plan  *plan;           /* shared-memory copy */
     XbRegs          R;
     char           *sm_entries;
     uint32_t        sm_mask;
     xb_gtable      *gt;
     xb_status      *st;
-    XbCounters      cnt;
-    bool            failed;
+    XbWarpState    *ws;
 };
 
-__device__ __noinline__ void xb_groupby(XbCtx &c, uint32_t act)
+__device__ __forceinline__ bool xb_failed(const XbCtx &c)
+{
+    return *(volatile uint32_t *)&c.ws->failed != 0;
+}
+__device__ __forceinline__ void xb_set_failed(const XbCtx &c)
+{
+    c.ws->failed = 1;
+}
+
+__device__ __noinline__ void xb_groupby(XbCtx c, uint32_t act)
 {
     const xb_plan *plan = c.plan;
     const uint32_t lane = xb_lane();
-    if (plan->gb_args.count && !xb_vm_run(plan->insns + plan->gb_args.start,
-                                         plan->gb_args.count, c.R, act, c.st)) {
-        c.failed = true;
+    /* the translator emits the key-hash program right after the argument
+     * program, so both run as one instruction stream */
+    const uint32_t n = plan->gb_args.count +
+                       (plan->has_groupby == 1 ? plan->gb_keyhash.count : 0);
+    if (n && !xb_vm_run(plan->insns + plan->gb_args.start, n, c.R, act, c.st)) {
+        xb_set_failed(c);
         return;
     }
     uint32_t hash = 0;
-    if (plan->has_groupby == 1) {
-        if (!xb_vm_run(plan->insns + plan->gb_keyhash.start,
-                       plan->gb_keyhash.count, c.R, act, c.st)) {
-            c.failed = true;
-            return;
-        }
+    if (plan->has_groupby == 1)
         hash = (uint32_t)RVAL(c.R, plan->gb_keyhash.result);
-    }
+    bool bad = false;
     if ((act >> lane) & 1u) {
         xb_keyimg keys[XB_MAX_KEYS];
         for (uint32_t k = 0; k < plan->nkeys; k++)
@@ -481,32 +492,49 @@ __device__ __noinline__ void xb_groupby(XbCtx &c, uint32_t act)
         if (e)
             xb_update_states(plan, e, c.R, lane, c.st);
         else
-            c.failed = true;
+            bad = true;
     }
     /* keep the failure flag warp-uniform: later full-mask ballots rely on it */
-    c.failed = __any_sync(XB_FULL, c.failed);
+    if (__any_sync(XB_FULL, bad))
+        xb_set_failed(c);
 }
 
 /* load the inner row's pre-decoded registers for lanes in 'cand' */
 __device__ __forceinline__ void
-xb_load_inner(const xb_inner *in, XbRegs &R, uint32_t lane, uint32_t cand, uint32_t row)
+xb_load_inner(const xb_inner *in, XbRegs R, uint32_t lane, uint32_t cand, uint32_t row,
+              const uint8_t *rk)
 {
     const bool mine = (cand >> lane) & 1u;
     const uint32_t words = (in->nitems + 31) / 32;
+    const uint32_t live = in->live, hasnull = in->hasnull;
     for (uint32_t k = 0; k < in->nloads; k++) {
-        uint32_t reg = in->load[k].reg;
-        bool isnull = true;
+        if (!((live >> k) & 1u))
+            continue;
+        const uint32_t reg = in->load[k].reg;
+        bool isnull = !mine;
         if (mine) {
             RVAL(R, reg) = __ldg((const unsigned long long *)&in->vals[(size_t)k * in->nitems + row]);
-            RAUX(R, reg) = __ldg(&in->auxs[(size_t)k * in->nitems + row]);
-            isnull = (__ldg(&in->nulls[(size_t)k * words + row / 32]) >> (row % 32)) & 1u;
+            if (rk[reg] == XB_RK_TEXT)
+                RAUX(R, reg) = __ldg(&in->auxs[(size_t)k * in->nitems + row]);
+            if ((hasnull >> k) & 1u)
+                isnull = (__ldg(&in->nulls[(size_t)k * words + row / 32]) >> (row % 32)) & 1u;
         }
         xb_set_null(R, reg, isnull);
     }
 }
 
+template <int D> __device__ __forceinline__ void xb_join_depth(const XbCtx &c, uint32_t act);
+
+/* depths beyond the second are entered through a call, bounding how much
+ * probe state is kept live in one function */
 template <int D>
-__device__ __noinline__ void xb_join_depth(XbCtx &c, uint32_t act)
+__device__ __noinline__ void xb_join_depth_call(XbCtx c, uint32_t act)
+{
+    xb_join_depth<D>(c, act);
+}
+
+template <int D>
+__device__ __forceinline__ void xb_join_depth(const XbCtx &c, uint32_t act)
 {
     const xb_plan *plan = c.plan;
     if constexpr (D > XB_MAX_DEPTH) {
@@ -514,58 +542,99 @@ __device__ __noinline__ void xb_join_depth(XbCtx &c, uint32_t act)
         return;
     } else {
         if ((uint32_t)D > plan->nrels) {
-            c.cnt.out += __popc(act);
+            if (xb_lane() == 0)
+                c.ws->out += __popc(act);
             if (plan->has_groupby)
                 xb_groupby(c, act);
             return;
         }
         const uint32_t lane = xb_lane();
         const xb_inner *in = &plan->inner[D];
-        const xb_prog &hp = plan->hash_value[D];
-        if (!xb_vm_run(plan->insns + hp.start, hp.count, c.R, act, c.st)) {
-            c.failed = true;
-            return;
-        }
-        const uint32_t hash = (uint32_t)RVAL(c.R, hp.result);
-        uint64_t pos = hash & in->cap_mask;
+        /* probe key: fused (inline hash of the outer key) or by the VM */
+        uint32_t hash;
         bool live = ((act >> lane) & 1u) && in->nitems > 0;
+        uint64_t okey = 0;
+        const int fast = in->fast_key;
+        if (fast >= 0) {
+            const uint32_t ox = in->fast_outer;
+            okey = RVAL(c.R, ox);
+            if (RISNULL(c.R, ox))
+                live = false;               /* NULL = anything is never true */
+            uint32_t hv;
+            switch (in->fast_hk) {
+            case XB_HK_W1: hv = xb_hash_u32((uint32_t)okey, 1); break;
+            case XB_HK_W2: hv = xb_hash_u32((uint32_t)okey, 2); break;
+            case XB_HK_W4: hv = xb_hash_u32((uint32_t)okey, 4); break;
+            default:       hv = xb_hash_u64(okey); break;
+            }
+            hash = xb_hash_merge(0xffffffffU, hv) ^ 0xffffffffU;
+        } else {
+            const xb_prog &hp = plan->hash_value[D];
+            if (!xb_vm_run(plan->insns + hp.start, hp.count, c.R, act, c.st)) {
+                xb_set_failed(c);
+                return;
+            }
+            hash = (uint32_t)RVAL(c.R, hp.result);
+        }
+        const bool key32 = fast >= 0 && in->key32;
+        uint32_t tag = hash;
+        if (key32) {
+            tag = (uint32_t)okey;
+            if ((int64_t)okey != (int64_t)(int32_t)okey)
+                live = false;               /* outside any 32-bit inner key */
+        }
+        const uint64_t *kcol = (fast >= 0 && !key32) ? in->vals + (size_t)fast * in->nitems : nullptr;
+        const uint32_t *kn = (kcol && ((in->hasnull >> fast) & 1u))
+                             ? in->nulls + (size_t)fast * ((in->nitems + 31) / 32) : nullptr;
+        uint64_t pos = hash & in->cap_mask;
         for (;;) {
             uint32_t row = 0;
             bool got = false;
             if (live) {
                 for (uint32_t probe = 0; probe <= in->cap_mask; probe++) {
-                    uint64_t ent = __ldg((const unsigned long long *)&in->index[pos]);
+                    const uint64_t ent = __ldg((const unsigned long long *)&in->index[pos]);
                     pos = (pos + 1) & in->cap_mask;
                     if (ent == 0) { live = false; break; }
-                    if ((uint32_t)(ent >> 32) == hash) {
-                        row = (uint32_t)ent - 1;
-                        got = true;
-                        if (in->unique_hash)
-                            live = false;
-                        break;
+                    if ((uint32_t)(ent >> 32) != tag)
+                        continue;
+                    const uint32_t r = (uint32_t)ent - 1;
+                    if (in->unique_hash)
+                        live = false;           /* no other inner row has this hash */
+                    if (kcol) {
+                        const bool knull = kn && ((__ldg(&kn[r / 32]) >> (r % 32)) & 1u);
+                        if (knull || __ldg((const unsigned long long *)&kcol[r]) != okey) {
+                            if (!live) break;
+                            continue;
+                        }
                     }
+                    row = r;
+                    got = true;
+                    break;
                 }
-                if (!got) live = false;
             }
             const uint32_t cand = __ballot_sync(XB_FULL, got);
             if (cand == 0)
                 break;
-            xb_load_inner(in, c.R, lane, cand, row);
+            xb_load_inner(in, c.R, lane, cand, row, plan->rk);
             uint32_t ok = cand;
             const xb_prog &jp = plan->join_quals[D];
             if (jp.count) {
                 if (!xb_vm_run(plan->insns + jp.start, jp.count, c.R, cand, c.st)) {
-                    c.failed = true;
+                    xb_set_failed(c);
                     return;
                 }
-                bool pass = ((cand >> lane) & 1u) && !RISNULL(c.R, jp.result) &&
-                            RVAL(c.R, jp.result) != 0;
+                const bool pass = ((cand >> lane) & 1u) && !RISNULL(c.R, jp.result) &&
+                                  RVAL(c.R, jp.result) != 0;
                 ok = __ballot_sync(XB_FULL, pass);
             }
-            c.cnt.depth[D] += __popc(ok);
+            if (lane == 0)
+                c.ws->depth[D] += __popc(ok);
             if (ok) {
-                xb_join_depth<D + 1>(c, ok);
-                if (c.failed)
+                if constexpr (D + 1 >= 3)
+                    xb_join_depth_call<D + 1>(c, ok);
+                else
+                    xb_join_depth<D + 1>(c, ok);
+                if (xb_failed(c))
                     return;
             }
         }
@@ -573,7 +642,7 @@ __device__ __noinline__ void xb_join_depth(XbCtx &c, uint32_t act)
 }
 
 /* scan quals + joins + group-by over one batch of 32 decoded rows */
-__device__ __forceinline__ void xb_process_batch(XbCtx &c, uint32_t loaded)
+__device__ __forceinline__ void xb_process_batch(const XbCtx &c, uint32_t loaded)
 {
     const xb_plan *plan = c.plan;
     const uint32_t lane = xb_lane();
@@ -581,40 +650,41 @@ __device__ __forceinline__ void xb_process_batch(XbCtx &c, uint32_t loaded)
     if (plan->scan_quals.count) {
         if (!xb_vm_run(plan->insns + plan->scan_quals.start, plan->scan_quals.count,
                        c.R, loaded, c.st)) {
-            c.failed = true;
+            xb_set_failed(c);
             return;
         }
-        int r = plan->scan_quals.result;
-        bool ok = ((loaded >> lane) & 1u) && !RISNULL(c.R, r) && RVAL(c.R, r) != 0;
+        const int r = plan->scan_quals.result;
+        const bool ok = ((loaded >> lane) & 1u) && !RISNULL(c.R, r) && RVAL(c.R, r) != 0;
         pass = __ballot_sync(XB_FULL, ok);
     }
-    c.cnt.in += __popc(pass);
+    if (lane == 0)
+        c.ws->in += __popc(pass);
     if (pass)
         xb_join_depth<1>(c, pass);
 }
 
 /* write the NULL ballots of the depth-0 load registers */
 __device__ __forceinline__ void
-xb_publish_load_nulls(const xb_plan *plan, XbRegs &R, bool ok, uint32_t nullbits)
+xb_publish_load_nulls(const xb_plan *plan, XbRegs R, bool ok, uint32_t nullbits)
 {
     for (uint32_t i = 0; i < plan->nload0; i++)
         xb_set_null(R, plan->load0[i].reg, !ok || ((nullbits >> i) & 1u));
 }
 
 __device__ __noinline__ void
-xb_scan_heap_page(XbCtx &c, const kern_data_store *kds, const XbCol *cols, int kds_ncols,
+xb_scan_heap_page(XbCtx c, const kern_data_store *kds, const XbCol *cols, int kds_ncols,
                   uint32_t block_id)
 {
     const xb_plan *plan = c.plan;
     const uint32_t lane = xb_lane();
     const uint8_t *page = (const uint8_t *)kds + kds->block_offset + (size_t)block_id * PGSTROM_BLCKSZ;
-    const uint32_t pd_lower = *(const uint16_t *)(page + 12);
+    const uint32_t pd_lower = (uint32_t)xb_fetch_le(page + 12, 2);
     uint32_t nlp = 0;
-    if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ)
+    if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ) {
         nlp = (pd_lower - SizeOfPageHeaderData) / sizeof(ItemIdData);
-    else if (pd_lower > PGSTROM_BLCKSZ) {
+    } else if (pd_lower > PGSTROM_BLCKSZ) {
         if (lane == 0) XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
-        c.failed = true;
+        xb_set_failed(c);
         return;
     }
     for (uint32_t base = 0; base < nlp; base += 32) {
@@ -622,7 +692,7 @@ xb_scan_heap_page(XbCtx &c, const kern_data_store *kds, const XbCol *cols, int k
         bool normal = false, ok = false;
         uint32_t nullbits = 0;
         if (idx < nlp) {
-            const uint32_t lp = ((const uint32_t *)(page + SizeOfPageHeaderData))[idx];
+            const uint32_t lp = (uint32_t)xb_fetch_le(page + SizeOfPageHeaderData + 4 * idx, 4);
             if (ITEMID_FLAGS(lp) == LP_NORMAL) {
                 const uint32_t off = ITEMID_OFF(lp), len = ITEMID_LEN(lp);
                 normal = true;
@@ -641,23 +711,23 @@ xb_scan_heap_page(XbCtx &c, const kern_data_store *kds, const XbCol *cols, int k
                                              plan->load0, plan->nload0,
                                              c.R.val + lane, c.R.aux + lane, 32, false, &nullbits);
                     }
-                    if (!ok) {
+                    if (!ok)
                         XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
-                    }
                 }
             }
         }
         const uint32_t nrm = __ballot_sync(XB_FULL, normal);
-        c.cnt.raw += __popc(nrm);
+        if (lane == 0)
+            c.ws->raw += __popc(nrm);
         if (__any_sync(XB_FULL, normal && !ok)) {
-            c.failed = true;
+            xb_set_failed(c);
             return;
         }
         xb_publish_load_nulls(plan, c.R, ok, nullbits);
         const uint32_t loaded = __ballot_sync(XB_FULL, ok);
         if (loaded)
             xb_process_batch(c, loaded);
-        if (c.failed)
+        if (xb_failed(c))
             return;
     }
 }
@@ -735,7 +805,7 @@ xb_arrow_load(const kern_data_store *kds, const kern_colmeta *cm, uint32_t row, 
 }
 
 __device__ __noinline__ void
-xb_scan_arrow_unit(XbCtx &c, const kern_data_store *kds, uint32_t unit)
+xb_scan_arrow_unit(XbCtx c, const kern_data_store *kds, uint32_t unit)
 {
     const xb_plan *plan = c.plan;
     const uint32_t lane = xb_lane();
@@ -763,22 +833,24 @@ xb_scan_arrow_unit(XbCtx &c, const kern_data_store *kds, uint32_t unit)
                 if (isnull) nullbits |= 1u << i;
             }
         }
-        c.cnt.raw += __popc(__ballot_sync(XB_FULL, exists));
+        const uint32_t ex = __ballot_sync(XB_FULL, exists);
+        if (lane == 0)
+            c.ws->raw += __popc(ex);
         if (__any_sync(XB_FULL, exists && !ok)) {
-            c.failed = true;
+            xb_set_failed(c);
             return;
         }
         xb_publish_load_nulls(plan, c.R, ok, nullbits);
         const uint32_t loaded = __ballot_sync(XB_FULL, ok);
         if (loaded)
             xb_process_batch(c, loaded);
-        if (c.failed)
+        if (xb_failed(c))
             return;
     }
 }
 
 __device__ __noinline__ void
-xb_scan_row_unit(XbCtx &c, const kern_data_store *kds, const XbCol *cols, uint32_t unit)
+xb_scan_row_unit(XbCtx c, const kern_data_store *kds, const XbCol *cols, uint32_t unit)
 {
     const xb_plan *plan = c.plan;
     const uint32_t lane = xb_lane();
@@ -804,23 +876,25 @@ xb_scan_row_unit(XbCtx &c, const kern_data_store *kds, const XbCol *cols, uint32
                 if (!ti->has_xact_attrs && ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 &&
                     pay <= ti->t_len && off >= ti->t_len &&
                     (!hasnull || 15u + (natts + 7) / 8 <= pay))
-                    ok = xb_decode_tuple(cols, natts, (ti->t_infomask & HEAP_HASNULL) ? ti->t_bits : nullptr,
+                    ok = xb_decode_tuple(cols, natts, hasnull ? ti->t_bits : nullptr,
                                          t + pay, ti->t_len - pay, plan->load0, plan->nload0,
                                          c.R.val + lane, c.R.aux + lane, 32, false, &nullbits);
             }
             if (exists && !ok)
                 XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
         }
-        c.cnt.raw += __popc(__ballot_sync(XB_FULL, exists));
+        const uint32_t ex = __ballot_sync(XB_FULL, exists);
+        if (lane == 0)
+            c.ws->raw += __popc(ex);
         if (__any_sync(XB_FULL, exists && !ok)) {
-            c.failed = true;
+            xb_set_failed(c);
             return;
         }
         xb_publish_load_nulls(plan, c.R, ok, nullbits);
         const uint32_t loaded = __ballot_sync(XB_FULL, ok);
         if (loaded)
             xb_process_batch(c, loaded);
-        if (c.failed)
+        if (xb_failed(c))
             return;
     }
 }
@@ -837,21 +911,34 @@ xb_find_task(const xb_task *tasks, uint32_t ntasks, uint64_t unit)
     return lo;
 }
 
+/*
+ * Shared memory of a CTA:
+ *   [plan copy: header + used code][column cache][group table][warp states]
+ *   [per-warp register files]
+ */
 __global__ void __launch_bounds__(XB_BLOCK, 3)
 xb_exec_kernel(XbExecArgs args)
 {
     extern __shared__ __align__(16) char smem[];
-    const xb_plan *plan = args.plan;
-    /* all chunks of a launch share one column layout (checked by the host) */
-    const kern_data_store *kds0 = args.tasks[0].kds;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
 
-    XbCol *cols = (XbCol *)smem;
-    char *sm_entries = smem + sizeof(XbCol) * XB_MAX_COLS;
-    const size_t sm_bytes = (size_t)args.sm_cap * plan->gent_size;
-    char *regs_base = sm_entries + sm_bytes + (size_t)warp * args.regs_bytes;
+    xb_plan *plan = (xb_plan *)smem;
+    XbCol *cols = (XbCol *)(smem + args.plan_bytes);
+    char *sm_entries = (char *)(cols + XB_MAX_COLS);
+    const size_t sm_bytes = (size_t)args.sm_cap * args.plan->gent_size;
+    XbWarpState *wstates = (XbWarpState *)(sm_entries + sm_bytes);
+    char *regs_base = (char *)(wstates + XB_WARPS) + (size_t)warp * args.regs_bytes;
 
+    /* stage the plan (and only the VM code it uses) in shared memory */
+    {
+        const uint4 *src = (const uint4 *)args.plan;
+        uint4 *dst = (uint4 *)plan;
+        for (uint32_t i = threadIdx.x; i < args.plan_bytes / 16; i += blockDim.x)
+            dst[i] = src[i];
+    }
+    /* all chunks of a launch share one column layout (checked by the host) */
+    const kern_data_store *kds0 = args.tasks[0].kds;
     const int kds_ncols = kds0->ncols < XB_MAX_COLS ? (int)kds0->ncols : XB_MAX_COLS;
     for (int i = threadIdx.x; i < kds_ncols; i += blockDim.x) {
         cols[i].attlen = kds0->colmeta[i].attlen;
@@ -860,6 +947,8 @@ xb_exec_kernel(XbExecArgs args)
     }
     for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
         ((uint32_t *)sm_entries)[i] = 0;
+    for (size_t i = threadIdx.x; i < sizeof(XbWarpState) * XB_WARPS / 4; i += blockDim.x)
+        ((uint32_t *)wstates)[i] = 0;
     __syncthreads();
 
     XbCtx c;
@@ -869,8 +958,7 @@ xb_exec_kernel(XbExecArgs args)
     c.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
     c.gt = args.gt;
     c.st = args.st;
-    memset(&c.cnt, 0, sizeof(c.cnt));
-    c.failed = false;
+    c.ws = &wstates[warp];
     for (uint32_t r = lane; r < plan->nregs; r += 32)
         c.R.nullm[r] = XB_FULL;
     __syncwarp();
@@ -881,7 +969,7 @@ xb_exec_kernel(XbExecArgs args)
         if (lane == 0)
             claim = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
         claim = __shfl_sync(XB_FULL, claim, 0);
-        while (claim < args.nunits && !c.failed) {
+        while (claim < args.nunits && !xb_failed(c)) {
             uint64_t next = 0;
             if (lane == 0)
                 next = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
@@ -896,7 +984,7 @@ xb_exec_kernel(XbExecArgs args)
                 if ((((uintptr_t)p) & 15) == 0)
                     xb_prefetch_l2(p, PGSTROM_BLCKSZ);
             }
-            for (uint32_t k = 0; k < stride && claim + k < args.nunits && !c.failed; k++) {
+            for (uint32_t k = 0; k < stride && claim + k < args.nunits && !xb_failed(c); k++) {
                 const uint64_t u = claim + k;
                 const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
                 xb_scan_heap_page(c, t.kds, cols, kds_ncols, (uint32_t)(u - t.unit_base));
@@ -911,7 +999,7 @@ xb_exec_kernel(XbExecArgs args)
             if (lane == 0)
                 unit = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
             unit = __shfl_sync(XB_FULL, unit, 0);
-            if (unit >= args.nunits || c.failed)
+            if (unit >= args.nunits || xb_failed(c))
                 break;
             const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, unit)];
             if (args.format == KDS_FORMAT_ARROW)
@@ -925,11 +1013,12 @@ xb_exec_kernel(XbExecArgs args)
 
     /* per-warp statistics */
     if (lane == 0) {
-        atomicAdd((unsigned long long *)&args.st->nitems_raw, c.cnt.raw);
-        atomicAdd((unsigned long long *)&args.st->nitems_in, c.cnt.in);
-        atomicAdd((unsigned long long *)&args.st->nitems_out, c.cnt.out);
+        const XbWarpState *w = c.ws;
+        atomicAdd((unsigned long long *)&args.st->nitems_raw, w->raw);
+        atomicAdd((unsigned long long *)&args.st->nitems_in, w->in);
+        atomicAdd((unsigned long long *)&args.st->nitems_out, w->out);
         for (uint32_t d = 1; d <= plan->nrels && d <= XB_MAX_DEPTH; d++)
-            atomicAdd((unsigned long long *)&args.st->nitems_depth[d], c.cnt.depth[d]);
+            atomicAdd((unsigned long long *)&args.st->nitems_depth[d], w->depth[d]);
     }
     __syncthreads();
 
@@ -1002,20 +1091,32 @@ xb_build_inner(XbBuildArgs args)
             XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
             continue;
         }
-        for (uint32_t k = 0; k < in->nloads; k++) {
-            if ((nullbits >> k) & 1u)
-                atomicOr(&in->nulls[(size_t)k * words + row / 32], 1u << (row % 32));
+        if (nullbits) {
+            for (uint32_t k = 0; k < in->nloads; k++) {
+                if ((nullbits >> k) & 1u)
+                    atomicOr(&in->nulls[(size_t)k * words + row / 32], 1u << (row % 32));
+            }
+            atomicOr(&in->hasnull, nullbits);
         }
-        /* index insert: (hash << 32) | (row + 1) */
+        /* index insert at hash & mask (linear probing).  Entries hold
+         * (hash << 32 | row + 1), or (key << 32 | row + 1) for a 32-bit
+         * fused join key; a NULL fused key can never satisfy the join. */
         const uint32_t hash = ti->hash;
-        const unsigned long long ent = ((unsigned long long)hash << 32) | (row + 1);
+        uint32_t tag = hash;
+        if (in->key32) {
+            const int k = in->fast_key;
+            if ((nullbits >> k) & 1u)
+                continue;
+            tag = (uint32_t)in->vals[(size_t)k * n + row];
+        }
+        const unsigned long long ent = ((unsigned long long)tag << 32) | (row + 1);
         uint64_t pos = hash & in->cap_mask;
         for (uint32_t probe = 0; probe <= in->cap_mask; probe++) {
             unsigned long long old = atomicCAS((unsigned long long *)&in->index[pos], 0ULL, ent);
             if (old == 0)
                 break;
-            if ((uint32_t)(old >> 32) == hash)
-                atomicExch(&in->unique_hash, 0u);
+            if ((uint32_t)(old >> 32) == tag)
+                atomicExch(&in->unique_hash, 0u);   /* a second row with this tag */
             pos = (pos + 1) & in->cap_mask;
         }
     }
@@ -1302,6 +1403,7 @@ struct xpuB200Session {
     uint32_t        d_tasks_cap = 0;
     uint32_t        sm_cap = 0;
     uint32_t        regs_bytes = 0;
+    uint32_t        plan_bytes = 0;
     size_t          smem_bytes = 0;
     int             grid = 0;
     uint64_t        total_raw = 0, total_in = 0, total_out = 0;
@@ -1555,8 +1657,10 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
 
     /* launch geometry */
     s->regs_bytes = (uint32_t)PGSTROM_TYPEALIGN(16, (size_t)plan->nregs * (32 * 8 + 32 * 4 + 4) + 4 * XB_MASK_STACK + 16);
-    s->smem_bytes = sizeof(XbCol) * XB_MAX_COLS + (size_t)s->sm_cap * plan->gent_size +
-                    (size_t)XB_WARPS * s->regs_bytes;
+    s->plan_bytes = (uint32_t)PGSTROM_TYPEALIGN(16, offsetof(xb_plan, insns) +
+                                                 sizeof(xb_insn) * (size_t)plan->ninsns);
+    s->smem_bytes = s->plan_bytes + sizeof(XbCol) * XB_MAX_COLS + (size_t)s->sm_cap * plan->gent_size +
+                    sizeof(XbWarpState) * XB_WARPS + (size_t)XB_WARPS * s->regs_bytes;
     if (cudaFuncSetAttribute(xb_exec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)s->smem_bytes) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "dynamic shared memory of %zu bytes not available", s->smem_bytes);
@@ -1592,6 +1696,7 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
 {
     XbExecArgs a;
     a.plan = s->d_plan;
+    a.plan_bytes = s->plan_bytes;
     a.tasks = d_tasks;
     a.ntasks = ntasks;
     a.nunits = nunits;

@@ -146,6 +146,14 @@ typedef struct xb_inner {
     uint64_t   *vals;           /* [nloads][nitems] register images */
     uint32_t   *auxs;           /* [nloads][nitems] */
     uint32_t   *nulls;          /* [nloads][(nitems+31)/32] bit = NULL */
+    uint32_t    hasnull;        /* bit k: inner column k has NULLs (set by the build) */
+    uint32_t    live;           /* bit k: register of load k is read after the join */
+    /* fused probe: HashValue(outer) + JoinQuals(outer = inner key) */
+    int16_t     fast_key;       /* load index of the inner key, -1: no fused probe */
+    uint8_t     fast_outer;     /* outer key register */
+    uint8_t     fast_hk;        /* hash kind of the outer key */
+    uint32_t    key32;          /* index entries hold (key32 << 32 | row + 1):
+                                 * the fused key is int2 / int4 / date */
     xb_load     load[XB_MAX_LOADS];
 } xb_inner;
 
