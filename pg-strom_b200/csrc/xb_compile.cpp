@@ -963,6 +963,51 @@ struct Compiler {
         }
     }
 
+    /*
+     * Hashes of text / numeric values that come straight from an inner
+     * relation's column (a group key taken from a dimension table, a join
+     * key carried to a deeper depth) depend only on the inner row: the
+     * build computes them once per inner row and HASH ops read that copy.
+     * Applies when the register is loaded at exactly one inner depth and
+     * never written by an instruction.
+     */
+    void mark_cached_hashes()
+    {
+        uint64_t written = 0;
+        for (uint32_t i = 0; i < plan->ninsns; i++) {
+            const xb_insn &x = plan->insns[i];
+            switch (x.op) {
+            case XB_OP_END: case XB_OP_MASK_PUSH: case XB_OP_MASK_NARROW: case XB_OP_MASK_POP:
+                break;
+            default:
+                written |= 1ULL << x.dst;
+                break;
+            }
+        }
+        uint64_t outer = 0;
+        for (uint32_t i = 0; i < plan->nload0; i++)
+            outer |= 1ULL << plan->load0[i].reg;
+        for (uint32_t i = 0; i < plan->ninsns; i++) {
+            xb_insn &x = plan->insns[i];
+            if ((x.op != XB_OP_HASH1 && x.op != XB_OP_HASH_ADD) ||
+                (x.sub != XB_HK_TEXT && x.sub != XB_HK_NUM))
+                continue;
+            const uint64_t bit = 1ULL << x.a;
+            if ((written & bit) || (outer & bit))
+                continue;
+            int found_d = -1, found_k = -1, nfound = 0;
+            for (uint32_t d = 1; d <= plan->nrels; d++)
+                for (uint32_t k = 0; k < plan->inner[d].nloads; k++)
+                    if (plan->inner[d].load[k].reg == x.a) {
+                        found_d = (int)d; found_k = (int)k; nfound++;
+                    }
+            if (nfound != 1)
+                continue;
+            plan->inner[found_d].hashed |= 1u << found_k;
+            x.sub = XB_HK_CACHED;
+        }
+    }
+
     bool run(const kern_multirels *kmrels)
     {
         memset(plan, 0, sizeof(xb_plan));
@@ -1046,6 +1091,13 @@ struct Compiler {
         if (!groupby())
             return false;
         compute_liveness();
+        mark_cached_hashes();
+        if (plan->has_groupby) {
+            const bool kh = plan->has_groupby == 1 && plan->gb_keyhash.count > 0;
+            plan->gb_all.start = plan->gb_args.count ? plan->gb_args.start : plan->gb_keyhash.start;
+            plan->gb_all.count = (uint16_t)(plan->gb_args.count + (kh ? plan->gb_keyhash.count : 0));
+            plan->gb_all.result = kh ? plan->gb_keyhash.result : (int16_t)-1;
+        }
         if (plan->has_groupby == 0 && !(plan->task_kind & DEVTASK__PREAGG))
             return fail("scan/join without device projection or GROUP BY is not supported");
         return err.empty();

@@ -22,8 +22,8 @@
 struct XbRegs {
     uint64_t   *val;        /* [nregs][32] */
     uint32_t   *aux;        /* [nregs][32] */
+    uint32_t   *hc;         /* [nregs][32] hash copied from an inner build */
     uint32_t   *nullm;      /* [nregs]  bit set = NULL */
-    uint32_t   *mstack;     /* [XB_MASK_STACK] */
 };
 
 __device__ __forceinline__ uint32_t xb_lane(void)
@@ -33,23 +33,22 @@ __device__ __forceinline__ uint32_t xb_lane(void)
     return r;
 }
 
-__device__ __forceinline__ size_t xb_regs_bytes(uint32_t nregs)
-{
-    return (size_t)nregs * (32 * 8 + 32 * 4 + 4) + 4 * XB_MASK_STACK + 16;
-}
+/* bytes of a register file of nregs registers (host and device) */
+#define XB_REGS_BYTES(nregs)    (((size_t)(nregs) * (32 * 8 + 32 * 4 + 32 * 4 + 4) + 15) & ~(size_t)15)
 
 __device__ __forceinline__ XbRegs xb_regs_setup(char *base, uint32_t nregs)
 {
     XbRegs R;
     R.val = (uint64_t *)base;
     R.aux = (uint32_t *)(base + (size_t)nregs * 256);
-    R.nullm = (uint32_t *)(base + (size_t)nregs * 384);
-    R.mstack = R.nullm + nregs;
+    R.hc = (uint32_t *)(base + (size_t)nregs * 384);
+    R.nullm = (uint32_t *)(base + (size_t)nregs * 512);
     return R;
 }
 
 #define RVAL(R, r)      ((R).val[(r) * 32 + lane])
 #define RAUX(R, r)      ((R).aux[(r) * 32 + lane])
+#define RHC(R, r)       ((R).hc[(r) * 32 + lane])
 #define RISNULL(R, r)   ((((R).nullm[r]) >> lane) & 1u)
 
 /* all lanes call this convergently; writes the NULL ballot of register r.
@@ -167,9 +166,9 @@ __device__ __noinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, i
  * 'active' lanes carry a row.  Memory is dereferenced and errors are
  * raised only for active lanes with non-NULL inputs.
  * --------------------------------------------------------------- */
-__device__ __noinline__ bool
-xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
-          uint32_t active_in, xb_status *st)
+__device__ __forceinline__ bool
+xb_vm_exec(const xb_insn *__restrict__ code, uint32_t count, const XbRegs &R,
+           uint32_t active_in, xb_status *st)
 {
     const uint32_t lane = xb_lane();
     uint32_t active = active_in;
@@ -228,7 +227,8 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
             uint32_t h = 0xffffffffU;
             if (!RISNULL(R, in.a)) {
                 bool bad = false;
-                const uint32_t hv = xb_hash_reg(in.sub, RVAL(R, in.a), RAUX(R, in.a), act, &bad);
+                const uint32_t hv = in.sub == XB_HK_CACHED ? RHC(R, in.a)
+                                  : xb_hash_reg(in.sub, RVAL(R, in.a), RAUX(R, in.a), act, &bad);
                 if (bad) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT); failed = true; }
                 h = xb_hash_merge(h, hv);
             }
@@ -451,7 +451,8 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
             uint32_t h = (uint32_t)RVAL(R, in.dst);
             if (!RISNULL(R, in.a)) {
                 bool bad = false;
-                const uint32_t hv = xb_hash_reg(in.sub, RVAL(R, in.a), RAUX(R, in.a), act, &bad);
+                const uint32_t hv = in.sub == XB_HK_CACHED ? RHC(R, in.a)
+                                  : xb_hash_reg(in.sub, RVAL(R, in.a), RAUX(R, in.a), act, &bad);
                 if (bad) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT); failed = true; }
                 h = xb_hash_merge(h, hv);
             }
@@ -491,6 +492,14 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
     }
     __syncwarp();
     return !__any_sync(XB_FULL, failed);
+}
+
+/* out-of-line entry for callers other than the executor's main loop */
+__device__ __noinline__ bool
+xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
+          uint32_t active_in, xb_status *st)
+{
+    return xb_vm_exec(code, count, R, active_in, st);
 }
 
 /* ---------------------------------------------------------------

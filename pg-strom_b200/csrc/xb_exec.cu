@@ -40,6 +40,7 @@
 #define XB_WARPS        (XB_BLOCK / 32)
 #define XB_CLAIM        4           /* heap pages claimed per warp at a time */
 #define XB_ROWS_UNIT    1024        /* rows per unit for ARROW / ROW chunks */
+#define XB_MIN_BLOCKS   2           /* resident CTAs per SM the kernel is built for */
 #define XB_PROBE_LIMIT  4096        /* max probes in the global group table */
 
 /* ================================================================
@@ -113,113 +114,6 @@ __device__ __noinline__ void xb_init_states(const xb_plan *plan, char *e)
         case KAGG_ACTION__PMAX_FP64:
             s[0] = (uint64_t)INT64_MIN;
             break;
-        default:
-            break;
-        }
-    }
-}
-
-/* __updateOneTupleGroupBy + __update_groupby__* (cuda_gpupreagg.cu:1196-1605) */
-__device__ __noinline__ void xb_update_states(const xb_plan *plan, char *e, const XbRegs &R,
-                                 uint32_t lane, xb_status *st)
-{
-    for (uint32_t i = 0; i < plan->naggs; i++) {
-        const xb_agg &a = plan->aggs[i];
-        if (a.state_sz == 0)
-            continue;
-        if (a.filter >= 0 && (RISNULL(R, a.filter) || RVAL(R, a.filter) == 0))
-            continue;
-        char *s = e + a.state_off;
-        bool n0 = a.arg0 < 0 ? true : (RISNULL(R, a.arg0) != 0);
-        uint64_t v0 = a.arg0 < 0 ? 0 : RVAL(R, a.arg0);
-        int rk0 = a.arg0 < 0 ? 0 : plan->rk[a.arg0];
-        switch (a.action) {
-        case KAGG_ACTION__NROWS_ANY:
-            atomicAdd((unsigned long long *)s, 1ULL);
-            break;
-        case KAGG_ACTION__NROWS_COND:
-            if (!n0) atomicAdd((unsigned long long *)s, 1ULL);
-            break;
-        case KAGG_ACTION__PMIN_INT32:
-        case KAGG_ACTION__PMIN_INT64:
-            if (!n0) { atomicOr((unsigned int *)(s + 8), 1u); atomicMin((long long *)s, (long long)v0); }
-            break;
-        case KAGG_ACTION__PMAX_INT32:
-        case KAGG_ACTION__PMAX_INT64:
-            if (!n0) { atomicOr((unsigned int *)(s + 8), 1u); atomicMax((long long *)s, (long long)v0); }
-            break;
-        case KAGG_ACTION__PMIN_FP64:
-            if (!n0) {
-                atomicOr((unsigned int *)(s + 8), 1u);
-                atomicMin((long long *)s, (long long)xb_f64_ordered(xb_reg_f64(v0, rk0)));
-            }
-            break;
-        case KAGG_ACTION__PMAX_FP64:
-            if (!n0) {
-                atomicOr((unsigned int *)(s + 8), 1u);
-                atomicMax((long long *)s, (long long)xb_f64_ordered(xb_reg_f64(v0, rk0)));
-            }
-            break;
-        case KAGG_ACTION__PSUM_INT:
-        case KAGG_ACTION__PAVG_INT:
-            if (!n0) {
-                atomicAdd((unsigned long long *)s, 1ULL);
-                atomicAdd((unsigned long long *)(s + 8), (unsigned long long)v0);
-            }
-            break;
-        case KAGG_ACTION__PSUM_INT64:
-        case KAGG_ACTION__PAVG_INT64:
-            if (!n0) {
-                atomicAdd((unsigned long long *)s, 1ULL);
-                xb_atomic_add_i128((uint64_t *)(s + 8), (xb_i128)(int64_t)v0);
-            }
-            break;
-        case KAGG_ACTION__PSUM_FP:
-        case KAGG_ACTION__PAVG_FP:
-            if (!n0) {
-                atomicAdd((unsigned long long *)s, 1ULL);
-                xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), xb_reg_f64(v0, rk0));
-            }
-            break;
-        case KAGG_ACTION__PSUM_NUMERIC:
-        case KAGG_ACTION__PAVG_NUMERIC:
-            if (!n0) {
-                uint8_t kind; int16_t w; xb_i128 v;
-                if (xb_numeric_decode((const uint8_t *)v0, &kind, &w, &v)) {
-                    XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
-                } else if (kind == XB_NUM_VALID) {
-                    atomicAdd((unsigned long long *)s, 1ULL);
-                    xb_atomic_add_i128((uint64_t *)(s + 8), xb_numeric_rescale(a.weight, w, v));
-                } else {
-                    uint32_t special = kind == XB_NUM_PINF ? PAGG_NUMERIC_ATTRS__PINF
-                                     : kind == XB_NUM_NINF ? PAGG_NUMERIC_ATTRS__NINF
-                                     : PAGG_NUMERIC_ATTRS__NAN;
-                    atomicOr((unsigned int *)(s + 24), special);
-                }
-            }
-            break;
-        case KAGG_ACTION__STDDEV:
-            if (!n0) {
-                double x = xb_reg_f64(v0, rk0);
-                atomicAdd((unsigned long long *)s, 1ULL);
-                xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
-                xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
-            }
-            break;
-        case KAGG_ACTION__COVAR: {
-            bool n1 = RISNULL(R, a.arg1) != 0;
-            if (!n0 && !n1) {
-                double x = xb_reg_f64(v0, rk0);
-                double y = xb_reg_f64(RVAL(R, a.arg1), plan->rk[a.arg1]);
-                atomicAdd((unsigned long long *)s, 1ULL);
-                xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
-                xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
-                xb_atomic_add_f64c((double *)(s + 40), (double *)(s + 48), y);
-                xb_atomic_add_f64c((double *)(s + 56), (double *)(s + 64), y * y);
-                xb_atomic_add_f64c((double *)(s + 72), (double *)(s + 80), x * y);
-            }
-            break;
-        }
         default:
             break;
         }
@@ -424,98 +318,452 @@ struct XbExecArgs {
     uint64_t        nunits;         /* total units over all tasks */
     uint32_t        format;         /* common KDS format of the tasks */
     uint32_t        sm_cap;         /* shared-memory group table entries (0: none) */
-    uint32_t        regs_bytes;     /* per-warp register file bytes */
+    uint32_t        warp_bytes;     /* shared memory of one warp: counters, cursors, registers */
     xb_gtable      *gt;
     xb_status      *st;
 };
 
-/* per-warp mutable state, in shared memory */
+/* per-warp counters, in shared memory */
 struct XbWarpState {
     unsigned long long raw, in, out;
     unsigned long long depth[XB_MAX_DEPTH + 1];
-    uint32_t failed;
+};
+
+/* probe cursor of one join depth for the 32 lanes of a warp (shared memory) */
+struct XbCursor {
+    unsigned long long okey[32];    /* outer key (fused probe comparing a key column) */
+    uint32_t pos[32];               /* next index slot to visit */
+    uint32_t tag[32];               /* hash value, or the 32-bit key */
+    uint32_t live;                  /* lanes whose probe chain may hold more rows */
+    uint32_t __pad[3];
+};
+
+/* fixed-offset loader of one depth-0 load */
+struct XbFix {
+    int32_t  off;                   /* attcacheoff of the column */
+    uint8_t  ld;
+    uint8_t  reg;
+    uint16_t __pad;
+};
+
+/* column layout shared by every chunk of a launch, and the fixed-offset
+ * loaders used while a tuple has no NULL bitmap */
+struct XbSrcMeta {
+    XbCol    cols[XB_MAX_COLS];
+    XbFix    fix[XB_MAX_LOADS];
+    int32_t  ncols;
+    uint32_t fixed;                 /* 1: every depth-0 load is fixed-width at a cached offset */
+    uint32_t fixed_end;             /* payload bytes those loads span */
     uint32_t __pad;
 };
 
-/* everything a warp needs, passed by value (registers) */
-struct XbCtx {
-    const xb_plan  *plan;           /* shared-memory copy */
-    XbRegs          R;
-    char           *sm_entries;
-    uint32_t        sm_mask;
-    xb_gtable      *gt;
-    xb_status      *st;
-    XbWarpState    *ws;
-};
+#define XB_WARP_HEAD    ((sizeof(XbWarpState) + 15) & ~(size_t)15)
 
-__device__ __forceinline__ bool xb_failed(const XbCtx &c)
+__device__ __forceinline__ uint32_t xb_ld_acquire_cta(const uint32_t *p)
 {
-    return *(volatile uint32_t *)&c.ws->failed != 0;
-}
-__device__ __forceinline__ void xb_set_failed(const XbCtx &c)
-{
-    c.ws->failed = 1;
+    uint32_t v;
+    asm volatile("ld.acquire.cta.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
-__device__ __noinline__ void xb_groupby(XbCtx c, uint32_t act)
+__device__ __forceinline__ void xb_st_release_cta(uint32_t *p, uint32_t v)
 {
-    const xb_plan *plan = c.plan;
-    const uint32_t lane = xb_lane();
-    /* the translator emits the key-hash program right after the argument
-     * program, so both run as one instruction stream */
-    const uint32_t n = plan->gb_args.count +
-                       (plan->has_groupby == 1 ? plan->gb_keyhash.count : 0);
-    if (n && !xb_vm_run(plan->insns + plan->gb_args.start, n, c.R, act, c.st)) {
-        xb_set_failed(c);
-        return;
+    asm volatile("st.release.cta.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+/* byte width of a fixed-width loader, 0 for varlena */
+__device__ __forceinline__ int xb_ld_width(int ld)
+{
+    switch (ld) {
+    case XB_LD_BOOL: return 1;
+    case XB_LD_INT2: return 2;
+    case XB_LD_INT4: case XB_LD_DATE: case XB_LD_FLT4: return 4;
+    case XB_LD_INT8: case XB_LD_FLT8: return 8;
     }
-    uint32_t hash = 0;
-    if (plan->has_groupby == 1)
-        hash = (uint32_t)RVAL(c.R, plan->gb_keyhash.result);
-    bool bad = false;
-    if ((act >> lane) & 1u) {
-        xb_keyimg keys[XB_MAX_KEYS];
-        for (uint32_t k = 0; k < plan->nkeys; k++)
-            xb_key_from_regs(plan->keys[k], c.R, lane, &keys[k]);
-        char *e = nullptr;
-        bool full = false;
-        if (c.sm_entries)
-            e = xb_group_find(plan, c.sm_entries, c.sm_mask, hash, keys, nullptr, c.st, &full);
-        if (!e) {
-            full = false;
-            e = xb_group_find(plan, c.gt->entries, c.gt->cap_mask, hash, keys, c.gt, c.st, &full);
-            if (!e && full) {
-                XB_RAISE(c.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
-                atomicOr(&c.gt->overflow, 1u);
+    return 0;
+}
+
+/* ---------------------------------------------------------------
+ * group table access from the register file
+ * --------------------------------------------------------------- */
+
+/* do the lane's group keys (registers) equal the entry's key images? */
+__device__ __forceinline__ bool
+xb_key_match(const xb_plan *plan, const char *e, const XbRegs &R, uint32_t lane)
+{
+    const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
+    for (uint32_t k = 0; k < plan->nkeys; k++) {
+        const xb_key &key = plan->keys[k];
+        const xb_keyimg x = img[k];
+        const bool rn = RISNULL(R, key.reg) != 0;
+        if (x.isnull || rn) {
+            if (!(x.isnull && rn))
+                return false;
+            continue;
+        }
+        const uint64_t v = RVAL(R, key.reg);
+        if (x.val == v && (key.rk != XB_RK_TEXT || x.len == RAUX(R, key.reg)))
+            continue;               /* same bits, or the same key bytes */
+        if (key.rk == XB_RK_TEXT) {
+            if (x.len != RAUX(R, key.reg) ||
+                !xb_bytes_eq_ool((const uint8_t *)x.val, (const uint8_t *)v, x.len))
+                return false;
+        } else if (key.rk == XB_RK_NUM) {
+            int err = 0;
+            if (xb_numeric_cmp((const uint8_t *)x.val, (const uint8_t *)v, &err) != 0 || err)
+                return false;
+        } else {
+            return false;
+        }
+    }
+    return true;
+}
+
+/*
+ * Claim an EMPTY entry for the lane's group: 0 = another lane claimed it
+ * first, 1 = claimed and published READY, 2 = claimed but the key bytes
+ * did not fit the arena (error raised).  Rare, so out of line.
+ */
+__device__ __noinline__ int
+xb_group_claim(const xb_plan *plan, char *e, XbRegs R, uint32_t hash,
+               xb_gtable *gt, xb_status *st)
+{
+    const uint32_t lane = xb_lane();
+    xb_gent_head *h = (xb_gent_head *)e;
+    if (atomicCAS(&h->state, XB_GSTATE_EMPTY, XB_GSTATE_BUSY) != XB_GSTATE_EMPTY)
+        return 0;
+    h->hash = hash;
+    xb_keyimg *img = (xb_keyimg *)(e + plan->gent_keys_off);
+    bool ok = true;
+    for (uint32_t k = 0; k < plan->nkeys; k++) {
+        const xb_key &key = plan->keys[k];
+        xb_keyimg src;
+        src.isnull = RISNULL(R, key.reg);
+        src.val = RVAL(R, key.reg);
+        src.len = RAUX(R, key.reg);
+        ok &= xb_key_store(key, src, &img[k], gt, st);
+    }
+    xb_init_states(plan, e);
+    if (gt) {
+        atomicAdd((unsigned long long *)&gt->nused, 1ULL);
+        xb_st_release(&h->state, XB_GSTATE_READY);
+    } else {
+        xb_st_release_cta(&h->state, XB_GSTATE_READY);
+    }
+    return ok ? 1 : 2;
+}
+
+/*
+ * Find or create the lane's group entry: the shared-memory table (SMEM,
+ * gt == nullptr; entries visible to this CTA only) or the global table.
+ * Returns nullptr when the table is full (*full) or on an error.
+ */
+template <bool SMEM>
+__device__ __forceinline__ char *
+xb_group_get(const xb_plan *plan, const XbRegs &R, uint32_t lane, char *entries,
+             uint64_t cap_mask, uint32_t hash, xb_gtable *gt, xb_status *st, bool *full)
+{
+    const uint32_t gsz = plan->gent_size;
+    uint64_t pos = hash & cap_mask;
+    const uint64_t limit = SMEM ? cap_mask : (cap_mask < XB_PROBE_LIMIT ? cap_mask : XB_PROBE_LIMIT);
+    for (uint64_t probe = 0; probe <= limit; probe++) {
+        char *e = entries + pos * gsz;
+        xb_gent_head *h = (xb_gent_head *)e;
+        uint32_t s = SMEM ? xb_ld_acquire_cta(&h->state) : xb_ld_acquire(&h->state);
+        if (s == XB_GSTATE_EMPTY) {
+            const int rc = xb_group_claim(plan, e, R, hash, gt, st);
+            if (rc == 1)
+                return e;
+            if (rc == 2)
+                return nullptr;
+            s = SMEM ? xb_ld_acquire_cta(&h->state) : xb_ld_acquire(&h->state);
+        }
+        uint32_t spins = 0;
+        while (s == XB_GSTATE_BUSY) {
+            if (++spins > XB_WAIT_LIMIT) {
+                XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_WAIT_TIMEOUT);
+                return nullptr;
+            }
+            __nanosleep(20);
+            s = SMEM ? xb_ld_acquire_cta(&h->state) : xb_ld_acquire(&h->state);
+        }
+        if (h->hash == hash && xb_key_match(plan, e, R, lane))
+            return e;
+        pos = (pos + 1) & cap_mask;
+    }
+    *full = true;
+    return nullptr;
+}
+
+/* per-lane update of the actions that are not combined across a warp */
+__device__ __forceinline__ void
+xb_update_one(const xb_agg &a, char *s, const XbRegs &R, uint32_t lane, const uint8_t *rk,
+              xb_status *st)
+{
+    const bool n0 = RISNULL(R, a.arg0) != 0;
+    const uint64_t v0 = RVAL(R, a.arg0);
+    switch (a.action) {
+    case KAGG_ACTION__PSUM_NUMERIC:
+    case KAGG_ACTION__PAVG_NUMERIC:
+        if (!n0) {
+            uint8_t kind; int16_t w; xb_i128 v;
+            if (xb_numeric_decode((const uint8_t *)v0, &kind, &w, &v)) {
+                XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
+            } else if (kind == XB_NUM_VALID) {
+                atomicAdd((unsigned long long *)s, 1ULL);
+                xb_atomic_add_i128((uint64_t *)(s + 8), xb_numeric_rescale(a.weight, w, v));
+            } else {
+                uint32_t special = kind == XB_NUM_PINF ? PAGG_NUMERIC_ATTRS__PINF
+                                 : kind == XB_NUM_NINF ? PAGG_NUMERIC_ATTRS__NINF
+                                 : PAGG_NUMERIC_ATTRS__NAN;
+                atomicOr((unsigned int *)(s + 24), special);
             }
         }
-        if (e)
-            xb_update_states(plan, e, c.R, lane, c.st);
-        else
-            bad = true;
+        break;
+    case KAGG_ACTION__STDDEV:
+        if (!n0) {
+            const double x = xb_reg_f64(v0, rk[a.arg0]);
+            atomicAdd((unsigned long long *)s, 1ULL);
+            xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
+            xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
+        }
+        break;
+    case KAGG_ACTION__COVAR: {
+        const bool n1 = RISNULL(R, a.arg1) != 0;
+        if (!n0 && !n1) {
+            const double x = xb_reg_f64(v0, rk[a.arg0]);
+            const double y = xb_reg_f64(RVAL(R, a.arg1), rk[a.arg1]);
+            atomicAdd((unsigned long long *)s, 1ULL);
+            xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
+            xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
+            xb_atomic_add_f64c((double *)(s + 40), (double *)(s + 48), y);
+            xb_atomic_add_f64c((double *)(s + 56), (double *)(s + 64), y * y);
+            xb_atomic_add_f64c((double *)(s + 72), (double *)(s + 80), x * y);
+        }
+        break;
     }
-    /* keep the failure flag warp-uniform: later full-mask ballots rely on it */
-    if (__any_sync(XB_FULL, bad))
-        xb_set_failed(c);
+    default:
+        break;
+    }
 }
 
-/* load the inner row's pre-decoded registers for lanes in 'cand' */
+/*
+ * __updateOneTupleGroupBy + __update_groupby__* (cuda_gpupreagg.cu:1196-1605)
+ * for a warp: lanes whose rows fall into the same group entry are combined
+ * first (the lowest such lane sums, counts, mins or maxes its peers' values
+ * from the register file) and one atomic per state field is issued per
+ * distinct group.  Numeric sums and the variance families stay per lane.
+ * All lanes call this; e == nullptr for lanes without a row.
+ */
 __device__ __forceinline__ void
-xb_load_inner(const xb_inner *in, XbRegs R, uint32_t lane, uint32_t cand, uint32_t row,
-              const uint8_t *rk)
+xb_update_states_warp(const xb_plan *plan, char *e, const XbRegs &R, uint32_t lane, xb_status *st)
+{
+    const uint32_t peers = __match_any_sync(XB_FULL, (unsigned long long)e);
+    const bool leader = e != nullptr && (uint32_t)(__ffs(peers) - 1) == lane;
+    for (uint32_t i = 0; i < plan->naggs; i++) {
+        const xb_agg &a = plan->aggs[i];
+        if (a.state_sz == 0 || !e)
+            continue;
+        char *s = e + a.state_off;
+        const uint32_t act = a.action;
+        const bool combined = !(act == KAGG_ACTION__PSUM_NUMERIC || act == KAGG_ACTION__PAVG_NUMERIC ||
+                                act == KAGG_ACTION__STDDEV || act == KAGG_ACTION__COVAR);
+        if (!combined) {
+            if (a.filter >= 0 && (RISNULL(R, a.filter) || RVAL(R, a.filter) == 0))
+                continue;
+            xb_update_one(a, s, R, lane, plan->rk, st);
+            continue;
+        }
+        if (!leader)
+            continue;
+        const bool flt = a.arg0 >= 0 && plan->rk[a.arg0] == XB_RK_FLT;
+        const uint32_t nm0 = a.arg0 >= 0 ? R.nullm[a.arg0] : XB_FULL;
+        const uint32_t nmf = a.filter >= 0 ? R.nullm[a.filter] : 0;
+        unsigned long long cnt = 0;
+        xb_i128 isum = 0;
+        double fs = 0.0, fc = 0.0;
+        long long mn = INT64_MAX, mx = INT64_MIN;
+        for (uint32_t m = peers; m; m &= m - 1) {
+            const uint32_t p = __ffs(m) - 1;
+            if (a.filter >= 0 && (((nmf >> p) & 1u) || R.val[a.filter * 32 + p] == 0))
+                continue;
+            if (act == KAGG_ACTION__NROWS_ANY) {
+                cnt++;
+                continue;
+            }
+            if ((nm0 >> p) & 1u)
+                continue;
+            const uint64_t v = R.val[a.arg0 * 32 + p];
+            cnt++;
+            switch (act) {
+            case KAGG_ACTION__PMIN_INT32: case KAGG_ACTION__PMIN_INT64:
+                mn = min(mn, (long long)v);
+                break;
+            case KAGG_ACTION__PMAX_INT32: case KAGG_ACTION__PMAX_INT64:
+                mx = max(mx, (long long)v);
+                break;
+            case KAGG_ACTION__PMIN_FP64:
+                mn = min(mn, (long long)xb_f64_ordered(xb_reg_f64(v, plan->rk[a.arg0])));
+                break;
+            case KAGG_ACTION__PMAX_FP64:
+                mx = max(mx, (long long)xb_f64_ordered(xb_reg_f64(v, plan->rk[a.arg0])));
+                break;
+            case KAGG_ACTION__PSUM_INT: case KAGG_ACTION__PAVG_INT:
+            case KAGG_ACTION__PSUM_INT64: case KAGG_ACTION__PAVG_INT64:
+                isum += (xb_i128)(int64_t)v;
+                break;
+            case KAGG_ACTION__PSUM_FP: case KAGG_ACTION__PAVG_FP: {
+                /* TwoSum: fs + fc carries the peers' sum exactly up to fc's rounding */
+                const double x = flt ? __longlong_as_double(v) : (double)(int64_t)v;
+                const double t = __dadd_rn(fs, x);
+                const double bp = __dsub_rn(t, fs);
+                fc += __dadd_rn(__dsub_rn(fs, __dsub_rn(t, bp)), __dsub_rn(x, bp));
+                fs = t;
+                break;
+            }
+            default:
+                break;
+            }
+        }
+        if (cnt == 0)
+            continue;
+        switch (act) {
+        case KAGG_ACTION__NROWS_ANY:
+        case KAGG_ACTION__NROWS_COND:
+            atomicAdd((unsigned long long *)s, cnt);
+            break;
+        case KAGG_ACTION__PMIN_INT32: case KAGG_ACTION__PMIN_INT64: case KAGG_ACTION__PMIN_FP64:
+            atomicOr((unsigned int *)(s + 8), 1u);
+            atomicMin((long long *)s, mn);
+            break;
+        case KAGG_ACTION__PMAX_INT32: case KAGG_ACTION__PMAX_INT64: case KAGG_ACTION__PMAX_FP64:
+            atomicOr((unsigned int *)(s + 8), 1u);
+            atomicMax((long long *)s, mx);
+            break;
+        case KAGG_ACTION__PSUM_INT: case KAGG_ACTION__PAVG_INT:
+            atomicAdd((unsigned long long *)s, cnt);
+            atomicAdd((unsigned long long *)(s + 8), (unsigned long long)(uint64_t)isum);
+            break;
+        case KAGG_ACTION__PSUM_INT64: case KAGG_ACTION__PAVG_INT64:
+            atomicAdd((unsigned long long *)s, cnt);
+            xb_atomic_add_i128((uint64_t *)(s + 8), isum);
+            break;
+        case KAGG_ACTION__PSUM_FP: case KAGG_ACTION__PAVG_FP:
+            atomicAdd((unsigned long long *)s, cnt);
+            xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), fs);
+            if (fc != 0.0)
+                atomicAdd((double *)(s + 16), fc);
+            break;
+        default:
+            break;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------
+ * hash-join probe cursors
+ * --------------------------------------------------------------- */
+
+/* start depth-d probes for the lanes with 'live' set */
+__device__ __forceinline__ void
+xb_cursor_start(const xb_inner *in, XbCursor *cu, uint32_t lane, bool live,
+                uint32_t hash, uint32_t tag, uint64_t okey)
+{
+    cu->pos[lane] = hash & in->cap_mask;
+    cu->tag[lane] = tag;
+    cu->okey[lane] = okey;
+    cu->live = __ballot_sync(XB_FULL, live && in->nitems > 0);
+}
+
+/* fused probe: hash the outer key register inline (HashValue of one
+ * int-family Var, xpu_basetype.cu datum_hash + pg_hash_merge) */
+__device__ __forceinline__ void
+xb_cursor_start_fused(const xb_inner *in, XbCursor *cu, const XbRegs &R, uint32_t lane, uint32_t mask)
+{
+    const uint32_t ox = in->fast_outer;
+    const uint64_t okey = RVAL(R, ox);
+    bool live = ((mask >> lane) & 1u) && !RISNULL(R, ox);   /* NULL = anything is never true */
+    uint32_t hv;
+    switch (in->fast_hk) {
+    case XB_HK_W1: hv = xb_hash_u32((uint32_t)okey, 1); break;
+    case XB_HK_W2: hv = xb_hash_u32((uint32_t)okey, 2); break;
+    case XB_HK_W4: hv = xb_hash_u32((uint32_t)okey, 4); break;
+    default:       hv = xb_hash_u64(okey); break;
+    }
+    const uint32_t hash = xb_hash_merge(0xffffffffU, hv) ^ 0xffffffffU;
+    uint32_t tag = hash;
+    if (in->key32) {
+        tag = (uint32_t)okey;
+        if ((int64_t)okey != (int64_t)(int32_t)okey)
+            live = false;               /* outside any 32-bit inner key */
+    }
+    xb_cursor_start(in, cu, lane, live, hash, tag, okey);
+}
+
+/* next candidate inner row of every live lane; returns the lanes that got one */
+__device__ __forceinline__ uint32_t
+xb_cursor_next(const xb_inner *in, XbCursor *cu, uint32_t lane, uint32_t *p_row)
+{
+    bool live = (cu->live >> lane) & 1u;
+    bool got = false;
+    uint32_t row = 0;
+    if (live) {
+        const int fast = in->fast_key;
+        const uint64_t *kcol = (fast >= 0 && !in->key32) ? in->vals + (size_t)fast * in->nitems : nullptr;
+        const uint32_t *kn = (kcol && ((in->hasnull >> fast) & 1u))
+                             ? in->nulls + (size_t)fast * ((in->nitems + 31) / 32) : nullptr;
+        const uint32_t cap_mask = in->cap_mask;
+        const uint32_t tag = cu->tag[lane];
+        const uint64_t okey = cu->okey[lane];
+        uint32_t pos = cu->pos[lane];
+        for (uint32_t probe = 0; probe <= cap_mask; probe++) {
+            const uint64_t ent = __ldg((const unsigned long long *)&in->index[pos]);
+            pos = (pos + 1) & cap_mask;
+            if (ent == 0) { live = false; break; }
+            if ((uint32_t)(ent >> 32) != tag)
+                continue;
+            const uint32_t r = (uint32_t)ent - 1;
+            if (in->unique_hash)
+                live = false;           /* no other inner row has this tag */
+            if (kcol) {
+                const bool knull = kn && ((__ldg(&kn[r / 32]) >> (r % 32)) & 1u);
+                if (knull || __ldg((const unsigned long long *)&kcol[r]) != okey) {
+                    if (!live) break;
+                    continue;
+                }
+            }
+            row = r;
+            got = true;
+            break;
+        }
+        cu->pos[lane] = pos;
+    }
+    cu->live = __ballot_sync(XB_FULL, live);
+    *p_row = row;
+    return __ballot_sync(XB_FULL, got);
+}
+
+/* copy the live pre-decoded inner columns of row 'row' into the registers
+ * of the lanes in 'cand' (other lanes read NULL) */
+__device__ __forceinline__ void
+xb_load_inner(const xb_inner *in, const XbRegs &R, const uint8_t *rk, uint32_t lane,
+              uint32_t cand, uint32_t row)
 {
     const bool mine = (cand >> lane) & 1u;
-    const uint32_t words = (in->nitems + 31) / 32;
-    const uint32_t live = in->live, hasnull = in->hasnull;
+    const uint32_t n = in->nitems;
+    const uint32_t words = (n + 31) / 32;
+    const uint32_t live = in->live, hasnull = in->hasnull, hashed = in->hashed;
     for (uint32_t k = 0; k < in->nloads; k++) {
         if (!((live >> k) & 1u))
             continue;
         const uint32_t reg = in->load[k].reg;
         bool isnull = !mine;
         if (mine) {
-            RVAL(R, reg) = __ldg((const unsigned long long *)&in->vals[(size_t)k * in->nitems + row]);
+            RVAL(R, reg) = __ldg((const unsigned long long *)&in->vals[(size_t)k * n + row]);
             if (rk[reg] == XB_RK_TEXT)
-                RAUX(R, reg) = __ldg(&in->auxs[(size_t)k * in->nitems + row]);
+                RAUX(R, reg) = __ldg(&in->auxs[(size_t)k * n + row]);
+            if ((hashed >> k) & 1u)
+                RHC(R, reg) = __ldg(&in->hashes[(size_t)k * n + row]);
             if ((hasnull >> k) & 1u)
                 isnull = (__ldg(&in->nulls[(size_t)k * words + row / 32]) >> (row % 32)) & 1u;
         }
@@ -523,219 +771,106 @@ xb_load_inner(const xb_inner *in, XbRegs R, uint32_t lane, uint32_t cand, uint32
     }
 }
 
-template <int D> __device__ __forceinline__ void xb_join_depth(const XbCtx &c, uint32_t act);
-
-/* depths beyond the second are entered through a call, bounding how much
- * probe state is kept live in one function */
-template <int D>
-__device__ __noinline__ void xb_join_depth_call(XbCtx c, uint32_t act)
+/* lanes of 'mask' where program p's result is TRUE (all of mask if p is empty) */
+__device__ __forceinline__ uint32_t
+xb_prog_pass(const xb_prog &p, const XbRegs &R, uint32_t lane, uint32_t mask)
 {
-    xb_join_depth<D>(c, act);
+    if (!p.count)
+        return mask;
+    const bool ok = ((mask >> lane) & 1u) && !RISNULL(R, p.result) && RVAL(R, p.result) != 0;
+    return __ballot_sync(XB_FULL, ok);
 }
 
-template <int D>
-__device__ __forceinline__ void xb_join_depth(const XbCtx &c, uint32_t act)
+/* ---------------------------------------------------------------
+ * source units and 32-row batches
+ * --------------------------------------------------------------- */
+struct XbSrc {
+    uint64_t unit;                  /* current unit (global index) */
+    uint64_t claim_end;             /* BLOCK: end of the current claim */
+    uint64_t next_claim;            /* BLOCK: first unit of the claim taken ahead */
+    const kern_data_store *kds;
+    const uint8_t *page;            /* BLOCK: current heap page */
+    uint32_t row0;                  /* ARROW / ROW: first row of the unit */
+    uint32_t item;                  /* next item of the unit */
+    uint32_t nitems;                /* items of the unit */
+};
+
+/* chunk owning global unit 'unit' (tasks are sorted by unit_base) */
+__device__ __forceinline__ uint32_t
+xb_find_task(const xb_task *tasks, uint32_t ntasks, uint64_t unit)
 {
-    const xb_plan *plan = c.plan;
-    if constexpr (D > XB_MAX_DEPTH) {
-        (void)plan; (void)act;
-        return;
-    } else {
-        if ((uint32_t)D > plan->nrels) {
-            if (xb_lane() == 0)
-                c.ws->out += __popc(act);
-            if (plan->has_groupby)
-                xb_groupby(c, act);
-            return;
-        }
-        const uint32_t lane = xb_lane();
-        const xb_inner *in = &plan->inner[D];
-        /* probe key: fused (inline hash of the outer key) or by the VM */
-        uint32_t hash;
-        bool live = ((act >> lane) & 1u) && in->nitems > 0;
-        uint64_t okey = 0;
-        const int fast = in->fast_key;
-        if (fast >= 0) {
-            const uint32_t ox = in->fast_outer;
-            okey = RVAL(c.R, ox);
-            if (RISNULL(c.R, ox))
-                live = false;               /* NULL = anything is never true */
-            uint32_t hv;
-            switch (in->fast_hk) {
-            case XB_HK_W1: hv = xb_hash_u32((uint32_t)okey, 1); break;
-            case XB_HK_W2: hv = xb_hash_u32((uint32_t)okey, 2); break;
-            case XB_HK_W4: hv = xb_hash_u32((uint32_t)okey, 4); break;
-            default:       hv = xb_hash_u64(okey); break;
-            }
-            hash = xb_hash_merge(0xffffffffU, hv) ^ 0xffffffffU;
-        } else {
-            const xb_prog &hp = plan->hash_value[D];
-            if (!xb_vm_run(plan->insns + hp.start, hp.count, c.R, act, c.st)) {
-                xb_set_failed(c);
-                return;
-            }
-            hash = (uint32_t)RVAL(c.R, hp.result);
-        }
-        const bool key32 = fast >= 0 && in->key32;
-        uint32_t tag = hash;
-        if (key32) {
-            tag = (uint32_t)okey;
-            if ((int64_t)okey != (int64_t)(int32_t)okey)
-                live = false;               /* outside any 32-bit inner key */
-        }
-        const uint64_t *kcol = (fast >= 0 && !key32) ? in->vals + (size_t)fast * in->nitems : nullptr;
-        const uint32_t *kn = (kcol && ((in->hasnull >> fast) & 1u))
-                             ? in->nulls + (size_t)fast * ((in->nitems + 31) / 32) : nullptr;
-        uint64_t pos = hash & in->cap_mask;
-        for (;;) {
-            uint32_t row = 0;
-            bool got = false;
-            if (live) {
-                for (uint32_t probe = 0; probe <= in->cap_mask; probe++) {
-                    const uint64_t ent = __ldg((const unsigned long long *)&in->index[pos]);
-                    pos = (pos + 1) & in->cap_mask;
-                    if (ent == 0) { live = false; break; }
-                    if ((uint32_t)(ent >> 32) != tag)
-                        continue;
-                    const uint32_t r = (uint32_t)ent - 1;
-                    if (in->unique_hash)
-                        live = false;           /* no other inner row has this hash */
-                    if (kcol) {
-                        const bool knull = kn && ((__ldg(&kn[r / 32]) >> (r % 32)) & 1u);
-                        if (knull || __ldg((const unsigned long long *)&kcol[r]) != okey) {
-                            if (!live) break;
-                            continue;
-                        }
-                    }
-                    row = r;
-                    got = true;
-                    break;
-                }
-            }
-            const uint32_t cand = __ballot_sync(XB_FULL, got);
-            if (cand == 0)
-                break;
-            xb_load_inner(in, c.R, lane, cand, row, plan->rk);
-            uint32_t ok = cand;
-            const xb_prog &jp = plan->join_quals[D];
-            if (jp.count) {
-                if (!xb_vm_run(plan->insns + jp.start, jp.count, c.R, cand, c.st)) {
-                    xb_set_failed(c);
-                    return;
-                }
-                const bool pass = ((cand >> lane) & 1u) && !RISNULL(c.R, jp.result) &&
-                                  RVAL(c.R, jp.result) != 0;
-                ok = __ballot_sync(XB_FULL, pass);
-            }
-            if (lane == 0)
-                c.ws->depth[D] += __popc(ok);
-            if (ok) {
-                if constexpr (D + 1 >= 3)
-                    xb_join_depth_call<D + 1>(c, ok);
-                else
-                    xb_join_depth<D + 1>(c, ok);
-                if (xb_failed(c))
-                    return;
-            }
-        }
+    uint32_t lo = 0, hi = ntasks;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (tasks[mid].unit_base <= unit) lo = mid; else hi = mid;
     }
+    return lo;
 }
 
-/* scan quals + joins + group-by over one batch of 32 decoded rows */
-__device__ __forceinline__ void xb_process_batch(const XbCtx &c, uint32_t loaded)
-{
-    const xb_plan *plan = c.plan;
-    const uint32_t lane = xb_lane();
-    uint32_t pass = loaded;
-    if (plan->scan_quals.count) {
-        if (!xb_vm_run(plan->insns + plan->scan_quals.start, plan->scan_quals.count,
-                       c.R, loaded, c.st)) {
-            xb_set_failed(c);
-            return;
-        }
-        const int r = plan->scan_quals.result;
-        const bool ok = ((loaded >> lane) & 1u) && !RISNULL(c.R, r) && RVAL(c.R, r) != 0;
-        pass = __ballot_sync(XB_FULL, ok);
-    }
-    if (lane == 0)
-        c.ws->in += __popc(pass);
-    if (pass)
-        xb_join_depth<1>(c, pass);
-}
-
-/* write the NULL ballots of the depth-0 load registers */
+/* pull a claim's heap pages into L2 (TMA bulk prefetch) */
 __device__ __forceinline__ void
-xb_publish_load_nulls(const xb_plan *plan, XbRegs R, bool ok, uint32_t nullbits)
+xb_prefetch_claim(const XbExecArgs &args, uint64_t claim, uint32_t lane)
 {
-    for (uint32_t i = 0; i < plan->nload0; i++)
-        xb_set_null(R, plan->load0[i].reg, !ok || ((nullbits >> i) & 1u));
+    if (lane < XB_CLAIM && claim + lane < args.nunits) {
+        const uint64_t u = claim + lane;
+        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
+        const char *p = (const char *)t.kds + t.kds->block_offset + (u - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
+        if ((((uintptr_t)p) & 15) == 0)
+            xb_prefetch_l2(p, PGSTROM_BLCKSZ);
+    }
 }
 
-__device__ __noinline__ void
-xb_scan_heap_page(XbCtx c, const kern_data_store *kds, const XbCol *cols, int kds_ncols,
-                  uint32_t block_id)
+/* move to the next unit; returns 0 = no more work, 1 = ok, 2 = corrupt page */
+__device__ __forceinline__ int
+xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane)
 {
-    const xb_plan *plan = c.plan;
-    const uint32_t lane = xb_lane();
-    const uint8_t *page = (const uint8_t *)kds + kds->block_offset + (size_t)block_id * PGSTROM_BLCKSZ;
-    const uint32_t pd_lower = (uint32_t)xb_fetch_le(page + 12, 2);
-    uint32_t nlp = 0;
-    if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ) {
-        nlp = (pd_lower - SizeOfPageHeaderData) / sizeof(ItemIdData);
-    } else if (pd_lower > PGSTROM_BLCKSZ) {
-        if (lane == 0) XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
-        xb_set_failed(c);
-        return;
-    }
-    for (uint32_t base = 0; base < nlp; base += 32) {
-        const uint32_t idx = base + lane;
-        bool normal = false, ok = false;
-        uint32_t nullbits = 0;
-        if (idx < nlp) {
-            const uint32_t lp = (uint32_t)xb_fetch_le(page + SizeOfPageHeaderData + 4 * idx, 4);
-            if (ITEMID_FLAGS(lp) == LP_NORMAL) {
-                const uint32_t off = ITEMID_OFF(lp), len = ITEMID_LEN(lp);
-                normal = true;
-                if (off >= SizeOfPageHeaderData && len >= SizeofHeapTupleHeader &&
-                    off + len <= PGSTROM_BLCKSZ) {
-                    const uint8_t *htup = page + off;
-                    const uint16_t infomask2 = (uint16_t)xb_fetch_le(htup + 18, 2);
-                    const uint16_t infomask = (uint16_t)xb_fetch_le(htup + 20, 2);
-                    const uint32_t t_hoff = htup[22];
-                    int natts = infomask2 & HEAP_NATTS_MASK;
-                    if (natts > kds_ncols) natts = kds_ncols;
-                    const uint8_t *nullmap = (infomask & HEAP_HASNULL) ? htup + SizeofHeapTupleHeader : nullptr;
-                    if (t_hoff >= SizeofHeapTupleHeader && t_hoff <= len &&
-                        (!nullmap || SizeofHeapTupleHeader + (natts + 7) / 8 <= t_hoff)) {
-                        ok = xb_decode_tuple(cols, natts, nullmap, htup + t_hoff, len - t_hoff,
-                                             plan->load0, plan->nload0,
-                                             c.R.val + lane, c.R.aux + lane, 32, false, &nullbits);
-                    }
-                    if (!ok)
-                        XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
-                }
-            }
+    if (*(volatile uint32_t *)&args.st->errcode != 0)
+        return 0;
+    if (args.format == KDS_FORMAT_BLOCK) {
+        s.unit++;
+        if (s.unit >= s.claim_end) {
+            s.unit = s.next_claim;
+            if (s.unit >= args.nunits)
+                return 0;
+            s.claim_end = min(s.unit + (uint64_t)XB_CLAIM, args.nunits);
+            unsigned long long nx = 0;
+            if (lane == 0)
+                nx = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)XB_CLAIM);
+            s.next_claim = __shfl_sync(XB_FULL, nx, 0);
+            xb_prefetch_claim(args, s.next_claim, lane);
         }
-        const uint32_t nrm = __ballot_sync(XB_FULL, normal);
-        if (lane == 0)
-            c.ws->raw += __popc(nrm);
-        if (__any_sync(XB_FULL, normal && !ok)) {
-            xb_set_failed(c);
-            return;
-        }
-        xb_publish_load_nulls(plan, c.R, ok, nullbits);
-        const uint32_t loaded = __ballot_sync(XB_FULL, ok);
-        if (loaded)
-            xb_process_batch(c, loaded);
-        if (xb_failed(c))
-            return;
+        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, s.unit)];
+        s.kds = t.kds;
+        s.page = (const uint8_t *)t.kds + t.kds->block_offset + (s.unit - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
+        const uint32_t pd_lower = (uint32_t)xb_fetch_le(s.page + 12, 2);
+        s.item = 0;
+        s.nitems = 0;
+        if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ)
+            s.nitems = (pd_lower - SizeOfPageHeaderData) / sizeof(ItemIdData);
+        else if (pd_lower > PGSTROM_BLCKSZ)
+            return 2;
+        return 1;
     }
+    unsigned long long u = 0;
+    if (lane == 0)
+        u = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
+    u = __shfl_sync(XB_FULL, u, 0);
+    if (u >= args.nunits)
+        return 0;
+    const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
+    s.unit = u;
+    s.kds = t.kds;
+    s.row0 = (uint32_t)(u - t.unit_base) * XB_ROWS_UNIT;
+    const uint32_t left = t.kds->nitems > s.row0 ? t.kds->nitems - s.row0 : 0;
+    s.nitems = left < XB_ROWS_UNIT ? left : XB_ROWS_UNIT;
+    s.item = 0;
+    return 1;
 }
 
 /* Arrow column -> register (xpu_*_datum_arrow_read) */
 __device__ __forceinline__ bool
 xb_arrow_load(const kern_data_store *kds, const kern_colmeta *cm, uint32_t row, int ld,
-              uint64_t *val, uint32_t *aux, bool *isnull, xb_status *st)
+              uint64_t *val, uint32_t *aux, bool *isnull)
 {
     if (cm->virtual_offset != 0) {
         if (cm->virtual_offset < 0) { *isnull = true; return true; }
@@ -804,119 +939,148 @@ xb_arrow_load(const kern_data_store *kds, const kern_colmeta *cm, uint32_t row, 
     }
 }
 
-__device__ __noinline__ void
-xb_scan_arrow_unit(XbCtx c, const kern_data_store *kds, uint32_t unit)
+/* decode one heap tuple (HeapTupleHeaderData at htup, lp_len len) */
+__device__ __forceinline__ bool
+xb_decode_heap(const xb_plan *plan, const XbSrcMeta *meta, const XbRegs &R, uint32_t lane,
+               const uint8_t *htup, uint32_t len, uint32_t *nullbits)
 {
-    const xb_plan *plan = c.plan;
-    const uint32_t lane = xb_lane();
-    const uint32_t row0 = unit * XB_ROWS_UNIT;
-    for (uint32_t b = 0; b < XB_ROWS_UNIT; b += 32) {
-        if (row0 + b >= kds->nitems)
-            break;
-        const uint32_t row = row0 + b + lane;
-        const bool exists = row < kds->nitems;
-        bool ok = exists;
-        uint32_t nullbits = 0;
-        if (exists) {
+    const uint16_t infomask2 = (uint16_t)xb_fetch_le(htup + 18, 2);
+    const uint16_t infomask = (uint16_t)xb_fetch_le(htup + 20, 2);
+    const uint32_t t_hoff = htup[22];
+    const int natts_raw = infomask2 & HEAP_NATTS_MASK;
+    if (t_hoff < SizeofHeapTupleHeader || t_hoff > len)
+        return false;
+    if (meta->fixed && !(infomask & HEAP_HASNULL) && natts_raw >= plan->max_resno0 &&
+        len - t_hoff >= meta->fixed_end) {
+        /* attcacheoff fast path: every loaded column sits at a known offset */
+        const uint8_t *payload = htup + t_hoff;
+        for (uint32_t i = 0; i < plan->nload0; i++) {
+            const XbFix f = meta->fix[i];
+            xb_load_datum(f.ld, payload + f.off, &RVAL(R, f.reg), &RAUX(R, f.reg));
+        }
+        *nullbits = 0;
+        return true;
+    }
+    int natts = natts_raw < meta->ncols ? natts_raw : meta->ncols;
+    const uint8_t *nullmap = (infomask & HEAP_HASNULL) ? htup + SizeofHeapTupleHeader : nullptr;
+    if (nullmap && SizeofHeapTupleHeader + (natts + 7) / 8 > t_hoff)
+        return false;
+    return xb_decode_tuple(meta->cols, natts, nullmap, htup + t_hoff, len - t_hoff,
+                           plan->load0, plan->nload0, R.val + lane, R.aux + lane, 32, false, nullbits);
+}
+
+/*
+ * Decode the next batch of up to 32 source rows into the register file.
+ * Returns the lanes holding a row; *done when the warp has no more work,
+ * *failed on corrupt input (error raised).
+ */
+__device__ __forceinline__ uint32_t
+xb_fetch_batch(const XbExecArgs &args, const xb_plan *plan, const XbSrcMeta *meta,
+               const XbRegs &R, XbSrc &s, uint32_t lane, XbWarpState *ws, bool *done, bool *failed)
+{
+    while (s.item >= s.nitems) {
+        const int rc = xb_next_unit(args, s, lane);
+        if (rc == 0) { *done = true; return 0; }
+        if (rc == 2) {
+            if (lane == 0) XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
+            *failed = true;
+            return 0;
+        }
+    }
+    const uint32_t idx = s.item + lane;
+    s.item += 32;
+    bool exists = false, ok = false;
+    uint32_t nullbits = 0;
+    if (idx < s.nitems) {
+        if (args.format == KDS_FORMAT_BLOCK) {
+            const uint32_t lp = (uint32_t)xb_fetch_le(s.page + SizeOfPageHeaderData + 4 * idx, 4);
+            if (ITEMID_FLAGS(lp) == LP_NORMAL) {
+                const uint32_t off = ITEMID_OFF(lp), len = ITEMID_LEN(lp);
+                exists = true;
+                if (off >= SizeOfPageHeaderData && len >= SizeofHeapTupleHeader &&
+                    off + len <= PGSTROM_BLCKSZ)
+                    ok = xb_decode_heap(plan, meta, R, lane, s.page + off, len, &nullbits);
+            }
+        } else if (args.format == KDS_FORMAT_ARROW) {
+            const uint32_t row = s.row0 + idx;
+            exists = true;
+            ok = true;
             for (uint32_t i = 0; i < plan->nload0; i++) {
                 const xb_load &ldd = plan->load0[i];
                 bool isnull = true;
-                if (ldd.resno <= (int)kds->ncols) {
-                    const kern_colmeta *cm = &kds->colmeta[ldd.resno - 1];
-                    if (!xb_arrow_load(kds, cm, row, ldd.ld, &RVAL(c.R, ldd.reg),
-                                       &RAUX(c.R, ldd.reg), &isnull, c.st)) {
+                if (ldd.resno <= (int)s.kds->ncols) {
+                    const kern_colmeta *cm = &s.kds->colmeta[ldd.resno - 1];
+                    if (!xb_arrow_load(s.kds, cm, row, ldd.ld, &RVAL(R, ldd.reg), &RAUX(R, ldd.reg), &isnull)) {
                         ok = false;
-                        XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_ARROW_TYPE);
+                        XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_ARROW_TYPE);
                         break;
                     }
                 }
                 if (isnull) nullbits |= 1u << i;
             }
-        }
-        const uint32_t ex = __ballot_sync(XB_FULL, exists);
-        if (lane == 0)
-            c.ws->raw += __popc(ex);
-        if (__any_sync(XB_FULL, exists && !ok)) {
-            xb_set_failed(c);
-            return;
-        }
-        xb_publish_load_nulls(plan, c.R, ok, nullbits);
-        const uint32_t loaded = __ballot_sync(XB_FULL, ok);
-        if (loaded)
-            xb_process_batch(c, loaded);
-        if (xb_failed(c))
-            return;
-    }
-}
-
-__device__ __noinline__ void
-xb_scan_row_unit(XbCtx c, const kern_data_store *kds, const XbCol *cols, uint32_t unit)
-{
-    const xb_plan *plan = c.plan;
-    const uint32_t lane = xb_lane();
-    const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
-    const uint32_t row0 = unit * XB_ROWS_UNIT;
-    for (uint32_t b = 0; b < XB_ROWS_UNIT; b += 32) {
-        if (row0 + b >= kds->nitems)
-            break;
-        const uint32_t row = row0 + b + lane;
-        bool exists = row < kds->nitems, ok = false;
-        uint32_t nullbits = 0;
-        if (exists) {
-            uint64_t off = rowindex[row];
-            if (off == 0) {
-                exists = false;
-            } else if (off <= kds->length && ((kds->length - off) & 7) == 0) {
-                const uint8_t *t = (const uint8_t *)kds + kds->length - off;
-                const kern_tupitem *ti = (const kern_tupitem *)t;
-                uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
-                int natts = ti->t_infomask2 & HEAP_NATTS_MASK;
-                if (natts > (int)kds->ncols) natts = kds->ncols;
-                bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
-                if (!ti->has_xact_attrs && ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 &&
-                    pay <= ti->t_len && off >= ti->t_len &&
-                    (!hasnull || 15u + (natts + 7) / 8 <= pay))
-                    ok = xb_decode_tuple(cols, natts, hasnull ? ti->t_bits : nullptr,
-                                         t + pay, ti->t_len - pay, plan->load0, plan->nload0,
-                                         c.R.val + lane, c.R.aux + lane, 32, false, &nullbits);
+        } else {
+            const kern_data_store *kds = s.kds;
+            const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
+            const uint64_t off = rowindex[s.row0 + idx];
+            if (off != 0) {
+                exists = true;
+                if (off <= kds->length && ((kds->length - off) & 7) == 0) {
+                    const uint8_t *t = (const uint8_t *)kds + kds->length - off;
+                    const kern_tupitem *ti = (const kern_tupitem *)t;
+                    const uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
+                    int natts = ti->t_infomask2 & HEAP_NATTS_MASK;
+                    if (natts > meta->ncols) natts = meta->ncols;
+                    const bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
+                    if (!ti->has_xact_attrs && ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 &&
+                        pay <= ti->t_len && off >= ti->t_len &&
+                        (!hasnull || 15u + (natts + 7) / 8 <= pay))
+                        ok = xb_decode_tuple(meta->cols, natts, hasnull ? ti->t_bits : nullptr,
+                                             t + pay, ti->t_len - pay, plan->load0, plan->nload0,
+                                             R.val + lane, R.aux + lane, 32, false, &nullbits);
+                }
             }
-            if (exists && !ok)
-                XB_RAISE(c.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
         }
-        const uint32_t ex = __ballot_sync(XB_FULL, exists);
-        if (lane == 0)
-            c.ws->raw += __popc(ex);
-        if (__any_sync(XB_FULL, exists && !ok)) {
-            xb_set_failed(c);
-            return;
-        }
-        xb_publish_load_nulls(plan, c.R, ok, nullbits);
-        const uint32_t loaded = __ballot_sync(XB_FULL, ok);
-        if (loaded)
-            xb_process_batch(c, loaded);
-        if (xb_failed(c))
-            return;
+        if (exists && !ok && args.format != KDS_FORMAT_ARROW)
+            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
     }
-}
-
-/* chunk owning global unit 'unit' (tasks are sorted by unit_base) */
-__device__ __forceinline__ uint32_t
-xb_find_task(const xb_task *tasks, uint32_t ntasks, uint64_t unit)
-{
-    uint32_t lo = 0, hi = ntasks;
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (tasks[mid].unit_base <= unit) lo = mid; else hi = mid;
+    const uint32_t ex = __ballot_sync(XB_FULL, exists);
+    if (lane == 0)
+        ws->raw += __popc(ex);
+    if (__any_sync(XB_FULL, exists && !ok)) {
+        *failed = true;
+        return 0;
     }
-    return lo;
+    for (uint32_t i = 0; i < plan->nload0; i++)
+        xb_set_null(R, plan->load0[i].reg, !ok || ((nullbits >> i) & 1u));
+    return __ballot_sync(XB_FULL, ok);
 }
 
 /*
+ * The executor: one persistent launch per batch of chunks.  Each warp runs
+ * the GpuScan / GpuJoin / GpuPreAgg pipeline of kern_gpujoin_main
+ * (cuda_gpujoin.cu:1050) as a depth state machine over 32-row batches:
+ *
+ *   FETCH   decode the next batch (heap page items, Arrow rows, ROW tuples),
+ *           run the scan quals                               depth 0
+ *   ENTER   start the hash probes of depth d for the passing lanes
+ *           (fused inline hash, or the HashValue program)    depth 1..n
+ *   PROBE   next candidate inner row per lane, load its pre-decoded
+ *           columns, run the join quals, descend on success; when no lane
+ *           has a candidate left, return to depth d-1
+ *   d > n   group-by: arguments + key hash program, group-table find or
+ *           create, warp-combined state updates
+ *
+ * Every program runs through the single interpreter call site of the loop.
+ *
  * Shared memory of a CTA:
- *   [plan copy: header + used code][column cache][group table][warp states]
- *   [per-warp register files]
+ *   [plan copy: header + used code][XbSrcMeta][group table]
+ *   [per warp: XbWarpState, XbCursor[nrels], register file]
  */
-__global__ void __launch_bounds__(XB_BLOCK, 3)
+#define XB_ST_FETCH     0
+#define XB_ST_ENTER     1
+#define XB_ST_PROBE     2
+
+__global__ void __launch_bounds__(XB_BLOCK, XB_MIN_BLOCKS)
 xb_exec_kernel(XbExecArgs args)
 {
     extern __shared__ __align__(16) char smem[];
@@ -924,11 +1088,13 @@ xb_exec_kernel(XbExecArgs args)
     const uint32_t warp = threadIdx.x >> 5;
 
     xb_plan *plan = (xb_plan *)smem;
-    XbCol *cols = (XbCol *)(smem + args.plan_bytes);
-    char *sm_entries = (char *)(cols + XB_MAX_COLS);
+    XbSrcMeta *meta = (XbSrcMeta *)(smem + args.plan_bytes);
+    char *sm_entries = (char *)meta + ((sizeof(XbSrcMeta) + 15) & ~(size_t)15);
     const size_t sm_bytes = (size_t)args.sm_cap * args.plan->gent_size;
-    XbWarpState *wstates = (XbWarpState *)(sm_entries + sm_bytes);
-    char *regs_base = (char *)(wstates + XB_WARPS) + (size_t)warp * args.regs_bytes;
+    char *wbase = sm_entries + sm_bytes + (size_t)warp * args.warp_bytes;
+    XbWarpState *ws = (XbWarpState *)wbase;
+    const uint32_t nrels_arg = args.plan->nrels;
+    XbCursor *cursors = (XbCursor *)(wbase + XB_WARP_HEAD);   /* cursors[d - 1] */
 
     /* stage the plan (and only the VM code it uses) in shared memory */
     {
@@ -939,86 +1105,182 @@ xb_exec_kernel(XbExecArgs args)
     }
     /* all chunks of a launch share one column layout (checked by the host) */
     const kern_data_store *kds0 = args.tasks[0].kds;
-    const int kds_ncols = kds0->ncols < XB_MAX_COLS ? (int)kds0->ncols : XB_MAX_COLS;
-    for (int i = threadIdx.x; i < kds_ncols; i += blockDim.x) {
-        cols[i].attlen = kds0->colmeta[i].attlen;
-        cols[i].attalign = kds0->colmeta[i].attalign > 0 ? kds0->colmeta[i].attalign : 1;
-        cols[i].attcacheoff = kds0->colmeta[i].attcacheoff;
+    const int ncols = kds0->ncols < XB_MAX_COLS ? (int)kds0->ncols : XB_MAX_COLS;
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) {
+        meta->cols[i].attlen = kds0->colmeta[i].attlen;
+        meta->cols[i].attalign = kds0->colmeta[i].attalign > 0 ? kds0->colmeta[i].attalign : 1;
+        meta->cols[i].attcacheoff = kds0->colmeta[i].attcacheoff;
+    }
+    if (threadIdx.x == 0) {
+        const xb_plan *gp = args.plan;
+        uint32_t fixed = (args.format != KDS_FORMAT_ARROW) ? 1u : 0u, end = 0;
+        for (uint32_t i = 0; i < gp->nload0; i++) {
+            const xb_load &l = gp->load0[i];
+            XbFix f;
+            f.off = 0; f.ld = l.ld; f.reg = l.reg; f.__pad = 0;
+            if (l.resno < 1 || l.resno > ncols) {
+                fixed = 0;
+            } else {
+                const kern_colmeta &cm = kds0->colmeta[l.resno - 1];
+                const int w = xb_ld_width(l.ld);
+                if (w == 0 || cm.attlen != w || cm.attcacheoff < 0) {
+                    fixed = 0;
+                } else {
+                    f.off = cm.attcacheoff;
+                    if ((uint32_t)(cm.attcacheoff + w) > end)
+                        end = cm.attcacheoff + w;
+                }
+            }
+            meta->fix[i] = f;
+        }
+        meta->ncols = ncols;
+        meta->fixed = fixed;
+        meta->fixed_end = end;
     }
     for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
         ((uint32_t *)sm_entries)[i] = 0;
-    for (size_t i = threadIdx.x; i < sizeof(XbWarpState) * XB_WARPS / 4; i += blockDim.x)
-        ((uint32_t *)wstates)[i] = 0;
+    for (size_t i = lane; i < XB_WARP_HEAD / 4; i += 32)
+        ((uint32_t *)ws)[i] = 0;
     __syncthreads();
 
-    XbCtx c;
-    c.plan = plan;
-    c.R = xb_regs_setup(regs_base, plan->nregs);
-    c.sm_entries = args.sm_cap ? sm_entries : nullptr;
-    c.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
-    c.gt = args.gt;
-    c.st = args.st;
-    c.ws = &wstates[warp];
+    const XbRegs R = xb_regs_setup(wbase + XB_WARP_HEAD + sizeof(XbCursor) * nrels_arg, plan->nregs);
     for (uint32_t r = lane; r < plan->nregs; r += 32)
-        c.R.nullm[r] = XB_FULL;
+        R.nullm[r] = XB_FULL;
+    if (lane == 0)
+        for (uint32_t d = 0; d < nrels_arg; d++)
+            cursors[d].live = 0;
     __syncwarp();
 
+    char *const sm_tab = args.sm_cap ? sm_entries : nullptr;
+    const uint32_t sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
+    xb_gtable *const gt = args.gt;
+    xb_status *const st = args.st;
+    const uint32_t nrels = plan->nrels;
+
+    XbSrc src;
+    src.unit = 0;
+    src.claim_end = 0;
+    src.next_claim = 0;
+    src.kds = nullptr;
+    src.page = nullptr;
+    src.row0 = 0;
+    src.item = 0;
+    src.nitems = 0;
     if (args.format == KDS_FORMAT_BLOCK) {
-        const uint32_t stride = XB_CLAIM;
-        uint64_t claim = 0;
+        unsigned long long c0 = 0;
         if (lane == 0)
-            claim = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
-        claim = __shfl_sync(XB_FULL, claim, 0);
-        while (claim < args.nunits && !xb_failed(c)) {
-            uint64_t next = 0;
-            if (lane == 0)
-                next = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)stride);
-            next = __shfl_sync(XB_FULL, next, 0);
-            /* pull the next claim's pages into L2 (TMA bulk prefetch) while
-             * these are decoded */
-            if (lane < stride && next + lane < args.nunits) {
-                const uint64_t u = next + lane;
-                const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
-                const char *p = (const char *)t.kds + t.kds->block_offset +
-                                (u - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
-                if ((((uintptr_t)p) & 15) == 0)
-                    xb_prefetch_l2(p, PGSTROM_BLCKSZ);
-            }
-            for (uint32_t k = 0; k < stride && claim + k < args.nunits && !xb_failed(c); k++) {
-                const uint64_t u = claim + k;
-                const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
-                xb_scan_heap_page(c, t.kds, cols, kds_ncols, (uint32_t)(u - t.unit_base));
-            }
-            if (*(volatile uint32_t *)&args.st->errcode != 0)
+            c0 = atomicAdd((unsigned long long *)&st->unit_cursor, (unsigned long long)XB_CLAIM);
+        src.next_claim = __shfl_sync(XB_FULL, c0, 0);
+        xb_prefetch_claim(args, src.next_claim, lane);
+    }
+
+    uint32_t stage = XB_ST_FETCH, d = 0, mask = 0;
+    for (;;) {
+        const xb_prog *prog;
+        if (stage == XB_ST_FETCH) {
+            bool done = false, failed = false;
+            mask = xb_fetch_batch(args, plan, meta, R, src, lane, ws, &done, &failed);
+            if (done || failed)
                 break;
-            claim = next;
+            if (!mask)
+                continue;
+            prog = &plan->scan_quals;
+        } else if (stage == XB_ST_ENTER) {
+            if (d > nrels) {
+                if (lane == 0)
+                    ws->out += __popc(mask);
+                if (!plan->has_groupby) {
+                    d = nrels;
+                    stage = nrels ? XB_ST_PROBE : XB_ST_FETCH;
+                    continue;
+                }
+                prog = &plan->gb_all;
+            } else {
+                const xb_inner *in = &plan->inner[d];
+                if (in->fast_key >= 0) {
+                    xb_cursor_start_fused(in, &cursors[d - 1], R, lane, mask);
+                    stage = XB_ST_PROBE;
+                    continue;
+                }
+                prog = &plan->hash_value[d];
+            }
+        } else {
+            uint32_t row;
+            const xb_inner *in = &plan->inner[d];
+            const uint32_t cand = xb_cursor_next(in, &cursors[d - 1], lane, &row);
+            if (!cand) {
+                d--;
+                stage = d ? XB_ST_PROBE : XB_ST_FETCH;
+                continue;
+            }
+            xb_load_inner(in, R, plan->rk, lane, cand, row);
+            mask = cand;
+            prog = &plan->join_quals[d];
         }
-    } else {
-        for (;;) {
-            uint64_t unit = 0;
+
+        /* the interpreter call site */
+        if (prog->count && !xb_vm_exec(plan->insns + prog->start, prog->count, R, mask, st))
+            break;
+
+        if (stage == XB_ST_FETCH) {
+            const uint32_t pass = xb_prog_pass(*prog, R, lane, mask);
             if (lane == 0)
-                unit = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
-            unit = __shfl_sync(XB_FULL, unit, 0);
-            if (unit >= args.nunits || xb_failed(c))
-                break;
-            const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, unit)];
-            if (args.format == KDS_FORMAT_ARROW)
-                xb_scan_arrow_unit(c, t.kds, (uint32_t)(unit - t.unit_base));
-            else
-                xb_scan_row_unit(c, t.kds, cols, (uint32_t)(unit - t.unit_base));
-            if (*(volatile uint32_t *)&args.st->errcode != 0)
-                break;
+                ws->in += __popc(pass);
+            if (pass) {
+                d = 1;
+                mask = pass;
+                stage = XB_ST_ENTER;
+            }
+        } else if (stage == XB_ST_ENTER) {
+            if (d > nrels) {
+                /* group-by: find or create each lane's group, then update */
+                const uint32_t hash = plan->has_groupby == 1 ? (uint32_t)RVAL(R, plan->gb_keyhash.result) : 0;
+                char *e = nullptr;
+                bool bad = false;
+                if ((mask >> lane) & 1u) {
+                    bool full = false;
+                    if (sm_tab)
+                        e = xb_group_get<true>(plan, R, lane, sm_tab, sm_mask, hash, nullptr, st, &full);
+                    if (!e) {
+                        full = false;
+                        e = xb_group_get<false>(plan, R, lane, gt->entries, gt->cap_mask, hash, gt, st, &full);
+                        if (!e && full) {
+                            XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+                            atomicOr(&gt->overflow, 1u);
+                        }
+                    }
+                    bad = (e == nullptr);
+                }
+                if (__any_sync(XB_FULL, bad))
+                    break;
+                xb_update_states_warp(plan, e, R, lane, st);
+                d = nrels;
+                stage = nrels ? XB_ST_PROBE : XB_ST_FETCH;
+            } else {
+                const xb_inner *in = &plan->inner[d];
+                const uint32_t hash = (uint32_t)RVAL(R, prog->result);
+                xb_cursor_start(in, &cursors[d - 1], lane, (mask >> lane) & 1u, hash, hash, 0);
+                stage = XB_ST_PROBE;
+            }
+        } else {
+            const uint32_t ok = xb_prog_pass(*prog, R, lane, mask);
+            if (lane == 0)
+                ws->depth[d] += __popc(ok);
+            if (ok) {
+                d++;
+                mask = ok;
+                stage = XB_ST_ENTER;
+            }
         }
     }
 
     /* per-warp statistics */
     if (lane == 0) {
-        const XbWarpState *w = c.ws;
-        atomicAdd((unsigned long long *)&args.st->nitems_raw, w->raw);
-        atomicAdd((unsigned long long *)&args.st->nitems_in, w->in);
-        atomicAdd((unsigned long long *)&args.st->nitems_out, w->out);
-        for (uint32_t d = 1; d <= plan->nrels && d <= XB_MAX_DEPTH; d++)
-            atomicAdd((unsigned long long *)&args.st->nitems_depth[d], w->depth[d]);
+        atomicAdd((unsigned long long *)&st->nitems_raw, ws->raw);
+        atomicAdd((unsigned long long *)&st->nitems_in, ws->in);
+        atomicAdd((unsigned long long *)&st->nitems_out, ws->out);
+        for (uint32_t dd = 1; dd <= nrels && dd <= XB_MAX_DEPTH; dd++)
+            atomicAdd((unsigned long long *)&st->nitems_depth[dd], ws->depth[dd]);
     }
     __syncthreads();
 
@@ -1031,13 +1293,12 @@ xb_exec_kernel(XbExecArgs args)
                 continue;
             const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
             bool full = false;
-            char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, h->hash,
-                                    img, args.gt, args.st, &full);
+            char *g = xb_group_find(plan, gt->entries, gt->cap_mask, h->hash, img, gt, st, &full);
             if (g)
                 xb_merge_states(plan, g, e);
             else if (full) {
-                XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
-                atomicOr(&args.gt->overflow, 1u);
+                XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+                atomicOr(&gt->overflow, 1u);
             }
         }
     }
@@ -1098,6 +1359,17 @@ xb_build_inner(XbBuildArgs args)
             }
             atomicOr(&in->hasnull, nullbits);
         }
+        /* datum hashes of the columns whose hash later stages read */
+        for (uint32_t k = 0; in->hashed && k < in->nloads; k++) {
+            if (!((in->hashed >> k) & 1u) || ((nullbits >> k) & 1u))
+                continue;
+            bool bad = false;
+            const uint32_t hk = in->load[k].ld == XB_LD_NUMERIC ? XB_HK_NUM : XB_HK_TEXT;
+            in->hashes[(size_t)k * n + row] = xb_hash_reg(hk, in->vals[(size_t)k * n + row],
+                                                          in->auxs[(size_t)k * n + row], true, &bad);
+            if (bad)
+                XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
+        }
         /* index insert at hash & mask (linear probing).  Entries hold
          * (hash << 32 | row + 1), or (key << 32 | row + 1) for a 32-bit
          * fused join key; a NULL fused key can never satisfy the join. */
@@ -1120,6 +1392,43 @@ xb_build_inner(XbBuildArgs args)
             pos = (pos + 1) & in->cap_mask;
         }
     }
+}
+
+/*
+ * Point every non-NULL value of text column k at the first-inserted row
+ * holding the same bytes (a per-column dedupe through a temporary
+ * open-addressing table of row + 1 entries).
+ */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_canon_text(xb_inner *in, uint32_t k, uint32_t *table, uint32_t tmask, xb_status *st)
+{
+    const uint32_t n = in->nitems;
+    const uint32_t words = (n + 31) / 32;
+    uint64_t *vals = in->vals + (size_t)k * n;
+    const uint32_t *auxs = in->auxs + (size_t)k * n;
+    const uint32_t *hashes = in->hashes + (size_t)k * n;
+    const uint32_t *nulls = in->nulls + (size_t)k * words;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n;
+         row += gridDim.x * blockDim.x) {
+        if ((nulls[row / 32] >> (row % 32)) & 1u)
+            continue;
+        const uint32_t h = hashes[row], len = auxs[row];
+        const uint8_t *v = (const uint8_t *)vals[row];
+        uint32_t pos = h & tmask;
+        for (uint32_t probe = 0; probe <= tmask; probe++) {
+            const uint32_t old = atomicCAS(&table[pos], 0u, row + 1);
+            if (old == 0)
+                break;                          /* this row represents its bytes */
+            const uint32_t r = old - 1;         /* a representative: never rewritten */
+            if (hashes[r] == h && auxs[r] == len &&
+                xb_bytes_eq((const uint8_t *)vals[r], v, len)) {
+                vals[row] = vals[r];
+                break;
+            }
+            pos = (pos + 1) & tmask;
+        }
+    }
+    (void)st;
 }
 
 /* ================================================================
@@ -1402,7 +1711,7 @@ struct xpuB200Session {
     xb_task        *d_tasks = nullptr;      /* work queue of single-chunk launches */
     uint32_t        d_tasks_cap = 0;
     uint32_t        sm_cap = 0;
-    uint32_t        regs_bytes = 0;
+    uint32_t        warp_bytes = 0;
     uint32_t        plan_bytes = 0;
     size_t          smem_bytes = 0;
     int             grid = 0;
@@ -1600,6 +1909,9 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             DALLOC((size_t)nl * n * 8, &in->vals);
             DALLOC((size_t)nl * n * 4, &in->auxs);
             DALLOC((size_t)nl * words * 4, &in->nulls);
+            in->hashes = nullptr;
+            if (in->hashed)
+                DALLOC((size_t)nl * n * 4, &in->hashes);
             cudaMemsetAsync(in->index, 0, cap * 8, st);
             cudaMemsetAsync(in->nulls, 0, (size_t)nl * words * 4, st);
         }
@@ -1647,6 +1959,26 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         if (grid > dev->nsm * 8) grid = dev->nsm * 8;
         xb_build_inner<<<grid, XB_BLOCK, 0, st>>>(ba);
     }
+    /* canonical text pointers for hashed text columns: equal strings of one
+     * inner column share one address, so group keys taken from them compare
+     * by pointer */
+    for (uint32_t d = 1; d <= plan->nrels; d++) {
+        const xb_inner *in = &plan->inner[d];
+        for (uint32_t k = 0; k < in->nloads; k++) {
+            if (!((in->hashed >> k) & 1u) || in->load[k].ld != XB_LD_TEXT || in->nitems == 0)
+                continue;
+            const uint64_t tcap = xb_next_pow2((uint64_t)in->nitems * 2 + 64);
+            uint32_t *table = nullptr;
+            if (cudaMallocAsync((void **)&table, tcap * 4, st) != cudaSuccess)
+                FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: no device memory for text canonicalisation");
+            cudaMemsetAsync(table, 0, tcap * 4, st);
+            int grid = (int)((in->nitems + XB_BLOCK - 1) / XB_BLOCK);
+            if (grid > dev->nsm * 8) grid = dev->nsm * 8;
+            xb_canon_text<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d], k, table,
+                                                      (uint32_t)(tcap - 1), s->d_status);
+            cudaFreeAsync(table, st);
+        }
+    }
     if (cudaStreamSynchronize(st) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));
     cudaMemcpy(s->h_status, s->d_status, sizeof(xb_status), cudaMemcpyDeviceToHost);
@@ -1656,11 +1988,11 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     cudaMemcpy(s->h_plan, s->d_plan, sizeof(xb_plan), cudaMemcpyDeviceToHost);
 
     /* launch geometry */
-    s->regs_bytes = (uint32_t)PGSTROM_TYPEALIGN(16, (size_t)plan->nregs * (32 * 8 + 32 * 4 + 4) + 4 * XB_MASK_STACK + 16);
+    s->warp_bytes = (uint32_t)(XB_WARP_HEAD + sizeof(XbCursor) * plan->nrels + XB_REGS_BYTES(plan->nregs));
     s->plan_bytes = (uint32_t)PGSTROM_TYPEALIGN(16, offsetof(xb_plan, insns) +
                                                  sizeof(xb_insn) * (size_t)plan->ninsns);
-    s->smem_bytes = s->plan_bytes + sizeof(XbCol) * XB_MAX_COLS + (size_t)s->sm_cap * plan->gent_size +
-                    sizeof(XbWarpState) * XB_WARPS + (size_t)XB_WARPS * s->regs_bytes;
+    s->smem_bytes = s->plan_bytes + PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) +
+                    (size_t)s->sm_cap * plan->gent_size + (size_t)XB_WARPS * s->warp_bytes;
     if (cudaFuncSetAttribute(xb_exec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)s->smem_bytes) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "dynamic shared memory of %zu bytes not available", s->smem_bytes);
@@ -1702,7 +2034,7 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     a.nunits = nunits;
     a.format = format;
     a.sm_cap = s->sm_cap;
-    a.regs_bytes = s->regs_bytes;
+    a.warp_bytes = s->warp_bytes;
     a.gt = s->d_gt;
     a.st = s->d_status;
     int grid = s->grid;

@@ -111,6 +111,8 @@
 #define XB_HK_W8    8
 #define XB_HK_TEXT  20
 #define XB_HK_NUM   21
+#define XB_HK_CACHED 22     /* hash precomputed by the inner build (text/numeric
+                             * column of a join's inner relation) */
 
 typedef struct xb_insn {
     uint8_t     op;
@@ -154,6 +156,8 @@ typedef struct xb_inner {
     uint8_t     fast_hk;        /* hash kind of the outer key */
     uint32_t    key32;          /* index entries hold (key32 << 32 | row + 1):
                                  * the fused key is int2 / int4 / date */
+    uint32_t    hashed;         /* bit k: hash of load k precomputed into hashes[] */
+    uint32_t   *hashes;         /* [nloads][nitems] datum hashes (hashed loads) */
     xb_load     load[XB_MAX_LOADS];
 } xb_inner;
 
@@ -207,6 +211,7 @@ typedef struct xb_plan {
     uint32_t    has_groupby;    /* 1: GROUP BY keys, 2: no-group aggregation */
     xb_prog     gb_args;        /* SaveExpr argument evaluation */
     xb_prog     gb_keyhash;
+    xb_prog     gb_all;         /* gb_args followed by gb_keyhash, as one program */
     uint32_t    nkeys;
     xb_key      keys[XB_MAX_KEYS];
     uint32_t    naggs;
