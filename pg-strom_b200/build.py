@@ -21,7 +21,7 @@ SOURCES = {
     "xb_exec.o": ("xb_exec.cu", "cuda"),
     "xb_compile.o": ("xb_compile.cpp", "cxx"),
 }
-HEADERS = ["xb_plan.h", "xb_device.cuh", "xb_hash.h", "xb_compile.h"]
+HEADERS = ["xb_plan.h", "xb_device.cuh", "xb_ops.cuh", "xb_hash.h", "xb_compile.h"]
 
 
 def _mtime(p):

@@ -12,6 +12,7 @@
 #include <stdint.h>
 #include "xb_plan.h"
 #include "xb_hash.h"
+#include "xb_ops.cuh"
 
 #define XB_FULL         0xffffffffU
 #define XB_WAIT_LIMIT   (1u << 22)      /* bounded spin on a BUSY group entry */
@@ -61,104 +62,6 @@ __device__ __forceinline__ void xb_set_null(const XbRegs &R, int r, bool isnull)
     R.nullm[r] = m;
 }
 
-/* rare, register-hungry datum operations kept out of line so that the
- * interpreter loop stays small */
-__device__ __noinline__ uint32_t xb_hash_text_ool(const uint8_t *p, uint32_t len)
-{
-    return xb_hash_bytes(p, len);
-}
-
-/* returns the hash, or sets *bad on a corrupt numeric */
-__device__ __noinline__ uint32_t xb_hash_numeric_ool(const uint8_t *vl, bool *bad)
-{
-    uint8_t k; int16_t w; xb_i128 v;
-    if (xb_numeric_decode(vl, &k, &w, &v)) {
-        *bad = true;
-        return 0;
-    }
-    return xb_hash_numeric(k, w, v);
-}
-
-/* hash of a register value of the given hash kind (xpu_*_datum_hash) */
-__device__ __forceinline__ uint32_t
-xb_hash_reg(uint32_t hk, uint64_t x, uint32_t aux, bool act, bool *bad)
-{
-    switch (hk) {
-    case XB_HK_W1: return xb_hash_u32((uint32_t)x, 1);
-    case XB_HK_W2: return xb_hash_u32((uint32_t)x, 2);
-    case XB_HK_W4: return xb_hash_u32((uint32_t)x, 4);
-    case XB_HK_W8: return xb_hash_u64(x);
-    case XB_HK_TEXT:
-        return act ? xb_hash_text_ool((const uint8_t *)x, aux) : 0;
-    case XB_HK_NUM:
-        return act ? xb_hash_numeric_ool((const uint8_t *)x, bad) : 0;
-    }
-    return 0;
-}
-
-/* ---------------------------------------------------------------
- * error reporting (first error wins, as STROM_WRITEBACK_ERROR_STATUS)
- * --------------------------------------------------------------- */
-__device__ __forceinline__ void xb_raise(xb_status *st, uint32_t code, uint32_t msg, int line)
-{
-    if (atomicCAS(&st->errcode, 0u, code) == 0u) {
-        st->msg_id = msg;
-        st->lineno = line;
-    }
-}
-#define XB_RAISE(st, code, msg) xb_raise((st), (code), (msg), __LINE__)
-
-/* ---------------------------------------------------------------
- * text helpers
- * --------------------------------------------------------------- */
-__device__ __noinline__ bool xb_bytes_eq_ool(const uint8_t *a, const uint8_t *b, uint32_t n);
-
-/* byte-string equality; within a 16-byte block the loads are independent
- * (no early exit), so they are issued back to back instead of as a chain */
-__device__ __forceinline__ bool xb_bytes_eq(const uint8_t *a, const uint8_t *b, uint32_t n)
-{
-    if (a == b)
-        return true;
-    uint32_t i = 0;
-    for (; i + 16 <= n; i += 16) {
-        uint32_t diff = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < 16; k++)
-            diff |= (uint32_t)(a[i + k] ^ b[i + k]);
-        if (diff)
-            return false;
-    }
-    uint32_t diff = 0;
-#pragma unroll
-    for (uint32_t k = 0; k < 15; k++)
-        if (i + k < n)
-            diff |= (uint32_t)(a[i + k] ^ b[i + k]);
-    return diff == 0;
-}
-
-__device__ __noinline__ bool xb_bytes_eq_ool(const uint8_t *a, const uint8_t *b, uint32_t n)
-{
-    return xb_bytes_eq(a, b, n);
-}
-
-__device__ __noinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, int *err)
-{
-    uint8_t ka, kb; int16_t wa, wb; xb_i128 va, vb;
-    if (xb_numeric_decode(a, &ka, &wa, &va) || xb_numeric_decode(b, &kb, &wb, &vb)) {
-        *err = 1;
-        return 0;
-    }
-    /* NaN sorts above +Inf, which sorts above every finite value */
-    auto rank = [](uint8_t k) { return k == XB_NUM_NAN ? 3 : k == XB_NUM_PINF ? 2 : k == XB_NUM_NINF ? 0 : 1; };
-    int ra = rank(ka), rb = rank(kb);
-    if (ra != rb) return ra < rb ? -1 : 1;
-    if (ra != 1) return 0;
-    int w = wa > wb ? wa : wb;
-    va = xb_numeric_rescale(w, wa, va);
-    vb = xb_numeric_rescale(w, wb, vb);
-    return va < vb ? -1 : (va > vb ? 1 : 0);
-}
-
 /* ---------------------------------------------------------------
  * the register VM
  *
@@ -201,23 +104,10 @@ xb_vm_exec(const xb_insn *__restrict__ code, uint32_t count, const XbRegs &R,
             bool res = false;
             if (!isnull) {
                 const uint64_t x = RVAL(R, in.a);
-                int c;
-                if (in.kind == XB_RK_INT) {
-                    const int64_t a = (int64_t)x, b = in.imm;
-                    c = a < b ? -1 : (a > b ? 1 : 0);
-                } else {
-                    const double a = __longlong_as_double(x), b = __longlong_as_double(in.imm);
-                    const bool na = (a != a), nb = (b != b);
-                    c = na ? (nb ? 0 : 1) : (nb ? -1 : (a < b ? -1 : (a > b ? 1 : 0)));
-                }
-                switch (in.sub) {
-                case XB_CMP_EQ: res = (c == 0); break;
-                case XB_CMP_NE: res = (c != 0); break;
-                case XB_CMP_LT: res = (c < 0); break;
-                case XB_CMP_LE: res = (c <= 0); break;
-                case XB_CMP_GT: res = (c > 0); break;
-                default:        res = (c >= 0); break;
-                }
+                const int c = in.kind == XB_RK_INT
+                    ? xb_cmp3_int((int64_t)x, in.imm)
+                    : xb_cmp3_flt(__longlong_as_double(x), __longlong_as_double(in.imm));
+                res = xb_cmp_sub(in.sub, c);
             }
             RVAL(R, in.dst) = res ? 1 : 0;
             xb_set_null(R, in.dst, isnull);
@@ -237,181 +127,67 @@ xb_vm_exec(const xb_insn *__restrict__ code, uint32_t count, const XbRegs &R,
             break;
         }
         case XB_OP_CMP: {
-            bool isnull = RISNULL(R, in.a) || RISNULL(R, in.b);
+            const bool isnull = RISNULL(R, in.a) || RISNULL(R, in.b);
             bool res = false;
             if (!isnull) {
-                uint64_t x = RVAL(R, in.a), y = RVAL(R, in.b);
-                int c = 0;
-                if (in.kind == XB_RK_INT) {
-                    int64_t a = (int64_t)x, b = (int64_t)y;
-                    c = a < b ? -1 : (a > b ? 1 : 0);
-                } else if (in.kind == XB_RK_FLT) {
-                    double a = __longlong_as_double(x), b = __longlong_as_double(y);
-                    bool na = (a != a), nb = (b != b);
-                    c = na ? (nb ? 0 : 1) : (nb ? -1 : (a < b ? -1 : (a > b ? 1 : 0)));
-                } else if (in.kind == XB_RK_TEXT) {
-                    uint32_t la = RAUX(R, in.a), lb = RAUX(R, in.b);
-                    if (act)
-                        c = (la == lb && xb_bytes_eq_ool((const uint8_t *)x, (const uint8_t *)y, la)) ? 0 : 1;
-                } else if (in.kind == XB_RK_NUM) {
-                    if (act) {
-                        int err = 0;
-                        c = xb_numeric_cmp((const uint8_t *)x, (const uint8_t *)y, &err);
-                        if (err) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT); failed = true; }
-                    }
-                }
-                switch (in.sub) {
-                case XB_CMP_EQ: res = (c == 0); break;
-                case XB_CMP_NE: res = (c != 0); break;
-                case XB_CMP_LT: res = (c < 0); break;
-                case XB_CMP_LE: res = (c <= 0); break;
-                case XB_CMP_GT: res = (c > 0); break;
-                default:        res = (c >= 0); break;
-                }
+                const int c = xb_cmp3(in.kind, RVAL(R, in.a), RAUX(R, in.a), RVAL(R, in.b), RAUX(R, in.b),
+                                      act, st, &failed);
+                res = xb_cmp_sub(in.sub, c);
             }
             RVAL(R, in.dst) = res ? 1 : 0;
             xb_set_null(R, in.dst, isnull);
             break;
         }
         case XB_OP_ARITH: {
-            bool isnull = RISNULL(R, in.a) || RISNULL(R, in.b);
+            const bool isnull = RISNULL(R, in.a) || RISNULL(R, in.b);
             uint64_t out = 0;
-            if (!isnull) {
-                uint64_t x = RVAL(R, in.a), y = RVAL(R, in.b);
-                int opr = in.sub & 0x0f;
-                if (in.kind == XB_RK_INT) {
-                    /* operands are int2/int4/int8 values sign-extended to 64 bits;
-                     * the result must fit the result type (xpu_basetype.cu:525-720) */
-                    const int w = in.sub & 0xf0;
-                    const int64_t a = (int64_t)x, b = (int64_t)y;
-                    int64_t r = 0;
-                    bool bad = false;
-                    if (opr == XB_AR_ADD) {
-                        r = (int64_t)((uint64_t)a + (uint64_t)b);
-                        bad = ((a ^ r) & (b ^ r)) < 0;
-                    } else if (opr == XB_AR_SUB) {
-                        r = (int64_t)((uint64_t)a - (uint64_t)b);
-                        bad = ((a ^ b) & (a ^ r)) < 0;
-                    } else if (opr == XB_AR_MUL) {
-                        r = (int64_t)((uint64_t)a * (uint64_t)b);
-                        const int64_t hi = __mul64hi(a, b);
-                        bad = hi != (r >> 63);
-                    } else if (b == 0) {
-                        if (act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_DIV_ZERO); failed = true; }
-                    } else if (b == -1) {
-                        bad = (a == INT64_MIN);
-                        r = (int64_t)(0 - (uint64_t)a);
-                    } else {
-                        r = a / b;
-                    }
-                    if (w == XB_AR_W2) bad |= (r < -32768 || r > 32767);
-                    else if (w == XB_AR_W4) bad |= (r < INT32_MIN || r > INT32_MAX);
-                    if (bad && act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_INT_RANGE); failed = true; }
-                    out = (uint64_t)r;
-                } else {
-                    double a = __longlong_as_double(x), b = __longlong_as_double(y), r;
-                    if (opr == XB_AR_ADD) r = a + b;
-                    else if (opr == XB_AR_SUB) r = a - b;
-                    else if (opr == XB_AR_MUL) r = a * b;
-                    else {
-                        if (b == 0.0) {
-                            if (act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_DIV_ZERO); failed = true; }
-                            r = 0.0;
-                        } else {
-                            r = a / b;
-                            if (r == 0.0 && a != 0.0 && act) {
-                                XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_FLT_RANGE); failed = true;
-                            }
-                        }
-                    }
-                    if (isinf(r) && !isinf(a) && !isinf(b) && act) {
-                        XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_FLT_RANGE); failed = true;
-                    }
-                    out = (uint64_t)__double_as_longlong(r);
-                }
-            }
+            if (!isnull)
+                out = in.kind == XB_RK_INT
+                    ? xb_arith_int(in.sub, RVAL(R, in.a), RVAL(R, in.b), act, st, &failed)
+                    : xb_arith_flt(in.sub, RVAL(R, in.a), RVAL(R, in.b), act, st, &failed);
             RVAL(R, in.dst) = out;
             xb_set_null(R, in.dst, isnull);
             break;
         }
         case XB_OP_CAST: {
-            bool isnull = RISNULL(R, in.a);
-            uint64_t x = RVAL(R, in.a), out = 0;
-            if (!isnull) {
-                int64_t v = (int64_t)x;
-                int64_t lo = INT64_MIN, hi = INT64_MAX;
-                bool from_flt = (in.sub == XB_CAST_F82I2 || in.sub == XB_CAST_F82I4 || in.sub == XB_CAST_F82I8);
-                if (in.sub == XB_CAST_I2I2 || in.sub == XB_CAST_F82I2) { lo = -32768; hi = 32767; }
-                if (in.sub == XB_CAST_I2I4 || in.sub == XB_CAST_F82I4) { lo = INT32_MIN; hi = INT32_MAX; }
-                if (in.sub == XB_CAST_I2F8) {
-                    out = (uint64_t)__double_as_longlong((double)v);
-                } else if (in.sub == XB_CAST_I2BOOL) {
-                    out = (v != 0) ? 1 : 0;
-                } else if (from_flt) {
-                    double d = rint(__longlong_as_double(x));
-                    bool ok = (d == d) && d >= (double)lo && d < -(double)lo;
-                    if (!ok && act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_INT_RANGE); failed = true; }
-                    out = ok ? (uint64_t)(int64_t)d : 0;
-                } else {
-                    if ((v < lo || v > hi) && act) { XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_INT_RANGE); failed = true; }
-                    out = (uint64_t)v;
-                }
-            }
+            const bool isnull = RISNULL(R, in.a);
+            uint64_t out = 0;
+            if (!isnull)
+                out = xb_cast_op(in.sub, RVAL(R, in.a), act, st, &failed);
             RVAL(R, in.dst) = out;
             xb_set_null(R, in.dst, isnull);
             break;
         }
         case XB_OP_NOT: {
-            bool isnull = RISNULL(R, in.a);
+            const bool isnull = RISNULL(R, in.a);
             RVAL(R, in.dst) = RVAL(R, in.a) ? 0 : 1;
             xb_set_null(R, in.dst, isnull);
             break;
         }
         case XB_OP_NULLTEST: {
-            bool isnull = RISNULL(R, in.a);
+            const bool isnull = RISNULL(R, in.a);
             RVAL(R, in.dst) = (in.sub == 0) ? (isnull ? 1 : 0) : (isnull ? 0 : 1);
             xb_set_null(R, in.dst, false);
             break;
         }
-        case XB_OP_BOOLTEST: {
-            bool isnull = RISNULL(R, in.a);
-            bool v = RVAL(R, in.a) != 0;
-            bool res;
-            switch (in.sub) {
-            case 0: res = !isnull && v; break;          /* IS TRUE */
-            case 1: res = isnull || !v; break;          /* IS NOT TRUE */
-            case 2: res = !isnull && !v; break;         /* IS FALSE */
-            case 3: res = isnull || v; break;           /* IS NOT FALSE */
-            case 4: res = isnull; break;                /* IS UNKNOWN */
-            default: res = !isnull; break;              /* IS NOT UNKNOWN */
-            }
-            RVAL(R, in.dst) = res ? 1 : 0;
+        case XB_OP_BOOLTEST:
+            RVAL(R, in.dst) = xb_booltest(in.sub, RISNULL(R, in.a), RVAL(R, in.a) != 0) ? 1 : 0;
             xb_set_null(R, in.dst, false);
             break;
-        }
         case XB_OP_BOOL_INIT:
             RVAL(R, in.dst) = (in.sub == 0) ? 1 : 0;
             xb_set_null(R, in.dst, false);
             break;
         case XB_OP_AND_ACC: {
-            /* dst AND a: false dominates, else NULL if any NULL */
-            bool dn = RISNULL(R, in.dst), an = RISNULL(R, in.a);
-            bool dv = RVAL(R, in.dst) != 0, av = RVAL(R, in.a) != 0;
-            bool dfalse = !dn && !dv, afalse = !an && !av;
-            bool rv, rn;
-            if (dfalse || afalse) { rv = false; rn = false; }
-            else { rv = true; rn = dn || an; }
+            bool rn, rv;
+            xb_and3(RISNULL(R, in.dst), RVAL(R, in.dst) != 0, RISNULL(R, in.a), RVAL(R, in.a) != 0, &rn, &rv);
             RVAL(R, in.dst) = rv ? 1 : 0;
             xb_set_null(R, in.dst, rn);
             break;
         }
         case XB_OP_OR_ACC: {
-            bool dn = RISNULL(R, in.dst), an = RISNULL(R, in.a);
-            bool dv = RVAL(R, in.dst) != 0, av = RVAL(R, in.a) != 0;
-            bool dtrue = !dn && dv, atrue = !an && av;
-            bool rv, rn;
-            if (dtrue || atrue) { rv = true; rn = false; }
-            else { rv = false; rn = dn || an; }
+            bool rn, rv;
+            xb_or3(RISNULL(R, in.dst), RVAL(R, in.dst) != 0, RISNULL(R, in.a), RVAL(R, in.a) != 0, &rn, &rv);
             RVAL(R, in.dst) = rv ? 1 : 0;
             xb_set_null(R, in.dst, rn);
             break;
@@ -462,27 +238,11 @@ xb_vm_exec(const xb_insn *__restrict__ code, uint32_t count, const XbRegs &R,
         case XB_OP_HASH_FINI:
             RVAL(R, in.dst) = (uint32_t)RVAL(R, in.dst) ^ 0xffffffffU;
             break;
-        case XB_OP_DISTINCT: {
-            bool an = RISNULL(R, in.a), bn = RISNULL(R, in.b);
-            bool res;
-            if (an || bn) {
-                res = (an != bn);
-            } else {
-                uint64_t x = RVAL(R, in.a), y = RVAL(R, in.b);
-                if (in.kind == XB_RK_TEXT) {
-                    uint32_t la = RAUX(R, in.a), lb = RAUX(R, in.b);
-                    res = !(act && la == lb && xb_bytes_eq((const uint8_t *)x, (const uint8_t *)y, la));
-                } else if (in.kind == XB_RK_FLT) {
-                    double a = __longlong_as_double(x), b = __longlong_as_double(y);
-                    res = !((a != a && b != b) || a == b);
-                } else {
-                    res = (x != y);
-                }
-            }
-            RVAL(R, in.dst) = res ? 1 : 0;
+        case XB_OP_DISTINCT:
+            RVAL(R, in.dst) = xb_distinct(in.kind, RISNULL(R, in.a), RVAL(R, in.a), RAUX(R, in.a),
+                                          RISNULL(R, in.b), RVAL(R, in.b), RAUX(R, in.b), act) ? 1 : 0;
             xb_set_null(R, in.dst, false);
             break;
-        }
         default:
             if (lane == 0) XB_RAISE(st, ERRCODE_DEVICE_FATAL, XB_MSG_NONE);
             failed = true;
