@@ -62,6 +62,7 @@ __device__ __forceinline__ void xb_set_null(const XbRegs &R, int r, bool isnull)
     R.nullm[r] = m;
 }
 
+#ifndef XB_JIT      /* the session-specialised kernels have no interpreter */
 /* ---------------------------------------------------------------
  * the register VM
  *
@@ -261,6 +262,8 @@ xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
 {
     return xb_vm_exec(code, count, R, active_in, st);
 }
+
+#endif  /* XB_JIT */
 
 /* ---------------------------------------------------------------
  * attribute loaders (heap datum image -> register), per

@@ -33,302 +33,14 @@
 #include <cstdarg>
 #include "xb_plan.h"
 #include "xb_device.cuh"
+#include "xb_exec_dev.cuh"
 #include "xb_compile.h"
+#include "xb_jit.h"
 #include "xpu_b200.h"
-
-#define XB_BLOCK        256
-#define XB_WARPS        (XB_BLOCK / 32)
-#define XB_CLAIM        4           /* heap pages claimed per warp at a time */
-#define XB_ROWS_UNIT    1024        /* rows per unit for ARROW / ROW chunks */
-#define XB_MIN_BLOCKS   2           /* resident CTAs per SM the kernel is built for */
-#define XB_PROBE_LIMIT  4096        /* max probes in the global group table */
-
-/* ================================================================
- * memory-order helpers (generic addresses: shared or global)
- * ================================================================ */
-__device__ __forceinline__ uint32_t xb_ld_acquire(const uint32_t *p)
-{
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void xb_st_release(uint32_t *p, uint32_t v)
-{
-    asm volatile("st.release.gpu.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
-}
-
-/* L2 prefetch of a contiguous range by the TMA engine (sm_90+) */
-__device__ __forceinline__ void xb_prefetch_l2(const void *p, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
-}
-
-/* ================================================================
- * partial-aggregate state arithmetic
- * ================================================================ */
-__device__ __forceinline__ void xb_atomic_add_i128(uint64_t *p, xb_i128 v)
-{
-    uint64_t lo = (uint64_t)v;
-    uint64_t hi = (uint64_t)((unsigned __int128)v >> 64);
-    uint64_t old = atomicAdd((unsigned long long *)&p[0], (unsigned long long)lo);
-    if (old + lo < old)
-        hi += 1;
-    if (hi)
-        atomicAdd((unsigned long long *)&p[1], (unsigned long long)hi);
-}
-
-/* compensated atomic sum: hi accumulates the rounded sum, lo the exact
- * rounding error of each addition (TwoSum on the value atomicAdd saw) */
-__device__ __forceinline__ void xb_atomic_add_f64c(double *hi, double *lo, double x)
-{
-    double old = atomicAdd(hi, x);
-    double s = __dadd_rn(old, x);
-    double bp = __dsub_rn(s, old);
-    double e = __dadd_rn(__dsub_rn(old, __dsub_rn(s, bp)), __dsub_rn(x, bp));
-    if (e != 0.0)
-        atomicAdd(lo, e);
-}
-
-__device__ __forceinline__ double xb_reg_f64(uint64_t v, int rk)
-{
-    return rk == XB_RK_FLT ? __longlong_as_double(v) : (double)(int64_t)v;
-}
-
-__device__ __noinline__ void xb_init_states(const xb_plan *plan, char *e)
-{
-    for (uint32_t i = 0; i < plan->naggs; i++) {
-        const xb_agg &a = plan->aggs[i];
-        if (a.state_sz == 0)
-            continue;
-        uint64_t *s = (uint64_t *)(e + a.state_off);
-        for (uint32_t k = 0; k < a.state_sz / 8; k++)
-            s[k] = 0;
-        switch (a.action) {
-        case KAGG_ACTION__PMIN_INT32:
-        case KAGG_ACTION__PMIN_INT64:
-        case KAGG_ACTION__PMIN_FP64:
-            s[0] = (uint64_t)INT64_MAX;
-            break;
-        case KAGG_ACTION__PMAX_INT32:
-        case KAGG_ACTION__PMAX_INT64:
-        case KAGG_ACTION__PMAX_FP64:
-            s[0] = (uint64_t)INT64_MIN;
-            break;
-        default:
-            break;
-        }
-    }
-}
-
-/* merge a shared-memory group entry's states into a global entry */
-__device__ __noinline__ void xb_merge_states(const xb_plan *plan, char *dst, const char *src)
-{
-    for (uint32_t i = 0; i < plan->naggs; i++) {
-        const xb_agg &a = plan->aggs[i];
-        if (a.state_sz == 0)
-            continue;
-        char *d = dst + a.state_off;
-        const char *s = src + a.state_off;
-        const uint64_t *su = (const uint64_t *)s;
-        switch (a.action) {
-        case KAGG_ACTION__NROWS_ANY:
-        case KAGG_ACTION__NROWS_COND:
-            if (su[0]) atomicAdd((unsigned long long *)d, su[0]);
-            break;
-        case KAGG_ACTION__PMIN_INT32:
-        case KAGG_ACTION__PMIN_INT64:
-        case KAGG_ACTION__PMIN_FP64:
-            if (*(const uint32_t *)(s + 8)) {
-                atomicOr((unsigned int *)(d + 8), 1u);
-                atomicMin((long long *)d, (long long)su[0]);
-            }
-            break;
-        case KAGG_ACTION__PMAX_INT32:
-        case KAGG_ACTION__PMAX_INT64:
-        case KAGG_ACTION__PMAX_FP64:
-            if (*(const uint32_t *)(s + 8)) {
-                atomicOr((unsigned int *)(d + 8), 1u);
-                atomicMax((long long *)d, (long long)su[0]);
-            }
-            break;
-        case KAGG_ACTION__PSUM_INT:
-        case KAGG_ACTION__PAVG_INT:
-            if (su[0]) {
-                atomicAdd((unsigned long long *)d, su[0]);
-                atomicAdd((unsigned long long *)(d + 8), su[1]);
-            }
-            break;
-        case KAGG_ACTION__PSUM_INT64:
-        case KAGG_ACTION__PAVG_INT64:
-        case KAGG_ACTION__PSUM_NUMERIC:
-        case KAGG_ACTION__PAVG_NUMERIC:
-            if (su[0]) {
-                atomicAdd((unsigned long long *)d, su[0]);
-                xb_atomic_add_i128((uint64_t *)(d + 8),
-                                   (xb_i128)(((unsigned __int128)su[2] << 64) | su[1]));
-            }
-            if (a.state_sz >= 32 && *(const uint32_t *)(s + 24))
-                atomicOr((unsigned int *)(d + 24), *(const uint32_t *)(s + 24));
-            break;
-        case KAGG_ACTION__PSUM_FP:
-        case KAGG_ACTION__PAVG_FP:
-        case KAGG_ACTION__STDDEV:
-        case KAGG_ACTION__COVAR:
-            if (su[0]) {
-                atomicAdd((unsigned long long *)d, su[0]);
-                for (uint32_t k = 8; k + 16 <= a.state_sz; k += 16) {
-                    xb_atomic_add_f64c((double *)(d + k), (double *)(d + k + 8),
-                                       *(const double *)(s + k));
-                    double lo = *(const double *)(s + k + 8);
-                    if (lo != 0.0)
-                        atomicAdd((double *)(d + k + 8), lo);
-                }
-            }
-            break;
-        default:
-            break;
-        }
-    }
-}
-
-/* ================================================================
- * group keys
- * ================================================================ */
-__device__ __forceinline__ uint32_t xb_numeric_varsize(const uint8_t *vl)
-{
-    if (vl[0] & 0x01)
-        return (vl[0] >> 1) & 0x7f;
-    return ((uint32_t)xb_fetch_le(vl, 4) >> 2) & 0x3fffffff;
-}
-
-/* key value of register 'reg' for this lane, as a key image */
-__device__ __forceinline__ void
-xb_key_from_regs(const xb_key &k, const XbRegs &R, uint32_t lane, xb_keyimg *img)
-{
-    img->isnull = RISNULL(R, k.reg);
-    img->val = RVAL(R, k.reg);
-    img->len = RAUX(R, k.reg);
-}
-
-__device__ __forceinline__ bool
-xb_key_equal(const xb_key &k, const xb_keyimg &x, const xb_keyimg &y)
-{
-    if (x.isnull || y.isnull)
-        return x.isnull && y.isnull;        /* NULLs group together */
-    if (k.rk == XB_RK_TEXT)
-        return x.len == y.len &&
-               xb_bytes_eq((const uint8_t *)x.val, (const uint8_t *)y.val, x.len);
-    if (k.rk == XB_RK_NUM) {
-        int err = 0;
-        return xb_numeric_cmp((const uint8_t *)x.val, (const uint8_t *)y.val, &err) == 0 && !err;
-    }
-    return x.val == y.val;
-}
-
-/* copy a key image into an entry; into the arena when 'gt' is given */
-__device__ __forceinline__ bool
-xb_key_store(const xb_key &k, const xb_keyimg &src, xb_keyimg *dst,
-             xb_gtable *gt, xb_status *st)
-{
-    *dst = src;
-    if (src.isnull || !gt)
-        return true;
-    if (k.rk == XB_RK_TEXT || k.rk == XB_RK_NUM) {
-        uint32_t nbytes = (k.rk == XB_RK_TEXT) ? src.len
-                                               : xb_numeric_varsize((const uint8_t *)src.val);
-        unsigned long long off = atomicAdd((unsigned long long *)&gt->arena_used,
-                                           (unsigned long long)((nbytes + 7) & ~7u));
-        if (off + nbytes > gt->arena_sz) {
-            XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_ARENA_FULL);
-            return false;
-        }
-        char *p = gt->arena + off;
-        const char *s = (const char *)src.val;
-        for (uint32_t i = 0; i < nbytes; i++)
-            p[i] = s[i];
-        dst->val = (uint64_t)p;
-    }
-    return true;
-}
-
-/*
- * Find the group whose keys equal 'keys', or create it.  Works on the
- * shared-memory table (gt == nullptr) and on the global table.  An entry
- * is claimed EMPTY->BUSY by CAS, initialised, then published READY with a
- * release store; readers wait (bounded) on BUSY entries.
- * Returns nullptr when the table is full (*full) or on error.
- */
-__device__ __noinline__ char *
-xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t hash,
-              const xb_keyimg *keys, xb_gtable *gt, xb_status *st, bool *full)
-{
-    const uint32_t gsz = plan->gent_size;
-    uint64_t pos = hash & cap_mask;
-    uint64_t limit = gt ? (cap_mask < XB_PROBE_LIMIT ? cap_mask : XB_PROBE_LIMIT) : cap_mask;
-    for (uint64_t probe = 0; probe <= limit; probe++) {
-        char *e = entries + pos * gsz;
-        xb_gent_head *h = (xb_gent_head *)e;
-        uint32_t s = xb_ld_acquire(&h->state);
-        if (s == XB_GSTATE_EMPTY) {
-            if (atomicCAS(&h->state, XB_GSTATE_EMPTY, XB_GSTATE_BUSY) == XB_GSTATE_EMPTY) {
-                h->hash = hash;
-                xb_keyimg *img = (xb_keyimg *)(e + plan->gent_keys_off);
-                bool ok = true;
-                for (uint32_t k = 0; k < plan->nkeys; k++)
-                    ok &= xb_key_store(plan->keys[k], keys[k], &img[k], gt, st);
-                xb_init_states(plan, e);
-                if (gt)
-                    atomicAdd((unsigned long long *)&gt->nused, 1ULL);
-                xb_st_release(&h->state, XB_GSTATE_READY);
-                return ok ? e : nullptr;
-            }
-            s = xb_ld_acquire(&h->state);
-        }
-        uint32_t spins = 0;
-        while (s == XB_GSTATE_BUSY) {
-            if (++spins > XB_WAIT_LIMIT) {
-                XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_WAIT_TIMEOUT);
-                return nullptr;
-            }
-            __nanosleep(20);
-            s = xb_ld_acquire(&h->state);
-        }
-        if (h->hash == hash) {
-            const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
-            bool eq = true;
-            for (uint32_t k = 0; k < plan->nkeys && eq; k++)
-                eq = xb_key_equal(plan->keys[k], img[k], keys[k]);
-            if (eq)
-                return e;
-        }
-        pos = (pos + 1) & cap_mask;
-    }
-    *full = true;
-    return nullptr;
-}
 
 /* ================================================================
  * executor kernel
  * ================================================================ */
-struct XbExecArgs {
-    const xb_plan  *plan;           /* device copy (copied into shared memory) */
-    uint32_t        plan_bytes;     /* bytes of the plan copy: header + used code */
-    const xb_task  *tasks;          /* work queue: chunks of this launch */
-    uint32_t        ntasks;
-    uint64_t        nunits;         /* total units over all tasks */
-    uint32_t        format;         /* common KDS format of the tasks */
-    uint32_t        sm_cap;         /* shared-memory group table entries (0: none) */
-    uint32_t        warp_bytes;     /* shared memory of one warp: counters, cursors, registers */
-    xb_gtable      *gt;
-    xb_status      *st;
-};
-
-/* per-warp counters, in shared memory */
-struct XbWarpState {
-    unsigned long long raw, in, out;
-    unsigned long long depth[XB_MAX_DEPTH + 1];
-};
-
 /* probe cursor of one join depth for the 32 lanes of a warp (shared memory) */
 struct XbCursor {
     unsigned long long okey[32];    /* outer key (fused probe comparing a key column) */
@@ -337,51 +49,6 @@ struct XbCursor {
     uint32_t live;                  /* lanes whose probe chain may hold more rows */
     uint32_t __pad[3];
 };
-
-/* fixed-offset loader of one depth-0 load */
-struct XbFix {
-    int32_t  off;                   /* attcacheoff of the column */
-    uint8_t  ld;
-    uint8_t  reg;
-    uint16_t __pad;
-};
-
-/* column layout shared by every chunk of a launch, and the fixed-offset
- * loaders used while a tuple has no NULL bitmap */
-struct XbSrcMeta {
-    XbCol    cols[XB_MAX_COLS];
-    XbFix    fix[XB_MAX_LOADS];
-    int32_t  ncols;
-    uint32_t fixed;                 /* 1: every depth-0 load is fixed-width at a cached offset */
-    uint32_t fixed_end;             /* payload bytes those loads span */
-    uint32_t __pad;
-};
-
-#define XB_WARP_HEAD    ((sizeof(XbWarpState) + 15) & ~(size_t)15)
-
-__device__ __forceinline__ uint32_t xb_ld_acquire_cta(const uint32_t *p)
-{
-    uint32_t v;
-    asm volatile("ld.acquire.cta.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void xb_st_release_cta(uint32_t *p, uint32_t v)
-{
-    asm volatile("st.release.cta.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
-}
-
-/* byte width of a fixed-width loader, 0 for varlena */
-__device__ __forceinline__ int xb_ld_width(int ld)
-{
-    switch (ld) {
-    case XB_LD_BOOL: return 1;
-    case XB_LD_INT2: return 2;
-    case XB_LD_INT4: case XB_LD_DATE: case XB_LD_FLT4: return 4;
-    case XB_LD_INT8: case XB_LD_FLT8: return 8;
-    }
-    return 0;
-}
 
 /* ---------------------------------------------------------------
  * group table access from the register file
@@ -500,48 +167,21 @@ __device__ __forceinline__ void
 xb_update_one(const xb_agg &a, char *s, const XbRegs &R, uint32_t lane, const uint8_t *rk,
               xb_status *st)
 {
-    const bool n0 = RISNULL(R, a.arg0) != 0;
+    if (RISNULL(R, a.arg0))
+        return;
     const uint64_t v0 = RVAL(R, a.arg0);
     switch (a.action) {
     case KAGG_ACTION__PSUM_NUMERIC:
     case KAGG_ACTION__PAVG_NUMERIC:
-        if (!n0) {
-            uint8_t kind; int16_t w; xb_i128 v;
-            if (xb_numeric_decode((const uint8_t *)v0, &kind, &w, &v)) {
-                XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
-            } else if (kind == XB_NUM_VALID) {
-                atomicAdd((unsigned long long *)s, 1ULL);
-                xb_atomic_add_i128((uint64_t *)(s + 8), xb_numeric_rescale(a.weight, w, v));
-            } else {
-                uint32_t special = kind == XB_NUM_PINF ? PAGG_NUMERIC_ATTRS__PINF
-                                 : kind == XB_NUM_NINF ? PAGG_NUMERIC_ATTRS__NINF
-                                 : PAGG_NUMERIC_ATTRS__NAN;
-                atomicOr((unsigned int *)(s + 24), special);
-            }
-        }
+        xb_agg_numeric_add(s, (const uint8_t *)v0, a.weight, st);
         break;
     case KAGG_ACTION__STDDEV:
-        if (!n0) {
-            const double x = xb_reg_f64(v0, rk[a.arg0]);
-            atomicAdd((unsigned long long *)s, 1ULL);
-            xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
-            xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
-        }
+        xb_agg_stddev_add(s, xb_reg_f64(v0, rk[a.arg0]));
         break;
-    case KAGG_ACTION__COVAR: {
-        const bool n1 = RISNULL(R, a.arg1) != 0;
-        if (!n0 && !n1) {
-            const double x = xb_reg_f64(v0, rk[a.arg0]);
-            const double y = xb_reg_f64(RVAL(R, a.arg1), rk[a.arg1]);
-            atomicAdd((unsigned long long *)s, 1ULL);
-            xb_atomic_add_f64c((double *)(s + 8), (double *)(s + 16), x);
-            xb_atomic_add_f64c((double *)(s + 24), (double *)(s + 32), x * x);
-            xb_atomic_add_f64c((double *)(s + 40), (double *)(s + 48), y);
-            xb_atomic_add_f64c((double *)(s + 56), (double *)(s + 64), y * y);
-            xb_atomic_add_f64c((double *)(s + 72), (double *)(s + 80), x * y);
-        }
+    case KAGG_ACTION__COVAR:
+        if (!RISNULL(R, a.arg1))
+            xb_agg_covar_add(s, xb_reg_f64(v0, rk[a.arg0]), xb_reg_f64(RVAL(R, a.arg1), rk[a.arg1]));
         break;
-    }
     default:
         break;
     }
@@ -781,164 +421,6 @@ xb_prog_pass(const xb_prog &p, const XbRegs &R, uint32_t lane, uint32_t mask)
     return __ballot_sync(XB_FULL, ok);
 }
 
-/* ---------------------------------------------------------------
- * source units and 32-row batches
- * --------------------------------------------------------------- */
-struct XbSrc {
-    uint64_t unit;                  /* current unit (global index) */
-    uint64_t claim_end;             /* BLOCK: end of the current claim */
-    uint64_t next_claim;            /* BLOCK: first unit of the claim taken ahead */
-    const kern_data_store *kds;
-    const uint8_t *page;            /* BLOCK: current heap page */
-    uint32_t row0;                  /* ARROW / ROW: first row of the unit */
-    uint32_t item;                  /* next item of the unit */
-    uint32_t nitems;                /* items of the unit */
-};
-
-/* chunk owning global unit 'unit' (tasks are sorted by unit_base) */
-__device__ __forceinline__ uint32_t
-xb_find_task(const xb_task *tasks, uint32_t ntasks, uint64_t unit)
-{
-    uint32_t lo = 0, hi = ntasks;
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (tasks[mid].unit_base <= unit) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
-/* pull a claim's heap pages into L2 (TMA bulk prefetch) */
-__device__ __forceinline__ void
-xb_prefetch_claim(const XbExecArgs &args, uint64_t claim, uint32_t lane)
-{
-    if (lane < XB_CLAIM && claim + lane < args.nunits) {
-        const uint64_t u = claim + lane;
-        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
-        const char *p = (const char *)t.kds + t.kds->block_offset + (u - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
-        if ((((uintptr_t)p) & 15) == 0)
-            xb_prefetch_l2(p, PGSTROM_BLCKSZ);
-    }
-}
-
-/* move to the next unit; returns 0 = no more work, 1 = ok, 2 = corrupt page */
-__device__ __forceinline__ int
-xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane)
-{
-    if (*(volatile uint32_t *)&args.st->errcode != 0)
-        return 0;
-    if (args.format == KDS_FORMAT_BLOCK) {
-        s.unit++;
-        if (s.unit >= s.claim_end) {
-            s.unit = s.next_claim;
-            if (s.unit >= args.nunits)
-                return 0;
-            s.claim_end = min(s.unit + (uint64_t)XB_CLAIM, args.nunits);
-            unsigned long long nx = 0;
-            if (lane == 0)
-                nx = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)XB_CLAIM);
-            s.next_claim = __shfl_sync(XB_FULL, nx, 0);
-            xb_prefetch_claim(args, s.next_claim, lane);
-        }
-        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, s.unit)];
-        s.kds = t.kds;
-        s.page = (const uint8_t *)t.kds + t.kds->block_offset + (s.unit - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
-        const uint32_t pd_lower = (uint32_t)xb_fetch_le(s.page + 12, 2);
-        s.item = 0;
-        s.nitems = 0;
-        if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ)
-            s.nitems = (pd_lower - SizeOfPageHeaderData) / sizeof(ItemIdData);
-        else if (pd_lower > PGSTROM_BLCKSZ)
-            return 2;
-        return 1;
-    }
-    unsigned long long u = 0;
-    if (lane == 0)
-        u = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
-    u = __shfl_sync(XB_FULL, u, 0);
-    if (u >= args.nunits)
-        return 0;
-    const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
-    s.unit = u;
-    s.kds = t.kds;
-    s.row0 = (uint32_t)(u - t.unit_base) * XB_ROWS_UNIT;
-    const uint32_t left = t.kds->nitems > s.row0 ? t.kds->nitems - s.row0 : 0;
-    s.nitems = left < XB_ROWS_UNIT ? left : XB_ROWS_UNIT;
-    s.item = 0;
-    return 1;
-}
-
-/* Arrow column -> register (xpu_*_datum_arrow_read) */
-__device__ __forceinline__ bool
-xb_arrow_load(const kern_data_store *kds, const kern_colmeta *cm, uint32_t row, int ld,
-              uint64_t *val, uint32_t *aux, bool *isnull)
-{
-    if (cm->virtual_offset != 0) {
-        if (cm->virtual_offset < 0) { *isnull = true; return true; }
-        *isnull = false;
-        return xb_load_datum(ld, (const uint8_t *)kds + cm->virtual_offset, val, aux);
-    }
-    if (cm->nullmap_offset) {
-        const uint8_t *nm = (const uint8_t *)kds + cm->nullmap_offset;
-        uint32_t b = row >> 3;
-        if (b >= cm->nullmap_length || !((nm[b] >> (row & 7)) & 1)) { *isnull = true; return true; }
-    }
-    const uint8_t *values = (const uint8_t *)kds + cm->values_offset;
-    const int tag = cm->attopts.tag;
-    *isnull = false;
-    *aux = 0;
-    switch (ld) {
-    case XB_LD_INT2: case XB_LD_INT4: case XB_LD_INT8: {
-        uint32_t w = ld == XB_LD_INT2 ? 2 : ld == XB_LD_INT4 ? 4 : 8;
-        if (tag != ArrowType__Int || cm->attopts.u.integer.bitWidth != w * 8) return false;
-        if ((uint64_t)w * (row + 1) > cm->values_length) { *isnull = true; return true; }
-        int64_t v = w == 2 ? (int64_t)((const int16_t *)values)[row]
-                  : w == 4 ? (int64_t)((const int32_t *)values)[row]
-                           : ((const int64_t *)values)[row];
-        *val = (uint64_t)v;
-        return true;
-    }
-    case XB_LD_FLT8:
-        if (tag != ArrowType__FloatingPoint || cm->attopts.u.floating_point.precision != ArrowPrecision__Double)
-            return false;
-        if (8ULL * (row + 1) > cm->values_length) { *isnull = true; return true; }
-        *val = ((const uint64_t *)values)[row];
-        return true;
-    case XB_LD_DATE:
-        if (tag != ArrowType__Date) return false;
-        if (cm->attopts.u.date.unit == ArrowDateUnit__Day) {
-            if (4ULL * (row + 1) > cm->values_length) { *isnull = true; return true; }
-            *val = (uint64_t)(int64_t)(int32_t)(((const uint32_t *)values)[row] - 10957u);
-        } else {
-            if (8ULL * (row + 1) > cm->values_length) { *isnull = true; return true; }
-            *val = (uint64_t)(int64_t)(int32_t)(((const uint64_t *)values)[row] / 86400000ULL - 10957ULL);
-        }
-        return true;
-    case XB_LD_BOOL:
-        if (tag != ArrowType__Bool) return false;
-        if ((row >> 3) >= cm->values_length) { *isnull = true; return true; }
-        *val = (values[row >> 3] >> (row & 7)) & 1;
-        return true;
-    case XB_LD_TEXT: {
-        if (tag != ArrowType__Utf8 && tag != ArrowType__Binary && tag != ArrowType__LargeUtf8) return false;
-        const uint8_t *extra = (const uint8_t *)kds + cm->extra_offset;
-        uint64_t s, e;
-        if (tag == ArrowType__LargeUtf8) {
-            if (8ULL * (row + 2) > cm->values_length + 8) { *isnull = true; return true; }
-            s = ((const uint64_t *)values)[row]; e = ((const uint64_t *)values)[row + 1];
-        } else {
-            if (4ULL * (row + 2) > cm->values_length + 4) { *isnull = true; return true; }
-            s = ((const uint32_t *)values)[row]; e = ((const uint32_t *)values)[row + 1];
-        }
-        if (s > e || e > cm->extra_length) { *isnull = true; return true; }
-        *val = (uint64_t)(extra + s);
-        *aux = (uint32_t)(e - s);
-        return true;
-    }
-    default:
-        return false;
-    }
-}
-
 /* decode one heap tuple (HeapTupleHeaderData at htup, lp_len len) */
 __device__ __forceinline__ bool
 xb_decode_heap(const xb_plan *plan, const XbSrcMeta *meta, const XbRegs &R, uint32_t lane,
@@ -1104,39 +586,7 @@ xb_exec_kernel(XbExecArgs args)
             dst[i] = src[i];
     }
     /* all chunks of a launch share one column layout (checked by the host) */
-    const kern_data_store *kds0 = args.tasks[0].kds;
-    const int ncols = kds0->ncols < XB_MAX_COLS ? (int)kds0->ncols : XB_MAX_COLS;
-    for (int i = threadIdx.x; i < ncols; i += blockDim.x) {
-        meta->cols[i].attlen = kds0->colmeta[i].attlen;
-        meta->cols[i].attalign = kds0->colmeta[i].attalign > 0 ? kds0->colmeta[i].attalign : 1;
-        meta->cols[i].attcacheoff = kds0->colmeta[i].attcacheoff;
-    }
-    if (threadIdx.x == 0) {
-        const xb_plan *gp = args.plan;
-        uint32_t fixed = (args.format != KDS_FORMAT_ARROW) ? 1u : 0u, end = 0;
-        for (uint32_t i = 0; i < gp->nload0; i++) {
-            const xb_load &l = gp->load0[i];
-            XbFix f;
-            f.off = 0; f.ld = l.ld; f.reg = l.reg; f.__pad = 0;
-            if (l.resno < 1 || l.resno > ncols) {
-                fixed = 0;
-            } else {
-                const kern_colmeta &cm = kds0->colmeta[l.resno - 1];
-                const int w = xb_ld_width(l.ld);
-                if (w == 0 || cm.attlen != w || cm.attcacheoff < 0) {
-                    fixed = 0;
-                } else {
-                    f.off = cm.attcacheoff;
-                    if ((uint32_t)(cm.attcacheoff + w) > end)
-                        end = cm.attcacheoff + w;
-                }
-            }
-            meta->fix[i] = f;
-        }
-        meta->ncols = ncols;
-        meta->fixed = fixed;
-        meta->fixed_end = end;
-    }
+    xb_setup_meta(args, meta);
     for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
         ((uint32_t *)sm_entries)[i] = 0;
     for (size_t i = lane; i < XB_WARP_HEAD / 4; i += 32)
@@ -1718,6 +1168,14 @@ struct xpuB200Session {
     uint64_t        total_raw = 0, total_in = 0, total_out = 0;
     uint64_t        total_depth[XB_MAX_DEPTH + 1] = {0};
     cudaEvent_t     ev0, ev1;
+    /* session-specialised kernels, per source format (index: KDS format) */
+    bool            jit_enabled = true;
+    bool            jit_tried[256] = {false};
+    void           *jit_fn[256] = {nullptr};
+    int             jit_grid[256] = {0};
+    size_t          jit_smem = 0;
+    double          jit_compile_ms = 0.0;
+    std::string     jit_msg;
 };
 
 static const char *xb_msg_text(uint32_t id)
@@ -2001,6 +1459,12 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     if (per_sm < 1)
         FAIL(ERRCODE_DEVICE_FATAL, "executor kernel does not fit on an SM (%zu bytes smem)", s->smem_bytes);
     s->grid = per_sm * dev->nsm;
+    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + (size_t)s->sm_cap * plan->gent_size;
+    {
+        const char *env = getenv("XPU_B200_JIT");
+        s->jit_enabled = !(env && env[0] == '0');
+        s->jit_msg = s->jit_enabled ? "not built yet" : "disabled";
+    }
 #undef FAIL
 #undef DALLOC
     *p_sess = s;
@@ -2037,12 +1501,39 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     a.warp_bytes = s->warp_bytes;
     a.gt = s->d_gt;
     a.st = s->d_status;
-    int grid = s->grid;
+    /* the session-specialised kernel of this format, built on first use */
+    void *fn = nullptr;
+    if (s->jit_enabled && format < 256) {
+        if (!s->jit_tried[format]) {
+            s->jit_tried[format] = true;
+            char msg[1024];
+            double ms = 0.0;
+            int per_sm = 0;
+            if (xb_jit_compile(s->h_plan, format, s->dev->dindex, &s->jit_fn[format], &ms, msg, sizeof(msg)) != 0) {
+                s->jit_fn[format] = nullptr;
+                s->jit_msg = msg;
+            } else if (xb_jit_prepare(s->jit_fn[format], XB_BLOCK, s->jit_smem, &per_sm) != 0) {
+                s->jit_fn[format] = nullptr;
+                s->jit_msg = "specialised kernel does not fit on an SM";
+            } else {
+                s->jit_grid[format] = per_sm * s->dev->nsm;
+                s->jit_compile_ms += ms;
+                s->jit_msg = "ok";
+            }
+        }
+        fn = s->jit_fn[format];
+    }
+    int grid = fn ? s->jit_grid[format] : s->grid;
     uint64_t warps_needed = (format == KDS_FORMAT_BLOCK) ? (nunits + XB_CLAIM - 1) / XB_CLAIM : nunits;
     if ((uint64_t)grid * XB_WARPS > warps_needed)
         grid = (int)((warps_needed + XB_WARPS - 1) / XB_WARPS);
     if (grid < 1) grid = 1;
-    xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, s->dev->stream>>>(a);
+    if (fn) {
+        if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem, (void *)s->dev->stream, &a) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
+    } else {
+        xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, s->dev->stream>>>(a);
+    }
     cudaError_t rc = cudaGetLastError();
     if (rc != cudaSuccess)
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "kernel launch: %s", cudaGetErrorString(rc));
@@ -2554,13 +2045,25 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
 {
     if (!s || !buf) return ERRCODE_DEVICE_ERROR;
     const xb_plan *p = s->h_plan;
+    /* which kernel runs each format: "jit" (session-specialised) or "vm" */
+    std::string kinds, msg;
+    for (int f : {KDS_FORMAT_ROW, KDS_FORMAT_BLOCK, KDS_FORMAT_ARROW}) {
+        if (!s->jit_tried[f])
+            continue;
+        if (!kinds.empty()) kinds += ", ";
+        kinds += std::string("\"") + (char)f + "\": \"" + (s->jit_fn[f] ? "jit" : "vm") + "\"";
+    }
+    for (char c : s->jit_msg)
+        msg += (c == '"' || c == '\\' || (unsigned char)c < 32) ? ' ' : c;
     snprintf(buf, buf_sz,
              "{\"nregs\": %u, \"nslots\": %u, \"nrels\": %u, \"ninsns\": %u, \"has_groupby\": %u, "
              "\"nkeys\": %u, \"naggs\": %u, \"gent_size\": %u, \"gtable_cap\": %llu, "
-             "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u]}",
+             "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u], "
+             "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\"}",
              p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
              p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
-             s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash);
+             s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash,
+             s->jit_enabled ? "true" : "false", kinds.c_str(), s->jit_compile_ms, msg.c_str());
     return 0;
 }
 

@@ -1,0 +1,41 @@
+/*
+ * xb_jit.h
+ *
+ * Session-specialised executor kernels: source generation from a translated
+ * session (xb_plan), NVRTC compilation for sm_100a and launch through the
+ * driver API.  See xb_jit.cpp.
+ */
+#ifndef XB_JIT_H
+#define XB_JIT_H
+#include <stddef.h>
+#include <stdint.h>
+#include "xb_plan.h"
+
+#define XBJ_MIN_BLOCKS_DEFAULT  2   /* resident CTAs of 256 threads per SM */
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* the generated CUDA source (for inspection); *p_len = its length */
+int xb_jit_source(const xb_plan *plan, uint32_t format, char *buf, size_t bufsz, size_t *p_len);
+
+/* build (or find in the process-wide cache) the kernel of plan + format on
+ * device dindex; *p_func is a CUfunction */
+int xb_jit_compile(const xb_plan *plan, uint32_t format, int dindex,
+                   void **p_func, double *p_compile_ms, char *errbuf, size_t errlen);
+
+/* compile only (no device needed): cubin size and NVRTC milliseconds */
+int xb_jit_check(const xb_plan *plan, uint32_t format, uint64_t *p_cubin_bytes, double *p_compile_ms,
+                 char *errbuf, size_t errlen);
+
+/* allow 'smem' bytes of dynamic shared memory; resident CTAs per SM */
+int xb_jit_prepare(void *func, int block, size_t smem, int *p_per_sm);
+
+/* launch with one kernel parameter block ('args' points to XbExecArgs) */
+int xb_jit_launch(void *func, int grid, int block, size_t smem, void *stream, void *args);
+
+#ifdef __cplusplus
+}
+#endif
+#endif  /* XB_JIT_H */

@@ -1,0 +1,174 @@
+/*
+ * xb_jit_rt.cuh
+ *
+ * Skeleton of the session-specialised executor kernel.  xb_jit.cpp emits,
+ * for one translated session (xb_plan) and one source format, a CUDA
+ * translation unit of the form
+ *
+ *     #include "xb_exec_dev.cuh"
+ *     #define XBJ_NREGS ... (plan constants)
+ *     struct XbjRegs { ... };          registers as plain locals
+ *     #include "xb_jit_rt.cuh"         this file: prototypes + kernel
+ *     ... generated definitions of xbj_decode / xbj_pipeline ...
+ *
+ * compiled by NVRTC for sm_100a.  Each lane carries one source row through
+ * decode, scan quals, every join depth (per-lane probe loops over the
+ * inner hash indexes) and the group-by update, with the plan's bytecode
+ * turned into straight-line code over registers.  Units (heap pages,
+ * 1024-row groups) are claimed per warp from the launch's work queue
+ * exactly as in the interpreting kernel (xb_exec.cu), and the statistics,
+ * shared-memory group table and error reporting are the same.
+ */
+#ifndef XB_JIT_RT_CUH
+#define XB_JIT_RT_CUH
+
+struct XbjEnv {
+    const xb_plan  *plan;           /* device plan (global memory) */
+    xb_status      *st;
+    xb_gtable      *gt;
+    char           *gt_entries;     /* global group table */
+    uint64_t        gt_mask;
+    char           *sm_tab;         /* shared-memory group table, or nullptr */
+    uint32_t        sm_mask;
+    uint32_t        lane;
+};
+
+struct XbjCnt {
+    unsigned long long raw, in, out;
+    unsigned long long depth[XB_MAX_DEPTH + 1];
+};
+
+/* generated per session */
+__device__ __forceinline__ bool
+xbj_decode(XbjRegs &R, const XbExecArgs &args, const XbSrc &s, const XbSrcMeta *meta,
+           uint32_t idx, bool &exists, xb_status *st);
+__device__ __forceinline__ void
+xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
+
+__device__ __forceinline__ unsigned long long xbj_warp_sum(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(XB_FULL, v, o);
+    return v;
+}
+
+extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
+xbj_kernel(XbExecArgs args)
+{
+    extern __shared__ __align__(16) char smem[];
+    const uint32_t lane = threadIdx.x & 31;
+    XbSrcMeta *meta = (XbSrcMeta *)smem;
+    char *sm_entries = smem + ((sizeof(XbSrcMeta) + 15) & ~(size_t)15);
+    const size_t sm_bytes = (size_t)args.sm_cap * XBJ_GENT_SIZE;
+
+    xb_setup_meta(args, meta);
+    for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
+        ((uint32_t *)sm_entries)[i] = 0;
+    __syncthreads();
+
+    XbjEnv E;
+    E.plan = args.plan;
+    E.st = args.st;
+    E.gt = args.gt;
+    E.gt_entries = args.gt ? args.gt->entries : nullptr;
+    E.gt_mask = args.gt ? args.gt->cap_mask : 0;
+    E.sm_tab = args.sm_cap ? sm_entries : nullptr;
+    E.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
+    E.lane = lane;
+    XbjCnt C;
+    C.raw = C.in = C.out = 0;
+#pragma unroll
+    for (int d = 0; d <= XB_MAX_DEPTH; d++)
+        C.depth[d] = 0;
+
+    XbSrc src;
+    src.unit = 0;
+    src.claim_end = 0;
+    src.next_claim = 0;
+    src.kds = nullptr;
+    src.page = nullptr;
+    src.row0 = 0;
+    src.item = 0;
+    src.nitems = 0;
+    if (args.format == KDS_FORMAT_BLOCK) {
+        unsigned long long c0 = 0;
+        if (lane == 0)
+            c0 = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)XB_CLAIM);
+        src.next_claim = __shfl_sync(XB_FULL, c0, 0);
+        xb_prefetch_claim(args, src.next_claim, lane);
+    }
+
+    for (;;) {
+        bool done = false;
+        while (src.item >= src.nitems) {
+            const int rc = xb_next_unit(args, src, lane);
+            if (rc == 0) { done = true; break; }
+            if (rc == 2) {
+                if (lane == 0) XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
+                done = true;
+                break;
+            }
+        }
+        if (done)
+            break;
+        const uint32_t idx = src.item + lane;
+        src.item += 32;
+        bool failed = false;
+        if (idx < src.nitems) {
+            XbjRegs R;
+            bool exists = false;
+            const bool ok = xbj_decode(R, args, src, meta, idx, exists, args.st);
+            if (exists)
+                C.raw++;
+            if (exists && !ok)
+                failed = true;
+            else if (ok)
+                xbj_pipeline(R, E, C, failed);
+        }
+        if (__any_sync(XB_FULL, failed))
+            break;
+    }
+
+    /* statistics */
+    {
+        const unsigned long long raw = xbj_warp_sum(C.raw);
+        const unsigned long long in = xbj_warp_sum(C.in);
+        const unsigned long long out = xbj_warp_sum(C.out);
+        if (lane == 0) {
+            atomicAdd((unsigned long long *)&args.st->nitems_raw, raw);
+            atomicAdd((unsigned long long *)&args.st->nitems_in, in);
+            atomicAdd((unsigned long long *)&args.st->nitems_out, out);
+        }
+#pragma unroll
+        for (int d = 1; d <= XBJ_NRELS; d++) {
+            const unsigned long long v = xbj_warp_sum(C.depth[d]);
+            if (lane == 0)
+                atomicAdd((unsigned long long *)&args.st->nitems_depth[d], v);
+        }
+    }
+    __syncthreads();
+
+    /* merge the shared-memory group table into the global table */
+    if (args.sm_cap) {
+        const xb_plan *plan = args.plan;
+        for (uint32_t i = threadIdx.x; i < args.sm_cap; i += blockDim.x) {
+            char *e = sm_entries + (size_t)i * XBJ_GENT_SIZE;
+            const xb_gent_head *h = (const xb_gent_head *)e;
+            if (h->state != XB_GSTATE_READY)
+                continue;
+            const xb_keyimg *img = (const xb_keyimg *)(e + XBJ_KEYS_OFF);
+            bool full = false;
+            char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, h->hash,
+                                    img, args.gt, args.st, &full);
+            if (g)
+                xb_merge_states(plan, g, e);
+            else if (full) {
+                XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+                atomicOr(&args.gt->overflow, 1u);
+            }
+        }
+    }
+}
+
+#endif  /* XB_JIT_RT_CUH */

@@ -175,8 +175,8 @@ class Session:
 
     def info(self):
         import json
-        b = ctypes.create_string_buffer(1024)
-        lib().xpuB200SessionInfo(self.h, b, 1024)
+        b = ctypes.create_string_buffer(4096)
+        lib().xpuB200SessionInfo(self.h, b, 4096)
         return json.loads(b.value.decode())
 
     def close(self):

@@ -1,6 +1,10 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle and with
 the generator's ground truth.  Integer / numeric / text states bit-exact;
-float8 sums within 1e-12 relative of the FP64 row-ordered sum."""
+float8 sums within 1e-12 relative of the FP64 row-ordered sum.
+
+Every test runs twice: on the session-specialised kernel ("jit", built by
+NVRTC at the first launch) and on the interpreting kernel ("vm",
+XPU_B200_JIT=0); each run checks that the intended kernel executed."""
 import numpy as np
 import pytest
 
@@ -12,7 +16,19 @@ import xpu_b200
 pytestmark = pytest.mark.gpu
 
 
-def run_gpu(device, sess, chunks, kmrels=None, nrels=0, on_device=False):
+@pytest.fixture(params=["jit", "vm"])
+def kernel(request, monkeypatch):
+    monkeypatch.setenv("XPU_B200_JIT", "1" if request.param == "jit" else "0")
+    return request.param
+
+
+def check_kernel(s, kernel):
+    info = s.info()
+    ran = set(info["kernels"].values())
+    assert ran == {kernel}, f"expected the {kernel} kernel, ran {info['kernels']}: {info['jit_msg']}"
+
+
+def run_gpu(device, sess, chunks, kmrels=None, nrels=0, on_device=False, kernel=None):
     s = xpu_b200.Session(device, sess, kmrels, nrels)
     totals = {"nitems_raw": 0, "nitems_in": 0, "nitems_out": 0, "depth_out": [0] * nrels}
     bufs = []
@@ -27,6 +43,8 @@ def run_gpu(device, sess, chunks, kmrels=None, nrels=0, on_device=False):
             totals[k] += r[k]
         for d in range(nrels):
             totals["depth_out"][d] += r["depth_out"][d]
+    if kernel:
+        check_kernel(s, kernel)
     final, res = s.final()
     s.close()
     for b in bufs:
@@ -45,10 +63,10 @@ def run_oracle(sess, chunks, kmrels=None):
 
 
 @pytest.mark.parametrize("nrows,ppc", [(20_000, 64), (400_000, 1000)])
-def test_scan_groupby_parity(device, nrows, ppc):
+def test_scan_groupby_parity(device, kernel, nrows, ppc):
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=nrows)
     chunks = tbl.block_chunks(pages_per_chunk=ppc)
-    final, st, res = run_gpu(device, sess, chunks)
+    final, st, res = run_gpu(device, sess, chunks, kernel=kernel)
     assert st["nitems_raw"] == meta["nitems_raw"]
     assert st["nitems_in"] == meta["nitems_in"]
     got = F.decode_kds_final(final, sess)
@@ -60,26 +78,26 @@ def test_scan_groupby_parity(device, nrows, ppc):
     assert res["final_nitems"] == len(truth)
 
 
-def test_scan_groupby_device_resident(device):
+def test_scan_groupby_device_resident(device, kernel):
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=100_000)
     chunks = tbl.block_chunks(pages_per_chunk=200)
-    final, st, _ = run_gpu(device, sess, chunks, on_device=True)
+    final, st, _ = run_gpu(device, sess, chunks, on_device=True, kernel=kernel)
     truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
     assert F.compare_groups(F.decode_kds_final(final, sess), truth) == []
 
 
-def test_scan_groupby_empty_result(device):
+def test_scan_groupby_empty_result(device, kernel):
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=10_000, a_limit=0)
-    final, st, res = run_gpu(device, sess, tbl.block_chunks())
+    final, st, res = run_gpu(device, sess, tbl.block_chunks(), kernel=kernel)
     assert st["nitems_in"] == 0
     assert F.decode_kds_final(final, sess) == {}
 
 
 @pytest.mark.parametrize("nfact,nd1,nd2,ppc", [(50_000, 2000, 300, 128), (1_000_000, 200_000, 10_000, 2048)])
-def test_join_groupby_parity(device, nfact, nd1, nd2, ppc):
+def test_join_groupby_parity(device, kernel, nfact, nd1, nd2, ppc):
     fact, sess, km, expect, meta = C.join_groupby(nfact=nfact, ndim1=nd1, ndim2=nd2)
     chunks = fact.block_chunks(pages_per_chunk=ppc)
-    final, st, res = run_gpu(device, sess, chunks, km, nrels=2)
+    final, st, res = run_gpu(device, sess, chunks, km, nrels=2, kernel=kernel)
     assert st["nitems_raw"] == meta["nitems_raw"]
     assert st["nitems_out"] == meta["nitems_out"]
     assert st["depth_out"] == meta["depth_out"]
@@ -91,22 +109,23 @@ def test_join_groupby_parity(device, nfact, nd1, nd2, ppc):
 
 
 @pytest.mark.parametrize("nrows,nkeys,rpc", [(300_000, 20_000, 100_000), (2_000_000, 1_000_000, 700_000)])
-def test_arrow_groupby_parity(device, nrows, nkeys, rpc):
+def test_arrow_groupby_parity(device, kernel, nrows, nkeys, rpc):
     chunks, sess, expect, meta = C.arrow_groupby(nrows=nrows, nkeys=nkeys, rows_per_chunk=rpc)
-    final, st, res = run_gpu(device, sess, chunks)
+    final, st, res = run_gpu(device, sess, chunks, kernel=kernel)
     assert st["nitems_raw"] == meta["nitems_raw"]
     assert st["nitems_in"] == meta["nitems_in"]
     got = F.decode_kds_final(final, sess)
     assert F.compare_groups(got, expect) == []
 
 
-def test_batch_matches_single_chunk_path(device):
+def test_batch_matches_single_chunk_path(device, kernel):
     fact, sess, km, expect, meta = C.join_groupby(nfact=300_000, ndim1=20_000, ndim2=2_000)
     chunks = fact.block_chunks(pages_per_chunk=300)
     s = xpu_b200.Session(device, sess, km, 2)
     ups = [device.upload(c) for c in chunks]
     b = s.batch([p for _, p in ups])
     r = b.exec()
+    check_kernel(s, kernel)
     assert r["nitems_raw"] == meta["nitems_raw"] and r["nitems_out"] == meta["nitems_out"]
     assert r["depth_out"] == meta["depth_out"]
     final, _ = s.final()

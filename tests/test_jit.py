@@ -1,0 +1,69 @@
+"""The session-specialised kernels: the source generated for each workload's
+translated session compiles for sm_100a with NVRTC.  Compilation needs no
+GPU; the kernels' results are checked against the oracle by the GPU parity
+tests (test_gpu_parity.py runs every case on both kernels)."""
+import ctypes
+import os
+
+import pytest
+
+import xb_configs as C
+import xpu_b200
+
+PLAN_BYTES = 1 << 20
+
+
+def _lib():
+    if not os.path.exists(xpu_b200.LIB_PATH):
+        pytest.skip("library not built")
+    return ctypes.CDLL(xpu_b200.LIB_PATH)
+
+
+def _translate(L, sess, km):
+    sb = bytes(sess)
+    kb = bytes(km) if km is not None else None
+    plan = ctypes.create_string_buffer(PLAN_BYTES)
+    err = ctypes.create_string_buffer(1024)
+    rc = L.xb_compile_session(sb, ctypes.c_size_t(len(sb)), ctypes.c_uint64(1 << 32), kb, plan, err,
+                              ctypes.c_size_t(len(err)))
+    assert rc == 0, err.value.decode()
+    return plan
+
+
+def _sessions():
+    _, s0, _, _, _ = C.scan_groupby(nrows=1000)
+    _, s1, k1, _, _ = C.join_groupby(nfact=1000, ndim1=100, ndim2=10)
+    _, s2, _, _ = C.arrow_groupby(nrows=1000, nkeys=100, rows_per_chunk=1000, with_expect=False)
+    return [("scan_groupby", s0, None, ord("b")), ("join_groupby", s1, k1, ord("b")),
+            ("arrow_groupby", s2, None, ord("a")), ("join_groupby_row", s1, k1, ord("r"))]
+
+
+@pytest.mark.parametrize("case", range(4))
+def test_specialised_kernel_compiles(case):
+    L = _lib()
+    name, sess, km, fmt = _sessions()[case]
+    plan = _translate(L, sess, km)
+    nbytes = ctypes.c_uint64(0)
+    ms = ctypes.c_double(0.0)
+    err = ctypes.create_string_buffer(2048)
+    rc = L.xb_jit_check(plan, ctypes.c_uint32(fmt), ctypes.byref(nbytes), ctypes.byref(ms), err,
+                        ctypes.c_size_t(len(err)))
+    msg = err.value.decode()
+    if rc != 0 and "libnvrtc" in msg:
+        pytest.skip(msg)
+    assert rc == 0, f"{name}: {msg}"
+    assert nbytes.value > 0
+
+
+def test_generated_source_names_the_plan():
+    L = _lib()
+    _, sess, km, _, _ = C.join_groupby(nfact=1000, ndim1=100, ndim2=10)
+    plan = _translate(L, sess, km)
+    n = ctypes.c_size_t(0)
+    buf = ctypes.create_string_buffer(1 << 20)
+    assert L.xb_jit_source(plan, ctypes.c_uint32(ord("b")), buf, ctypes.c_size_t(len(buf)), ctypes.byref(n)) == 0
+    src = buf.value.decode()
+    assert n.value == len(src)
+    # two join depths, a group-by and no interpreter loop
+    assert "/* depth 1 */" in src and "/* depth 2 */" in src and "/* depth 3 */" not in src
+    assert "xbj_group_get<true>" in src and "xb_vm_exec" not in src
