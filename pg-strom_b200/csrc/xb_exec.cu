@@ -1172,6 +1172,7 @@ struct xpuB200Session {
     bool            jit_enabled = true;
     bool            jit_tried[256] = {false};
     void           *jit_fn[256] = {nullptr};
+    char            ran_kind[256] = {0};   /* 'j' / 'v': kernel last launched per format */
     int             jit_grid[256] = {0};
     size_t          jit_smem = 0;
     double          jit_compile_ms = 0.0;
@@ -1528,6 +1529,8 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     if ((uint64_t)grid * XB_WARPS > warps_needed)
         grid = (int)((warps_needed + XB_WARPS - 1) / XB_WARPS);
     if (grid < 1) grid = 1;
+    if (format < 256)
+        s->ran_kind[format] = fn ? 'j' : 'v';
     if (fn) {
         if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem, (void *)s->dev->stream, &a) != 0)
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
@@ -2048,10 +2051,10 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
     /* which kernel runs each format: "jit" (session-specialised) or "vm" */
     std::string kinds, msg;
     for (int f : {KDS_FORMAT_ROW, KDS_FORMAT_BLOCK, KDS_FORMAT_ARROW}) {
-        if (!s->jit_tried[f])
+        if (!s->ran_kind[f])
             continue;
         if (!kinds.empty()) kinds += ", ";
-        kinds += std::string("\"") + (char)f + "\": \"" + (s->jit_fn[f] ? "jit" : "vm") + "\"";
+        kinds += std::string("\"") + (char)f + "\": \"" + (s->ran_kind[f] == 'j' ? "jit" : "vm") + "\"";
     }
     for (char c : s->jit_msg)
         msg += (c == '"' || c == '\\' || (unsigned char)c < 32) ? ' ' : c;
