@@ -83,6 +83,32 @@ int  xpuB200Final(xpuB200Session *sess, void *kds_final_buf, uint64_t buf_sz,
                   uint64_t *p_required, kern_exec_results *results,
                   kern_errorbuf *err);
 
+/*
+ * xpuB200Final for callers that cannot allocate GPU memory: a service that
+ * reserved the device's memory at start-up and sub-allocates its own pool,
+ * or one that must not call cudaMalloc / cudaFree while other sessions run
+ * (cudaFree waits for the whole device).  No counterpart in the reference:
+ * its GPU service allocates kds_final itself.
+ *
+ * kds_final is written in the same layout as xpuB200Final's, but into
+ * kds_final_dev, memory the caller owns on the session's GPU (device
+ * memory, managed memory or mapped pinned host memory), of buf_sz bytes.
+ * With kds_final_dev NULL and buf_sz 0 only *p_required is set.  Nothing is
+ * allocated: the work arrays live in one fixed 8 MiB array per GPU,
+ * enough for a session whose group table has up to 262,144 slots (tables
+ * are powers of two; about 65,000 groups at the default sizing).  Larger
+ * tables are rejected with ERRCODE_DEVICE_ERROR and a message saying so
+ * (use xpuB200Final for them).
+ *
+ * The first call on each GPU looks up the array's device address; make
+ * that first call before capturing any stream.  All calls in a process
+ * share the array: they are serialised by a lock and each returns after
+ * its GPU work has finished.  Work that overlapped on the GPU would race
+ * on the shared array.
+ */
+int  xpuB200FinalNoAlloc(xpuB200Session *sess, void *kds_final_dev, uint64_t buf_sz,
+                         uint64_t *p_required, kern_exec_results *results, kern_errorbuf *err);
+
 void xpuB200CloseSession(xpuB200Session *sess);
 
 /*

@@ -1827,6 +1827,177 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
 }
 
 /* ----------------------------------------------------------------
+ * Final without device allocations
+ *
+ * xpuB200Final allocates its work arrays (per-slot tuple sizes, their
+ * prefix sums, CUB scan storage) and a device copy of kds_final with
+ * cudaMalloc on every call.  Some callers cannot do that: a service that
+ * has reserved the GPU's memory up front and hands out pieces of its own
+ * pool (as PG-Strom's GPU service does with its device memory), or one
+ * that must not call cudaMalloc / cudaFree while other sessions' kernels
+ * run, because cudaFree waits for the whole device.  This variant writes
+ * kds_final into memory the caller already owns and keeps its work arrays
+ * in the fixed array below, which lives in the library's module on every
+ * GPU that loads it until the process exits.
+ * ---------------------------------------------------------------- */
+#define XB_FINAL_SCRATCH_BYTES  (8ULL << 20)        /* 8 MiB per GPU */
+#define XB_FINAL_SCRATCH_DEVS   64
+
+static __device__ __align__(256) char xb_final_scratch[XB_FINAL_SCRATCH_BYTES];
+
+/* device address of xb_final_scratch on each GPU, looked up once per device
+ * (the host-side symbol is not a device address) */
+static void *xb_final_scratch_dptr[XB_FINAL_SCRATCH_DEVS];
+/* every session of the process shares the array: one call at a time */
+static std::mutex xb_final_scratch_lock;
+
+static inline uint64_t xb_align256(uint64_t x)
+{
+    return (x + 255) & ~255ULL;
+}
+
+extern "C" int
+xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uint64_t *p_required,
+                    kern_exec_results *results, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid FinalNoAlloc arguments");
+    std::lock_guard<std::mutex> g(s->lock);
+    std::lock_guard<std::mutex> gs(xb_final_scratch_lock);
+    const int dindex = s->dev->dindex;
+    if (dindex < 0 || dindex >= XB_FINAL_SCRATCH_DEVS)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "FinalNoAlloc supports GPUs 0..%d", XB_FINAL_SCRATCH_DEVS - 1);
+    XB_CUDA(cudaSetDevice(dindex), err);
+    if (!xb_final_scratch_dptr[dindex]) {
+        void *ptr = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress(&ptr, xb_final_scratch);
+        if (rc != cudaSuccess || !ptr) {
+            cudaGetLastError();
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalNoAlloc: scratch address on GPU %d: %s",
+                          dindex, cudaGetErrorString(rc));
+        }
+        xb_final_scratch_dptr[dindex] = ptr;
+    }
+    char *scratch = (char *)xb_final_scratch_dptr[dindex];
+    cudaStream_t st = s->dev->stream;
+    const xb_plan *plan = s->h_plan;
+    if (results) {
+        uint32_t cap = results->num_rels;
+        results->nitems_raw = (uint32_t)s->total_raw;
+        results->nitems_in = (uint32_t)s->total_in;
+        results->nitems_out = (uint32_t)s->total_out;
+        results->num_rels = plan->nrels;
+        for (uint32_t d = 1; d <= plan->nrels && d <= cap; d++)
+            results->stats[d - 1].nitems_out = (uint32_t)s->total_depth[d];
+        results->final_plan_task = true;
+    }
+    if (!plan->has_groupby) {
+        if (p_required) *p_required = 0;
+        return 0;
+    }
+    const kern_session_info *session = (const kern_session_info *)s->h_session.data();
+    const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
+    const uint64_t head_len = KDS_HEAD_LENGTH(fh);
+    const uint64_t cap = s->h_gt.cap_mask + 1;
+
+    /* scratch layout: sizes | size prefix sums | flags | flag prefix sums | scan storage */
+    const uint64_t off_sscan = xb_align256(cap * 8);
+    const uint64_t off_flags = off_sscan + xb_align256(cap * 8);
+    const uint64_t off_fscan = off_flags + xb_align256(cap * 4);
+    const uint64_t off_temp = off_fscan + xb_align256(cap * 4);
+    uint64_t *d_sizes = (uint64_t *)scratch;
+    uint64_t *d_size_scan = (uint64_t *)(scratch + off_sscan);
+    uint32_t *d_flags = (uint32_t *)(scratch + off_flags);
+    uint32_t *d_flag_scan = (uint32_t *)(scratch + off_fscan);
+    void *d_temp = scratch + off_temp;
+    size_t temp1 = 0, temp2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, temp1, d_sizes, d_size_scan, (int64_t)cap, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, temp2, d_flags, d_flag_scan, (int64_t)cap, st);
+    const uint64_t tsz_max = temp1 > temp2 ? temp1 : temp2;
+    if (off_temp + tsz_max > XB_FINAL_SCRATCH_BYTES)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR,
+                      "FinalNoAlloc: the session's group table has %llu slots and needs %llu bytes of work "
+                      "space, above this entry point's fixed %llu bytes; use xpuB200Final",
+                      (unsigned long long)cap, (unsigned long long)(off_temp + tsz_max),
+                      (unsigned long long)XB_FINAL_SCRATCH_BYTES);
+    if (kds_final_dev) {
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, kds_final_dev) != cudaSuccess) {
+            cudaGetLastError();
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "FinalNoAlloc: kds_final_dev is not CUDA memory");
+        }
+        const bool ok = (pa.type == cudaMemoryTypeDevice && pa.device == dindex) ||
+                        pa.type == cudaMemoryTypeManaged ||
+                        (pa.type == cudaMemoryTypeHost && pa.devicePointer == kds_final_dev);
+        if (!ok)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR,
+                          "FinalNoAlloc: kds_final_dev must be memory of GPU %d (or mapped host memory)", dindex);
+    }
+    /* the previous call's values are still in the array; start clean */
+    cudaMemsetAsync(d_sizes, 0, cap * 8, st);
+    cudaMemsetAsync(d_flags, 0, cap * 4, st);
+    XbFinalArgs fa;
+    memset(&fa, 0, sizeof(fa));
+    fa.plan = s->d_plan;
+    fa.gt = s->d_gt;
+    fa.cap = cap;
+    fa.sizes = d_sizes;
+    fa.flags = d_flags;
+    fa.size_scan = d_size_scan;
+    fa.flag_scan = d_flag_scan;
+    const int grid = s->dev->nsm * 8;
+    xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
+    size_t tsz = tsz_max;
+    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_sizes, d_size_scan, (int64_t)cap, st);
+    tsz = tsz_max;
+    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_flags, d_flag_scan, (int64_t)cap, st);
+    uint64_t last_size = 0, last_scan = 0;
+    uint32_t last_flag = 0, last_fscan = 0;
+    cudaMemcpyAsync(&last_size, d_sizes + cap - 1, 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last_scan, d_size_scan + cap - 1, 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last_flag, d_flags + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last_fscan, d_flag_scan + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalNoAlloc: %s", cudaGetErrorString(cudaGetLastError()));
+    const uint64_t items = last_scan + last_size;
+    const uint64_t ngroups = (uint64_t)last_fscan + last_flag;
+    const uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(ngroups);
+    const uint64_t items_base = head_len + 8 * nslots + 8 * ngroups;
+    const uint64_t length = items_base + items;
+    if (p_required) *p_required = length;
+    if (results) {
+        results->final_nitems = (uint32_t)ngroups;
+        results->final_usage = items;
+        results->final_total = length;
+    }
+    if (!kds_final_dev || buf_sz < length) {
+        if (!kds_final_dev && buf_sz == 0)
+            return 0;           /* size query only */
+        return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE, "kds_final needs %llu bytes (buffer %llu)",
+                      (unsigned long long)length, (unsigned long long)buf_sz);
+    }
+    char *d_out = (char *)kds_final_dev;
+    std::vector<char> head((const char *)fh, (const char *)fh + head_len);
+    kern_data_store *kh = (kern_data_store *)head.data();
+    kh->length = length;
+    kh->usage = items;
+    kh->nitems = (uint32_t)ngroups;
+    kh->format = KDS_FORMAT_HASH;
+    kh->hash_nslots = (uint32_t)nslots;
+    cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(d_out + head_len, 0, 8 * nslots + 8 * ngroups, st);
+    fa.kds_final = d_out;
+    fa.items_base = items_base;
+    fa.length = length;
+    fa.nslots = (uint32_t)nslots;
+    xb_final_write<<<grid, XB_BLOCK, 0, st>>>(fa);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalNoAlloc: %s", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+/* ----------------------------------------------------------------
  * prepared batches: many device-resident chunks in one persistent launch
  * ---------------------------------------------------------------- */
 struct xpuB200Batch {
