@@ -101,17 +101,41 @@ def shard_seed(rank):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 2 ms from a thread (the timed region of a step
+    is tens of milliseconds), else nvidia-smi at its 200 ms floor.  Reads
+    only; changes no GPU setting."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index):
-        self.gpu = gpu_index
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        self.gpu = int(ids[gpu_index]) if gpu_index < len(ids) and ids[gpu_index].isdigit() else gpu_index
         self.proc = None
         self.lines = []
+        self.samples = []
+        self.nvml = None
+        self.stop_ev = threading.Event()
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.nvml = (pynvml, h, reasons)
+            self.smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -121,13 +145,29 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        pynvml, h, reasons = self.nvml
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), reasons(h)))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml:
+            self.stop_ev.set()
+            self.thread.join(timeout=5)
+            sm = [c for c, _ in self.samples]
+            reasons = sorted({nm for _, r in self.samples for nm, bit in self.BITS.items() if r & bit})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "samples": len(sm), "reasons": reasons, "source": "nvml 2 ms"}
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -149,7 +189,7 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "reasons": sorted(reasons), "source": "nvidia-smi 200 ms"}
 
 
 def build_workload(nrows, rank):
@@ -262,6 +302,9 @@ def run_b200(args, rank, world, local):
     # sanity: the batch really did the work
     r2 = batch.exec()
     assert r2["nitems_out"] == meta["nitems_out"], (r2, meta)
+    info = s.info()
+    kernel = ("xbj_kernel (session-specialised, NVRTC sm_100a)" if "jit" in info["kernels"].values()
+              else "xb_exec_kernel (interpreter)")
     batch.close()
     s.close()
 
@@ -330,7 +373,7 @@ def run_b200(args, rank, world, local):
                            "parallelism": f"dp{world} (independent shards, no collective)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
-                             "kernel": "xb_exec_kernel",
+                             "kernel": kernel,
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes + km.nbytes + len(sess),
                         "d2h_bytes_per_step": d2h, "ms_per_step": 1000.0 * e2e_el,
