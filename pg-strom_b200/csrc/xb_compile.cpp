@@ -964,6 +964,66 @@ struct Compiler {
     }
 
     /*
+     * Join quals that read only the inner row of their own depth (and
+     * constants), e.g. "d.flag < 3", give the same answer for every outer
+     * row that meets that inner row.  When they cannot raise an error they
+     * run once per inner row in the build instead, and rows that fail are
+     * left out of the hash index: every probe is spared the qual and the
+     * load of its inputs.  Outer rows that matched only such inner rows
+     * find no match either way, and the depth's row counts are unchanged.
+     */
+    void hoist_inner_quals(uint32_t d)
+    {
+        xb_prog &q = plan->join_quals[d];
+        const xb_inner *in = &plan->inner[d];
+        if (!q.count)
+            return;
+        uint64_t avail = 0;
+        for (uint32_t k = 0; k < in->nloads; k++)
+            avail |= 1ULL << in->load[k].reg;
+        for (uint32_t i = q.start; i < (uint32_t)q.start + q.count; i++) {
+            const xb_insn &x = plan->insns[i];
+            uint64_t reads = 0;
+            bool safe = true;
+            switch (x.op) {
+            case XB_OP_END: case XB_OP_MASK_PUSH: case XB_OP_MASK_POP:
+            case XB_OP_CONST: case XB_OP_BOOL_INIT:
+                break;
+            case XB_OP_MOVE: case XB_OP_NOT: case XB_OP_NULLTEST: case XB_OP_BOOLTEST:
+            case XB_OP_MASK_NARROW:
+                reads = 1ULL << x.a;
+                break;
+            case XB_OP_CMPI:
+                reads = 1ULL << x.a;
+                safe = x.kind == XB_RK_INT || x.kind == XB_RK_FLT;
+                break;
+            case XB_OP_CMP: case XB_OP_DISTINCT:
+                reads = (1ULL << x.a) | (1ULL << x.b);
+                safe = x.kind == XB_RK_INT || x.kind == XB_RK_FLT || x.kind == XB_RK_TEXT;
+                break;
+            case XB_OP_AND_ACC: case XB_OP_OR_ACC:
+                reads = (1ULL << x.a) | (1ULL << x.dst);
+                break;
+            default:
+                safe = false;       /* arithmetic, casts, hashes: may raise */
+                break;
+            }
+            if (!safe || (reads & ~avail))
+                return;
+            switch (x.op) {
+            case XB_OP_END: case XB_OP_MASK_PUSH: case XB_OP_MASK_POP: case XB_OP_MASK_NARROW:
+                break;
+            default:
+                avail |= 1ULL << x.dst;     /* later instructions may read it */
+                break;
+            }
+        }
+        plan->inner[d].build_qual = q;
+        q.count = 0;
+        q.result = -1;
+    }
+
+    /*
      * Hashes of text / numeric values that come straight from an inner
      * relation's column (a group key taken from a dimension table, a join
      * key carried to a deeper depth) depend only on the inner row: the
@@ -1087,6 +1147,7 @@ struct Compiler {
             if (!err.empty()) return false;
             if (!join_program(kj, &plan->join_quals[d], skip))
                 return false;
+            hoist_inner_quals(d);
         }
         if (!groupby())
             return false;

@@ -760,49 +760,67 @@ xb_exec_kernel(XbExecArgs args)
 struct XbBuildArgs {
     const kern_data_store *kds;     /* KDS_FORMAT_HASH inner buffer (device) */
     xb_inner       *in;             /* device copy of the plan's inner descriptor */
+    const xb_plan  *plan;           /* device plan: code of the build-time quals */
     xb_status      *st;
 };
 
+/*
+ * Decode an inner relation into SoA register images and insert its rows
+ * into the hash index.  Warps take 32 rows at a time; when the depth has
+ * join quals over the inner row alone (xb_inner.build_qual), they run here
+ * through the interpreter on a per-warp register file in dynamic shared
+ * memory and only passing rows are indexed.
+ */
 __global__ void __launch_bounds__(XB_BLOCK)
 xb_build_inner(XbBuildArgs args)
 {
     __shared__ XbCol cols[XB_MAX_COLS];
+    extern __shared__ __align__(16) char bregs[];
     const kern_data_store *kds = args.kds;
     xb_inner *in = args.in;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = threadIdx.x >> 5;
     const int ncols = kds->ncols < XB_MAX_COLS ? (int)kds->ncols : XB_MAX_COLS;
     for (int i = threadIdx.x; i < ncols; i += blockDim.x) {
         cols[i].attlen = kds->colmeta[i].attlen;
         cols[i].attalign = kds->colmeta[i].attalign > 0 ? kds->colmeta[i].attalign : 1;
         cols[i].attcacheoff = kds->colmeta[i].attcacheoff;
     }
+    const xb_prog q = in->build_qual;
+    const bool filter = q.count > 0;
+    const uint32_t nregs = args.plan->nregs;
+    XbRegs R = xb_regs_setup(bregs + (size_t)warp * XB_REGS_BYTES(nregs), nregs);
+    if (filter)
+        for (uint32_t r = lane; r < nregs; r += 32)
+            R.nullm[r] = XB_FULL;
     __syncthreads();
     const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
     const uint32_t n = in->nitems;
     const uint32_t words = (n + 31) / 32;
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n;
-         row += gridDim.x * blockDim.x) {
-        uint64_t off = rowindex[row];
-        if (off == 0 || off > kds->length || ((kds->length - off) & 7) != 0) {
-            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
-            continue;
-        }
-        const kern_tupitem *ti = (const kern_tupitem *)((const char *)kds + kds->length - off);
-        uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
-        int natts = ti->t_infomask2 & HEAP_NATTS_MASK;
-        if (natts > ncols) natts = ncols;
-        uint32_t nullbits = 0;
+    const uint32_t stride = gridDim.x * XB_WARPS * 32;
+    for (uint32_t base = (blockIdx.x * XB_WARPS + warp) * 32; base < n; base += stride) {
+        const uint32_t row = base + lane;
+        uint32_t nullbits = 0, hash = 0;
         bool ok = false;
-        const bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
-        if (ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 && pay <= ti->t_len && off >= ti->t_len &&
-            (!hasnull || 15u + (natts + 7) / 8 <= pay))
-            ok = xb_decode_tuple(cols, natts, (ti->t_infomask & HEAP_HASNULL) ? ti->t_bits : nullptr,
-                                 (const uint8_t *)ti + pay, ti->t_len - pay, in->load, in->nloads,
-                                 in->vals + row, in->auxs + row, n, true, &nullbits);
-        if (!ok) {
-            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
-            continue;
+        if (row < n) {
+            const uint64_t off = rowindex[row];
+            if (off != 0 && off <= kds->length && ((kds->length - off) & 7) == 0) {
+                const kern_tupitem *ti = (const kern_tupitem *)((const char *)kds + kds->length - off);
+                const uint32_t pay = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
+                int natts = ti->t_infomask2 & HEAP_NATTS_MASK;
+                if (natts > ncols) natts = ncols;
+                const bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
+                if (ti->t_hoff >= MINIMAL_TUPLE_OFFSET + 15 && pay <= ti->t_len && off >= ti->t_len &&
+                    (!hasnull || 15u + (natts + 7) / 8 <= pay))
+                    ok = xb_decode_tuple(cols, natts, hasnull ? ti->t_bits : nullptr,
+                                         (const uint8_t *)ti + pay, ti->t_len - pay, in->load, in->nloads,
+                                         in->vals + row, in->auxs + row, n, true, &nullbits);
+                hash = ti->hash;
+            }
+            if (!ok)
+                XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
         }
-        if (nullbits) {
+        if (ok && nullbits) {
             for (uint32_t k = 0; k < in->nloads; k++) {
                 if ((nullbits >> k) & 1u)
                     atomicOr(&in->nulls[(size_t)k * words + row / 32], 1u << (row % 32));
@@ -810,7 +828,7 @@ xb_build_inner(XbBuildArgs args)
             atomicOr(&in->hasnull, nullbits);
         }
         /* datum hashes of the columns whose hash later stages read */
-        for (uint32_t k = 0; in->hashed && k < in->nloads; k++) {
+        for (uint32_t k = 0; ok && in->hashed && k < in->nloads; k++) {
             if (!((in->hashed >> k) & 1u) || ((nullbits >> k) & 1u))
                 continue;
             bool bad = false;
@@ -820,10 +838,30 @@ xb_build_inner(XbBuildArgs args)
             if (bad)
                 XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
         }
+        bool pass = ok;
+        if (filter) {
+            /* the row's loaded columns into the register file, then the quals */
+            for (uint32_t k = 0; k < in->nloads; k++) {
+                const uint32_t reg = in->load[k].reg;
+                if (ok) {
+                    RVAL(R, reg) = in->vals[(size_t)k * n + row];
+                    RAUX(R, reg) = in->auxs[(size_t)k * n + row];
+                }
+                xb_set_null(R, reg, !ok || ((nullbits >> k) & 1u));
+            }
+            const uint32_t m = __ballot_sync(XB_FULL, ok);
+            if (m) {
+                if (!xb_vm_run(args.plan->insns + q.start, q.count, R, m, args.st))
+                    pass = false;
+                else
+                    pass = ok && !RISNULL(R, q.result) && RVAL(R, q.result) != 0;
+            }
+        }
+        if (!pass)
+            continue;
         /* index insert at hash & mask (linear probing).  Entries hold
          * (hash << 32 | row + 1), or (key << 32 | row + 1) for a 32-bit
          * fused join key; a NULL fused key can never satisfy the join. */
-        const uint32_t hash = ti->hash;
         uint32_t tag = hash;
         if (in->key32) {
             const int k = in->fast_key;
@@ -1411,12 +1449,17 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         XbBuildArgs ba;
         ba.kds = (const kern_data_store *)(s->d_kmrels + kmrels->chunks[d - 1].kds_offset);
         ba.in = &s->d_plan->inner[d];
+        ba.plan = s->d_plan;
         ba.st = s->d_status;
         uint32_t n = plan->inner[d].nitems;
         int grid = (int)((n + XB_BLOCK - 1) / XB_BLOCK);
         if (grid < 1) grid = 1;
         if (grid > dev->nsm * 8) grid = dev->nsm * 8;
-        xb_build_inner<<<grid, XB_BLOCK, 0, st>>>(ba);
+        const size_t bsmem = plan->inner[d].build_qual.count ? (size_t)XB_WARPS * XB_REGS_BYTES(plan->nregs) : 0;
+        if (bsmem > 48 * 1024 &&
+            cudaFuncSetAttribute(xb_build_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem) != cudaSuccess)
+            FAIL(ERRCODE_DEVICE_FATAL, "inner build needs %zu bytes of shared memory", bsmem);
+        xb_build_inner<<<grid, XB_BLOCK, bsmem, st>>>(ba);
     }
     /* canonical text pointers for hashed text columns: equal strings of one
      * inner column share one address, so group keys taken from them compare

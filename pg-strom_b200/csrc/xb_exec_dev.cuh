@@ -13,7 +13,9 @@
 
 #define XB_BLOCK        256
 #define XB_WARPS        (XB_BLOCK / 32)
-#define XB_CLAIM        4           /* heap pages claimed per warp at a time */
+#define XB_CLAIM        1           /* heap pages claimed per warp at a time: with one page
+                                     * prefetched ahead, resident warps keep ~16 KB each in
+                                     * flight, well inside L2 (4-page claims overflowed it) */
 #define XB_ROWS_UNIT    1024        /* rows per unit for ARROW / ROW chunks */
 #define XB_MIN_BLOCKS   2           /* resident CTAs per SM the kernel is built for */
 #define XB_PROBE_LIMIT  4096        /* max probes in the global group table */

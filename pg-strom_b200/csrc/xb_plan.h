@@ -156,6 +156,8 @@ typedef struct xb_inner {
     uint8_t     fast_hk;        /* hash kind of the outer key */
     uint32_t    key32;          /* index entries hold (key32 << 32 | row + 1):
                                  * the fused key is int2 / int4 / date */
+    xb_prog     build_qual;     /* join quals over this inner row alone, run once per
+                                 * inner row by the build; failing rows stay out of index */
     uint32_t    hashed;         /* bit k: hash of load k precomputed into hashes[] */
     uint32_t   *hashes;         /* [nloads][nitems] datum hashes (hashed loads) */
     xb_load     load[XB_MAX_LOADS];
