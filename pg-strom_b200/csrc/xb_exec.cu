@@ -879,6 +879,26 @@ xb_build_inner(XbBuildArgs args)
                 atomicExch(&in->unique_hash, 0u);   /* a second row with this tag */
             pos = (pos + 1) & in->cap_mask;
         }
+        if (in->key32) {
+            atomicMin(&in->dkey_min, (int32_t)tag);
+            atomicMax(&in->dkey_max, (int32_t)tag);
+            atomicAdd(&in->nindexed, 1u);
+        }
+    }
+}
+
+/* fill the direct-address table of a unique 32-bit key from the index */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_build_direct(xb_inner *in)
+{
+    const uint64_t cap = (uint64_t)in->cap_mask + 1;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t ent = in->index[i];
+        if (ent == 0)
+            continue;
+        const int32_t key = (int32_t)(uint32_t)(ent >> 32);
+        in->dtab[(uint32_t)((int64_t)key - in->dkey_min)] = (uint32_t)ent;     /* row + 1 */
     }
 }
 
@@ -1407,6 +1427,12 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             DALLOC((size_t)nl * n * 4, &in->auxs);
             DALLOC((size_t)nl * words * 4, &in->nulls);
             in->hashes = nullptr;
+            in->dkey_min = INT32_MAX;
+            in->dkey_max = INT32_MIN;
+            in->nindexed = 0;
+            in->direct = 0;
+            in->drange = 0;
+            in->dtab = nullptr;
             if (in->hashed)
                 DALLOC((size_t)nl * n * 4, &in->hashes);
             cudaMemsetAsync(in->index, 0, cap * 8, st);
@@ -1488,6 +1514,27 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         FAIL(s->h_status->errcode, "inner relation build: %s", xb_msg_text(s->h_status->msg_id));
     /* refresh the host copy of the inner descriptors (unique_hash) */
     cudaMemcpy(s->h_plan, s->d_plan, sizeof(xb_plan), cudaMemcpyDeviceToHost);
+    /* direct-address tables for unique, dense 32-bit join keys (used by the
+     * session-specialised kernels; the interpreter keeps probing the index) */
+    for (uint32_t d = 1; d <= plan->nrels; d++) {
+        xb_inner *in = &s->h_plan->inner[d];
+        if (!in->key32 || !in->unique_hash || in->nindexed == 0 || in->dkey_max < in->dkey_min)
+            continue;
+        const uint64_t range = (uint64_t)((int64_t)in->dkey_max - in->dkey_min) + 1;
+        const uint64_t limit = (uint64_t)in->nitems * 4 > 4096 ? (uint64_t)in->nitems * 4 : 4096;
+        if (range > limit || range > (1ULL << 28))
+            continue;
+        DALLOC(range * 4, &in->dtab);
+        cudaMemsetAsync(in->dtab, 0, range * 4, st);
+        in->drange = (uint32_t)range;
+        in->direct = 1;
+        cudaMemcpyAsync(&s->d_plan->inner[d], in, sizeof(xb_inner), cudaMemcpyHostToDevice, st);
+        int grid = (int)((in->cap_mask + 1ULL + XB_BLOCK - 1) / XB_BLOCK);
+        if (grid > dev->nsm * 8) grid = dev->nsm * 8;
+        xb_build_direct<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d]);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));
 
     /* launch geometry */
     s->warp_bytes = (uint32_t)(XB_WARP_HEAD + sizeof(XbCursor) * plan->nrels + XB_REGS_BYTES(plan->nregs));

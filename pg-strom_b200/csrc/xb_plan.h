@@ -158,6 +158,14 @@ typedef struct xb_inner {
                                  * the fused key is int2 / int4 / date */
     xb_prog     build_qual;     /* join quals over this inner row alone, run once per
                                  * inner row by the build; failing rows stay out of index */
+    /* direct addressing: a unique, dense 32-bit fused key maps straight to
+     * its row through dtab[key - dkey_min] (row + 1, 0 = none) */
+    int32_t     dkey_min;       /* smallest / largest indexed key (build) */
+    int32_t     dkey_max;
+    uint32_t    nindexed;       /* rows inserted into the index (build) */
+    uint32_t    direct;         /* 1: dtab is valid */
+    uint32_t    drange;         /* dkey_max - dkey_min + 1 */
+    uint32_t   *dtab;
     uint32_t    hashed;         /* bit k: hash of load k precomputed into hashes[] */
     uint32_t   *hashes;         /* [nloads][nitems] datum hashes (hashed loads) */
     xb_load     load[XB_MAX_LOADS];

@@ -105,16 +105,25 @@ def zipf_bounded(r, n, s, size):
     return (np.searchsorted(cdf, u, side="right") + 1).astype(np.int32)
 
 
-def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3):
+def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3,
+                 key_stride=1, dim1_copies=1, miss_frac=0.0):
+    """Two-way hash join + group-by.  Defaults give the headline workload:
+    dense unique dimension keys 1..n, every fact row matching.  Variants for
+    the join paths: key_stride spreads the keys (k * stride; sparse keys
+    take the hashed probe instead of direct addressing), dim1_copies > 1
+    repeats every dim1 key with its own region (several matches per probe),
+    miss_frac makes that share of fact rows reference no dim1 row."""
     r1 = rng_for(seed_config, 1)
     r2 = rng_for(seed_config, 2)
     rf = rng_for(seed_config, 0)
     # dimensions
-    pk1 = np.arange(1, ndim1 + 1, dtype=np.int32)
-    reg_code = r1.integers(0, len(REGIONS), ndim1)
+    pk1_one = np.arange(1, ndim1 + 1, dtype=np.int64) * key_stride
+    pk1 = np.tile(pk1_one, dim1_copies).astype(np.int32)
+    reg_code = r1.integers(0, len(REGIONS), ndim1 * dim1_copies)
     dim1 = Table("dim1", [Column("pk", "int4", values=pk1),
-                          Column("region", "text", values=encode_text_from_dict(reg_code, REGIONS))], ndim1)
-    pk2 = np.arange(1, ndim2 + 1, dtype=np.int32)
+                          Column("region", "text", values=encode_text_from_dict(reg_code, REGIONS))],
+                 ndim1 * dim1_copies)
+    pk2 = (np.arange(1, ndim2 + 1, dtype=np.int64) * key_stride).astype(np.int32)
     flag = r2.integers(0, 5, ndim2, dtype=np.int16)
     dim2 = Table("dim2", [Column("pk", "int4", values=pk2), Column("flag", "int2", values=flag)], ndim2)
     # fact
@@ -122,6 +131,15 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
     fk2 = zipf_bounded(rf, ndim2, 1.1, nfact)
     qty = rf.integers(1, 51, nfact, dtype=np.int32)
     price = rf.integers(100, 1_000_001, nfact, dtype=np.int64)
+    idx1 = fk1.astype(np.int64) - 1
+    idx2 = fk2.astype(np.int64) - 1
+    miss = np.zeros(nfact, dtype=bool)
+    if miss_frac > 0:
+        miss = rf.random(nfact) < miss_frac
+        fk1 = np.where(miss, fk1 + ndim1, fk1).astype(np.int32)     # beyond every dim1 key
+    if key_stride != 1:
+        fk1 = (fk1.astype(np.int64) * key_stride).astype(np.int32)
+        fk2 = (fk2.astype(np.int64) * key_stride).astype(np.int32)
     fact = Table("fact", [Column("fk1", "int4", values=fk1), Column("fk2", "int4", values=fk2),
                           Column("qty", "int4", values=qty), Column("price", "int8", values=price)], nfact)
     kmrels = kern_multirels([dim1.hash_kds(host_join_hash_int4(pk1)),
@@ -139,19 +157,25 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
         aggs=[Agg("PSUM_INT64", Func("int48mul", [f_qty, f_price], "int8")),
               Agg("NROWS_ANY")],
         ngroups_estimate=25.0)
-    # expected
-    region_row = reg_code[fk1 - 1]
-    m = flag[fk2 - 1] < flag_limit
-    expect = {}
+    # expected: every (fact row, dim1 copy) pair that passes both joins
+    m = (flag[idx2] < flag_limit) & ~miss
     amount = qty.astype(np.int64) * price
+    cnt = np.zeros(len(REGIONS), dtype=np.int64)
+    tot = [0] * len(REGIONS)
+    for c in range(dim1_copies):
+        region_row = reg_code[c * ndim1 + idx1]
+        for k in range(len(REGIONS)):
+            sel = m & (region_row == k)
+            cnt[k] += int(sel.sum())
+            tot[k] += int(amount[sel].sum())
+    expect = {}
     for k in range(len(REGIONS)):
-        sel = m & (region_row == k)
-        n = int(sel.sum())
-        if n == 0:
-            continue
-        expect[(REGIONS[k].encode(),)] = {"sum_amount": (n, int(amount[sel].sum())), "nrows": n}
-    meta = {"nitems_raw": nfact, "nitems_in": nfact, "nitems_out": int(m.sum()),
-            "depth_out": [nfact, int(m.sum())], "agg_names": ["sum_amount", "nrows"], "nkeys": 1}
+        if cnt[k]:
+            expect[(REGIONS[k].encode(),)] = {"sum_amount": (int(cnt[k]), tot[k]), "nrows": int(cnt[k])}
+    hit1 = int((~miss).sum()) * dim1_copies
+    out = int(m.sum()) * dim1_copies
+    meta = {"nitems_raw": nfact, "nitems_in": nfact, "nitems_out": out,
+            "depth_out": [hit1, out], "agg_names": ["sum_amount", "nrows"], "nkeys": 1}
     return fact, session, kmrels, expect, meta
 
 

@@ -108,6 +108,23 @@ def test_join_groupby_parity(device, kernel, nfact, nd1, nd2, ppc):
     assert F.compare_groups(got, F.decode_kds_final(ofinal, sess)) == []
 
 
+@pytest.mark.parametrize("stride,copies,miss", [(7, 1, 0.0), (1, 3, 0.2), (13, 2, 0.1)])
+def test_join_probe_variants_parity(device, kernel, stride, copies, miss):
+    """Sparse keys (hashed probe instead of direct addressing), repeated
+    inner keys (several matches per probe) and fact rows without a match."""
+    fact, sess, km, expect, meta = C.join_groupby(nfact=200_000, ndim1=5_000, ndim2=700, key_stride=stride,
+                                                  dim1_copies=copies, miss_frac=miss)
+    chunks = fact.block_chunks(pages_per_chunk=300)
+    final, st, res = run_gpu(device, sess, chunks, km, nrels=2, kernel=kernel)
+    assert st["nitems_out"] == meta["nitems_out"]
+    assert st["depth_out"] == meta["depth_out"]
+    got = F.decode_kds_final(final, sess)
+    truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+    assert F.compare_groups(got, truth) == []
+    ofinal, _ = run_oracle(sess, chunks, km)
+    assert F.compare_groups(got, F.decode_kds_final(ofinal, sess)) == []
+
+
 @pytest.mark.parametrize("nrows,nkeys,rpc", [(300_000, 20_000, 100_000), (2_000_000, 1_000_000, 700_000)])
 def test_arrow_groupby_parity(device, kernel, nrows, nkeys, rpc):
     chunks, sess, expect, meta = C.arrow_groupby(nrows=nrows, nkeys=nkeys, rows_per_chunk=rpc)
