@@ -887,6 +887,37 @@ xb_build_inner(XbBuildArgs args)
     }
 }
 
+/* pack the live columns of every indexed row into its direct record */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_build_drec(xb_inner *in, const xb_plan *plan)
+{
+    const uint64_t cap = (uint64_t)in->cap_mask + 1;
+    const uint32_t n = in->nitems;
+    const uint32_t words = (n + 31) / 32;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t ent = in->index[i];
+        if (ent == 0)
+            continue;
+        const int32_t key = (int32_t)(uint32_t)(ent >> 32);
+        const uint32_t row = (uint32_t)ent - 1;
+        char *rec = in->dpay + (size_t)(uint32_t)((int64_t)key - in->dkey_min) * in->drec_size;
+        uint32_t head = 0x80000000U;
+        for (uint32_t k = 0; k < in->nloads; k++) {
+            if (!((in->live >> k) & 1u))
+                continue;
+            int ov, oa, oh;
+            xb_drec_layout(in, plan->rk, (int)k, &ov, &oa, &oh);
+            if ((in->nulls[(size_t)k * words + row / 32] >> (row % 32)) & 1u)
+                head |= 1u << k;
+            *(uint64_t *)(rec + ov) = in->vals[(size_t)k * n + row];
+            if (oa >= 0) *(uint32_t *)(rec + oa) = in->auxs[(size_t)k * n + row];
+            if (oh >= 0) *(uint32_t *)(rec + oh) = in->hashes[(size_t)k * n + row];
+        }
+        *(uint32_t *)rec = head;
+    }
+}
+
 /* fill the direct-address table of a unique 32-bit key from the index */
 __global__ void __launch_bounds__(XB_BLOCK)
 xb_build_direct(xb_inner *in)
@@ -1433,6 +1464,8 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             in->direct = 0;
             in->drange = 0;
             in->dtab = nullptr;
+            in->drec_size = 0;
+            in->dpay = nullptr;
             if (in->hashed)
                 DALLOC((size_t)nl * n * 4, &in->hashes);
             cudaMemsetAsync(in->index, 0, cap * 8, st);
@@ -1528,10 +1561,19 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         cudaMemsetAsync(in->dtab, 0, range * 4, st);
         in->drange = (uint32_t)range;
         in->direct = 1;
+        /* live columns packed per key when the records stay small */
+        const uint32_t rs = xb_drec_layout(in, s->h_plan->rk, -1, nullptr, nullptr, nullptr);
+        if (in->live && rs <= 64) {
+            DALLOC(range * rs, &in->dpay);
+            cudaMemsetAsync(in->dpay, 0, range * rs, st);
+            in->drec_size = rs;
+        }
         cudaMemcpyAsync(&s->d_plan->inner[d], in, sizeof(xb_inner), cudaMemcpyHostToDevice, st);
         int grid = (int)((in->cap_mask + 1ULL + XB_BLOCK - 1) / XB_BLOCK);
         if (grid > dev->nsm * 8) grid = dev->nsm * 8;
         xb_build_direct<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d]);
+        if (in->dpay)
+            xb_build_drec<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d], s->d_plan);
     }
     if (cudaStreamSynchronize(st) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));

@@ -166,6 +166,11 @@ typedef struct xb_inner {
     uint32_t    direct;         /* 1: dtab is valid */
     uint32_t    drange;         /* dkey_max - dkey_min + 1 */
     uint32_t   *dtab;
+    /* direct records: the live columns of the row of key k packed at
+     * dpay + (k - dkey_min) * drec_size (layout: xb_drec_layout) */
+    uint32_t    drec_size;
+    uint32_t    __pad_d;
+    char       *dpay;
     uint32_t    hashed;         /* bit k: hash of load k precomputed into hashes[] */
     uint32_t   *hashes;         /* [nloads][nitems] datum hashes (hashed loads) */
     xb_load     load[XB_MAX_LOADS];
@@ -236,6 +241,48 @@ typedef struct xb_plan {
 } xb_plan;
 
 #define XB_PLAN_MAGIC   0x78623230U     /* 'xb20' */
+
+#ifdef __CUDACC__
+#define XB_PLAN_HD __host__ __device__ inline
+#else
+#define XB_PLAN_HD static inline
+#endif
+
+/*
+ * Layout of a direct record: a u32 header (bit 31: a row holds this key,
+ * bit k: load k is NULL), then one u32 per live text length and per live
+ * precomputed hash, then the u64 value of every live load (8-aligned);
+ * the size is a multiple of 16.  Offsets of load k are -1 where absent.
+ * Returns the record size.
+ */
+XB_PLAN_HD uint32_t
+xb_drec_layout(const xb_inner *in, const uint8_t *rk, int k, int *off_val, int *off_aux, int *off_hash)
+{
+    uint32_t off = 4;
+    if (off_val) *off_val = -1;
+    if (off_aux) *off_aux = -1;
+    if (off_hash) *off_hash = -1;
+    for (uint32_t j = 0; j < in->nloads; j++) {
+        if (!((in->live >> j) & 1u))
+            continue;
+        if (rk[in->load[j].reg] == XB_RK_TEXT) {
+            if ((int)j == k && off_aux) *off_aux = (int)off;
+            off += 4;
+        }
+        if ((in->hashed >> j) & 1u) {
+            if ((int)j == k && off_hash) *off_hash = (int)off;
+            off += 4;
+        }
+    }
+    off = (off + 7) & ~7u;
+    for (uint32_t j = 0; j < in->nloads; j++) {
+        if (!((in->live >> j) & 1u))
+            continue;
+        if ((int)j == k && off_val) *off_val = (int)off;
+        off += 8;
+    }
+    return (off + 15) & ~15u;
+}
 
 /* group entry header (global and shared-memory tables) */
 #define XB_GSTATE_EMPTY 0u
