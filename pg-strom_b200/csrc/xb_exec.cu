@@ -608,21 +608,7 @@ xb_exec_kernel(XbExecArgs args)
     const uint32_t nrels = plan->nrels;
 
     XbSrc src;
-    src.unit = 0;
-    src.claim_end = 0;
-    src.next_claim = 0;
-    src.kds = nullptr;
-    src.page = nullptr;
-    src.row0 = 0;
-    src.item = 0;
-    src.nitems = 0;
-    if (args.format == KDS_FORMAT_BLOCK) {
-        unsigned long long c0 = 0;
-        if (lane == 0)
-            c0 = atomicAdd((unsigned long long *)&st->unit_cursor, (unsigned long long)XB_CLAIM);
-        src.next_claim = __shfl_sync(XB_FULL, c0, 0);
-        xb_prefetch_claim(args, src.next_claim, lane);
-    }
+    xb_src_start(args, src, lane);
 
     uint32_t stage = XB_ST_FETCH, d = 0, mask = 0;
     for (;;) {
@@ -1592,7 +1578,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     if (per_sm < 1)
         FAIL(ERRCODE_DEVICE_FATAL, "executor kernel does not fit on an SM (%zu bytes smem)", s->smem_bytes);
     s->grid = per_sm * dev->nsm;
-    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + (size_t)s->sm_cap * plan->gent_size;
+    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + sizeof(XbSrc) * XB_WARPS + (size_t)s->sm_cap * plan->gent_size;
     {
         const char *env = getenv("XPU_B200_JIT");
         s->jit_enabled = !(env && env[0] == '0');

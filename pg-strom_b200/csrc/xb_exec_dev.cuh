@@ -13,9 +13,9 @@
 
 #define XB_BLOCK        256
 #define XB_WARPS        (XB_BLOCK / 32)
-#define XB_CLAIM        1           /* heap pages claimed per warp at a time: with one page
-                                     * prefetched ahead, resident warps keep ~16 KB each in
-                                     * flight, well inside L2 (4-page claims overflowed it) */
+#define XB_CLAIM        8           /* heap pages claimed per warp with one atomic; only the
+                                     * page after the current one is prefetched into L2, so
+                                     * resident warps keep ~16 KB each in flight */
 #define XB_ROWS_UNIT    1024        /* rows per unit for ARROW / ROW chunks */
 #define XB_MIN_BLOCKS   2           /* resident CTAs per SM the kernel is built for */
 #define XB_PROBE_LIMIT  4096        /* max probes in the global group table */
@@ -392,13 +392,19 @@ __device__ __forceinline__ int xb_ld_width(int ld)
 struct XbSrc {
     uint64_t unit;                  /* current unit (global index) */
     uint64_t claim_end;             /* BLOCK: end of the current claim */
-    uint64_t next_claim;            /* BLOCK: first unit of the claim taken ahead */
+    unsigned long long nx_l0;       /* BLOCK, lane 0: first unit of the claim taken ahead */
+    unsigned long long sz_l0;       /* BLOCK, lane 0: its size */
+    unsigned long long last_dyn;    /* BLOCK, lane 0: start of the last dynamic claim */
+    uint64_t static_base;           /* BLOCK: units below are handed out statically */
+    uint64_t task_base;             /* units [task_base, task_end) belong to kds */
+    uint64_t task_end;
     const kern_data_store *kds;
+    const uint8_t *blocks;          /* BLOCK: first heap page of kds */
     const uint8_t *page;            /* BLOCK: current heap page */
     uint32_t row0;                  /* ARROW / ROW: first row of the unit */
     uint32_t item;                  /* next item of the unit */
     uint32_t nitems;                /* items of the unit */
-};
+} __attribute__((aligned(16)));
 
 /* chunk owning global unit 'unit' (tasks are sorted by unit_base) */
 __device__ __forceinline__ uint32_t
@@ -412,41 +418,118 @@ xb_find_task(const xb_task *tasks, uint32_t ntasks, uint64_t unit)
     return lo;
 }
 
-/* pull a claim's heap pages into L2 (TMA bulk prefetch) */
+/* make the chunk owning 'unit' the source's current chunk */
 __device__ __forceinline__ void
-xb_prefetch_claim(const XbExecArgs &args, uint64_t claim, uint32_t lane)
+xb_src_task(const XbExecArgs &args, XbSrc &s, uint64_t unit)
 {
-    if (lane < XB_CLAIM && claim + lane < args.nunits) {
-        const uint64_t u = claim + lane;
-        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
-        const char *p = (const char *)t.kds + t.kds->block_offset + (u - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
-        if ((((uintptr_t)p) & 15) == 0)
-            xb_prefetch_l2(p, PGSTROM_BLCKSZ);
+    const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, unit)];
+    s.kds = t.kds;
+    s.task_base = t.unit_base;
+    s.task_end = t.unit_base + t.nunits;
+    s.blocks = (args.format == KDS_FORMAT_BLOCK) ? (const uint8_t *)t.kds + t.kds->block_offset : nullptr;
+}
+
+/* pull heap page 'unit' into L2 (TMA bulk prefetch); lane 0 issues it */
+__device__ __forceinline__ void
+xb_prefetch_page(const XbExecArgs &args, const XbSrc &s, uint64_t unit, uint32_t lane)
+{
+    if (lane != 0 || unit >= args.nunits)
+        return;
+    const char *p;
+    if (unit >= s.task_base && unit < s.task_end) {
+        p = (const char *)s.blocks + (unit - s.task_base) * (size_t)PGSTROM_BLCKSZ;
+    } else {
+        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, unit)];
+        p = (const char *)t.kds + t.kds->block_offset + (unit - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
     }
+    if ((((uintptr_t)p) & 15) == 0)
+        xb_prefetch_l2(p, PGSTROM_BLCKSZ);
+}
+
+/*
+ * Set up a warp's first claim.  Heap pages: each warp first takes a static
+ * share of 3/5 of the launch's pages (contiguous, no atomic), then claims
+ * the rest dynamically; Arrow / row units are all claimed dynamically.
+ */
+__device__ __forceinline__ void
+xb_src_start(const XbExecArgs &args, XbSrc &s, uint32_t lane)
+{
+    s.unit = 0;
+    s.claim_end = 0;
+    s.static_base = 0;
+    s.task_base = 0;
+    s.task_end = 0;
+    s.kds = nullptr;
+    s.blocks = nullptr;
+    s.page = nullptr;
+    s.row0 = 0;
+    s.item = 0;
+    s.nitems = 0;
+    if (args.format != KDS_FORMAT_BLOCK) {
+        if (lane == 0) {
+            s.nx_l0 = 0;
+            s.sz_l0 = 1;
+            s.last_dyn = 0;
+        }
+        __syncwarp();
+        return;
+    }
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    const uint64_t wid = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const uint64_t share = (args.nunits * 3 / 5) / warps;
+    s.static_base = share * warps;
+    /* the lane-0 fields are written by lane 0 only (the state may live in
+     * shared memory, read back by every lane) */
+    if (lane == 0) {
+        s.last_dyn = s.static_base;
+        if (share > 0) {
+            s.nx_l0 = wid * share;
+            s.sz_l0 = share;
+        } else {
+            s.nx_l0 = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
+            s.sz_l0 = 1;
+            s.last_dyn = s.nx_l0;
+        }
+    }
+    __syncwarp();
+    xb_prefetch_page(args, s, __shfl_sync(XB_FULL, s.nx_l0, 0), lane);
 }
 
 /* move to the next unit; returns 0 = no more work, 1 = ok, 2 = corrupt page */
 __device__ __forceinline__ int
 xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane)
 {
-    if (*(volatile uint32_t *)&args.st->errcode != 0)
-        return 0;
     if (args.format == KDS_FORMAT_BLOCK) {
         s.unit++;
+        if ((s.unit & 7) == 0 && *(volatile uint32_t *)&args.st->errcode != 0)
+            return 0;                   /* another warp failed: stop early */
         if (s.unit >= s.claim_end) {
-            s.unit = s.next_claim;
-            if (s.unit >= args.nunits)
+            /* the claim taken ahead (its atomic has long returned to lane 0) */
+            s.unit = __shfl_sync(XB_FULL, s.nx_l0, 0);
+            const uint32_t size = (uint32_t)__shfl_sync(XB_FULL, s.sz_l0, 0);
+            if (s.unit >= args.nunits || *(volatile uint32_t *)&args.st->errcode != 0)
                 return 0;
-            s.claim_end = min(s.unit + (uint64_t)XB_CLAIM, args.nunits);
-            unsigned long long nx = 0;
-            if (lane == 0)
-                nx = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)XB_CLAIM);
-            s.next_claim = __shfl_sync(XB_FULL, nx, 0);
-            xb_prefetch_claim(args, s.next_claim, lane);
+            s.claim_end = min(s.unit + size, args.nunits);
+            /* guided self-scheduling of the dynamic part: large claims while
+             * plenty of it is left, single pages near the end so no warp
+             * is left with a long tail; lane 0 keeps the result until the
+             * claim starts */
+            if (lane == 0) {
+                const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
+                const unsigned long long left = s.last_dyn < args.nunits ? args.nunits - s.last_dyn : 0;
+                unsigned long long sz = left / (4 * warps);
+                sz = sz < 1 ? 1 : (sz > XB_CLAIM ? XB_CLAIM : sz);
+                s.sz_l0 = sz;
+                s.nx_l0 = s.static_base + atomicAdd((unsigned long long *)&args.st->unit_cursor, sz);
+                s.last_dyn = s.nx_l0;
+            }
         }
-        const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, s.unit)];
-        s.kds = t.kds;
-        s.page = (const uint8_t *)t.kds + t.kds->block_offset + (s.unit - t.unit_base) * (size_t)PGSTROM_BLCKSZ;
+        if (s.unit < s.task_base || s.unit >= s.task_end)
+            xb_src_task(args, s, s.unit);
+        s.page = s.blocks + (s.unit - s.task_base) * (size_t)PGSTROM_BLCKSZ;
+        /* the page after this one streams into L2 while this one is decoded */
+        const uint64_t nu = s.unit + 1 < s.claim_end ? s.unit + 1 : __shfl_sync(XB_FULL, s.nx_l0, 0);
+        xb_prefetch_page(args, s, nu, lane);
         const uint32_t pd_lower = (uint32_t)xb_fetch_le(s.page + 12, 2);
         s.item = 0;
         s.nitems = 0;
@@ -456,17 +539,19 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane)
             return 2;
         return 1;
     }
+    if (*(volatile uint32_t *)&args.st->errcode != 0)
+        return 0;
     unsigned long long u = 0;
     if (lane == 0)
         u = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
     u = __shfl_sync(XB_FULL, u, 0);
     if (u >= args.nunits)
         return 0;
-    const xb_task &t = args.tasks[xb_find_task(args.tasks, args.ntasks, u)];
+    if (u < s.task_base || u >= s.task_end)
+        xb_src_task(args, s, u);
     s.unit = u;
-    s.kds = t.kds;
-    s.row0 = (uint32_t)(u - t.unit_base) * XB_ROWS_UNIT;
-    const uint32_t left = t.kds->nitems > s.row0 ? t.kds->nitems - s.row0 : 0;
+    s.row0 = (uint32_t)(u - s.task_base) * XB_ROWS_UNIT;
+    const uint32_t left = s.kds->nitems > s.row0 ? s.kds->nitems - s.row0 : 0;
     s.nitems = left < XB_ROWS_UNIT ? left : XB_ROWS_UNIT;
     s.item = 0;
     return 1;

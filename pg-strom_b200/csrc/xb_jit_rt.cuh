@@ -33,15 +33,39 @@ struct XbjEnv {
     uint32_t        lane;
 };
 
+/* per-thread counters, 32-bit to spare registers; flushed into the launch
+ * totals whenever one passes 2^31 (checked once per batch) */
 struct XbjCnt {
-    unsigned long long raw, in, out;
-    unsigned long long depth[XB_MAX_DEPTH + 1];
+    uint32_t raw, in, out;
+    uint32_t depth[XB_MAX_DEPTH + 1];
 };
 
-/* generated per session */
+__device__ __forceinline__ void xbj_flush_cnt(XbjCnt &C, xb_status *st)
+{
+    atomicAdd((unsigned long long *)&st->nitems_raw, (unsigned long long)C.raw);
+    atomicAdd((unsigned long long *)&st->nitems_in, (unsigned long long)C.in);
+    atomicAdd((unsigned long long *)&st->nitems_out, (unsigned long long)C.out);
+    C.raw = C.in = C.out = 0;
+#pragma unroll
+    for (int d = 1; d <= XBJ_NRELS; d++) {
+        atomicAdd((unsigned long long *)&st->nitems_depth[d], (unsigned long long)C.depth[d]);
+        C.depth[d] = 0;
+    }
+}
+
+/* generated per session: decode item idx of the current unit (page: heap
+ * page of a BLOCK chunk; kds / row0: chunk and first row of an ARROW or ROW
+ * unit; lp: the heap item's line pointer) */
 __device__ __forceinline__ bool
-xbj_decode(XbjRegs &R, const XbExecArgs &args, const XbSrc &s, const XbSrcMeta *meta,
-           uint32_t idx, bool &exists, xb_status *st);
+xbj_decode(XbjRegs &R, const XbExecArgs &args, const uint8_t *page, const kern_data_store *kds,
+           uint32_t row0, const XbSrcMeta *meta, uint32_t idx, uint32_t lp, bool &exists, xb_status *st);
+
+/* line pointer i of a heap page of nitems items (0 = LP_UNUSED past the end) */
+__device__ __forceinline__ uint32_t xbj_itemid(const uint8_t *page, uint32_t nitems, uint32_t i)
+{
+    return i < nitems ? (uint32_t)xb_fetch_le(page + SizeOfPageHeaderData + 4 * i, 4) : 0u;
+}
+
 __device__ __forceinline__ void
 xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
 
@@ -59,7 +83,10 @@ xbj_kernel(XbExecArgs args)
     extern __shared__ __align__(16) char smem[];
     const uint32_t lane = threadIdx.x & 31;
     XbSrcMeta *meta = (XbSrcMeta *)smem;
-    char *sm_entries = smem + ((sizeof(XbSrcMeta) + 15) & ~(size_t)15);
+    /* warp-uniform work-distribution state lives in shared memory, not in
+     * registers (read once per unit) */
+    XbSrc *wsrc = (XbSrc *)(smem + ((sizeof(XbSrcMeta) + 15) & ~(size_t)15));
+    char *sm_entries = (char *)(wsrc + XB_WARPS);
     const size_t sm_bytes = (size_t)args.sm_cap * XBJ_GENT_SIZE;
 
     xb_setup_meta(args, meta);
@@ -82,26 +109,15 @@ xbj_kernel(XbExecArgs args)
     for (int d = 0; d <= XB_MAX_DEPTH; d++)
         C.depth[d] = 0;
 
-    XbSrc src;
-    src.unit = 0;
-    src.claim_end = 0;
-    src.next_claim = 0;
-    src.kds = nullptr;
-    src.page = nullptr;
-    src.row0 = 0;
-    src.item = 0;
-    src.nitems = 0;
-    if (args.format == KDS_FORMAT_BLOCK) {
-        unsigned long long c0 = 0;
-        if (lane == 0)
-            c0 = atomicAdd((unsigned long long *)&args.st->unit_cursor, (unsigned long long)XB_CLAIM);
-        src.next_claim = __shfl_sync(XB_FULL, c0, 0);
-        xb_prefetch_claim(args, src.next_claim, lane);
-    }
+    XbSrc &src = wsrc[threadIdx.x >> 5];
+    xb_src_start(args, src, lane);
+    const uint8_t *page = nullptr;
+    const kern_data_store *kds = nullptr;
+    uint32_t row0 = 0, item = 0, nitems = 0;
 
     for (;;) {
         bool done = false;
-        while (src.item >= src.nitems) {
+        while (item >= nitems) {
             const int rc = xb_next_unit(args, src, lane);
             if (rc == 0) { done = true; break; }
             if (rc == 2) {
@@ -109,16 +125,22 @@ xbj_kernel(XbExecArgs args)
                 done = true;
                 break;
             }
+            page = src.page;
+            kds = src.kds;
+            row0 = src.row0;
+            item = 0;
+            nitems = src.nitems;
         }
         if (done)
             break;
-        const uint32_t idx = src.item + lane;
-        src.item += 32;
+        const uint32_t idx = item + lane;
+        const uint32_t lp = args.format == KDS_FORMAT_BLOCK ? xbj_itemid(page, nitems, idx) : 0u;
+        item += 32;
         bool failed = false;
-        if (idx < src.nitems) {
+        if (idx < nitems) {
             XbjRegs R;
             bool exists = false;
-            const bool ok = xbj_decode(R, args, src, meta, idx, exists, args.st);
+            const bool ok = xbj_decode(R, args, page, kds, row0, meta, idx, lp, exists, args.st);
             if (exists)
                 C.raw++;
             if (exists && !ok)
@@ -126,6 +148,12 @@ xbj_kernel(XbExecArgs args)
             else if (ok)
                 xbj_pipeline(R, E, C, failed);
         }
+        uint32_t big = C.out | C.in | C.raw;
+#pragma unroll
+        for (int d = 1; d <= XBJ_NRELS; d++)
+            big |= C.depth[d];
+        if (big & 0x80000000u)
+            xbj_flush_cnt(C, args.st);
         if (__any_sync(XB_FULL, failed))
             break;
     }
@@ -135,6 +163,7 @@ xbj_kernel(XbExecArgs args)
         const unsigned long long raw = xbj_warp_sum(C.raw);
         const unsigned long long in = xbj_warp_sum(C.in);
         const unsigned long long out = xbj_warp_sum(C.out);
+        /* (64-bit sums: 32 lanes' 32-bit counts may exceed 2^32) */
         if (lane == 0) {
             atomicAdd((unsigned long long *)&args.st->nitems_raw, raw);
             atomicAdd((unsigned long long *)&args.st->nitems_in, in);

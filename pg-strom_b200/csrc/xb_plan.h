@@ -327,11 +327,15 @@ typedef struct xb_status {
     int32_t     lineno;
     uint32_t    msg_id;
     uint32_t    __pad;
-    uint64_t    unit_cursor;    /* work distribution counter */
     uint64_t    nitems_raw;
     uint64_t    nitems_in;
     uint64_t    nitems_out;
     uint64_t    nitems_depth[XB_MAX_DEPTH + 1];
+    uint64_t    __pad1[4];
+    /* work distribution counter, alone in its 128-byte line: every warp's
+     * claim lands here, away from the error word every warp polls */
+    uint64_t    unit_cursor;
+    uint64_t    __pad2[15];
 } xb_status;
 
 /* error message ids reported by device code */
