@@ -389,7 +389,7 @@ __device__ __forceinline__ int xb_ld_width(int ld)
 /* ---------------------------------------------------------------
  * source units and 32-row batches
  * --------------------------------------------------------------- */
-struct XbSrc {
+struct alignas(16) XbSrc {
     uint64_t unit;                  /* current unit (global index) */
     uint64_t claim_end;             /* BLOCK: end of the current claim */
     unsigned long long nx_l0;       /* BLOCK, lane 0: first unit of the claim taken ahead */
@@ -404,7 +404,7 @@ struct XbSrc {
     uint32_t row0;                  /* ARROW / ROW: first row of the unit */
     uint32_t item;                  /* next item of the unit */
     uint32_t nitems;                /* items of the unit */
-} __attribute__((aligned(16)));
+};
 
 /* chunk owning global unit 'unit' (tasks are sorted by unit_base) */
 __device__ __forceinline__ uint32_t

@@ -66,6 +66,23 @@ __device__ __forceinline__ uint32_t xbj_itemid(const uint8_t *page, uint32_t nit
     return i < nitems ? (uint32_t)xb_fetch_le(page + SizeOfPageHeaderData + 4 * i, 4) : 0u;
 }
 
+__device__ __forceinline__ void xbj_prefetch_l1(const void *p)
+{
+    asm volatile("prefetch.global.L1 [%0];" :: "l"(p));
+}
+
+/* pull the tuple of line pointer lp into L1 (both ends: it may straddle a line) */
+__device__ __forceinline__ void xbj_prefetch_tuple(const uint8_t *page, uint32_t lp)
+{
+    if (ITEMID_FLAGS(lp) == LP_NORMAL) {
+        const uint32_t off = ITEMID_OFF(lp), len = ITEMID_LEN(lp);
+        if (len > 0 && off + len <= PGSTROM_BLCKSZ) {
+            xbj_prefetch_l1(page + off);
+            xbj_prefetch_l1(page + off + len - 1);
+        }
+    }
+}
+
 __device__ __forceinline__ void
 xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
 
@@ -114,6 +131,11 @@ xbj_kernel(XbExecArgs args)
     const uint8_t *page = nullptr;
     const kern_data_store *kds = nullptr;
     uint32_t row0 = 0, item = 0, nitems = 0;
+    /* heap pages are software-pipelined over the batches of a page: the
+     * line pointers of the next batch are in registers and its tuples are
+     * being pulled into L1 while this batch runs; the line pointers of the
+     * batch after that are in flight */
+    uint32_t lp_next = 0, lp_after = 0;
 
     for (;;) {
         bool done = false;
@@ -130,11 +152,21 @@ xbj_kernel(XbExecArgs args)
             row0 = src.row0;
             item = 0;
             nitems = src.nitems;
+            if (args.format == KDS_FORMAT_BLOCK) {
+                lp_next = xbj_itemid(page, nitems, lane);
+                lp_after = xbj_itemid(page, nitems, lane + 32);
+            }
         }
         if (done)
             break;
         const uint32_t idx = item + lane;
-        const uint32_t lp = args.format == KDS_FORMAT_BLOCK ? xbj_itemid(page, nitems, idx) : 0u;
+        uint32_t lp = 0;
+        if (args.format == KDS_FORMAT_BLOCK) {
+            lp = lp_next;
+            lp_next = lp_after;
+            xbj_prefetch_tuple(page, lp_next);
+            lp_after = xbj_itemid(page, nitems, idx + 64);
+        }
         item += 32;
         bool failed = false;
         if (idx < nitems) {
