@@ -1024,6 +1024,47 @@ struct Compiler {
     }
 
     /*
+     * GROUP BY keys that are all columns loaded at one inner depth (a
+     * grouping by dimension attributes): the build numbers the distinct key
+     * tuples among that relation's rows, and the specialised kernel finds
+     * a row's group entry by that number.  Keys must compare by their bits:
+     * integers, floats, and text whose hash is cached (those columns get
+     * canonical pointers, one address per distinct string).
+     */
+    void choose_gid_depth()
+    {
+        plan->gid_depth = 0;
+        if (plan->has_groupby != 1 || plan->nkeys == 0)
+            return;
+        uint64_t written = 0;
+        for (uint32_t i = 0; i < plan->ninsns; i++) {
+            const xb_insn &x = plan->insns[i];
+            if (x.op != XB_OP_END && x.op != XB_OP_MASK_PUSH && x.op != XB_OP_MASK_NARROW &&
+                x.op != XB_OP_MASK_POP)
+                written |= 1ULL << x.dst;
+        }
+        int dd = -1;
+        for (uint32_t k = 0; k < plan->nkeys; k++) {
+            const xb_key &key = plan->keys[k];
+            if (key.rk == XB_RK_NUM || (written & (1ULL << key.reg)))
+                return;
+            int found = -1;
+            for (uint32_t d = 1; d <= plan->nrels && found < 0; d++)
+                for (uint32_t j = 0; j < plan->inner[d].nloads; j++)
+                    if (plan->inner[d].load[j].reg == key.reg) {
+                        found = (int)d;
+                        if (key.rk == XB_RK_TEXT && !((plan->inner[d].hashed >> j) & 1u))
+                            return;
+                        break;
+                    }
+            if (found < 0 || (dd >= 0 && found != dd))
+                return;
+            dd = found;
+        }
+        plan->gid_depth = (uint32_t)dd;
+    }
+
+    /*
      * Hashes of text / numeric values that come straight from an inner
      * relation's column (a group key taken from a dimension table, a join
      * key carried to a deeper depth) depend only on the inner row: the
@@ -1153,6 +1194,7 @@ struct Compiler {
             return false;
         compute_liveness();
         mark_cached_hashes();
+        choose_gid_depth();
         if (plan->has_groupby) {
             const bool kh = plan->has_groupby == 1 && plan->gb_keyhash.count > 0;
             plan->gb_all.start = plan->gb_args.count ? plan->gb_args.start : plan->gb_keyhash.start;

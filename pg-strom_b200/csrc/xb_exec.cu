@@ -889,6 +889,8 @@ xb_build_drec(xb_inner *in, const xb_plan *plan)
         const uint32_t row = (uint32_t)ent - 1;
         char *rec = in->dpay + (size_t)(uint32_t)((int64_t)key - in->dkey_min) * in->drec_size;
         uint32_t head = 0x80000000U;
+        if (in->gid_on)
+            *(uint32_t *)(rec + 4) = in->gids[row];
         for (uint32_t k = 0; k < in->nloads; k++) {
             if (!((in->live >> k) & 1u))
                 continue;
@@ -902,6 +904,89 @@ xb_build_drec(xb_inner *in, const xb_plan *plan)
         }
         *(uint32_t *)rec = head;
     }
+}
+
+/* ---------------------------------------------------------------
+ * dense group ids of an inner relation's GROUP BY key tuples
+ * --------------------------------------------------------------- */
+
+/* load index (at this depth) of group key k, or -1 */
+__device__ __forceinline__ int xb_gid_load(const xb_plan *plan, const xb_inner *in, uint32_t k)
+{
+    for (uint32_t j = 0; j < in->nloads; j++)
+        if (in->load[j].reg == plan->keys[k].reg)
+            return (int)j;
+    return -1;
+}
+
+/* do inner rows a and b hold the same key tuple (NULLs equal, values by bits) */
+__device__ __forceinline__ bool
+xb_gid_same(const xb_plan *plan, const xb_inner *in, uint32_t a, uint32_t b)
+{
+    const uint32_t n = in->nitems, words = (n + 31) / 32;
+    for (uint32_t k = 0; k < plan->nkeys; k++) {
+        const int j = xb_gid_load(plan, in, k);
+        const bool na = (in->nulls[(size_t)j * words + a / 32] >> (a % 32)) & 1u;
+        const bool nb = (in->nulls[(size_t)j * words + b / 32] >> (b % 32)) & 1u;
+        if (na != nb)
+            return false;
+        if (na)
+            continue;
+        if (in->vals[(size_t)j * n + a] != in->vals[(size_t)j * n + b])
+            return false;
+        if (plan->keys[k].rk == XB_RK_TEXT && in->auxs[(size_t)j * n + a] != in->auxs[(size_t)j * n + b])
+            return false;
+    }
+    return true;
+}
+
+/* rep[row] = first-inserted row with the same key tuple */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_gid_rep(const xb_plan *plan, const xb_inner *in, uint32_t *table, uint32_t tmask, uint32_t *rep)
+{
+    const uint32_t n = in->nitems, words = (n + 31) / 32;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n;
+         row += gridDim.x * blockDim.x) {
+        uint64_t h = 0x9e3779b97f4a7c15ULL;
+        for (uint32_t k = 0; k < plan->nkeys; k++) {
+            const int j = xb_gid_load(plan, in, k);
+            const bool isnull = (in->nulls[(size_t)j * words + row / 32] >> (row % 32)) & 1u;
+            const uint64_t v = isnull ? 0x5a5a5a5aULL : in->vals[(size_t)j * n + row];
+            h = (h ^ v) * 0x100000001b3ULL;
+            h ^= h >> 29;
+        }
+        uint32_t pos = (uint32_t)h & tmask;
+        rep[row] = row;
+        for (uint32_t probe = 0; probe <= tmask; probe++) {
+            const uint32_t old = atomicCAS(&table[pos], 0u, row + 1);
+            if (old == 0)
+                break;
+            if (xb_gid_same(plan, in, old - 1, row)) {
+                rep[row] = old - 1;
+                break;
+            }
+            pos = (pos + 1) & tmask;
+        }
+    }
+}
+
+/* number the representatives, then give every row its representative's id */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_gid_number(xb_inner *in, const uint32_t *rep, uint32_t *counter)
+{
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < in->nitems;
+         row += gridDim.x * blockDim.x)
+        if (rep[row] == row)
+            in->gids[row] = atomicAdd(counter, 1u);
+}
+
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_gid_fill(xb_inner *in, const uint32_t *rep)
+{
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < in->nitems;
+         row += gridDim.x * blockDim.x)
+        if (rep[row] != row)
+            in->gids[row] = in->gids[rep[row]];
 }
 
 /* fill the direct-address table of a unique 32-bit key from the index */
@@ -1452,6 +1537,9 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             in->dtab = nullptr;
             in->drec_size = 0;
             in->dpay = nullptr;
+            in->gid_on = 0;
+            in->ngids = 0;
+            in->gids = nullptr;
             if (in->hashed)
                 DALLOC((size_t)nl * n * 4, &in->hashes);
             cudaMemsetAsync(in->index, 0, cap * 8, st);
@@ -1533,6 +1621,47 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         FAIL(s->h_status->errcode, "inner relation build: %s", xb_msg_text(s->h_status->msg_id));
     /* refresh the host copy of the inner descriptors (unique_hash) */
     cudaMemcpy(s->h_plan, s->d_plan, sizeof(xb_plan), cudaMemcpyDeviceToHost);
+    /* dense group ids when every GROUP BY key is a column of one inner
+     * relation; the specialised kernels then index the shared-memory group
+     * table by id.  Needs the shared table to hold every id. */
+    if (s->h_plan->gid_depth >= 1 && s->h_plan->gid_depth <= plan->nrels && plan->gent_size > 0) {
+        const uint32_t d = s->h_plan->gid_depth;
+        xb_inner *in = &s->h_plan->inner[d];
+        const uint32_t n = in->nitems;
+        const uint32_t limit = (48 * 1024) / plan->gent_size;
+        if (n > 0) {
+            DALLOC((size_t)n * 4, &in->gids);
+            cudaMemcpyAsync(&s->d_plan->inner[d], in, sizeof(xb_inner), cudaMemcpyHostToDevice, st);
+            const uint64_t tcap = xb_next_pow2((uint64_t)n * 2 + 64);
+            uint32_t *table = nullptr, *rep = nullptr, *counter = nullptr;
+            if (cudaMallocAsync((void **)&table, tcap * 4, st) != cudaSuccess ||
+                cudaMallocAsync((void **)&rep, (size_t)n * 4, st) != cudaSuccess ||
+                cudaMallocAsync((void **)&counter, 4, st) != cudaSuccess)
+                FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: no device memory for group ids");
+            cudaMemsetAsync(table, 0, tcap * 4, st);
+            cudaMemsetAsync(counter, 0, 4, st);
+            int grid = (int)((n + XB_BLOCK - 1) / XB_BLOCK);
+            if (grid > dev->nsm * 8) grid = dev->nsm * 8;
+            xb_gid_rep<<<grid, XB_BLOCK, 0, st>>>(s->d_plan, &s->d_plan->inner[d], table, (uint32_t)(tcap - 1), rep);
+            xb_gid_number<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d], rep, counter);
+            xb_gid_fill<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d], rep);
+            uint32_t ngids = 0;
+            cudaMemcpyAsync(&ngids, counter, 4, cudaMemcpyDeviceToHost, st);
+            cudaFreeAsync(table, st);
+            cudaFreeAsync(rep, st);
+            cudaFreeAsync(counter, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess)
+                FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));
+            const uint32_t cap = (uint32_t)xb_next_pow2(ngids > 32 ? ngids : 32);
+            if (ngids >= 1 && ngids <= limit && (size_t)cap * plan->gent_size <= 48 * 1024) {
+                in->gid_on = 1;
+                in->ngids = ngids;
+                if (s->sm_cap < cap)
+                    s->sm_cap = cap;
+                cudaMemcpyAsync(&s->d_plan->inner[d], in, sizeof(xb_inner), cudaMemcpyHostToDevice, st);
+            }
+        }
+    }
     /* direct-address tables for unique, dense 32-bit join keys (used by the
      * session-specialised kernels; the interpreter keeps probing the index) */
     for (uint32_t d = 1; d <= plan->nrels; d++) {

@@ -20,6 +20,19 @@
 #define XB_MIN_BLOCKS   2           /* resident CTAs per SM the kernel is built for */
 #define XB_PROBE_LIMIT  4096        /* max probes in the global group table */
 
+/*
+ * Hide a pointer's address space from the compiler.  Group-state atomics
+ * (64-bit adds, int128 carries, compensated double adds) on the shared
+ * group table measured far faster (0.45 vs 0.68 ms on the 20M-row join
+ * workload) when issued through a pointer that may be shared or global
+ * than through one the compiler has proven to be shared memory.
+ */
+__device__ __forceinline__ char *xb_generic_ptr(char *p)
+{
+    asm volatile("mov.b64 %0, %0;" : "+l"(p));
+    return p;
+}
+
 /* ================================================================
  * memory-order helpers (generic addresses: shared or global)
  * ================================================================ */

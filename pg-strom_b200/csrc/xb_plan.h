@@ -166,6 +166,11 @@ typedef struct xb_inner {
     uint32_t    direct;         /* 1: dtab is valid */
     uint32_t    drange;         /* dkey_max - dkey_min + 1 */
     uint32_t   *dtab;
+    /* dense group ids: when every GROUP BY key is a column of this depth,
+     * gids[row] numbers the distinct key tuples of the inner rows (0..ngids-1) */
+    uint32_t    gid_on;         /* 1: gids valid (and carried in direct records) */
+    uint32_t    ngids;
+    uint32_t   *gids;
     /* direct records: the live columns of the row of key k packed at
      * dpay + (k - dkey_min) * drec_size (layout: xb_drec_layout) */
     uint32_t    drec_size;
@@ -232,6 +237,7 @@ typedef struct xb_plan {
     uint32_t    naggs;
     xb_agg      aggs[XB_MAX_AGGS];
     uint32_t    gent_size;      /* bytes of one group entry (multiple of 16) */
+    uint32_t    gid_depth;      /* inner depth holding every group key (0: none) */
     uint32_t    gent_keys_off;
     uint32_t    nkeys_text;     /* number of text/numeric keys (arena use) */
 
@@ -250,7 +256,8 @@ typedef struct xb_plan {
 
 /*
  * Layout of a direct record: a u32 header (bit 31: a row holds this key,
- * bit k: load k is NULL), then one u32 per live text length and per live
+ * bit k: load k is NULL), the u32 group id when gid_on, then one u32 per
+ * live text length and per live
  * precomputed hash, then the u64 value of every live load (8-aligned);
  * the size is a multiple of 16.  Offsets of load k are -1 where absent.
  * Returns the record size.
@@ -258,7 +265,7 @@ typedef struct xb_plan {
 XB_PLAN_HD uint32_t
 xb_drec_layout(const xb_inner *in, const uint8_t *rk, int k, int *off_val, int *off_aux, int *off_hash)
 {
-    uint32_t off = 4;
+    uint32_t off = in->gid_on ? 8 : 4;      /* header, then the group id */
     if (off_val) *off_val = -1;
     if (off_aux) *off_aux = -1;
     if (off_hash) *off_hash = -1;
