@@ -72,6 +72,31 @@ int  xpuB200ExecTask(xpuB200Session *sess,
                      kern_exec_results *results, kern_errorbuf *err);
 
 /*
+ * Execute one chunk of a session whose bytecode projects rows
+ * (kern_session_info.xpucode_projection without GROUP BY): every row that
+ * passes the scan quals and the joins is formed as a kern_tupitem and
+ * written into kds_dst, a KDS_FORMAT_ROW buffer of dst_sz bytes laid out
+ * like the session's projection_kds_dst header (row index after the
+ * header, tuples packed from the end).  kds_dst is a host pointer unless
+ * kds_dst_on_device is non-zero (then a device pointer on this GPU, 8-byte
+ * aligned).  *p_required receives the bytes the chunk's rows need.  If they
+ * do not fit, ERRCODE_SUSPEND_NO_SPACE is returned, kds_dst's header is not
+ * written (a host kds_dst is not touched at all) and the caller runs the
+ * chunk again with a buffer of *p_required bytes; the statistics of that
+ * failed run are not accumulated.
+ * Replaces the kds_dst allocation of gpuservHandleGpuTaskExec
+ * (gpu_service.c:4158-4176) together with the projection step of the
+ * kernels (execGpuJoinProjection, cuda_gpujoin.cu:753-900) and the
+ * NO_SPACE write-back of
+ * __gpuservLaunchGpuTaskExecKernel (gpu_service.c:3894-3908).
+ */
+int  xpuB200ExecTaskDst(xpuB200Session *sess,
+                        const kern_data_store *kds_src, int kds_src_on_device,
+                        void *kds_dst, uint64_t dst_sz, int kds_dst_on_device,
+                        uint64_t *p_required,
+                        kern_exec_results *results, kern_errorbuf *err);
+
+/*
  * Materialise the final buffer in the reference's KDS_FORMAT_HASH layout
  * (kern_hashitem tuples with kagg_state__* partial states), as read by
  * pgstromScanNextTuple (executor.c:861-883) and finalised by aggfuncs.c.

@@ -22,6 +22,8 @@
  *   GROUP BY            cuda_gpupreagg.cu:1196-1774: SaveExpr arguments,
  *                       key hash, key equality, partial-state updates
  *   kds_final tuples    cuda_gpupreagg.cu:18-223 (__writeOutOneTuplePreAgg)
+ *   projected rows      cuda_gpujoin.cu:753-800 + xpu_common.cu:1096-1184
+ *                       (execGpuJoinProjection, __kern_form_minimal_tuple)
  * Floating-point sums are accumulated in row order in plain FP64: this is
  * the "FP64 sequentially ordered sum" the GPU results are compared with.
  */
@@ -245,6 +247,11 @@ typedef struct xo_sess {
     int         has_keys;
     int         nattrs;
     const kern_data_store *kds_final_head;
+    /* device projection: formed rows, MAXALIGNed one after another */
+    const kern_expression *proj;
+    const kern_data_store *kds_dst_head;
+    uint8_t    *proj_buf;
+    uint64_t    proj_len, proj_cap, proj_nrows, proj_usage;
     xo_datum    slot[XO_MAXSLOTS];
     /* groups */
     xo_group  **htab;
@@ -728,11 +735,107 @@ static int join_quals_ok(xo_sess *s, const kern_expression *kj, int *ok)
     return 1;
 }
 
+/* one projected datum at t of base (measure only when base is NULL);
+ * returns its length (the xpu_*_datum_write of the slot's type) */
+static uint32_t proj_datum(const xo_datum *d, uint8_t *base)
+{
+    switch (d->type_code) {
+    case TypeOpCode__bool:   if (base) base[0] = d->i ? 1 : 0; return 1;
+    case TypeOpCode__int2:   { int16_t v = (int16_t)d->i; if (base) memcpy(base, &v, 2); return 2; }
+    case TypeOpCode__int4:
+    case TypeOpCode__date:   { int32_t v = (int32_t)d->i; if (base) memcpy(base, &v, 4); return 4; }
+    case TypeOpCode__int8:
+    case TypeOpCode__time:
+    case TypeOpCode__timestamp:
+    case TypeOpCode__timestamptz: { if (base) memcpy(base, &d->i, 8); return 8; }
+    case TypeOpCode__float8: { if (base) memcpy(base, &d->f, 8); return 8; }
+    case TypeOpCode__text:
+    case TypeOpCode__bytea: {
+        uint32_t n = 4 + d->len;
+        if (base) { uint32_t h = n << 2; memcpy(base, &h, 4); memcpy(base + 4, d->p, d->len); }
+        return n;
+    }
+    case TypeOpCode__numeric: {
+        uint32_t n = numeric_varsize(d->p);
+        if (base) memcpy(base, d->p, n);
+        return n;
+    }
+    }
+    return 0;
+}
+
+/* form one row (__kern_form_minimal_tuple, xpu_common.cu:1096-1184) into
+ * base, or measure it when base is NULL; returns t_len */
+static uint32_t proj_form(xo_sess *s, int nattrs, uint8_t *base, uint32_t rowid)
+{
+    const uint16_t *slot_id = s->proj->u.proj.slot_id;
+    const kern_data_store *kd = s->kds_dst_head;
+    int hasnull = 0;
+    for (int j = 0; j < nattrs; j++)
+        if (slot_id[j] >= s->nslots || s->slot[slot_id[j]].kind == DK_NULL) { hasnull = 1; break; }
+    uint32_t t = (uint32_t)PGSTROM_MAXALIGN(offsetof(kern_tupitem, t_bits) + (hasnull ? (nattrs + 7) / 8 : 0));
+    uint16_t infomask = hasnull ? HEAP_HASNULL : 0;
+    kern_tupitem *ti = (kern_tupitem *)base;
+    if (base) {
+        memset(base, 0, t);
+        ti->t_infomask2 = (uint16_t)(nattrs & HEAP_NATTS_MASK);
+        ti->t_hoff = (uint8_t)(t + MINIMAL_TUPLE_OFFSET);
+    }
+    for (int j = 0; j < nattrs; j++) {
+        if (slot_id[j] >= s->nslots) continue;
+        const xo_datum *d = &s->slot[slot_id[j]];
+        if (d->kind == DK_NULL) continue;
+        int al = kd->colmeta[j].attalign > 0 ? kd->colmeta[j].attalign : 1;
+        uint32_t tn = (uint32_t)PGSTROM_TYPEALIGN(al, t);
+        if (base && tn > t) memset(base + t, 0, tn - t);
+        uint32_t n = proj_datum(d, base ? base + tn : NULL);
+        if (kd->colmeta[j].attlen == -1) infomask |= HEAP_HASVARWIDTH;
+        if (base && hasnull) ti->t_bits[j >> 3] |= (uint8_t)(1u << (j & 7));
+        t = tn + n;
+    }
+    t += ROWID_SIZE;
+    if (base) {
+        ti->t_len = t;
+        ti->t_infomask = infomask;
+        memcpy(base + t - ROWID_SIZE, &rowid, 4);
+    }
+    return t;
+}
+
+/* projection of one output row: the Projection arguments fill their
+ * slots, then the row is formed (execGpuJoinProjection,
+ * cuda_gpujoin.cu:753-800, kern_estimate_minimal_tuple xpu_common.cu:1245-1292) */
+static int proj_row(xo_sess *s)
+{
+    const kern_expression *kp = s->proj;
+    const kern_expression *a = first_arg(kp);
+    for (uint32_t i = 0; i < kp->nr_args; i++, a = next_arg(a)) {
+        xo_datum d;
+        if (!eval(s, a, &d)) return 0;
+    }
+    int nattrs = kp->u.proj.nattrs;
+    if (nattrs > (int)s->kds_dst_head->ncols) nattrs = s->kds_dst_head->ncols;
+    uint32_t tl = proj_form(s, nattrs, NULL, 0);
+    uint64_t need = PGSTROM_MAXALIGN(tl);
+    if (s->proj_len + need > s->proj_cap) {
+        uint64_t cap = s->proj_cap ? s->proj_cap * 2 : 1 << 16;
+        while (cap < s->proj_len + need) cap *= 2;
+        s->proj_buf = (uint8_t *)realloc(s->proj_buf, cap);
+        s->proj_cap = cap;
+    }
+    memset(s->proj_buf + s->proj_len, 0, need);
+    proj_form(s, nattrs, s->proj_buf + s->proj_len, (uint32_t)s->proj_nrows);
+    s->proj_len += need;
+    s->proj_nrows++;
+    s->proj_usage += PGSTROM_MAXALIGN(PGSTROM_MAXALIGN(tl) + s->session->gpusort_htup_margin);
+    return 1;
+}
+
 static int process_depth(xo_sess *s, int depth)
 {
     if (depth > s->nrels) {
         s->nitems_out++;
-        return s->gb_actions ? groupby_row(s) : 1;
+        return s->gb_actions ? groupby_row(s) : s->proj ? proj_row(s) : 1;
     }
     xo_datum h;
     if (!eval(s, s->hash_value[depth], &h)) return 0;
@@ -806,6 +909,10 @@ int xo_open(const void *session, uint64_t session_sz, const void *kmrels, uint64
     if (s->gb_actions) {
         s->nattrs = s->gb_actions->u.pagg.nattrs;
         s->kds_final_head = (const kern_data_store *)((const char *)session + s->session->groupby_kds_final);
+    }
+    if (!s->gb_actions && s->session->xpucode_projection) {
+        s->proj = kexp_at(s, s->session->xpucode_projection);
+        s->kds_dst_head = (const kern_data_store *)((const char *)session + s->session->projection_kds_dst);
     }
     s->hsize = 1 << 20;
     s->htab = (xo_group **)calloc(s->hsize, sizeof(xo_group *));
@@ -1042,9 +1149,28 @@ uint64_t xo_final(xo_sess *s, void *buf, uint64_t buf_sz)
     return length;
 }
 
+/* projected rows so far: copies them (MAXALIGNed kern_tupitems, row id =
+ * their order) into buf when it is large enough; returns their bytes and
+ * sets the row count and the kds_dst usage the reference would take */
+uint64_t xo_proj_rows(xo_sess *s, void *buf, uint64_t buf_sz, uint64_t *p_nrows, uint64_t *p_usage)
+{
+    if (p_nrows) *p_nrows = s->proj_nrows;
+    if (p_usage) *p_usage = s->proj_usage;
+    if (buf && buf_sz >= s->proj_len && s->proj_len)
+        memcpy(buf, s->proj_buf, s->proj_len);
+    return s->proj_len;
+}
+
+/* forget the projected rows (next chunk's kds_dst) */
+void xo_proj_reset(xo_sess *s)
+{
+    s->proj_len = s->proj_nrows = s->proj_usage = 0;
+}
+
 void xo_close(xo_sess *s)
 {
     if (!s) return;
+    free(s->proj_buf);
     for (uint64_t i = 0; i < s->ngroups; i++) {
         free(s->order[i]->keybytes);
         free(s->order[i]);

@@ -28,6 +28,9 @@ def lib():
         L.xo_final.argtypes = [P, P, U64]
         L.xo_final.restype = ctypes.c_uint64
         L.xo_close.argtypes = [P]
+        L.xo_proj_rows.argtypes = [P, P, U64, ctypes.POINTER(U64), ctypes.POINTER(U64)]
+        L.xo_proj_rows.restype = ctypes.c_uint64
+        L.xo_proj_reset.argtypes = [P]
         L.xo_hash_bytes.argtypes = [P, ctypes.c_uint32]
         L.xo_hash_bytes.restype = ctypes.c_uint32
         _LIB = L
@@ -67,6 +70,22 @@ class Oracle:
         buf = np.zeros(n, dtype=np.uint8)
         lib().xo_final(self.h, _p(buf), n)
         return buf
+
+    def proj_rows(self, reset=False):
+        """Projected rows since the last reset: (list of tuple images with
+        the row id cut off, kds_dst usage the rows take)."""
+        n, usage = ctypes.c_uint64(), ctypes.c_uint64()
+        nb = lib().xo_proj_rows(self.h, None, 0, ctypes.byref(n), ctypes.byref(usage))
+        buf = np.zeros(max(nb, 8), dtype=np.uint8)
+        lib().xo_proj_rows(self.h, _p(buf), nb, ctypes.byref(n), ctypes.byref(usage))
+        rows, pos = [], 0
+        for _ in range(n.value):
+            t_len = int(buf[pos:pos + 4].view(np.uint32)[0])
+            rows.append(bytes(buf[pos:pos + t_len - 4]))
+            pos += (t_len + 7) & ~7
+        if reset:
+            lib().xo_proj_reset(self.h)
+        return rows, usage.value
 
     def close(self):
         if self.h:

@@ -667,6 +667,91 @@ struct Compiler {
         return err.empty();
     }
 
+    /*
+     * Device projection (codegen_build_projection, codegen.c:3880-3950):
+     * the Projection expression's arguments are VarExpr (the slot already
+     * holds the value) or SaveExpr (compute into a slot); u.proj.slot_id[]
+     * names the slot of every output attribute, and the session's
+     * projection_kds_dst is the KDS_FORMAT_ROW header rows are written to.
+     */
+    bool projection()
+    {
+        plan->has_proj = 0;
+        if (!session->xpucode_projection)
+            return true;
+        const kern_expression *kp = kexp_at(session->xpucode_projection);
+        if (!err.empty()) return false;
+        if (!kp || kp->opcode != FuncOpCode__Projection)
+            return fail("malformed Projection expression");
+        const int nattrs = kp->u.proj.nattrs;
+        if (nattrs < 1 || nattrs > XB_MAX_PROJ ||
+            offsetof(kern_expression, u.proj.slot_id) + sizeof(uint16_t) * nattrs > kp->len)
+            return fail("Projection has %d attributes (max %d)", nattrs, XB_MAX_PROJ);
+        if (kp->u.proj.hash != 0)
+            return fail("Projection with a hash value (pinned inner buffer) is not supported");
+        /* argument programs: SaveExpr into slots; VarExpr needs nothing */
+        plan->proj_args.start = (uint16_t)plan->ninsns;
+        plan->proj_args.count = 0;
+        plan->proj_args.result = -1;
+        ntemps = plan->nslots;
+        const kern_expression *karg = first_arg(kp);
+        for (uint32_t i = 0; i < kp->nr_args; i++) {
+            if (!karg) return fail("Projection argument %u is broken", i);
+            if (karg->opcode == FuncOpCode__SaveExpr) {
+                if (expr(karg) < 0)
+                    return false;
+            } else if (karg->opcode != FuncOpCode__VarExpr) {
+                return fail("Projection argument %u is neither VarExpr nor SaveExpr", i);
+            }
+            if (i + 1 < kp->nr_args)
+                karg = next_arg(kp, karg);
+        }
+        plan->proj_args.count = (uint16_t)(plan->ninsns - plan->proj_args.start);
+        if ((uint32_t)ntemps > plan->nregs)
+            plan->nregs = ntemps;
+        /* the destination header */
+        const uint64_t off = session->projection_kds_dst;
+        if (off == 0 || off + sizeof(kern_data_store) > session_sz)
+            return fail("projection without a kds_dst header");
+        const kern_data_store *kd = (const kern_data_store *)((const char *)session + off);
+        if (kd->format != KDS_FORMAT_ROW)
+            return fail("projection into KDS format '%c' is not supported", kd->format);
+        const uint64_t hl = KDS_HEAD_LENGTH(kd);
+        if (off + hl > session_sz || kd->hash_nslots != 0)
+            return fail("projection kds_dst header is broken");
+        /* attributes past kds_dst's columns are not written (as in
+         * __kern_form_minimal_tuple, xpu_common.cu:1113-1114) */
+        const int nout = (int)kd->ncols < nattrs ? (int)kd->ncols : nattrs;
+        if (nout < 1)
+            return fail("projection kds_dst has no columns");
+        for (int j = 0; j < nout; j++) {
+            const int slot = kp->u.proj.slot_id[j];
+            if (slot < 0 || slot >= (int)plan->nslots)
+                return fail("projected slot %d out of range", slot);
+            const kern_colmeta &cm = kd->colmeta[j];
+            xb_projcol &pc = plan->proj[j];
+            pc.reg = (uint8_t)slot;
+            pc.ld = (uint8_t)slot_ld[slot];
+            pc.attlen = cm.attlen;
+            pc.attalign = cm.attalign > 0 ? cm.attalign : 1;
+            int w = 0;
+            switch (pc.ld) {
+            case XB_LD_BOOL: w = 1; break;
+            case XB_LD_INT2: w = 2; break;
+            case XB_LD_INT4: case XB_LD_DATE: case XB_LD_FLT4: w = 4; break;
+            case XB_LD_INT8: case XB_LD_FLT8: w = 8; break;
+            default: w = -1; break;
+            }
+            if (pc.attlen != w)
+                return fail("projected attribute %d: column length %d does not fit its value", j, pc.attlen);
+        }
+        plan->proj_nattrs = (uint32_t)nout;
+        plan->proj_margin = session->gpusort_htup_margin;
+        plan->proj_head_len = (uint32_t)hl;
+        plan->has_proj = 1;
+        return true;
+    }
+
     bool loadvars(const kern_expression *kexp, int depth, xb_load *out, uint32_t *nout)
     {
         *nout = 0;
@@ -942,6 +1027,9 @@ struct Compiler {
         uint64_t later = 0;     /* registers read by group-by and aggregates */
         reads_of(plan->gb_args, &later);
         reads_of(plan->gb_keyhash, &later);
+        reads_of(plan->proj_args, &later);
+        for (uint32_t j = 0; plan->has_proj && j < plan->proj_nattrs; j++)
+            later |= 1ULL << plan->proj[j].reg;
         for (uint32_t j = 0; j < plan->naggs; j++)
             for (int16_t r : {plan->aggs[j].arg0, plan->aggs[j].arg1, plan->aggs[j].filter})
                 if (r >= 0) later |= 1ULL << r;
@@ -1141,8 +1229,7 @@ struct Compiler {
         if (nrels > XB_MAX_DEPTH)
             return fail("%u inner relations (max %d)", nrels, XB_MAX_DEPTH);
         plan->nrels = nrels;
-        if (session->xpucode_projection)
-            return fail("device projection (kds_dst output) is not supported by this build");
+
         if (session->xpucode_gist_evals_packed)
             return fail("GiST-index joins are not supported by this build");
 
@@ -1192,6 +1279,8 @@ struct Compiler {
         }
         if (!groupby())
             return false;
+        if (!projection())
+            return false;
         compute_liveness();
         mark_cached_hashes();
         choose_gid_depth();
@@ -1201,8 +1290,10 @@ struct Compiler {
             plan->gb_all.count = (uint16_t)(plan->gb_args.count + (kh ? plan->gb_keyhash.count : 0));
             plan->gb_all.result = kh ? plan->gb_keyhash.result : (int16_t)-1;
         }
-        if (plan->has_groupby == 0 && !(plan->task_kind & DEVTASK__PREAGG))
+        if (plan->has_groupby == 0 && !plan->has_proj && !(plan->task_kind & DEVTASK__PREAGG))
             return fail("scan/join without device projection or GROUP BY is not supported");
+        if (plan->has_groupby && plan->has_proj)
+            return fail("a session with both GROUP BY and device projection is not supported");
         return err.empty();
     }
 };

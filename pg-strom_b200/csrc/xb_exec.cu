@@ -625,12 +625,12 @@ xb_exec_kernel(XbExecArgs args)
             if (d > nrels) {
                 if (lane == 0)
                     ws->out += __popc(mask);
-                if (!plan->has_groupby) {
+                if (!plan->has_groupby && !plan->has_proj) {
                     d = nrels;
                     stage = nrels ? XB_ST_PROBE : XB_ST_FETCH;
                     continue;
                 }
-                prog = &plan->gb_all;
+                prog = plan->has_proj ? &plan->proj_args : &plan->gb_all;
             } else {
                 const xb_inner *in = &plan->inner[d];
                 if (in->fast_key >= 0) {
@@ -668,7 +668,24 @@ xb_exec_kernel(XbExecArgs args)
                 stage = XB_ST_ENTER;
             }
         } else if (stage == XB_ST_ENTER) {
-            if (d > nrels) {
+            if (d > nrels && plan->has_proj) {
+                /* projection: each passing lane writes one row into kds_dst */
+                uint64_t pv[XB_MAX_PROJ];
+                uint32_t pa[XB_MAX_PROJ];
+                uint32_t pn = 0;
+                for (uint32_t j = 0; j < plan->proj_nattrs; j++) {
+                    const uint32_t r = plan->proj[j].reg;
+                    pv[j] = RVAL(R, r);
+                    pa[j] = RAUX(R, r);
+                    if (RISNULL(R, r))
+                        pn |= 1u << j;
+                }
+                if ((mask >> lane) & 1u)
+                    xb_proj_emit(plan, args.dst, args.dst_len, pv, pa, pn, st);
+                __syncwarp();
+                d = nrels;
+                stage = nrels ? XB_ST_PROBE : XB_ST_FETCH;
+            } else if (d > nrels) {
                 /* group-by: find or create each lane's group, then update */
                 const uint32_t hash = plan->has_groupby == 1 ? (uint32_t)RVAL(R, plan->gb_keyhash.result) : 0;
                 char *e = nullptr;
@@ -1061,12 +1078,6 @@ struct XbFinalArgs {
 /* byte-wise store: kds_final columns follow the header's attalign, and the
  * trailing row-id sits right after a variable-length key, so no store in a
  * group tuple may assume natural alignment */
-__device__ __forceinline__ void xb_store(char *dst, const void *src, uint32_t n)
-{
-    const char *s = (const char *)src;
-    for (uint32_t i = 0; i < n; i++)
-        dst[i] = s[i];
-}
 
 /* one partial-aggregate tuple (__writeOutOneTuplePreAgg layout,
  * cuda_gpupreagg.cu:18-223); returns t_len.  ti == nullptr only measures. */
@@ -1333,6 +1344,12 @@ struct xpuB200Session {
     bool            jit_tried[256] = {false};
     void           *jit_fn[256] = {nullptr};
     char            ran_kind[256] = {0};   /* 'j' / 'v': kernel last launched per format */
+    /* device projection: staging buffer for host kds_dst, and the buffer of
+     * the launch in progress */
+    char           *d_dst = nullptr;
+    uint64_t        d_dst_cap = 0;
+    char           *launch_dst = nullptr;
+    uint64_t        launch_dst_len = 0;
     int             jit_grid[256] = {0};
     size_t          jit_smem = 0;
     double          jit_compile_ms = 0.0;
@@ -1437,6 +1454,7 @@ static void xb_session_free(xpuB200Session *s)
         cudaFree(p);
     if (s->d_src) cudaFree(s->d_src);
     if (s->d_tasks) cudaFree(s->d_tasks);
+    if (s->d_dst) cudaFree(s->d_dst);
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->h_plan) free(s->h_plan);
     cudaEventDestroy(s->ev0);
@@ -1747,6 +1765,8 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     a.format = format;
     a.sm_cap = s->sm_cap;
     a.warp_bytes = s->warp_bytes;
+    a.dst = s->launch_dst;
+    a.dst_len = s->launch_dst_len;
     a.gt = s->d_gt;
     a.st = s->d_status;
     /* the session-specialised kernel of this format, built on first use */
@@ -1839,7 +1859,8 @@ static int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
     return 0;
 }
 
-static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_errorbuf *err)
+/* wait for the launch and read its status (errors reported by the kernel) */
+static int xb_wait_status(xpuB200Session *s, kern_errorbuf *err)
 {
     cudaStream_t st = s->dev->stream;
     cudaMemcpyAsync(s->h_status, s->d_status, sizeof(xb_status), cudaMemcpyDeviceToHost, st);
@@ -1849,6 +1870,13 @@ static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_er
     const xb_status *hs = s->h_status;
     if (hs->errcode)
         return xb_set_error(err, hs->errcode, "xb_exec_kernel", hs->lineno, "%s", xb_msg_text(hs->msg_id));
+    return 0;
+}
+
+/* add a finished launch's statistics to the session and to *results */
+static void xb_account(xpuB200Session *s, kern_exec_results *results)
+{
+    const xb_status *hs = s->h_status;
     s->total_raw += hs->nitems_raw;
     s->total_in += hs->nitems_in;
     s->total_out += hs->nitems_out;
@@ -1866,8 +1894,20 @@ static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_er
             results->stats[d - 1].nitems_out = (uint32_t)hs->nitems_depth[d];
         }
     }
+}
+
+static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_errorbuf *err)
+{
+    int rc = xb_wait_status(s, err);
+    if (rc)
+        return rc;
+    xb_account(s, results);
     return 0;
 }
+
+static int xb_place_src(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
+                        kern_data_store *p_head, std::vector<char> *p_hbuf,
+                        const kern_data_store **p_dkds, kern_errorbuf *err);
 
 extern "C" int
 xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
@@ -1877,11 +1917,31 @@ xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_o
     if (!s || !kds_src)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid ExecTask arguments");
     std::lock_guard<std::mutex> g(s->lock);
+    if (s->h_plan->has_proj)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR,
+                      "the session projects rows into kds_dst: use xpuB200ExecTaskDst");
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->dev->stream;
     kern_data_store head;
     const kern_data_store *d_kds;
     std::vector<char> hbuf;
+    int rc = xb_place_src(s, kds_src, kds_src_on_device, &head, &hbuf, &d_kds, err);
+    if (rc) return rc;
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->dev->stream), err);
+    rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
+    if (rc) return rc;
+    return xb_finish_task(s, results, err);
+}
+
+/* validate a chunk and make it device-resident: host chunks are copied to
+ * the session's staging buffer so that heap pages start 16-byte aligned */
+static int xb_place_src(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
+                        kern_data_store *p_head, std::vector<char> *p_hbuf,
+                        const kern_data_store **p_dkds, kern_errorbuf *err)
+{
+    cudaStream_t st = s->dev->stream;
+    kern_data_store &head = *p_head;
+    std::vector<char> &hbuf = *p_hbuf;
+    const kern_data_store *d_kds;
     if (kds_src_on_device) {
         if (((uintptr_t)kds_src & 7) != 0)
             return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
@@ -1909,10 +1969,89 @@ xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_o
         XB_CUDA(cudaMemcpyAsync(s->d_src + shift, kds_src, kds_src->length, cudaMemcpyHostToDevice, st), err);
         d_kds = (const kern_data_store *)(s->d_src + shift);
     }
-    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
-    int rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
+    *p_dkds = d_kds;
+    return 0;
+}
+
+extern "C" int
+xpuB200ExecTaskDst(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
+                   void *kds_dst, uint64_t dst_sz, int kds_dst_on_device, uint64_t *p_required,
+                   kern_exec_results *results, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s || !kds_src || !kds_dst)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid ExecTaskDst arguments");
+    std::lock_guard<std::mutex> g(s->lock);
+    const xb_plan *plan = s->h_plan;
+    if (!plan->has_proj)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "the session has no device projection");
+    const kern_session_info *session = (const kern_session_info *)s->h_session.data();
+    const kern_data_store *tmpl = (const kern_data_store *)(s->h_session.data() + session->projection_kds_dst);
+    const uint64_t head_len = plan->proj_head_len;
+    const uint64_t len = dst_sz & ~7ULL;
+    if (len < head_len + 8)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "kds_dst of %llu bytes cannot hold a row",
+                      (unsigned long long)dst_sz);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    cudaStream_t st = s->dev->stream;
+    kern_data_store head;
+    const kern_data_store *d_kds;
+    std::vector<char> hbuf;
+    int rc = xb_place_src(s, kds_src, kds_src_on_device, &head, &hbuf, &d_kds, err);
     if (rc) return rc;
-    return xb_finish_task(s, results, err);
+    char *d_dst;
+    if (kds_dst_on_device) {
+        if (((uintptr_t)kds_dst & 7) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device kds_dst is not 8-byte aligned");
+        d_dst = (char *)kds_dst;
+    } else {
+        if (len > s->d_dst_cap) {
+            if (s->d_dst) cudaFree(s->d_dst);
+            s->d_dst = nullptr;
+            s->d_dst_cap = 0;
+            XB_CUDA(cudaMalloc((void **)&s->d_dst, len), err);
+            s->d_dst_cap = len;
+        }
+        d_dst = s->d_dst;
+    }
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+    s->launch_dst = d_dst;
+    s->launch_dst_len = len;
+    rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
+    s->launch_dst = nullptr;
+    s->launch_dst_len = 0;
+    if (rc) return rc;
+    rc = xb_wait_status(s, err);
+    if (rc) return rc;
+    const xb_status *hs = s->h_status;
+    const uint64_t nitems = hs->proj_nitems, usage = hs->proj_usage;
+    const uint64_t required = head_len + hs->proj_need;
+    if (p_required)
+        *p_required = required;
+    if (hs->proj_overflow)
+        return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE, "kds_dst needs %llu bytes (buffer %llu)",
+                      (unsigned long long)required, (unsigned long long)len);
+    /* the header: the session's kds_dst definition with this chunk's rows */
+    std::vector<char> hd((const char *)tmpl, (const char *)tmpl + head_len);
+    kern_data_store *kh = (kern_data_store *)hd.data();
+    kh->length = len;
+    kh->nitems = (uint32_t)nitems;
+    kh->usage = usage;
+    kh->format = KDS_FORMAT_ROW;
+    kh->hash_nslots = 0;
+    if (kds_dst_on_device) {
+        XB_CUDA(cudaMemcpyAsync(d_dst, hd.data(), head_len, cudaMemcpyHostToDevice, st), err);
+    } else {
+        char *h = (char *)kds_dst;
+        memcpy(h, hd.data(), head_len);
+        if (nitems)
+            XB_CUDA(cudaMemcpyAsync(h + head_len, d_dst + head_len, 8 * nitems, cudaMemcpyDeviceToHost, st), err);
+        if (usage)
+            XB_CUDA(cudaMemcpyAsync(h + len - usage, d_dst + len - usage, usage, cudaMemcpyDeviceToHost, st), err);
+    }
+    XB_CUDA(cudaStreamSynchronize(st), err);
+    xb_account(s, results);
+    return 0;
 }
 
 extern "C" int
@@ -2266,6 +2405,9 @@ xpuB200BatchCreate(xpuB200Session *s, const kern_data_store *const *kds_dev, uin
     if (!s || !kds_dev || nchunks == 0)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid batch arguments");
     std::lock_guard<std::mutex> g(s->lock);
+    if (s->h_plan->has_proj)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR,
+                      "the session projects rows into kds_dst: use xpuB200ExecTaskDst");
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
     std::vector<xb_task> tasks(nchunks);
     std::vector<char> first_head;
@@ -2400,6 +2542,34 @@ xpuB200HandleCommand(xpuB200Device *dev, xpuB200Session **p_sess, const XpuComma
         if (resp_sz < rsz) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
         memset(&resp->u.results, 0, rsz - head);
         resp->u.results.num_rels = nrels;
+        if ((*p_sess)->h_plan->has_proj) {
+            /* the projected rows follow the results as one KDS_FORMAT_ROW
+             * chunk, cut down to header + row index + tuples like
+             * __gpuClientWriteBackOneChunk (gpu_service.c:2818-2846) */
+            const uint64_t rhead = PGSTROM_MAXALIGN(rsz);
+            if (resp_sz < rhead + 64) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
+            char *dst = (char *)resp + rhead;
+            const uint64_t len = (resp_sz - rhead) & ~7ULL;
+            uint64_t required = 0;
+            rc = xpuB200ExecTaskDst(*p_sess, kds, 0, dst, len, 0, &required, &resp->u.results, &ebuf);
+            if (rc == ERRCODE_SUSPEND_NO_SPACE) {
+                rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR,
+                            "response buffer too small for the projected rows (%llu bytes needed)",
+                            (unsigned long long)(rhead + required));
+                break;
+            }
+            if (rc) break;
+            kern_data_store *kd = (kern_data_store *)dst;
+            const uint64_t hsz = KDS_HEAD_LENGTH(kd) + PGSTROM_MAXALIGN(8 * (uint64_t)kd->nitems);
+            if (kd->usage)
+                memmove(dst + hsz, dst + len - kd->usage, kd->usage);
+            kd->length = hsz + kd->usage;
+            resp->u.results.chunks_offset = (uint32_t)rhead;
+            resp->u.results.chunks_nitems = 1;
+            resp->tag = XpuCommandTag__Success;
+            resp->length = rhead + kd->length;
+            break;
+        }
         rc = xpuB200ExecTask(*p_sess, kds, 0, &resp->u.results, &ebuf);
         if (!rc) {
             resp->tag = XpuCommandTag__Success;

@@ -344,6 +344,8 @@ struct XbExecArgs {
     uint32_t        format;         /* common KDS format of the tasks */
     uint32_t        sm_cap;         /* shared-memory group table entries (0: none) */
     uint32_t        warp_bytes;     /* shared memory of one warp: counters, cursors, registers */
+    char           *dst;            /* projection: device kds_dst buffer, or nullptr */
+    uint64_t        dst_len;
     xb_gtable      *gt;
     xb_status      *st;
 };
@@ -642,6 +644,212 @@ xb_arrow_load(const kern_data_store *kds, const kern_colmeta *cm, uint32_t row, 
     }
 }
 
+
+/* ================================================================
+ * device projection: rows into a KDS_FORMAT_ROW kds_dst
+ * ================================================================ */
+
+/* byte-wise store: tuple attributes follow attalign only, and the trailing
+ * row id sits right after a variable-length attribute, so no store into a
+ * tuple may assume natural alignment */
+__device__ __forceinline__ void xb_store(char *dst, const void *src, uint32_t n)
+{
+    const char *s = (const char *)src;
+    for (uint32_t i = 0; i < n; i++)
+        dst[i] = s[i];
+}
+
+/*
+ * Projected rows are kern_tupitems in the layout of __kern_form_minimal_tuple
+ * (xpu_common.cu:1096-1184): a MAXALIGNed header with a NULL bitmap when any
+ * attribute is NULL, each non-NULL attribute at its kds_dst column's
+ * attalign, text with a 4-byte varlena header, numeric copied as its
+ * varlena, and the row id after the last attribute.  The helpers below are
+ * called once per attribute with constant ld / attalign by the specialised
+ * kernel and from a loop over plan->proj[] by the interpreter.
+ */
+
+/* header length (t_hoff, excluding MINIMAL_TUPLE_OFFSET) */
+__device__ __forceinline__ uint32_t xb_proj_hoff(uint32_t nattrs, bool hasnull)
+{
+    return (uint32_t)PGSTROM_MAXALIGN(offsetof(kern_tupitem, t_bits) + (hasnull ? (nattrs + 7) / 8 : 0));
+}
+
+/* place attribute (ld, attalign) of value v / aux at offset t of the tuple
+ * at base (measure only when base is nullptr); returns the offset after it */
+__device__ __forceinline__ uint32_t
+xb_proj_attr(char *base, uint32_t t, int attalign, int ld, uint64_t v, uint32_t aux, uint16_t &infomask)
+{
+    const uint32_t t_next = (uint32_t)PGSTROM_TYPEALIGN(attalign, t);
+    char *buf = nullptr;
+    if (base) {
+        for (uint32_t i = t; i < t_next; i++)
+            base[i] = 0;
+        buf = base + t_next;
+    }
+    uint32_t nbytes = 0;
+    switch (ld) {
+    case XB_LD_BOOL: { const uint8_t x = v ? 1 : 0; nbytes = 1; if (buf) xb_store(buf, &x, 1); break; }
+    case XB_LD_INT2: { const int16_t x = (int16_t)v; nbytes = 2; if (buf) xb_store(buf, &x, 2); break; }
+    case XB_LD_INT4:
+    case XB_LD_DATE: { const int32_t x = (int32_t)v; nbytes = 4; if (buf) xb_store(buf, &x, 4); break; }
+    case XB_LD_INT8:
+    case XB_LD_FLT8: { nbytes = 8; if (buf) xb_store(buf, &v, 8); break; }
+    case XB_LD_TEXT: {
+        nbytes = 4 + aux;
+        if (buf) {
+            const uint32_t hdr = nbytes << 2;               /* SET_VARSIZE */
+            xb_store(buf, &hdr, 4);
+            xb_store(buf + 4, (const void *)v, aux);
+        }
+        infomask |= HEAP_HASVARWIDTH;
+        break;
+    }
+    case XB_LD_NUMERIC: {
+        const uint8_t *vl = (const uint8_t *)v;
+        nbytes = xb_numeric_varsize(vl);
+        if (buf) xb_store(buf, vl, nbytes);
+        infomask |= HEAP_HASVARWIDTH;
+        break;
+    }
+    default:
+        break;
+    }
+    return t_next + nbytes;
+}
+
+/* zero the header and set t_infomask2 / t_hoff / the NULL bitmap */
+__device__ __forceinline__ void
+xb_proj_head(char *base, uint32_t nattrs, uint32_t hoff, uint32_t nulls)
+{
+    for (uint32_t i = 0; i < hoff; i++)
+        base[i] = 0;
+    const uint16_t im2 = (uint16_t)(nattrs & HEAP_NATTS_MASK);
+    const uint8_t th = (uint8_t)(hoff + MINIMAL_TUPLE_OFFSET);
+    xb_store(base + offsetof(kern_tupitem, t_infomask2), &im2, 2);
+    xb_store(base + offsetof(kern_tupitem, t_hoff), &th, 1);
+    if (nulls) {
+        for (uint32_t j = 0; j < nattrs; j++)
+            if (!((nulls >> j) & 1u))
+                base[offsetof(kern_tupitem, t_bits) + (j >> 3)] |= (char)(1 << (j & 7));
+    }
+}
+
+/* t_len, t_infomask and the trailing row id */
+__device__ __forceinline__ void
+xb_proj_tail(char *base, uint32_t t_len, uint16_t infomask, uint32_t rowid)
+{
+    xb_store(base + offsetof(kern_tupitem, t_infomask), &infomask, 2);
+    xb_store(base, &t_len, 4);
+    xb_store(base + t_len - ROWID_SIZE, &rowid, 4);
+}
+
+/* kds_dst bytes one row of tuple length t_len takes (the reference's
+ * MAXALIGN(MAXALIGN(t_len) + gpusort_htup_margin), cuda_gpujoin.cu:795) */
+__device__ __forceinline__ uint32_t xb_proj_rowsz(uint32_t t_len, uint32_t margin)
+{
+    return (uint32_t)PGSTROM_MAXALIGN(PGSTROM_MAXALIGN(t_len) + margin);
+}
+
+/*
+ * Claim sz bytes of kds_dst for one row.  Called by the lanes that emit a
+ * row, in any divergence: the lanes that arrive together share one claim
+ * (the reference instead locks kds_dst->nitems per block,
+ * cuda_gpujoin.cu:836-870).  Rows grow from the end of kds_dst, the row
+ * index (8-byte offsets from the end) follows the header.
+ *
+ * The claim first adds its row index and tuple bytes to proj_need; it fits
+ * when the sum stays within kds_dst.  proj_need only grows, so the claims
+ * that fit are exactly those added before the first one that did not, and
+ * together they need at most the buffer: only they then take row slots
+ * (proj_nitems) and tuple bytes (proj_usage), so no two of them overlap.
+ * Returns the tuple's address and sets *rowid, or returns nullptr (and sets
+ * proj_overflow) when the claim does not fit.
+ */
+__device__ __forceinline__ char *
+xb_proj_claim(char *dst, uint64_t dst_len, uint64_t head, uint32_t sz, xb_status *st, uint32_t *rowid)
+{
+    const uint32_t am = __activemask();
+    const uint32_t lane = xb_lane();
+    uint32_t incl = sz, total;
+    if (am == XB_FULL) {
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(XB_FULL, incl, o);
+            if (lane >= o)
+                incl += t;
+        }
+        total = __shfl_sync(XB_FULL, incl, 31);
+    } else {
+        incl = 0;
+        total = 0;
+        for (uint32_t m = am; m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            const uint32_t v = __shfl_sync(am, sz, l);
+            total += v;
+            if ((uint32_t)l <= lane)
+                incl += v;
+        }
+    }
+    const int leader = __ffs(am) - 1;
+    const uint32_t count = __popc(am);
+    unsigned long long bu = 0;
+    uint32_t bn = 0;
+    int fits = 0;
+    if (lane == (uint32_t)leader) {
+        const unsigned long long add = 8ULL * count + total;
+        const unsigned long long need = atomicAdd((unsigned long long *)&st->proj_need, add) + add;
+        fits = head + need <= dst_len;
+        if (fits) {
+            bu = atomicAdd((unsigned long long *)&st->proj_usage, (unsigned long long)total);
+            bn = atomicAdd(&st->proj_nitems, count);
+        } else {
+            atomicOr(&st->proj_overflow, 1u);
+        }
+    }
+    fits = __shfl_sync(am, fits, leader);
+    if (!fits)
+        return nullptr;
+    bu = __shfl_sync(am, bu, leader);
+    bn = __shfl_sync(am, bn, leader);
+    *rowid = bn + __popc(am & ((1u << lane) - 1));
+    return dst + dst_len - (bu + incl);
+}
+
+/* publish row rowid of the tuple at tp (after the tuple is written) */
+__device__ __forceinline__ void
+xb_proj_index(char *dst, uint64_t dst_len, uint64_t head, uint32_t rowid, const char *tp)
+{
+    *(uint64_t *)(dst + head + 8 * (uint64_t)rowid) = (uint64_t)(dst + dst_len - tp);
+}
+
+/* interpreter: form and write one row whose attribute j is vals[j] /
+ * auxs[j], NULL when bit j of nulls is set */
+__device__ __forceinline__ void
+xb_proj_emit(const xb_plan *plan, char *dst, uint64_t dst_len,
+             const uint64_t *vals, const uint32_t *auxs, uint32_t nulls, xb_status *st)
+{
+    const uint32_t n = plan->proj_nattrs;
+    const uint32_t hoff = xb_proj_hoff(n, nulls != 0);
+    uint16_t im = nulls ? HEAP_HASNULL : 0;
+    uint32_t t = hoff;
+    for (uint32_t j = 0; j < n; j++)
+        if (!((nulls >> j) & 1u))
+            t = xb_proj_attr(nullptr, t, plan->proj[j].attalign, plan->proj[j].ld, vals[j], auxs[j], im);
+    const uint32_t t_len = t + ROWID_SIZE;
+    const uint64_t head = plan->proj_head_len;
+    uint32_t rowid;
+    char *tp = xb_proj_claim(dst, dst_len, head, xb_proj_rowsz(t_len, plan->proj_margin), st, &rowid);
+    if (!tp)
+        return;
+    xb_proj_head(tp, n, hoff, nulls);
+    t = hoff;
+    for (uint32_t j = 0; j < n; j++)
+        if (!((nulls >> j) & 1u))
+            t = xb_proj_attr(tp, t, plan->proj[j].attalign, plan->proj[j].ld, vals[j], auxs[j], im);
+    xb_proj_tail(tp, t_len, im, rowid);
+    xb_proj_index(dst, dst_len, head, rowid, tp);
+}
 
 /* stage the column layout shared by a launch's chunks and the fixed-offset
  * loaders of the depth-0 loads; all threads of the CTA call this, followed

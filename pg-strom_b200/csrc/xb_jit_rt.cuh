@@ -31,6 +31,8 @@ struct XbjEnv {
     char           *sm_tab;         /* shared-memory group table, or nullptr */
     uint32_t        sm_mask;
     uint32_t        lane;
+    char           *dst;            /* projection: kds_dst and its length */
+    uint64_t        dst_len;
 };
 
 /* per-thread counters, 32-bit to spare registers; flushed into the launch
@@ -120,6 +122,8 @@ xbj_kernel(XbExecArgs args)
     E.sm_tab = args.sm_cap ? sm_entries : nullptr;
     E.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
     E.lane = lane;
+    E.dst = args.dst;
+    E.dst_len = args.dst_len;
     XbjCnt C;
     C.raw = C.in = C.out = 0;
 #pragma unroll

@@ -35,6 +35,7 @@
 #define XB_MAX_AGGS         32      /* partial aggregate columns */
 #define XB_MAX_INSNS        384     /* VM instructions per session */
 #define XB_MAX_COLS         64      /* source columns decoded per tuple */
+#define XB_MAX_PROJ         32      /* attributes of a projected row */
 #define XB_MASK_STACK       8
 
 /* register kinds */
@@ -207,6 +208,15 @@ typedef struct xb_key {
     uint16_t    __pad;
 } xb_key;
 
+/* one attribute of a projected row (kds_dst column) */
+typedef struct xb_projcol {
+    int16_t     attlen;         /* kds_dst column */
+    int8_t      attalign;
+    uint8_t     ld;             /* XB_LD_* of the source slot: how to write it */
+    uint8_t     reg;            /* source register (kvars slot) */
+    uint8_t     __pad[3];
+} xb_projcol;
+
 typedef struct xb_plan {
     uint32_t    magic;
     uint32_t    plan_sz;
@@ -240,6 +250,14 @@ typedef struct xb_plan {
     uint32_t    gid_depth;      /* inner depth holding every group key (0: none) */
     uint32_t    gent_keys_off;
     uint32_t    nkeys_text;     /* number of text/numeric keys (arena use) */
+
+    /* device projection into kds_dst (execGpuJoinProjection) */
+    uint32_t    has_proj;
+    uint32_t    proj_nattrs;
+    uint32_t    proj_margin;    /* gpusort_htup_margin added to every row */
+    uint32_t    proj_head_len;  /* KDS_HEAD_LENGTH of the kds_dst template */
+    xb_prog     proj_args;      /* SaveExpr programs filling the projected slots */
+    xb_projcol  proj[XB_MAX_PROJ];
 
     /* VM code */
     uint32_t    ninsns;
@@ -343,6 +361,15 @@ typedef struct xb_status {
      * claim lands here, away from the error word every warp polls */
     uint64_t    unit_cursor;
     uint64_t    __pad2[15];
+    /* projection output: proj_need counts the row index and tuple bytes
+     * of every claim, including those past the end of kds_dst (so that
+     * the host learns the size needed); proj_usage / proj_nitems place
+     * only the claims that fit */
+    uint64_t    proj_need;
+    uint64_t    proj_usage;
+    uint32_t    proj_nitems;
+    uint32_t    proj_overflow;
+    uint64_t    __pad3[13];
 } xb_status;
 
 /* error message ids reported by device code */

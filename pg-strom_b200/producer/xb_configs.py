@@ -11,6 +11,10 @@ the benchmark configurations (test and benchmark infrastructure).
                    1..10000 into dim2(pk int4, flag int2 in 0..4);
                    JOIN dim1, dim2 WHERE flag < 3 GROUP BY region ->
                    sum(qty*price), count(*)
+  scan_projection  the scan_groupby table, WHERE a < 300 projected to
+                   (id, a, b, c, a * 2 + g) rows (no GROUP BY)
+  join_projection  the join_groupby tables, projected to
+                   (fk1, qty * price, region, flag) rows
 
 Every generator also returns the expected per-group aggregates computed
 directly from the column arrays with numpy (independent of any page or
@@ -106,13 +110,15 @@ def zipf_bounded(r, n, s, size):
 
 
 def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3,
-                 key_stride=1, dim1_copies=1, miss_frac=0.0):
+                 key_stride=1, dim1_copies=1, miss_frac=0.0, with_rows=False):
     """Two-way hash join + group-by.  Defaults give the headline workload:
     dense unique dimension keys 1..n, every fact row matching.  Variants for
     the join paths: key_stride spreads the keys (k * stride; sparse keys
     take the hashed probe instead of direct addressing), dim1_copies > 1
     repeats every dim1 key with its own region (several matches per probe),
-    miss_frac makes that share of fact rows reference no dim1 row."""
+    miss_frac makes that share of fact rows reference no dim1 row.
+    with_rows adds meta["rows"]: the sorted (fk1, qty * price, region,
+    flag) tuples of every joined row."""
     r1 = rng_for(seed_config, 1)
     r2 = rng_for(seed_config, 2)
     rf = rng_for(seed_config, 0)
@@ -172,10 +178,20 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
     for k in range(len(REGIONS)):
         if cnt[k]:
             expect[(REGIONS[k].encode(),)] = {"sum_amount": (int(cnt[k]), tot[k]), "nrows": int(cnt[k])}
+    if with_rows:
+        rows = []
+        sel = np.flatnonzero(m)
+        for c in range(dim1_copies):
+            region_row = reg_code[c * ndim1 + idx1[sel]]
+            rows += list(zip(fk1[sel].tolist(), amount[sel].tolist(),
+                             [REGIONS[k].encode() for k in region_row], flag[idx2[sel]].tolist()))
+        rows.sort()
     hit1 = int((~miss).sum()) * dim1_copies
     out = int(m.sum()) * dim1_copies
     meta = {"nitems_raw": nfact, "nitems_in": nfact, "nitems_out": out,
             "depth_out": [hit1, out], "agg_names": ["sum_amount", "nrows"], "nkeys": 1}
+    if with_rows:
+        meta["rows"] = rows
     return fact, session, kmrels, expect, meta
 
 
@@ -251,3 +267,53 @@ def arrow_groupby(nrows=500_000_000, nkeys=10_000_000, seed_config=2, rows_per_c
                                       (1, float(vals.max())), (cnt, fsum)]
         meta.update({"nitems_in": int(m.sum()), "nitems_out": int(m.sum())})
     return chunks, session, expect, meta
+
+
+# ---------------------------------------------------------------------------
+def scan_projection(nrows=200_000, seed_config=0, null_frac=0.05, a_limit=300, htup_margin=0):
+    """The scan_groupby table and filter, rows projected into kds_dst:
+    (id int8, a int4, b float8 with NULLs, c numeric, a * 2 + g int4).
+    expect maps id -> (a, b or None, c unscaled, a * 2 + g)."""
+    tbl, _, _, _, _ = scan_groupby(nrows=nrows, seed_config=seed_config, null_frac=null_frac,
+                                   a_limit=a_limit)
+    id_ = tbl.col("id").values
+    a, g = tbl.col("a").values, tbl.col("g").values
+    b, bnull = tbl.col("b").values, tbl.col("b").nulls
+    typmod_c = numeric_typmod(12, 2)
+    vid, va, vb, vc, vg = (Var(0, 1, "int8"), Var(0, 2, "int4"), Var(0, 3, "float8"),
+                           Var(0, 4, "numeric", typmod_c), Var(0, 5, "int4"))
+    sb = SessionBuilder(0, DEVTASK_SCAN | DEVKIND_GPU)
+    session = sb.build(
+        scan_quals=Func("int4lt", [va, Const("int4", a_limit)], "bool"),
+        projection=[vid, va, vb, vc,
+                    Func("int4pl", [Func("int4mul", [va, Const("int4", 2)], "int4"), vg], "int4")],
+        htup_margin=htup_margin)
+    m = a < a_limit
+    expect = {}
+    for i in np.flatnonzero(m):
+        expect[int(id_[i])] = (int(a[i]), None if bnull[i] else float(b[i]), int(a[i]) * 2 + int(g[i]))
+    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum())}
+    return tbl, session, expect, meta
+
+
+def join_projection(nfact=60_000, ndim1=3_000, ndim2=400, seed_config=1, flag_limit=3,
+                    dim1_copies=1, miss_frac=0.0, key_stride=1):
+    """The join_groupby tables and joins, rows projected into kds_dst:
+    (fk1 int4, qty * price int8, region text, flag int2), one row per fact
+    row and matching dim1 copy.  Returns (fact, session, kmrels, meta);
+    meta["rows"] is the sorted list of expected value tuples."""
+    fact, _, kmrels, _, meta = join_groupby(nfact=nfact, ndim1=ndim1, ndim2=ndim2,
+                                             seed_config=seed_config, flag_limit=flag_limit,
+                                             key_stride=key_stride, dim1_copies=dim1_copies,
+                                             miss_frac=miss_frac, with_rows=True)
+    f_fk1, f_fk2, f_qty, f_price = (Var(0, 1, "int4"), Var(0, 2, "int4"),
+                                    Var(0, 3, "int4"), Var(0, 4, "int8"))
+    d1_pk, d1_region = Var(1, 1, "int4"), Var(1, 2, "text")
+    d2_pk, d2_flag = Var(2, 1, "int4"), Var(2, 2, "int2")
+    sb = SessionBuilder(2, DEVTASK_JOIN | DEVKIND_GPU)
+    session = sb.build(
+        joins=[([f_fk1], [Func("int4eq", [f_fk1, d1_pk], "bool")], []),
+               ([f_fk2], [Func("int4eq", [f_fk2, d2_pk], "bool")],
+                [Func("int24lt", [d2_flag, Const("int4", flag_limit)], "bool")])],
+        projection=[f_fk1, Func("int48mul", [f_qty, f_price], "int8"), d1_region, d2_flag])
+    return fact, session, kmrels, meta

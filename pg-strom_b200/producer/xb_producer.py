@@ -837,14 +837,43 @@ class SessionBuilder:
         return bytes(buf.b)
 
     # -- the whole session --
+    def build_projection(self, tlist, depth):
+        """Projection kexp (codegen_build_projection, codegen.c:3880-3950):
+        one SaveExpr per target entry into a kvars slot, skipped when an
+        earlier entry already saved into the same slot
+        (try_inject_projection_expression, codegen.c:3412-3437);
+        u.proj.slot_id[] names each output attribute's slot."""
+        nattrs = len(tlist)
+        head_sz = maxalign(48 + 2 * nattrs)
+        buf = _Buf()
+        buf.b += bytearray(head_sz)
+        slots, nargs = [], 0
+        for e in tlist:
+            pos = len(buf.b)
+            d = self.emit_save(buf, e, depth)
+            if d.slot in slots:
+                del buf.b[pos:]
+            else:
+                nargs += 1
+            slots.append(d.slot)
+        head = _kexp_head(TOP("int4"), FOP("Projection"), nargs, head_sz) + \
+            struct.pack("<Ii", 0, nattrs) + struct.pack("<%dH" % nattrs, *slots)
+        buf.b[:len(head)] = head
+        buf.finish_kexp(0)
+        return bytes(buf.b)
+
     def build(self, *, scan_quals=None, joins=(), groupby_keys=(), aggs=(),
-              ngroups_estimate=100.0, final_tlist=None) -> bytes:
+              ngroups_estimate=100.0, final_tlist=None, projection=None,
+              htup_margin=0) -> bytes:
         """joins: list of (outer_hash_keys, join_quals, other_quals) for
         depth 1..n.  groupby_keys: list of Expr; aggs: list of Agg.  The
         partial-aggregation target list is aggs then keys (gpu_preagg.c:
-        2080-2097)."""
+        2080-2097).  projection: list of Expr written as KDS_FORMAT_ROW rows
+        (a scan/join without GROUP BY); htup_margin is
+        gpusort_htup_margin."""
         nrels = self.nrels
         blobs = {}
+        self.htup_margin = htup_margin
         if scan_quals is not None:
             blobs["scan"] = self.build_expr(scan_quals, 0)
         jq, hv = {}, {}
@@ -936,6 +965,11 @@ class SessionBuilder:
             buf.b[:len(head)] = head
             buf.finish_kexp(0)
             blobs["actions"] = bytes(buf.b)
+        if projection:
+            blobs["projection"] = self.build_projection(projection, gdepth)
+            dt = Table("kds_dst", [Column(f"c{i}", e.typ, getattr(e, "typmod", -1))
+                                   for i, e in enumerate(projection)], 0)
+            blobs["kds_dst"] = bytes(dt.kds_header("r", 0))
         # LoadVars / MoveVars packed
         lv = {d: self.build_loadvars(d) for d in range(0, nrels + 1)}
         lv = {d: b for d, b in lv.items() if b is not None}
@@ -976,7 +1010,8 @@ class SessionBuilder:
                                 d.offset, 0, 0, 0)
         offs["kvars"] = out.append_aligned(desc) if desc else 0
         for key in ("loadvars", "movevars", "scan", "joinquals", "hashvalues",
-                    "keyhash", "keyload", "keycomp", "actions", "kds_final"):
+                    "keyhash", "keyload", "keycomp", "actions", "kds_final",
+                    "projection", "kds_dst"):
             b = blobs.get(key)
             offs[key] = out.append_aligned(b) if b else 0
         poffs = []
@@ -987,9 +1022,12 @@ class SessionBuilder:
                          typealign(16, self.kvecs_usage), self.nrels + 1, 0, 0, self.flags)
         struct.pack_into("<q", b, 40, -1)
         struct.pack_into("<IIIIIIIIIIII", b, 48, offs["loadvars"], offs["movevars"], offs["scan"],
-                         offs["joinquals"], offs["hashvalues"], 0, 0, offs["keyhash"], offs["keyload"],
+                         offs["joinquals"], offs["hashvalues"], 0, offs["projection"], offs["keyhash"],
+                         offs["keyload"],
                          offs["keycomp"], offs["actions"], 0)
+        struct.pack_into("<I", b, 128, offs["kds_dst"])
         struct.pack_into("<I", b, 156, offs["kds_final"])
+        struct.pack_into("<I", b, 168, getattr(self, "htup_margin", 0))
         struct.pack_into("<If", b, 160, 0, float(ngroups_estimate))
         struct.pack_into("<I", b, 188, nparams)
         for i, p in enumerate(poffs):

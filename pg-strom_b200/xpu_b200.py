@@ -46,6 +46,7 @@ def lib():
         L.xpuB200Shutdown.argtypes = [P]
         L.xpuB200OpenSession.argtypes = [P, P, U64, P, U64, ctypes.POINTER(P), EB]
         L.xpuB200ExecTask.argtypes = [P, P, I, P, EB]
+        L.xpuB200ExecTaskDst.argtypes = [P, P, I, P, U64, I, ctypes.POINTER(U64), P, EB]
         L.xpuB200Final.argtypes = [P, P, U64, ctypes.POINTER(U64), P, EB]
         L.xpuB200CloseSession.argtypes = [P]
         L.xpuB200HandleCommand.argtypes = [P, ctypes.POINTER(P), P, P, U64, P, U64]
@@ -145,6 +146,29 @@ class Session:
         if rc:
             raise XpuB200Error(rc, e)
         return parse_results(res)
+
+    def exec_dst(self, kds, dst_size=1 << 20, on_device=False):
+        """Run one chunk of a projection session.  Returns (kds_dst bytes,
+        results, retried): kds_dst is dst_size bytes, or the size the
+        library asked for when the rows did not fit (SUSPEND_NO_SPACE,
+        then the chunk runs again)."""
+        retried = False
+        while True:
+            res = results_buffer(self.nrels)
+            struct.pack_into("<I", res, 92, self.nrels)
+            e = KernErrorbuf()
+            req = ctypes.c_uint64()
+            dst = np.zeros(dst_size, dtype=np.uint8)
+            p = ctypes.c_void_p(kds) if on_device else _ptr(kds)
+            rc = lib().xpuB200ExecTaskDst(self.h, p, 1 if on_device else 0, _ptr(dst), dst.nbytes, 0,
+                                          ctypes.byref(req), _ptr(res), ctypes.byref(e))
+            if rc == ord("d") and not retried:
+                dst_size = (req.value + 7) & ~7
+                retried = True
+                continue
+            if rc:
+                raise XpuB200Error(rc, e)
+            return dst, parse_results(res), retried
 
     def time_exec(self, dptr, niters):
         ms = ctypes.c_double()
