@@ -137,6 +137,31 @@ int  xpuB200FinalNoAlloc(xpuB200Session *sess, void *kds_final_dev, uint64_t buf
 void xpuB200CloseSession(xpuB200Session *sess);
 
 /*
+ * Mixed batches (the batched form of many sessions' XpuTaskExec): chunk
+ * commands of different sessions, each a device-resident chunk of its own
+ * session, run together in ONE persistent kernel fed from a device work
+ * queue.  CTAs are sent to commands largest first, several to a large one;
+ * each claims the command's units dynamically, runs the command's own
+ * bytecode against its own group table, and moves on.  A run is captured
+ * once as a CUDA graph (status reset, kernel, status read-back) and
+ * replayed by every xpuB200MixExec / xpuB200MixTime.
+ * xpuB200MixExec fills results[i] and errs[i] per command (either array
+ * may be NULL) and returns 0, or the first command error.  Each command's
+ * groups accumulate in its session, as with xpuB200ExecTask.  No
+ * counterpart in the reference, whose service launches one kernel per
+ * command (__gpuservLaunchGpuTaskExecKernel, gpu_service.c:3760-4003).
+ */
+typedef struct xpuB200Mix xpuB200Mix;
+int  xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess,
+                      const kern_data_store *const *kds_dev, xpuB200Mix **p_mix,
+                      kern_errorbuf *err);
+int  xpuB200MixExec(xpuB200Mix *mix, kern_exec_results *const *results, kern_errorbuf *errs);
+int  xpuB200MixTime(xpuB200Mix *mix, int niters, double *p_msec, kern_errorbuf *err);
+int  xpuB200MixInfo(const xpuB200Mix *mix, uint64_t *p_bytes, uint64_t *p_units,
+                    uint32_t *p_items, int *p_grid);
+void xpuB200MixDestroy(xpuB200Mix *mix);
+
+/*
  * Whole-command entry point for a service loop: handles the three command
  * tags gpuservGpuWorkerMain dispatches (gpu_service.c:5951-5964):
  *   XpuCommandTag__OpenSession  -> *p_sess is created (kmrels may be NULL)

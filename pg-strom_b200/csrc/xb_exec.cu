@@ -24,6 +24,7 @@
  */
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
+#include <algorithm>
 #include <mutex>
 #include <vector>
 #include <string>
@@ -562,10 +563,12 @@ xb_fetch_batch(const XbExecArgs &args, const xb_plan *plan, const XbSrcMeta *met
 #define XB_ST_ENTER     1
 #define XB_ST_PROBE     2
 
-__global__ void __launch_bounds__(XB_BLOCK, XB_MIN_BLOCKS)
-xb_exec_kernel(XbExecArgs args)
+/* one launch's (or one mixed-launch command's) work for this CTA; ends
+ * with the CTA's counters and shared group table flushed, without a final
+ * barrier */
+__device__ __forceinline__ void
+xb_exec_body(const XbExecArgs &args, char *smem)
 {
-    extern __shared__ __align__(16) char smem[];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
 
@@ -754,6 +757,50 @@ xb_exec_kernel(XbExecArgs args)
                 atomicOr(&gt->overflow, 1u);
             }
         }
+    }
+}
+
+__global__ void __launch_bounds__(XB_BLOCK, XB_MIN_BLOCKS)
+xb_exec_kernel(const __grid_constant__ XbExecArgs args)
+{
+    extern __shared__ __align__(16) char smem[];
+    xb_exec_body(args, smem);
+}
+
+/*
+ * Mixed launch: commands of many sessions (each one chunk, its own plan,
+ * group table and status) in one persistent kernel fed from a device work
+ * queue.  Work item i sends a CTA to command items[i]: it stages that
+ * command's plan and column layout, claims the command's units
+ * dynamically with the other CTAs that joined it until none is left,
+ * merges its shared group table into the command's table and takes the
+ * next item.  A large command is listed several times so that several CTAs
+ * join it; items are ordered largest command first.
+ */
+struct XbMixArgs {
+    const XbExecArgs *cmds;
+    const uint32_t   *items;
+    uint32_t          nitems;
+    uint32_t         *cursor;       /* next item (zero at launch) */
+};
+
+__global__ void __launch_bounds__(XB_BLOCK, XB_MIN_BLOCKS)
+xb_mixed_kernel(const __grid_constant__ XbMixArgs m)
+{
+    extern __shared__ __align__(16) char smem[];
+    __shared__ XbExecArgs cmd;
+    __shared__ uint32_t item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            item = atomicAdd(m.cursor, 1u);
+            if (item < m.nitems)
+                cmd = m.cmds[m.items[item]];
+        }
+        __syncthreads();
+        if (item >= m.nitems)
+            break;
+        xb_exec_body(cmd, smem);
+        __syncthreads();
     }
 }
 
@@ -1311,6 +1358,7 @@ struct xpuB200Device {
     int             dindex;
     int             nsm;
     uint64_t        hbm_budget;
+    size_t          smem_optin;     /* dynamic shared memory a CTA may opt in to */
     cudaStream_t    stream;
 };
 
@@ -1427,6 +1475,19 @@ xpuB200Init(int cuda_dindex, uint64_t hbm_budget, xpuB200Device **p_dev, kern_er
         hbm_budget = (uint64_t)(fr * 0.9);
     }
     dev->hbm_budget = hbm_budget;
+    /* the kernels shared by all sessions opt in to the whole of shared
+     * memory once, so that no session lowers another's limit */
+    dev->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaFuncSetAttribute(xb_exec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev->smem_optin) != cudaSuccess ||
+        cudaFuncSetAttribute(xb_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(dev->smem_optin - sizeof(XbExecArgs) - 16)) != cudaSuccess ||
+        cudaFuncSetAttribute(xb_build_inner, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(dev->smem_optin - sizeof(XbCol) * XB_MAX_COLS)) != cudaSuccess) {
+        delete dev;
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cannot opt in to %zu bytes of shared memory",
+                      (size_t)prop.sharedMemPerBlockOptin);
+    }
     cudaError_t rc = cudaStreamCreateWithFlags(&dev->stream, cudaStreamNonBlocking);
     if (rc != cudaSuccess) {
         delete dev;
@@ -1607,8 +1668,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         if (grid < 1) grid = 1;
         if (grid > dev->nsm * 8) grid = dev->nsm * 8;
         const size_t bsmem = plan->inner[d].build_qual.count ? (size_t)XB_WARPS * XB_REGS_BYTES(plan->nregs) : 0;
-        if (bsmem > 48 * 1024 &&
-            cudaFuncSetAttribute(xb_build_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem) != cudaSuccess)
+        if (bsmem + sizeof(XbCol) * XB_MAX_COLS > dev->smem_optin)
             FAIL(ERRCODE_DEVICE_FATAL, "inner build needs %zu bytes of shared memory", bsmem);
         xb_build_inner<<<grid, XB_BLOCK, bsmem, st>>>(ba);
     }
@@ -1717,8 +1777,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
                                                  sizeof(xb_insn) * (size_t)plan->ninsns);
     s->smem_bytes = s->plan_bytes + PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) +
                     (size_t)s->sm_cap * plan->gent_size + (size_t)XB_WARPS * s->warp_bytes;
-    if (cudaFuncSetAttribute(xb_exec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)s->smem_bytes) != cudaSuccess)
+    if (s->smem_bytes > dev->smem_optin)
         FAIL(ERRCODE_DEVICE_FATAL, "dynamic shared memory of %zu bytes not available", s->smem_bytes);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_exec_kernel, XB_BLOCK, s->smem_bytes);
@@ -1767,6 +1826,8 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     a.warp_bytes = s->warp_bytes;
     a.dst = s->launch_dst;
     a.dst_len = s->launch_dst_len;
+    a.dyn_only = 0;
+    a.__pad = 0;
     a.gt = s->d_gt;
     a.st = s->d_status;
     /* the session-specialised kernel of this format, built on first use */
@@ -1873,10 +1934,10 @@ static int xb_wait_status(xpuB200Session *s, kern_errorbuf *err)
     return 0;
 }
 
-/* add a finished launch's statistics to the session and to *results */
-static void xb_account(xpuB200Session *s, kern_exec_results *results)
+/* add a finished launch's statistics (status hs) to the session and to
+ * *results */
+static void xb_account_status(xpuB200Session *s, const xb_status *hs, kern_exec_results *results)
 {
-    const xb_status *hs = s->h_status;
     s->total_raw += hs->nitems_raw;
     s->total_in += hs->nitems_in;
     s->total_out += hs->nitems_out;
@@ -1894,6 +1955,11 @@ static void xb_account(xpuB200Session *s, kern_exec_results *results)
             results->stats[d - 1].nitems_out = (uint32_t)hs->nitems_depth[d];
         }
     }
+}
+
+static void xb_account(xpuB200Session *s, kern_exec_results *results)
+{
+    xb_account_status(s, s->h_status, results);
 }
 
 static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_errorbuf *err)
@@ -2505,6 +2571,252 @@ xpuB200BatchDestroy(xpuB200Batch *b)
     cudaSetDevice(b->sess->dev->dindex);
     cudaFree(b->d_tasks);
     delete b;
+}
+
+/* ================================================================
+ * mixed batches: chunk commands of many sessions in one launch
+ * ================================================================ */
+struct xpuB200Mix {
+    xpuB200Device  *dev;
+    uint32_t        ncmds = 0;
+    std::vector<xpuB200Session *> sess;
+    xb_task        *d_tasks = nullptr;
+    XbExecArgs     *d_cmds = nullptr;
+    uint32_t       *d_items = nullptr;
+    uint32_t        nitems = 0;
+    uint32_t       *d_cursor = nullptr;
+    xb_status      *d_status = nullptr;
+    xb_status      *h_status = nullptr;     /* pinned */
+    cudaStream_t    stream = nullptr;
+    cudaGraph_t     graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t     ev0 = nullptr, ev1 = nullptr;
+    size_t          smem = 0;
+    int             grid = 0;
+    uint64_t        bytes = 0, units = 0;
+};
+
+/* units one CTA takes of a command before another CTA is sent to join it */
+#define XB_MIX_JOIN_UNITS   16
+
+static void xb_mix_free(xpuB200Mix *m)
+{
+    if (!m) return;
+    cudaSetDevice(m->dev->dindex);
+    if (m->gexec) cudaGraphExecDestroy(m->gexec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    if (m->ev0) cudaEventDestroy(m->ev0);
+    if (m->ev1) cudaEventDestroy(m->ev1);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    cudaFree(m->d_tasks);
+    cudaFree(m->d_cmds);
+    cudaFree(m->d_items);
+    cudaFree(m->d_cursor);
+    cudaFree(m->d_status);
+    if (m->h_status) cudaFreeHost(m->h_status);
+    delete m;
+}
+
+extern "C" int
+xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess,
+                 const kern_data_store *const *kds_dev, xpuB200Mix **p_mix, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    *p_mix = nullptr;
+    if (!dev || !sess || !kds_dev || ncmds == 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid mixed batch arguments");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    std::vector<xb_task> tasks(ncmds);
+    std::vector<uint64_t> units(ncmds);
+    size_t smem = 0;
+    uint64_t bytes = 0, total_units = 0;
+    for (uint32_t i = 0; i < ncmds; i++) {
+        xpuB200Session *s = sess[i];
+        if (!s || s->dev != dev)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "command %u: no session on this GPU", i);
+        if (s->h_plan->has_proj)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "command %u: projection sessions run through xpuB200ExecTaskDst", i);
+        if (((uintptr_t)kds_dev[i] & 7) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "command %u: chunk is not 8-byte aligned", i);
+        kern_data_store head;
+        XB_CUDA(cudaMemcpy(&head, kds_dev[i], offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+        std::vector<char> hb(KDS_HEAD_LENGTH(&head));
+        XB_CUDA(cudaMemcpy(hb.data(), kds_dev[i], hb.size(), cudaMemcpyDeviceToHost), err);
+        const kern_data_store *h = (const kern_data_store *)hb.data();
+        int rc = xb_check_kds(h, err);
+        if (rc) return rc;
+        tasks[i].kds = kds_dev[i];
+        tasks[i].unit_base = 0;
+        tasks[i].nunits = xb_chunk_units(h);
+        tasks[i].format = (uint32_t)h->format;
+        units[i] = tasks[i].nunits;
+        total_units += units[i];
+        bytes += h->length;
+        if (s->smem_bytes > smem)
+            smem = s->smem_bytes;
+    }
+    if (smem + sizeof(XbExecArgs) + 16 > dev->smem_optin)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch needs %zu bytes of shared memory", smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_mixed_kernel, XB_BLOCK, smem);
+    if (per_sm < 1)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed kernel does not fit on an SM (%zu bytes)", smem);
+    const int grid = per_sm * dev->nsm;
+    /* work items: the largest command first, each listed once per
+     * XB_MIX_JOIN_UNITS of its units (at most once per CTA) */
+    std::vector<uint32_t> order(ncmds);
+    for (uint32_t i = 0; i < ncmds; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return units[a] > units[b]; });
+    std::vector<uint32_t> items;
+    for (uint32_t i : order) {
+        uint64_t k = (units[i] + XB_MIX_JOIN_UNITS - 1) / XB_MIX_JOIN_UNITS;
+        if (k < 1) k = 1;
+        if (k > (uint64_t)grid) k = grid;
+        for (uint64_t j = 0; j < k; j++) items.push_back(i);
+    }
+    xpuB200Mix *m = new xpuB200Mix();
+    m->dev = dev;
+    m->ncmds = ncmds;
+    m->sess.assign(sess, sess + ncmds);
+    m->nitems = (uint32_t)items.size();
+    m->smem = smem;
+    m->grid = grid;
+    m->bytes = bytes;
+    m->units = total_units;
+    auto fail = [&](const char *what) {
+        xb_mix_free(m);
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed batch: %s", what);
+    };
+    if (cudaMalloc((void **)&m->d_tasks, sizeof(xb_task) * ncmds) != cudaSuccess ||
+        cudaMalloc((void **)&m->d_cmds, sizeof(XbExecArgs) * ncmds) != cudaSuccess ||
+        cudaMalloc((void **)&m->d_items, sizeof(uint32_t) * items.size()) != cudaSuccess ||
+        cudaMalloc((void **)&m->d_cursor, 16) != cudaSuccess ||
+        cudaMalloc((void **)&m->d_status, sizeof(xb_status) * ncmds) != cudaSuccess ||
+        cudaMallocHost((void **)&m->h_status, sizeof(xb_status) * ncmds) != cudaSuccess)
+        return fail("out of memory");
+    std::vector<XbExecArgs> cmds(ncmds);
+    for (uint32_t i = 0; i < ncmds; i++) {
+        xpuB200Session *s = sess[i];
+        XbExecArgs &a = cmds[i];
+        memset(&a, 0, sizeof(a));
+        a.plan = s->d_plan;
+        a.plan_bytes = s->plan_bytes;
+        a.tasks = m->d_tasks + i;
+        a.ntasks = 1;
+        a.nunits = tasks[i].nunits;
+        a.format = tasks[i].format;
+        a.sm_cap = s->sm_cap;
+        a.warp_bytes = s->warp_bytes;
+        a.gt = s->d_gt;
+        a.st = m->d_status + i;
+        a.dyn_only = 1;
+    }
+    if (cudaMemcpy(m->d_tasks, tasks.data(), sizeof(xb_task) * ncmds, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->d_cmds, cmds.data(), sizeof(XbExecArgs) * ncmds, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->d_items, items.data(), sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail("upload failed");
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&m->ev0) != cudaSuccess || cudaEventCreate(&m->ev1) != cudaSuccess)
+        return fail("stream setup failed");
+    /* one run = clear the statuses and the queue cursor, the persistent
+     * kernel, the statuses back to the host: captured once, replayed */
+    XbMixArgs ma;
+    ma.cmds = m->d_cmds;
+    ma.items = m->d_items;
+    ma.nitems = m->nitems;
+    ma.cursor = m->d_cursor;
+    if (cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail("stream capture failed");
+    cudaMemsetAsync(m->d_status, 0, sizeof(xb_status) * ncmds, m->stream);
+    cudaMemsetAsync(m->d_cursor, 0, 16, m->stream);
+    xb_mixed_kernel<<<grid, XB_BLOCK, smem, m->stream>>>(ma);
+    cudaMemcpyAsync(m->h_status, m->d_status, sizeof(xb_status) * ncmds, cudaMemcpyDeviceToHost, m->stream);
+    if (cudaStreamEndCapture(m->stream, &m->graph) != cudaSuccess ||
+        cudaGraphInstantiate(&m->gexec, m->graph, 0) != cudaSuccess)
+        return fail("graph capture failed");
+    *p_mix = m;
+    return 0;
+}
+
+/* lock the distinct sessions of a mixed batch, in address order */
+static std::vector<std::unique_lock<std::mutex>> xb_mix_lock(xpuB200Mix *m)
+{
+    std::vector<xpuB200Session *> u(m->sess);
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (xpuB200Session *s : u)
+        locks.emplace_back(s->lock);
+    return locks;
+}
+
+extern "C" int
+xpuB200MixExec(xpuB200Mix *m, kern_exec_results *const *results, kern_errorbuf *errs)
+{
+    if (!m)
+        return ERRCODE_DEVICE_ERROR;
+    for (uint32_t i = 0; errs && i < m->ncmds; i++)
+        xb_clear_error(&errs[i]);
+    auto locks = xb_mix_lock(m);
+    kern_errorbuf *e0 = errs;
+    XB_CUDA(cudaSetDevice(m->dev->dindex), e0);
+    XB_CUDA(cudaGraphLaunch(m->gexec, m->stream), e0);
+    XB_CUDA(cudaStreamSynchronize(m->stream), e0);
+    int first = 0;
+    for (uint32_t i = 0; i < m->ncmds; i++) {
+        const xb_status *hs = &m->h_status[i];
+        if (hs->errcode) {
+            int rc = xb_set_error(errs ? &errs[i] : nullptr, hs->errcode, "xb_mixed_kernel", hs->lineno,
+                                  "%s", xb_msg_text(hs->msg_id));
+            if (!first) first = rc;
+            continue;
+        }
+        xb_account_status(m->sess[i], hs, results ? results[i] : nullptr);
+    }
+    return first;
+}
+
+extern "C" int
+xpuB200MixTime(xpuB200Mix *m, int niters, double *p_msec, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!m)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid mixed batch");
+    auto locks = xb_mix_lock(m);
+    XB_CUDA(cudaSetDevice(m->dev->dindex), err);
+    float total = 0.0f;
+    for (int it = 0; it < niters; it++) {
+        XB_CUDA(cudaEventRecord(m->ev0, m->stream), err);
+        XB_CUDA(cudaGraphLaunch(m->gexec, m->stream), err);
+        XB_CUDA(cudaEventRecord(m->ev1, m->stream), err);
+        XB_CUDA(cudaStreamSynchronize(m->stream), err);
+        for (uint32_t i = 0; i < m->ncmds; i++)
+            if (m->h_status[i].errcode)
+                return xb_set_error(err, m->h_status[i].errcode, "xb_mixed_kernel", m->h_status[i].lineno,
+                                    "command %u: %s", i, xb_msg_text(m->h_status[i].msg_id));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, m->ev0, m->ev1);
+        total += ms;
+    }
+    *p_msec = niters > 0 ? total / niters : 0.0;
+    return 0;
+}
+
+extern "C" int
+xpuB200MixInfo(const xpuB200Mix *m, uint64_t *p_bytes, uint64_t *p_units, uint32_t *p_items, int *p_grid)
+{
+    if (!m) return ERRCODE_DEVICE_ERROR;
+    if (p_bytes) *p_bytes = m->bytes;
+    if (p_units) *p_units = m->units;
+    if (p_items) *p_items = m->nitems;
+    if (p_grid) *p_grid = m->grid;
+    return 0;
+}
+
+extern "C" void
+xpuB200MixDestroy(xpuB200Mix *m)
+{
+    xb_mix_free(m);
 }
 
 extern "C" int

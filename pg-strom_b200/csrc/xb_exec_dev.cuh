@@ -348,6 +348,9 @@ struct XbExecArgs {
     uint64_t        dst_len;
     xb_gtable      *gt;
     xb_status      *st;
+    uint32_t        dyn_only;       /* claim every unit dynamically (CTAs join
+                                     * the launch at any time: mixed launches) */
+    uint32_t        __pad;
 };
 
 /* per-warp counters, in shared memory */
@@ -491,7 +494,7 @@ xb_src_start(const XbExecArgs &args, XbSrc &s, uint32_t lane)
     }
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
     const uint64_t wid = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    const uint64_t share = (args.nunits * 3 / 5) / warps;
+    const uint64_t share = args.dyn_only ? 0 : (args.nunits * 3 / 5) / warps;
     s.static_base = share * warps;
     /* the lane-0 fields are written by lane 0 only (the state may live in
      * shared memory, read back by every lane) */

@@ -11,6 +11,9 @@ the benchmark configurations (test and benchmark infrastructure).
                    1..10000 into dim2(pk int4, flag int2 in 0..4);
                    JOIN dim1, dim2 WHERE flag < 3 GROUP BY region ->
                    sum(qty*price), count(*)
+  mixed_commands   batched chunk commands on the scan_groupby schema: chunk
+                   sizes log-uniform, selectivity (a < t) uniform, group
+                   counts (the domain of g) log-uniform, one session each
   scan_projection  the scan_groupby table, WHERE a < 300 projected to
                    (id, a, b, c, a * 2 + g) rows (no GROUP BY)
   join_projection  the join_groupby tables, projected to
@@ -22,6 +25,7 @@ bytecode decoding), so the oracle itself can be pinned against them.
 """
 import numpy as np
 
+from xb_final import Approx
 from xb_producer import (Table, Column, Var, Const, Func, Agg, SessionBuilder,
                          encode_numeric_array, encode_text_array, encode_text_from_dict,
                          hash_u32_array, hash_merge_array, kern_multirels, numeric_typmod)
@@ -45,14 +49,16 @@ def host_join_hash_int4(keys: np.ndarray) -> np.ndarray:
 
 
 # ---------------------------------------------------------------------------
-def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300):
+def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ngroups=64):
+    """The plain scan + filter + group-by table; ngroups sets the domain of
+    g (64 in the benchmark configuration)."""
     r = rng_for(seed_config, 0)
     id_ = np.arange(nrows, dtype=np.int64)
     a = r.integers(0, 1000, nrows, dtype=np.int32)
     b = r.standard_normal(nrows)
     bnull = r.random(nrows) < null_frac
     c_unscaled = r.integers(0, 1_000_000, nrows, dtype=np.int64)
-    g = r.integers(0, 64, nrows, dtype=np.int32)
+    g = r.integers(0, ngroups, nrows, dtype=np.int32)
     typmod_c = numeric_typmod(12, 2)
     tbl = Table("t0", [
         Column("id", "int8", values=id_),
@@ -71,27 +77,26 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300):
               Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")),
               Agg("PSUM_NUMERIC", vc, typmod_c),
               Agg("PAVG_FP", vb)],
-        ngroups_estimate=64.0)
+        ngroups_estimate=float(ngroups))
     # expected partial states per group, straight from the arrays
     m = a < a_limit
-    expect = {}
-    cnt = np.bincount(g[m], minlength=64)
-    suma = np.bincount(g[m], weights=None, minlength=64)
-    sa = np.zeros(64, dtype=np.int64)
-    np.add.at(sa, g[m], a[m].astype(np.int64))
-    sc = np.zeros(64, dtype=object)
-    sc[:] = 0
-    for k in range(64):
-        sc[k] = int(c_unscaled[m & (g == k)].sum())
+    gm = g[m]
+    cnt = np.bincount(gm, minlength=ngroups)
+    sa = np.zeros(ngroups, dtype=np.int64)
+    np.add.at(sa, gm, a[m].astype(np.int64))
+    sc = np.zeros(ngroups, dtype=np.int64)
+    np.add.at(sc, gm, c_unscaled[m])
     mb = m & ~bnull
-    sb_ = np.zeros(64, dtype=np.float64)
-    np.add.at(sb_, g[mb], b[mb])                 # sequential, row order
-    nb = np.bincount(g[mb], minlength=64)
-    for k in range(64):
-        if cnt[k] == 0:
-            continue
+    sb_ = np.zeros(ngroups, dtype=np.float64)
+    np.add.at(sb_, g[mb], b[mb])                 # unbuffered: row order per group
+    nb = np.bincount(g[mb], minlength=ngroups)
+    sab = np.zeros(ngroups, dtype=np.float64)
+    np.add.at(sab, g[mb], np.abs(b[mb]))
+    expect = {}
+    for k in np.flatnonzero(cnt).tolist():
         expect[(k,)] = {"nrows": int(cnt[k]), "sum_a": (int(cnt[k]), int(sa[k])),
-                        "sum_c": (int(cnt[k]), sc[k], 2), "avg_b": (int(nb[k]), float(sb_[k]))}
+                        "sum_c": (int(cnt[k]), int(sc[k]), 2),
+                        "avg_b": (int(nb[k]), Approx(float(sb_[k]), float(sab[k])))}
     meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()),
             "agg_names": ["nrows", "sum_a", "sum_c", "avg_b"], "nkeys": 1}
     return tbl, session, None, expect, meta
@@ -317,3 +322,33 @@ def join_projection(nfact=60_000, ndim1=3_000, ndim2=400, seed_config=1, flag_li
                 [Func("int24lt", [d2_flag, Const("int4", flag_limit)], "bool")])],
         projection=[f_fk1, Func("int48mul", [f_qty, f_price], "int8"), d1_region, d2_flag])
     return fact, session, kmrels, meta
+
+
+# ---------------------------------------------------------------------------
+HEAP_ROW_BYTES = 68          # scan_groupby tuple + line pointer, in heap pages
+
+
+def mixed_commands(ncmds=256, min_bytes=64 << 10, max_bytes=64 << 20, min_sel=0.001, max_sel=0.9,
+                   max_groups=1_000_000, seed_config=3):
+    """Chunk commands on the scan_groupby schema, each its own session and
+    one KDS_FORMAT_BLOCK chunk: chunk bytes log-uniform in [min_bytes,
+    max_bytes], selectivity of a < t uniform in [min_sel, max_sel], group
+    count (domain of g) log-uniform in [1, max_groups].  Returns a list of
+    dicts (chunk, session, truth, meta, params)."""
+    r = rng_for(seed_config, 0)
+    out = []
+    for i in range(ncmds):
+        nbytes = float(np.exp(r.uniform(np.log(min_bytes), np.log(max_bytes))))
+        sel = float(r.uniform(min_sel, max_sel))
+        groups = int(np.exp(r.uniform(0.0, np.log(max_groups))))
+        nrows = max(1, int(nbytes // HEAP_ROW_BYTES))
+        a_limit = max(1, int(round(sel * 1000)))
+        tbl, sess, _, expect, meta = scan_groupby(nrows=nrows, seed_config=1000 + i, a_limit=a_limit,
+                                                  ngroups=max(1, groups))
+        chunks = tbl.block_chunks(pages_per_chunk=nrows // 60 + 2)   # >= 60 rows fill a page
+        assert len(chunks) == 1
+        chunk = chunks[0]
+        truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
+        out.append({"chunk": chunk, "session": sess, "truth": truth, "meta": meta,
+                    "params": {"rows": nrows, "a_limit": a_limit, "groups": groups}})
+    return out

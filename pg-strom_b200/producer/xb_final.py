@@ -125,9 +125,21 @@ def decode_kds_final(buf, session: bytes):
     return out
 
 
+class Approx(float):
+    """An expected float sum with the sum of its terms' magnitudes: a sum
+    whose terms cancel is only defined to rtol of that magnitude (the
+    row-ordered FP64 sum itself carries n * eps * sum|x| of error)."""
+
+    def __new__(cls, value, scale):
+        obj = super().__new__(cls, value)
+        obj.scale = float(scale)
+        return obj
+
+
 def compare_groups(got, want, rtol=1e-12):
-    """Integer / numeric states exact, float states within rtol relative.
-    Returns a list of mismatch descriptions (empty when equal)."""
+    """Integer / numeric states exact, float states within rtol relative
+    (relative to the sum of magnitudes when the expected value is an
+    Approx).  Returns a list of mismatch descriptions (empty when equal)."""
     errs = []
     if set(got) != set(want):
         errs.append(f"group keys differ: only-got={sorted(set(got) - set(want))[:5]} "
@@ -142,7 +154,8 @@ def compare_groups(got, want, rtol=1e-12):
             if isinstance(y, tuple):
                 for xe, ye in zip(x, y):
                     if isinstance(ye, float):
-                        if not (abs(xe - ye) <= rtol * max(abs(ye), 1e-300) or xe == ye):
+                        tol = rtol * max(abs(ye), getattr(ye, "scale", 0.0), 1e-300)
+                        if not (abs(xe - ye) <= tol or xe == ye):
                             errs.append(f"{k}[{j}]: float {xe!r} vs {ye!r}")
                     elif xe != ye:
                         errs.append(f"{k}[{j}]: {xe!r} vs {ye!r}")

@@ -58,6 +58,12 @@ def lib():
         L.xpuB200BatchExec.argtypes = [P, P, EB]
         L.xpuB200BatchTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
         L.xpuB200BatchDestroy.argtypes = [P]
+        L.xpuB200MixCreate.argtypes = [P, ctypes.c_uint32, P, P, ctypes.POINTER(P), EB]
+        L.xpuB200MixExec.argtypes = [P, P, P]
+        L.xpuB200MixTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
+        L.xpuB200MixInfo.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64),
+                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(I)]
+        L.xpuB200MixDestroy.argtypes = [P]
         L.xpuB200SessionInfo.argtypes = [P, ctypes.c_char_p, U64]
         L.xpuB200HashBytes.argtypes = [P, ctypes.c_uint32]
         L.xpuB200HashBytes.restype = ctypes.c_uint32
@@ -241,4 +247,58 @@ class Batch:
     def close(self):
         if self.h:
             lib().xpuB200BatchDestroy(self.h)
+            self.h = ctypes.c_void_p()
+
+
+class Mix:
+    """Chunk commands of many sessions run as one persistent launch (a
+    captured CUDA graph, replayed by every run)."""
+
+    def __init__(self, dev: Device, sessions, dptrs):
+        self.dev = dev
+        self.sessions = list(sessions)
+        n = len(self.sessions)
+        self.h = ctypes.c_void_p()
+        hs = (ctypes.c_void_p * n)(*[s.h.value for s in self.sessions])
+        ks = (ctypes.c_void_p * n)(*dptrs)
+        e = KernErrorbuf()
+        rc = lib().xpuB200MixCreate(dev.h, n, hs, ks, ctypes.byref(self.h), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+
+    def exec(self):
+        """Returns [(results dict or None, error message or None)] per command."""
+        n = len(self.sessions)
+        bufs = []
+        for s in self.sessions:
+            r = results_buffer(s.nrels)
+            struct.pack_into("<I", r, 92, s.nrels)
+            bufs.append(r)
+        ptrs = (ctypes.c_void_p * n)(*[b.ctypes.data for b in bufs])
+        errs = (KernErrorbuf * n)()
+        lib().xpuB200MixExec(self.h, ptrs, errs)
+        out = []
+        for b, e in zip(bufs, errs):
+            if e.errcode:
+                out.append((None, XpuB200Error(e.errcode, e)))
+            else:
+                out.append((parse_results(b), None))
+        return out
+
+    def time(self, niters):
+        ms = ctypes.c_double()
+        e = KernErrorbuf()
+        rc = lib().xpuB200MixTime(self.h, niters, ctypes.byref(ms), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return ms.value
+
+    def info(self):
+        b, u, it, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_int()
+        lib().xpuB200MixInfo(self.h, ctypes.byref(b), ctypes.byref(u), ctypes.byref(it), ctypes.byref(g))
+        return {"bytes": b.value, "units": u.value, "items": it.value, "grid": g.value}
+
+    def close(self):
+        if self.h:
+            lib().xpuB200MixDestroy(self.h)
             self.h = ctypes.c_void_p()
