@@ -137,6 +137,34 @@ int  xpuB200FinalNoAlloc(xpuB200Session *sess, void *kds_final_dev, uint64_t buf
 void xpuB200CloseSession(xpuB200Session *sess);
 
 /*
+ * Serving form: asynchronous chunk commands with continuous batching.
+ * xpuB200Submit queues one chunk command of a session (kds_src a host
+ * pointer, or a device pointer when kds_src_on_device; a host chunk must
+ * stay valid until its ticket is polled done) and returns a ticket.  The
+ * device keeps up to 4 launches in flight on their own streams: whenever
+ * one is free (checked on every Submit and Poll) the queued commands are
+ * admitted in arrival order while their staging bytes fit the admission
+ * budget; a command of at least alone_units units (heap pages or 1024-row
+ * groups; default 256) runs alone on its session's specialised kernel, the
+ * smaller ones run together in one mixed launch.  xpuB200Poll reports
+ * whether a ticket is done (waiting for it when wait is non-zero) and then
+ * returns its statistics in *results, or its error; a ticket is reported
+ * done once.  Groups accumulate in the session as with xpuB200ExecTask;
+ * xpuB200Final and xpuB200CloseSession first wait for the session's
+ * submitted commands.  xpuB200ServeConfig sets the admission budget in
+ * bytes (default a quarter of the device's budget) and alone_units (0
+ * keeps a value).  Replaces the per-command worker threads of
+ * gpuservGpuWorkerMain (gpu_service.c:5951-5964) with one scheduler per
+ * GPU.
+ */
+int  xpuB200Submit(xpuB200Session *sess, const kern_data_store *kds_src, int kds_src_on_device,
+                   uint64_t *p_ticket, kern_errorbuf *err);
+int  xpuB200Poll(xpuB200Device *dev, uint64_t ticket, int wait, int *p_done,
+                 kern_exec_results *results, kern_errorbuf *err);
+int  xpuB200ServeConfig(xpuB200Device *dev, uint64_t admit_bytes, uint32_t alone_units,
+                        kern_errorbuf *err);
+
+/*
  * Mixed batches (the batched form of many sessions' XpuTaskExec): chunk
  * commands of different sessions, each a device-resident chunk of its own
  * session, run together in ONE persistent kernel fed from a device work

@@ -25,7 +25,9 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 #include <algorithm>
+#include <deque>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 #include <string>
 #include <cstring>
@@ -1360,7 +1362,11 @@ struct xpuB200Device {
     uint64_t        hbm_budget;
     size_t          smem_optin;     /* dynamic shared memory a CTA may opt in to */
     cudaStream_t    stream;
+    struct xb_sched *sched = nullptr; /* asynchronous commands (created by the first submit) */
 };
+
+static void xb_sched_drain_session(xpuB200Session *s);
+static void xb_sched_destroy(xpuB200Device *dev);
 
 struct xpuB200Session {
     xpuB200Device  *dev;
@@ -1392,6 +1398,7 @@ struct xpuB200Session {
     bool            jit_tried[256] = {false};
     void           *jit_fn[256] = {nullptr};
     char            ran_kind[256] = {0};   /* 'j' / 'v': kernel last launched per format */
+    uint32_t        sched_refs = 0;        /* submitted commands not yet finished */
     /* device projection: staging buffer for host kds_dst, and the buffer of
      * the launch in progress */
     char           *d_dst = nullptr;
@@ -1502,6 +1509,7 @@ xpuB200Shutdown(xpuB200Device *dev)
 {
     if (!dev) return;
     cudaSetDevice(dev->dindex);
+    xb_sched_destroy(dev);
     cudaStreamSynchronize(dev->stream);
     cudaStreamDestroy(dev->stream);
     delete dev;
@@ -1799,8 +1807,10 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
 extern "C" void
 xpuB200CloseSession(xpuB200Session *sess)
 {
-    if (sess)
+    if (sess) {
+        xb_sched_drain_session(sess);
         xb_session_free(sess);
+    }
 }
 
 /* units of one chunk (pages, or 1024-row groups) */
@@ -1811,9 +1821,21 @@ static uint32_t xb_chunk_units(const kern_data_store *head)
     return (head->nitems + XB_ROWS_UNIT - 1) / XB_ROWS_UNIT;
 }
 
-/* launch the executor over a device-resident task table */
+/* launch the executor over a device-resident task table, on a stream
+ * with a status of the caller's */
+static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
+                        uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
+                        kern_errorbuf *err);
+
 static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                            uint64_t nunits, uint32_t format, kern_errorbuf *err)
+{
+    return xb_launch_on(s, d_tasks, ntasks, nunits, format, s->dev->stream, s->d_status, err);
+}
+
+static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
+                        uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
+                        kern_errorbuf *err)
 {
     XbExecArgs a;
     a.plan = s->d_plan;
@@ -1829,7 +1851,7 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     a.dyn_only = 0;
     a.__pad = 0;
     a.gt = s->d_gt;
-    a.st = s->d_status;
+    a.st = d_status;
     /* the session-specialised kernel of this format, built on first use */
     void *fn = nullptr;
     if (s->jit_enabled && format < 256) {
@@ -1860,10 +1882,10 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     if (format < 256)
         s->ran_kind[format] = fn ? 'j' : 'v';
     if (fn) {
-        if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem, (void *)s->dev->stream, &a) != 0)
+        if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem, (void *)stream, &a) != 0)
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
     } else {
-        xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, s->dev->stream>>>(a);
+        xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, stream>>>(a);
     }
     cudaError_t rc = cudaGetLastError();
     if (rc != cudaSuccess)
@@ -1934,6 +1956,23 @@ static int xb_wait_status(xpuB200Session *s, kern_errorbuf *err)
     return 0;
 }
 
+/* a finished launch's statistics (status hs) into *results */
+static void xb_fill_results(const xb_status *hs, uint32_t nrels, kern_exec_results *results)
+{
+    if (!results)
+        return;
+    uint32_t cap = results->num_rels;
+    results->nitems_raw = (uint32_t)hs->nitems_raw;
+    results->nitems_in = (uint32_t)hs->nitems_in;
+    results->nitems_out = (uint32_t)hs->nitems_out;
+    results->num_rels = nrels;
+    for (uint32_t d = 1; d <= nrels && d <= cap; d++) {
+        results->stats[d - 1].nitems_roj = 0;
+        results->stats[d - 1].nitems_gist = 0;
+        results->stats[d - 1].nitems_out = (uint32_t)hs->nitems_depth[d];
+    }
+}
+
 /* add a finished launch's statistics (status hs) to the session and to
  * *results */
 static void xb_account_status(xpuB200Session *s, const xb_status *hs, kern_exec_results *results)
@@ -1943,18 +1982,7 @@ static void xb_account_status(xpuB200Session *s, const xb_status *hs, kern_exec_
     s->total_out += hs->nitems_out;
     for (uint32_t d = 1; d <= s->h_plan->nrels; d++)
         s->total_depth[d] += hs->nitems_depth[d];
-    if (results) {
-        uint32_t cap = results->num_rels;
-        results->nitems_raw = (uint32_t)hs->nitems_raw;
-        results->nitems_in = (uint32_t)hs->nitems_in;
-        results->nitems_out = (uint32_t)hs->nitems_out;
-        results->num_rels = s->h_plan->nrels;
-        for (uint32_t d = 1; d <= s->h_plan->nrels && d <= cap; d++) {
-            results->stats[d - 1].nitems_roj = 0;
-            results->stats[d - 1].nitems_gist = 0;
-            results->stats[d - 1].nitems_out = (uint32_t)hs->nitems_depth[d];
-        }
-    }
+    xb_fill_results(hs, s->h_plan->nrels, results);
 }
 
 static void xb_account(xpuB200Session *s, kern_exec_results *results)
@@ -2160,6 +2188,7 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     xb_clear_error(err);
     if (!s)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid Final arguments");
+    xb_sched_drain_session(s);
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
     cudaStream_t st = s->dev->stream;
@@ -2315,6 +2344,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     xb_clear_error(err);
     if (!s)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid FinalNoAlloc arguments");
+    xb_sched_drain_session(s);
     std::lock_guard<std::mutex> g(s->lock);
     std::lock_guard<std::mutex> gs(xb_final_scratch_lock);
     const int dindex = s->dev->dindex;
@@ -2817,6 +2847,491 @@ extern "C" void
 xpuB200MixDestroy(xpuB200Mix *m)
 {
     xb_mix_free(m);
+}
+
+/* ================================================================
+ * serving: asynchronous chunk commands with continuous batching
+ * ================================================================
+ *
+ * xpuB200Submit queues a chunk command of any session; the scheduler keeps
+ * up to XB_SLOTS launches in flight on their own streams.  Whenever a slot
+ * is free (checked on every Submit and Poll), the queued commands are
+ * admitted in arrival order while their staging bytes fit the admission
+ * budget: a large command of a session with a specialised kernel runs
+ * alone on it, the small ones go together into one mixed launch
+ * (xb_mixed_kernel).  Commands that arrive while others are on the GPU are
+ * admitted as slots and memory free up, so their work overlaps on the
+ * device.  A finished command's statistics are added to its session and
+ * kept for xpuB200Poll; its groups are in the session's group table.
+ */
+#define XB_SLOTS            4       /* launches in flight per GPU */
+#define XB_SLOT_CMDS        256     /* commands of one mixed launch */
+#define XB_ALONE_UNITS      256     /* commands of this many units run alone */
+
+struct xb_cmd {
+    uint64_t        ticket;
+    xpuB200Session *s;
+    const kern_data_store *kds;     /* the caller's chunk */
+    int             on_device;
+    uint64_t        length;
+    uint64_t        shift;          /* staging offset that aligns heap pages */
+    uint64_t        units;
+    uint32_t        format;
+    const kern_data_store *d_kds;   /* the chunk on the device, once launched */
+};
+
+struct xb_done {
+    int             rc;             /* 0, or the command's error code */
+    kern_errorbuf   err;
+    xb_status       st;
+    uint32_t        nrels;
+};
+
+struct xb_slot {
+    cudaStream_t    stream = nullptr;
+    cudaEvent_t     done = nullptr;
+    bool            busy = false;
+    bool            alone = false;
+    std::vector<xb_cmd> cmds;
+    uint64_t        staged = 0;     /* admission bytes held by this launch */
+    char           *d_stage = nullptr;
+    uint64_t        stage_cap = 0;
+    xb_status      *d_status = nullptr;
+    xb_status      *h_status = nullptr;     /* pinned */
+    xb_task        *d_tasks = nullptr, *h_tasks = nullptr;
+    XbExecArgs     *d_cmds = nullptr, *h_cmds = nullptr;
+    uint32_t       *d_items = nullptr, *h_items = nullptr;
+    uint32_t        items_cap = 0;
+    uint32_t       *d_cursor = nullptr;
+};
+
+struct xb_sched {
+    std::mutex      lock;
+    uint64_t        next_ticket = 1;
+    std::deque<xb_cmd> pending;
+    xb_slot         slot[XB_SLOTS];
+    std::unordered_map<uint64_t, xb_done> done;
+    uint64_t        admit_bytes = 0;
+    uint64_t        inflight_bytes = 0;
+    uint32_t        alone_units = XB_ALONE_UNITS;
+    int             mix_grid_per_sm[2] = {0, 0};
+};
+
+static void xb_slot_free(xb_slot &sl)
+{
+    if (sl.stream) { cudaStreamSynchronize(sl.stream); cudaStreamDestroy(sl.stream); }
+    if (sl.done) cudaEventDestroy(sl.done);
+    cudaFree(sl.d_stage);
+    cudaFree(sl.d_status);
+    cudaFree(sl.d_tasks);
+    cudaFree(sl.d_cmds);
+    cudaFree(sl.d_items);
+    cudaFree(sl.d_cursor);
+    if (sl.h_status) cudaFreeHost(sl.h_status);
+    if (sl.h_tasks) cudaFreeHost(sl.h_tasks);
+    if (sl.h_cmds) cudaFreeHost(sl.h_cmds);
+    if (sl.h_items) cudaFreeHost(sl.h_items);
+    sl = xb_slot();
+}
+
+static int xb_sched_init(xpuB200Device *dev, kern_errorbuf *err)
+{
+    if (dev->sched)
+        return 0;
+    xb_sched *q = new xb_sched();
+    q->admit_bytes = dev->hbm_budget / 4;
+    for (int i = 0; i < XB_SLOTS; i++) {
+        xb_slot &sl = q->slot[i];
+        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_status, sizeof(xb_status) * XB_SLOT_CMDS) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_status, sizeof(xb_status) * XB_SLOT_CMDS) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_tasks, sizeof(xb_task) * XB_SLOT_CMDS) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_tasks, sizeof(xb_task) * XB_SLOT_CMDS) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_cmds, sizeof(XbExecArgs) * XB_SLOT_CMDS) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_cmds, sizeof(XbExecArgs) * XB_SLOT_CMDS) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_cursor, 16) != cudaSuccess) {
+            for (int j = 0; j <= i; j++)
+                xb_slot_free(q->slot[j]);
+            delete q;
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cannot set up the command scheduler");
+        }
+    }
+    dev->sched = q;
+    return 0;
+}
+
+/* finish the launch of slot sl if its work is done; sched lock held */
+static void xb_sched_retire(xb_sched *q, xb_slot &sl, bool wait)
+{
+    if (!sl.busy)
+        return;
+    cudaError_t rc = wait ? cudaEventSynchronize(sl.done) : cudaEventQuery(sl.done);
+    if (rc == cudaErrorNotReady)
+        return;
+    for (size_t i = 0; i < sl.cmds.size(); i++) {
+        const xb_cmd &c = sl.cmds[i];
+        xb_done d;
+        memset(&d, 0, sizeof(d));
+        d.nrels = c.s->h_plan->nrels;
+        if (rc != cudaSuccess) {
+            d.rc = xb_set_error(&d.err, ERRCODE_DEVICE_FATAL, "xpuB200Poll", __LINE__, "%s",
+                                cudaGetErrorString(rc));
+        } else {
+            d.st = sl.h_status[i];
+            if (d.st.errcode) {
+                d.rc = xb_set_error(&d.err, d.st.errcode, sl.alone ? "xb_exec_kernel" : "xb_mixed_kernel",
+                                    d.st.lineno, "%s", xb_msg_text(d.st.msg_id));
+            } else {
+                std::lock_guard<std::mutex> g(c.s->lock);
+                xb_account_status(c.s, &d.st, nullptr);
+            }
+        }
+        c.s->sched_refs--;
+        q->done[c.ticket] = d;
+    }
+    q->inflight_bytes -= sl.staged;
+    sl.staged = 0;
+    sl.cmds.clear();
+    sl.busy = false;
+}
+
+/* copy the host chunks of cmds into the slot's staging buffer; sched lock held */
+static int xb_sched_stage(xb_slot &sl, std::vector<xb_cmd> &cmds, kern_errorbuf *err)
+{
+    uint64_t need = 0;
+    for (const xb_cmd &c : cmds)
+        if (!c.on_device)
+            need += PGSTROM_TYPEALIGN(256, c.length + c.shift);
+    if (need > sl.stage_cap) {
+        cudaStreamSynchronize(sl.stream);
+        cudaFree(sl.d_stage);
+        sl.d_stage = nullptr;
+        sl.stage_cap = 0;
+        uint64_t cap = need < (64ULL << 20) ? (64ULL << 20) : need;
+        XB_CUDA(cudaMalloc((void **)&sl.d_stage, cap), err);
+        sl.stage_cap = cap;
+    }
+    uint64_t off = 0;
+    for (xb_cmd &c : cmds) {
+        if (c.on_device) {
+            c.d_kds = c.kds;
+            continue;
+        }
+        XB_CUDA(cudaMemcpyAsync(sl.d_stage + off + c.shift, c.kds, c.length, cudaMemcpyHostToDevice, sl.stream), err);
+        c.d_kds = (const kern_data_store *)(sl.d_stage + off + c.shift);
+        off += PGSTROM_TYPEALIGN(256, c.length + c.shift);
+    }
+    return 0;
+}
+
+/* launch the next admitted commands on slot sl; sched lock held */
+static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_errorbuf *err)
+{
+    std::vector<xb_cmd> take;
+    uint64_t bytes = 0;
+    const xb_cmd &f = q->pending.front();
+    const bool alone = f.units >= q->alone_units && f.s->jit_enabled;
+    while (!q->pending.empty() && take.size() < (alone ? 1u : (size_t)XB_SLOT_CMDS)) {
+        const xb_cmd &c = q->pending.front();
+        if (!alone && c.units >= q->alone_units && c.s->jit_enabled)
+            break;                      /* a large one runs alone, in a later launch */
+        const uint64_t b = c.on_device ? 0 : c.length + c.shift + 256;
+        if (q->inflight_bytes + bytes + b > q->admit_bytes && (!take.empty() || q->inflight_bytes > 0))
+            break;                      /* admission: wait for memory to free up */
+        bytes += b;
+        take.push_back(c);
+        q->pending.pop_front();
+    }
+    if (take.empty())
+        return 0;
+    sl.busy = true;
+    sl.alone = alone;
+    sl.staged = bytes;
+    q->inflight_bytes += bytes;
+    sl.cmds = take;
+    int rc = xb_sched_stage(sl, sl.cmds, err);
+    const uint32_t n = (uint32_t)sl.cmds.size();
+    if (!rc) {
+        for (uint32_t i = 0; i < n; i++) {
+            const xb_cmd &c = sl.cmds[i];
+            sl.h_tasks[i].kds = c.d_kds;
+            sl.h_tasks[i].unit_base = 0;
+            sl.h_tasks[i].nunits = c.units;
+            sl.h_tasks[i].format = c.format;
+        }
+        if (cudaMemcpyAsync(sl.d_tasks, sl.h_tasks, sizeof(xb_task) * n, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
+            cudaMemsetAsync(sl.d_status, 0, sizeof(xb_status) * n, sl.stream) != cudaSuccess)
+            rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler upload failed");
+    }
+    if (!rc && alone) {
+        xpuB200Session *s = sl.cmds[0].s;
+        std::lock_guard<std::mutex> g(s->lock);
+        rc = xb_launch_on(s, sl.d_tasks, 1, sl.cmds[0].units, sl.cmds[0].format, sl.stream, sl.d_status, err);
+    } else if (!rc) {
+        /* one mixed launch: work items largest command first */
+        size_t smem = 0;
+        std::vector<uint32_t> order(n);
+        for (uint32_t i = 0; i < n; i++) {
+            order[i] = i;
+            if (sl.cmds[i].s->smem_bytes > smem)
+                smem = sl.cmds[i].s->smem_bytes;
+        }
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_mixed_kernel, XB_BLOCK, smem);
+        const int grid = (per_sm > 0 ? per_sm : 1) * dev->nsm;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t a, uint32_t b) { return sl.cmds[a].units > sl.cmds[b].units; });
+        std::vector<uint32_t> items;
+        for (uint32_t i : order) {
+            uint64_t k = (sl.cmds[i].units + XB_MIX_JOIN_UNITS - 1) / XB_MIX_JOIN_UNITS;
+            k = k < 1 ? 1 : (k > (uint64_t)grid ? grid : k);
+            for (uint64_t j = 0; j < k; j++) items.push_back(i);
+        }
+        if (items.size() > sl.items_cap) {
+            cudaStreamSynchronize(sl.stream);
+            cudaFree(sl.d_items);
+            if (sl.h_items) cudaFreeHost(sl.h_items);
+            sl.d_items = nullptr;
+            sl.h_items = nullptr;
+            sl.items_cap = 0;
+            const uint32_t cap = (uint32_t)items.size() * 2;
+            if (cudaMalloc((void **)&sl.d_items, sizeof(uint32_t) * cap) != cudaSuccess ||
+                cudaMallocHost((void **)&sl.h_items, sizeof(uint32_t) * cap) != cudaSuccess)
+                rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler: out of memory for the work queue");
+            else
+                sl.items_cap = cap;
+        }
+        if (!rc) {
+            memcpy(sl.h_items, items.data(), sizeof(uint32_t) * items.size());
+            for (uint32_t i = 0; i < n; i++) {
+                xpuB200Session *s = sl.cmds[i].s;
+                XbExecArgs &a = sl.h_cmds[i];
+                memset(&a, 0, sizeof(a));
+                a.plan = s->d_plan;
+                a.plan_bytes = s->plan_bytes;
+                a.tasks = sl.d_tasks + i;
+                a.ntasks = 1;
+                a.nunits = sl.cmds[i].units;
+                a.format = sl.cmds[i].format;
+                a.sm_cap = s->sm_cap;
+                a.warp_bytes = s->warp_bytes;
+                a.gt = s->d_gt;
+                a.st = sl.d_status + i;
+                a.dyn_only = 1;
+            }
+            XbMixArgs ma;
+            ma.cmds = sl.d_cmds;
+            ma.items = sl.d_items;
+            ma.nitems = (uint32_t)items.size();
+            ma.cursor = sl.d_cursor;
+            cudaMemcpyAsync(sl.d_cmds, sl.h_cmds, sizeof(XbExecArgs) * n, cudaMemcpyHostToDevice, sl.stream);
+            cudaMemcpyAsync(sl.d_items, sl.h_items, sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice, sl.stream);
+            cudaMemsetAsync(sl.d_cursor, 0, 16, sl.stream);
+            xb_mixed_kernel<<<grid, XB_BLOCK, smem, sl.stream>>>(ma);
+            cudaError_t lrc = cudaGetLastError();
+            if (lrc != cudaSuccess)
+                rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch: %s", cudaGetErrorString(lrc));
+        }
+    }
+    if (!rc) {
+        if (cudaMemcpyAsync(sl.h_status, sl.d_status, sizeof(xb_status) * n, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
+            cudaEventRecord(sl.done, sl.stream) != cudaSuccess)
+            rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler: status read-back failed");
+    }
+    if (rc) {
+        /* the launch did not happen: its commands finish with the error */
+        cudaStreamSynchronize(sl.stream);
+        for (const xb_cmd &c : sl.cmds) {
+            xb_done d;
+            memset(&d, 0, sizeof(d));
+            d.rc = rc;
+            if (err) d.err = *err;
+            d.nrels = c.s->h_plan->nrels;
+            c.s->sched_refs--;
+            q->done[c.ticket] = d;
+        }
+        q->inflight_bytes -= sl.staged;
+        sl.staged = 0;
+        sl.cmds.clear();
+        sl.busy = false;
+    }
+    return rc;
+}
+
+/* retire finished launches and launch admitted commands; sched lock held */
+static void xb_sched_progress(xpuB200Device *dev, xb_sched *q)
+{
+    for (int i = 0; i < XB_SLOTS; i++)
+        xb_sched_retire(q, q->slot[i], false);
+    for (int i = 0; i < XB_SLOTS && !q->pending.empty(); i++) {
+        xb_slot &sl = q->slot[i];
+        if (sl.busy)
+            continue;
+        kern_errorbuf e;
+        xb_sched_launch(dev, q, sl, &e);    /* errors are recorded per command */
+    }
+}
+
+/* block until one in-flight launch finishes (one holding 'who' if given);
+ * called with the lock held through lk, which is released while waiting */
+static void xb_sched_wait_one(xb_sched *q, std::unique_lock<std::mutex> &lk, const xpuB200Session *who)
+{
+    int pick = -1;
+    for (int i = 0; i < XB_SLOTS && pick < 0; i++) {
+        if (!q->slot[i].busy)
+            continue;
+        if (!who)
+            pick = i;
+        for (const xb_cmd &c : q->slot[i].cmds)
+            if (c.s == who)
+                pick = i;
+    }
+    for (int i = 0; i < XB_SLOTS && pick < 0; i++)
+        if (q->slot[i].busy)
+            pick = i;
+    if (pick < 0)
+        return;
+    cudaEvent_t ev = q->slot[pick].done;
+    lk.unlock();
+    cudaEventSynchronize(ev);
+    lk.lock();
+}
+
+static void xb_sched_drain_session(xpuB200Session *s)
+{
+    xpuB200Device *dev = s->dev;
+    xb_sched *q = dev->sched;
+    if (!q)
+        return;
+    cudaSetDevice(dev->dindex);
+    std::unique_lock<std::mutex> lk(q->lock);
+    for (;;) {
+        xb_sched_progress(dev, q);
+        if (s->sched_refs == 0)
+            break;
+        xb_sched_wait_one(q, lk, s);
+    }
+}
+
+static void xb_sched_destroy(xpuB200Device *dev)
+{
+    xb_sched *q = dev->sched;
+    if (!q)
+        return;
+    for (int i = 0; i < XB_SLOTS; i++)
+        xb_slot_free(q->slot[i]);
+    delete q;
+    dev->sched = nullptr;
+}
+
+extern "C" int
+xpuB200ServeConfig(xpuB200Device *dev, uint64_t admit_bytes, uint32_t alone_units, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!dev)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid device");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    int rc = xb_sched_init(dev, err);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(dev->sched->lock);
+    if (admit_bytes)
+        dev->sched->admit_bytes = admit_bytes;
+    if (alone_units)
+        dev->sched->alone_units = alone_units;
+    return 0;
+}
+
+extern "C" int
+xpuB200Submit(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
+              uint64_t *p_ticket, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s || !kds_src || !p_ticket)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid Submit arguments");
+    if (s->h_plan->has_proj)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "projection sessions run through xpuB200ExecTaskDst");
+    xpuB200Device *dev = s->dev;
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    int rc = xb_sched_init(dev, err);
+    if (rc) return rc;
+    /* the chunk header, checked now */
+    xb_cmd c;
+    memset(&c, 0, sizeof(c));
+    std::vector<char> hb;
+    kern_data_store head;
+    if (kds_src_on_device) {
+        if (((uintptr_t)kds_src & 7) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
+        XB_CUDA(cudaMemcpy(&head, kds_src, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+        hb.resize(KDS_HEAD_LENGTH(&head));
+        XB_CUDA(cudaMemcpy(hb.data(), kds_src, hb.size(), cudaMemcpyDeviceToHost), err);
+    } else {
+        hb.assign((const char *)kds_src, (const char *)kds_src + KDS_HEAD_LENGTH(kds_src));
+    }
+    const kern_data_store *h = (const kern_data_store *)hb.data();
+    rc = xb_check_kds(h, err);
+    if (rc) return rc;
+    if (kds_src_on_device && h->format == KDS_FORMAT_BLOCK &&
+        (((uintptr_t)kds_src + h->block_offset) & 15) != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "heap pages of a device chunk must start 16-byte aligned");
+    c.s = s;
+    c.kds = kds_src;
+    c.on_device = kds_src_on_device;
+    c.length = h->length;
+    c.shift = (!kds_src_on_device && h->format == KDS_FORMAT_BLOCK) ? ((16 - (h->block_offset & 15)) & 15) : 0;
+    c.units = xb_chunk_units(h);
+    c.format = (uint32_t)h->format;
+    xb_sched *q = dev->sched;
+    std::lock_guard<std::mutex> g(q->lock);
+    c.ticket = q->next_ticket++;
+    s->sched_refs++;
+    q->pending.push_back(c);
+    xb_sched_progress(dev, q);
+    *p_ticket = c.ticket;
+    return 0;
+}
+
+extern "C" int
+xpuB200Poll(xpuB200Device *dev, uint64_t ticket, int wait, int *p_done,
+            kern_exec_results *results, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (p_done) *p_done = 0;
+    if (!dev || !dev->sched)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "no command was submitted on this device");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    xb_sched *q = dev->sched;
+    std::unique_lock<std::mutex> lk(q->lock);
+    for (;;) {
+        xb_sched_progress(dev, q);
+        auto it = q->done.find(ticket);
+        if (it != q->done.end()) {
+            const xb_done d = it->second;
+            q->done.erase(it);
+            if (p_done) *p_done = 1;
+            if (d.rc) {
+                if (err) *err = d.err;
+                return d.rc;
+            }
+            xb_fill_results(&d.st, d.nrels, results);
+            return 0;
+        }
+        bool known = ticket > 0 && ticket < q->next_ticket;
+        if (known) {
+            known = false;
+            for (const xb_cmd &c : q->pending)
+                if (c.ticket == ticket) known = true;
+            for (int i = 0; i < XB_SLOTS && !known; i++)
+                for (const xb_cmd &c : q->slot[i].cmds)
+                    if (c.ticket == ticket) known = true;
+        }
+        if (!known)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unknown ticket %llu", (unsigned long long)ticket);
+        if (!wait)
+            return 0;
+        xb_sched_wait_one(q, lk, nullptr);
+    }
 }
 
 extern "C" int

@@ -58,6 +58,9 @@ def lib():
         L.xpuB200BatchExec.argtypes = [P, P, EB]
         L.xpuB200BatchTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
         L.xpuB200BatchDestroy.argtypes = [P]
+        L.xpuB200Submit.argtypes = [P, P, I, ctypes.POINTER(U64), EB]
+        L.xpuB200Poll.argtypes = [P, U64, I, ctypes.POINTER(I), P, EB]
+        L.xpuB200ServeConfig.argtypes = [P, U64, ctypes.c_uint32, EB]
         L.xpuB200MixCreate.argtypes = [P, ctypes.c_uint32, P, P, ctypes.POINTER(P), EB]
         L.xpuB200MixExec.argtypes = [P, P, P]
         L.xpuB200MixTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
@@ -121,6 +124,34 @@ class Device:
         if lib().xpuB200CopyToDevice(self.h, ctypes.c_void_p(base + shift), _ptr(arr), arr.nbytes):
             raise RuntimeError("upload failed")
         return base, base + shift
+
+    def serve_config(self, admit_bytes=0, alone_units=0):
+        e = KernErrorbuf()
+        rc = lib().xpuB200ServeConfig(self.h, admit_bytes, alone_units, ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+
+    def submit(self, sess, kds, on_device=False):
+        """Queue one chunk command of sess; returns its ticket.  A host
+        chunk must stay alive until the ticket is polled done."""
+        t = ctypes.c_uint64()
+        e = KernErrorbuf()
+        p = ctypes.c_void_p(kds) if on_device else _ptr(kds)
+        rc = lib().xpuB200Submit(sess.h, p, 1 if on_device else 0, ctypes.byref(t), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return t.value
+
+    def poll(self, ticket, nrels=0, wait=True):
+        """Results of a submitted command (None while it runs, wait=False)."""
+        res = results_buffer(nrels)
+        struct.pack_into("<I", res, 92, nrels)
+        done = ctypes.c_int()
+        e = KernErrorbuf()
+        rc = lib().xpuB200Poll(self.h, ticket, 1 if wait else 0, ctypes.byref(done), _ptr(res), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return parse_results(res) if done.value else None
 
     def close(self):
         if self.h:
