@@ -167,12 +167,16 @@ int  xpuB200ServeConfig(xpuB200Device *dev, uint64_t admit_bytes, uint32_t alone
 /*
  * Mixed batches (the batched form of many sessions' XpuTaskExec): chunk
  * commands of different sessions, each a device-resident chunk of its own
- * session, run together in ONE persistent kernel fed from a device work
+ * session, run together in one persistent kernel fed from a device work
  * queue.  CTAs are sent to commands largest first, several to a large one;
  * each claims the command's units dynamically, runs the command's own
- * bytecode against its own group table, and moves on.  A run is captured
- * once as a CUDA graph (status reset, kernel, status read-back) and
- * replayed by every xpuB200MixExec / xpuB200MixTime.
+ * bytecode against its own group table, and moves on.  Sessions of one
+ * plan shape (bytecode equal up to constants) share one specialised
+ * kernel; the batch runs one persistent launch per kernel (the
+ * interpreter's for the rest), concurrently.  A run is captured once as a
+ * CUDA graph (status reset, the launches, status read-back) and replayed by
+ * every xpuB200MixExec / xpuB200MixTime.  xpuB200MixInfo reports the
+ * launches of a run and how many commands run specialised code.
  * xpuB200MixExec fills results[i] and errs[i] per command (either array
  * may be NULL) and returns 0, or the first command error.  Each command's
  * groups accumulate in its session, as with xpuB200ExecTask.  No
@@ -186,7 +190,7 @@ int  xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const 
 int  xpuB200MixExec(xpuB200Mix *mix, kern_exec_results *const *results, kern_errorbuf *errs);
 int  xpuB200MixTime(xpuB200Mix *mix, int niters, double *p_msec, kern_errorbuf *err);
 int  xpuB200MixInfo(const xpuB200Mix *mix, uint64_t *p_bytes, uint64_t *p_units,
-                    uint32_t *p_items, int *p_grid);
+                    uint32_t *p_items, uint32_t *p_launches, uint32_t *p_specialised);
 void xpuB200MixDestroy(xpuB200Mix *mix);
 
 /*

@@ -779,13 +779,6 @@ xb_exec_kernel(const __grid_constant__ XbExecArgs args)
  * next item.  A large command is listed several times so that several CTAs
  * join it; items are ordered largest command first.
  */
-struct XbMixArgs {
-    const XbExecArgs *cmds;
-    const uint32_t   *items;
-    uint32_t          nitems;
-    uint32_t         *cursor;       /* next item (zero at launch) */
-};
-
 __global__ void __launch_bounds__(XB_BLOCK, XB_MIN_BLOCKS)
 xb_mixed_kernel(const __grid_constant__ XbMixArgs m)
 {
@@ -1397,6 +1390,7 @@ struct xpuB200Session {
     bool            jit_enabled = true;
     bool            jit_tried[256] = {false};
     void           *jit_fn[256] = {nullptr};
+    void           *jit_mixfn[256] = {nullptr};    /* its mixed-launch kernel */
     char            ran_kind[256] = {0};   /* 'j' / 'v': kernel last launched per format */
     uint32_t        sched_refs = 0;        /* submitted commands not yet finished */
     /* device projection: staging buffer for host kds_dst, and the buffer of
@@ -1827,6 +1821,40 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
                         uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
                         kern_errorbuf *err);
 
+/* the session-specialised kernel of this format (nullptr: use the
+ * interpreter), built on first use; session lock held */
+static void *xb_session_jit(xpuB200Session *s, uint32_t format)
+{
+    if (!s->jit_enabled || format >= 256)
+        return nullptr;
+    if (!s->jit_tried[format]) {
+        s->jit_tried[format] = true;
+        char msg[1024];
+        double ms = 0.0;
+        int per_sm = 0, mix_sm = 0;
+        if (xb_jit_compile(s->h_plan, format, s->dev->dindex, &s->jit_fn[format], &s->jit_mixfn[format],
+                           &ms, msg, sizeof(msg)) != 0) {
+            s->jit_fn[format] = nullptr;
+            s->jit_mixfn[format] = nullptr;
+            s->jit_msg = msg;
+        } else if (xb_jit_prepare(s->jit_fn[format], XB_BLOCK, s->jit_smem, &per_sm) != 0) {
+            s->jit_fn[format] = nullptr;
+            s->jit_mixfn[format] = nullptr;
+            s->jit_msg = "specialised kernel does not fit on an SM";
+        } else {
+            /* the mixed kernel is shared by sessions of one plan shape with
+             * their own table sizes: it opts in to all shared memory */
+            if (xb_jit_prepare(s->jit_mixfn[format], XB_BLOCK, s->dev->smem_optin - sizeof(XbExecArgs) - 16,
+                               &mix_sm) != 0)
+                s->jit_mixfn[format] = nullptr;
+            s->jit_grid[format] = per_sm * s->dev->nsm;
+            s->jit_compile_ms += ms;
+            s->jit_msg = "ok";
+        }
+    }
+    return s->jit_fn[format];
+}
+
 static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                            uint64_t nunits, uint32_t format, kern_errorbuf *err)
 {
@@ -1852,28 +1880,7 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     a.__pad = 0;
     a.gt = s->d_gt;
     a.st = d_status;
-    /* the session-specialised kernel of this format, built on first use */
-    void *fn = nullptr;
-    if (s->jit_enabled && format < 256) {
-        if (!s->jit_tried[format]) {
-            s->jit_tried[format] = true;
-            char msg[1024];
-            double ms = 0.0;
-            int per_sm = 0;
-            if (xb_jit_compile(s->h_plan, format, s->dev->dindex, &s->jit_fn[format], &ms, msg, sizeof(msg)) != 0) {
-                s->jit_fn[format] = nullptr;
-                s->jit_msg = msg;
-            } else if (xb_jit_prepare(s->jit_fn[format], XB_BLOCK, s->jit_smem, &per_sm) != 0) {
-                s->jit_fn[format] = nullptr;
-                s->jit_msg = "specialised kernel does not fit on an SM";
-            } else {
-                s->jit_grid[format] = per_sm * s->dev->nsm;
-                s->jit_compile_ms += ms;
-                s->jit_msg = "ok";
-            }
-        }
-        fn = s->jit_fn[format];
-    }
+    void *fn = xb_session_jit(s, format);
     int grid = fn ? s->jit_grid[format] : s->grid;
     uint64_t warps_needed = (format == KDS_FORMAT_BLOCK) ? (nunits + XB_CLAIM - 1) / XB_CLAIM : nunits;
     if ((uint64_t)grid * XB_WARPS > warps_needed)
@@ -2606,28 +2613,107 @@ xpuB200BatchDestroy(xpuB200Batch *b)
 /* ================================================================
  * mixed batches: chunk commands of many sessions in one launch
  * ================================================================ */
+/* units one CTA takes of a command before another CTA is sent to join it */
+#define XB_MIX_JOIN_UNITS   16
+
+/* one persistent launch of a mixed batch: the commands that share a kernel
+ * (a specialised mixed kernel of one plan shape, or the interpreter) */
+struct xb_mix_group {
+    void           *jfn = nullptr;  /* xbj_mixed_kernel, or nullptr: xb_mixed_kernel */
+    std::vector<uint32_t> cmds;     /* command indexes */
+    std::vector<uint32_t> items;    /* work queue: command index per item */
+    size_t          smem = 0;
+    int             grid = 0;
+};
+
+/* the mixed kernel a command of session s (chunk format) runs on */
+static void *xb_mix_kernel_of(xpuB200Session *s, uint32_t format)
+{
+    std::lock_guard<std::mutex> g(s->lock);
+    return xb_session_jit(s, format) ? s->jit_mixfn[format] : nullptr;
+}
+
+/* split commands into launches by kernel and build each work queue:
+ * largest command first, listed once per XB_MIX_JOIN_UNITS of its units
+ * (at most once per CTA) */
+static int xb_mix_plan(xpuB200Device *dev, const std::vector<xpuB200Session *> &sess,
+                       const std::vector<uint32_t> &formats, const std::vector<uint64_t> &units,
+                       std::vector<xb_mix_group> &groups, kern_errorbuf *err)
+{
+    groups.clear();
+    for (uint32_t i = 0; i < sess.size(); i++) {
+        void *k = xb_mix_kernel_of(sess[i], formats[i]);
+        size_t g = 0;
+        while (g < groups.size() && groups[g].jfn != k)
+            g++;
+        if (g == groups.size()) {
+            groups.emplace_back();
+            groups.back().jfn = k;
+        }
+        groups[g].cmds.push_back(i);
+        const size_t sm = k ? sess[i]->jit_smem : sess[i]->smem_bytes;
+        if (sm > groups[g].smem)
+            groups[g].smem = sm;
+    }
+    for (xb_mix_group &g : groups) {
+        if (g.smem + sizeof(XbExecArgs) + 16 > dev->smem_optin)
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch needs %zu bytes of shared memory", g.smem);
+        int per_sm = 0;
+        if (g.jfn)
+            xb_jit_occupancy(g.jfn, XB_BLOCK, g.smem, &per_sm);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_mixed_kernel, XB_BLOCK, g.smem);
+        if (per_sm < 1)
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed kernel does not fit on an SM (%zu bytes)", g.smem);
+        g.grid = per_sm * dev->nsm;
+        std::vector<uint32_t> order(g.cmds);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return units[a] > units[b]; });
+        for (uint32_t i : order) {
+            uint64_t k = (units[i] + XB_MIX_JOIN_UNITS - 1) / XB_MIX_JOIN_UNITS;
+            k = k < 1 ? 1 : (k > (uint64_t)g.grid ? g.grid : k);
+            for (uint64_t j = 0; j < k; j++)
+                g.items.push_back(i);
+        }
+    }
+    return 0;
+}
+
+/* launch one group of a mixed batch on a stream */
+static int xb_mix_launch(const xb_mix_group &g, const XbMixArgs &ma, cudaStream_t stream, kern_errorbuf *err)
+{
+    if (g.jfn) {
+        XbMixArgs a = ma;
+        if (xb_jit_launch(g.jfn, g.grid, XB_BLOCK, g.smem, (void *)stream, &a) != 0)
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised mixed kernel launch failed");
+    } else {
+        xb_mixed_kernel<<<g.grid, XB_BLOCK, g.smem, stream>>>(ma);
+    }
+    cudaError_t rc = cudaGetLastError();
+    if (rc != cudaSuccess)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch: %s", cudaGetErrorString(rc));
+    return 0;
+}
+
 struct xpuB200Mix {
     xpuB200Device  *dev;
     uint32_t        ncmds = 0;
     std::vector<xpuB200Session *> sess;
+    std::vector<xb_mix_group> groups;
     xb_task        *d_tasks = nullptr;
     XbExecArgs     *d_cmds = nullptr;
     uint32_t       *d_items = nullptr;
     uint32_t        nitems = 0;
-    uint32_t       *d_cursor = nullptr;
+    uint32_t       *d_cursor = nullptr;     /* one per group, 32 bytes apart */
     xb_status      *d_status = nullptr;
     xb_status      *h_status = nullptr;     /* pinned */
     cudaStream_t    stream = nullptr;
+    std::vector<cudaStream_t> aux;          /* a branch per further group */
+    std::vector<cudaEvent_t> forks, joins;
     cudaGraph_t     graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaEvent_t     ev0 = nullptr, ev1 = nullptr;
-    size_t          smem = 0;
-    int             grid = 0;
     uint64_t        bytes = 0, units = 0;
 };
-
-/* units one CTA takes of a command before another CTA is sent to join it */
-#define XB_MIX_JOIN_UNITS   16
 
 static void xb_mix_free(xpuB200Mix *m)
 {
@@ -2637,6 +2723,9 @@ static void xb_mix_free(xpuB200Mix *m)
     if (m->graph) cudaGraphDestroy(m->graph);
     if (m->ev0) cudaEventDestroy(m->ev0);
     if (m->ev1) cudaEventDestroy(m->ev1);
+    for (cudaEvent_t e : m->forks) cudaEventDestroy(e);
+    for (cudaEvent_t e : m->joins) cudaEventDestroy(e);
+    for (cudaStream_t a : m->aux) cudaStreamDestroy(a);
     if (m->stream) cudaStreamDestroy(m->stream);
     cudaFree(m->d_tasks);
     cudaFree(m->d_cmds);
@@ -2658,7 +2747,7 @@ xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess
     XB_CUDA(cudaSetDevice(dev->dindex), err);
     std::vector<xb_task> tasks(ncmds);
     std::vector<uint64_t> units(ncmds);
-    size_t smem = 0;
+    std::vector<uint32_t> formats(ncmds);
     uint64_t bytes = 0, total_units = 0;
     for (uint32_t i = 0; i < ncmds; i++) {
         xpuB200Session *s = sess[i];
@@ -2680,39 +2769,29 @@ xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess
         tasks[i].nunits = xb_chunk_units(h);
         tasks[i].format = (uint32_t)h->format;
         units[i] = tasks[i].nunits;
+        formats[i] = tasks[i].format;
         total_units += units[i];
         bytes += h->length;
-        if (s->smem_bytes > smem)
-            smem = s->smem_bytes;
-    }
-    if (smem + sizeof(XbExecArgs) + 16 > dev->smem_optin)
-        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch needs %zu bytes of shared memory", smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_mixed_kernel, XB_BLOCK, smem);
-    if (per_sm < 1)
-        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed kernel does not fit on an SM (%zu bytes)", smem);
-    const int grid = per_sm * dev->nsm;
-    /* work items: the largest command first, each listed once per
-     * XB_MIX_JOIN_UNITS of its units (at most once per CTA) */
-    std::vector<uint32_t> order(ncmds);
-    for (uint32_t i = 0; i < ncmds; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return units[a] > units[b]; });
-    std::vector<uint32_t> items;
-    for (uint32_t i : order) {
-        uint64_t k = (units[i] + XB_MIX_JOIN_UNITS - 1) / XB_MIX_JOIN_UNITS;
-        if (k < 1) k = 1;
-        if (k > (uint64_t)grid) k = grid;
-        for (uint64_t j = 0; j < k; j++) items.push_back(i);
     }
     xpuB200Mix *m = new xpuB200Mix();
     m->dev = dev;
     m->ncmds = ncmds;
     m->sess.assign(sess, sess + ncmds);
-    m->nitems = (uint32_t)items.size();
-    m->smem = smem;
-    m->grid = grid;
     m->bytes = bytes;
     m->units = total_units;
+    int rc = xb_mix_plan(dev, m->sess, formats, units, m->groups, err);
+    if (rc) {
+        xb_mix_free(m);
+        return rc;
+    }
+    const size_t ng = m->groups.size();
+    std::vector<uint32_t> items;
+    std::vector<size_t> item_off;
+    for (const xb_mix_group &g : m->groups) {
+        item_off.push_back(items.size());
+        items.insert(items.end(), g.items.begin(), g.items.end());
+    }
+    m->nitems = (uint32_t)items.size();
     auto fail = [&](const char *what) {
         xb_mix_free(m);
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed batch: %s", what);
@@ -2720,7 +2799,7 @@ xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess
     if (cudaMalloc((void **)&m->d_tasks, sizeof(xb_task) * ncmds) != cudaSuccess ||
         cudaMalloc((void **)&m->d_cmds, sizeof(XbExecArgs) * ncmds) != cudaSuccess ||
         cudaMalloc((void **)&m->d_items, sizeof(uint32_t) * items.size()) != cudaSuccess ||
-        cudaMalloc((void **)&m->d_cursor, 16) != cudaSuccess ||
+        cudaMalloc((void **)&m->d_cursor, 32 * ng) != cudaSuccess ||
         cudaMalloc((void **)&m->d_status, sizeof(xb_status) * ncmds) != cudaSuccess ||
         cudaMallocHost((void **)&m->h_status, sizeof(xb_status) * ncmds) != cudaSuccess)
         return fail("out of memory");
@@ -2748,21 +2827,52 @@ xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&m->ev0) != cudaSuccess || cudaEventCreate(&m->ev1) != cudaSuccess)
         return fail("stream setup failed");
-    /* one run = clear the statuses and the queue cursor, the persistent
-     * kernel, the statuses back to the host: captured once, replayed */
-    XbMixArgs ma;
-    ma.cmds = m->d_cmds;
-    ma.items = m->d_items;
-    ma.nitems = m->nitems;
-    ma.cursor = m->d_cursor;
+    for (size_t g = 1; g < ng; g++) {
+        cudaStream_t a;
+        cudaEvent_t f, j;
+        if (cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) != cudaSuccess)
+            return fail("stream setup failed");
+        m->aux.push_back(a);
+        if (cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess)
+            return fail("event setup failed");
+        m->forks.push_back(f);
+        if (cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess)
+            return fail("event setup failed");
+        m->joins.push_back(j);
+    }
+    /* one run = clear the statuses and the queue cursors, one persistent
+     * launch per kernel group (concurrent branches), the statuses back to
+     * the host: captured once, replayed */
     if (cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return fail("stream capture failed");
+    kern_errorbuf lerr;
+    int lrc = 0;
     cudaMemsetAsync(m->d_status, 0, sizeof(xb_status) * ncmds, m->stream);
-    cudaMemsetAsync(m->d_cursor, 0, 16, m->stream);
-    xb_mixed_kernel<<<grid, XB_BLOCK, smem, m->stream>>>(ma);
+    cudaMemsetAsync(m->d_cursor, 0, 32 * ng, m->stream);
+    for (size_t g = 1; g < ng; g++) {
+        cudaEventRecord(m->forks[g - 1], m->stream);
+        cudaStreamWaitEvent(m->aux[g - 1], m->forks[g - 1], 0);
+    }
+    for (size_t g = 0; g < ng && !lrc; g++) {
+        XbMixArgs ma;
+        ma.cmds = m->d_cmds;
+        ma.items = m->d_items + item_off[g];
+        ma.nitems = (uint32_t)m->groups[g].items.size();
+        ma.cursor = m->d_cursor + 8 * g;
+        lrc = xb_mix_launch(m->groups[g], ma, g == 0 ? m->stream : m->aux[g - 1], &lerr);
+    }
+    for (size_t g = 1; g < ng; g++) {
+        cudaEventRecord(m->joins[g - 1], m->aux[g - 1]);
+        cudaStreamWaitEvent(m->stream, m->joins[g - 1], 0);
+    }
     cudaMemcpyAsync(m->h_status, m->d_status, sizeof(xb_status) * ncmds, cudaMemcpyDeviceToHost, m->stream);
-    if (cudaStreamEndCapture(m->stream, &m->graph) != cudaSuccess ||
-        cudaGraphInstantiate(&m->gexec, m->graph, 0) != cudaSuccess)
+    cudaError_t crc = cudaStreamEndCapture(m->stream, &m->graph);
+    if (lrc) {
+        if (err) *err = lerr;
+        xb_mix_free(m);
+        return lrc;
+    }
+    if (crc != cudaSuccess || cudaGraphInstantiate(&m->gexec, m->graph, 0) != cudaSuccess)
         return fail("graph capture failed");
     *p_mix = m;
     return 0;
@@ -2833,13 +2943,20 @@ xpuB200MixTime(xpuB200Mix *m, int niters, double *p_msec, kern_errorbuf *err)
 }
 
 extern "C" int
-xpuB200MixInfo(const xpuB200Mix *m, uint64_t *p_bytes, uint64_t *p_units, uint32_t *p_items, int *p_grid)
+xpuB200MixInfo(const xpuB200Mix *m, uint64_t *p_bytes, uint64_t *p_units, uint32_t *p_items,
+               uint32_t *p_launches, uint32_t *p_specialised)
 {
     if (!m) return ERRCODE_DEVICE_ERROR;
     if (p_bytes) *p_bytes = m->bytes;
     if (p_units) *p_units = m->units;
     if (p_items) *p_items = m->nitems;
-    if (p_grid) *p_grid = m->grid;
+    if (p_launches) *p_launches = (uint32_t)m->groups.size();
+    if (p_specialised) {
+        uint32_t n = 0;
+        for (const xb_mix_group &g : m->groups)
+            if (g.jfn) n += (uint32_t)g.cmds.size();
+        *p_specialised = n;
+    }
     return 0;
 }
 
@@ -3032,10 +3149,13 @@ static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_er
     uint64_t bytes = 0;
     const xb_cmd &f = q->pending.front();
     const bool alone = f.units >= q->alone_units && f.s->jit_enabled;
+    void *kern = alone ? nullptr : xb_mix_kernel_of(f.s, f.format);
     while (!q->pending.empty() && take.size() < (alone ? 1u : (size_t)XB_SLOT_CMDS)) {
         const xb_cmd &c = q->pending.front();
         if (!alone && c.units >= q->alone_units && c.s->jit_enabled)
             break;                      /* a large one runs alone, in a later launch */
+        if (!alone && xb_mix_kernel_of(c.s, c.format) != kern)
+            break;                      /* another kernel: a launch of its own */
         const uint64_t b = c.on_device ? 0 : c.length + c.shift + 256;
         if (q->inflight_bytes + bytes + b > q->admit_bytes && (!take.empty() || q->inflight_bytes > 0))
             break;                      /* admission: wait for memory to free up */
@@ -3069,41 +3189,34 @@ static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_er
         std::lock_guard<std::mutex> g(s->lock);
         rc = xb_launch_on(s, sl.d_tasks, 1, sl.cmds[0].units, sl.cmds[0].format, sl.stream, sl.d_status, err);
     } else if (!rc) {
-        /* one mixed launch: work items largest command first */
-        size_t smem = 0;
-        std::vector<uint32_t> order(n);
+        /* one mixed launch of commands that share a kernel */
+        std::vector<xpuB200Session *> ss(n);
+        std::vector<uint32_t> fm(n);
+        std::vector<uint64_t> un(n);
         for (uint32_t i = 0; i < n; i++) {
-            order[i] = i;
-            if (sl.cmds[i].s->smem_bytes > smem)
-                smem = sl.cmds[i].s->smem_bytes;
+            ss[i] = sl.cmds[i].s;
+            fm[i] = sl.cmds[i].format;
+            un[i] = sl.cmds[i].units;
         }
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_mixed_kernel, XB_BLOCK, smem);
-        const int grid = (per_sm > 0 ? per_sm : 1) * dev->nsm;
-        std::stable_sort(order.begin(), order.end(),
-                         [&](uint32_t a, uint32_t b) { return sl.cmds[a].units > sl.cmds[b].units; });
-        std::vector<uint32_t> items;
-        for (uint32_t i : order) {
-            uint64_t k = (sl.cmds[i].units + XB_MIX_JOIN_UNITS - 1) / XB_MIX_JOIN_UNITS;
-            k = k < 1 ? 1 : (k > (uint64_t)grid ? grid : k);
-            for (uint64_t j = 0; j < k; j++) items.push_back(i);
-        }
-        if (items.size() > sl.items_cap) {
+        std::vector<xb_mix_group> groups;
+        rc = xb_mix_plan(dev, ss, fm, un, groups, err);
+        const xb_mix_group *g = groups.empty() ? nullptr : &groups[0];
+        if (!rc && g && g->items.size() > sl.items_cap) {
             cudaStreamSynchronize(sl.stream);
             cudaFree(sl.d_items);
             if (sl.h_items) cudaFreeHost(sl.h_items);
             sl.d_items = nullptr;
             sl.h_items = nullptr;
             sl.items_cap = 0;
-            const uint32_t cap = (uint32_t)items.size() * 2;
+            const uint32_t cap = (uint32_t)g->items.size() * 2;
             if (cudaMalloc((void **)&sl.d_items, sizeof(uint32_t) * cap) != cudaSuccess ||
                 cudaMallocHost((void **)&sl.h_items, sizeof(uint32_t) * cap) != cudaSuccess)
                 rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler: out of memory for the work queue");
             else
                 sl.items_cap = cap;
         }
-        if (!rc) {
-            memcpy(sl.h_items, items.data(), sizeof(uint32_t) * items.size());
+        if (!rc && g) {
+            memcpy(sl.h_items, g->items.data(), sizeof(uint32_t) * g->items.size());
             for (uint32_t i = 0; i < n; i++) {
                 xpuB200Session *s = sl.cmds[i].s;
                 XbExecArgs &a = sl.h_cmds[i];
@@ -3123,15 +3236,12 @@ static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_er
             XbMixArgs ma;
             ma.cmds = sl.d_cmds;
             ma.items = sl.d_items;
-            ma.nitems = (uint32_t)items.size();
+            ma.nitems = (uint32_t)g->items.size();
             ma.cursor = sl.d_cursor;
             cudaMemcpyAsync(sl.d_cmds, sl.h_cmds, sizeof(XbExecArgs) * n, cudaMemcpyHostToDevice, sl.stream);
-            cudaMemcpyAsync(sl.d_items, sl.h_items, sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice, sl.stream);
+            cudaMemcpyAsync(sl.d_items, sl.h_items, sizeof(uint32_t) * g->items.size(), cudaMemcpyHostToDevice, sl.stream);
             cudaMemsetAsync(sl.d_cursor, 0, 16, sl.stream);
-            xb_mixed_kernel<<<grid, XB_BLOCK, smem, sl.stream>>>(ma);
-            cudaError_t lrc = cudaGetLastError();
-            if (lrc != cudaSuccess)
-                rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch: %s", cudaGetErrorString(lrc));
+            rc = xb_mix_launch(*g, ma, sl.stream, err);
         }
     }
     if (!rc) {

@@ -353,6 +353,14 @@ struct XbExecArgs {
     uint32_t        __pad;
 };
 
+/* a mixed launch: work item i sends a CTA to command items[i] */
+struct XbMixArgs {
+    const XbExecArgs *cmds;
+    const uint32_t   *items;
+    uint32_t          nitems;
+    uint32_t         *cursor;       /* next item (zero at launch) */
+};
+
 /* per-warp counters, in shared memory */
 struct XbWarpState {
     unsigned long long raw, in, out;

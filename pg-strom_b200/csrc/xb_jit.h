@@ -20,10 +20,12 @@ extern "C" {
 /* the generated CUDA source (for inspection); *p_len = its length */
 int xb_jit_source(const xb_plan *plan, uint32_t format, char *buf, size_t bufsz, size_t *p_len);
 
-/* build (or find in the process-wide cache) the kernel of plan + format on
- * device dindex; *p_func is a CUfunction */
+/* build (or find in the process-wide cache) the kernels of plan + format
+ * on device dindex: *p_func the per-launch kernel (xbj_kernel), *p_mixfn
+ * (if not NULL) the mixed-launch kernel (xbj_mixed_kernel, parameter block
+ * XbMixArgs); both CUfunctions */
 int xb_jit_compile(const xb_plan *plan, uint32_t format, int dindex,
-                   void **p_func, double *p_compile_ms, char *errbuf, size_t errlen);
+                   void **p_func, void **p_mixfn, double *p_compile_ms, char *errbuf, size_t errlen);
 
 /* compile only (no device needed): cubin size and NVRTC milliseconds */
 int xb_jit_check(const xb_plan *plan, uint32_t format, uint64_t *p_cubin_bytes, double *p_compile_ms,
@@ -32,7 +34,11 @@ int xb_jit_check(const xb_plan *plan, uint32_t format, uint64_t *p_cubin_bytes, 
 /* allow 'smem' bytes of dynamic shared memory; resident CTAs per SM */
 int xb_jit_prepare(void *func, int block, size_t smem, int *p_per_sm);
 
-/* launch with one kernel parameter block ('args' points to XbExecArgs) */
+/* resident CTAs per SM with 'smem' bytes (the limit already allowed) */
+int xb_jit_occupancy(void *func, int block, size_t smem, int *p_per_sm);
+
+/* launch with one kernel parameter block ('args' points to XbExecArgs,
+ * or to XbMixArgs for the mixed-launch kernel) */
 int xb_jit_launch(void *func, int grid, int block, size_t smem, void *stream, void *args);
 
 #ifdef __cplusplus

@@ -96,10 +96,12 @@ __device__ __forceinline__ unsigned long long xbj_warp_sum(unsigned long long v)
     return v;
 }
 
-extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
-xbj_kernel(XbExecArgs args)
+/* one launch's (or one mixed-launch command's) work for this CTA; ends
+ * with the counters and the shared group table flushed, without a final
+ * barrier */
+__device__ __forceinline__ void
+xbj_body(const XbExecArgs &args, char *smem)
 {
-    extern __shared__ __align__(16) char smem[];
     const uint32_t lane = threadIdx.x & 31;
     XbSrcMeta *meta = (XbSrcMeta *)smem;
     /* warp-uniform work-distribution state lives in shared memory, not in
@@ -233,6 +235,36 @@ xbj_kernel(XbExecArgs args)
                 atomicOr(&args.gt->overflow, 1u);
             }
         }
+    }
+}
+
+extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
+xbj_kernel(const __grid_constant__ XbExecArgs args)
+{
+    extern __shared__ __align__(16) char smem[];
+    xbj_body(args, smem);
+}
+
+/* mixed launch of commands of sessions that share this kernel (same plan
+ * shape; their constants, tables and statuses come with each command):
+ * work item i sends a CTA to command items[i], as in xb_mixed_kernel */
+extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
+xbj_mixed_kernel(const __grid_constant__ XbMixArgs m)
+{
+    extern __shared__ __align__(16) char smem[];
+    __shared__ XbExecArgs cmd;
+    __shared__ uint32_t item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            item = atomicAdd(m.cursor, 1u);
+            if (item < m.nitems)
+                cmd = m.cmds[m.items[item]];
+        }
+        __syncthreads();
+        if (item >= m.nitems)
+            break;
+        xbj_body(cmd, smem);
+        __syncthreads();
     }
 }
 

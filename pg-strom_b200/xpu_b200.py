@@ -65,7 +65,8 @@ def lib():
         L.xpuB200MixExec.argtypes = [P, P, P]
         L.xpuB200MixTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
         L.xpuB200MixInfo.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64),
-                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(I)]
+                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                                     ctypes.POINTER(ctypes.c_uint32)]
         L.xpuB200MixDestroy.argtypes = [P]
         L.xpuB200SessionInfo.argtypes = [P, ctypes.c_char_p, U64]
         L.xpuB200HashBytes.argtypes = [P, ctypes.c_uint32]
@@ -325,9 +326,12 @@ class Mix:
         return ms.value
 
     def info(self):
-        b, u, it, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_int()
-        lib().xpuB200MixInfo(self.h, ctypes.byref(b), ctypes.byref(u), ctypes.byref(it), ctypes.byref(g))
-        return {"bytes": b.value, "units": u.value, "items": it.value, "grid": g.value}
+        b, u = ctypes.c_uint64(), ctypes.c_uint64()
+        it, nl, ns = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        lib().xpuB200MixInfo(self.h, ctypes.byref(b), ctypes.byref(u), ctypes.byref(it), ctypes.byref(nl),
+                             ctypes.byref(ns))
+        return {"bytes": b.value, "units": u.value, "items": it.value, "launches": nl.value,
+                "specialised": ns.value}
 
     def close(self):
         if self.h:

@@ -31,13 +31,22 @@ def _close_all(device, sessions, bases):
         device.free(b)
 
 
-def test_mixed_batch_matches_truth_and_oracle(device):
+@pytest.fixture(params=["jit", "vm"])
+def kernel(request, monkeypatch):
+    monkeypatch.setenv("XPU_B200_JIT", "1" if request.param == "jit" else "0")
+    return request.param
+
+
+def test_mixed_batch_matches_truth_and_oracle(device, kernel):
     cmds = C.mixed_commands(ncmds=96, max_bytes=4 << 20, max_groups=100_000)
     sessions, bases, dptrs = _open_all(device, cmds)
     mix = xpu_b200.Mix(device, sessions, dptrs)
     try:
         info = mix.info()
         assert info["items"] >= len(cmds)
+        # one plan shape: one persistent launch, specialised unless disabled
+        assert info["launches"] == 1
+        assert info["specialised"] == (len(cmds) if kernel == "jit" else 0)
         out = mix.exec()
         for i, ((res, err), c, s) in enumerate(zip(out, cmds, sessions)):
             assert err is None, f"command {i}: {err}"
@@ -110,3 +119,35 @@ def test_mixed_batch_several_chunks_of_one_session(device):
         for b in bases:
             device.free(b)
         _close_all(device, o_sessions, o_bases)
+
+
+def test_mixed_batch_of_two_plan_shapes(device):
+    # join commands and scan commands: one persistent launch per kernel,
+    # running concurrently inside the replayed graph
+    fact, jsess, km, expect, _ = C.join_groupby(nfact=200_000, ndim1=20_000, ndim2=2_000)
+    jchunks = fact.block_chunks(pages_per_chunk=400)
+    scans = C.mixed_commands(ncmds=10, max_bytes=1 << 20, max_groups=5_000, seed_config=8)
+    js = xpu_b200.Session(device, jsess, km, 2)
+    s_sessions, s_bases, s_dptrs = _open_all(device, scans)
+    j_bases, j_dptrs = [], []
+    for ch in jchunks:
+        b, p = device.upload(ch)
+        j_bases.append(b)
+        j_dptrs.append(p)
+    mix = xpu_b200.Mix(device, [js] * len(jchunks) + s_sessions, j_dptrs + s_dptrs)
+    try:
+        assert mix.info()["launches"] == 2
+        assert all(err is None for _, err in mix.exec())
+        jf, _ = js.final()
+        truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+        assert F.compare_groups(F.decode_kds_final(jf, jsess), truth) == []
+        for c, s in zip(scans, s_sessions):
+            f, _ = s.final()
+            got = F.decode_kds_final(f, c["session"]) if f is not None else {}
+            assert F.compare_groups(got, c["truth"]) == []
+    finally:
+        mix.close()
+        js.close()
+        for b in j_bases:
+            device.free(b)
+        _close_all(device, s_sessions, s_bases)
