@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--rows", type=int, default=100_000_000)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default="join_groupby", choices=["join_groupby", "mixed", "served"],
+                    help="join_groupby: the headline line; mixed: 256 batched chunk commands; "
+                         "served: Poisson-arrival query mix through the serving scheduler")
+    ap.add_argument("--requests", type=int, default=400)
+    ap.add_argument("--qps", type=float, default=200.0)
     return ap.parse_args()
 
 
@@ -388,8 +393,263 @@ def run_b200(args, rank, world, local):
     dev.close()
 
 
+# ------------------------------------------------------------------ batched commands
+def run_mixed(args):
+    """256 chunk commands on the plain scan schema (one session each; chunk
+    sizes log-uniform 64 KB-64 MB, selectivity U[0.1%,90%], group counts
+    log-uniform 1-1M) as one mixed batch: one persistent launch per kernel,
+    replayed from a captured CUDA graph.  Beside it: the same commands as
+    plain per-command xpuB200ExecTask calls on the same resident chunks."""
+    import torch
+    import xb_configs as C
+    import xpu_b200
+    t0 = time.time()
+    cmds = C.mixed_commands(ncmds=256)
+    gen_s = time.time() - t0
+    dev = xpu_b200.Device(0)
+    sessions = [xpu_b200.Session(dev, c["session"]) for c in cmds]
+    ups = [dev.upload(c["chunk"]) for c in cmds]
+    mix = xpu_b200.Mix(dev, sessions, [p for _, p in ups])
+    out = mix.exec()
+    assert all(err is None for _, err in out), [str(e) for _, e in out if e][:3]
+    for (r, _), c in zip(out, cmds):
+        assert r["nitems_in"] == c["meta"]["nitems_in"]
+    for _ in range(max(0, args.warmup - 1)):
+        mix.exec()
+    sampler = ClockSampler(0)
+    torch.cuda.synchronize()
+    sampler.start()
+    ms = mix.time(args.steps)
+    clocks = sampler.stop()
+    info = mix.info()
+    rows = sum(c["params"]["rows"] for c in cmds)
+    # plain drop-in: one ExecTask per command, each waiting for its result
+    for s, (_, p) in zip(sessions, ups):
+        s.exec(p, on_device=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        for s, (_, p) in zip(sessions, ups):
+            s.exec(p, on_device=True)
+    plain_ms = 1000.0 * (time.perf_counter() - t1) / args.steps
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = info["bytes"] / (ms / 1000.0) / 1e9
+    line = {"metric": "batched chunk commands rows/s", "value": rows / (ms / 1000.0), "unit": "rows/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "256 scan/pre-agg commands on the plain scan schema, chunks log-uniform "
+                                   "64 KB-64 MB, selectivity U[0.1%,90%], group counts log-uniform 1-1M",
+                       "commands": len(cmds), "rows": rows, "chunk_bytes": info["bytes"],
+                       "launches_per_run": info["launches"], "specialised_commands": info["specialised"],
+                       "work_items": info["items"], "generation_s": round(gen_s, 1),
+                       "l2_note": "inputs (2.2 GB) exceed L2 (126 MB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+            "plain": {"ms_per_run": plain_ms, "rows_per_s": rows / (plain_ms / 1000.0),
+                      "how": "one xpuB200ExecTask per command on the same resident chunks, sequential"},
+            "clocks": clocks, "gpu_launches": args.steps * info["launches"]}
+    print(json.dumps(line), flush=True)
+    mix.close()
+    for s in sessions:
+        s.close()
+    for b, _ in ups:
+        dev.free(b)
+    dev.close()
+
+
+# ------------------------------------------------------------------ served mix
+class _Tables:
+    """Device-resident tables of the three query templates."""
+
+    def __init__(self, dev, rows0, rows1, rows2):
+        import xb_configs as C
+        self.bytes = 0
+
+        def up(chunks):
+            self.bytes += sum(c.nbytes for c in chunks)
+            return [dev.upload(c) for c in chunks]
+        tbl0, _, _, _, _ = C.scan_groupby(nrows=rows0, seed_config=20)
+        self.t0 = up(tbl0.block_chunks(pages_per_chunk=8190))
+        self.rows0 = rows0
+        del tbl0
+        fact, _, km, _, _ = C.join_groupby(nfact=rows1, seed_config=21)
+        self.t1 = up(fact.block_chunks(pages_per_chunk=8190))
+        self.km = km
+        self.rows1 = rows1
+        del fact
+        chunks2, _, _, _ = C.arrow_groupby(nrows=rows2, nkeys=10_000_000, seed_config=22,
+                                           rows_per_chunk=2_500_000, with_expect=False)
+        self.t2 = up(chunks2)
+        self.rows2 = rows2
+
+    def free(self, dev):
+        for t in (self.t0, self.t1, self.t2):
+            for b, _ in t:
+                dev.free(b)
+
+
+def _requests(tables, n, qps, seed=0x5EED):
+    """Poisson arrivals; templates 50/30/20; rows log-uniform from 1M to
+    the table; randomized predicate constants."""
+    import xb_configs as C
+    r = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for i in range(n):
+        t += r.exponential(1.0 / qps)
+        u = r.random()
+        if u < 0.5:
+            rows = int(np.exp(r.uniform(np.log(1e6), np.log(tables.rows0))))
+            k = max(1, round(rows / tables.rows0 * len(tables.t0)))
+            sess = C.scan_groupby_session(a_limit=int(r.integers(1, 1000)), ngroups=64)
+            out.append({"t": t, "tpl": 0, "session": sess, "km": None, "nrels": 0,
+                        "chunks": [p for _, p in tables.t0[:k]]})
+        elif u < 0.8:
+            rows = int(np.exp(r.uniform(np.log(1e6), np.log(tables.rows1))))
+            k = max(1, round(rows / tables.rows1 * len(tables.t1)))
+            sess = C.join_groupby_session(flag_limit=int(r.integers(1, 5)))
+            out.append({"t": t, "tpl": 1, "session": sess, "km": tables.km, "nrels": 2,
+                        "chunks": [p for _, p in tables.t1[:k]]})
+        else:
+            rows = int(np.exp(r.uniform(np.log(1e6), np.log(tables.rows2))))
+            k = max(1, round(rows / tables.rows2 * len(tables.t2)))
+            lo = 16436 + int(r.integers(0, 3652 - 730))
+            est = min(10_000_000, k * 2_500_000 // 5)
+            sess = C.arrow_groupby_session(lo_day=lo, hi_day=lo + 730, ngroups_estimate=est)
+            out.append({"t": t, "tpl": 2, "session": sess, "km": None, "nrels": 0,
+                        "chunks": [p for _, p in tables.t2[:k]]})
+    return out
+
+
+def _serve_plain(dev, reqs, start):
+    """One query at a time in arrival order: OpenSession, ExecTask per
+    chunk, Final, CloseSession (the plain drop-in)."""
+    import xpu_b200
+    lat = []
+    for q in reqs:
+        while time.perf_counter() - start < q["t"]:
+            pass
+        s = xpu_b200.Session(dev, q["session"], q["km"], q["nrels"])
+        for p in q["chunks"]:
+            s.exec(p, on_device=True)
+        s.final()
+        s.close()
+        lat.append(time.perf_counter() - start - q["t"])
+    return lat, time.perf_counter() - start
+
+
+MAX_ACTIVE = 16                 # queries admitted at once (each holds its group table)
+FINAL_THREADS = 4               # kds_final read-backs in flight
+FINAL_BUF_BYTES = 1536 << 20    # pinned response buffer per read-back
+
+
+def _pinned_buffers():
+    import queue
+    import torch
+    q = queue.Queue()
+    for _ in range(FINAL_THREADS):
+        q.put(torch.empty(FINAL_BUF_BYTES, dtype=torch.uint8, pin_memory=True).numpy())
+    return q
+
+
+def _serve_batched(dev, reqs, start, bufs):
+    """Continuous batching: a query's chunks are submitted when it arrives
+    and a query slot is free; finished queries are finalised (kds_final read
+    back) by worker threads while other queries run on the GPU."""
+    from concurrent.futures import ThreadPoolExecutor
+    import xpu_b200
+    lat = [None] * len(reqs)
+    running, finishing = {}, {}
+    nxt, ndone = 0, 0
+
+    def finish(i, s):
+        buf = bufs.get()
+        try:
+            s.final(out=buf)
+        finally:
+            bufs.put(buf)
+        s.close()
+        lat[i] = time.perf_counter() - start - reqs[i]["t"]
+
+    with ThreadPoolExecutor(max_workers=FINAL_THREADS) as pool:
+        while ndone < len(reqs):
+            now = time.perf_counter() - start
+            while (nxt < len(reqs) and reqs[nxt]["t"] <= now and
+                   len(running) + len(finishing) < MAX_ACTIVE):
+                q = reqs[nxt]
+                s = xpu_b200.Session(dev, q["session"], q["km"], q["nrels"])
+                running[nxt] = (s, [dev.submit(s, p, on_device=True) for p in q["chunks"]])
+                nxt += 1
+            for i in list(running):
+                s, tickets = running[i]
+                left = [t for t in tickets if dev.poll(t, nrels=reqs[i]["nrels"], wait=False) is None]
+                if left:
+                    running[i] = (s, left)
+                    continue
+                del running[i]
+                finishing[i] = pool.submit(finish, i, s)
+            for i in list(finishing):
+                if finishing[i].done():
+                    finishing.pop(i).result()
+                    ndone += 1
+    return lat, time.perf_counter() - start
+
+
+def run_served(args):
+    """Served mixed workload: Poisson arrivals (mean --qps) of queries drawn
+    50/30/20 from the three templates over device-resident tables, served
+    by the plain drop-in (one query at a time) and by the serving scheduler
+    (Submit/Poll, continuous batching).  Open-loop latency p50/p99 at the
+    offered rate, and saturation throughput (every query queued at once)."""
+    import xpu_b200
+    dev = xpu_b200.Device(0)
+    t0 = time.time()
+    tables = _Tables(dev, rows0=16_000_000, rows1=50_000_000, rows2=50_000_000)
+    gen_s = time.time() - t0
+    reqs = _requests(tables, args.requests, args.qps)
+    warm = _requests(tables, 30, args.qps, seed=7)
+    bufs = _pinned_buffers()
+    served = lambda d, r, t: _serve_batched(d, r, t, bufs)
+    _serve_plain(dev, warm, time.perf_counter())      # kernel cache, pools
+    served(dev, warm, time.perf_counter())
+    res = {}
+    for mode, fn in (("plain", _serve_plain), ("served", served)):
+        lat, el = fn(dev, reqs, time.perf_counter())
+        sat = [dict(q, t=0.0) for q in reqs]
+        _, sat_el = fn(dev, sat, time.perf_counter())
+        res[mode] = {"qps": len(reqs) / el, "p50_ms": 1000 * float(np.percentile(lat, 50)),
+                     "p99_ms": 1000 * float(np.percentile(lat, 99)),
+                     "saturation_qps": len(reqs) / sat_el}
+    mix = {k: sum(1 for q in reqs if q["tpl"] == k) for k in range(3)}
+    line = {"metric": "served QPS (p50/p99 latency)", "value": res["served"]["saturation_qps"],
+            "unit": "queries/s", "n_gpus": 1, "higher_is_better": True, "vs_baseline": None,
+            "dtype": "int64", "data": "synthetic (seeded)",
+            "config": {"workload": "Poisson arrivals, templates 50/30/20 (scan+group-by 16M-row heap, "
+                                   "two-way join 50M-row heap, Arrow group-by 50M rows), rows log-uniform "
+                                   "1M..table per query, randomized constants, tables resident in HBM",
+                       "requests": len(reqs), "offered_qps": args.qps, "template_counts": mix,
+                       "resident_bytes": tables.bytes, "generation_s": round(gen_s, 1)},
+            "served": res["served"], "plain": res["plain"],
+            "saturation_ratio": res["served"]["saturation_qps"] / res["plain"]["saturation_qps"]}
+    print(json.dumps(line), flush=True)
+    tables.free(dev)
+    dev.close()
+
+
 def main():
     args = parse()
+    if args.workload != "join_groupby":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
+                                                                  "form of this path"}), flush=True)
+            return
+        return run_mixed(args) if args.workload == "mixed" else run_served(args)
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

@@ -1356,13 +1356,67 @@ struct xpuB200Device {
     size_t          smem_optin;     /* dynamic shared memory a CTA may opt in to */
     cudaStream_t    stream;
     struct xb_sched *sched = nullptr; /* asynchronous commands (created by the first submit) */
+    /* recycled per-session resources: creating a stream or pinning host
+     * memory costs far more than a query's own host work */
+    std::mutex      pool_lock;
+    std::vector<cudaStream_t> free_streams;
+    std::vector<xb_status *> free_status;
+    std::vector<xb_status *> status_blocks;
 };
+
+static cudaStream_t xb_get_stream(xpuB200Device *dev)
+{
+    {
+        std::lock_guard<std::mutex> g(dev->pool_lock);
+        if (!dev->free_streams.empty()) {
+            cudaStream_t st = dev->free_streams.back();
+            dev->free_streams.pop_back();
+            return st;
+        }
+    }
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        return nullptr;
+    return st;
+}
+
+static void xb_put_stream(xpuB200Device *dev, cudaStream_t st)
+{
+    if (!st) return;
+    std::lock_guard<std::mutex> g(dev->pool_lock);
+    dev->free_streams.push_back(st);
+}
+
+static xb_status *xb_get_status(xpuB200Device *dev)
+{
+    std::lock_guard<std::mutex> g(dev->pool_lock);
+    if (dev->free_status.empty()) {
+        const int n = 64;
+        xb_status *blk = nullptr;
+        if (cudaMallocHost((void **)&blk, sizeof(xb_status) * n) != cudaSuccess)
+            return nullptr;
+        dev->status_blocks.push_back(blk);
+        for (int i = 0; i < n; i++)
+            dev->free_status.push_back(blk + i);
+    }
+    xb_status *p = dev->free_status.back();
+    dev->free_status.pop_back();
+    return p;
+}
+
+static void xb_put_status(xpuB200Device *dev, xb_status *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> g(dev->pool_lock);
+    dev->free_status.push_back(p);
+}
 
 static void xb_sched_drain_session(xpuB200Session *s);
 static void xb_sched_destroy(xpuB200Device *dev);
 
 struct xpuB200Session {
     xpuB200Device  *dev;
+    cudaStream_t    stream = nullptr;
     std::mutex      lock;
     std::vector<char> h_session;
     char           *d_session = nullptr;
@@ -1476,6 +1530,15 @@ xpuB200Init(int cuda_dindex, uint64_t hbm_budget, xpuB200Device **p_dev, kern_er
         hbm_budget = (uint64_t)(fr * 0.9);
     }
     dev->hbm_budget = hbm_budget;
+    /* sessions allocate from the device's stream-ordered pool; keep freed
+     * memory in the pool instead of returning it at every synchronisation */
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, cuda_dindex) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     /* the kernels shared by all sessions opt in to the whole of shared
      * memory once, so that no session lowers another's limit */
     dev->smem_optin = prop.sharedMemPerBlockOptin;
@@ -1506,28 +1569,38 @@ xpuB200Shutdown(xpuB200Device *dev)
     xb_sched_destroy(dev);
     cudaStreamSynchronize(dev->stream);
     cudaStreamDestroy(dev->stream);
+    for (cudaStream_t st : dev->free_streams)
+        cudaStreamDestroy(st);
+    for (xb_status *b : dev->status_blocks)
+        cudaFreeHost(b);
     delete dev;
 }
 
 static void xb_session_free(xpuB200Session *s)
 {
     cudaSetDevice(s->dev->dindex);
-    cudaStreamSynchronize(s->dev->stream);
+    /* session memory comes from the device's stream-ordered pool, on the
+     * session's stream: freeing it waits for no other stream (a plain
+     * cudaFree would wait for the whole device, i.e. every other session's
+     * work) */
+    cudaStream_t st = s->stream;
     for (void *p : s->d_allocs)
-        cudaFree(p);
-    if (s->d_src) cudaFree(s->d_src);
-    if (s->d_tasks) cudaFree(s->d_tasks);
-    if (s->d_dst) cudaFree(s->d_dst);
-    if (s->h_status) cudaFreeHost(s->h_status);
+        cudaFreeAsync(p, st);
+    if (s->d_src) cudaFreeAsync(s->d_src, st);
+    if (s->d_tasks) cudaFreeAsync(s->d_tasks, st);
+    if (s->d_dst) cudaFreeAsync(s->d_dst, st);
+    cudaStreamSynchronize(st);
+    xb_put_status(s->dev, s->h_status);
     if (s->h_plan) free(s->h_plan);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);
+    xb_put_stream(s->dev, s->stream);
     delete s;
 }
 
 static int xb_dalloc(xpuB200Session *s, size_t sz, void **p, kern_errorbuf *err)
 {
-    cudaError_t rc = cudaMalloc(p, sz < 256 ? 256 : sz);
+    cudaError_t rc = cudaMallocAsync(p, sz < 256 ? 256 : sz, s->stream);
     if (rc != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -1556,6 +1629,13 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     XB_CUDA(cudaSetDevice(dev->dindex), err);
     xpuB200Session *s = new xpuB200Session();
     s->dev = dev;
+    /* every session has its own stream, so that one session's launches,
+     * copies and waits never wait for another's */
+    s->stream = xb_get_stream(dev);
+    if (!s->stream) {
+        delete s;
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cudaStreamCreate failed");
+    }
     cudaEventCreate(&s->ev0);
     cudaEventCreate(&s->ev1);
     int rc;
@@ -1576,11 +1656,12 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
                            s->h_plan, msg, sizeof(msg)) != 0)
         FAIL(ERRCODE_DEVICE_ERROR, "bytecode translation: %s", msg);
     xb_plan *plan = s->h_plan;
-    cudaStream_t st = dev->stream;
+    cudaStream_t st = s->stream;
     if (cudaMemcpyAsync(s->d_session, session, session_sz, cudaMemcpyHostToDevice, st) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "session upload failed");
     DALLOC(sizeof(xb_status), &s->d_status);
-    if (cudaMallocHost((void **)&s->h_status, sizeof(xb_status)) != cudaSuccess)
+    s->h_status = xb_get_status(dev);
+    if (!s->h_status)
         FAIL(ERRCODE_DEVICE_FATAL, "cudaMallocHost failed");
     cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st);
 
@@ -1632,7 +1713,9 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         double est = ((const kern_session_info *)s->h_session.data())->groupby_ngroups_estimation;
         if (!(est >= 1.0)) est = 1.0;
         if (plan->has_groupby == 2) est = 1.0;
-        uint64_t cap = xb_next_pow2((uint64_t)(est * 4) + 1024);
+        /* open addressing at a load of at most 1/4 (small tables) or 1/2
+         * (above a million groups, where the table's bytes matter) */
+        uint64_t cap = xb_next_pow2((uint64_t)(est * (est > 1e6 ? 2 : 4)) + 1024);
         uint64_t max_cap = (dev->hbm_budget / 4) / plan->gent_size;
         if (cap > max_cap) cap = xb_next_pow2(max_cap / 2 + 1);
         uint64_t arena = plan->nkeys_text ? (64ULL << 20) + cap * 32 : 256;
@@ -1858,7 +1941,7 @@ static void *xb_session_jit(xpuB200Session *s, uint32_t format)
 static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                            uint64_t nunits, uint32_t format, kern_errorbuf *err)
 {
-    return xb_launch_on(s, d_tasks, ntasks, nunits, format, s->dev->stream, s->d_status, err);
+    return xb_launch_on(s, d_tasks, ntasks, nunits, format, s->stream, s->d_status, err);
 }
 
 static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
@@ -1908,7 +1991,7 @@ static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
         h_kds_head->format != KDS_FORMAT_ROW)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", h_kds_head->format);
     if (!s->d_tasks) {
-        XB_CUDA(cudaMalloc((void **)&s->d_tasks, sizeof(xb_task) * 16), err);
+        XB_CUDA(cudaMallocAsync((void **)&s->d_tasks, sizeof(xb_task) * 16, s->stream), err);
         s->d_tasks_cap = 16;
     }
     xb_task t;
@@ -1916,7 +1999,7 @@ static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
     t.unit_base = 0;
     t.nunits = xb_chunk_units(h_kds_head);
     t.format = (uint32_t)h_kds_head->format;
-    XB_CUDA(cudaMemcpyAsync(s->d_tasks, &t, sizeof(t), cudaMemcpyHostToDevice, s->dev->stream), err);
+    XB_CUDA(cudaMemcpyAsync(s->d_tasks, &t, sizeof(t), cudaMemcpyHostToDevice, s->stream), err);
     return xb_launch_tasks(s, s->d_tasks, 1, t.nunits, t.format, err);
 }
 
@@ -1952,7 +2035,7 @@ static int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
 /* wait for the launch and read its status (errors reported by the kernel) */
 static int xb_wait_status(xpuB200Session *s, kern_errorbuf *err)
 {
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     cudaMemcpyAsync(s->h_status, s->d_status, sizeof(xb_status), cudaMemcpyDeviceToHost, st);
     cudaError_t rc = cudaStreamSynchronize(st);
     if (rc != cudaSuccess)
@@ -2027,7 +2110,7 @@ xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_o
     std::vector<char> hbuf;
     int rc = xb_place_src(s, kds_src, kds_src_on_device, &head, &hbuf, &d_kds, err);
     if (rc) return rc;
-    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->dev->stream), err);
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
     rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
     if (rc) return rc;
     return xb_finish_task(s, results, err);
@@ -2039,7 +2122,7 @@ static int xb_place_src(xpuB200Session *s, const kern_data_store *kds_src, int k
                         kern_data_store *p_head, std::vector<char> *p_hbuf,
                         const kern_data_store **p_dkds, kern_errorbuf *err)
 {
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     kern_data_store &head = *p_head;
     std::vector<char> &hbuf = *p_hbuf;
     const kern_data_store *d_kds;
@@ -2061,10 +2144,10 @@ static int xb_place_src(xpuB200Session *s, const kern_data_store *kds_src, int k
         uint64_t shift = (kds_src->format == KDS_FORMAT_BLOCK) ? ((16 - (kds_src->block_offset & 15)) & 15) : 0;
         uint64_t need = kds_src->length + shift + 64;
         if (need > s->d_src_cap) {
-            if (s->d_src) cudaFree(s->d_src);
+            if (s->d_src) cudaFreeAsync(s->d_src, st);
             s->d_src = nullptr;
             s->d_src_cap = 0;
-            XB_CUDA(cudaMalloc((void **)&s->d_src, need + (need >> 3)), err);
+            XB_CUDA(cudaMallocAsync((void **)&s->d_src, need + (need >> 3), st), err);
             s->d_src_cap = need + (need >> 3);
         }
         XB_CUDA(cudaMemcpyAsync(s->d_src + shift, kds_src, kds_src->length, cudaMemcpyHostToDevice, st), err);
@@ -2094,7 +2177,7 @@ xpuB200ExecTaskDst(xpuB200Session *s, const kern_data_store *kds_src, int kds_sr
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "kds_dst of %llu bytes cannot hold a row",
                       (unsigned long long)dst_sz);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     kern_data_store head;
     const kern_data_store *d_kds;
     std::vector<char> hbuf;
@@ -2107,10 +2190,10 @@ xpuB200ExecTaskDst(xpuB200Session *s, const kern_data_store *kds_src, int kds_sr
         d_dst = (char *)kds_dst;
     } else {
         if (len > s->d_dst_cap) {
-            if (s->d_dst) cudaFree(s->d_dst);
+            if (s->d_dst) cudaFreeAsync(s->d_dst, st);
             s->d_dst = nullptr;
             s->d_dst_cap = 0;
-            XB_CUDA(cudaMalloc((void **)&s->d_dst, len), err);
+            XB_CUDA(cudaMallocAsync((void **)&s->d_dst, len, st), err);
             s->d_dst_cap = len;
         }
         d_dst = s->d_dst;
@@ -2162,7 +2245,7 @@ xpuB200TimeExecTask(xpuB200Session *s, const kern_data_store *kds_src_dev, int n
     xb_clear_error(err);
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     kern_data_store head;
     if (((uintptr_t)kds_src_dev & 7) != 0)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
@@ -2198,7 +2281,7 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     xb_sched_drain_session(s);
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     const xb_plan *plan = s->h_plan;
     if (results) {
         uint32_t cap = results->num_rels;
@@ -2227,11 +2310,11 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     int rc = 0;
     std::vector<void *> tmp;
     auto alloc = [&](size_t sz, void **p) -> bool {
-        if (cudaMalloc(p, sz < 256 ? 256 : sz) != cudaSuccess) { cudaGetLastError(); return false; }
+        if (cudaMallocAsync(p, sz < 256 ? 256 : sz, st) != cudaSuccess) { cudaGetLastError(); return false; }
         tmp.push_back(*p);
         return true;
     };
-    auto cleanup = [&]() { for (void *p : tmp) cudaFree(p); };
+    auto cleanup = [&]() { for (void *p : tmp) cudaFreeAsync(p, st); };
     if (!alloc(cap * 8, (void **)&d_sizes) || !alloc(cap * 8, (void **)&d_size_scan) ||
         !alloc(cap * 4, (void **)&d_flags) || !alloc(cap * 4, (void **)&d_flag_scan)) {
         cleanup();
@@ -2318,12 +2401,12 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
  * Final without device allocations
  *
  * xpuB200Final allocates its work arrays (per-slot tuple sizes, their
- * prefix sums, CUB scan storage) and a device copy of kds_final with
- * cudaMalloc on every call.  Some callers cannot do that: a service that
- * has reserved the GPU's memory up front and hands out pieces of its own
- * pool (as PG-Strom's GPU service does with its device memory), or one
- * that must not call cudaMalloc / cudaFree while other sessions' kernels
- * run, because cudaFree waits for the whole device.  This variant writes
+ * prefix sums, CUB scan storage) and a device copy of kds_final from the
+ * device's memory pool on every call.  Some callers cannot do that: a
+ * service that has reserved the GPU's memory up front and hands out pieces
+ * of its own pool (as PG-Strom's GPU service does with its device memory),
+ * or one that must not allocate device memory while other sessions'
+ * kernels run (a plain cudaFree waits for the whole device).  This variant writes
  * kds_final into memory the caller already owns and keeps its work arrays
  * in the fixed array below, which lives in the library's module on every
  * GPU that loads it until the process exits.
@@ -2369,7 +2452,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
         xb_final_scratch_dptr[dindex] = ptr;
     }
     char *scratch = (char *)xb_final_scratch_dptr[dindex];
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     const xb_plan *plan = s->h_plan;
     if (results) {
         uint32_t cap = results->num_rels;
@@ -2570,7 +2653,7 @@ xpuB200BatchExec(xpuB200Batch *b, kern_exec_results *results, kern_errorbuf *err
     xpuB200Session *s = b->sess;
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->dev->stream), err);
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
     int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
     if (rc) return rc;
     return xb_finish_task(s, results, err);
@@ -2583,7 +2666,7 @@ xpuB200BatchTime(xpuB200Batch *b, int niters, double *p_msec, kern_errorbuf *err
     xpuB200Session *s = b->sess;
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->dev->stream;
+    cudaStream_t st = s->stream;
     float total = 0.0f;
     for (int i = 0; i < niters; i++) {
         XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);

@@ -49,6 +49,22 @@ def host_join_hash_int4(keys: np.ndarray) -> np.ndarray:
 
 
 # ---------------------------------------------------------------------------
+def scan_groupby_session(a_limit=300, ngroups=64):
+    """WHERE a < a_limit GROUP BY g -> count(*), sum(a), sum(c), avg(b)."""
+    typmod_c = numeric_typmod(12, 2)
+    va, vb, vc, vg = (Var(0, 2, "int4"), Var(0, 3, "float8"),
+                      Var(0, 4, "numeric", typmod_c), Var(0, 5, "int4"))
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    return sb.build(
+        scan_quals=Func("int4lt", [va, Const("int4", a_limit)], "bool"),
+        groupby_keys=[vg],
+        aggs=[Agg("NROWS_ANY"),
+              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")),
+              Agg("PSUM_NUMERIC", vc, typmod_c),
+              Agg("PAVG_FP", vb)],
+        ngroups_estimate=float(ngroups))
+
+
 def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ngroups=64):
     """The plain scan + filter + group-by table; ngroups sets the domain of
     g (64 in the benchmark configuration)."""
@@ -67,17 +83,7 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ng
         Column("c", "numeric", typmod=typmod_c, values=encode_numeric_array(c_unscaled, 2)),
         Column("g", "int4", values=g),
     ], nrows)
-    va, vb, vc, vg = (Var(0, 2, "int4"), Var(0, 3, "float8"),
-                      Var(0, 4, "numeric", typmod_c), Var(0, 5, "int4"))
-    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
-    session = sb.build(
-        scan_quals=Func("int4lt", [va, Const("int4", a_limit)], "bool"),
-        groupby_keys=[vg],
-        aggs=[Agg("NROWS_ANY"),
-              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")),
-              Agg("PSUM_NUMERIC", vc, typmod_c),
-              Agg("PAVG_FP", vb)],
-        ngroups_estimate=float(ngroups))
+    session = scan_groupby_session(a_limit, ngroups)
     # expected partial states per group, straight from the arrays
     m = a < a_limit
     gm = g[m]
@@ -112,6 +118,24 @@ def zipf_bounded(r, n, s, size):
     cdf /= cdf[-1]
     u = r.random(size)
     return (np.searchsorted(cdf, u, side="right") + 1).astype(np.int32)
+
+
+def join_groupby_session(flag_limit=3):
+    """fact JOIN dim1 ON fk1 = pk JOIN dim2 ON fk2 = pk AND flag < flag_limit
+    GROUP BY region -> sum(qty * price), count(*)."""
+    f_fk1, f_fk2, f_qty, f_price = (Var(0, 1, "int4"), Var(0, 2, "int4"),
+                                    Var(0, 3, "int4"), Var(0, 4, "int8"))
+    d1_pk, d1_region = Var(1, 1, "int4"), Var(1, 2, "text")
+    d2_pk, d2_flag = Var(2, 1, "int4"), Var(2, 2, "int2")
+    sb = SessionBuilder(2, DEVTASK_JOIN | DEVTASK_PREAGG | DEVKIND_GPU)
+    return sb.build(
+        joins=[([f_fk1], [Func("int4eq", [f_fk1, d1_pk], "bool")], []),
+               ([f_fk2], [Func("int4eq", [f_fk2, d2_pk], "bool")],
+                [Func("int24lt", [d2_flag, Const("int4", flag_limit)], "bool")])],
+        groupby_keys=[d1_region],
+        aggs=[Agg("PSUM_INT64", Func("int48mul", [f_qty, f_price], "int8")),
+              Agg("NROWS_ANY")],
+        ngroups_estimate=25.0)
 
 
 def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3,
@@ -155,19 +179,7 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
                           Column("qty", "int4", values=qty), Column("price", "int8", values=price)], nfact)
     kmrels = kern_multirels([dim1.hash_kds(host_join_hash_int4(pk1)),
                              dim2.hash_kds(host_join_hash_int4(pk2))])
-    f_fk1, f_fk2, f_qty, f_price = (Var(0, 1, "int4"), Var(0, 2, "int4"),
-                                    Var(0, 3, "int4"), Var(0, 4, "int8"))
-    d1_pk, d1_region = Var(1, 1, "int4"), Var(1, 2, "text")
-    d2_pk, d2_flag = Var(2, 1, "int4"), Var(2, 2, "int2")
-    sb = SessionBuilder(2, DEVTASK_JOIN | DEVTASK_PREAGG | DEVKIND_GPU)
-    session = sb.build(
-        joins=[([f_fk1], [Func("int4eq", [f_fk1, d1_pk], "bool")], []),
-               ([f_fk2], [Func("int4eq", [f_fk2, d2_pk], "bool")],
-                [Func("int24lt", [d2_flag, Const("int4", flag_limit)], "bool")])],
-        groupby_keys=[d1_region],
-        aggs=[Agg("PSUM_INT64", Func("int48mul", [f_qty, f_price], "int8")),
-              Agg("NROWS_ANY")],
-        ngroups_estimate=25.0)
+    session = join_groupby_session(flag_limit)
     # expected: every (fact row, dim1 copy) pair that passes both joins
     m = (flag[idx2] < flag_limit) & ~miss
     amount = qty.astype(np.int64) * price
@@ -203,6 +215,21 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
 UNIX_TO_PG_DAYS = 10957                     # POSTGRES_EPOCH_JDATE - UNIX_EPOCH_JDATE
 
 
+def arrow_groupby_session(lo_day=17532, hi_day=18262, ngroups_estimate=10_000_000.0):
+    """WHERE d >= lo_day AND d < hi_day (Unix days) GROUP BY k -> count(*),
+    sum(v1), min(v2), max(v2), sum(v2)."""
+    from xb_producer import BoolOp
+    vk, vv1, vv2, vd = Var(0, 1, "int8"), Var(0, 2, "int4"), Var(0, 3, "float8"), Var(0, 4, "date")
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    return sb.build(
+        scan_quals=BoolOp("And", [Func("date_ge", [vd, Const("date", lo_day - UNIX_TO_PG_DAYS)], "bool"),
+                                  Func("date_lt", [vd, Const("date", hi_day - UNIX_TO_PG_DAYS)], "bool")]),
+        groupby_keys=[vk],
+        aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Func("int4_to_int8", [vv1], "int8")),
+              Agg("PMIN_FP64", vv2), Agg("PMAX_FP64", vv2), Agg("PSUM_FP", vv2)],
+        ngroups_estimate=float(ngroups_estimate))
+
+
 def arrow_groupby(nrows=500_000_000, nkeys=10_000_000, seed_config=2, rows_per_chunk=2_500_000,
                   with_expect=True):
     """Arrow columnar high-cardinality pre-aggregation:
@@ -216,17 +243,7 @@ def arrow_groupby(nrows=500_000_000, nkeys=10_000_000, seed_config=2, rows_per_c
     d0 = 16436                                  # 2015-01-01 in Unix days
     lo_day, hi_day = 17532, 18262               # 2018-01-01, 2020-01-01
     typs = [("k", "int8"), ("v1", "int4"), ("v2", "float8"), ("d", "date"), ("s", "text")]
-    tbl = Table("t2", [Column(n, t) for n, t in typs], 0)
-    vk, vv1, vv2, vd = Var(0, 1, "int8"), Var(0, 2, "int4"), Var(0, 3, "float8"), Var(0, 4, "date")
-    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
-    from xb_producer import BoolOp
-    session = sb.build(
-        scan_quals=BoolOp("And", [Func("date_ge", [vd, Const("date", lo_day - UNIX_TO_PG_DAYS)], "bool"),
-                                  Func("date_lt", [vd, Const("date", hi_day - UNIX_TO_PG_DAYS)], "bool")]),
-        groupby_keys=[vk],
-        aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Func("int4_to_int8", [vv1], "int8")),
-              Agg("PMIN_FP64", vv2), Agg("PMAX_FP64", vv2), Agg("PSUM_FP", vv2)],
-        ngroups_estimate=float(min(nkeys, nrows)))
+    session = arrow_groupby_session(lo_day, hi_day, float(min(nkeys, nrows)))
     chunks = []
     cols_all = {"k": [], "v1": [], "v2": [], "d": []}
     done = 0

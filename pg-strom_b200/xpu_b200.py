@@ -216,11 +216,20 @@ class Session:
             raise XpuB200Error(rc, e)
         return ms.value
 
-    def final(self):
+    def final(self, out=None):
+        """kds_final (and the results).  With 'out' (a uint8 array, e.g. of
+        pinned memory) large enough, kds_final is written there in one call
+        and a view of it is returned."""
         req = ctypes.c_uint64()
         res = results_buffer(self.nrels)
         struct.pack_into("<I", res, 92, self.nrels)
         e = KernErrorbuf()
+        if out is not None:
+            rc = lib().xpuB200Final(self.h, _ptr(out), out.nbytes, ctypes.byref(req), _ptr(res), ctypes.byref(e))
+            if rc == 0:
+                return (out[:req.value] if req.value else None), parse_results(res)
+            if rc != ord("d"):
+                raise XpuB200Error(rc, e)
         rc = lib().xpuB200Final(self.h, None, 0, ctypes.byref(req), _ptr(res), ctypes.byref(e))
         if rc:
             raise XpuB200Error(rc, e)
