@@ -11,7 +11,7 @@
 #include <stdint.h>
 #include "xb_plan.h"
 
-#define XBJ_MIN_BLOCKS_DEFAULT  3   /* resident CTAs of 256 threads per SM (measured best for joins) */
+#define XBJ_MIN_BLOCKS_DEFAULT  4   /* resident CTAs of 256 threads per SM (measured best for the join and Arrow workloads) */
 
 #ifdef __cplusplus
 extern "C" {

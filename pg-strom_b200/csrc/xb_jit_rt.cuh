@@ -88,6 +88,12 @@ __device__ __forceinline__ void xbj_prefetch_tuple(const uint8_t *page, uint32_t
 __device__ __forceinline__ void
 xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
 
+#ifdef XBJ_MERGE_SM
+/* generated: merge of a shared-table entry (shared form) into the global
+ * table's entry g */
+__device__ __noinline__ void xbj_merge_sm(char *g, const char *e);
+#endif
+
 __device__ __forceinline__ unsigned long long xbj_warp_sum(unsigned long long v)
 {
 #pragma unroll
@@ -229,7 +235,11 @@ xbj_body(const XbExecArgs &args, char *smem)
             char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, h->hash,
                                     img, args.gt, args.st, &full);
             if (g)
+#ifdef XBJ_MERGE_SM
+                xbj_merge_sm(g, e);
+#else
                 xb_merge_states(plan, g, e);
+#endif
             else if (full) {
                 XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
                 atomicOr(&args.gt->overflow, 1u);
