@@ -887,7 +887,8 @@ xb_setup_meta(const XbExecArgs &args, XbSrcMeta *meta)
             } else {
                 const kern_colmeta &cm = kds0->colmeta[l.resno - 1];
                 const int w = xb_ld_width(l.ld);
-                if (w == 0 || cm.attlen != w || cm.attcacheoff < 0) {
+                /* fixed: a known offset of a naturally aligned datum */
+                if (w == 0 || cm.attlen != w || cm.attcacheoff < 0 || (cm.attcacheoff % w) != 0) {
                     fixed = 0;
                 } else {
                     f.off = cm.attcacheoff;
