@@ -1454,7 +1454,8 @@ struct xpuB200Session {
     char           *launch_dst = nullptr;
     uint64_t        launch_dst_len = 0;
     int             jit_grid[256] = {0};
-    size_t          jit_smem = 0;
+    size_t          jit_smem = 0;           /* without page staging */
+    size_t          jit_smem_fmt[256] = {0}; /* per format, with its page staging */
     double          jit_compile_ms = 0.0;
     std::string     jit_msg;
 };
@@ -1477,6 +1478,8 @@ static const char *xb_msg_text(uint32_t id)
     default:                      return "device error";
     }
 }
+
+static_assert(XBJ_WARPS_PER_CTA == XB_WARPS, "specialised kernels assume the executor's CTA size");
 
 static int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int line,
                         const char *fmt, ...)
@@ -1890,6 +1893,39 @@ xpuB200CloseSession(xpuB200Session *sess)
     }
 }
 
+/* remember the heap layout of the first heap chunk a session sees, before
+ * its specialised kernel is built: the kernel reads the depth-0 columns at
+ * these offsets (and checks each launch's layout against them); session
+ * lock held */
+static void xb_note_layout(xpuB200Session *s, const kern_data_store *h)
+{
+    xb_plan *p = s->h_plan;
+    if (h->format != KDS_FORMAT_BLOCK || p->lay_valid || s->jit_tried[KDS_FORMAT_BLOCK])
+        return;
+    uint32_t end = 0;
+    for (uint32_t i = 0; i < p->nload0; i++) {
+        const xb_load &l = p->load0[i];
+        int w = 0;
+        switch (l.ld) {
+        case XB_LD_BOOL: w = 1; break;
+        case XB_LD_INT2: w = 2; break;
+        case XB_LD_INT4: case XB_LD_DATE: case XB_LD_FLT4: w = 4; break;
+        case XB_LD_INT8: case XB_LD_FLT8: w = 8; break;
+        default: return;
+        }
+        if (l.resno < 1 || l.resno > (int)h->ncols || l.resno > (int)h->nr_colmeta)
+            return;
+        const kern_colmeta &cm = h->colmeta[l.resno - 1];
+        if (cm.attlen != w || cm.attcacheoff < 0 || (cm.attcacheoff % w) != 0)
+            return;
+        p->lay_off[i] = cm.attcacheoff;
+        if ((uint32_t)(cm.attcacheoff + w) > end)
+            end = cm.attcacheoff + w;
+    }
+    p->lay_end = end;
+    p->lay_valid = p->nload0 > 0 ? 1 : 0;
+}
+
 /* units of one chunk (pages, or 1024-row groups) */
 static uint32_t xb_chunk_units(const kern_data_store *head)
 {
@@ -1920,7 +1956,8 @@ static void *xb_session_jit(xpuB200Session *s, uint32_t format)
             s->jit_fn[format] = nullptr;
             s->jit_mixfn[format] = nullptr;
             s->jit_msg = msg;
-        } else if (xb_jit_prepare(s->jit_fn[format], XB_BLOCK, s->jit_smem, &per_sm) != 0) {
+        } else if ((s->jit_smem_fmt[format] = s->jit_smem + xb_jit_stage_bytes(format)) == 0 ||
+                   xb_jit_prepare(s->jit_fn[format], XB_BLOCK, s->jit_smem_fmt[format], &per_sm) != 0) {
             s->jit_fn[format] = nullptr;
             s->jit_mixfn[format] = nullptr;
             s->jit_msg = "specialised kernel does not fit on an SM";
@@ -1972,7 +2009,7 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     if (format < 256)
         s->ran_kind[format] = fn ? 'j' : 'v';
     if (fn) {
-        if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem, (void *)stream, &a) != 0)
+        if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem_fmt[format], (void *)stream, &a) != 0)
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
     } else {
         xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, stream>>>(a);
@@ -2153,6 +2190,7 @@ static int xb_place_src(xpuB200Session *s, const kern_data_store *kds_src, int k
         XB_CUDA(cudaMemcpyAsync(s->d_src + shift, kds_src, kds_src->length, cudaMemcpyHostToDevice, st), err);
         d_kds = (const kern_data_store *)(s->d_src + shift);
     }
+    xb_note_layout(s, kds_src_on_device ? (const kern_data_store *)hbuf.data() : kds_src);
     *p_dkds = d_kds;
     return 0;
 }
@@ -2612,6 +2650,7 @@ xpuB200BatchCreate(xpuB200Session *s, const kern_data_store *const *kds_dev, uin
         if (i == 0) {
             first_head = hb;
             format = (uint32_t)h->format;
+            xb_note_layout(s, h);
         } else {
             /* one launch decodes every chunk with the same column layout */
             const kern_data_store *f = (const kern_data_store *)first_head.data();
@@ -2734,7 +2773,7 @@ static int xb_mix_plan(xpuB200Device *dev, const std::vector<xpuB200Session *> &
             groups.back().jfn = k;
         }
         groups[g].cmds.push_back(i);
-        const size_t sm = k ? sess[i]->jit_smem : sess[i]->smem_bytes;
+        const size_t sm = k ? sess[i]->jit_smem_fmt[formats[i]] : sess[i]->smem_bytes;
         if (sm > groups[g].smem)
             groups[g].smem = sm;
     }
@@ -2847,6 +2886,10 @@ xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess
         const kern_data_store *h = (const kern_data_store *)hb.data();
         int rc = xb_check_kds(h, err);
         if (rc) return rc;
+        {
+            std::lock_guard<std::mutex> g(s->lock);
+            xb_note_layout(s, h);
+        }
         tasks[i].kds = kds_dev[i];
         tasks[i].unit_base = 0;
         tasks[i].nunits = xb_chunk_units(h);
@@ -3468,6 +3511,10 @@ xpuB200Submit(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_
     if (kds_src_on_device && h->format == KDS_FORMAT_BLOCK &&
         (((uintptr_t)kds_src + h->block_offset) & 15) != 0)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "heap pages of a device chunk must start 16-byte aligned");
+    {
+        std::lock_guard<std::mutex> g(s->lock);
+        xb_note_layout(s, h);
+    }
     c.s = s;
     c.kds = kds_src;
     c.on_device = kds_src_on_device;

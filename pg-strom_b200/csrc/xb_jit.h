@@ -11,11 +11,16 @@
 #include <stdint.h>
 #include "xb_plan.h"
 
+#define XBJ_WARPS_PER_CTA       8   /* 256-thread CTAs (XB_BLOCK) */
 #define XBJ_MIN_BLOCKS_DEFAULT  4   /* resident CTAs of 256 threads per SM (measured best for the join and Arrow workloads) */
 
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+/* shared memory the specialised kernel of 'format' adds for staging
+ * heap pages (0: pages are read in place; XPU_B200_JIT_STAGE=1 enables) */
+size_t xb_jit_stage_bytes(uint32_t format);
 
 /* the generated CUDA source (for inspection); *p_len = its length */
 int xb_jit_source(const xb_plan *plan, uint32_t format, char *buf, size_t bufsz, size_t *p_len);

@@ -60,7 +60,13 @@ __device__ __forceinline__ void xbj_flush_cnt(XbjCnt &C, xb_status *st)
  * unit; lp: the heap item's line pointer) */
 __device__ __forceinline__ bool
 xbj_decode(XbjRegs &R, const XbExecArgs &args, const uint8_t *page, const kern_data_store *kds,
-           uint32_t row0, const XbSrcMeta *meta, uint32_t idx, uint32_t lp, bool &exists, xb_status *st);
+           uint32_t row0, const XbSrcMeta *meta, uint32_t idx, uint32_t lp, bool lay_ok, bool &exists,
+           xb_status *st);
+
+#ifdef XBJ_LAYOUT
+/* generated: the launch's heap layout is the one the kernel is built for */
+__device__ __forceinline__ bool xbj_layout_ok(const XbSrcMeta *meta);
+#endif
 
 /* line pointer i of a heap page of nitems items (0 = LP_UNUSED past the end) */
 __device__ __forceinline__ uint32_t xbj_itemid(const uint8_t *page, uint32_t nitems, uint32_t i)
@@ -94,6 +100,55 @@ xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
 __device__ __noinline__ void xbj_merge_sm(char *g, const char *e);
 #endif
 
+#ifdef XBJ_STAGE
+/* ---- heap pages staged in shared memory ------------------------------
+ * Every warp owns one 8 KB page buffer and an mbarrier.  A page whose
+ * address is 16-byte aligned is copied into the buffer by one bulk copy
+ * (cp.async.bulk, the TMA engine: one instruction for the whole page, no
+ * per-lane global loads) and the warp decodes it from shared memory; a
+ * page that is not aligned is read in place.  Waits are bounded. */
+#define XBJ_STAGE_WAIT_LIMIT    (1u << 22)
+
+__device__ __forceinline__ uint32_t xbj_smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void xbj_mbar_init(uint64_t *mbar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(xbj_smem_addr(mbar)) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+/* lane 0: copy 8 KB from global gsrc into the shared buffer, completing
+ * on mbar (generic reads of the buffer before this are ordered first) */
+__device__ __forceinline__ void xbj_stage_issue(void *buf, const void *gsrc, uint64_t *mbar)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(xbj_smem_addr(mbar)), "r"((uint32_t)PGSTROM_BLCKSZ) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(xbj_smem_addr(buf)), "l"(gsrc), "r"((uint32_t)PGSTROM_BLCKSZ), "r"(xbj_smem_addr(mbar))
+                 : "memory");
+}
+
+/* wait for phase 'parity' of mbar; false when the wait gave up */
+__device__ __forceinline__ bool xbj_stage_wait(uint64_t *mbar, uint32_t parity)
+{
+    const uint32_t a = xbj_smem_addr(mbar);
+    for (uint32_t i = 0; i < XBJ_STAGE_WAIT_LIMIT; i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+#endif
+
 __device__ __forceinline__ unsigned long long xbj_warp_sum(unsigned long long v)
 {
 #pragma unroll
@@ -121,6 +176,11 @@ xbj_body(const XbExecArgs &args, char *smem)
         ((uint32_t *)sm_entries)[i] = 0;
     __syncthreads();
 
+#ifdef XBJ_LAYOUT
+    const bool lay_ok = xbj_layout_ok(meta);
+#else
+    const bool lay_ok = false;
+#endif
     XbjEnv E;
     E.plan = args.plan;
     E.st = args.st;
@@ -139,6 +199,17 @@ xbj_body(const XbExecArgs &args, char *smem)
         C.depth[d] = 0;
 
     XbSrc &src = wsrc[threadIdx.x >> 5];
+#ifdef XBJ_STAGE
+    /* this warp's page buffer and its mbarrier, after the group table */
+    char *stage_base = (char *)(((uintptr_t)(sm_entries + sm_bytes) + 127) & ~(uintptr_t)127);
+    char *sbuf = stage_base + (size_t)(threadIdx.x >> 5) * PGSTROM_BLCKSZ;
+    uint64_t *mbar = (uint64_t *)(stage_base + (size_t)XB_WARPS * PGSTROM_BLCKSZ) + (threadIdx.x >> 5);
+    uint32_t sphase = 0;
+    bool staged = false;            /* the current page is in sbuf */
+    if (lane == 0)
+        xbj_mbar_init(mbar);
+    __syncwarp();
+#endif
     xb_src_start(args, src, lane);
     const uint8_t *page = nullptr;
     const kern_data_store *kds = nullptr;
@@ -164,6 +235,26 @@ xbj_body(const XbExecArgs &args, char *smem)
             row0 = src.row0;
             item = 0;
             nitems = src.nitems;
+#ifdef XBJ_STAGE
+            staged = false;
+            if ((((uintptr_t)page) & 15) == 0) {
+                __syncwarp();           /* every lane is done with the buffer */
+                if (lane == 0)
+                    xbj_stage_issue(sbuf, page, mbar);
+                __syncwarp();
+                const bool ok_ = xbj_stage_wait(mbar, sphase);
+                sphase ^= 1u;
+                if (!__all_sync(XB_FULL, ok_)) {
+                    if (lane == 0) XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_WAIT_TIMEOUT);
+                    /* the copy is still owed to this barrier: wait once more */
+                    xbj_stage_wait(mbar, sphase ^ 1u);
+                    done = true;
+                    break;
+                }
+                page = (const uint8_t *)sbuf;
+                staged = true;
+            }
+#endif
             if (args.format == KDS_FORMAT_BLOCK) {
                 lp_next = xbj_itemid(page, nitems, lane);
                 lp_after = xbj_itemid(page, nitems, lane + 32);
@@ -176,6 +267,9 @@ xbj_body(const XbExecArgs &args, char *smem)
         if (args.format == KDS_FORMAT_BLOCK) {
             lp = lp_next;
             lp_next = lp_after;
+#ifdef XBJ_STAGE
+            if (!staged)
+#endif
             xbj_prefetch_tuple(page, lp_next);
             lp_after = xbj_itemid(page, nitems, idx + 64);
         }
@@ -184,7 +278,7 @@ xbj_body(const XbExecArgs &args, char *smem)
         if (idx < nitems) {
             XbjRegs R;
             bool exists = false;
-            const bool ok = xbj_decode(R, args, page, kds, row0, meta, idx, lp, exists, args.st);
+            const bool ok = xbj_decode(R, args, page, kds, row0, meta, idx, lp, lay_ok, exists, args.st);
             if (exists)
                 C.raw++;
             if (exists && !ok)
@@ -202,6 +296,12 @@ xbj_body(const XbExecArgs &args, char *smem)
             break;
     }
 
+#ifdef XBJ_STAGE
+    /* the barrier's memory becomes group-table or buffer space again */
+    __syncwarp();
+    if (lane == 0)
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(xbj_smem_addr(mbar)) : "memory");
+#endif
     /* statistics */
     {
         const unsigned long long raw = xbj_warp_sum(C.raw);

@@ -229,6 +229,12 @@ typedef struct xb_plan {
     /* depth 0: source tuples */
     uint32_t    nload0;
     int32_t     max_resno0;
+    /* heap layout the specialised kernel is built for (host side, from the
+     * first heap chunk a session sees): the cached offset of every depth-0
+     * load, all fixed-width and naturally aligned, and their end */
+    uint32_t    lay_valid;
+    uint32_t    lay_end;
+    int32_t     lay_off[XB_MAX_LOADS];
     xb_load     load0[XB_MAX_LOADS];
     xb_prog     scan_quals;
 
