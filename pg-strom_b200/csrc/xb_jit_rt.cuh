@@ -267,10 +267,14 @@ xbj_body(const XbExecArgs &args, char *smem)
         if (args.format == KDS_FORMAT_BLOCK) {
             lp = lp_next;
             lp_next = lp_after;
+            /* (the fast decode of a known layout reads the tuple with two
+             * wide loads; there the L1 prefetch only costs issue slots) */
+            if (!lay_ok
 #ifdef XBJ_STAGE
-            if (!staged)
+                && !staged
 #endif
-            xbj_prefetch_tuple(page, lp_next);
+                )
+                xbj_prefetch_tuple(page, lp_next);
             lp_after = xbj_itemid(page, nitems, idx + 64);
         }
         item += 32;
