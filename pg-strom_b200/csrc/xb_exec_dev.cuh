@@ -521,9 +521,18 @@ xb_src_start(const XbExecArgs &args, XbSrc &s, uint32_t lane)
     xb_prefetch_page(args, s, __shfl_sync(XB_FULL, s.nx_l0, 0), lane);
 }
 
-/* move to the next unit; returns 0 = no more work, 1 = ok, 2 = corrupt page */
+/* the unit this warp takes after its current one (heap pages), or
+ * args.nunits when its claims are exhausted */
+__device__ __forceinline__ uint64_t xb_following_unit(const XbSrc &s)
+{
+    return s.unit + 1 < s.claim_end ? s.unit + 1 : __shfl_sync(XB_FULL, s.nx_l0, 0);
+}
+
+/* move to the next unit; returns 0 = no more work, 1 = ok, 2 = corrupt page.
+ * With pf_next the page after it is prefetched into L2 right away (callers
+ * that process a page slowly prefetch it later themselves, closer to use) */
 __device__ __forceinline__ int
-xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane)
+xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = true)
 {
     if (args.format == KDS_FORMAT_BLOCK) {
         s.unit++;
@@ -554,8 +563,8 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane)
             xb_src_task(args, s, s.unit);
         s.page = s.blocks + (s.unit - s.task_base) * (size_t)PGSTROM_BLCKSZ;
         /* the page after this one streams into L2 while this one is decoded */
-        const uint64_t nu = s.unit + 1 < s.claim_end ? s.unit + 1 : __shfl_sync(XB_FULL, s.nx_l0, 0);
-        xb_prefetch_page(args, s, nu, lane);
+        if (pf_next)
+            xb_prefetch_page(args, s, xb_following_unit(s), lane);
         const uint32_t pd_lower = (uint32_t)xb_fetch_le(s.page + 12, 2);
         s.item = 0;
         s.nitems = 0;

@@ -22,6 +22,10 @@
 #ifndef XB_JIT_RT_CUH
 #define XB_JIT_RT_CUH
 
+#ifndef XBJ_PF_LEAD
+#define XBJ_PF_LEAD     32      /* rows of a page left when the next page is prefetched (0: none) */
+#endif
+
 struct XbjEnv {
     const xb_plan  *plan;           /* device plan (global memory) */
     xb_status      *st;
@@ -223,7 +227,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     for (;;) {
         bool done = false;
         while (item >= nitems) {
-            const int rc = xb_next_unit(args, src, lane);
+            const int rc = xb_next_unit(args, src, lane, args.format != KDS_FORMAT_BLOCK);
             if (rc == 0) { done = true; break; }
             if (rc == 2) {
                 if (lane == 0) XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
@@ -264,6 +268,13 @@ xbj_body(const XbExecArgs &args, char *smem)
             break;
         const uint32_t idx = item + lane;
         uint32_t lp = 0;
+        /* the warp's next heap page streams into L2 while the last
+         * XBJ_PF_LEAD rows of this one are processed: early enough to
+         * arrive, late enough not to be evicted by the pages streaming
+         * through L2 meanwhile */
+        if (XBJ_PF_LEAD > 0 && args.format == KDS_FORMAT_BLOCK && item + XBJ_PF_LEAD >= nitems &&
+            (item < 32 || item + XBJ_PF_LEAD < nitems + 32))
+            xb_prefetch_page(args, src, xb_following_unit(src), lane);
         if (args.format == KDS_FORMAT_BLOCK) {
             lp = lp_next;
             lp_next = lp_after;
