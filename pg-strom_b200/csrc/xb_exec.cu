@@ -932,6 +932,22 @@ xb_build_inner(XbBuildArgs args)
     }
 }
 
+/* existence bitmap of a direct table: one thread per 32 keys */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_build_dbits(xb_inner *in)
+{
+    const uint32_t words = in->dbits_words;
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+        uint32_t bits = 0;
+        for (uint32_t b = 0; b < 32; b++) {
+            const uint32_t k = w * 32 + b;
+            if (k < in->drange && in->dtab[k] != 0)
+                bits |= 1u << b;
+        }
+        in->dbits[w] = bits;
+    }
+}
+
 /* pack the live columns of every indexed row into its direct record */
 __global__ void __launch_bounds__(XB_BLOCK)
 xb_build_drec(xb_inner *in, const xb_plan *plan)
@@ -1705,6 +1721,8 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             in->gid_on = 0;
             in->ngids = 0;
             in->gids = nullptr;
+            in->dbits_words = 0;
+            in->dbits = nullptr;
             if (in->hashed)
                 DALLOC((size_t)nl * n * 4, &in->hashes);
             cudaMemsetAsync(in->index, 0, cap * 8, st);
@@ -1849,12 +1867,23 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             cudaMemsetAsync(in->dpay, 0, range * rs, st);
             in->drec_size = rs;
         }
+        /* a depth that only filters (no columns of its rows are used):
+         * an existence bitmap, staged in shared memory by the specialised
+         * kernels when it is small */
+        if (!in->live && range <= XB_DBITS_MAX_KEYS) {
+            in->dbits_words = (uint32_t)((range + 31) / 32);
+            DALLOC((size_t)in->dbits_words * 4, &in->dbits);
+        }
         cudaMemcpyAsync(&s->d_plan->inner[d], in, sizeof(xb_inner), cudaMemcpyHostToDevice, st);
         int grid = (int)((in->cap_mask + 1ULL + XB_BLOCK - 1) / XB_BLOCK);
         if (grid > dev->nsm * 8) grid = dev->nsm * 8;
         xb_build_direct<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d]);
         if (in->dpay)
             xb_build_drec<<<grid, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d], s->d_plan);
+        if (in->dbits) {
+            int g2 = (int)((in->dbits_words + XB_BLOCK - 1) / XB_BLOCK);
+            xb_build_dbits<<<g2 > 0 ? g2 : 1, XB_BLOCK, 0, st>>>(&s->d_plan->inner[d]);
+        }
     }
     if (cudaStreamSynchronize(st) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1873,6 +1902,14 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         FAIL(ERRCODE_DEVICE_FATAL, "executor kernel does not fit on an SM (%zu bytes smem)", s->smem_bytes);
     s->grid = per_sm * dev->nsm;
     s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + sizeof(XbSrc) * XB_WARPS + (size_t)s->sm_cap * plan->gent_size;
+    /* existence bitmaps staged after the group table (16-byte aligned) */
+    {
+        size_t bits = 0;
+        for (uint32_t d = 1; d <= plan->nrels; d++)
+            bits += (size_t)plan->inner[d].dbits_words * 4;
+        if (bits)
+            s->jit_smem = PGSTROM_TYPEALIGN(16, s->jit_smem) + PGSTROM_TYPEALIGN(16, bits);
+    }
     {
         const char *env = getenv("XPU_B200_JIT");
         s->jit_enabled = !(env && env[0] == '0');

@@ -353,6 +353,9 @@ struct XbExecArgs {
     uint32_t        __pad;
 };
 
+/* largest existence bitmap of a direct depth (keys), 16 KB */
+#define XB_DBITS_MAX_KEYS   (1u << 17)
+
 /* a mixed launch: work item i sends a CTA to command items[i] */
 struct XbMixArgs {
     const XbExecArgs *cmds;

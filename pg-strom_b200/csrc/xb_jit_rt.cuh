@@ -37,6 +37,7 @@ struct XbjEnv {
     uint32_t        lane;
     char           *dst;            /* projection: kds_dst and its length */
     uint64_t        dst_len;
+    const uint32_t *sbits;          /* existence bitmaps in shared memory */
 };
 
 /* per-thread counters, 32-bit to spare registers; flushed into the launch
@@ -66,6 +67,12 @@ __device__ __forceinline__ bool
 xbj_decode(XbjRegs &R, const XbExecArgs &args, const uint8_t *page, const kern_data_store *kds,
            uint32_t row0, const XbSrcMeta *meta, uint32_t idx, uint32_t lp, bool lay_ok, bool &exists,
            xb_status *st);
+
+#ifdef XBJ_BITS
+/* generated: copy the filter depths' existence bitmaps into shared memory
+ * (all threads of the CTA); returns their bytes */
+__device__ __forceinline__ uint32_t xbj_stage_bits(uint32_t *sb, const xb_plan *plan);
+#endif
 
 #ifdef XBJ_LAYOUT
 /* generated: the launch's heap layout is the one the kernel is built for */
@@ -178,6 +185,13 @@ xbj_body(const XbExecArgs &args, char *smem)
     xb_setup_meta(args, meta);
     for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
         ((uint32_t *)sm_entries)[i] = 0;
+    /* after the group table: the existence bitmaps of filter depths */
+    uint32_t *sbits = (uint32_t *)(((uintptr_t)(sm_entries + sm_bytes) + 15) & ~(uintptr_t)15);
+#ifdef XBJ_BITS
+    const uint32_t sbits_bytes = xbj_stage_bits(sbits, args.plan);
+#else
+    const uint32_t sbits_bytes = 0;
+#endif
     __syncthreads();
 
 #ifdef XBJ_LAYOUT
@@ -196,6 +210,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     E.lane = lane;
     E.dst = args.dst;
     E.dst_len = args.dst_len;
+    E.sbits = sbits;
     XbjCnt C;
     C.raw = C.in = C.out = 0;
 #pragma unroll
@@ -205,7 +220,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     XbSrc &src = wsrc[threadIdx.x >> 5];
 #ifdef XBJ_STAGE
     /* this warp's page buffer and its mbarrier, after the group table */
-    char *stage_base = (char *)(((uintptr_t)(sm_entries + sm_bytes) + 127) & ~(uintptr_t)127);
+    char *stage_base = (char *)(((uintptr_t)((char *)sbits + sbits_bytes) + 127) & ~(uintptr_t)127);
     char *sbuf = stage_base + (size_t)(threadIdx.x >> 5) * PGSTROM_BLCKSZ;
     uint64_t *mbar = (uint64_t *)(stage_base + (size_t)XB_WARPS * PGSTROM_BLCKSZ) + (threadIdx.x >> 5);
     uint32_t sphase = 0;

@@ -175,8 +175,12 @@ typedef struct xb_inner {
     /* direct records: the live columns of the row of key k packed at
      * dpay + (k - dkey_min) * drec_size (layout: xb_drec_layout) */
     uint32_t    drec_size;
-    uint32_t    __pad_d;
+    /* existence bitmap of a direct depth whose rows carry no columns (a
+     * pure filter): bit k - dkey_min is set when key k has a row; small
+     * enough to be staged in shared memory by the specialised kernels */
+    uint32_t    dbits_words;    /* 0: none */
     char       *dpay;
+    uint32_t   *dbits;
     uint32_t    hashed;         /* bit k: hash of load k precomputed into hashes[] */
     uint32_t   *hashes;         /* [nloads][nitems] datum hashes (hashed loads) */
     xb_load     load[XB_MAX_LOADS];
