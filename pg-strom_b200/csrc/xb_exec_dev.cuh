@@ -33,6 +33,13 @@ __device__ __forceinline__ char *xb_generic_ptr(char *p)
     return p;
 }
 
+/* 32-bit add to a counter in shared memory given by a generic address:
+ * the native shared-memory atomic (64-bit shared atomics are not native) */
+__device__ __forceinline__ void xb_red_shared_add_u32(void *p, uint32_t v)
+{
+    asm volatile("red.shared.add.u32 [%0], %1;" :: "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+
 /* ================================================================
  * memory-order helpers (generic addresses: shared or global)
  * ================================================================ */

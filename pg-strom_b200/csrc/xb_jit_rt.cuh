@@ -45,6 +45,7 @@ struct XbjEnv {
 struct XbjCnt {
     uint32_t raw, in, out;
     uint32_t depth[XB_MAX_DEPTH + 1];
+    uint64_t gready;                /* group-id entries this lane has seen ready */
 };
 
 __device__ __forceinline__ void xbj_flush_cnt(XbjCnt &C, xb_status *st)
@@ -213,6 +214,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     E.sbits = sbits;
     XbjCnt C;
     C.raw = C.in = C.out = 0;
+    C.gready = 0;
 #pragma unroll
     for (int d = 0; d <= XB_MAX_DEPTH; d++)
         C.depth[d] = 0;
