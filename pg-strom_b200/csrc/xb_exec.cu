@@ -1901,7 +1901,8 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     if (per_sm < 1)
         FAIL(ERRCODE_DEVICE_FATAL, "executor kernel does not fit on an SM (%zu bytes smem)", s->smem_bytes);
     s->grid = per_sm * dev->nsm;
-    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + sizeof(XbSrc) * XB_WARPS + (size_t)s->sm_cap * plan->gent_size;
+    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + sizeof(XbSrc) * XB_WARPS +
+                  (size_t)s->sm_cap * xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16);
     /* existence bitmaps staged after the group table (16-byte aligned) */
     {
         size_t bits = 0;

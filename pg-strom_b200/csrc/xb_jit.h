@@ -18,6 +18,9 @@
 extern "C" {
 #endif
 
+/* bytes between the entries of a specialised kernel's shared group table */
+uint32_t xb_jit_sm_stride(uint32_t gent_size);
+
 /* shared memory the specialised kernel of 'format' adds for staging
  * heap pages (0: pages are read in place; XPU_B200_JIT_STAGE=1 enables) */
 size_t xb_jit_stage_bytes(uint32_t format);

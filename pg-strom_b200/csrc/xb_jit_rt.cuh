@@ -181,7 +181,7 @@ xbj_body(const XbExecArgs &args, char *smem)
      * registers (read once per unit) */
     XbSrc *wsrc = (XbSrc *)(smem + ((sizeof(XbSrcMeta) + 15) & ~(size_t)15));
     char *sm_entries = (char *)(wsrc + XB_WARPS);
-    const size_t sm_bytes = (size_t)args.sm_cap * XBJ_GENT_SIZE;
+    const size_t sm_bytes = (size_t)args.sm_cap * XBJ_SM_STRIDE;
 
     xb_setup_meta(args, meta);
     for (size_t i = threadIdx.x; i < sm_bytes / 4; i += blockDim.x)
@@ -358,7 +358,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     if (args.sm_cap) {
         const xb_plan *plan = args.plan;
         for (uint32_t i = threadIdx.x; i < args.sm_cap; i += blockDim.x) {
-            char *e = sm_entries + (size_t)i * XBJ_GENT_SIZE;
+            char *e = sm_entries + (size_t)i * XBJ_SM_STRIDE;
             const xb_gent_head *h = (const xb_gent_head *)e;
             if (h->state != XB_GSTATE_READY)
                 continue;
