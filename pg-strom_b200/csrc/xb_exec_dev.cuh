@@ -40,6 +40,40 @@ __device__ __forceinline__ void xb_red_shared_add_u32(void *p, uint32_t v)
     asm volatile("red.shared.add.u32 [%0], %1;" :: "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
 }
 
+/* add to a little-endian multi-word integer in shared memory (generic
+ * address) with native 32-bit shared atomics: each word is added with the
+ * carry of the word below, and a carry out of a word is added to the next;
+ * words that receive nothing are not touched, so a small positive value
+ * costs one atomic.  The carry out of the top word is dropped (the sum is
+ * modulo 2^(32 * nwords), as a two's complement accumulator is). */
+__device__ __forceinline__ void xb_shared_add_words(void *p, const uint32_t *w, int nwords)
+{
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(p);
+    uint32_t c = 0;
+    for (int k = 0; k < nwords; k++) {
+        const uint64_t add = (uint64_t)w[k] + c;
+        if (add == 0) { c = 0; continue; }
+        if (add == 0x100000000ULL) { c = 1; continue; }
+        const uint32_t a = (uint32_t)add;
+        uint32_t old;
+        asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(base + 4 * k), "r"(a) : "memory");
+        c = (old + a < old) ? 1u : 0u;
+    }
+}
+
+__device__ __forceinline__ void xb_shared_add_u64w(void *p, uint64_t v)
+{
+    const uint32_t w[2] = {(uint32_t)v, (uint32_t)(v >> 32)};
+    xb_shared_add_words(p, w, 2);
+}
+
+__device__ __forceinline__ void xb_shared_add_i128w(void *p, xb_i128 v)
+{
+    const unsigned __int128 u = (unsigned __int128)v;
+    const uint32_t w[4] = {(uint32_t)u, (uint32_t)(u >> 32), (uint32_t)(u >> 64), (uint32_t)(u >> 96)};
+    xb_shared_add_words(p, w, 4);
+}
+
 /* ================================================================
  * memory-order helpers (generic addresses: shared or global)
  * ================================================================ */
@@ -91,17 +125,119 @@ __device__ __forceinline__ double xb_reg_f64(uint64_t v, int rk)
     return rk == XB_RK_FLT ? __longlong_as_double(v) : (double)(int64_t)v;
 }
 
+/* 10^k for k = 0..18 */
+__device__ __forceinline__ int64_t xb_pow10_i64(int k)
+{
+    int64_t p = 1;
+    for (int i = 0; i < k; i++)
+        p *= 10;
+    return p;
+}
+
+/*
+ * The value of a numeric varlena rescaled to weight_d, for sums: the same
+ * number as xb_numeric_rescale(weight_d, w, v) of xb_numeric_decode, which
+ * normalises trailing zeros away first; rescaling the digits as stored
+ * gives the same result (the removed digits are zeros).  Short numerics of
+ * up to four base-10000 digits are read with aligned 8-byte loads (every
+ * aligned word that overlaps the datum lies in its page or buffer) and
+ * rescaled in 64-bit arithmetic; others take the general decode.
+ * Returns 0, or 1 on a corrupt datum.
+ */
+__device__ __forceinline__ int
+xb_numeric_sum_value(const uint8_t *vl, int weight_d, uint8_t *p_kind, xb_i128 *p_out)
+{
+    const uintptr_t a = (uintptr_t)vl;
+    const uint64_t *wp = (const uint64_t *)(a & ~(uintptr_t)7);
+    const uint32_t o = (uint32_t)(a & 7);
+    const uint64_t w0 = wp[0];
+    const uint32_t h = (uint32_t)(w0 >> (8 * o)) & 0xff;
+    const uint32_t len = (h >> 1) & 0x7f;
+    /* short varlena, short-format numeric, 0..4 digits, within 3 words */
+    if ((h & 1) && h != 1 && len >= 3 && len <= 11 && o + len <= 24) {
+        const uint64_t w1 = (o + len > 8) ? wp[1] : 0;
+        const uint64_t w2 = (o + len > 16) ? wp[2] : 0;
+        auto byte = [&](uint32_t i) -> uint32_t {
+            const uint32_t k = o + i;
+            const uint64_t w = k < 8 ? w0 : (k < 16 ? w1 : w2);
+            return (uint32_t)(w >> (8 * (k & 7))) & 0xff;
+        };
+        const uint32_t n_head = byte(1) | (byte(2) << 8);
+        if ((n_head & 0xC000) == 0x8000 && ((len - 3) & 1) == 0) {
+            const uint32_t ndigits = (len - 3) / 2;
+            int pgweight = n_head & 0x003F;
+            if (n_head & 0x0040)
+                pgweight |= ~0x003F;
+            int64_t v = 0;
+            for (uint32_t i = 0; i < ndigits; i++)
+                v = v * 10000 + (int16_t)(byte(3 + 2 * i) | (byte(4 + 2 * i) << 8));
+            if (n_head & 0x2000)
+                v = -v;
+            const int weight_s = 4 * ((int)ndigits - (pgweight + 1));
+            const int shift = weight_d - weight_s;
+            if (shift == 0 || v == 0) {
+                *p_kind = XB_NUM_VALID;
+                *p_out = v;
+                return 0;
+            }
+            if (shift < 0 && shift >= -18) {
+                *p_kind = XB_NUM_VALID;
+                *p_out = v / xb_pow10_i64(-shift);       /* truncates toward zero */
+                return 0;
+            }
+            if (shift > 0 && shift <= 18) {
+                const int64_t p = xb_pow10_i64(shift);
+                const uint64_t m = v < 0 ? (uint64_t)(-(v + 1)) + 1 : (uint64_t)v;
+                if (m <= (uint64_t)INT64_MAX / (uint64_t)p) {
+                    *p_kind = XB_NUM_VALID;
+                    *p_out = v * p;
+                    return 0;
+                }
+            }
+        }
+    }
+    int16_t w;
+    xb_i128 v;
+    if (xb_numeric_decode(vl, p_kind, &w, &v))
+        return 1;
+    *p_out = (*p_kind == XB_NUM_VALID) ? xb_numeric_rescale(weight_d, w, v) : 0;
+    return 0;
+}
+
 /* per-value updates of the actions that are not combined across lanes */
 __device__ __forceinline__ void
 xb_agg_numeric_add(char *s, const uint8_t *vl, int16_t weight, xb_status *st)
 {
-    uint8_t kind; int16_t w; xb_i128 v;
-    if (xb_numeric_decode(vl, &kind, &w, &v)) {
+    uint8_t kind; xb_i128 v;
+    if (xb_numeric_sum_value(vl, weight, &kind, &v)) {
         XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
     } else if (kind == XB_NUM_VALID) {
         atomicAdd((unsigned long long *)s, 1ULL);
-        xb_atomic_add_i128((uint64_t *)(s + 8), xb_numeric_rescale(weight, w, v));
+        xb_atomic_add_i128((uint64_t *)(s + 8), v);
     } else {
+        const uint32_t special = kind == XB_NUM_PINF ? PAGG_NUMERIC_ATTRS__PINF
+                               : kind == XB_NUM_NINF ? PAGG_NUMERIC_ATTRS__NINF
+                               : PAGG_NUMERIC_ATTRS__NAN;
+        atomicOr((unsigned int *)(s + 24), special);
+    }
+}
+
+/* xb_agg_numeric_add for an entry of a shared-memory group table (shared
+ * form): 32-bit counter, 128-bit sum by word atomics; with nc the counter
+ * holds the rows NOT counted (a special value, the caller adds NULLs) */
+__device__ __forceinline__ void
+xb_agg_numeric_add_sm(char *s, const uint8_t *vl, int16_t weight, xb_status *st, bool nc)
+{
+    uint8_t kind; xb_i128 v;
+    if (xb_numeric_sum_value(vl, weight, &kind, &v)) {
+        XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_NUMERIC_CORRUPT);
+    } else if (kind == XB_NUM_VALID) {
+        if (!nc)
+            xb_red_shared_add_u32(s, 1u);
+        xb_shared_add_i128w(s + 8, v);
+    } else {
+        if (nc)
+            xb_red_shared_add_u32(s, 1u);
         const uint32_t special = kind == XB_NUM_PINF ? PAGG_NUMERIC_ATTRS__PINF
                                : kind == XB_NUM_NINF ? PAGG_NUMERIC_ATTRS__NINF
                                : PAGG_NUMERIC_ATTRS__NAN;
