@@ -51,9 +51,13 @@ def parse():
     ap.add_argument("--rows", type=int, default=100_000_000)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="join_groupby", choices=["join_groupby", "mixed", "served"],
-                    help="join_groupby: the headline line; mixed: 256 batched chunk commands; "
-                         "served: Poisson-arrival query mix through the serving scheduler")
+    ap.add_argument("--workload", default="join_groupby",
+                    choices=["join_groupby", "scan_groupby", "arrow_groupby", "mixed", "served"],
+                    help="join_groupby: the headline line; scan_groupby / arrow_groupby: the plain "
+                         "scan and the Arrow high-cardinality configurations (--rows, --keys); mixed: "
+                         "256 batched chunk commands; served: Poisson-arrival query mix through the "
+                         "serving scheduler")
+    ap.add_argument("--keys", type=int, default=10_000_000)
     ap.add_argument("--requests", type=int, default=400)
     ap.add_argument("--qps", type=float, default=200.0)
     return ap.parse_args()
@@ -393,6 +397,74 @@ def run_b200(args, rank, world, local):
     dev.close()
 
 
+# ------------------------------------------------------------------ other configurations
+def run_config(args):
+    """One persistent launch per pass over resident chunks of the plain
+    scan + group-by table (heap) or the Arrow high-cardinality table;
+    rows/s and the referenced bytes against HBM bandwidth."""
+    import torch
+    import xb_configs as C
+    import xpu_b200
+    t0 = time.time()
+    if args.workload == "scan_groupby":
+        tbl, sess, _, expect, meta = C.scan_groupby(nrows=args.rows)
+        chunks = tbl.block_chunks(pages_per_chunk=8190)
+        nbytes = sum(c.nbytes for c in chunks)
+        ref_bytes = nbytes
+        desc = (f"plain scan + filter + group-by over heap pages: {args.rows} rows, WHERE a < 300 "
+                "GROUP BY g (64 groups) -> count, sum(a), sum(c numeric), avg(b)")
+        truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
+    else:
+        chunks, sess, _, meta = C.arrow_groupby(nrows=args.rows, nkeys=args.keys, with_expect=False)
+        nbytes = sum(c.nbytes for c in chunks)
+        ref_bytes = 24 * args.rows            # k, v1, v2, d: the referenced columns
+        desc = (f"Arrow high-cardinality pre-aggregation: {args.rows} rows, {args.keys} keys, 2-year date "
+                "window -> GROUP BY k: count, sum(v1), min/max/sum(v2)")
+        truth = None
+    gen_s = time.time() - t0
+    dev = xpu_b200.Device(0)
+    s = xpu_b200.Session(dev, sess)
+    ups = [dev.upload(c) for c in chunks]
+    batch = s.batch([p for _, p in ups])
+    r = batch.exec()
+    assert r["nitems_raw"] == meta["nitems_raw"], r
+    if truth is not None:
+        import xb_final as F
+        final, _ = s.final()
+        assert F.compare_groups(F.decode_kds_final(final, sess), truth) == []
+    for _ in range(max(0, args.warmup - 1)):
+        batch.exec()
+    sampler = ClockSampler(0)
+    torch.cuda.synchronize()
+    sampler.start()
+    ms = batch.time(args.steps)
+    clocks = sampler.stop()
+    info = s.info()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = ref_bytes / (ms / 1000.0) / 1e9
+    line = {"metric": METRIC, "value": args.rows / (ms / 1000.0), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "rows": args.rows, "chunks": len(chunks), "chunk_bytes": nbytes,
+                       "generation_s": round(gen_s, 1)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "algorithmic_bytes": ref_bytes,
+                         "kernel": ("xbj_kernel" if "jit" in info["kernels"].values() else "xb_exec_kernel"),
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+            "clocks": clocks, "gpu_launches": args.steps}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    s.close()
+    for b, _ in ups:
+        dev.free(b)
+    dev.close()
+
+
 # ------------------------------------------------------------------ batched commands
 def run_mixed(args):
     """256 chunk commands on the plain scan schema (one session each; chunk
@@ -649,6 +721,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
                                                                   "form of this path"}), flush=True)
             return
+        if args.workload in ("scan_groupby", "arrow_groupby"):
+            return run_config(args)
         return run_mixed(args) if args.workload == "mixed" else run_served(args)
     rank, world, local = dist_setup(args.gpus)
     try:
