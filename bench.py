@@ -104,6 +104,22 @@ def sum_over_ranks(x, world):
     return _reduce(x, world, dist.ReduceOp.SUM if world > 1 else None)
 
 
+def gather_finals(final, rank, world):
+    """Every rank's kds_final (uint8 array or None) collected on rank 0 in
+    rank order, as the GPU service collects one kds_final per GPU before
+    merging them (gpu_service.c:5442-5518); None on the other ranks."""
+    import numpy as np
+    import torch.distributed as dist
+    if world == 1:
+        return [final]
+    out = [None] * world if rank == 0 else None
+    payload = None if final is None else memoryview(final).tobytes()
+    dist.gather_object(payload, out, dst=0)
+    if rank != 0:
+        return None
+    return [None if b is None else np.frombuffer(b, dtype=np.uint8).copy() for b in out]
+
+
 def shard_seed(rank):
     """Weak scaling: every rank generates and owns a distinct fact shard."""
     return 1 + 16 * rank
@@ -283,6 +299,7 @@ def run_reference(args, rank, world):
 # ------------------------------------------------------------------ GPU arm
 def run_b200(args, rank, world, local):
     import torch
+    import xb_final as F
     import xpu_b200
     torch.cuda.set_device(local)
     fact, sess, km, chunks, meta = build_workload(args.rows, rank)
@@ -345,6 +362,27 @@ def run_b200(args, rank, world, local):
     e2e_el = max_over_ranks(sum(e2e_times) / len(e2e_times), world)
     e2e_value = rows_total / e2e_el
 
+    # ---- N>1: every rank's kds_final merged on rank 0's GPU (the service's
+    # final step over per-GPU results); checked against the ranks' row counts
+    merge = None
+    if world > 1:
+        finals = gather_finals(final, rank, world)
+        nout = sum_over_ranks(float(meta["nitems_out"]), world)
+        if rank == 0:
+            t0 = time.perf_counter()
+            sm = xpu_b200.Session(dev, sess, kmp, 2)
+            for f in finals:
+                if f is not None:
+                    sm.merge_final(f)
+            merged, _ = sm.final()
+            sm.close()
+            merge_ms = 1000.0 * (time.perf_counter() - t0)
+            groups = F.decode_kds_final(merged, sess)
+            assert sum(v[1] for v in groups.values()) == int(nout), "merged row count"
+            merge = {"ranks": world, "groups": len(groups), "ms": merge_ms,
+                     "includes": "OpenSession, one MergeFinal per rank's kds_final (host copy), Final"}
+        barrier(world)
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1:
@@ -391,6 +429,8 @@ def run_b200(args, rank, world, local):
                 "clocks": clocks,
                 "gpu_launches": args.steps,
                 "cpu_baseline": cpu}
+        if merge:
+            line["final_merge"] = merge
         print(json.dumps(line), flush=True)
     for base, _ in ups:
         dev.free(base)

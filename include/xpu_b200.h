@@ -134,6 +134,24 @@ int  xpuB200Final(xpuB200Session *sess, void *kds_final_buf, uint64_t buf_sz,
 int  xpuB200FinalNoAlloc(xpuB200Session *sess, void *kds_final_dev, uint64_t buf_sz,
                          uint64_t *p_required, kern_exec_results *results, kern_errorbuf *err);
 
+/*
+ * Merge another GPU's (or session's) partial-aggregation result into this
+ * session's group table, so that a following xpuB200Final returns the
+ * groups of both.  kds_final is a KDS_FORMAT_HASH buffer that xpuB200Final
+ * (or xpuB200FinalNoAlloc) of a session with the same GROUP BY program
+ * wrote: every group tuple is decoded, its keys looked up (or inserted) by
+ * the tuple's hash and its partial states added into the matching entry
+ * with the same reduction operations the chunk launches use.
+ * kds_final_on_device != 0: kds_final is device memory readable by this
+ * session's GPU (its own memory, or a peer's with peer access enabled);
+ * otherwise it is host memory that is copied in first.
+ * Replaces the secondary-buffer merge of __gpuservHandleGpuPreAggFinal
+ * (gpu_service.c:5442-5518) that launches kern_gpupreagg_final_merge
+ * (cuda_gpupreagg.cu:2329-2432).
+ */
+int  xpuB200MergeFinal(xpuB200Session *sess, const kern_data_store *kds_final,
+                       int kds_final_on_device, kern_errorbuf *err);
+
 void xpuB200CloseSession(xpuB200Session *sess);
 
 /*

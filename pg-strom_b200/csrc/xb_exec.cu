@@ -1362,6 +1362,199 @@ __global__ void xb_final_write(XbFinalArgs args)
     }
 }
 
+/* ----------------------------------------------------------------
+ * merge of another kds_final (kern_gpupreagg_final_merge,
+ * cuda_gpupreagg.cu:2331-2432, reading the keys back as
+ * ExecLoadKeysFromGroupByFinal does, xpu_common.cu:1675-1727)
+ * ---------------------------------------------------------------- */
+#define XB_GENT_MAX     2048    /* largest group entry a merge stages per thread */
+
+struct XbMergeArgs {
+    const xb_plan          *plan;
+    const kern_data_store  *kds;        /* the other kds_final (device copy) */
+    xb_gtable              *gt;
+    xb_status              *st;
+};
+
+/* one packed partial state back into the group-entry form (the inverse of
+ * xb_write_group_tuple); returns its bytes in the tuple */
+__device__ uint32_t
+xb_read_state(const xb_agg &a, const char *p, bool present, uint64_t *su)
+{
+    for (uint32_t k = 0; k < a.state_sz / 8; k++)
+        su[k] = 0;
+    switch (a.action) {
+    case KAGG_ACTION__NROWS_ANY:
+    case KAGG_ACTION__NROWS_COND:
+        if (present) xb_store((char *)su, p, 8);
+        return 8;
+    case KAGG_ACTION__PMIN_INT32: case KAGG_ACTION__PMIN_INT64:
+    case KAGG_ACTION__PMAX_INT32: case KAGG_ACTION__PMAX_INT64: {
+        kagg_state__pminmax_int64_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        su[0] = (uint64_t)r.value;
+        *(uint32_t *)(su + 1) = (r.attrs & PAGG_MINMAX_ATTRS__VALID) ? 1u : 0u;
+        return sizeof(r);
+    }
+    case KAGG_ACTION__PMIN_FP64: case KAGG_ACTION__PMAX_FP64: {
+        kagg_state__pminmax_fp64_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        const bool valid = (r.attrs & PAGG_MINMAX_ATTRS__VALID) != 0;
+        su[0] = valid ? (uint64_t)xb_f64_ordered(r.value) : 0;
+        *(uint32_t *)(su + 1) = valid ? 1u : 0u;
+        return sizeof(r);
+    }
+    case KAGG_ACTION__PSUM_INT: case KAGG_ACTION__PAVG_INT: {
+        kagg_state__psum_int_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        su[0] = (uint64_t)r.nitems;
+        su[1] = (uint64_t)r.sum;
+        return sizeof(r);
+    }
+    case KAGG_ACTION__PSUM_INT64: case KAGG_ACTION__PAVG_INT64:
+    case KAGG_ACTION__PSUM_NUMERIC: case KAGG_ACTION__PAVG_NUMERIC: {
+        kagg_state__psum_numeric_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        su[0] = r.nitems;
+        su[1] = r.sum.u64_lo;
+        su[2] = r.sum.u64_hi;
+        if (a.state_sz >= 32)
+            *(uint32_t *)(su + 3) = r.attrs & ~PAGG_NUMERIC_ATTRS__WEIGHT;
+        return sizeof(r);
+    }
+    case KAGG_ACTION__PSUM_FP: case KAGG_ACTION__PAVG_FP: {
+        kagg_state__psum_fp_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        su[0] = (uint64_t)r.nitems;
+        ((double *)su)[1] = r.sum;
+        return sizeof(r);
+    }
+    case KAGG_ACTION__STDDEV: {
+        kagg_state__stddev_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        su[0] = (uint64_t)r.nitems;
+        ((double *)su)[1] = r.sum_x;
+        ((double *)su)[3] = r.sum_x2;
+        return sizeof(r);
+    }
+    case KAGG_ACTION__COVAR: {
+        kagg_state__covar_packed r;
+        if (!present) return sizeof(r);
+        xb_store((char *)&r, p, sizeof(r));
+        su[0] = (uint64_t)r.nitems;
+        ((double *)su)[1] = r.sum_x;
+        ((double *)su)[3] = r.sum_xx;
+        ((double *)su)[5] = r.sum_y;
+        ((double *)su)[7] = r.sum_yy;
+        ((double *)su)[9] = r.sum_xy;
+        return sizeof(r);
+    }
+    default:
+        return 0;
+    }
+}
+
+/* every group tuple of the other kds_final: its keys are looked up (or
+ * created) in this session's global table and its partial states merged */
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_merge_final(XbMergeArgs args)
+{
+    const xb_plan *plan = args.plan;
+    const kern_data_store *kds = args.kds;
+    const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kds->nitems; i += gridDim.x * blockDim.x) {
+        const uint64_t off = rowindex[i];
+        if (off == 0 || off > kds->length || ((kds->length - off) & 7) != 0) {
+            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+            continue;
+        }
+        const kern_tupitem *ti = (const kern_tupitem *)((const char *)kds + kds->length - off);
+        const char *base = (const char *)ti;
+        const uint32_t t_len = ti->t_len;
+        uint32_t t = (uint32_t)ti->t_hoff - MINIMAL_TUPLE_OFFSET;
+        const bool hasnull = (ti->t_infomask & HEAP_HASNULL) != 0;
+        if (off < t_len || t > t_len) {
+            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+            continue;
+        }
+        /* the source entry in the group-entry form */
+        alignas(16) char src[XB_GENT_MAX];
+        for (uint32_t k = 0; k < plan->gent_size && k < XB_GENT_MAX; k++)
+            src[k] = 0;
+        xb_keyimg *img = (xb_keyimg *)(src + plan->gent_keys_off);
+        bool bad = false;
+        for (uint32_t j = 0; j < plan->naggs && !bad; j++) {
+            const xb_agg &a = plan->aggs[j];
+            const bool present = !hasnull || ((ti->t_bits[j >> 3] >> (j & 7)) & 1u);
+            t = (uint32_t)PGSTROM_TYPEALIGN(a.attalign > 0 ? a.attalign : 1, t);
+            const char *p = base + t;
+            uint32_t nbytes = 0;
+            if (a.action == KAGG_ACTION__VREF) {
+                if (a.key_index < 0)
+                    continue;
+                const xb_key &k = plan->keys[a.key_index];
+                xb_keyimg &ki = img[a.key_index];
+                ki.isnull = !present;
+                if (!present)
+                    continue;
+                switch (k.ld) {
+                case XB_LD_BOOL: ki.val = *(const uint8_t *)p; nbytes = 1; break;
+                case XB_LD_INT2: { int16_t v; xb_store((char *)&v, p, 2); ki.val = (uint64_t)(int64_t)v; nbytes = 2; break; }
+                case XB_LD_INT4:
+                case XB_LD_DATE: { int32_t v; xb_store((char *)&v, p, 4); ki.val = (uint64_t)(int64_t)v; nbytes = 4; break; }
+                case XB_LD_INT8:
+                case XB_LD_FLT8: xb_store((char *)&ki.val, p, 8); nbytes = 8; break;
+                case XB_LD_FLT4: {
+                    float v; xb_store((char *)&v, p, 4);
+                    ki.val = (uint64_t)__double_as_longlong((double)v);
+                    nbytes = 4;
+                    break;
+                }
+                case XB_LD_TEXT: {
+                    uint32_t h; xb_store((char *)&h, p, 4);
+                    nbytes = h >> 2;
+                    ki.val = (uint64_t)(p + 4);
+                    ki.len = nbytes - 4;
+                    break;
+                }
+                case XB_LD_NUMERIC:
+                    nbytes = xb_numeric_varsize((const uint8_t *)p);
+                    ki.val = (uint64_t)p;
+                    ki.len = 0;
+                    break;
+                default:
+                    bad = true;
+                    break;
+                }
+            } else {
+                nbytes = xb_read_state(a, p, present, (uint64_t *)(src + a.state_off));
+            }
+            if (present)
+                t += nbytes;
+            if (t > t_len)
+                bad = true;
+        }
+        if (bad) {
+            XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
+            continue;
+        }
+        bool full = false;
+        char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, ti->hash, img, args.gt, args.st, &full);
+        if (g)
+            xb_merge_states(plan, g, src);
+        else if (full) {
+            XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+            atomicOr(&args.gt->overflow, 1u);
+        }
+    }
+}
+
 /* ================================================================
  * host side
  * ================================================================ */
@@ -2471,6 +2664,59 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
         rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "Final: %s", cudaGetErrorString(cudaGetLastError()));
     cleanup();
     return rc;
+}
+
+extern "C" int
+xpuB200MergeFinal(xpuB200Session *s, const kern_data_store *kds_final, int kds_final_on_device,
+                  kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s || !kds_final)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid MergeFinal arguments");
+    xb_sched_drain_session(s);
+    std::lock_guard<std::mutex> g(s->lock);
+    const xb_plan *plan = s->h_plan;
+    if (!plan->has_groupby)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "the session has no GROUP BY");
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    cudaStream_t st = s->stream;
+    /* the header, checked on the host */
+    kern_data_store head;
+    std::vector<char> hb;
+    if (kds_final_on_device) {
+        XB_CUDA(cudaMemcpy(&head, kds_final, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+        hb.resize(KDS_HEAD_LENGTH(&head));
+        XB_CUDA(cudaMemcpy(hb.data(), kds_final, hb.size(), cudaMemcpyDeviceToHost), err);
+    } else {
+        hb.assign((const char *)kds_final, (const char *)kds_final + KDS_HEAD_LENGTH(kds_final));
+    }
+    const kern_data_store *h = (const kern_data_store *)hb.data();
+    if (h->format != KDS_FORMAT_HASH || h->ncols != plan->naggs ||
+        KDS_HEAD_LENGTH(h) + 8 * ((uint64_t)h->hash_nslots + h->nitems) > h->length)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "kds_final to merge is not this session's KDS_FORMAT_HASH");
+    if (h->nitems == 0)
+        return 0;
+    if (plan->gent_size > XB_GENT_MAX)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "group entries of %u bytes cannot be merged", plan->gent_size);
+    const kern_data_store *d_kds = kds_final;
+    char *d_copy = nullptr;
+    if (!kds_final_on_device) {
+        XB_CUDA(cudaMallocAsync((void **)&d_copy, h->length, st), err);
+        XB_CUDA(cudaMemcpyAsync(d_copy, kds_final, h->length, cudaMemcpyHostToDevice, st), err);
+        d_kds = (const kern_data_store *)d_copy;
+    }
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+    XbMergeArgs ma;
+    ma.plan = s->d_plan;
+    ma.kds = d_kds;
+    ma.gt = s->d_gt;
+    ma.st = s->d_status;
+    int grid = (int)((h->nitems + XB_BLOCK - 1) / XB_BLOCK);
+    if (grid > s->dev->nsm * 8) grid = s->dev->nsm * 8;
+    xb_merge_final<<<grid, XB_BLOCK, 0, st>>>(ma);
+    if (d_copy)
+        cudaFreeAsync(d_copy, st);
+    return xb_wait_status(s, err);
 }
 
 /* ----------------------------------------------------------------

@@ -65,9 +65,9 @@ def scan_groupby_session(a_limit=300, ngroups=64):
         ngroups_estimate=float(ngroups))
 
 
-def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ngroups=64):
-    """The plain scan + filter + group-by table; ngroups sets the domain of
-    g (64 in the benchmark configuration)."""
+def _scan_table(nrows, seed_config, null_frac, ngroups):
+    """t0 (id int8, a int4, b float8 with NULLs, c numeric(12,2), g int4)
+    and its column arrays."""
     r = rng_for(seed_config, 0)
     id_ = np.arange(nrows, dtype=np.int64)
     a = r.integers(0, 1000, nrows, dtype=np.int32)
@@ -83,6 +83,13 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ng
         Column("c", "numeric", typmod=typmod_c, values=encode_numeric_array(c_unscaled, 2)),
         Column("g", "int4", values=g),
     ], nrows)
+    return tbl, a, b, bnull, c_unscaled, g
+
+
+def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ngroups=64):
+    """The plain scan + filter + group-by table; ngroups sets the domain of
+    g (64 in the benchmark configuration)."""
+    tbl, a, b, bnull, c_unscaled, g = _scan_table(nrows, seed_config, null_frac, ngroups)
     session = scan_groupby_session(a_limit, ngroups)
     # expected partial states per group, straight from the arrays
     m = a < a_limit
@@ -105,6 +112,79 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ng
                         "avg_b": (int(nb[k]), Approx(float(sb_[k]), float(sab[k])))}
     meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()),
             "agg_names": ["nrows", "sum_a", "sum_c", "avg_b"], "nkeys": 1}
+    return tbl, session, None, expect, meta
+
+
+def wide_groupby_session(a_limit=600, ngroups=3000):
+    """WHERE a < a_limit GROUP BY g -> count(*), count(b), min(a),
+    max(a::int8), min(b), max(b), sum(b), avg(c), stddev(b), covar(b, a):
+    every partial state form of kds_final."""
+    typmod_c = numeric_typmod(12, 2)
+    va, vb, vc, vg = (Var(0, 2, "int4"), Var(0, 3, "float8"),
+                      Var(0, 4, "numeric", typmod_c), Var(0, 5, "int4"))
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    return sb.build(
+        scan_quals=Func("int4lt", [va, Const("int4", a_limit)], "bool"),
+        groupby_keys=[vg],
+        aggs=[Agg("NROWS_ANY"),
+              Agg("NROWS_COND", vb),
+              Agg("PMIN_INT32", va),
+              Agg("PMAX_INT64", Func("int4_to_int8", [va], "int8")),
+              Agg("PMIN_FP64", vb),
+              Agg("PMAX_FP64", vb),
+              Agg("PSUM_FP", vb),
+              Agg("PAVG_NUMERIC", vc, typmod_c),
+              Agg("STDDEV", vb),
+              Agg("COVAR", vb, arg1=Func("int4_to_float8", [va], "float8"))],
+        ngroups_estimate=float(ngroups))
+
+
+def _group_sum(g, m, x, n):
+    out = np.zeros(n, dtype=np.float64)
+    np.add.at(out, g[m], x[m])                   # unbuffered: row order per group
+    return out
+
+
+def wide_groupby(nrows=200_000, seed_config=5, null_frac=0.05, a_limit=600, ngroups=3000):
+    """The scan table under wide_groupby_session, with the expected
+    partial states per group (float sums as Approx with their terms'
+    magnitude)."""
+    tbl, a, b, bnull, c_unscaled, g = _scan_table(nrows, seed_config, null_frac, ngroups)
+    session = wide_groupby_session(a_limit, ngroups)
+    m = a < a_limit
+    mb = m & ~bnull
+    cnt = np.bincount(g[m], minlength=ngroups)
+    nb = np.bincount(g[mb], minlength=ngroups)
+    amin = np.full(ngroups, np.iinfo(np.int64).max)
+    np.minimum.at(amin, g[m], a[m].astype(np.int64))
+    amax = np.full(ngroups, np.iinfo(np.int64).min)
+    np.maximum.at(amax, g[m], a[m].astype(np.int64))
+    bmin = np.full(ngroups, np.inf)
+    np.minimum.at(bmin, g[mb], b[mb])
+    bmax = np.full(ngroups, -np.inf)
+    np.maximum.at(bmax, g[mb], b[mb])
+    sc = np.zeros(ngroups, dtype=np.int64)
+    np.add.at(sc, g[m], c_unscaled[m])
+    af = a.astype(np.float64)
+    sx, sax = _group_sum(g, mb, b, ngroups), _group_sum(g, mb, np.abs(b), ngroups)
+    sxx = _group_sum(g, mb, b * b, ngroups)
+    sy, syy = _group_sum(g, mb, af, ngroups), _group_sum(g, mb, af * af, ngroups)
+    sxy, saxy = _group_sum(g, mb, b * af, ngroups), _group_sum(g, mb, np.abs(b * af), ngroups)
+    expect = {}
+    for k in np.flatnonzero(cnt).tolist():
+        valid = 1 if nb[k] else 0
+        expect[(k,)] = [
+            int(cnt[k]), int(nb[k]),
+            (1, int(amin[k])), (1, int(amax[k])),
+            (valid, float(bmin[k]) if valid else None), (valid, float(bmax[k]) if valid else None),
+            (int(nb[k]), Approx(float(sx[k]), float(sax[k]))),
+            (int(cnt[k]), int(sc[k]), 2),
+            (int(nb[k]), Approx(float(sx[k]), float(sax[k])), Approx(float(sxx[k]), float(sxx[k]))),
+            (int(nb[k]), Approx(float(sx[k]), float(sax[k])), Approx(float(sxx[k]), float(sxx[k])),
+             Approx(float(sy[k]), float(sy[k])), Approx(float(syy[k]), float(syy[k])),
+             Approx(float(sxy[k]), float(saxy[k]))),
+        ]
+    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()), "nkeys": 1}
     return tbl, session, None, expect, meta
 
 

@@ -633,6 +633,7 @@ class Agg:
     action: str             # KAGG action name
     arg: Expr = None
     typmod: int = -1
+    arg1: Expr = None       # COVAR's second argument (Y)
 
 
 def const_image(typ, value):
@@ -940,17 +941,20 @@ class SessionBuilder:
             nargs = 0
             used = set()
             for a in aggs:
-                slot = -1
-                if a.arg is not None:
-                    pos = len(buf.b)
-                    d = self.emit_save(buf, a.arg, gdepth)
-                    slot = d.slot
-                    if slot in used:
-                        del buf.b[pos:]
-                    else:
-                        used.add(slot)
-                        nargs += 1
-                descs.append((KAGG[a.action], slot, -1, -1, a.typmod))
+                slots = []
+                for arg in (a.arg, a.arg1):
+                    slot = -1
+                    if arg is not None:
+                        pos = len(buf.b)
+                        d = self.emit_save(buf, arg, gdepth)
+                        slot = d.slot
+                        if slot in used:
+                            del buf.b[pos:]
+                        else:
+                            used.add(slot)
+                            nargs += 1
+                    slots.append(slot)
+                descs.append((KAGG[a.action], slots[0], slots[1], -1, a.typmod))
             for k, ks in zip(groupby_keys, keyslots):
                 pos = len(buf.b)
                 d = self.emit_save(buf, k, gdepth)

@@ -48,6 +48,7 @@ def lib():
         L.xpuB200ExecTask.argtypes = [P, P, I, P, EB]
         L.xpuB200ExecTaskDst.argtypes = [P, P, I, P, U64, I, ctypes.POINTER(U64), P, EB]
         L.xpuB200Final.argtypes = [P, P, U64, ctypes.POINTER(U64), P, EB]
+        L.xpuB200MergeFinal.argtypes = [P, P, I, EB]
         L.xpuB200CloseSession.argtypes = [P]
         L.xpuB200HandleCommand.argtypes = [P, ctypes.POINTER(P), P, P, U64, P, U64]
         L.xpuB200DeviceAlloc.argtypes = [P, U64, ctypes.POINTER(P)]
@@ -240,6 +241,15 @@ class Session:
         if rc:
             raise XpuB200Error(rc, e)
         return buf, parse_results(res)
+
+    def merge_final(self, kds, on_device=False):
+        """Merge another session's kds_final (a uint8 array from final(), or
+        a device address with on_device) into this session's groups."""
+        e = KernErrorbuf()
+        p = ctypes.c_void_p(kds) if on_device else _ptr(kds)
+        rc = lib().xpuB200MergeFinal(self.h, p, 1 if on_device else 0, ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
 
     def batch(self, dptrs):
         return Batch(self, dptrs)

@@ -78,6 +78,23 @@ def test_scan_groupby_parity(device, kernel, nrows, ppc):
     assert res["final_nitems"] == len(truth)
 
 
+def test_every_partial_state_form_parity(device, kernel):
+    # count(x), min/max of int4 / int8 / float8, sum float8, avg numeric,
+    # stddev and covar states, against the column arrays and the oracle
+    tbl, sess, _, expect, meta = C.wide_groupby(nrows=300_000, ngroups=3000)
+    chunks = tbl.block_chunks(pages_per_chunk=256)
+    final, st, res = run_gpu(device, sess, chunks, kernel=kernel)
+    assert st["nitems_in"] == meta["nitems_in"]
+    got = F.decode_kds_final(final, sess)
+    assert F.compare_groups(got, expect) == []
+    ofinal, _ = run_oracle(sess, chunks)
+    want = F.decode_kds_final(ofinal, sess)
+    assert set(got) == set(want)
+    for k in want:
+        # integer and numeric states bit-exact with the oracle
+        assert got[k][:4] == want[k][:4] and got[k][7] == want[k][7], k
+
+
 def test_scan_groupby_device_resident(device, kernel):
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=100_000)
     chunks = tbl.block_chunks(pages_per_chunk=200)

@@ -1,8 +1,9 @@
 """The N>1 host logic of bench.py on CPU: two gloo ranks, each owning its
 own shard; the job time is the max over ranks, the row count the sum, and
 the per-rank shards are disjoint (distinct seeds).  Each rank runs the
-oracle on its shard and rank 0 checks the per-rank results add up to the
-union's."""
+oracle on its shard; the ranks' kds_final buffers are gathered on rank 0
+(the input of the device merge that follows at N>1) and their states add up
+to the union's."""
 import os
 import socket
 import sys
@@ -26,6 +27,7 @@ def _worker(rank, world, port, q):
         sys.path.insert(0, os.path.join(ROOT, sub))
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
                       WORLD_SIZE=str(world))
+    import numpy as np
     import torch.distributed as dist
     from datetime import timedelta
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
@@ -39,7 +41,8 @@ def _worker(rank, world, port, q):
         o = O.Oracle(sess, km)
         for ch in fact.block_chunks(pages_per_chunk=100):
             o.exec(ch)
-        got = F.decode_kds_final(o.final(), sess)
+        o_final = o.final()
+        got = F.decode_kds_final(o_final, sess)
         o.close()
         truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
         ok = F.compare_groups(got, truth) == []
@@ -47,7 +50,21 @@ def _worker(rank, world, port, q):
         n = bench.sum_over_ranks(1000.0, world)
         objs = [None] * world
         dist.all_gather_object(objs, (rank, ok, sorted(got.items())[:3]))
-        q.put((rank, ok, t, n, objs))
+        # per-rank kds_final collected on rank 0 (the input of the device
+        # merge); the union's groups are the sum of the ranks' states
+        fin = o_final
+        finals = bench.gather_finals(fin, rank, world)
+        union = None
+        if rank == 0:
+            union = {}
+            for f in finals:
+                for k, v in F.decode_kds_final(f, sess).items():
+                    u = union.setdefault(k, [(0, 0), 0])
+                    union[k] = [(u[0][0] + v[0][0], u[0][1] + v[0][1]), u[1] + v[1]]
+            assert all(isinstance(f, np.ndarray) for f in finals)
+        else:
+            assert finals is None
+        q.put((rank, ok, t, n, objs, union, sum(v[1] for v in got.values())))
     finally:
         dist.destroy_process_group()
 
@@ -63,11 +80,13 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    res.sort()
-    for rank, ok, t, n, objs in res:
+    res.sort(key=lambda x: x[0])
+    for rank, ok, t, n, objs, union, nrows in res:
         assert ok
         assert t == 2.0          # max over ranks
         assert n == 2000.0       # sum over ranks
+    union = res[0][5]
+    assert sum(v[1] for v in union.values()) == sum(r[6] for r in res)
     # shards differ: the first groups' states are not identical across ranks
     objs = res[0][4]
     assert objs[0][2] != objs[1][2]

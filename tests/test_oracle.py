@@ -36,6 +36,18 @@ def test_oracle_join_groupby():
     o.close()
 
 
+def test_oracle_every_partial_state_form():
+    # count, count(x), min/max int and float8, sum float8, avg numeric,
+    # stddev and covar partial states against the column arrays
+    tbl, sess, _, expect, meta = C.wide_groupby(nrows=60_000, ngroups=500)
+    o = O.Oracle(sess)
+    for ch in tbl.block_chunks(pages_per_chunk=100):
+        o.exec(ch)
+    assert o.stats()["nitems_in"] == meta["nitems_in"]
+    assert F.compare_groups(F.decode_kds_final(o.final(), sess), expect) == []
+    o.close()
+
+
 def test_oracle_all_filtered_out():
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=5000, a_limit=0)
     o = O.Oracle(sess)
