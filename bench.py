@@ -57,6 +57,8 @@ def parse():
                          "scan and the Arrow high-cardinality configurations (--rows, --keys); mixed: "
                          "256 batched chunk commands; served: Poisson-arrival query mix through the "
                          "serving scheduler")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="keep the default launch shape (no xpuB200BatchTune before timing)")
     ap.add_argument("--keys", type=int, default=10_000_000)
     ap.add_argument("--requests", type=int, default=400)
     ap.add_argument("--qps", type=float, default=200.0)
@@ -118,6 +120,17 @@ def gather_finals(final, rank, world):
     if rank != 0:
         return None
     return [None if b is None else np.frombuffer(b, dtype=np.uint8).copy() for b in out]
+
+
+def _tune(batch, args):
+    """The launch shape the timed passes use: tuned on the batch itself
+    (xpuB200BatchTune, before any pass counts) unless --no-tune."""
+    if not args.tune:
+        return {"tuned": False}
+    rep = batch.tune()
+    return {"tuned": True, "ctas_per_sm": rep["best"]["ctas_per_sm"], "sm_groups": rep["best"]["sm_groups"],
+            "default_sm_groups": rep["default_sm_groups"],
+            "measured_ms": {f'{c["ctas_per_sm"]}/{c["sm_groups"]}': round(c["ms"], 4) for c in rep["candidates"]}}
 
 
 def shard_seed(rank):
@@ -310,6 +323,7 @@ def run_b200(args, rank, world, local):
     s = xpu_b200.Session(dev, sess, km, 2)
     ups = [dev.upload(c) for c in chunks]
     batch = s.batch([p for _, p in ups])
+    shape = _tune(batch, args)
     r = batch.exec()
     assert r["nitems_raw"] == meta["nitems_raw"], r
     for _ in range(max(0, args.warmup - 1)):
@@ -417,7 +431,8 @@ def run_b200(args, rank, world, local):
                            "fact_rows_per_gpu": args.rows, "chunks_per_gpu": len(chunks),
                            "chunk_bytes": "64 MB KDS_FORMAT_BLOCK", "heap_bytes_per_gpu": nbytes,
                            "l2_note": "inputs (5.2 GB) exceed L2 (126 MB) by 40x",
-                           "parallelism": f"dp{world} (independent shards, no collective)"},
+                           "parallelism": f"dp{world} (independent shards, no collective)",
+                           "launch_shape": shape},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "kernel": kernel,
@@ -466,6 +481,7 @@ def run_config(args):
     s = xpu_b200.Session(dev, sess)
     ups = [dev.upload(c) for c in chunks]
     batch = s.batch([p for _, p in ups])
+    shape = _tune(batch, args)
     r = batch.exec()
     assert r["nitems_raw"] == meta["nitems_raw"], r
     if truth is not None:
@@ -491,7 +507,7 @@ def run_config(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
             "config": {"workload": desc, "rows": args.rows, "chunks": len(chunks), "chunk_bytes": nbytes,
-                       "generation_s": round(gen_s, 1)},
+                       "generation_s": round(gen_s, 1), "launch_shape": shape},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "algorithmic_bytes": ref_bytes,
                          "kernel": ("xbj_kernel" if "jit" in info["kernels"].values() else "xb_exec_kernel"),
@@ -519,8 +535,19 @@ def run_mixed(args):
     cmds = C.mixed_commands(ncmds=256)
     gen_s = time.time() - t0
     dev = xpu_b200.Device(0)
-    sessions = [xpu_b200.Session(dev, c["session"]) for c in cmds]
     ups = [dev.upload(c["chunk"]) for c in cmds]
+    # launch shape tuned on the largest command (a session of its own); the
+    # commands' sessions adopt its CTA bound at their first launch
+    shape = {"tuned": False}
+    if args.tune:
+        big = max(range(len(cmds)), key=lambda i: cmds[i]["chunk"].nbytes)
+        ts = xpu_b200.Session(dev, cmds[big]["session"])
+        tb = ts.batch([ups[big][1]])
+        shape = _tune(tb, args)
+        shape["tuned_on"] = f"command {big} ({cmds[big]['chunk'].nbytes} bytes)"
+        tb.close()
+        ts.close()
+    sessions = [xpu_b200.Session(dev, c["session"]) for c in cmds]
     mix = xpu_b200.Mix(dev, sessions, [p for _, p in ups])
     out = mix.exec()
     assert all(err is None for _, err in out), [str(e) for _, e in out if e][:3]
@@ -560,6 +587,7 @@ def run_mixed(args):
                        "commands": len(cmds), "rows": rows, "chunk_bytes": info["bytes"],
                        "launches_per_run": info["launches"], "specialised_commands": info["specialised"],
                        "work_items": info["items"], "generation_s": round(gen_s, 1),
+                       "launch_shape": shape,
                        "l2_note": "inputs (2.2 GB) exceed L2 (126 MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,

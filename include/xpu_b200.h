@@ -241,6 +241,27 @@ int  xpuB200BatchExec(xpuB200Batch *batch, kern_exec_results *results, kern_erro
 /* runs the batch niters times; average kernel milliseconds (CUDA events on
  * the session stream) in *p_msec */
 int  xpuB200BatchTime(xpuB200Batch *batch, int niters, double *p_msec, kern_errorbuf *err);
+/*
+ * Autotuning of the session's launch shape on the batch's chunks: the
+ * resident CTAs per SM the session-specialised kernel is built for (2, 3, 4,
+ * 6, 8; each a separately compiled kernel) and then the capacity of the
+ * per-CTA shared-memory group table (the default, twice it, none), each
+ * measured with CUDA events on a fresh group table.  The fastest shape is
+ * kept by the session and remembered for this GPU: later sessions of the
+ * same plan shape and default table capacity (every chunk command of one
+ * query template) adopt it at their first launch; sessions of the same plan
+ * shape with another default capacity (other group-count estimates, as in
+ * a mixed batch) adopt its CTA bound.  Call it before the session executes chunks (otherwise
+ * ERRCODE_DEVICE_ERROR); the group table is empty again on return.  flags
+ * must be 0.  report (if not NULL) receives a JSON text with every measured
+ * shape.  Join partition fan-out is not a parameter: inner relations are
+ * kept whole (direct-address tables or one hash index) in HBM/L2.
+ * No counterpart in the reference (its launch shape comes from
+ * gpuOptimalBlockSize, gpu_service.c:3797-3810, over the
+ * occupancy calculation of gpu_device.c:1121).
+ */
+int  xpuB200BatchTune(xpuB200Batch *batch, uint32_t flags, char *report, size_t report_len,
+                      kern_errorbuf *err);
 void xpuB200BatchDestroy(xpuB200Batch *batch);
 
 /* Device memory helpers for callers that keep chunks resident in HBM. */

@@ -26,7 +26,9 @@
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <deque>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 #include <string>
@@ -1667,7 +1669,43 @@ struct xpuB200Session {
     size_t          jit_smem_fmt[256] = {0}; /* per format, with its page staging */
     double          jit_compile_ms = 0.0;
     std::string     jit_msg;
+    /* launch shape: resident CTAs per SM the specialised kernels are built
+     * for (0: default) and the shared group table's default capacity, as
+     * tuned by xpuB200BatchTune or adopted from its process-wide cache */
+    int             jit_minb = 0;
+    uint32_t        sm_cap_default = 0;
+    bool            tune_looked_up = false;
 };
+
+/* shared group-table capacity 'cap' and the launch geometry that follows
+ * from it (shared memory of both kernels, the interpreter's grid); the
+ * specialised kernels are prepared again at their next launch */
+static int xb_set_sm_cap(xpuB200Session *s, uint32_t cap)
+{
+    const xb_plan *plan = s->h_plan;
+    size_t smem = s->plan_bytes + PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) +
+                  (size_t)cap * plan->gent_size + (size_t)XB_WARPS * s->warp_bytes;
+    s->smem_bytes = smem;
+    if (smem > s->dev->smem_optin)
+        return -1;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_exec_kernel, XB_BLOCK, smem);
+    if (per_sm < 1)
+        return -1;
+    s->sm_cap = cap;
+    s->grid = per_sm * s->dev->nsm;
+    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + sizeof(XbSrc) * XB_WARPS +
+                  (size_t)cap * xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16);
+    /* existence bitmaps staged after the group table (16-byte aligned) */
+    size_t bits = 0;
+    for (uint32_t d = 1; d <= plan->nrels; d++)
+        bits += (size_t)plan->inner[d].dbits_words * 4;
+    if (bits)
+        s->jit_smem = PGSTROM_TYPEALIGN(16, s->jit_smem) + PGSTROM_TYPEALIGN(16, bits);
+    for (int f = 0; f < 256; f++)
+        s->jit_tried[f] = false;
+    return 0;
+}
 
 static const char *xb_msg_text(uint32_t id)
 {
@@ -2085,25 +2123,9 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     s->warp_bytes = (uint32_t)(XB_WARP_HEAD + sizeof(XbCursor) * plan->nrels + XB_REGS_BYTES(plan->nregs));
     s->plan_bytes = (uint32_t)PGSTROM_TYPEALIGN(16, offsetof(xb_plan, insns) +
                                                  sizeof(xb_insn) * (size_t)plan->ninsns);
-    s->smem_bytes = s->plan_bytes + PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) +
-                    (size_t)s->sm_cap * plan->gent_size + (size_t)XB_WARPS * s->warp_bytes;
-    if (s->smem_bytes > dev->smem_optin)
-        FAIL(ERRCODE_DEVICE_FATAL, "dynamic shared memory of %zu bytes not available", s->smem_bytes);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_exec_kernel, XB_BLOCK, s->smem_bytes);
-    if (per_sm < 1)
+    s->sm_cap_default = s->sm_cap;
+    if (xb_set_sm_cap(s, s->sm_cap) != 0)
         FAIL(ERRCODE_DEVICE_FATAL, "executor kernel does not fit on an SM (%zu bytes smem)", s->smem_bytes);
-    s->grid = per_sm * dev->nsm;
-    s->jit_smem = PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) + sizeof(XbSrc) * XB_WARPS +
-                  (size_t)s->sm_cap * xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16);
-    /* existence bitmaps staged after the group table (16-byte aligned) */
-    {
-        size_t bits = 0;
-        for (uint32_t d = 1; d <= plan->nrels; d++)
-            bits += (size_t)plan->inner[d].dbits_words * 4;
-        if (bits)
-            s->jit_smem = PGSTROM_TYPEALIGN(16, s->jit_smem) + PGSTROM_TYPEALIGN(16, bits);
-    }
     {
         const char *env = getenv("XPU_B200_JIT");
         s->jit_enabled = !(env && env[0] == '0');
@@ -2171,19 +2193,73 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
                         uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
                         kern_errorbuf *err);
 
+/* ----------------------------------------------------------------
+ * launch-shape tuning: resident CTAs per SM of the specialised kernels and
+ * the shared group table's capacity, measured on a batch of chunks and
+ * remembered per GPU for every session of the same plan shape and default
+ * table capacity (the caller's group-count estimate)
+ * ---------------------------------------------------------------- */
+struct xb_tune_choice {
+    int         minb;
+    uint32_t    sm_cap;
+};
+static std::mutex g_tune_lock;
+static std::map<std::tuple<int, uint64_t, uint32_t>, xb_tune_choice> g_tune;
+/* per plan shape alone: the CTA bound last tuned for it, adopted by
+ * sessions whose default table capacity was not tuned (another group-count
+ * estimate) */
+static std::map<std::pair<int, uint64_t>, int> g_tune_minb;
+
+static std::tuple<int, uint64_t, uint32_t> xb_tune_key(xpuB200Session *s, uint32_t format)
+{
+    return std::make_tuple(s->dev->dindex, xb_jit_shape_key(s->h_plan, format), s->sm_cap_default);
+}
+
+static bool xb_tune_lookup(xpuB200Session *s, uint32_t format, xb_tune_choice *c)
+{
+    {
+        std::lock_guard<std::mutex> g(g_tune_lock);
+        if (g_tune.empty())
+            return false;
+    }
+    const auto key = xb_tune_key(s, format);
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+        *c = it->second;
+        return true;
+    }
+    auto im = g_tune_minb.find(std::make_pair(std::get<0>(key), std::get<1>(key)));
+    if (im == g_tune_minb.end())
+        return false;
+    c->minb = im->second;
+    c->sm_cap = s->sm_cap;
+    return true;
+}
+
 /* the session-specialised kernel of this format (nullptr: use the
  * interpreter), built on first use; session lock held */
 static void *xb_session_jit(xpuB200Session *s, uint32_t format)
 {
     if (!s->jit_enabled || format >= 256)
         return nullptr;
+    if (!s->tune_looked_up) {
+        /* a launch shape tuned for this plan shape by another session */
+        s->tune_looked_up = true;
+        xb_tune_choice c;
+        if (xb_tune_lookup(s, format, &c)) {
+            s->jit_minb = c.minb;
+            if (c.sm_cap != s->sm_cap && xb_set_sm_cap(s, c.sm_cap) != 0)
+                xb_set_sm_cap(s, s->sm_cap_default);
+        }
+    }
     if (!s->jit_tried[format]) {
         s->jit_tried[format] = true;
         char msg[1024];
         double ms = 0.0;
         int per_sm = 0, mix_sm = 0;
-        if (xb_jit_compile(s->h_plan, format, s->dev->dindex, &s->jit_fn[format], &s->jit_mixfn[format],
-                           &ms, msg, sizeof(msg)) != 0) {
+        if (xb_jit_compile_minb(s->h_plan, format, s->dev->dindex, s->jit_minb, &s->jit_fn[format],
+                                &s->jit_mixfn[format], &ms, msg, sizeof(msg)) != 0) {
             s->jit_fn[format] = nullptr;
             s->jit_mixfn[format] = nullptr;
             s->jit_msg = msg;
@@ -3004,6 +3080,132 @@ xpuB200BatchTime(xpuB200Batch *b, int niters, double *p_msec, kern_errorbuf *err
         total += ms;
     }
     *p_msec = niters > 0 ? total / niters : 0.0;
+    return 0;
+}
+
+/* the session's group table and statistics back to their state after
+ * OpenSession; session lock held */
+static void xb_reset_groups(xpuB200Session *s)
+{
+    cudaStream_t st = s->stream;
+    if (s->h_plan->has_groupby) {
+        cudaMemsetAsync(s->h_gt.entries, 0, (s->h_gt.cap_mask + 1) * s->h_plan->gent_size, st);
+        s->h_gt.nused = 0;
+        s->h_gt.arena_used = 0;
+        s->h_gt.overflow = 0;
+        cudaMemcpyAsync(s->d_gt, &s->h_gt, sizeof(xb_gtable), cudaMemcpyHostToDevice, st);
+    }
+    cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st);
+    cudaStreamSynchronize(st);
+    s->total_raw = s->total_in = s->total_out = 0;
+    for (uint32_t d = 0; d <= XB_MAX_DEPTH; d++)
+        s->total_depth[d] = 0;
+}
+
+extern "C" int
+xpuB200BatchTune(xpuB200Batch *b, uint32_t flags, char *report, size_t report_len, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!b || flags != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid BatchTune arguments");
+    xpuB200Session *s = b->sess;
+    xb_sched_drain_session(s);
+    std::lock_guard<std::mutex> g(s->lock);
+    if (s->total_raw != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "tune a session before it executes chunks");
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    s->tune_looked_up = true;               /* measured here, not adopted */
+    const xb_plan *plan = s->h_plan;
+    const uint32_t fmt = b->format;
+    cudaStream_t st = s->stream;
+    bool gid = false;
+    for (uint32_t d = 1; d <= plan->nrels; d++)
+        gid |= plan->inner[d].gid_on != 0;
+    const uint32_t sm0 = s->sm_cap_default;
+    /* group ids index the shared table directly: its size is then fixed */
+    std::vector<uint32_t> sms;
+    if (!gid && plan->has_groupby && sm0 > 0) {
+        if ((size_t)sm0 * 2 * plan->gent_size <= 48 * 1024)
+            sms.push_back(sm0 * 2);
+        sms.push_back(0);
+    }
+    std::vector<int> minbs;
+    if (s->jit_enabled)
+        minbs = {2, 3, 4, 6, 8};
+    else
+        minbs = {0};
+    struct cand { int minb; uint32_t sm; double ms; const char *kernel; };
+    std::vector<cand> done;
+    int rc = 0;
+    auto measure = [&](int minb, uint32_t smc) -> int {
+        s->jit_minb = minb;
+        if (xb_set_sm_cap(s, smc) != 0)
+            return 1;                       /* does not fit: skipped */
+        double best = 1e30;
+        for (int r = 0; r < 3 && rc == 0; r++) {      /* the first run builds and warms */
+            xb_reset_groups(s);
+            cudaEventRecord(s->ev0, st);
+            rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, fmt, err);
+            if (rc) break;
+            cudaEventRecord(s->ev1, st);
+            rc = xb_wait_status(s, err);
+            if (rc) break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+            if (r > 0 && ms < best) best = ms;
+        }
+        if (rc)
+            return -1;
+        if (minb > 0 && !s->jit_fn[fmt])
+            return 1;                       /* the specialised kernel was not built */
+        done.push_back({minb, smc, best, s->jit_fn[fmt] ? "jit" : "vm"});
+        return 0;
+    };
+    /* coordinate search: CTAs per SM at the default table, then the table */
+    for (int m : minbs)
+        if (measure(m, sm0) < 0) break;
+    if (rc == 0 && !done.empty()) {
+        int bm = done[0].minb;
+        double bt = done[0].ms;
+        for (const cand &c : done)
+            if (c.ms < bt) { bt = c.ms; bm = c.minb; }
+        for (uint32_t c : sms)
+            if (measure(bm, c) < 0) break;
+    }
+    cand best = {0, sm0, 0.0, "none"};
+    if (rc == 0 && !done.empty()) {
+        best = done[0];
+        for (const cand &c : done)
+            if (c.ms < best.ms) best = c;
+    }
+    s->jit_minb = best.minb;
+    if (xb_set_sm_cap(s, best.sm) != 0)
+        xb_set_sm_cap(s, sm0);
+    xb_reset_groups(s);
+    s->tune_looked_up = true;
+    if (rc)
+        return rc;
+    if (done.empty())
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "no launch shape could be measured");
+    {
+        const auto key = xb_tune_key(s, fmt);
+        std::lock_guard<std::mutex> tg(g_tune_lock);
+        g_tune[key] = xb_tune_choice{best.minb, best.sm};
+        g_tune_minb[std::make_pair(std::get<0>(key), std::get<1>(key))] = best.minb;
+    }
+    if (report && report_len) {
+        std::string r = "{\"format\": \"" + std::string(1, (char)fmt) + "\", \"candidates\": [";
+        char buf[256];
+        for (size_t i = 0; i < done.size(); i++) {
+            snprintf(buf, sizeof(buf), "%s{\"ctas_per_sm\": %d, \"sm_groups\": %u, \"kernel\": \"%s\", \"ms\": %.4f}",
+                     i ? ", " : "", done[i].minb, done[i].sm, done[i].kernel, done[i].ms);
+            r += buf;
+        }
+        snprintf(buf, sizeof(buf), "], \"best\": {\"ctas_per_sm\": %d, \"sm_groups\": %u, \"ms\": %.4f}, "
+                 "\"default_sm_groups\": %u}", best.minb, best.sm, best.ms, sm0);
+        r += buf;
+        snprintf(report, report_len, "%s", r.c_str());
+    }
     return 0;
 }
 
@@ -4001,11 +4203,13 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
              "{\"nregs\": %u, \"nslots\": %u, \"nrels\": %u, \"ninsns\": %u, \"has_groupby\": %u, "
              "\"nkeys\": %u, \"naggs\": %u, \"gent_size\": %u, \"gtable_cap\": %llu, "
              "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u], "
-             "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\"}",
+             "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\", "
+             "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u}",
              p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
              p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
              s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash,
-             s->jit_enabled ? "true" : "false", kinds.c_str(), s->jit_compile_ms, msg.c_str());
+             s->jit_enabled ? "true" : "false", kinds.c_str(), s->jit_compile_ms, msg.c_str(),
+             s->jit_minb, s->sm_cap_default);
     return 0;
 }
 

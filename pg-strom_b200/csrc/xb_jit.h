@@ -35,6 +35,15 @@ int xb_jit_source(const xb_plan *plan, uint32_t format, char *buf, size_t bufsz,
 int xb_jit_compile(const xb_plan *plan, uint32_t format, int dindex,
                    void **p_func, void **p_mixfn, double *p_compile_ms, char *errbuf, size_t errlen);
 
+/* xb_jit_compile for kernels bounded to min_blocks resident CTAs of 256
+ * threads per SM (1..8; 0: the default) */
+int xb_jit_compile_minb(const xb_plan *plan, uint32_t format, int dindex, int min_blocks,
+                        void **p_func, void **p_mixfn, double *p_compile_ms, char *errbuf, size_t errlen);
+
+/* a key naming the plan shape of plan + format: sessions whose specialised
+ * kernels differ only in their launch bounds share it */
+uint64_t xb_jit_shape_key(const xb_plan *plan, uint32_t format);
+
 /* compile only (no device needed): cubin size and NVRTC milliseconds */
 int xb_jit_check(const xb_plan *plan, uint32_t format, uint64_t *p_cubin_bytes, double *p_compile_ms,
                  char *errbuf, size_t errlen);

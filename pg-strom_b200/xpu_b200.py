@@ -58,6 +58,7 @@ def lib():
         L.xpuB200BatchCreate.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(P), EB]
         L.xpuB200BatchExec.argtypes = [P, P, EB]
         L.xpuB200BatchTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
+        L.xpuB200BatchTune.argtypes = [P, ctypes.c_uint32, ctypes.c_char_p, U64, EB]
         L.xpuB200BatchDestroy.argtypes = [P]
         L.xpuB200Submit.argtypes = [P, P, I, ctypes.POINTER(U64), EB]
         L.xpuB200Poll.argtypes = [P, U64, I, ctypes.POINTER(I), P, EB]
@@ -294,6 +295,17 @@ class Batch:
         if rc:
             raise XpuB200Error(rc, e)
         return ms.value
+
+    def tune(self):
+        """Measure the session's launch shapes on this batch and keep the
+        fastest (xpuB200BatchTune); returns the report (a dict)."""
+        import json
+        b = ctypes.create_string_buffer(8192)
+        e = KernErrorbuf()
+        rc = lib().xpuB200BatchTune(self.h, 0, b, 8192, ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return json.loads(b.value.decode())
 
     def close(self):
         if self.h:
