@@ -40,6 +40,35 @@ __device__ __forceinline__ void xb_red_shared_add_u32(void *p, uint32_t v)
     asm volatile("red.shared.add.u32 [%0], %1;" :: "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
 }
 
+/* reductions on global memory given by a generic address that is known to
+ * be global: fire-and-forget (red), so the issuing warp does not wait for
+ * the L2 round trip as it does for an atomic whose old value it may use
+ * (a generic-address atomic is issued as one) */
+__device__ __forceinline__ void xb_red_g_add_u64(void *p, unsigned long long v)
+{
+    asm volatile("red.global.add.u64 [%0], %1;" :: "l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void xb_red_g_or_u32(void *p, uint32_t v)
+{
+    asm volatile("red.global.or.b32 [%0], %1;" :: "l"(__cvta_generic_to_global(p)), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void xb_red_g_min_s64(void *p, long long v)
+{
+    asm volatile("red.global.min.s64 [%0], %1;" :: "l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void xb_red_g_max_s64(void *p, long long v)
+{
+    asm volatile("red.global.max.s64 [%0], %1;" :: "l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void xb_red_g_add_f64(void *p, double v)
+{
+    asm volatile("red.global.add.f64 [%0], %1;" :: "l"(__cvta_generic_to_global(p)), "d"(v) : "memory");
+}
+
 /* add to a little-endian multi-word integer in shared memory (generic
  * address) with native 32-bit shared atomics: each word is added with the
  * carry of the word below, and a carry out of a word is added to the next;
@@ -118,6 +147,29 @@ __device__ __forceinline__ void xb_atomic_add_f64c(double *hi, double *lo, doubl
     double e = __dadd_rn(__dsub_rn(old, __dsub_rn(s, bp)), __dsub_rn(x, bp));
     if (e != 0.0)
         atomicAdd(lo, e);
+}
+
+/* the same two for state in global memory: only the additions whose old
+ * value is needed wait for it */
+__device__ __forceinline__ void xb_atomic_add_i128_g(uint64_t *p, xb_i128 v)
+{
+    uint64_t lo = (uint64_t)v;
+    uint64_t hi = (uint64_t)((unsigned __int128)v >> 64);
+    uint64_t old = atomicAdd((unsigned long long *)&p[0], (unsigned long long)lo);
+    if (old + lo < old)
+        hi += 1;
+    if (hi)
+        xb_red_g_add_u64(&p[1], hi);
+}
+
+__device__ __forceinline__ void xb_atomic_add_f64c_g(double *hi, double *lo, double x)
+{
+    double old = atomicAdd(hi, x);
+    double s = __dadd_rn(old, x);
+    double bp = __dsub_rn(s, old);
+    double e = __dadd_rn(__dsub_rn(old, __dsub_rn(s, bp)), __dsub_rn(x, bp));
+    if (e != 0.0)
+        xb_red_g_add_f64(lo, e);
 }
 
 __device__ __forceinline__ double xb_reg_f64(uint64_t v, int rk)
