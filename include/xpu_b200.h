@@ -264,10 +264,35 @@ int  xpuB200BatchTune(xpuB200Batch *batch, uint32_t flags, char *report, size_t 
                       kern_errorbuf *err);
 void xpuB200BatchDestroy(xpuB200Batch *batch);
 
+/*
+ * Pinned inner buffers: rows that a scan projected into a KDS_FORMAT_HASH
+ * kds_dst (a session whose Projection carries a hash value, u.proj.hash)
+ * are appended into one KDS_FORMAT_HASH buffer on the device and chained
+ * into its hash slots, ready to be the inner relation of a join.  Both
+ * buffers are device memory of this GPU.  kds_dst: a KDS_FORMAT_HASH
+ * header with its length, hash_nslots, nitems and usage (0 and 0 when
+ * empty; every call appends), the hash slots zeroed before the first call.
+ * kds_src: KDS_FORMAT_HASH or KDS_FORMAT_ROW whose tuples carry their
+ * hash, with the same columns.  hash_divisor >= 2 appends only the rows
+ * with hash % hash_divisor == hash_remainder (one partition of the inner
+ * relation, for a join whose inner side is split across GPUs); 0 appends
+ * every row.  *p_required (if not NULL) receives the bytes kds_dst's rows
+ * take; when they do not fit, ERRCODE_SUSPEND_NO_SPACE is returned and
+ * kds_dst must be rebuilt larger.  Row order is not deterministic (rows
+ * are claimed concurrently), as in the reference.
+ * Replaces kern_buffer_reconstruction (cuda_gpujoin.cu:18-71) and
+ * kern_buffer_partitioning (cuda_gpujoin.cu:76-138), launched by the GPU
+ * service's pinned inner-buffer setup (gpu_service.c:1748-2197).
+ */
+int  xpuB200InnerRebuild(xpuB200Device *dev, kern_data_store *kds_dst, const kern_data_store *kds_src,
+                         uint32_t hash_divisor, uint32_t hash_remainder, uint64_t *p_required,
+                         kern_errorbuf *err);
+
 /* Device memory helpers for callers that keep chunks resident in HBM. */
 int  xpuB200DeviceAlloc(xpuB200Device *dev, uint64_t sz, void **p_dptr);
 int  xpuB200DeviceFree(xpuB200Device *dev, void *dptr);
 int  xpuB200CopyToDevice(xpuB200Device *dev, void *dptr, const void *src, uint64_t sz);
+int  xpuB200CopyToHost(xpuB200Device *dev, void *dst, const void *dptr, uint64_t sz);
 
 /*
  * Time one ExecTask over a device-resident chunk 'niters' times with CUDA

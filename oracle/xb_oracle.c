@@ -813,6 +813,14 @@ static int proj_row(xo_sess *s)
         xo_datum d;
         if (!eval(s, a, &d)) return 0;
     }
+    /* rows bound for a pinned inner buffer carry their hash value
+     * (execGpuJoinProjection, cuda_gpujoin.cu:797-823) */
+    uint32_t hash = 0;
+    if (kp->u.proj.hash != 0) {
+        xo_datum h;
+        if (!eval(s, (const kern_expression *)((const char *)kp + kp->u.proj.hash), &h)) return 0;
+        hash = (uint32_t)h.i;
+    }
     int nattrs = kp->u.proj.nattrs;
     if (nattrs > (int)s->kds_dst_head->ncols) nattrs = s->kds_dst_head->ncols;
     uint32_t tl = proj_form(s, nattrs, NULL, 0);
@@ -825,6 +833,7 @@ static int proj_row(xo_sess *s)
     }
     memset(s->proj_buf + s->proj_len, 0, need);
     proj_form(s, nattrs, s->proj_buf + s->proj_len, (uint32_t)s->proj_nrows);
+    ((kern_tupitem *)(s->proj_buf + s->proj_len))->hash = hash;
     s->proj_len += need;
     s->proj_nrows++;
     s->proj_usage += PGSTROM_MAXALIGN(PGSTROM_MAXALIGN(tl) + s->session->gpusort_htup_margin);

@@ -687,8 +687,6 @@ struct Compiler {
         if (nattrs < 1 || nattrs > XB_MAX_PROJ ||
             offsetof(kern_expression, u.proj.slot_id) + sizeof(uint16_t) * nattrs > kp->len)
             return fail("Projection has %d attributes (max %d)", nattrs, XB_MAX_PROJ);
-        if (kp->u.proj.hash != 0)
-            return fail("Projection with a hash value (pinned inner buffer) is not supported");
         /* argument programs: SaveExpr into slots; VarExpr needs nothing */
         plan->proj_args.start = (uint16_t)plan->ninsns;
         plan->proj_args.count = 0;
@@ -707,6 +705,21 @@ struct Compiler {
                 karg = next_arg(kp, karg);
         }
         plan->proj_args.count = (uint16_t)(plan->ninsns - plan->proj_args.start);
+        /* the hash value of a row bound for a pinned inner buffer
+         * (execGpuJoinProjection, cuda_gpujoin.cu:797-823) */
+        plan->proj_hashed = 0;
+        if (kp->u.proj.hash != 0) {
+            const kern_expression *kh = (const kern_expression *)((const char *)kp + kp->u.proj.hash);
+            if (kp->u.proj.hash + offsetof(kern_expression, u) > kp->len || kh->len < offsetof(kern_expression, u) ||
+                kp->u.proj.hash + kh->len > kp->len || kh->opcode != FuncOpCode__HashValue)
+                return fail("malformed Projection hash value");
+            if (!program(kh, &plan->proj_hash, false))
+                return false;
+            plan->proj_hashed = 1;
+        }
+        plan->proj_all.start = plan->proj_args.start;
+        plan->proj_all.count = (uint16_t)(plan->ninsns - plan->proj_args.start);
+        plan->proj_all.result = -1;
         if ((uint32_t)ntemps > plan->nregs)
             plan->nregs = ntemps;
         /* the destination header */
@@ -714,11 +727,13 @@ struct Compiler {
         if (off == 0 || off + sizeof(kern_data_store) > session_sz)
             return fail("projection without a kds_dst header");
         const kern_data_store *kd = (const kern_data_store *)((const char *)session + off);
-        if (kd->format != KDS_FORMAT_ROW)
-            return fail("projection into KDS format '%c' is not supported", kd->format);
+        if (kd->format != (plan->proj_hashed ? KDS_FORMAT_HASH : KDS_FORMAT_ROW))
+            return fail("projection into KDS format '%c' is not supported%s", kd->format,
+                        plan->proj_hashed ? " (a hashed projection writes KDS_FORMAT_HASH)" : "");
         const uint64_t hl = KDS_HEAD_LENGTH(kd);
-        if (off + hl > session_sz || kd->hash_nslots != 0)
+        if (off + hl > session_sz || (plan->proj_hashed ? kd->hash_nslots == 0 : kd->hash_nslots != 0))
             return fail("projection kds_dst header is broken");
+        plan->proj_nslots = kd->hash_nslots;
         /* attributes past kds_dst's columns are not written (as in
          * __kern_form_minimal_tuple, xpu_common.cu:1113-1114) */
         const int nout = (int)kd->ncols < nattrs ? (int)kd->ncols : nattrs;
@@ -747,7 +762,9 @@ struct Compiler {
         }
         plan->proj_nattrs = (uint32_t)nout;
         plan->proj_margin = session->gpusort_htup_margin;
-        plan->proj_head_len = (uint32_t)hl;
+        /* a hashed kds_dst keeps its hash slots between the header and the
+         * row index */
+        plan->proj_head_len = (uint32_t)(hl + (plan->proj_hashed ? 8ULL * kd->hash_nslots : 0));
         plan->has_proj = 1;
         return true;
     }
@@ -1028,6 +1045,7 @@ struct Compiler {
         reads_of(plan->gb_args, &later);
         reads_of(plan->gb_keyhash, &later);
         reads_of(plan->proj_args, &later);
+        reads_of(plan->proj_hash, &later);
         for (uint32_t j = 0; plan->has_proj && j < plan->proj_nattrs; j++)
             later |= 1ULL << plan->proj[j].reg;
         for (uint32_t j = 0; j < plan->naggs; j++)

@@ -637,7 +637,7 @@ xb_exec_body(const XbExecArgs &args, char *smem)
                     stage = nrels ? XB_ST_PROBE : XB_ST_FETCH;
                     continue;
                 }
-                prog = plan->has_proj ? &plan->proj_args : &plan->gb_all;
+                prog = plan->has_proj ? &plan->proj_all : &plan->gb_all;
             } else {
                 const xb_inner *in = &plan->inner[d];
                 if (in->fast_key >= 0) {
@@ -687,8 +687,9 @@ xb_exec_body(const XbExecArgs &args, char *smem)
                     if (RISNULL(R, r))
                         pn |= 1u << j;
                 }
+                const uint32_t ph = plan->proj_hashed ? (uint32_t)RVAL(R, plan->proj_hash.result) : 0;
                 if ((mask >> lane) & 1u)
-                    xb_proj_emit(plan, args.dst, args.dst_len, pv, pa, pn, st);
+                    xb_proj_emit(plan, args.dst, args.dst_len, pv, pa, pn, ph, st);
                 __syncwarp();
                 d = nrels;
                 stage = nrels ? XB_ST_PROBE : XB_ST_FETCH;
@@ -1554,6 +1555,91 @@ xb_merge_final(XbMergeArgs args)
             XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
             atomicOr(&args.gt->overflow, 1u);
         }
+    }
+}
+
+/* ----------------------------------------------------------------
+ * inner-buffer rebuild: rows of a hashed projection (or any HASH / ROW
+ * chunk whose tuples carry their hash) appended into a KDS_FORMAT_HASH
+ * buffer and chained into its hash slots (kern_buffer_reconstruction,
+ * cuda_gpujoin.cu:18-71); with a divisor, only the rows whose hash falls
+ * into one partition (kern_buffer_partitioning, cuda_gpujoin.cu:76-138)
+ * ---------------------------------------------------------------- */
+struct XbRebuildArgs {
+    kern_data_store        *dst;
+    const kern_data_store  *src;
+    uint64_t                dst_head;   /* KDS_HEAD_LENGTH(dst) */
+    uint64_t                src_rowidx; /* offset of src's row index */
+    uint32_t                divisor;    /* 0: every row */
+    uint32_t                remainder;
+    uint32_t               *overflow;
+};
+
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_inner_rebuild(XbRebuildArgs args)
+{
+    kern_data_store *dst = args.dst;
+    const kern_data_store *src = args.src;
+    const uint64_t *rowidx = (const uint64_t *)((const char *)src + args.src_rowidx);
+    const uint32_t nslots = dst->hash_nslots;
+    uint64_t *slots = (uint64_t *)((char *)dst + args.dst_head);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t n = src->nitems;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const kern_tupitem *t = nullptr;
+        uint32_t sz = 0;
+        if (i < n) {
+            const uint64_t off = rowidx[i];
+            if (off < sizeof(kern_tupitem) || off > src->length - args.src_rowidx || (off & 7) != 0) {
+                atomicOr(args.overflow, 2u);            /* a broken row index */
+            } else {
+                t = (const kern_tupitem *)((const char *)src + src->length - off);
+                const uint32_t t_len = t->t_len;
+                if (t_len < offsetof(kern_tupitem, t_bits) || t_len > off)
+                    atomicOr(args.overflow, 2u);
+                else if (args.divisor < 2 || t->hash % args.divisor == args.remainder)
+                    sz = (uint32_t)PGSTROM_MAXALIGN(offsetof(kern_hashitem, t) + t_len);
+            }
+        }
+        /* one claim of row ids and bytes per warp */
+        const uint32_t want = __ballot_sync(XB_FULL, sz > 0);
+        uint32_t incl = sz;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(XB_FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(XB_FULL, incl, 31);
+        unsigned long long bu = 0;
+        uint32_t bn = 0;
+        if (lane == 0 && want) {
+            bn = atomicAdd(&dst->nitems, (uint32_t)__popc(want));
+            bu = atomicAdd((unsigned long long *)&dst->usage, (unsigned long long)total);
+        }
+        bn = __shfl_sync(XB_FULL, bn, 0);
+        bu = __shfl_sync(XB_FULL, bu, 0);
+        if (!sz)
+            continue;
+        const uint32_t row_id = bn + __popc(want & ((1u << lane) - 1));
+        const uint64_t offset = bu + incl;              /* from the end to the item */
+        const uint64_t need = args.dst_head + 8ULL * nslots + 8ULL * ((uint64_t)row_id + 1);
+        if (offset > dst->length || dst->length - offset < need) {
+            atomicOr(args.overflow, 1u);
+            continue;
+        }
+        char *item = (char *)dst + dst->length - offset;
+        /* the tuple in 8-byte words: both items are MAXALIGN'd and sized */
+        const uint32_t t_len = t->t_len;
+        const uint64_t *sw = (const uint64_t *)t;
+        uint64_t *dw = (uint64_t *)(item + offsetof(kern_hashitem, t));
+        for (uint32_t k = 0; k < (t_len + 7) / 8; k++)
+            dw[k] = sw[k];
+        xb_store(item + offsetof(kern_hashitem, t) + t_len - ROWID_SIZE, &row_id, 4);
+        const uint32_t hash = t->hash;
+        *(uint64_t *)item = atomicExch((unsigned long long *)&slots[hash % nslots], (unsigned long long)offset);
+        uint64_t *dri = (uint64_t *)((char *)dst + args.dst_head) + nslots;
+        dri[row_id] = offset - offsetof(kern_hashitem, t);
     }
 }
 
@@ -2544,6 +2630,9 @@ xpuB200ExecTaskDst(xpuB200Session *s, const kern_data_store *kds_src, int kds_sr
         d_dst = s->d_dst;
     }
     XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+    const uint64_t hl0 = KDS_HEAD_LENGTH(tmpl);     /* hash slots follow, when hashed */
+    if (plan->proj_hashed)
+        XB_CUDA(cudaMemsetAsync(d_dst + hl0, 0, head_len - hl0, st), err);
     s->launch_dst = d_dst;
     s->launch_dst_len = len;
     rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
@@ -2560,19 +2649,22 @@ xpuB200ExecTaskDst(xpuB200Session *s, const kern_data_store *kds_src, int kds_sr
     if (hs->proj_overflow)
         return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE, "kds_dst needs %llu bytes (buffer %llu)",
                       (unsigned long long)required, (unsigned long long)len);
-    /* the header: the session's kds_dst definition with this chunk's rows */
-    std::vector<char> hd((const char *)tmpl, (const char *)tmpl + head_len);
+    /* the header: the session's kds_dst definition with this chunk's rows
+     * (a hashed kds_dst keeps the hash slots the kernel chained) */
+    std::vector<char> hd((const char *)tmpl, (const char *)tmpl + hl0);
     kern_data_store *kh = (kern_data_store *)hd.data();
     kh->length = len;
     kh->nitems = (uint32_t)nitems;
     kh->usage = usage;
-    kh->format = KDS_FORMAT_ROW;
-    kh->hash_nslots = 0;
+    kh->format = plan->proj_hashed ? KDS_FORMAT_HASH : KDS_FORMAT_ROW;
+    kh->hash_nslots = plan->proj_hashed ? plan->proj_nslots : 0;
     if (kds_dst_on_device) {
-        XB_CUDA(cudaMemcpyAsync(d_dst, hd.data(), head_len, cudaMemcpyHostToDevice, st), err);
+        XB_CUDA(cudaMemcpyAsync(d_dst, hd.data(), hl0, cudaMemcpyHostToDevice, st), err);
     } else {
         char *h = (char *)kds_dst;
-        memcpy(h, hd.data(), head_len);
+        memcpy(h, hd.data(), hl0);
+        if (head_len > hl0)
+            XB_CUDA(cudaMemcpyAsync(h + hl0, d_dst + hl0, head_len - hl0, cudaMemcpyDeviceToHost, st), err);
         if (nitems)
             XB_CUDA(cudaMemcpyAsync(h + head_len, d_dst + head_len, 8 * nitems, cudaMemcpyDeviceToHost, st), err);
         if (usage)
@@ -4113,7 +4205,9 @@ xpuB200HandleCommand(xpuB200Device *dev, xpuB200Session **p_sess, const XpuComma
             }
             if (rc) break;
             kern_data_store *kd = (kern_data_store *)dst;
-            const uint64_t hsz = KDS_HEAD_LENGTH(kd) + PGSTROM_MAXALIGN(8 * (uint64_t)kd->nitems);
+            /* offsets from the end (row index, hash chains) stay valid */
+            const uint64_t hsz = KDS_HEAD_LENGTH(kd) + 8 * (uint64_t)kd->hash_nslots +
+                                 PGSTROM_MAXALIGN(8 * (uint64_t)kd->nitems);
             if (kd->usage)
                 memmove(dst + hsz, dst + len - kd->usage, kd->usage);
             kd->length = hsz + kd->usage;
@@ -4178,10 +4272,90 @@ xpuB200DeviceFree(xpuB200Device *dev, void *dptr)
 }
 
 extern "C" int
+xpuB200InnerRebuild(xpuB200Device *dev, kern_data_store *kds_dst, const kern_data_store *kds_src,
+                    uint32_t hash_divisor, uint32_t hash_remainder, uint64_t *p_required, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!dev || !kds_dst || !kds_src || (hash_divisor >= 2 && hash_remainder >= hash_divisor))
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid InnerRebuild arguments");
+    if (((uintptr_t)kds_dst & 7) != 0 || ((uintptr_t)kds_src & 7) != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "InnerRebuild buffers must be 8-byte aligned");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    kern_data_store hd, hs;
+    XB_CUDA(cudaMemcpy(&hd, kds_dst, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+    XB_CUDA(cudaMemcpy(&hs, kds_src, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
+    if (hd.format != KDS_FORMAT_HASH || hd.hash_nslots == 0 || hd.nr_colmeta > 4096 ||
+        (hd.length & 7) != 0 || (hd.usage & 7) != 0 ||
+        KDS_HEAD_LENGTH(&hd) + 8ULL * ((uint64_t)hd.hash_nslots + hd.nitems) + hd.usage > hd.length)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "InnerRebuild destination is not a KDS_FORMAT_HASH buffer");
+    if ((hs.format != KDS_FORMAT_HASH && hs.format != KDS_FORMAT_ROW) || hs.nr_colmeta > 4096 ||
+        (hs.length & 7) != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "InnerRebuild source must be KDS_FORMAT_HASH or _ROW");
+    if (hd.ncols != hs.ncols)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "InnerRebuild source has %u columns, destination %u",
+                      hs.ncols, hd.ncols);
+    const uint64_t src_rowidx = KDS_HEAD_LENGTH(&hs) + (hs.format == KDS_FORMAT_HASH ? 8ULL * hs.hash_nslots : 0);
+    if (src_rowidx + 8ULL * hs.nitems > hs.length)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "InnerRebuild source row index is out of the buffer");
+    if (hs.nitems == 0) {
+        if (p_required)
+            *p_required = KDS_HEAD_LENGTH(&hd) + 8ULL * (hd.hash_nslots + hd.nitems) + hd.usage;
+        return 0;
+    }
+    cudaStream_t st = xb_get_stream(dev);
+    if (!st)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "no stream");
+    uint32_t *d_flag = nullptr;
+    int rc = 0;
+    if (cudaMallocAsync((void **)&d_flag, sizeof(uint32_t), st) != cudaSuccess) {
+        xb_put_stream(dev, st);
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory");
+    }
+    cudaMemsetAsync(d_flag, 0, sizeof(uint32_t), st);
+    XbRebuildArgs ra;
+    ra.dst = kds_dst;
+    ra.src = kds_src;
+    ra.dst_head = KDS_HEAD_LENGTH(&hd);
+    ra.src_rowidx = src_rowidx;
+    ra.divisor = hash_divisor;
+    ra.remainder = hash_remainder;
+    ra.overflow = d_flag;
+    int grid = (int)((hs.nitems + XB_BLOCK - 1) / XB_BLOCK);
+    if (grid > dev->nsm * 8) grid = dev->nsm * 8;
+    xb_inner_rebuild<<<grid, XB_BLOCK, 0, st>>>(ra);
+    uint32_t flag = 0;
+    cudaMemcpyAsync(&flag, d_flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&hd, kds_dst, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d_flag, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "InnerRebuild: %s", cudaGetErrorString(cudaGetLastError()));
+    xb_put_stream(dev, st);
+    if (rc)
+        return rc;
+    const uint64_t required = KDS_HEAD_LENGTH(&hd) + 8ULL * (hd.hash_nslots + hd.nitems) + hd.usage;
+    if (p_required)
+        *p_required = required;
+    if (flag & 2u)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "InnerRebuild source has a broken row");
+    /* rows claimed concurrently fit only when all of them do */
+    if ((flag & 1u) || required > hd.length)
+        return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE, "InnerRebuild destination needs %llu bytes (buffer %llu)",
+                      (unsigned long long)required, (unsigned long long)hd.length);
+    return 0;
+}
+
+extern "C" int
 xpuB200CopyToDevice(xpuB200Device *dev, void *dptr, const void *src, uint64_t sz)
 {
     cudaSetDevice(dev->dindex);
     return cudaMemcpy(dptr, src, sz, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : ERRCODE_DEVICE_FATAL;
+}
+
+extern "C" int
+xpuB200CopyToHost(xpuB200Device *dev, void *dst, const void *dptr, uint64_t sz)
+{
+    cudaSetDevice(dev->dindex);
+    return cudaMemcpy(dst, dptr, sz, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : ERRCODE_DEVICE_FATAL;
 }
 
 extern "C" int

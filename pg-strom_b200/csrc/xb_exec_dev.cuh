@@ -1042,10 +1042,13 @@ xb_proj_index(char *dst, uint64_t dst_len, uint64_t head, uint32_t rowid, const 
 }
 
 /* interpreter: form and write one row whose attribute j is vals[j] /
- * auxs[j], NULL when bit j of nulls is set */
+ * auxs[j], NULL when bit j of nulls is set.  Into a hashed kds_dst (a
+ * pinned inner buffer) the row is a kern_hashitem: its tuple carries the
+ * row's hash value and the item is chained into the hash slot
+ * (execGpuJoinProjection, cuda_gpujoin.cu:897-915) */
 __device__ __forceinline__ void
 xb_proj_emit(const xb_plan *plan, char *dst, uint64_t dst_len,
-             const uint64_t *vals, const uint32_t *auxs, uint32_t nulls, xb_status *st)
+             const uint64_t *vals, const uint32_t *auxs, uint32_t nulls, uint32_t hash, xb_status *st)
 {
     const uint32_t n = plan->proj_nattrs;
     const uint32_t hoff = xb_proj_hoff(n, nulls != 0);
@@ -1056,16 +1059,27 @@ xb_proj_emit(const xb_plan *plan, char *dst, uint64_t dst_len,
             t = xb_proj_attr(nullptr, t, plan->proj[j].attalign, plan->proj[j].ld, vals[j], auxs[j], im);
     const uint32_t t_len = t + ROWID_SIZE;
     const uint64_t head = plan->proj_head_len;
+    const uint32_t item = plan->proj_hashed ? (uint32_t)offsetof(kern_hashitem, t) : 0;
     uint32_t rowid;
-    char *tp = xb_proj_claim(dst, dst_len, head, xb_proj_rowsz(t_len, plan->proj_margin), st, &rowid);
-    if (!tp)
+    char *ip = xb_proj_claim(dst, dst_len, head, item + xb_proj_rowsz(t_len, plan->proj_margin), st, &rowid);
+    if (!ip)
         return;
+    char *tp = ip + item;
     xb_proj_head(tp, n, hoff, nulls);
+    if (item)
+        xb_store(tp + offsetof(kern_tupitem, hash), &hash, 4);
     t = hoff;
     for (uint32_t j = 0; j < n; j++)
         if (!((nulls >> j) & 1u))
             t = xb_proj_attr(tp, t, plan->proj[j].attalign, plan->proj[j].ld, vals[j], auxs[j], im);
     xb_proj_tail(tp, t_len, im, rowid);
+    if (item) {
+        uint64_t *slots = (uint64_t *)(dst + head) - plan->proj_nslots;
+        const unsigned long long next =
+            atomicExch((unsigned long long *)&slots[hash % plan->proj_nslots],
+                       (unsigned long long)(dst + dst_len - ip));
+        *(uint64_t *)ip = next;
+    }
     xb_proj_index(dst, dst_len, head, rowid, tp);
 }
 

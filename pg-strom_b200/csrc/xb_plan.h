@@ -268,6 +268,12 @@ typedef struct xb_plan {
     uint32_t    proj_head_len;  /* KDS_HEAD_LENGTH of the kds_dst template */
     xb_prog     proj_args;      /* SaveExpr programs filling the projected slots */
     xb_projcol  proj[XB_MAX_PROJ];
+    /* rows go into a KDS_FORMAT_HASH kds_dst (a pinned inner buffer): the
+     * hash of every row (u.proj.hash) and the destination's hash slots */
+    uint32_t    proj_hashed;
+    uint32_t    proj_nslots;
+    xb_prog     proj_hash;
+    xb_prog     proj_all;       /* proj_args, then proj_hash: one program */
 
     /* VM code */
     uint32_t    ninsns;

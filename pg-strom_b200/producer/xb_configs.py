@@ -23,6 +23,8 @@ Every generator also returns the expected per-group aggregates computed
 directly from the column arrays with numpy (independent of any page or
 bytecode decoding), so the oracle itself can be pinned against them.
 """
+import struct
+
 import numpy as np
 
 from xb_final import Approx
@@ -259,6 +261,7 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
                           Column("qty", "int4", values=qty), Column("price", "int8", values=price)], nfact)
     kmrels = kern_multirels([dim1.hash_kds(host_join_hash_int4(pk1)),
                              dim2.hash_kds(host_join_hash_int4(pk2))])
+    dims = {"dim1": dim1, "dim2": dim2, "pk1": pk1, "pk2": pk2}
     session = join_groupby_session(flag_limit)
     # expected: every (fact row, dim1 copy) pair that passes both joins
     m = (flag[idx2] < flag_limit) & ~miss
@@ -289,6 +292,7 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
             "depth_out": [hit1, out], "agg_names": ["sum_amount", "nrows"], "nkeys": 1}
     if with_rows:
         meta["rows"] = rows
+    meta["dims"] = dims
     return fact, session, kmrels, expect, meta
 
 
@@ -423,6 +427,26 @@ def join_projection(nfact=60_000, ndim1=3_000, ndim2=400, seed_config=1, flag_li
 
 # ---------------------------------------------------------------------------
 HEAP_ROW_BYTES = 68          # scan_groupby tuple + line pointer, in heap pages
+
+
+def pinned_dim1_session(nslots=8192):
+    """GpuScan of the join's dim1 (pk int4, region text) projecting its
+    rows into a pinned inner buffer: KDS_FORMAT_HASH rows hashed by
+    HashValue(pk), the inner hash of the fact-dim1 join."""
+    pk, region = Var(0, 1, "int4"), Var(0, 2, "text")
+    sb = SessionBuilder(0, DEVTASK_SCAN | DEVKIND_GPU)
+    return sb.build(projection=[pk, region], projection_hash=[pk], proj_nslots=nslots)
+
+
+def empty_hash_kds(table, length, nslots):
+    """An empty KDS_FORMAT_HASH buffer of table's columns: length bytes,
+    nslots zeroed hash slots, no rows."""
+    head = table.kds_header("h", 0)
+    buf = np.zeros(length, dtype=np.uint8)
+    buf[:len(head)] = np.frombuffer(bytes(head), dtype=np.uint8)
+    struct.pack_into("<QQ", buf, 0, length, 0)
+    struct.pack_into("<I", buf, 40, nslots)
+    return buf
 
 
 def mixed_commands(ncmds=256, min_bytes=64 << 10, max_bytes=64 << 20, min_sel=0.001, max_sel=0.9,

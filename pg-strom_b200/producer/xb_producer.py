@@ -838,12 +838,14 @@ class SessionBuilder:
         return bytes(buf.b)
 
     # -- the whole session --
-    def build_projection(self, tlist, depth):
+    def build_projection(self, tlist, depth, hash_keys=None):
         """Projection kexp (codegen_build_projection, codegen.c:3880-3950):
         one SaveExpr per target entry into a kvars slot, skipped when an
         earlier entry already saved into the same slot
         (try_inject_projection_expression, codegen.c:3412-3437);
-        u.proj.slot_id[] names each output attribute's slot."""
+        u.proj.slot_id[] names each output attribute's slot.  hash_keys
+        (rows for a pinned inner buffer) appends a HashValue over them,
+        found at u.proj.hash (codegen.c:3933-3941)."""
         nattrs = len(tlist)
         head_sz = maxalign(48 + 2 * nattrs)
         buf = _Buf()
@@ -857,21 +859,27 @@ class SessionBuilder:
             else:
                 nargs += 1
             slots.append(d.slot)
+        hash_off = 0
+        if hash_keys:
+            hash_off = buf.append_aligned(self.build_hash_value(hash_keys, depth))
         head = _kexp_head(TOP("int4"), FOP("Projection"), nargs, head_sz) + \
-            struct.pack("<Ii", 0, nattrs) + struct.pack("<%dH" % nattrs, *slots)
+            struct.pack("<Ii", hash_off, nattrs) + struct.pack("<%dH" % nattrs, *slots)
         buf.b[:len(head)] = head
         buf.finish_kexp(0)
         return bytes(buf.b)
 
     def build(self, *, scan_quals=None, joins=(), groupby_keys=(), aggs=(),
               ngroups_estimate=100.0, final_tlist=None, projection=None,
-              htup_margin=0) -> bytes:
+              htup_margin=0, projection_hash=None, proj_nslots=0) -> bytes:
         """joins: list of (outer_hash_keys, join_quals, other_quals) for
         depth 1..n.  groupby_keys: list of Expr; aggs: list of Agg.  The
         partial-aggregation target list is aggs then keys (gpu_preagg.c:
         2080-2097).  projection: list of Expr written as KDS_FORMAT_ROW rows
         (a scan/join without GROUP BY); htup_margin is
-        gpusort_htup_margin."""
+        gpusort_htup_margin.  projection_hash: list of Expr whose HashValue
+        every projected row carries, written as kern_hashitems into a
+        KDS_FORMAT_HASH kds_dst of proj_nslots slots (a pinned inner
+        buffer)."""
         nrels = self.nrels
         blobs = {}
         self.htup_margin = htup_margin
@@ -970,10 +978,13 @@ class SessionBuilder:
             buf.finish_kexp(0)
             blobs["actions"] = bytes(buf.b)
         if projection:
-            blobs["projection"] = self.build_projection(projection, gdepth)
+            blobs["projection"] = self.build_projection(projection, gdepth, projection_hash)
             dt = Table("kds_dst", [Column(f"c{i}", e.typ, getattr(e, "typmod", -1))
                                    for i, e in enumerate(projection)], 0)
-            blobs["kds_dst"] = bytes(dt.kds_header("r", 0))
+            kd = dt.kds_header("h" if projection_hash else "r", 0)
+            if projection_hash:
+                struct.pack_into("<I", kd, 40, proj_nslots)     # hash_nslots
+            blobs["kds_dst"] = bytes(kd)
         # LoadVars / MoveVars packed
         lv = {d: self.build_loadvars(d) for d in range(0, nrels + 1)}
         lv = {d: b for d, b in lv.items() if b is not None}

@@ -49,11 +49,13 @@ def lib():
         L.xpuB200ExecTaskDst.argtypes = [P, P, I, P, U64, I, ctypes.POINTER(U64), P, EB]
         L.xpuB200Final.argtypes = [P, P, U64, ctypes.POINTER(U64), P, EB]
         L.xpuB200MergeFinal.argtypes = [P, P, I, EB]
+        L.xpuB200InnerRebuild.argtypes = [P, P, P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(U64), EB]
         L.xpuB200CloseSession.argtypes = [P]
         L.xpuB200HandleCommand.argtypes = [P, ctypes.POINTER(P), P, P, U64, P, U64]
         L.xpuB200DeviceAlloc.argtypes = [P, U64, ctypes.POINTER(P)]
         L.xpuB200DeviceFree.argtypes = [P, P]
         L.xpuB200CopyToDevice.argtypes = [P, P, P, U64]
+        L.xpuB200CopyToHost.argtypes = [P, P, P, U64]
         L.xpuB200TimeExecTask.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_double), EB]
         L.xpuB200BatchCreate.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(P), EB]
         L.xpuB200BatchExec.argtypes = [P, P, EB]
@@ -114,6 +116,26 @@ class Device:
 
     def free(self, dptr):
         lib().xpuB200DeviceFree(self.h, ctypes.c_void_p(dptr))
+
+    def inner_rebuild(self, dst, src, divisor=0, remainder=0):
+        """Append the rows of the device chunk src (HASH or ROW, tuples
+        carrying their hash) into the device KDS_FORMAT_HASH buffer dst
+        (xpuB200InnerRebuild); with divisor >= 2 only the rows whose hash %
+        divisor == remainder.  Returns the bytes dst's rows take."""
+        e = KernErrorbuf()
+        req = ctypes.c_uint64()
+        rc = lib().xpuB200InnerRebuild(self.h, ctypes.c_void_p(dst), ctypes.c_void_p(src), divisor, remainder,
+                                       ctypes.byref(req), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return req.value
+
+    def download(self, dptr, nbytes):
+        """Copy nbytes of device memory at dptr into a new uint8 array."""
+        out = np.zeros(nbytes, dtype=np.uint8)
+        if lib().xpuB200CopyToHost(self.h, _ptr(out), ctypes.c_void_p(dptr), nbytes):
+            raise RuntimeError("download failed")
+        return out
 
     def upload(self, arr: np.ndarray, align_pages=True):
         """Copy a KDS chunk into device memory; heap pages land 16B aligned."""

@@ -97,3 +97,24 @@ def test_specialised_kernel_compiles_for_projection():
     fact, sess2, km, _ = C.join_projection(nfact=1000)
     rc, msg = _compile_ok(sess2, km)
     assert rc == 0, msg
+
+
+def test_oracle_pinned_inner_projection():
+    # a scan of dim1 projecting (pk, region) rows that carry HashValue(pk):
+    # the hash is the join's inner hash, the values the dim1 columns
+    fact, sess, km, expect, meta = C.join_groupby(nfact=1000, ndim1=3000, ndim2=70)
+    dims = meta["dims"]
+    ps = C.pinned_dim1_session(nslots=1024)
+    rows, usage, st = _oracle_rows(ps, dims["dim1"].block_chunks(pages_per_chunk=5))
+    assert len(rows) == 3000
+    cols = _dst_columns(ps)
+    got = {}
+    for img in rows:
+        h, = struct.unpack_from("<I", img, 4)
+        pk, region = RW.decode_tuple(img + b"\0" * 8, 0, cols)
+        got[pk] = (h, region.decode())
+    pk1 = dims["pk1"]
+    want_h = C.host_join_hash_int4(pk1)
+    assert sorted(got) == sorted(int(x) for x in pk1)
+    for i, pk in enumerate(pk1.tolist()):
+        assert got[pk][0] == int(want_h[i])
