@@ -318,6 +318,39 @@ typedef struct {
     int32_t     typmod;
 } kern_aggregate_desc;
 
+/* GPU-Sort key descriptors (xpu_common.h:2474-2520) */
+#define KSORT_KEY_KIND__VREF                0
+#define KSORT_KEY_KIND__PMINMAX_INT64       1
+#define KSORT_KEY_KIND__PMINMAX_FP64        2
+#define KSORT_KEY_KIND__PSUM_INT64          3
+#define KSORT_KEY_KIND__PSUM_FP64           4
+#define KSORT_KEY_KIND__PSUM_NUMERIC        5
+#define KSORT_KEY_KIND__PAVG_INT64          6
+#define KSORT_KEY_KIND__PAVG_FP64           7
+#define KSORT_KEY_KIND__PAVG_NUMERIC        8
+#define KSORT_KEY_KIND__PVARIANCE_SAMP      9
+#define KSORT_KEY_KIND__PVARIANCE_POP       10
+#define KSORT_KEY_KIND__PCOVAR_CORR         11
+#define KSORT_KEY_KIND__PCOVAR_SAMP         12
+#define KSORT_KEY_KIND__PCOVAR_POP          13
+#define KSORT_KEY_KIND__PCOVAR_AVGX         14
+#define KSORT_KEY_KIND__PCOVAR_AVGY         15
+#define KSORT_KEY_KIND__PCOVAR_COUNT        16
+#define KSORT_KEY_KIND__NITEMS              23
+#define KSORT_WINDOW_FUNC__ROW_NUMBER       'n'
+#define KSORT_WINDOW_FUNC__RANK             'r'
+#define KSORT_WINDOW_FUNC__DENSE_RANK       'd'
+
+typedef struct {
+    uint16_t    kind;               /* KSORT_KEY_KIND__* */
+    int8_t      nulls_first;
+    int8_t      order_asc;
+    uint16_t    src_anum;           /* attribute of the kds_final tuple */
+    uint16_t    buf_offset;
+    int32_t     key_type_code;      /* TypeOpCode */
+    uint64_t    key_ops;            /* device pointer slot, unused here */
+} kern_sortkey_desc;
+
 /* ---------------------------------------------------------------
  * kern_expression bytecode (xpu_common.h:2507-2723)
  * --------------------------------------------------------------- */
@@ -389,11 +422,7 @@ typedef struct kern_expression {
             uint32_t    window_rank_limit;
             uint16_t    window_partby_nkeys;
             uint16_t    window_orderby_nkeys;
-            struct {
-                uint16_t kind; int8_t nulls_first; int8_t order_asc;
-                uint16_t src_anum; uint16_t buf_offset;
-                int32_t  key_type_code; uint64_t key_ops;
-            } desc[1];
+            kern_sortkey_desc desc[1];
         } sort;
     } u;
 } kern_expression;

@@ -769,6 +769,110 @@ struct Compiler {
         return true;
     }
 
+    /* GPU-Sort of the final groups (kern_gpusort_prep_buffer and the
+     * comparators of cuda_gpusort.cu:15-400): each key becomes one or two
+     * order-preserving 64-bit words computed from the group entry */
+    bool gpusort()
+    {
+        plan->nsort = 0;
+        plan->sort_window = 0;
+        plan->sort_limit = 0;
+        if (!session->xpucode_gpusort_keydesc)
+            return true;
+        if (!plan->has_groupby)
+            return fail("GPU-Sort without GROUP BY is not supported");
+        const kern_expression *ks = kexp_at(session->xpucode_gpusort_keydesc);
+        if (!err.empty()) return false;
+        if (!ks || ks->opcode != FuncOpCode__SortKeys)
+            return fail("malformed SortKeys expression");
+        const int nkeys = ks->u.sort.nkeys;
+        if (nkeys < 1 || nkeys > XB_MAX_SORTKEYS ||
+            offsetof(kern_expression, u.sort.desc) + sizeof(kern_sortkey_desc) * (size_t)nkeys > ks->len)
+            return fail("SortKeys has %d keys (1..%d)", nkeys, XB_MAX_SORTKEYS);
+        for (int i = 0; i < nkeys; i++) {
+            const kern_sortkey_desc &d = ks->u.sort.desc[i];
+            if (d.src_anum < 1 || d.src_anum > plan->naggs)
+                return fail("sort key %d: attribute %u out of range", i, d.src_anum);
+            const xb_agg &a = plan->aggs[d.src_anum - 1];
+            xb_sortkey &k = plan->sort[i];
+            k.kind = d.kind;
+            k.agg = (uint16_t)(d.src_anum - 1);
+            k.asc = d.order_asc ? 1 : 0;
+            k.nulls_first = d.nulls_first ? 1 : 0;
+            k.words = 1;
+            bool ok = false;
+            switch (d.kind) {
+            case KSORT_KEY_KIND__VREF:
+                if (a.action == KAGG_ACTION__NROWS_ANY || a.action == KAGG_ACTION__NROWS_COND)
+                    ok = true;
+                else if (a.action == KAGG_ACTION__VREF && a.key_index >= 0) {
+                    const uint8_t ld = plan->keys[a.key_index].ld;
+                    ok = ld == XB_LD_BOOL || ld == XB_LD_INT2 || ld == XB_LD_INT4 || ld == XB_LD_INT8 ||
+                         ld == XB_LD_DATE || ld == XB_LD_FLT8 || ld == XB_LD_FLT4;
+                }
+                break;
+            case KSORT_KEY_KIND__PMINMAX_INT64:
+                ok = a.action == KAGG_ACTION__PMIN_INT32 || a.action == KAGG_ACTION__PMIN_INT64 ||
+                     a.action == KAGG_ACTION__PMAX_INT32 || a.action == KAGG_ACTION__PMAX_INT64;
+                break;
+            case KSORT_KEY_KIND__PMINMAX_FP64:
+                ok = a.action == KAGG_ACTION__PMIN_FP64 || a.action == KAGG_ACTION__PMAX_FP64;
+                break;
+            case KSORT_KEY_KIND__PSUM_INT64:
+            case KSORT_KEY_KIND__PSUM_NUMERIC:
+                ok = a.action == KAGG_ACTION__PSUM_INT || a.action == KAGG_ACTION__PSUM_INT64 ||
+                     a.action == KAGG_ACTION__PSUM_NUMERIC;
+                if (a.action != KAGG_ACTION__PSUM_INT)
+                    k.words = 2;                /* 128-bit sums */
+                break;
+            case KSORT_KEY_KIND__PSUM_FP64:
+                ok = a.action == KAGG_ACTION__PSUM_FP;
+                break;
+            case KSORT_KEY_KIND__PAVG_INT64:
+            case KSORT_KEY_KIND__PAVG_FP64:
+            case KSORT_KEY_KIND__PAVG_NUMERIC:
+                ok = a.action == KAGG_ACTION__PAVG_INT || a.action == KAGG_ACTION__PAVG_INT64 ||
+                     a.action == KAGG_ACTION__PAVG_FP || a.action == KAGG_ACTION__PAVG_NUMERIC;
+                break;
+            case KSORT_KEY_KIND__PVARIANCE_SAMP:
+            case KSORT_KEY_KIND__PVARIANCE_POP:
+                ok = a.action == KAGG_ACTION__STDDEV;
+                break;
+            case KSORT_KEY_KIND__PCOVAR_CORR: case KSORT_KEY_KIND__PCOVAR_SAMP:
+            case KSORT_KEY_KIND__PCOVAR_POP: case KSORT_KEY_KIND__PCOVAR_AVGX:
+            case KSORT_KEY_KIND__PCOVAR_AVGY: case KSORT_KEY_KIND__PCOVAR_COUNT:
+                ok = a.action == KAGG_ACTION__COVAR;
+                break;
+            case KSORT_KEY_KIND__NITEMS:
+                ok = a.state_sz >= 8 && a.action != KAGG_ACTION__VREF &&
+                     a.action != KAGG_ACTION__NROWS_ANY && a.action != KAGG_ACTION__NROWS_COND &&
+                     !(a.action >= KAGG_ACTION__PMIN_INT32 && a.action <= KAGG_ACTION__PMAX_FP64);
+                break;
+            default:
+                break;
+            }
+            if (!ok)
+                return fail("sort key %d: kind %u over attribute %u (action %u) is not supported",
+                            i, d.kind, d.src_anum, a.action);
+        }
+        plan->nsort = (uint32_t)nkeys;
+        const char wf = ks->u.sort.window_rank_func;
+        if (wf) {
+            if (wf != KSORT_WINDOW_FUNC__ROW_NUMBER && wf != KSORT_WINDOW_FUNC__RANK &&
+                wf != KSORT_WINDOW_FUNC__DENSE_RANK)
+                return fail("unknown window function '%c'", wf);
+            if ((int)ks->u.sort.window_partby_nkeys + (int)ks->u.sort.window_orderby_nkeys > nkeys)
+                return fail("window keys exceed the sort keys");
+            plan->sort_window = wf;
+            plan->sort_partby = (uint8_t)ks->u.sort.window_partby_nkeys;
+            plan->sort_orderby = (uint8_t)ks->u.sort.window_orderby_nkeys;
+            plan->sort_rank_limit = ks->u.sort.window_rank_limit;
+        } else if (session->gpusort_limit_count > 0) {
+            plan->sort_limit = session->gpusort_limit_count;
+        }
+        return true;
+    }
+
     bool loadvars(const kern_expression *kexp, int depth, xb_load *out, uint32_t *nout)
     {
         *nout = 0;
@@ -1298,6 +1402,8 @@ struct Compiler {
         if (!groupby())
             return false;
         if (!projection())
+            return false;
+        if (!gpusort())
             return false;
         compute_liveness();
         mark_cached_hashes();

@@ -1134,6 +1134,8 @@ struct XbFinalArgs {
     uint64_t        items_base;     /* offset of the first item */
     uint64_t        length;
     uint32_t        nslots;
+    const int64_t  *keep;           /* GPU-Sort: output position per entry, -1 dropped
+                                     * (nullptr: every group, in table order) */
 };
 
 /* byte-wise store: kds_final columns follow the header's attalign, and the
@@ -1331,7 +1333,7 @@ __global__ void xb_final_sizes(XbFinalArgs args)
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < args.cap;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const char *e = args.gt->entries + i * plan->gent_size;
-        if (((const xb_gent_head *)e)->state == XB_GSTATE_READY) {
+        if (((const xb_gent_head *)e)->state == XB_GSTATE_READY && (!args.keep || args.keep[i] >= 0)) {
             uint32_t t_len = xb_write_group_tuple(plan, e, nullptr, 0);
             args.sizes[i] = PGSTROM_MAXALIGN(offsetof(kern_hashitem, t) + t_len);
             args.flags[i] = 1;
@@ -1353,7 +1355,7 @@ __global__ void xb_final_write(XbFinalArgs args)
         if (!args.flags[i])
             continue;
         const char *e = args.gt->entries + i * plan->gent_size;
-        const uint32_t rank = args.flag_scan[i];
+        const uint32_t rank = args.keep ? (uint32_t)args.keep[i] : args.flag_scan[i];
         const uint64_t item_off = args.items_base + args.size_scan[i];
         kern_hashitem *hitem = (kern_hashitem *)(args.kds_final + item_off);
         xb_write_group_tuple(plan, e, &hitem->t, rank);
@@ -1363,6 +1365,271 @@ __global__ void xb_final_write(XbFinalArgs args)
         unsigned long long prev = atomicExch((unsigned long long *)&hslots[hash % args.nslots], mine);
         hitem->next = prev;
     }
+}
+
+/* ----------------------------------------------------------------
+ * GPU-Sort of the final groups (kern_gpusort_prep_buffer,
+ * kern_gpusort_exec_bitonic and the window-rank kernels of
+ * cuda_gpusort.cu:15-996): every sort key of a group becomes one or two
+ * 64-bit words whose unsigned order is the key's SQL order (descending
+ * keys complemented) and a NULL flag; the groups are then ordered by
+ * stable radix passes from the last key's lowest word to the first key's
+ * NULL flag, and LIMIT or the window rank picks the groups kept.
+ * ---------------------------------------------------------------- */
+struct XbSortArgs {
+    const xb_plan  *plan;
+    const xb_gtable *gt;
+    uint64_t        cap;
+    const uint32_t *flags;          /* per entry: 1 if ready */
+    const uint32_t *flag_scan;
+    uint32_t       *ents;           /* per rank: entry index */
+    uint64_t       *keyw;           /* word w of key k at keyw[(2k + w) * n + r] */
+    uint8_t        *nul;            /* NULL flag of key k at nul[k * n + r] */
+    uint32_t        n;
+};
+
+__device__ __forceinline__ uint64_t xb_sort_i64(int64_t v)
+{
+    return (uint64_t)v ^ (1ULL << 63);
+}
+
+__device__ __forceinline__ uint64_t xb_sort_f64(double d)
+{
+    if (d != d)
+        return ~0ULL;                               /* NaN sorts above every value */
+    if (d == 0.0)
+        d = 0.0;                                    /* -0 equals +0 */
+    const uint64_t b = (uint64_t)__double_as_longlong(d);
+    return (b >> 63) ? ~b : (b | (1ULL << 63));
+}
+
+__global__ void xb_sort_gather(XbSortArgs a)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.cap;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        if (a.flags[i])
+            a.ents[a.flag_scan[i]] = (uint32_t)i;
+}
+
+__global__ void xb_sort_keys(XbSortArgs a)
+{
+    const xb_plan *plan = a.plan;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < a.n; r += gridDim.x * blockDim.x) {
+        const char *e = a.gt->entries + (uint64_t)a.ents[r] * plan->gent_size;
+        const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
+        for (uint32_t k = 0; k < plan->nsort; k++) {
+            const xb_sortkey &sk = plan->sort[k];
+            const xb_agg &ag = plan->aggs[sk.agg];
+            const uint64_t *su = (const uint64_t *)(e + ag.state_off);
+            const double *sd = (const double *)su;
+            bool isnull = false;
+            uint64_t hi = 0, lo = 0;
+            const int64_t n = (int64_t)su[0];
+            switch (sk.kind) {
+            case KSORT_KEY_KIND__VREF:
+                if (ag.action == KAGG_ACTION__VREF) {
+                    const xb_keyimg &ki = img[ag.key_index];
+                    const uint8_t ld = plan->keys[ag.key_index].ld;
+                    isnull = ki.isnull != 0;
+                    hi = (ld == XB_LD_FLT8 || ld == XB_LD_FLT4) ? xb_sort_f64(__longlong_as_double(ki.val))
+                                                               : xb_sort_i64((int64_t)ki.val);
+                } else {
+                    hi = xb_sort_i64((int64_t)su[0]);       /* count */
+                }
+                break;
+            case KSORT_KEY_KIND__PMINMAX_INT64:
+            case KSORT_KEY_KIND__PMINMAX_FP64:
+                /* the state is an order-preserving int64 (xb_f64_ordered for
+                 * float8) with its valid flag */
+                isnull = *(const uint32_t *)(su + 1) == 0;
+                hi = xb_sort_i64((int64_t)su[0]);
+                break;
+            case KSORT_KEY_KIND__PSUM_INT64:
+            case KSORT_KEY_KIND__PSUM_NUMERIC:
+                isnull = n == 0;
+                if (sk.words == 1) {
+                    hi = xb_sort_i64((int64_t)su[1]);
+                } else {
+                    hi = xb_sort_i64((int64_t)su[2]);
+                    lo = su[1];
+                    const uint32_t sp = ag.state_sz >= 32 ? (*(const uint32_t *)(su + 3) & ~PAGG_NUMERIC_ATTRS__WEIGHT) : 0;
+                    if (sp & PAGG_NUMERIC_ATTRS__NAN) { hi = ~0ULL; lo = ~0ULL; }
+                    else if (sp & PAGG_NUMERIC_ATTRS__PINF) { hi = ~0ULL; lo = ~1ULL; }
+                    else if (sp & PAGG_NUMERIC_ATTRS__NINF) { hi = 0; lo = 0; }
+                }
+                break;
+            case KSORT_KEY_KIND__PSUM_FP64:
+                isnull = n == 0;
+                hi = xb_sort_f64(sd[1] + sd[2]);
+                break;
+            case KSORT_KEY_KIND__PAVG_INT64:
+            case KSORT_KEY_KIND__PAVG_FP64:
+            case KSORT_KEY_KIND__PAVG_NUMERIC: {
+                isnull = n == 0;
+                double sum;
+                if (ag.action == KAGG_ACTION__PAVG_INT)
+                    sum = (double)(int64_t)su[1];
+                else if (ag.action == KAGG_ACTION__PAVG_FP)
+                    sum = sd[1] + sd[2];
+                else    /* 128-bit sum; the scale is one per column, so it keeps the order */
+                    sum = (double)(xb_i128)(((unsigned __int128)su[2] << 64) | su[1]);
+                hi = xb_sort_f64(isnull ? 0.0 : sum / (double)n);
+                break;
+            }
+            case KSORT_KEY_KIND__PVARIANCE_SAMP:
+            case KSORT_KEY_KIND__PVARIANCE_POP: {
+                const bool samp = sk.kind == KSORT_KEY_KIND__PVARIANCE_SAMP;
+                isnull = samp ? n < 2 : n < 1;
+                const double dn = (double)n, sx = sd[1] + sd[2], sxx = sd[3] + sd[4];
+                const double num = dn * sxx - sx * sx;
+                hi = xb_sort_f64(isnull ? 0.0 : (num < 0.0 ? 0.0 : num) / (dn * (samp ? dn - 1.0 : dn)));
+                break;
+            }
+            case KSORT_KEY_KIND__PCOVAR_CORR: case KSORT_KEY_KIND__PCOVAR_SAMP:
+            case KSORT_KEY_KIND__PCOVAR_POP: case KSORT_KEY_KIND__PCOVAR_AVGX:
+            case KSORT_KEY_KIND__PCOVAR_AVGY: case KSORT_KEY_KIND__PCOVAR_COUNT: {
+                const double dn = (double)n;
+                const double sx = sd[1] + sd[2], sxx = sd[3] + sd[4], sy = sd[5] + sd[6];
+                const double syy = sd[7] + sd[8], sxy = sd[9] + sd[10];
+                double v = 0.0;
+                switch (sk.kind) {
+                case KSORT_KEY_KIND__PCOVAR_COUNT: v = dn; break;
+                case KSORT_KEY_KIND__PCOVAR_AVGX: isnull = n < 1; v = sx / dn; break;
+                case KSORT_KEY_KIND__PCOVAR_AVGY: isnull = n < 1; v = sy / dn; break;
+                case KSORT_KEY_KIND__PCOVAR_POP: isnull = n < 1; v = (sxy - sx * sy / dn) / dn; break;
+                case KSORT_KEY_KIND__PCOVAR_SAMP: isnull = n < 2; v = (sxy - sx * sy / dn) / (dn - 1.0); break;
+                default: {
+                    const double vx = dn * sxx - sx * sx, vy = dn * syy - sy * sy;
+                    isnull = n < 1 || vx <= 0.0 || vy <= 0.0;
+                    v = (dn * sxy - sx * sy) / sqrt(vx * vy);
+                    break;
+                }
+                }
+                hi = xb_sort_f64(isnull ? 0.0 : v);
+                break;
+            }
+            case KSORT_KEY_KIND__NITEMS:
+                hi = xb_sort_i64(n);
+                break;
+            default:
+                break;
+            }
+            if (isnull) {
+                hi = 0;
+                lo = 0;
+            } else if (!sk.asc) {
+                hi = ~hi;
+                lo = ~lo;
+            }
+            a.keyw[(2ULL * k) * a.n + r] = hi;
+            a.keyw[(2ULL * k + 1) * a.n + r] = lo;
+            /* the flag sorts as the key's most significant part */
+            a.nul[(uint64_t)k * a.n + r] = (uint8_t)(isnull ? (sk.nulls_first ? 0 : 1) : (sk.nulls_first ? 1 : 0));
+        }
+    }
+}
+
+/* the key of one radix pass, in the current order */
+__global__ void xb_sort_pass_key64(const uint64_t *col, const uint32_t *idx, uint64_t *out, uint32_t n)
+{
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        out[p] = col[idx[p]];
+}
+
+__global__ void xb_sort_pass_key8(const uint8_t *col, const uint32_t *idx, uint8_t *out, uint32_t n)
+{
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        out[p] = col[idx[p]];
+}
+
+/* groups kept, in order: LIMIT, or the window rank of each group within
+ * its partition (row_number / rank / dense_rank) against its limit */
+struct XbRankArgs {
+    const xb_plan  *plan;
+    const uint32_t *idx;            /* rank of the group at each sorted position */
+    const uint64_t *keyw;
+    const uint8_t  *nul;
+    uint32_t        n;
+    uint32_t       *part_start;     /* position that starts a new partition, else 0 */
+    uint32_t       *peer_start;     /* position that starts a new peer group, else 0 */
+    uint32_t       *peer_flag;      /* 1 where a peer group starts */
+};
+
+__device__ __forceinline__ bool
+xb_sort_keys_equal(const XbRankArgs &a, uint32_t k0, uint32_t k1, uint32_t r, uint32_t q)
+{
+    for (uint32_t k = k0; k < k1; k++) {
+        if (a.nul[(uint64_t)k * a.n + r] != a.nul[(uint64_t)k * a.n + q] ||
+            a.keyw[(2ULL * k) * a.n + r] != a.keyw[(2ULL * k) * a.n + q] ||
+            a.keyw[(2ULL * k + 1) * a.n + r] != a.keyw[(2ULL * k + 1) * a.n + q])
+            return false;
+    }
+    return true;
+}
+
+__global__ void xb_sort_bounds(XbRankArgs a)
+{
+    const uint32_t pb = a.plan->sort_partby, ob = a.plan->sort_orderby;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        bool part = p == 0, peer = p == 0;
+        if (p > 0) {
+            const uint32_t r = a.idx[p], q = a.idx[p - 1];
+            part = !xb_sort_keys_equal(a, 0, pb, r, q);
+            peer = part || !xb_sort_keys_equal(a, pb, pb + ob, r, q);
+        }
+        a.part_start[p] = part ? p : 0;
+        a.peer_start[p] = peer ? p : 0;
+        a.peer_flag[p] = peer ? 1 : 0;
+    }
+}
+
+struct XbKeepArgs {
+    const xb_plan  *plan;
+    const uint32_t *idx;
+    const uint32_t *ents;
+    uint32_t        n;
+    const uint32_t *part_start;     /* after the max-scan: the partition's first position */
+    const uint32_t *peer_start;     /* after the max-scan */
+    const uint32_t *peer_cnt;       /* inclusive sum of peer_flag */
+    uint32_t       *keep_flag;
+};
+
+__global__ void xb_sort_keepflag(XbKeepArgs a)
+{
+    const xb_plan *plan = a.plan;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        bool keep = true;
+        if (plan->sort_window) {
+            const uint32_t ps = a.part_start[p];
+            uint64_t rank;
+            if (plan->sort_window == KSORT_WINDOW_FUNC__ROW_NUMBER)
+                rank = p - ps + 1;
+            else if (plan->sort_window == KSORT_WINDOW_FUNC__RANK)
+                rank = a.peer_start[p] - ps + 1;
+            else
+                rank = a.peer_cnt[p] - a.peer_cnt[ps] + 1;
+            keep = plan->sort_rank_limit == 0 || rank <= plan->sort_rank_limit;
+        } else if (plan->sort_limit > 0) {
+            keep = (int64_t)p < plan->sort_limit;
+        }
+        a.keep_flag[p] = keep ? 1 : 0;
+    }
+}
+
+__global__ void xb_sort_keep(XbKeepArgs a, const uint32_t *keep_scan, int64_t *keep)
+{
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x)
+        keep[a.ents[a.idx[p]]] = a.keep_flag[p] ? (int64_t)keep_scan[p] : -1;
+}
+
+struct XbMaxOp {
+    __device__ __forceinline__ uint32_t operator()(uint32_t x, uint32_t y) const { return x > y ? x : y; }
+};
+
+__global__ void xb_iota_u32(uint32_t *out, uint32_t n)
+{
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        out[p] = p;
 }
 
 /* ----------------------------------------------------------------
@@ -2708,6 +2975,122 @@ xpuB200TimeExecTask(xpuB200Session *s, const kern_data_store *kds_src_dev, int n
     return 0;
 }
 
+/* GPU-Sort of the session's groups: *p_keep receives, per group-table
+ * entry, the group's output position or -1 (dropped by LIMIT or the window
+ * rank).  fa carries the table and the flag arrays; alloc places device
+ * memory that the caller frees.  Returns 0, or -1 when out of memory. */
+template <typename Alloc>
+static int xb_final_sort(xpuB200Session *s, XbFinalArgs fa, cudaStream_t st, Alloc alloc, int64_t **p_keep)
+{
+    const xb_plan *plan = s->h_plan;
+    const uint64_t cap = fa.cap;
+    const int grid = s->dev->nsm * 8;
+    fa.keep = nullptr;
+    xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);              /* flags of every group */
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, fa.flags, fa.flag_scan, (int64_t)cap, st);
+    void *d_t = nullptr;
+    if (!alloc(tb, &d_t)) return -1;
+    cub::DeviceScan::ExclusiveSum(d_t, tb, fa.flags, fa.flag_scan, (int64_t)cap, st);
+    uint32_t lf = 0, ls = 0;
+    cudaMemcpyAsync(&lf, fa.flags + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&ls, fa.flag_scan + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -1;
+    const uint32_t n = lf + ls;
+    int64_t *keep = nullptr;
+    if (!alloc(cap * 8, (void **)&keep)) return -1;
+    cudaMemsetAsync(keep, 0xff, cap * 8, st);
+    *p_keep = keep;
+    if (n == 0)
+        return 0;
+    const uint32_t nk = plan->nsort;
+    uint32_t *ents, *idx, *idx2, *part, *peer, *pflag, *pcnt, *kflag, *kscan;
+    uint64_t *keyw, *k64a, *k64b;
+    uint8_t *nul, *k8a, *k8b;
+    if (!alloc((size_t)n * 4, (void **)&ents) || !alloc((size_t)n * 4, (void **)&idx) ||
+        !alloc((size_t)n * 4, (void **)&idx2) || !alloc((size_t)n * 16 * nk, (void **)&keyw) ||
+        !alloc((size_t)n * nk, (void **)&nul) || !alloc((size_t)n * 8, (void **)&k64a) ||
+        !alloc((size_t)n * 8, (void **)&k64b) || !alloc((size_t)n, (void **)&k8a) ||
+        !alloc((size_t)n, (void **)&k8b) || !alloc((size_t)n * 4, (void **)&part) ||
+        !alloc((size_t)n * 4, (void **)&peer) || !alloc((size_t)n * 4, (void **)&pflag) ||
+        !alloc((size_t)n * 4, (void **)&pcnt) || !alloc((size_t)n * 4, (void **)&kflag) ||
+        !alloc((size_t)n * 4, (void **)&kscan))
+        return -1;
+    XbSortArgs sa;
+    sa.plan = s->d_plan;
+    sa.gt = s->d_gt;
+    sa.cap = cap;
+    sa.flags = fa.flags;
+    sa.flag_scan = fa.flag_scan;
+    sa.ents = ents;
+    sa.keyw = keyw;
+    sa.nul = nul;
+    sa.n = n;
+    int g2 = (int)((n + XB_BLOCK - 1) / XB_BLOCK);
+    if (g2 > grid) g2 = grid;
+    xb_sort_gather<<<grid, XB_BLOCK, 0, st>>>(sa);
+    xb_sort_keys<<<g2, XB_BLOCK, 0, st>>>(sa);
+    xb_iota_u32<<<g2, XB_BLOCK, 0, st>>>(idx, n);
+    /* temporary storage for the largest of the library passes */
+    size_t t64 = 0, t8 = 0, tmax = 0, tsum = 0, tex = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t64, k64a, k64b, idx, idx2, (int64_t)n, 0, 64, st);
+    cub::DeviceRadixSort::SortPairs(nullptr, t8, k8a, k8b, idx, idx2, (int64_t)n, 0, 1, st);
+    cub::DeviceScan::InclusiveScan(nullptr, tmax, part, part, XbMaxOp(), (int64_t)n, st);
+    cub::DeviceScan::InclusiveSum(nullptr, tsum, pflag, pcnt, (int64_t)n, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, tex, kflag, kscan, (int64_t)n, st);
+    size_t tt = std::max(std::max(t64, t8), std::max(tmax, std::max(tsum, tex)));
+    void *d_tt = nullptr;
+    if (!alloc(tt, &d_tt)) return -1;
+    /* stable passes, least significant first: for each key from the last,
+     * its low word, its high word, then its NULL flag */
+    for (int k = (int)nk - 1; k >= 0; k--) {
+        for (int w = 1; w >= 0; w--) {
+            if (w == 1 && plan->sort[k].words < 2)
+                continue;
+            xb_sort_pass_key64<<<g2, XB_BLOCK, 0, st>>>(keyw + (2ULL * k + w) * n, idx, k64a, n);
+            size_t t = tt;
+            cub::DeviceRadixSort::SortPairs(d_tt, t, k64a, k64b, idx, idx2, (int64_t)n, 0, 64, st);
+            std::swap(idx, idx2);
+        }
+        xb_sort_pass_key8<<<g2, XB_BLOCK, 0, st>>>(nul + (uint64_t)k * n, idx, k8a, n);
+        size_t t = tt;
+        cub::DeviceRadixSort::SortPairs(d_tt, t, k8a, k8b, idx, idx2, (int64_t)n, 0, 1, st);
+        std::swap(idx, idx2);
+    }
+    XbRankArgs ra;
+    ra.plan = s->d_plan;
+    ra.idx = idx;
+    ra.keyw = keyw;
+    ra.nul = nul;
+    ra.n = n;
+    ra.part_start = part;
+    ra.peer_start = peer;
+    ra.peer_flag = pflag;
+    if (plan->sort_window) {
+        xb_sort_bounds<<<g2, XB_BLOCK, 0, st>>>(ra);
+        size_t t = tt;
+        cub::DeviceScan::InclusiveScan(d_tt, t, part, part, XbMaxOp(), (int64_t)n, st);
+        t = tt;
+        cub::DeviceScan::InclusiveScan(d_tt, t, peer, peer, XbMaxOp(), (int64_t)n, st);
+        t = tt;
+        cub::DeviceScan::InclusiveSum(d_tt, t, pflag, pcnt, (int64_t)n, st);
+    }
+    XbKeepArgs ka;
+    ka.plan = s->d_plan;
+    ka.idx = idx;
+    ka.ents = ents;
+    ka.n = n;
+    ka.part_start = part;
+    ka.peer_start = peer;
+    ka.peer_cnt = pcnt;
+    ka.keep_flag = kflag;
+    xb_sort_keepflag<<<g2, XB_BLOCK, 0, st>>>(ka);
+    size_t t = tt;
+    cub::DeviceScan::ExclusiveSum(d_tt, t, kflag, kscan, (int64_t)n, st);
+    xb_sort_keep<<<g2, XB_BLOCK, 0, st>>>(ka, kscan, keep);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 extern "C" int
 xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *p_required,
              kern_exec_results *results, kern_errorbuf *err)
@@ -2767,6 +3150,15 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     fa.size_scan = d_size_scan;
     fa.flag_scan = d_flag_scan;
     int grid = s->dev->nsm * 8;
+    if (plan->nsort) {
+        int64_t *d_keep = nullptr;
+        if (xb_final_sort(s, fa, st, alloc, &d_keep) != 0) {
+            cleanup();
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "GPU-Sort of the groups failed (%s)",
+                          cudaGetErrorString(cudaGetLastError()));
+        }
+        fa.keep = d_keep;
+    }
     /* the global table's entries pointer lives in h_gt */
     xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
     cub::DeviceScan::ExclusiveSum(nullptr, temp1, d_sizes, d_size_scan, (int64_t)cap, st);
@@ -2954,6 +3346,8 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
             results->stats[d - 1].nitems_out = (uint32_t)s->total_depth[d];
         results->final_plan_task = true;
     }
+    if (plan->nsort)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "a session with GPU-Sort keys needs xpuB200Final");
     if (!plan->has_groupby) {
         if (p_required) *p_required = 0;
         return 0;

@@ -186,6 +186,17 @@ typedef struct xb_inner {
     xb_load     load[XB_MAX_LOADS];
 } xb_inner;
 
+/* one GPU-Sort key over the group entries (kern_sortkey_desc) */
+#define XB_MAX_SORTKEYS 8
+typedef struct xb_sortkey {
+    uint16_t    kind;           /* KSORT_KEY_KIND__* */
+    uint16_t    agg;            /* index into aggs[] (src_anum - 1) */
+    uint8_t     asc;
+    uint8_t     nulls_first;
+    uint8_t     words;          /* 64-bit words of the encoded key (1 or 2) */
+    uint8_t     __pad;
+} xb_sortkey;
+
 /* one partial-aggregate (or grouping key) column of the kds_final tuple */
 typedef struct xb_agg {
     uint16_t    action;         /* KAGG_ACTION__* */
@@ -274,6 +285,16 @@ typedef struct xb_plan {
     uint32_t    proj_nslots;
     xb_prog     proj_hash;
     xb_prog     proj_all;       /* proj_args, then proj_hash: one program */
+
+    /* GPU-Sort of the groups at Final (SortKeys, gpusort_limit_count) */
+    uint32_t    nsort;
+    xb_sortkey  sort[XB_MAX_SORTKEYS];
+    char        sort_window;    /* KSORT_WINDOW_FUNC__*, or 0 */
+    uint8_t     sort_partby;    /* leading keys that partition the window */
+    uint8_t     sort_orderby;   /* keys after them that order it */
+    uint8_t     __pad4;
+    uint32_t    sort_rank_limit;
+    int64_t     sort_limit;     /* LIMIT without a window function; 0: none */
 
     /* VM code */
     uint32_t    ninsns;

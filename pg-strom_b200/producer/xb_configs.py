@@ -117,10 +117,13 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ng
     return tbl, session, None, expect, meta
 
 
-def wide_groupby_session(a_limit=600, ngroups=3000):
+def wide_groupby_session(a_limit=600, ngroups=3000, sort=None):
     """WHERE a < a_limit GROUP BY g -> count(*), count(b), min(a),
     max(a::int8), min(b), max(b), sum(b), avg(c), stddev(b), covar(b, a):
-    every partial state form of kds_final."""
+    every partial state form of kds_final (attributes 1..10, g is 11).
+    sort: dict(keys=[(kind, attribute, asc, nulls_first)], window=(func,
+    partition keys, order keys, rank limit), limit=n) for a GPU-Sort of the
+    groups at Final."""
     typmod_c = numeric_typmod(12, 2)
     va, vb, vc, vg = (Var(0, 2, "int4"), Var(0, 3, "float8"),
                       Var(0, 4, "numeric", typmod_c), Var(0, 5, "int4"))
@@ -138,7 +141,14 @@ def wide_groupby_session(a_limit=600, ngroups=3000):
               Agg("PAVG_NUMERIC", vc, typmod_c),
               Agg("STDDEV", vb),
               Agg("COVAR", vb, arg1=Func("int4_to_float8", [va], "float8"))],
-        ngroups_estimate=float(ngroups))
+        ngroups_estimate=float(ngroups),
+        **_sort_args(sort))
+
+
+def _sort_args(sort):
+    if not sort:
+        return {}
+    return {"sort_keys": sort["keys"], "sort_window": sort.get("window"), "sort_limit": sort.get("limit", 0)}
 
 
 def _group_sum(g, m, x, n):
@@ -202,7 +212,7 @@ def zipf_bounded(r, n, s, size):
     return (np.searchsorted(cdf, u, side="right") + 1).astype(np.int32)
 
 
-def join_groupby_session(flag_limit=3):
+def join_groupby_session(flag_limit=3, sort=None):
     """fact JOIN dim1 ON fk1 = pk JOIN dim2 ON fk2 = pk AND flag < flag_limit
     GROUP BY region -> sum(qty * price), count(*)."""
     f_fk1, f_fk2, f_qty, f_price = (Var(0, 1, "int4"), Var(0, 2, "int4"),
@@ -217,7 +227,8 @@ def join_groupby_session(flag_limit=3):
         groupby_keys=[d1_region],
         aggs=[Agg("PSUM_INT64", Func("int48mul", [f_qty, f_price], "int8")),
               Agg("NROWS_ANY")],
-        ngroups_estimate=25.0)
+        ngroups_estimate=25.0,
+        **_sort_args(sort))
 
 
 def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3,

@@ -164,3 +164,99 @@ def compare_groups(got, want, rtol=1e-12):
             elif x != y:
                 errs.append(f"{k}[{j}]: {x!r} vs {y!r}")
     return errs
+
+
+# ---------------------------------------------------------------------------
+# GPU-Sort restated: the order of final groups by SortKeys (the comparators
+# and prep functions of cuda_gpusort.cu:15-400), LIMIT and window ranks
+# (cuda_gpusort.cu:816-996), over decoded groups
+# ---------------------------------------------------------------------------
+def sort_key_values(row, session, sort_keys):
+    """The SQL value (None for NULL) of each sort key of one decoded group
+    (key tuple, states); sort_keys as given to build_sort_keys."""
+    import math
+    keys, states = row
+    aggs = session_aggs(session)
+    out = []
+    for kind, anum, _asc, _nf in sort_keys:
+        action = aggs[anum - 1][0]
+        if action == VREF:
+            out.append(keys[sum(1 for a in aggs[:anum - 1] if a[0] == VREF)])
+            continue
+        st = states[sum(1 for a in aggs[:anum - 1] if a[0] != VREF)]
+        if kind == "VREF":
+            out.append(st)
+        elif kind in ("PMINMAX_INT64", "PMINMAX_FP64"):
+            out.append(st[1] if st[0] else None)
+        elif kind in ("PSUM_INT64", "PSUM_NUMERIC", "PSUM_FP64"):
+            out.append(st[1] if st[0] else None)
+        elif kind in ("PAVG_INT64", "PAVG_FP64", "PAVG_NUMERIC"):
+            out.append(float(st[1]) / st[0] if st[0] else None)
+        elif kind in ("PVARIANCE_SAMP", "PVARIANCE_POP"):
+            n, sx, sxx = st
+            samp = kind == "PVARIANCE_SAMP"
+            if n < (2 if samp else 1):
+                out.append(None)
+            else:
+                num = max(n * sxx - sx * sx, 0.0)
+                out.append(num / (n * (n - 1 if samp else n)))
+        elif kind.startswith("PCOVAR_"):
+            n, sx, sxx, sy, syy, sxy = st
+            if kind == "PCOVAR_COUNT":
+                out.append(float(n))
+            elif n < 1 or (kind == "PCOVAR_SAMP" and n < 2):
+                out.append(None)
+            elif kind == "PCOVAR_AVGX":
+                out.append(sx / n)
+            elif kind == "PCOVAR_AVGY":
+                out.append(sy / n)
+            elif kind == "PCOVAR_POP":
+                out.append((sxy - sx * sy / n) / n)
+            elif kind == "PCOVAR_SAMP":
+                out.append((sxy - sx * sy / n) / (n - 1))
+            else:
+                vx, vy = n * sxx - sx * sx, n * syy - sy * sy
+                out.append(None if vx <= 0 or vy <= 0 else (n * sxy - sx * sy) / math.sqrt(vx * vy))
+        elif kind == "NITEMS":
+            out.append(st[0])
+        else:
+            raise ValueError(kind)
+    return out
+
+
+def _cmp_values(a, b, sort_keys):
+    for (kind, _anum, asc, nulls_first), x, y in zip(sort_keys, a, b):
+        if x is None or y is None:
+            if x is None and y is None:
+                continue
+            xn = x is None
+            return (-1 if xn else 1) if nulls_first else (1 if xn else -1)
+        if x != y:
+            c = -1 if x < y else 1
+            return c if asc else -c
+    return 0
+
+
+def order_groups(rows, session, sort_keys, window=None, limit=0):
+    """Expected output of a GPU-Sort Final: the decoded groups (key tuple,
+    states) in sort order, cut by LIMIT or filtered by the window rank
+    (window = (function 'n' / 'r' / 'd', partition keys, order keys,
+    rank limit)).  Rows with equal sort keys may come in any order."""
+    import functools
+    vals = [(sort_key_values(r, session, sort_keys), r) for r in rows]
+    vals.sort(key=functools.cmp_to_key(lambda a, b: _cmp_values(a[0], b[0], sort_keys)))
+    if window:
+        wf, pb, ob, lim = window
+        out, ps, peer, dense = [], 0, 0, 0
+        for p, (v, r) in enumerate(vals):
+            if p == 0 or _cmp_values(v[:pb], vals[p - 1][0][:pb], sort_keys[:pb]) != 0:
+                ps, peer, dense = p, p, 1
+            elif _cmp_values(v[pb:pb + ob], vals[p - 1][0][pb:pb + ob], sort_keys[pb:pb + ob]) != 0:
+                peer, dense = p, dense + 1
+            rank = {"n": p - ps + 1, "r": peer - ps + 1, "d": dense}[wf]
+            if lim == 0 or rank <= lim:
+                out.append((v, r))
+        vals = out
+    elif limit > 0:
+        vals = vals[:limit]
+    return vals

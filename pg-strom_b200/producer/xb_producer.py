@@ -678,6 +678,26 @@ class _Buf:
         struct.pack_into("<I", self.b, head_pos, len(self.b) - head_pos)
 
 
+KSORT = dict(VREF=0, PMINMAX_INT64=1, PMINMAX_FP64=2, PSUM_INT64=3, PSUM_FP64=4, PSUM_NUMERIC=5,
+             PAVG_INT64=6, PAVG_FP64=7, PAVG_NUMERIC=8, PVARIANCE_SAMP=9, PVARIANCE_POP=10,
+             PCOVAR_CORR=11, PCOVAR_SAMP=12, PCOVAR_POP=13, PCOVAR_AVGX=14, PCOVAR_AVGY=15,
+             PCOVAR_COUNT=16, NITEMS=23)
+
+
+def build_sort_keys(keys, window=None):
+    """SortKeys kexp (xpu_common.h:2676-2684): keys = list of (kind name,
+    kds_final attribute number, ascending, nulls first); window = (function
+    'n' / 'r' / 'd', partition keys, order keys, rank limit) or None."""
+    wf, pb, ob, lim = window if window else ("\0", 0, 0, 0)
+    body = struct.pack("<i?cxxIHH", len(keys), True, wf.encode(), lim, pb, ob)
+    for kind, anum, asc, nf in keys:
+        body += struct.pack("<HbbHHixxxxQ", KSORT[kind], 1 if nf else 0, 1 if asc else 0, anum, 0, 0, 0)
+    buf = _Buf()
+    buf.b += _kexp_head(TOP("int4"), FOP("SortKeys"), 0, 0) + body
+    buf.finish_kexp(0)
+    return bytes(buf.b)
+
+
 def _kexp_head(exptype, opcode, nr_args=0, args_offset=0, flags=0):
     return struct.pack("<IiQIiQII", 0, exptype, 0, flags, opcode, 0, nr_args, args_offset)
 
@@ -870,7 +890,8 @@ class SessionBuilder:
 
     def build(self, *, scan_quals=None, joins=(), groupby_keys=(), aggs=(),
               ngroups_estimate=100.0, final_tlist=None, projection=None,
-              htup_margin=0, projection_hash=None, proj_nslots=0) -> bytes:
+              htup_margin=0, projection_hash=None, proj_nslots=0, sort_keys=None,
+              sort_window=None, sort_limit=0) -> bytes:
         """joins: list of (outer_hash_keys, join_quals, other_quals) for
         depth 1..n.  groupby_keys: list of Expr; aggs: list of Agg.  The
         partial-aggregation target list is aggs then keys (gpu_preagg.c:
@@ -883,6 +904,9 @@ class SessionBuilder:
         nrels = self.nrels
         blobs = {}
         self.htup_margin = htup_margin
+        self.sort_limit = sort_limit
+        if sort_keys:
+            blobs["gpusort"] = build_sort_keys(sort_keys, sort_window)
         if scan_quals is not None:
             blobs["scan"] = self.build_expr(scan_quals, 0)
         jq, hv = {}, {}
@@ -1026,7 +1050,7 @@ class SessionBuilder:
         offs["kvars"] = out.append_aligned(desc) if desc else 0
         for key in ("loadvars", "movevars", "scan", "joinquals", "hashvalues",
                     "keyhash", "keyload", "keycomp", "actions", "kds_final",
-                    "projection", "kds_dst"):
+                    "projection", "kds_dst", "gpusort"):
             b = blobs.get(key)
             offs[key] = out.append_aligned(b) if b else 0
         poffs = []
@@ -1039,10 +1063,10 @@ class SessionBuilder:
         struct.pack_into("<IIIIIIIIIIII", b, 48, offs["loadvars"], offs["movevars"], offs["scan"],
                          offs["joinquals"], offs["hashvalues"], 0, offs["projection"], offs["keyhash"],
                          offs["keyload"],
-                         offs["keycomp"], offs["actions"], 0)
+                         offs["keycomp"], offs["actions"], offs["gpusort"])
         struct.pack_into("<I", b, 128, offs["kds_dst"])
         struct.pack_into("<I", b, 156, offs["kds_final"])
-        struct.pack_into("<I", b, 168, getattr(self, "htup_margin", 0))
+        struct.pack_into("<Ii", b, 168, getattr(self, "htup_margin", 0), getattr(self, "sort_limit", 0))
         struct.pack_into("<If", b, 160, 0, float(ngroups_estimate))
         struct.pack_into("<I", b, 188, nparams)
         for i, p in enumerate(poffs):
