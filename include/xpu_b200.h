@@ -284,6 +284,23 @@ void xpuB200BatchDestroy(xpuB200Batch *batch);
  * kern_buffer_partitioning (cuda_gpujoin.cu:76-138), launched by the GPU
  * service's pinned inner-buffer setup (gpu_service.c:1748-2197).
  */
+/*
+ * Inner relations resident across sessions.  A session whose
+ * kern_session_info.join_inner_handle is not 0 keeps the inner relations
+ * it uploaded and indexed (kern_multirels) on the device under that handle:
+ * a later session with the same handle and the same build inputs (the
+ * translated inner descriptors and the join quals evaluated at the build,
+ * constants included) uses them as they are, with no upload and no build.
+ * The caller guarantees that one handle always names the same
+ * kern_multirels contents, as the reference's join_inner_handle names one
+ * inner buffer shared by the sessions of a query (gpu_service.c:2357-2412).
+ * Built relations stay after their last session closes while the cache
+ * holds at most max_bytes (default 16 GiB; least recently used first out).
+ * max_bytes == UINT64_MAX only reads *p_cached_bytes (the bytes held now).
+ */
+int  xpuB200InnerCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes,
+                             kern_errorbuf *err);
+
 int  xpuB200InnerRebuild(xpuB200Device *dev, kern_data_store *kds_dst, const kern_data_store *kds_src,
                          uint32_t hash_divisor, uint32_t hash_remainder, uint64_t *p_required,
                          kern_errorbuf *err);

@@ -1926,7 +1926,105 @@ struct xpuB200Device {
     std::vector<cudaStream_t> free_streams;
     std::vector<xb_status *> free_status;
     std::vector<xb_status *> status_blocks;
+    /* inner relations built for sessions with a join_inner_handle, kept
+     * while sessions use them and, within inner_budget bytes, after */
+    std::mutex      inner_lock;
+    std::vector<struct xb_inner_entry *> inner_cache;
+    uint64_t        inner_budget = 16ULL << 30;
+    uint64_t        inner_bytes = 0;
+    uint64_t        inner_clock = 0;
 };
+
+/* one cached set of inner relations: the built descriptors (with their
+ * device memory) of every depth */
+struct xb_inner_entry {
+    uint64_t        key;
+    uint32_t        nrels;
+    xb_inner        inner[XB_MAX_DEPTH + 1];
+    uint32_t        gid_cap;        /* shared table slots the group ids need (0: none) */
+    std::vector<void *> allocs;
+    uint64_t        bytes = 0;
+    uint32_t        refs = 0;
+    uint64_t        last_use = 0;
+};
+
+static void xb_inner_entry_free(xpuB200Device *dev, xb_inner_entry *e)
+{
+    for (void *p : e->allocs)
+        cudaFreeAsync(p, dev->stream);
+    cudaStreamSynchronize(dev->stream);
+    delete e;
+}
+
+/* drop unreferenced entries, least recently used first, while the cache
+ * holds more than its budget; inner_lock held */
+static void xb_inner_evict_locked(xpuB200Device *dev)
+{
+    while (dev->inner_bytes > dev->inner_budget) {
+        int victim = -1;
+        for (size_t i = 0; i < dev->inner_cache.size(); i++) {
+            xb_inner_entry *e = dev->inner_cache[i];
+            if (e->refs == 0 && (victim < 0 || e->last_use < dev->inner_cache[victim]->last_use))
+                victim = (int)i;
+        }
+        if (victim < 0)
+            return;
+        xb_inner_entry *e = dev->inner_cache[victim];
+        dev->inner_cache.erase(dev->inner_cache.begin() + victim);
+        dev->inner_bytes -= e->bytes;
+        xb_inner_entry_free(dev, e);
+    }
+}
+
+/* the identity of an inner build: the caller's handle for the inner
+ * relations' contents, and everything of the translated session the build
+ * reads (descriptors before the build, the programs of the join quals it
+ * evaluates with their constants, the group-id inputs) */
+static uint64_t xb_inner_key(const xpuB200Device *dev, uint64_t handle, const xb_plan *plan, uint64_t kmrels_sz)
+{
+    uint64_t h = 1469598103934665603ULL;
+    auto mix = [&](const void *p, size_t n) {
+        const unsigned char *c = (const unsigned char *)p;
+        for (size_t i = 0; i < n; i++) { h ^= c[i]; h *= 1099511628211ULL; }
+    };
+    mix(&dev->dindex, sizeof(dev->dindex));
+    mix(&handle, sizeof(handle));
+    mix(&kmrels_sz, sizeof(kmrels_sz));
+    mix(&plan->nrels, sizeof(plan->nrels));
+    mix(&plan->gid_depth, sizeof(plan->gid_depth));
+    mix(&plan->gent_size, sizeof(plan->gent_size));
+    mix(&plan->nkeys, sizeof(plan->nkeys));
+    mix(plan->keys, sizeof(xb_key) * plan->nkeys);
+    mix(&plan->nregs, sizeof(plan->nregs));
+    for (uint32_t d = 1; d <= plan->nrels; d++) {
+        mix(&plan->inner[d], sizeof(xb_inner));
+        const xb_prog &q = plan->inner[d].build_qual;
+        if (q.count && q.start + q.count <= plan->ninsns)
+            mix(plan->insns + q.start, sizeof(xb_insn) * q.count);
+    }
+    return h;
+}
+
+static xb_inner_entry *xb_inner_cache_get(xpuB200Device *dev, uint64_t key)
+{
+    std::lock_guard<std::mutex> g(dev->inner_lock);
+    for (xb_inner_entry *e : dev->inner_cache)
+        if (e->key == key) {
+            e->refs++;
+            e->last_use = ++dev->inner_clock;
+            return e;
+        }
+    return nullptr;
+}
+
+static void xb_inner_cache_put(xpuB200Device *dev, xb_inner_entry *e)
+{
+    std::lock_guard<std::mutex> g(dev->inner_lock);
+    if (e->refs > 0)
+        e->refs--;
+    e->last_use = ++dev->inner_clock;
+    xb_inner_evict_locked(dev);
+}
 
 static cudaStream_t xb_get_stream(xpuB200Device *dev)
 {
@@ -1988,6 +2086,9 @@ struct xpuB200Session {
     xb_plan        *h_plan = nullptr;
     xb_plan        *d_plan = nullptr;
     std::vector<void *> d_allocs;
+    std::vector<uint64_t> d_alloc_sz;
+    xb_inner_entry *inner_entry = nullptr;  /* cached inner relations in use */
+    bool            inner_hit = false;      /* found built by an earlier session */
     xb_gtable       h_gt;
     xb_gtable      *d_gt = nullptr;
     xb_status      *d_status = nullptr;
@@ -2170,6 +2271,9 @@ xpuB200Shutdown(xpuB200Device *dev)
     if (!dev) return;
     cudaSetDevice(dev->dindex);
     xb_sched_destroy(dev);
+    for (xb_inner_entry *e : dev->inner_cache)
+        xb_inner_entry_free(dev, e);
+    dev->inner_cache.clear();
     cudaStreamSynchronize(dev->stream);
     cudaStreamDestroy(dev->stream);
     for (cudaStream_t st : dev->free_streams)
@@ -2193,6 +2297,8 @@ static void xb_session_free(xpuB200Session *s)
     if (s->d_tasks) cudaFreeAsync(s->d_tasks, st);
     if (s->d_dst) cudaFreeAsync(s->d_dst, st);
     cudaStreamSynchronize(st);
+    if (s->inner_entry)
+        xb_inner_cache_put(s->dev, s->inner_entry);
     xb_put_status(s->dev, s->h_status);
     if (s->h_plan) free(s->h_plan);
     cudaEventDestroy(s->ev0);
@@ -2210,6 +2316,7 @@ static int xb_dalloc(xpuB200Session *s, size_t sz, void **p, kern_errorbuf *err)
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cudaMalloc(%zu): %s", sz, cudaGetErrorString(rc));
     }
     s->d_allocs.push_back(*p);
+    s->d_alloc_sz.push_back(sz);
     return 0;
 }
 
@@ -2268,8 +2375,24 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         FAIL(ERRCODE_DEVICE_FATAL, "cudaMallocHost failed");
     cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st);
 
+    /* inner relations built before for the same join_inner_handle and
+     * build inputs are used as they are */
+    xb_inner_entry *hit = nullptr;
+    uint64_t ikey = 0;
+    const uint64_t ihandle = ((const kern_session_info *)session)->join_inner_handle;
+    if (kmrels && plan->nrels > 0 && ihandle != 0) {
+        ikey = xb_inner_key(dev, ihandle, plan, kmrels_sz);
+        hit = xb_inner_cache_get(dev, ikey);
+        if (hit) {
+            for (uint32_t d = 1; d <= plan->nrels; d++)
+                plan->inner[d] = hit->inner[d];
+            s->inner_entry = hit;
+            s->inner_hit = true;
+        }
+    }
+    const size_t ia0 = s->d_allocs.size();
     /* inner relations: upload and build indexes */
-    if (kmrels && plan->nrels > 0) {
+    if (kmrels && plan->nrels > 0 && !hit) {
         DALLOC(kmrels_sz, &s->d_kmrels);
         if (cudaMemcpyAsync(s->d_kmrels, kmrels, kmrels_sz, cudaMemcpyHostToDevice, st) != cudaSuccess)
             FAIL(ERRCODE_DEVICE_FATAL, "inner buffer upload failed");
@@ -2313,6 +2436,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
             cudaMemsetAsync(in->nulls, 0, (size_t)nl * words * 4, st);
         }
     }
+    const size_t ia1 = s->d_allocs.size();
     /* group-by tables */
     if (plan->has_groupby) {
         double est = ((const kern_session_info *)s->h_session.data())->groupby_ngroups_estimation;
@@ -2347,7 +2471,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     cudaMemcpyAsync(s->d_plan, plan, sizeof(xb_plan), cudaMemcpyHostToDevice, st);
 
     /* build inner indexes on the device */
-    for (uint32_t d = 1; d <= plan->nrels; d++) {
+    for (uint32_t d = 1; !hit && d <= plan->nrels; d++) {
         XbBuildArgs ba;
         ba.kds = (const kern_data_store *)(s->d_kmrels + kmrels->chunks[d - 1].kds_offset);
         ba.in = &s->d_plan->inner[d];
@@ -2365,7 +2489,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     /* canonical text pointers for hashed text columns: equal strings of one
      * inner column share one address, so group keys taken from them compare
      * by pointer */
-    for (uint32_t d = 1; d <= plan->nrels; d++) {
+    for (uint32_t d = 1; !hit && d <= plan->nrels; d++) {
         const xb_inner *in = &plan->inner[d];
         for (uint32_t k = 0; k < in->nloads; k++) {
             if (!((in->hashed >> k) & 1u) || in->load[k].ld != XB_LD_TEXT || in->nitems == 0)
@@ -2392,7 +2516,10 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     /* dense group ids when every GROUP BY key is a column of one inner
      * relation; the specialised kernels then index the shared-memory group
      * table by id.  Needs the shared table to hold every id. */
-    if (s->h_plan->gid_depth >= 1 && s->h_plan->gid_depth <= plan->nrels && plan->gent_size > 0) {
+    const size_t ia2 = s->d_allocs.size();
+    if (hit && hit->gid_cap && s->sm_cap < hit->gid_cap)
+        s->sm_cap = hit->gid_cap;
+    if (!hit && s->h_plan->gid_depth >= 1 && s->h_plan->gid_depth <= plan->nrels && plan->gent_size > 0) {
         const uint32_t d = s->h_plan->gid_depth;
         xb_inner *in = &s->h_plan->inner[d];
         const uint32_t n = in->nitems;
@@ -2432,7 +2559,7 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     }
     /* direct-address tables for unique, dense 32-bit join keys (used by the
      * session-specialised kernels; the interpreter keeps probing the index) */
-    for (uint32_t d = 1; d <= plan->nrels; d++) {
+    for (uint32_t d = 1; !hit && d <= plan->nrels; d++) {
         xb_inner *in = &s->h_plan->inner[d];
         if (!in->key32 || !in->unique_hash || in->nindexed == 0 || in->dkey_max < in->dkey_min)
             continue;
@@ -2471,6 +2598,39 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     }
     if (cudaStreamSynchronize(st) != cudaSuccess)
         FAIL(ERRCODE_DEVICE_FATAL, "OpenSession: %s", cudaGetErrorString(cudaGetLastError()));
+    const size_t ia3 = s->d_allocs.size();
+    /* a new build with a handle goes into the cache: its device memory
+     * leaves the session's and stays while any session uses it */
+    if (!hit && ikey != 0) {
+        xb_inner_entry *e = new xb_inner_entry();
+        e->key = ikey;
+        e->nrels = plan->nrels;
+        for (uint32_t d = 0; d <= XB_MAX_DEPTH; d++)
+            e->inner[d] = s->h_plan->inner[d];
+        const uint32_t gd = s->h_plan->gid_depth;
+        e->gid_cap = (gd >= 1 && gd <= plan->nrels && s->h_plan->inner[gd].gid_on)
+            ? (uint32_t)xb_next_pow2(s->h_plan->inner[gd].ngids > 32 ? s->h_plan->inner[gd].ngids : 32) : 0;
+        std::vector<void *> keep_p;
+        std::vector<uint64_t> keep_sz;
+        for (size_t i = 0; i < s->d_allocs.size(); i++) {
+            if ((i >= ia0 && i < ia1) || (i >= ia2 && i < ia3)) {
+                e->allocs.push_back(s->d_allocs[i]);
+                e->bytes += s->d_alloc_sz[i];
+            } else {
+                keep_p.push_back(s->d_allocs[i]);
+                keep_sz.push_back(s->d_alloc_sz[i]);
+            }
+        }
+        s->d_allocs.swap(keep_p);
+        s->d_alloc_sz.swap(keep_sz);
+        s->d_kmrels = nullptr;
+        e->refs = 1;
+        std::lock_guard<std::mutex> g(dev->inner_lock);
+        e->last_use = ++dev->inner_clock;
+        dev->inner_cache.push_back(e);
+        dev->inner_bytes += e->bytes;
+        s->inner_entry = e;
+    }
 
     /* launch geometry */
     s->warp_bytes = (uint32_t)(XB_WARP_HEAD + sizeof(XbCursor) * plan->nrels + XB_REGS_BYTES(plan->nregs));
@@ -4666,6 +4826,22 @@ xpuB200DeviceFree(xpuB200Device *dev, void *dptr)
 }
 
 extern "C" int
+xpuB200InnerCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!dev)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid InnerCacheConfig arguments");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    std::lock_guard<std::mutex> g(dev->inner_lock);
+    if (max_bytes != UINT64_MAX)
+        dev->inner_budget = max_bytes;
+    xb_inner_evict_locked(dev);
+    if (p_cached_bytes)
+        *p_cached_bytes = dev->inner_bytes;
+    return 0;
+}
+
+extern "C" int
 xpuB200InnerRebuild(xpuB200Device *dev, kern_data_store *kds_dst, const kern_data_store *kds_src,
                     uint32_t hash_divisor, uint32_t hash_remainder, uint64_t *p_required, kern_errorbuf *err)
 {
@@ -4772,12 +4948,13 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
              "\"nkeys\": %u, \"naggs\": %u, \"gent_size\": %u, \"gtable_cap\": %llu, "
              "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u], "
              "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\", "
-             "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u}",
+             "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u, \"inner_cache\": %s}",
              p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
              p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
              s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash,
              s->jit_enabled ? "true" : "false", kinds.c_str(), s->jit_compile_ms, msg.c_str(),
-             s->jit_minb, s->sm_cap_default);
+             s->jit_minb, s->sm_cap_default,
+             s->inner_hit ? "\"hit\"" : s->inner_entry ? "\"built\"" : "\"none\"");
     return 0;
 }
 

@@ -212,7 +212,7 @@ def zipf_bounded(r, n, s, size):
     return (np.searchsorted(cdf, u, side="right") + 1).astype(np.int32)
 
 
-def join_groupby_session(flag_limit=3, sort=None):
+def join_groupby_session(flag_limit=3, sort=None, inner_handle=0):
     """fact JOIN dim1 ON fk1 = pk JOIN dim2 ON fk2 = pk AND flag < flag_limit
     GROUP BY region -> sum(qty * price), count(*)."""
     f_fk1, f_fk2, f_qty, f_price = (Var(0, 1, "int4"), Var(0, 2, "int4"),
@@ -227,7 +227,7 @@ def join_groupby_session(flag_limit=3, sort=None):
         groupby_keys=[d1_region],
         aggs=[Agg("PSUM_INT64", Func("int48mul", [f_qty, f_price], "int8")),
               Agg("NROWS_ANY")],
-        ngroups_estimate=25.0,
+        ngroups_estimate=25.0, join_inner_handle=inner_handle,
         **_sort_args(sort))
 
 

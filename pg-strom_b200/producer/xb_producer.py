@@ -891,7 +891,7 @@ class SessionBuilder:
     def build(self, *, scan_quals=None, joins=(), groupby_keys=(), aggs=(),
               ngroups_estimate=100.0, final_tlist=None, projection=None,
               htup_margin=0, projection_hash=None, proj_nslots=0, sort_keys=None,
-              sort_window=None, sort_limit=0) -> bytes:
+              sort_window=None, sort_limit=0, join_inner_handle=0) -> bytes:
         """joins: list of (outer_hash_keys, join_quals, other_quals) for
         depth 1..n.  groupby_keys: list of Expr; aggs: list of Agg.  The
         partial-aggregation target list is aggs then keys (gpu_preagg.c:
@@ -905,6 +905,7 @@ class SessionBuilder:
         blobs = {}
         self.htup_margin = htup_margin
         self.sort_limit = sort_limit
+        self.join_inner_handle = join_inner_handle
         if sort_keys:
             blobs["gpusort"] = build_sort_keys(sort_keys, sort_window)
         if scan_quals is not None:
@@ -1065,7 +1066,7 @@ class SessionBuilder:
                          offs["keyload"],
                          offs["keycomp"], offs["actions"], offs["gpusort"])
         struct.pack_into("<I", b, 128, offs["kds_dst"])
-        struct.pack_into("<I", b, 156, offs["kds_final"])
+        struct.pack_into("<II", b, 152, getattr(self, "join_inner_handle", 0), offs["kds_final"])
         struct.pack_into("<Ii", b, 168, getattr(self, "htup_margin", 0), getattr(self, "sort_limit", 0))
         struct.pack_into("<If", b, 160, 0, float(ngroups_estimate))
         struct.pack_into("<I", b, 188, nparams)

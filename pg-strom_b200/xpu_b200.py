@@ -49,6 +49,7 @@ def lib():
         L.xpuB200ExecTaskDst.argtypes = [P, P, I, P, U64, I, ctypes.POINTER(U64), P, EB]
         L.xpuB200Final.argtypes = [P, P, U64, ctypes.POINTER(U64), P, EB]
         L.xpuB200MergeFinal.argtypes = [P, P, I, EB]
+        L.xpuB200InnerCacheConfig.argtypes = [P, U64, ctypes.POINTER(U64), EB]
         L.xpuB200InnerRebuild.argtypes = [P, P, P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(U64), EB]
         L.xpuB200CloseSession.argtypes = [P]
         L.xpuB200HandleCommand.argtypes = [P, ctypes.POINTER(P), P, P, U64, P, U64]
@@ -116,6 +117,17 @@ class Device:
 
     def free(self, dptr):
         lib().xpuB200DeviceFree(self.h, ctypes.c_void_p(dptr))
+
+    def inner_cache(self, max_bytes=None):
+        """Set the budget of inner relations kept across sessions
+        (xpuB200InnerCacheConfig); returns the bytes cached now."""
+        e = KernErrorbuf()
+        got = ctypes.c_uint64()
+        rc = lib().xpuB200InnerCacheConfig(self.h, (1 << 64) - 1 if max_bytes is None else max_bytes,
+                                           ctypes.byref(got), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return got.value
 
     def inner_rebuild(self, dst, src, divisor=0, remainder=0):
         """Append the rows of the device chunk src (HASH or ROW, tuples
