@@ -59,6 +59,9 @@ def parse():
                          "serving scheduler")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="keep the default launch shape (no xpuB200BatchTune before timing)")
+    ap.add_argument("--final-merge", default="gather", choices=["gather", "exchange"],
+                    help="N>1: merge every rank's kds_final on rank 0 (gather), or split the groups "
+                         "by hash across the ranks (exchange: all-to-all, each rank merges its share)")
     ap.add_argument("--keys", type=int, default=10_000_000)
     ap.add_argument("--requests", type=int, default=400)
     ap.add_argument("--qps", type=float, default=200.0)
@@ -379,7 +382,20 @@ def run_b200(args, rank, world, local):
     # ---- N>1: every rank's kds_final merged on rank 0's GPU (the service's
     # final step over per-GPU results); checked against the ranks' row counts
     merge = None
-    if world > 1:
+    if world > 1 and args.final_merge == "exchange":
+        import xb_exchange as X
+        t0 = time.perf_counter()
+        share = X.exchange_final(dev, sess, final, rank, world, kmp, 2, device=f"cuda:{local}")
+        ms_x = max_over_ranks(1000.0 * (time.perf_counter() - t0), world)
+        mine = F.decode_kds_final(share, sess) if share is not None else {}
+        groups = sum_over_ranks(float(len(mine)), world)
+        rows = sum_over_ranks(float(sum(v[1] for v in mine.values())), world)
+        nout = sum_over_ranks(float(meta["nitems_out"]), world)
+        assert rows == nout, "exchanged row count"
+        merge = {"ranks": world, "groups": int(groups), "ms": ms_x,
+                 "includes": "split by hash % N on each GPU, all-to-all of the parts, MergeFinal of "
+                             "the received parts into a fresh session, Final"}
+    elif world > 1:
         finals = gather_finals(final, rank, world)
         nout = sum_over_ranks(float(meta["nitems_out"]), world)
         if rank == 0:

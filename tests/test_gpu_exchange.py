@@ -1,0 +1,81 @@
+"""The device side of the hash-partitioned multi-GPU merge, with three
+ranks emulated on one GPU: each rank's kds_final is split by hash % 3
+(xb_exchange.split_final, xpuB200InnerRebuild on group tuples) and rank r
+merges part r of every rank (xpuB200MergeFinal).  Every group must end on
+exactly one rank with the states of one session over all chunks; the
+exchange of the bytes between processes is tested with gloo ranks in
+test_multirank.py."""
+import struct
+
+import pytest
+
+import xb_configs as C
+import xb_exchange as X
+import xb_final as F
+import xpu_b200
+
+pytestmark = pytest.mark.gpu
+
+WORLD = 3
+
+
+def _finals(device, sess, chunks, km=None, nrels=0):
+    out = []
+    for r in range(WORLD):
+        s = xpu_b200.Session(device, sess, km, nrels)
+        try:
+            for ch in chunks[r::WORLD]:
+                s.exec(ch)
+            f, _ = s.final()
+        finally:
+            s.close()
+        out.append(f)
+    return out
+
+
+def _exchange(device, sess, finals, km=None, nrels=0):
+    parts = [X.split_final(device, sess, f, WORLD) for f in finals]
+    for s_, ps in enumerate(parts):
+        for r, p in enumerate(ps):
+            if p is None:
+                continue
+            # every tuple of part r hashes to r
+            n, = struct.unpack_from("<I", p, 16)
+            ncol, = struct.unpack_from("<I", p, 68)
+            nslots, = struct.unpack_from("<I", p, 40)
+            hl = (72 + 168 * ncol + 7) & ~7
+            length = len(p)
+            for i in range(n):
+                off, = struct.unpack_from("<Q", p, hl + 8 * nslots + 8 * i)
+                h, = struct.unpack_from("<I", p, length - off + 4)
+                assert h % WORLD == r
+    shares = [X.merge_parts(device, sess, [parts[s_][r] for s_ in range(WORLD)], km, nrels)
+              for r in range(WORLD)]
+    merged = {}
+    for f in shares:
+        d = F.decode_kds_final(f, sess) if f is not None else {}
+        assert not (set(d) & set(merged))              # a group lives on one rank only
+        merged.update(d)
+    return merged
+
+
+def test_exchange_wide_groupby(device):
+    tbl, sess, _, expect, meta = C.wide_groupby(nrows=300_000, ngroups=5000, seed_config=61)
+    chunks = tbl.block_chunks(pages_per_chunk=128)
+    merged = _exchange(device, sess, _finals(device, sess, chunks))
+    assert F.compare_groups(merged, expect) == []
+
+
+def test_exchange_arrow_many_groups(device):
+    chunks, sess, expect, meta = C.arrow_groupby(nrows=900_000, nkeys=300_000, rows_per_chunk=100_000,
+                                                 seed_config=62)
+    merged = _exchange(device, sess, _finals(device, sess, chunks))
+    assert F.compare_groups(merged, expect) == []
+
+
+def test_exchange_join_text_keys(device):
+    fact, sess, km, expect, meta = C.join_groupby(nfact=150_000, ndim1=5000, ndim2=700, seed_config=63)
+    chunks = fact.block_chunks(pages_per_chunk=100)
+    merged = _exchange(device, sess, _finals(device, sess, chunks, km, 2), km, 2)
+    truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+    assert F.compare_groups(merged, truth) == []

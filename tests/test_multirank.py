@@ -90,3 +90,49 @@ def test_two_gloo_ranks():
     # shards differ: the first groups' states are not identical across ranks
     objs = res[0][4]
     assert objs[0][2] != objs[1][2]
+
+
+def _a2a_worker(rank, world, port, q):
+    for sub in ("pg-strom_b200", os.path.join("pg-strom_b200", "producer"), "oracle", ""):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    import numpy as np
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        import xb_exchange as X
+        # part r of rank s: (s, r) repeated s + r + 1 times; rank 1 sends nothing to rank 0
+        parts = []
+        for r in range(world):
+            if rank == 1 and r == 0:
+                parts.append(None)
+            else:
+                parts.append(np.full(7 * (rank + r + 1), 16 * rank + r, dtype=np.uint8))
+        got = X.alltoall_bytes(parts, rank, world)
+        q.put((rank, [None if g is None else (len(g), int(g[0]), bool((g == g[0]).all())) for g in got]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_alltoall_of_final_parts_over_gloo():
+    """The byte exchange of the hash-partitioned final merge: every rank
+    receives, in rank order, exactly the part each rank addressed to it."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    world = 3
+    procs = [ctx.Process(target=_a2a_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in range(world):
+        for s_, g in enumerate(res[r]):
+            if s_ == 1 and r == 0:
+                assert g is None
+            else:
+                assert g == (7 * (s_ + r + 1), 16 * s_ + r, True)
