@@ -241,12 +241,13 @@ def build_workload(nrows, rank):
 
 
 # ------------------------------------------------------------------ CPU arms
-def cpu_rows_per_sec(sess, km, chunks, seconds, threads):
+def cpu_rows_per_sec(sess, km, chunks, seconds, threads, allow_ref=True):
     """Runs the reference's host-compiled functions (or the C oracle) over
-    chunks on 'threads' threads until 'seconds' of wall time; rows/s."""
+    chunks on 'threads' threads until 'seconds' of wall time; rows/s.  The
+    reference harness reads heap chunks only (allow_ref=False for Arrow)."""
     import ref_pin
     import xb_oracle as O
-    use_ref = ref_pin.available()
+    use_ref = allow_ref and ref_pin.available()
     kind = "reference" if use_ref else "port"
     lock = threading.Lock()
     state = {"rows": 0, "next": 0}
@@ -469,29 +470,62 @@ def run_b200(args, rank, world, local):
 
 
 # ------------------------------------------------------------------ other configurations
+def _config_workload(args, nrows):
+    """(chunks, session, truth or None, meta, description, referenced bytes)
+    of the scan or Arrow configuration at nrows"""
+    import xb_configs as C
+    if args.workload == "scan_groupby":
+        tbl, sess, _, expect, meta = C.scan_groupby(nrows=nrows)
+        chunks = tbl.block_chunks(pages_per_chunk=8190)
+        desc = (f"plain scan + filter + group-by over heap pages: {nrows} rows, WHERE a < 300 "
+                "GROUP BY g (64 groups) -> count, sum(a), sum(c numeric), avg(b)")
+        truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
+        return chunks, sess, truth, meta, desc, sum(c.nbytes for c in chunks)
+    chunks, sess, _, meta = C.arrow_groupby(nrows=nrows, nkeys=args.keys, with_expect=False)
+    desc = (f"Arrow high-cardinality pre-aggregation: {nrows} rows, {args.keys} keys, 2-year date "
+            "window -> GROUP BY k: count, sum(v1), min/max/sum(v2)")
+    return chunks, sess, None, meta, desc, 24 * nrows
+
+
+def run_reference_config(args):
+    """The reference arm of the scan and Arrow configurations: the
+    reference's host-compiled functions (heap) or the C restatement (Arrow,
+    which the reference harness does not read) on every host thread, over
+    a bounded sample of the same workload per step."""
+    nrows = min(args.rows, 20_000_000)
+    chunks, sess, _, meta, desc, _ = _config_workload(args, nrows)
+    threads = os.cpu_count() or 1
+    heap = args.workload == "scan_groupby"
+    per_step = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_rows_per_sec(sess, None, chunks, per_step / 2, threads, allow_ref=heap)
+    total_rows, total_s, kind = 0, 0.0, "port"
+    for _ in range(args.steps):
+        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks, per_step, threads, allow_ref=heap)
+        total_rows += rows
+        total_s += el
+    value = total_rows / total_s
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic", "config": {"workload": desc + " (bounded sample per step)",
+                                            "rows_generated": nrows, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{total_rows} rows over {total_s:.1f} s ({per_step:.1f} s per step)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_config(args):
     """One persistent launch per pass over resident chunks of the plain
     scan + group-by table (heap) or the Arrow high-cardinality table;
     rows/s and the referenced bytes against HBM bandwidth."""
     import torch
-    import xb_configs as C
     import xpu_b200
     t0 = time.time()
-    if args.workload == "scan_groupby":
-        tbl, sess, _, expect, meta = C.scan_groupby(nrows=args.rows)
-        chunks = tbl.block_chunks(pages_per_chunk=8190)
-        nbytes = sum(c.nbytes for c in chunks)
-        ref_bytes = nbytes
-        desc = (f"plain scan + filter + group-by over heap pages: {args.rows} rows, WHERE a < 300 "
-                "GROUP BY g (64 groups) -> count, sum(a), sum(c numeric), avg(b)")
-        truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
-    else:
-        chunks, sess, _, meta = C.arrow_groupby(nrows=args.rows, nkeys=args.keys, with_expect=False)
-        nbytes = sum(c.nbytes for c in chunks)
-        ref_bytes = 24 * args.rows            # k, v1, v2, d: the referenced columns
-        desc = (f"Arrow high-cardinality pre-aggregation: {args.rows} rows, {args.keys} keys, 2-year date "
-                "window -> GROUP BY k: count, sum(v1), min/max/sum(v2)")
-        truth = None
+    # heap: every chunk byte; Arrow: k, v1, v2, d, the referenced columns
+    chunks, sess, truth, meta, desc, ref_bytes = _config_workload(args, args.rows)
+    nbytes = sum(c.nbytes for c in chunks)
     gen_s = time.time() - t0
     dev = xpu_b200.Device(0)
     s = xpu_b200.Session(dev, sess)
@@ -529,6 +563,13 @@ def run_config(args):
                          "kernel": ("xbj_kernel" if "jit" in info["kernels"].values() else "xb_exec_kernel"),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
             "clocks": clocks, "gpu_launches": args.steps}
+    if args.cpu_seconds > 0:
+        threads = os.cpu_count() or 1
+        heap = args.workload == "scan_groupby"
+        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks[:8], args.cpu_seconds, threads, allow_ref=heap)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": f"{rows} rows of the same workload in {el:.1f} s on {threads} threads "
+                                          f"({'PG-Strom expression library host-compiled from the reference' if kind == 'reference' else 'C restatement'})"}
     print(json.dumps(line), flush=True)
     batch.close()
     s.close()
@@ -810,6 +851,8 @@ def main():
     args = parse()
     if args.workload != "join_groupby":
         if args.impl == "reference":
+            if args.workload in ("scan_groupby", "arrow_groupby"):
+                return run_reference_config(args)
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served "
                                                                   "form of this path"}), flush=True)
             return
