@@ -232,7 +232,7 @@ def join_groupby_session(flag_limit=3, sort=None, inner_handle=0):
 
 
 def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3,
-                 key_stride=1, dim1_copies=1, miss_frac=0.0, with_rows=False):
+                 key_stride=1, dim1_copies=1, miss_frac=0.0, with_rows=False, price_hi=1_000_000):
     """Two-way hash join + group-by.  Defaults give the headline workload:
     dense unique dimension keys 1..n, every fact row matching.  Variants for
     the join paths: key_stride spreads the keys (k * stride; sparse keys
@@ -258,7 +258,7 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
     fk1 = rf.integers(1, ndim1 + 1, nfact, dtype=np.int32)
     fk2 = zipf_bounded(rf, ndim2, 1.1, nfact)
     qty = rf.integers(1, 51, nfact, dtype=np.int32)
-    price = rf.integers(100, 1_000_001, nfact, dtype=np.int64)
+    price = rf.integers(100, price_hi + 1, nfact, dtype=np.int64)
     idx1 = fk1.astype(np.int64) - 1
     idx2 = fk2.astype(np.int64) - 1
     miss = np.zeros(nfact, dtype=bool)

@@ -1,0 +1,60 @@
+"""The error and suspend protocol on the GPU (kern_errorbuf codes): an
+expression error in a row stops the chunk with the reference's message,
+as the oracle does; a group table with no room left returns
+ERRCODE_SUSPEND_NO_SPACE instead of losing groups; and a session stays
+usable for the caller to close after either.  Both kernels."""
+import pytest
+
+import xb_configs as C
+import xb_oracle as O
+import xpu_b200
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=["jit", "vm"])
+def kernel(request, monkeypatch):
+    monkeypatch.setenv("XPU_B200_JIT", "1" if request.param == "jit" else "0")
+    return request.param
+
+
+def test_int8_overflow_in_join_expression(device, kernel):
+    # qty * price with price up to 4e17 and qty up to 50 leaves int8
+    fact, sess, km, _, _ = C.join_groupby(nfact=50_000, ndim1=2000, ndim2=300, seed_config=71,
+                                          price_hi=400_000_000_000_000_000)
+    chunks = fact.block_chunks(pages_per_chunk=64)
+    o = O.Oracle(sess, km)
+    with pytest.raises(Exception, match="out of range"):
+        for ch in chunks:
+            o.exec(ch)
+    o.close()
+    s = xpu_b200.Session(device, sess, km, 2)
+    try:
+        with pytest.raises(xpu_b200.XpuB200Error, match="integer value out of range"):
+            for ch in chunks:
+                s.exec(ch)
+    finally:
+        s.close()
+
+
+def test_group_table_without_room_suspends(device, kernel):
+    # 60,000 groups into a session sized for one (a 2,048-slot table)
+    tbl, _, _, _, _ = C.scan_groupby(nrows=200_000, ngroups=60_000, a_limit=1000, seed_config=72)
+    sess = C.scan_groupby_session(a_limit=1000, ngroups=1)
+    s = xpu_b200.Session(device, sess)
+    try:
+        with pytest.raises(xpu_b200.XpuB200Error) as ei:
+            for ch in tbl.block_chunks(pages_per_chunk=256):
+                s.exec(ch)
+        assert ei.value.errcode == ord("d") or "no space" in str(ei.value), str(ei.value)
+    finally:
+        s.close()
+    # a new session of the same plan with a fitting estimate runs
+    s2 = xpu_b200.Session(device, C.scan_groupby_session(a_limit=1000, ngroups=60_000))
+    try:
+        for ch in tbl.block_chunks(pages_per_chunk=256):
+            s2.exec(ch)
+        final, res = s2.final()
+        assert res["final_nitems"] > 50_000
+    finally:
+        s2.close()
