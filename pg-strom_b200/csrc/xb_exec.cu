@@ -2129,6 +2129,18 @@ struct xpuB200Session {
     int             jit_minb = 0;
     uint32_t        sm_cap_default = 0;
     bool            tune_looked_up = false;
+    /* partitioned aggregation: deferred rows bucketed by table slot */
+    void           *jit_replay[256] = {nullptr};
+    int             jit_replay_grid[256] = {0};
+    char           *part_buf = nullptr;
+    uint32_t       *part_cnt = nullptr;
+    uint64_t        part_bytes = 0;
+    uint32_t        part_cap = 0;
+    uint32_t        part_shift = 0;
+    uint32_t        nparts = 0;
+    uint32_t        part_rec = 0;
+    bool            part_used = false;
+    bool            in_batch = false;       /* a prepared batch's launch is being issued */
 };
 
 /* shared group-table capacity 'cap' and the launch geometry that follows
@@ -2296,6 +2308,8 @@ static void xb_session_free(xpuB200Session *s)
     if (s->d_src) cudaFreeAsync(s->d_src, st);
     if (s->d_tasks) cudaFreeAsync(s->d_tasks, st);
     if (s->d_dst) cudaFreeAsync(s->d_dst, st);
+    if (s->part_buf) cudaFreeAsync(s->part_buf, st);
+    if (s->part_cnt) cudaFreeAsync(s->part_cnt, st);
     cudaStreamSynchronize(st);
     if (s->inner_entry)
         xb_inner_cache_put(s->dev, s->inner_entry);
@@ -2772,7 +2786,7 @@ static void *xb_session_jit(xpuB200Session *s, uint32_t format)
         double ms = 0.0;
         int per_sm = 0, mix_sm = 0;
         if (xb_jit_compile_minb(s->h_plan, format, s->dev->dindex, s->jit_minb, &s->jit_fn[format],
-                                &s->jit_mixfn[format], &ms, msg, sizeof(msg)) != 0) {
+                                &s->jit_mixfn[format], &s->jit_replay[format], &ms, msg, sizeof(msg)) != 0) {
             s->jit_fn[format] = nullptr;
             s->jit_mixfn[format] = nullptr;
             s->jit_msg = msg;
@@ -2788,6 +2802,10 @@ static void *xb_session_jit(xpuB200Session *s, uint32_t format)
                                &mix_sm) != 0)
                 s->jit_mixfn[format] = nullptr;
             s->jit_grid[format] = per_sm * s->dev->nsm;
+            int rp = 0;
+            if (s->jit_replay[format] && xb_jit_prepare(s->jit_replay[format], XB_BLOCK, 0, &rp) != 0)
+                s->jit_replay[format] = nullptr;
+            s->jit_replay_grid[format] = rp * s->dev->nsm;
             s->jit_compile_ms += ms;
             s->jit_msg = "ok";
         }
@@ -2801,11 +2819,75 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
     return xb_launch_on(s, d_tasks, ntasks, nunits, format, s->stream, s->d_status, err);
 }
 
+/* partitioned aggregation for this launch: a keyed GROUP BY whose groups
+ * live in a global table larger than L2 defers each row's update into the
+ * bucket of its table slot; the buckets cover slices of the table small
+ * enough to stay in L2 while the replay works on them.  Rows past a full
+ * bucket are updated in place, so any bucket size is correct.  Used by
+ * prepared batches whose table is several times L2 (the records of a batch
+ * take device memory in proportion to its rows, which the serving path's
+ * admission does not budget); XPU_B200_PARTITION=1 uses it for every
+ * launch over a table above 64 MB, =0 never.  Session lock held.  Returns
+ * whether it is used. */
+static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format, cudaStream_t stream)
+{
+    const char *env = getenv("XPU_B200_PARTITION");
+    const bool force = env && env[0] == '1';
+    if ((env && env[0] == '0') || (!force && !s->in_batch))
+        return false;
+    const xb_plan *plan = s->h_plan;
+    if (plan->has_groupby != 1 || s->sm_cap != 0)
+        return false;
+    const uint32_t rec = xb_jit_part_rec_size(plan);
+    const uint64_t cap = s->h_gt.cap_mask + 1;
+    const uint64_t table = cap * plan->gent_size;
+    if (rec == 0 || table <= (force ? (64ULL << 20) : (512ULL << 20)))
+        return false;
+    /* buckets of about 16 MB of table, at most 4096 */
+    uint64_t np = 8;
+    while (np < 4096 && table / np > (16ULL << 20) && np * 2 <= cap)
+        np *= 2;
+    uint32_t lg_cap = 0, lg_np = 0;
+    while ((1ULL << lg_cap) < cap) lg_cap++;
+    while ((1ULL << lg_np) < np) lg_np++;
+    const uint64_t rows = format == KDS_FORMAT_BLOCK ? nunits * 291ULL : nunits * (uint64_t)XB_ROWS_UNIT;
+    uint64_t per = (rows + rows / 4) / np + 1024;
+    /* at most a quarter of the device budget for the records */
+    const uint64_t limit = s->dev->hbm_budget / 4;
+    if (per * np * rec > limit)
+        per = limit / (np * rec);
+    if (per < 1024 || per > 0xffffffffULL)
+        return false;
+    const uint64_t bytes = per * np * rec;
+    if (!s->part_buf || s->part_bytes < bytes || s->nparts != np) {
+        if (s->part_buf) cudaFreeAsync(s->part_buf, stream);
+        if (s->part_cnt) cudaFreeAsync(s->part_cnt, stream);
+        s->part_buf = nullptr;
+        s->part_cnt = nullptr;
+        s->part_bytes = 0;
+        if (cudaMallocAsync((void **)&s->part_buf, bytes, stream) != cudaSuccess ||
+            cudaMallocAsync((void **)&s->part_cnt, sizeof(uint32_t) * XB_PART_CNT_STRIDE * np, stream) != cudaSuccess) {
+            cudaGetLastError();
+            if (s->part_buf) cudaFreeAsync(s->part_buf, stream);
+            s->part_buf = nullptr;
+            s->part_cnt = nullptr;
+            return false;
+        }
+        s->part_bytes = bytes;
+    }
+    s->part_cap = (uint32_t)(s->part_bytes / (np * rec));
+    s->nparts = (uint32_t)np;
+    s->part_shift = lg_cap - lg_np;
+    s->part_rec = rec;
+    return true;
+}
+
 static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                         uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
                         kern_errorbuf *err)
 {
     XbExecArgs a;
+    memset(&a, 0, sizeof(a));
     a.plan = s->d_plan;
     a.plan_bytes = s->plan_bytes;
     a.tasks = d_tasks;
@@ -2828,9 +2910,30 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     if (grid < 1) grid = 1;
     if (format < 256)
         s->ran_kind[format] = fn ? 'j' : 'v';
+    const bool part = fn && s->jit_replay[format] && xb_part_prepare(s, nunits, format, stream);
+    if (part) {
+        a.part_buf = s->part_buf;
+        a.part_cnt = s->part_cnt;
+        a.part_cap = s->part_cap;
+        a.part_shift = s->part_shift;
+        cudaMemsetAsync(s->part_cnt, 0, sizeof(uint32_t) * XB_PART_CNT_STRIDE * s->nparts, stream);
+        s->part_used = true;
+    }
     if (fn) {
         if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem_fmt[format], (void *)stream, &a) != 0)
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
+        if (part) {
+            XbReplayArgs ra;
+            ra.plan = s->d_plan;
+            ra.gt = s->d_gt;
+            ra.st = d_status;
+            ra.part_buf = s->part_buf;
+            ra.part_cnt = s->part_cnt;
+            ra.part_cap = s->part_cap;
+            ra.nparts = s->nparts;
+            if (xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK, 0, (void *)stream, &ra) != 0)
+                return XB_ERR(err, ERRCODE_DEVICE_FATAL, "replay kernel launch failed");
+        }
     } else {
         xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, stream>>>(a);
     }
@@ -3699,7 +3802,9 @@ xpuB200BatchExec(xpuB200Batch *b, kern_exec_results *results, kern_errorbuf *err
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
     XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
+    s->in_batch = true;
     int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
+    s->in_batch = false;
     if (rc) return rc;
     return xb_finish_task(s, results, err);
 }
@@ -3716,7 +3821,9 @@ xpuB200BatchTime(xpuB200Batch *b, int niters, double *p_msec, kern_errorbuf *err
     for (int i = 0; i < niters; i++) {
         XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
         cudaEventRecord(s->ev0, st);
+        s->in_batch = true;
         int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
+        s->in_batch = false;
         if (rc) return rc;
         cudaEventRecord(s->ev1, st);
         rc = xb_finish_task(s, nullptr, err);
@@ -3791,7 +3898,9 @@ xpuB200BatchTune(xpuB200Batch *b, uint32_t flags, char *report, size_t report_le
         for (int r = 0; r < 3 && rc == 0; r++) {      /* the first run builds and warms */
             xb_reset_groups(s);
             cudaEventRecord(s->ev0, st);
+            s->in_batch = true;
             rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, fmt, err);
+            s->in_batch = false;
             if (rc) break;
             cudaEventRecord(s->ev1, st);
             rc = xb_wait_status(s, err);
@@ -4948,13 +5057,15 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
              "\"nkeys\": %u, \"naggs\": %u, \"gent_size\": %u, \"gtable_cap\": %llu, "
              "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u], "
              "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\", "
-             "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u, \"inner_cache\": %s}",
+             "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u, \"inner_cache\": %s, "
+             "\"partitions\": %u, \"partition_used\": %s}",
              p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
              p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
              s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash,
              s->jit_enabled ? "true" : "false", kinds.c_str(), s->jit_compile_ms, msg.c_str(),
              s->jit_minb, s->sm_cap_default,
-             s->inner_hit ? "\"hit\"" : s->inner_entry ? "\"built\"" : "\"none\"");
+             s->inner_hit ? "\"hit\"" : s->inner_entry ? "\"built\"" : "\"none\"",
+             s->nparts, s->part_used ? "true" : "false");
     return 0;
 }
 

@@ -545,7 +545,27 @@ struct XbExecArgs {
     xb_status      *st;
     uint32_t        dyn_only;       /* claim every unit dynamically (CTAs join
                                      * the launch at any time: mixed launches) */
+    uint32_t        part_cap;       /* partitioned aggregation: records per bucket */
+    char           *part_buf;       /* bucket-major records, or nullptr (update in place) */
+    uint32_t       *part_cnt;       /* records claimed per bucket */
+    uint32_t        part_shift;     /* bucket = (hash & table mask) >> part_shift */
     uint32_t        __pad;
+};
+
+/* bucket counters of partitioned aggregation sit one per 128-byte line:
+ * every aggregated row claims its slot with an atomic on its bucket's
+ * counter, and counters sharing a line would serialise in one L2 slice */
+#define XB_PART_CNT_STRIDE  32
+
+/* the replay launch of partitioned aggregation (xbj_replay) */
+struct XbReplayArgs {
+    const xb_plan  *plan;
+    xb_gtable      *gt;
+    xb_status      *st;
+    const char     *part_buf;
+    const uint32_t *part_cnt;
+    uint32_t        part_cap;
+    uint32_t        nparts;
 };
 
 /* largest existence bitmap of a direct depth (keys), 16 KB */

@@ -38,7 +38,14 @@ int xb_jit_compile(const xb_plan *plan, uint32_t format, int dindex,
 /* xb_jit_compile for kernels bounded to min_blocks resident CTAs of 256
  * threads per SM (1..8; 0: the default) */
 int xb_jit_compile_minb(const xb_plan *plan, uint32_t format, int dindex, int min_blocks,
-                        void **p_func, void **p_mixfn, double *p_compile_ms, char *errbuf, size_t errlen);
+                        void **p_func, void **p_mixfn, void **p_replay, double *p_compile_ms,
+                        char *errbuf, size_t errlen);
+
+/* bytes of one deferred-row record of partitioned aggregation for plan
+ * (0: the plan does not defer its group updates); the replay kernel is
+ * xbj_replay (parameter block XbReplayArgs), returned by
+ * xb_jit_compile_minb's p_replay */
+uint32_t xb_jit_part_rec_size(const xb_plan *plan);
 
 /* a key naming the plan shape of plan + format: sessions whose specialised
  * kernels differ only in their launch bounds share it */

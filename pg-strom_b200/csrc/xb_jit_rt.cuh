@@ -38,6 +38,10 @@ struct XbjEnv {
     char           *dst;            /* projection: kds_dst and its length */
     uint64_t        dst_len;
     const uint32_t *sbits;          /* existence bitmaps in shared memory */
+    char           *part_buf;       /* partitioned aggregation (XbExecArgs) */
+    uint32_t       *part_cnt;
+    uint32_t        part_cap;
+    uint32_t        part_shift;
 };
 
 /* per-thread counters, 32-bit to spare registers; flushed into the launch
@@ -105,6 +109,12 @@ __device__ __forceinline__ void xbj_prefetch_tuple(const uint8_t *page, uint32_t
 
 __device__ __forceinline__ void
 xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
+
+#ifdef XBJ_PART
+/* generated: a deferred row's record, and the group update of one row */
+__device__ __forceinline__ void xbj_rec_load(const char *rec, XbjRegs &R, uint32_t &ghash);
+__device__ __forceinline__ void xbj_group_row(XbjRegs &R, const XbjEnv &E, const uint32_t ghash, bool &failed);
+#endif
 
 #ifdef XBJ_MERGE_SM
 /* generated: merge of a shared-table entry (shared form) into the global
@@ -212,6 +222,10 @@ xbj_body(const XbExecArgs &args, char *smem)
     E.dst = args.dst;
     E.dst_len = args.dst_len;
     E.sbits = sbits;
+    E.part_buf = args.part_buf;
+    E.part_cnt = args.part_cnt;
+    E.part_cap = args.part_cap;
+    E.part_shift = args.part_shift;
     XbjCnt C;
     C.raw = C.in = C.out = 0;
     C.gready = 0;
@@ -409,5 +423,46 @@ xbj_mixed_kernel(const __grid_constant__ XbMixArgs m)
         __syncthreads();
     }
 }
+
+#ifdef XBJ_PART
+/* replay of the deferred rows, bucket after bucket: the grid sweeps the
+ * bucket-major record array in order, so the CTAs work on neighbouring
+ * buckets together and the slice of the group table they update (the
+ * buckets are ranges of table slots) stays in L2 */
+extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
+xbj_replay(const __grid_constant__ XbReplayArgs args)
+{
+    XbjEnv E;
+    E.plan = args.plan;
+    E.st = args.st;
+    E.gt = args.gt;
+    E.gt_entries = args.gt->entries;
+    E.gt_mask = args.gt->cap_mask;
+    E.sm_tab = nullptr;
+    E.sm_mask = 0;
+    E.lane = threadIdx.x & 31;
+    E.dst = nullptr;
+    E.dst_len = 0;
+    E.sbits = nullptr;
+    E.part_buf = nullptr;
+    E.part_cnt = nullptr;
+    E.part_cap = 0;
+    E.part_shift = 0;
+    const uint64_t total = (uint64_t)args.nparts * args.part_cap;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = (uint32_t)(i / args.part_cap);
+        const uint32_t slot = (uint32_t)(i - (uint64_t)b * args.part_cap);
+        const uint32_t n = args.part_cnt[b * XB_PART_CNT_STRIDE];
+        if (slot >= (n < args.part_cap ? n : args.part_cap))
+            continue;
+        XbjRegs R;
+        uint32_t ghash;
+        xbj_rec_load(args.part_buf + i * XBJ_REC_SIZE, R, ghash);
+        bool failed = false;
+        xbj_group_row(R, E, ghash, failed);
+    }
+}
+#endif
 
 #endif  /* XB_JIT_RT_CUH */

@@ -1,0 +1,56 @@
+"""Partitioned aggregation: a keyed GROUP BY into a global table several
+times L2 defers every row's group update as a record bucketed by table
+slot and replays the buckets in order (prepared batches by default,
+XPU_B200_PARTITION=1 forces it, =0 disables it).  The groups must be those
+of the in-place path: integer and numeric states exact, float states
+within the float tolerance, on every partial-state form."""
+import pytest
+
+import xb_configs as C
+import xb_final as F
+import xpu_b200
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(device, sess, chunks):
+    s = xpu_b200.Session(device, sess)
+    try:
+        ups = [device.upload(c) for c in chunks]
+        b = s.batch([p for _, p in ups])
+        b.exec()
+        b.close()
+        final, res = s.final()
+        info = s.info()
+    finally:
+        s.close()
+        for base, _ in ups:
+            device.free(base)
+    return final, info
+
+
+def test_partitioned_arrow_groupby(device, monkeypatch):
+    monkeypatch.delenv("XPU_B200_PARTITION", raising=False)     # the default: on for this batch
+    chunks, sess, expect, meta = C.arrow_groupby(nrows=3_000_000, nkeys=1_000_000, rows_per_chunk=500_000,
+                                                 seed_config=81)
+    final, info = _run(device, sess, chunks)
+    assert info["partition_used"] and info["partitions"] >= 8, info
+    assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
+
+
+def test_partitioned_every_state_form(device, monkeypatch):
+    monkeypatch.setenv("XPU_B200_PARTITION", "1")
+    tbl, _, _, expect, meta = C.wide_groupby(nrows=300_000, ngroups=3000, seed_config=82)
+    sess = C.wide_groupby_session(ngroups=2_000_000)          # a table far larger than L2
+    final, info = _run(device, sess, tbl.block_chunks(pages_per_chunk=256))
+    assert info["partition_used"], info
+    assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
+
+
+def test_in_place_without_the_switch(device, monkeypatch):
+    monkeypatch.setenv("XPU_B200_PARTITION", "0")
+    chunks, sess, expect, meta = C.arrow_groupby(nrows=1_000_000, nkeys=300_000, rows_per_chunk=500_000,
+                                                 seed_config=83)
+    final, info = _run(device, sess, chunks)
+    assert not info["partition_used"]
+    assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
