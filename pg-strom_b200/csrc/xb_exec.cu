@@ -2856,6 +2856,9 @@ static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format,
     const uint64_t limit = s->dev->hbm_budget / 4;
     if (per * np * rec > limit)
         per = limit / (np * rec);
+    /* the replay numbers records in 32 bits */
+    if (per * np > (1ULL << 31))
+        per = (1ULL << 31) / np;
     if (per < 1024 || per > 0xffffffffULL)
         return false;
     const uint64_t bytes = per * np * rec;

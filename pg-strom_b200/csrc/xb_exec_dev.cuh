@@ -556,6 +556,7 @@ struct XbExecArgs {
  * every aggregated row claims its slot with an atomic on its bucket's
  * counter, and counters sharing a line would serialise in one L2 slice */
 #define XB_PART_CNT_STRIDE  32
+#define XB_PART_MAX         4096    /* buckets of one partitioned launch */
 
 /* the replay launch of partitioned aggregation (xbj_replay) */
 struct XbReplayArgs {

@@ -448,14 +448,51 @@ xbj_replay(const __grid_constant__ XbReplayArgs args)
     E.part_cnt = nullptr;
     E.part_cap = 0;
     E.part_shift = 0;
-    const uint64_t total = (uint64_t)args.nparts * args.part_cap;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = (uint32_t)(i / args.part_cap);
-        const uint32_t slot = (uint32_t)(i - (uint64_t)b * args.part_cap);
+    /* the records of every bucket, numbered in bucket order: pre[b] is the
+     * number of records before bucket b (bucket counts clipped to the
+     * bucket size; counts past it were updated in place) */
+    __shared__ uint32_t pre[XB_PART_MAX + 1];
+    __shared__ uint32_t wsum[XB_WARPS];
+    const uint32_t np = args.nparts;
+    const uint32_t per_t = (np + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = threadIdx.x * per_t;
+    uint32_t mine = 0;
+    for (uint32_t b = b0; b < b0 + per_t && b < np; b++) {
         const uint32_t n = args.part_cnt[b * XB_PART_CNT_STRIDE];
-        if (slot >= (n < args.part_cap ? n : args.part_cap))
-            continue;
+        mine += n < args.part_cap ? n : args.part_cap;
+    }
+    /* exclusive scan of the per-thread sums over the CTA */
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = mine;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(XB_FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31)
+        wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (uint32_t w = 0; w < warp; w++)
+        before += wsum[w];
+    uint32_t run = before + incl - mine;
+    for (uint32_t b = b0; b < b0 + per_t && b < np; b++) {
+        pre[b] = run;
+        const uint32_t n = args.part_cnt[b * XB_PART_CNT_STRIDE];
+        run += n < args.part_cap ? n : args.part_cap;
+    }
+    if (threadIdx.x == blockDim.x - 1)
+        pre[np] = before + incl;
+    __syncthreads();
+    const uint32_t total = pre[np];
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+        /* the bucket of record v: the last b with pre[b] <= v */
+        uint32_t lo = 0, hi = np - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= v) lo = mid; else hi = mid - 1;
+        }
+        const uint64_t i = (uint64_t)lo * args.part_cap + (v - pre[lo]);
         XbjRegs R;
         uint32_t ghash;
         xbj_rec_load(args.part_buf + i * XBJ_REC_SIZE, R, ghash);

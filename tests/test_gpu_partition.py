@@ -31,8 +31,10 @@ def _run(device, sess, chunks):
 
 def test_partitioned_arrow_groupby(device, monkeypatch):
     monkeypatch.delenv("XPU_B200_PARTITION", raising=False)     # the default: on for this batch
-    chunks, sess, expect, meta = C.arrow_groupby(nrows=3_000_000, nkeys=1_000_000, rows_per_chunk=500_000,
-                                                 seed_config=81)
+    chunks, _, expect, meta = C.arrow_groupby(nrows=3_000_000, nkeys=1_000_000, rows_per_chunk=500_000,
+                                              seed_config=81)
+    # a 10M-group estimate: a 3.6 GB table, far beyond L2
+    sess = C.arrow_groupby_session(ngroups_estimate=10_000_000.0)
     final, info = _run(device, sess, chunks)
     assert info["partition_used"] and info["partitions"] >= 8, info
     assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
