@@ -56,3 +56,25 @@ def test_in_place_without_the_switch(device, monkeypatch):
     final, info = _run(device, sess, chunks)
     assert not info["partition_used"]
     assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
+
+
+def test_partitioned_text_keys(device, monkeypatch):
+    # GROUP BY a text column (the record carries the key's length) with a
+    # large estimate, against the oracle
+    import xb_oracle as O
+    from xb_producer import Agg, SessionBuilder, Var
+    monkeypatch.setenv("XPU_B200_PARTITION", "1")
+    fact, _, km, _, meta = C.join_groupby(nfact=1000, ndim1=200_000, ndim2=70, seed_config=84)
+    dim1 = meta["dims"]["dim1"]
+    sess = SessionBuilder(0, C.DEVTASK_PREAGG | C.DEVKIND_GPU).build(
+        groupby_keys=[Var(0, 2, "text")], aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Var(0, 1, "int4"))],
+        ngroups_estimate=2_000_000.0)
+    chunks = dim1.block_chunks(pages_per_chunk=256)
+    final, info = _run(device, sess, chunks)
+    assert info["partition_used"], info
+    o = O.Oracle(sess)
+    for ch in chunks:
+        o.exec(ch)
+    want = F.decode_kds_final(o.final(), sess)
+    o.close()
+    assert F.compare_groups(F.decode_kds_final(final, sess), want) == []
