@@ -237,6 +237,7 @@ def build_workload(nrows, rank):
     import xb_configs as C
     fact, sess, km, expect, meta = C.join_groupby(nfact=nrows, seed_config=shard_seed(rank))
     chunks = fact.block_chunks(pages_per_chunk=8190)
+    meta["truth"] = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
     return fact, sess, km, chunks, meta
 
 
@@ -351,6 +352,17 @@ def run_b200(args, rank, world, local):
               else "xb_exec_kernel (interpreter)")
     batch.close()
     s.close()
+    # parity at full size: one pass of the timed batch path on a fresh
+    # session, its kds_final decoded and compared with the generator's
+    # per-region truth (int128 sums and counts, exact)
+    sp = xpu_b200.Session(dev, sess, km, 2)
+    bp = sp.batch([p for _, p in ups])
+    bp.exec()
+    bp.close()
+    final_b, _ = sp.final()
+    sp.close()
+    batch_errs = F.compare_groups(F.decode_kds_final(final_b, sess), meta["truth"], rtol=0.0)
+    assert batch_errs == [], batch_errs[:3]
 
     # ---- e2e: whole query through the C ABI from pinned host memory
     pinned = []
@@ -379,6 +391,12 @@ def run_b200(args, rank, world, local):
             e2e_times.append(el)
     e2e_el = max_over_ranks(sum(e2e_times) / len(e2e_times), world)
     e2e_value = rows_total / e2e_el
+    e2e_errs = F.compare_groups(F.decode_kds_final(final, sess), meta["truth"], rtol=0.0)
+    assert e2e_errs == [], e2e_errs[:3]
+    parity = {"groups": len(meta["truth"]), "rows_checked_per_gpu": args.rows,
+              "batch_equals_truth": True, "e2e_equals_truth": True,
+              "compared": "every group's int128 sum(qty*price) and count(*), exact, against the "
+                          "generator's column arrays"}
 
     # ---- N>1: every rank's kds_final merged on rank 0's GPU (the service's
     # final step over per-GPU results); checked against the ranks' row counts
@@ -460,6 +478,7 @@ def run_b200(args, rank, world, local):
                                     "chunk from pinned host memory, Final read-back, CloseSession"},
                 "clocks": clocks,
                 "gpu_launches": args.steps,
+                "parity": parity,
                 "cpu_baseline": cpu}
         if merge:
             line["final_merge"] = merge

@@ -127,9 +127,9 @@ int  xpuB200Final(xpuB200Session *sess, void *kds_final_buf, uint64_t buf_sz,
  *
  * The first call on each GPU looks up the array's device address; make
  * that first call before capturing any stream.  All calls in a process
- * share the array: they are serialised by a lock and each returns after
- * its GPU work has finished.  Work that overlapped on the GPU would race
- * on the shared array.
+ * for one GPU share that GPU's array: they are serialised by a lock per
+ * GPU and each returns after its GPU work has finished.  Work that
+ * overlapped on the GPU would race on the shared array.
  */
 int  xpuB200FinalNoAlloc(xpuB200Session *sess, void *kds_final_dev, uint64_t buf_sz,
                          uint64_t *p_required, kern_exec_results *results, kern_errorbuf *err);

@@ -9,7 +9,8 @@
  * __resolveDevicePointers does (gpu_service.c:3115-3317), then runs a
  * sequential scan -> hash join -> group-by loop in which every tuple
  * decode, qualifier, hash value and aggregate argument is computed by the
- * reference's functions (ExecLoadVarsOuterHeap, ExecLoadVarsMinimalTuple,
+ * reference's functions (ExecLoadVarsOuterHeap, ExecLoadVarsOuterArrow,
+ * ExecLoadVarsMinimalTuple,
  * ExecMoveKernelVariables, EXEC_KERN_EXPRESSION, ExecGpuJoinQuals,
  * pg_hash_any, xpu_*_datum_write).  Only the group accumulation itself is
  * restated (its reference form is device-only code), with exact int128
@@ -280,8 +281,36 @@ extern "C" int ref_exec(void *handle, const kern_data_store *kds, char *errbuf, 
     kern_context *kcxt;
     INIT_KERNEL_CONTEXT(kcxt, session, NULL);
     std::vector<std::vector<char>> kvecs(s->nrels + 2, std::vector<char>(session->kcxt_kvecs_bufsz + 64));
+    if (kds->format == KDS_FORMAT_ARROW) {
+        /* Arrow columns: rows by index through the reference's Arrow
+         * readers (ExecLoadVarsOuterArrow -> kern_extract_arrow_tuple,
+         * xpu_common.cu:1636-1673, :257-378) */
+        for (uint32_t i = 0; i < kds->nitems; i++) {
+            s->nraw++;
+            kcxt_reset(kcxt);
+            kcxt->kvecs_curr_buffer = NULL;
+            kcxt->kvecs_curr_id = 0;
+            if (!ExecLoadVarsOuterArrow(kcxt, SESSION_KEXP_LOAD_VARS(session, 0),
+                                        SESSION_KEXP_SCAN_QUALS(session), kds, i)) {
+                if (kcxt->errcode) { snprintf(errbuf, errlen, "%s", kcxt->error_message); return -1; }
+                continue;
+            }
+            s->nin++;
+            if (!ExecMoveKernelVariables(kcxt, SESSION_KEXP_MOVE_VARS(session, 0), kvecs[0].data(), 0)) {
+                snprintf(errbuf, errlen, "move vars at depth 0 failed");
+                return -1;
+            }
+            process_depth(s, kcxt, 1, kvecs);
+            if (!s->err.empty() || kcxt->errcode) {
+                snprintf(errbuf, errlen, "%s %s", s->err.c_str(),
+                         kcxt->error_message ? kcxt->error_message : "");
+                return -1;
+            }
+        }
+        return 0;
+    }
     if (kds->format != KDS_FORMAT_BLOCK) {
-        snprintf(errbuf, errlen, "ref harness handles KDS_FORMAT_BLOCK only");
+        snprintf(errbuf, errlen, "ref harness handles KDS_FORMAT_BLOCK and KDS_FORMAT_ARROW");
         return -1;
     }
     for (uint32_t b = 0; b < kds->nitems; b++) {

@@ -1007,14 +1007,21 @@ void xo_stats(xo_sess *s, uint64_t *out)
 }
 
 /* write kds_final (the same layout as __writeOutOneTuplePreAgg); returns
- * required length, writing only if buf_sz is large enough */
+ * required length, writing only if buf_sz is large enough.  Grouped
+ * results are KDS_FORMAT_HASH (kern_hashitems chained into hash slots);
+ * an aggregate without GROUP BY keys writes its one tuple into a
+ * KDS_FORMAT_ROW buffer (no hash slots, a bare kern_tupitem), as
+ * __insertOneTupleNoGroups does (cuda_gpupreagg.cu:1005-1036) into the
+ * ROW header executor.c:690-695 sets up */
 uint64_t xo_final(xo_sess *s, void *buf, uint64_t buf_sz)
 {
     if (!s->gb_actions) return 0;
     const kern_data_store *fh = s->kds_final_head;
     uint64_t head_len = KDS_HEAD_LENGTH(fh);
     uint64_t ng = s->ngroups;
-    uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(ng);
+    const int row_fmt = fh->format == KDS_FORMAT_ROW;
+    const uint64_t link = row_fmt ? 0 : 8;     /* kern_hashitem.next */
+    uint64_t nslots = row_fmt ? 0 : KDS_GET_HASHSLOT_WIDTH(ng);
     int nattrs = s->nattrs;
     uint32_t hoff0 = (uint32_t)PGSTROM_MAXALIGN(15 + (nattrs + 7) / 8);
     /* pass 1: sizes */
@@ -1053,7 +1060,7 @@ uint64_t xo_final(xo_sess *s, void *buf, uint64_t buf_sz)
             }
         }
         t += 4;
-        sizes[gi] = PGSTROM_MAXALIGN(8 + t);
+        sizes[gi] = PGSTROM_MAXALIGN(link + t);
         items += sizes[gi];
     }
     uint64_t length = head_len + 8 * nslots + 8 * ng + items;
@@ -1063,14 +1070,14 @@ uint64_t xo_final(xo_sess *s, void *buf, uint64_t buf_sz)
     memcpy(out, fh, head_len);
     kern_data_store *kh = (kern_data_store *)out;
     kh->length = length; kh->usage = items; kh->nitems = (uint32_t)ng;
-    kh->format = KDS_FORMAT_HASH; kh->hash_nslots = (uint32_t)nslots;
+    kh->format = row_fmt ? KDS_FORMAT_ROW : KDS_FORMAT_HASH; kh->hash_nslots = (uint32_t)nslots;
     uint64_t *hslot = (uint64_t *)(out + head_len);
     uint64_t *rowidx = hslot + nslots;
     uint64_t pos = head_len + 8 * nslots + 8 * ng;
     for (uint64_t gi = 0; gi < ng; gi++) {
         xo_group *g = s->order[gi];
         kern_hashitem *hi = (kern_hashitem *)(out + pos);
-        kern_tupitem *ti = &hi->t;
+        kern_tupitem *ti = (kern_tupitem *)(out + pos + link);
         char *base = (char *)ti;
         uint16_t infomask = HEAP_HASNULL;
         uint32_t t = hoff0;
@@ -1148,10 +1155,12 @@ uint64_t xo_final(xo_sess *s, void *buf, uint64_t buf_sz)
         ti->t_infomask = infomask;
         uint32_t rowid = (uint32_t)gi;
         memcpy(base + t - 4, &rowid, 4);
-        rowidx[gi] = length - (pos + 8);
-        uint64_t slot = g->hash % nslots;
-        hi->next = hslot[slot];
-        hslot[slot] = length - pos;
+        rowidx[gi] = length - (pos + link);
+        if (!row_fmt) {
+            uint64_t slot = g->hash % nslots;
+            hi->next = hslot[slot];
+            hslot[slot] = length - pos;
+        }
         pos += sizes[gi];
     }
     free(sizes);

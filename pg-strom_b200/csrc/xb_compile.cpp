@@ -979,6 +979,12 @@ struct Compiler {
                 return fail("groupby_kds_final header is out of the session");
             if (kds_final->ncols < (uint32_t)nattrs)
                 return fail("kds_final has %u columns but AggFuncs has %d", kds_final->ncols, nattrs);
+            /* grouped results are KDS_FORMAT_HASH; the single tuple of an
+             * aggregate without GROUP BY is KDS_FORMAT_ROW
+             * (executor.c:655-697, cuda_gpupreagg.cu:1015-1016) */
+            if (kds_final->format != KDS_FORMAT_HASH &&
+                !(plan->has_groupby == 2 && kds_final->format == KDS_FORMAT_ROW))
+                return fail("kds_final format '%c' does not fit the GROUP BY", kds_final->format);
         } else {
             return fail("GROUP BY session without groupby_kds_final");
         }

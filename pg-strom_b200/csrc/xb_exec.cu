@@ -1134,6 +1134,8 @@ struct XbFinalArgs {
     uint64_t        items_base;     /* offset of the first item */
     uint64_t        length;
     uint32_t        nslots;
+    uint32_t        row_format;     /* KDS_FORMAT_ROW (no GROUP BY keys): kern_tupitems
+                                     * without hash links, nslots 0 */
     const int64_t  *keep;           /* GPU-Sort: output position per entry, -1 dropped
                                      * (nullptr: every group, in table order) */
 };
@@ -1335,7 +1337,7 @@ __global__ void xb_final_sizes(XbFinalArgs args)
         const char *e = args.gt->entries + i * plan->gent_size;
         if (((const xb_gent_head *)e)->state == XB_GSTATE_READY && (!args.keep || args.keep[i] >= 0)) {
             uint32_t t_len = xb_write_group_tuple(plan, e, nullptr, 0);
-            args.sizes[i] = PGSTROM_MAXALIGN(offsetof(kern_hashitem, t) + t_len);
+            args.sizes[i] = PGSTROM_MAXALIGN((args.row_format ? 0 : offsetof(kern_hashitem, t)) + t_len);
             args.flags[i] = 1;
         } else {
             args.sizes[i] = 0;
@@ -1357,6 +1359,13 @@ __global__ void xb_final_write(XbFinalArgs args)
         const char *e = args.gt->entries + i * plan->gent_size;
         const uint32_t rank = args.keep ? (uint32_t)args.keep[i] : args.flag_scan[i];
         const uint64_t item_off = args.items_base + args.size_scan[i];
+        if (args.row_format) {
+            /* KDS_FORMAT_ROW: the tuple itself, found through the row index */
+            kern_tupitem *ti = (kern_tupitem *)(args.kds_final + item_off);
+            xb_write_group_tuple(plan, e, ti, rank);
+            rowindex[rank] = args.length - item_off;
+            continue;
+        }
         kern_hashitem *hitem = (kern_hashitem *)(args.kds_final + item_off);
         xb_write_group_tuple(plan, e, &hitem->t, rank);
         rowindex[rank] = args.length - (item_off + offsetof(kern_hashitem, t));
@@ -2827,18 +2836,26 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
  * prepared batches whose table is several times L2 (the records of a batch
  * take device memory in proportion to its rows, which the serving path's
  * admission does not budget); XPU_B200_PARTITION=1 uses it for every
- * launch over a table above 64 MB, =0 never.  Session lock held.  Returns
- * whether it is used. */
+ * launch on the session's stream over a table above 64 MB, =0 never;
+ * XPU_B200_PART_CAP=n (a test hook) clips the buckets to n records, so
+ * that rows past full buckets are updated in place while others of the
+ * same groups are deferred.  Session lock held.  Returns whether it is
+ * used. */
 static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format, cudaStream_t stream)
 {
     const char *env = getenv("XPU_B200_PARTITION");
     const bool force = env && env[0] == '1';
     if ((env && env[0] == '0') || (!force && !s->in_batch))
         return false;
+    /* the bucket buffers are the session's: only launches on the session's
+     * own stream use them (served launches on pooled slot streams may run
+     * concurrently with each other and would share them) */
+    if (stream != s->stream)
+        return false;
     const xb_plan *plan = s->h_plan;
     if (plan->has_groupby != 1 || s->sm_cap != 0)
         return false;
-    const uint32_t rec = xb_jit_part_rec_size(plan);
+    const uint32_t rec = xb_jit_part_rec_size(plan, format);
     const uint64_t cap = s->h_gt.cap_mask + 1;
     const uint64_t table = cap * plan->gent_size;
     if (rec == 0 || table <= (force ? (64ULL << 20) : (512ULL << 20)))
@@ -2861,6 +2878,8 @@ static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format,
         per = (1ULL << 31) / np;
     if (per < 1024 || per > 0xffffffffULL)
         return false;
+    const char *cap_env = getenv("XPU_B200_PART_CAP");
+    const uint64_t cap_force = cap_env ? strtoull(cap_env, nullptr, 10) : 0;
     const uint64_t bytes = per * np * rec;
     if (!s->part_buf || s->part_bytes < bytes || s->nparts != np) {
         if (s->part_buf) cudaFreeAsync(s->part_buf, stream);
@@ -2879,6 +2898,8 @@ static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format,
         s->part_bytes = bytes;
     }
     s->part_cap = (uint32_t)(s->part_bytes / (np * rec));
+    if (cap_force > 0 && cap_force < s->part_cap)
+        s->part_cap = (uint32_t)cap_force;
     s->nparts = (uint32_t)np;
     s->part_shift = lg_cap - lg_np;
     s->part_rec = rec;
@@ -3387,6 +3408,7 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
     const uint64_t head_len = KDS_HEAD_LENGTH(fh);
     const uint64_t cap = s->h_gt.cap_mask + 1;
+    const bool row_fmt = fh->format == KDS_FORMAT_ROW;
 
     uint64_t *d_sizes = nullptr, *d_size_scan = nullptr;
     uint32_t *d_flags = nullptr, *d_flag_scan = nullptr;
@@ -3415,6 +3437,7 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     fa.flags = d_flags;
     fa.size_scan = d_size_scan;
     fa.flag_scan = d_flag_scan;
+    fa.row_format = row_fmt ? 1 : 0;
     int grid = s->dev->nsm * 8;
     if (plan->nsort) {
         int64_t *d_keep = nullptr;
@@ -3449,7 +3472,7 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     }
     const uint64_t items = last_scan + last_size;
     const uint64_t ngroups = (uint64_t)last_fscan + last_flag;
-    const uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(ngroups);
+    const uint64_t nslots = row_fmt ? 0 : KDS_GET_HASHSLOT_WIDTH(ngroups);
     const uint64_t items_base = head_len + 8 * nslots + 8 * ngroups;
     const uint64_t length = items_base + items;
     if (p_required) *p_required = length;
@@ -3476,7 +3499,7 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     kh->length = length;
     kh->usage = items;
     kh->nitems = (uint32_t)ngroups;
-    kh->format = KDS_FORMAT_HASH;
+    kh->format = row_fmt ? KDS_FORMAT_ROW : KDS_FORMAT_HASH;
     kh->hash_nslots = (uint32_t)nslots;
     cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_out + head_len, 0, 8 * nslots + 8 * ngroups, st);
@@ -3517,9 +3540,12 @@ xpuB200MergeFinal(xpuB200Session *s, const kern_data_store *kds_final, int kds_f
         hb.assign((const char *)kds_final, (const char *)kds_final + KDS_HEAD_LENGTH(kds_final));
     }
     const kern_data_store *h = (const kern_data_store *)hb.data();
-    if (h->format != KDS_FORMAT_HASH || h->ncols != plan->naggs ||
+    const kern_session_info *session = (const kern_session_info *)s->h_session.data();
+    const char fmt = ((const kern_data_store *)(s->h_session.data() + session->groupby_kds_final))->format;
+    if (h->format != fmt || h->ncols != plan->naggs || (fmt == KDS_FORMAT_ROW && h->hash_nslots != 0) ||
         KDS_HEAD_LENGTH(h) + 8 * ((uint64_t)h->hash_nslots + h->nitems) > h->length)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "kds_final to merge is not this session's KDS_FORMAT_HASH");
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "kds_final to merge is not this session's KDS_FORMAT_%s",
+                      fmt == KDS_FORMAT_ROW ? "ROW" : "HASH");
     if (h->nitems == 0)
         return 0;
     if (plan->gent_size > XB_GENT_MAX)
@@ -3567,8 +3593,9 @@ static __device__ __align__(256) char xb_final_scratch[XB_FINAL_SCRATCH_BYTES];
 /* device address of xb_final_scratch on each GPU, looked up once per device
  * (the host-side symbol is not a device address) */
 static void *xb_final_scratch_dptr[XB_FINAL_SCRATCH_DEVS];
-/* every session of the process shares the array: one call at a time */
-static std::mutex xb_final_scratch_lock;
+/* every session on one GPU shares that GPU's array: one call at a time
+ * per GPU (calls for different GPUs use different arrays and run freely) */
+static std::mutex xb_final_scratch_lock[XB_FINAL_SCRATCH_DEVS];
 
 static inline uint64_t xb_align256(uint64_t x)
 {
@@ -3584,10 +3611,10 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid FinalNoAlloc arguments");
     xb_sched_drain_session(s);
     std::lock_guard<std::mutex> g(s->lock);
-    std::lock_guard<std::mutex> gs(xb_final_scratch_lock);
     const int dindex = s->dev->dindex;
     if (dindex < 0 || dindex >= XB_FINAL_SCRATCH_DEVS)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "FinalNoAlloc supports GPUs 0..%d", XB_FINAL_SCRATCH_DEVS - 1);
+    std::lock_guard<std::mutex> gs(xb_final_scratch_lock[dindex]);
     XB_CUDA(cudaSetDevice(dindex), err);
     if (!xb_final_scratch_dptr[dindex]) {
         void *ptr = nullptr;
@@ -3622,6 +3649,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
     const uint64_t head_len = KDS_HEAD_LENGTH(fh);
     const uint64_t cap = s->h_gt.cap_mask + 1;
+    const bool row_fmt = fh->format == KDS_FORMAT_ROW;
 
     /* scratch layout: sizes | size prefix sums | flags | flag prefix sums | scan storage */
     const uint64_t off_sscan = xb_align256(cap * 8);
@@ -3656,9 +3684,9 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
             return XB_ERR(err, ERRCODE_DEVICE_ERROR,
                           "FinalNoAlloc: kds_final_dev must be memory of GPU %d (or mapped host memory)", dindex);
     }
-    /* the previous call's values are still in the array; start clean */
-    cudaMemsetAsync(d_sizes, 0, cap * 8, st);
-    cudaMemsetAsync(d_flags, 0, cap * 4, st);
+    /* the previous call's values are still in the array: xb_final_sizes
+     * writes every size and flag below cap, and the scans overwrite their
+     * outputs, so no part of it needs clearing first */
     XbFinalArgs fa;
     memset(&fa, 0, sizeof(fa));
     fa.plan = s->d_plan;
@@ -3668,6 +3696,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     fa.flags = d_flags;
     fa.size_scan = d_size_scan;
     fa.flag_scan = d_flag_scan;
+    fa.row_format = row_fmt ? 1 : 0;
     const int grid = s->dev->nsm * 8;
     xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
     size_t tsz = tsz_max;
@@ -3684,7 +3713,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalNoAlloc: %s", cudaGetErrorString(cudaGetLastError()));
     const uint64_t items = last_scan + last_size;
     const uint64_t ngroups = (uint64_t)last_fscan + last_flag;
-    const uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(ngroups);
+    const uint64_t nslots = row_fmt ? 0 : KDS_GET_HASHSLOT_WIDTH(ngroups);
     const uint64_t items_base = head_len + 8 * nslots + 8 * ngroups;
     const uint64_t length = items_base + items;
     if (p_required) *p_required = length;
@@ -3705,7 +3734,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     kh->length = length;
     kh->usage = items;
     kh->nitems = (uint32_t)ngroups;
-    kh->format = KDS_FORMAT_HASH;
+    kh->format = row_fmt ? KDS_FORMAT_ROW : KDS_FORMAT_HASH;
     kh->hash_nslots = (uint32_t)nslots;
     cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_out + head_len, 0, 8 * nslots + 8 * ngroups, st);

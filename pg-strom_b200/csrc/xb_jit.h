@@ -42,10 +42,10 @@ int xb_jit_compile_minb(const xb_plan *plan, uint32_t format, int dindex, int mi
                         char *errbuf, size_t errlen);
 
 /* bytes of one deferred-row record of partitioned aggregation for plan
- * (0: the plan does not defer its group updates); the replay kernel is
+ * and source format (0: its kernel does not defer group updates); the replay kernel is
  * xbj_replay (parameter block XbReplayArgs), returned by
  * xb_jit_compile_minb's p_replay */
-uint32_t xb_jit_part_rec_size(const xb_plan *plan);
+uint32_t xb_jit_part_rec_size(const xb_plan *plan, uint32_t format);
 
 /* a key naming the plan shape of plan + format: sessions whose specialised
  * kernels differ only in their launch bounds share it */

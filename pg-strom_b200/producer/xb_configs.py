@@ -29,7 +29,7 @@ import numpy as np
 
 from xb_final import Approx
 from xb_producer import (Table, Column, Var, Const, Func, Agg, SessionBuilder,
-                         encode_numeric_array, encode_text_array, encode_text_from_dict,
+                         encode_numeric, encode_varlena_list, encode_numeric_array, encode_text_array, encode_text_from_dict,
                          hash_u32_array, hash_merge_array, kern_multirels, numeric_typmod)
 
 DEVKIND_GPU = 0x00000001
@@ -145,6 +145,126 @@ def wide_groupby_session(a_limit=600, ngroups=3000, sort=None):
         **_sort_args(sort))
 
 
+def scan_nogroup_session(a_limit=300):
+    """WHERE a < a_limit -> count(*), count(b), sum(a), sum(c), avg(b),
+    min(b), max(b): an aggregate without GROUP BY keys (one result tuple,
+    KDS_FORMAT_ROW kds_final).  max(float8) is the state the reference's
+    no-group global-memory path updates with an atomic minimum
+    (cuda_gpupreagg.cu:524-526); the SQL result is the maximum."""
+    typmod_c = numeric_typmod(12, 2)
+    va, vb, vc = Var(0, 2, "int4"), Var(0, 3, "float8"), Var(0, 4, "numeric", typmod_c)
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    return sb.build(
+        scan_quals=Func("int4lt", [va, Const("int4", a_limit)], "bool"),
+        groupby_keys=[],
+        aggs=[Agg("NROWS_ANY"),
+              Agg("NROWS_COND", vb),
+              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")),
+              Agg("PSUM_NUMERIC", vc, typmod_c),
+              Agg("PAVG_FP", vb),
+              Agg("PMIN_FP64", vb),
+              Agg("PMAX_FP64", vb)],
+        ngroups_estimate=1.0)
+
+
+def scan_nogroup(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300):
+    """The plain scan table under scan_nogroup_session, with the one
+    expected result tuple (key ()) computed from the column arrays; no
+    tuple at all when no row qualifies."""
+    tbl, a, b, bnull, c_unscaled, g = _scan_table(nrows, seed_config, null_frac, 64)
+    session = scan_nogroup_session(a_limit)
+    m = a < a_limit
+    mb = m & ~bnull
+    n, nb = int(m.sum()), int(mb.sum())
+    expect = {}
+    if n:
+        bs = b[mb]
+        fsum = 0.0
+        for x in bs:                                # row-ordered FP64 sum
+            fsum += float(x)
+        valid = 1 if nb else 0
+        expect[()] = [n, nb, (n, int(a[m].astype(np.int64).sum())), (n, int(c_unscaled[m].sum()), 2),
+                      (nb, Approx(fsum, float(np.abs(bs).sum()))),
+                      (valid, float(bs.min()) if nb else None), (valid, float(bs.max()) if nb else None)]
+    meta = {"nitems_raw": nrows, "nitems_in": n, "nitems_out": n, "nkeys": 0}
+    return tbl, session, None, expect, meta
+
+
+def long_strings(n, seed=7, lo=20, hi=300):
+    """n distinct strings whose lengths straddle the 1-byte varlena limit:
+    the first ones are 1, 126, 127, 128 and 300 bytes long (126 is the
+    longest payload of a 1-byte header), the rest uniform in [lo, hi]."""
+    r = np.random.Generator(np.random.PCG64(seed))
+    fixed = [1, 126, 127, 128, 300]
+    lens = fixed[:n] + r.integers(lo, hi + 1, max(0, n - len(fixed))).tolist()
+    out = []
+    for i, L in enumerate(lens):
+        head = "%d:" % i
+        body = "".join(chr(97 + (i * 7 + 3 * j) % 26) for j in range(L))
+        out.append((head + body)[:L] if L > len(head) else chr(65 + i % 26) * L)
+    assert len(set(out)) == n
+    return out
+
+
+def long_varlena_session(v_limit=700, ngroups=150):
+    """WHERE v < v_limit GROUP BY t -> count(*), count(n), sum(n), avg(n),
+    sum(v) over (id int8, t text, n numeric(18,4), v int4)."""
+    typmod_n = numeric_typmod(18, 4)
+    vt, vn, vv = Var(0, 2, "text"), Var(0, 3, "numeric", typmod_n), Var(0, 4, "int4")
+    sb = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU)
+    return sb.build(
+        scan_quals=Func("int4lt", [vv, Const("int4", v_limit)], "bool"),
+        groupby_keys=[vt],
+        aggs=[Agg("NROWS_ANY"), Agg("NROWS_COND", vn),
+              Agg("PSUM_NUMERIC", vn, typmod_n), Agg("PAVG_NUMERIC", vn, typmod_n),
+              Agg("PSUM_INT", Func("int4_to_int8", [vv], "int8"))],
+        ngroups_estimate=float(ngroups))
+
+
+def long_varlena_groupby(nrows=100_000, ngroups=150, seed_config=6, null_frac=0.03, v_limit=700):
+    """Heap table (id int8, t text, n numeric(18,4), v int4) whose varlenas
+    take every on-disk form the heap decoder must read: t is one of
+    ngroups strings of 1..300 bytes (those above 126 bytes carry a 4-byte
+    header, aligned to 4 in the tuple); n is U(-1e8, 1e8) at 4 decimals
+    with 3% NULLs, one third in the short numeric format, one third in the
+    NUMERIC_LONG format (n_sign_dscale + n_weight), one third in the long
+    format with a 4-byte varlena header.  Expected states from the
+    arrays."""
+    r = rng_for(seed_config, 0)
+    words = long_strings(ngroups, seed=SEED_BASE + seed_config)
+    code = r.integers(0, ngroups, nrows)
+    v = r.integers(0, 1000, nrows, dtype=np.int32)
+    n_unscaled = r.integers(-10 ** 12, 10 ** 12, nrows, dtype=np.int64)
+    nnull = r.random(nrows) < null_frac
+    form = r.integers(0, 3, nrows)
+    nimg = [encode_numeric(int(x), 4, long_fmt=f >= 1, hdr4=f == 2)
+            for x, f in zip(n_unscaled.tolist(), form.tolist())]
+    typmod_n = numeric_typmod(18, 4)
+    tbl = Table("t6", [
+        Column("id", "int8", values=np.arange(nrows, dtype=np.int64)),
+        Column("t", "text", values=encode_text_from_dict(code, words)),
+        Column("n", "numeric", typmod=typmod_n, values=encode_varlena_list(nimg), nulls=nnull),
+        Column("v", "int4", values=v),
+    ], nrows)
+    session = long_varlena_session(v_limit, ngroups)
+    m = v < v_limit
+    mn = m & ~nnull
+    cnt = np.bincount(code[m], minlength=ngroups)
+    cn = np.bincount(code[mn], minlength=ngroups)
+    sv = np.zeros(ngroups, dtype=np.int64)
+    np.add.at(sv, code[m], v[m].astype(np.int64))
+    sn = [0] * ngroups
+    for k, x in zip(code[mn].tolist(), n_unscaled[mn].tolist()):
+        sn[k] += x
+    expect = {}
+    for k in np.flatnonzero(cnt).tolist():
+        expect[(words[k].encode(),)] = [int(cnt[k]), int(cn[k]), (int(cn[k]), sn[k], 4), (int(cn[k]), sn[k], 4),
+                                        (int(cnt[k]), int(sv[k]))]
+    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()), "nkeys": 1,
+            "words": words}
+    return tbl, session, None, expect, meta
+
+
 def _sort_args(sort):
     if not sort:
         return {}
@@ -232,7 +352,8 @@ def join_groupby_session(flag_limit=3, sort=None, inner_handle=0):
 
 
 def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, flag_limit=3,
-                 key_stride=1, dim1_copies=1, miss_frac=0.0, with_rows=False, price_hi=1_000_000):
+                 key_stride=1, dim1_copies=1, miss_frac=0.0, with_rows=False, price_hi=1_000_000,
+                 regions=None):
     """Two-way hash join + group-by.  Defaults give the headline workload:
     dense unique dimension keys 1..n, every fact row matching.  Variants for
     the join paths: key_stride spreads the keys (k * stride; sparse keys
@@ -240,16 +361,19 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
     repeats every dim1 key with its own region (several matches per probe),
     miss_frac makes that share of fact rows reference no dim1 row.
     with_rows adds meta["rows"]: the sorted (fk1, qty * price, region,
-    flag) tuples of every joined row."""
+    flag) tuples of every joined row.regions replaces the 25 region strings (e.g. strings longer than 126
+    bytes, whose varlena header is 4 bytes).
+    """
+    REG = REGIONS if regions is None else regions
     r1 = rng_for(seed_config, 1)
     r2 = rng_for(seed_config, 2)
     rf = rng_for(seed_config, 0)
     # dimensions
     pk1_one = np.arange(1, ndim1 + 1, dtype=np.int64) * key_stride
     pk1 = np.tile(pk1_one, dim1_copies).astype(np.int32)
-    reg_code = r1.integers(0, len(REGIONS), ndim1 * dim1_copies)
+    reg_code = r1.integers(0, len(REG), ndim1 * dim1_copies)
     dim1 = Table("dim1", [Column("pk", "int4", values=pk1),
-                          Column("region", "text", values=encode_text_from_dict(reg_code, REGIONS))],
+                          Column("region", "text", values=encode_text_from_dict(reg_code, REG))],
                  ndim1 * dim1_copies)
     pk2 = (np.arange(1, ndim2 + 1, dtype=np.int64) * key_stride).astype(np.int32)
     flag = r2.integers(0, 5, ndim2, dtype=np.int16)
@@ -277,25 +401,25 @@ def join_groupby(nfact=100_000_000, ndim1=200_000, ndim2=10_000, seed_config=1, 
     # expected: every (fact row, dim1 copy) pair that passes both joins
     m = (flag[idx2] < flag_limit) & ~miss
     amount = qty.astype(np.int64) * price
-    cnt = np.zeros(len(REGIONS), dtype=np.int64)
-    tot = [0] * len(REGIONS)
+    cnt = np.zeros(len(REG), dtype=np.int64)
+    tot = [0] * len(REG)
     for c in range(dim1_copies):
         region_row = reg_code[c * ndim1 + idx1]
-        for k in range(len(REGIONS)):
+        for k in range(len(REG)):
             sel = m & (region_row == k)
             cnt[k] += int(sel.sum())
             tot[k] += int(amount[sel].sum())
     expect = {}
-    for k in range(len(REGIONS)):
+    for k in range(len(REG)):
         if cnt[k]:
-            expect[(REGIONS[k].encode(),)] = {"sum_amount": (int(cnt[k]), tot[k]), "nrows": int(cnt[k])}
+            expect[(REG[k].encode(),)] = {"sum_amount": (int(cnt[k]), tot[k]), "nrows": int(cnt[k])}
     if with_rows:
         rows = []
         sel = np.flatnonzero(m)
         for c in range(dim1_copies):
             region_row = reg_code[c * ndim1 + idx1[sel]]
             rows += list(zip(fk1[sel].tolist(), amount[sel].tolist(),
-                             [REGIONS[k].encode() for k in region_row], flag[idx2[sel]].tolist()))
+                             [REG[k].encode() for k in region_row], flag[idx2[sel]].tolist()))
         rows.sort()
     hit1 = int((~miss).sum()) * dim1_copies
     out = int(m.sum()) * dim1_copies

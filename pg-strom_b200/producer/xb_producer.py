@@ -112,17 +112,22 @@ def numeric_typmod(precision, scale):
 # ---------------------------------------------------------------------------
 # datum encoders
 # ---------------------------------------------------------------------------
-def encode_varlena(payload: bytes) -> bytes:
-    """PostgreSQL on-disk varlena: 1-byte header when it fits, else 4-byte."""
+def encode_varlena(payload: bytes, hdr4=False) -> bytes:
+    """PostgreSQL on-disk varlena: 1-byte header when it fits, else (or
+    with hdr4) the 4-byte header of an inline uncompressed datum."""
     n = len(payload)
-    if n + 1 <= 127:
+    if n + 1 <= 127 and not hdr4:
         return bytes([((n + 1) << 1) | 1]) + payload
     return struct.pack("<I", (n + 4) << 2) + payload
 
 
-def encode_numeric(unscaled: int, scale: int) -> bytes:
+def encode_numeric(unscaled: int, scale: int, long_fmt=False, hdr4=False) -> bytes:
     """numeric value unscaled * 10^-scale in PostgreSQL's short (or long)
-    on-disk format: base-10000 digits, weight of the first digit, dscale."""
+    on-disk format: base-10000 digits, weight of the first digit, dscale.
+    long_fmt writes the NUMERIC_LONG header (n_sign_dscale, n_weight) that
+    PostgreSQL uses when dscale or weight do not fit the short header (and
+    wrote for every value before 9.1); hdr4 gives the datum a 4-byte
+    varlena header."""
     neg = unscaled < 0
     v = -unscaled if neg else unscaled
     # decimal digits aligned so that the fractional part fills whole groups
@@ -147,13 +152,20 @@ def encode_numeric(unscaled: int, scale: int) -> bytes:
     if not digits:
         weight = 0
         neg = False
-    if scale <= 0x3F and -64 <= weight <= 63:
+    if scale <= 0x3F and -64 <= weight <= 63 and not long_fmt:
         head = 0x8000 | (0x2000 if neg else 0) | (scale << 7) | (weight & 0x7F)
         body = struct.pack("<H", head) + b"".join(struct.pack("<h", d) for d in digits)
     else:
         head = (0x4000 if neg else 0) | (scale & 0x3FFF)
         body = struct.pack("<Hh", head, weight) + b"".join(struct.pack("<h", d) for d in digits)
-    return encode_varlena(body)
+    return encode_varlena(body, hdr4)
+
+
+def encode_varlena_list(images):
+    """List of encoded datums (bytes) -> (blob, offsets)."""
+    offs = np.zeros(len(images) + 1, dtype=np.int64)
+    np.cumsum([len(p) for p in images], out=offs[1:])
+    return np.frombuffer(b"".join(images), dtype=np.uint8).copy(), offs
 
 
 def encode_numeric_array(unscaled: np.ndarray, scale: int):
@@ -1031,8 +1043,14 @@ class SessionBuilder:
             for i, k in enumerate(groupby_keys):
                 final_cols.append(Column(f"key{i}", k.typ, getattr(k, "typmod", -1)))
             ft = Table("kds_final", final_cols, 0)
-            kf = ft.kds_header("h", 0)
-            struct.pack_into("<Q", kf, 0, 1 << 30)
+            if groupby_keys:
+                kf = ft.kds_header("h", 0)
+                struct.pack_into("<Q", kf, 0, 1 << 30)
+            else:
+                # an aggregate without GROUP BY keys: one tuple in a 4 MB
+                # KDS_FORMAT_ROW buffer, no hash slots (executor.c:690-695)
+                kf = ft.kds_header("r", 0)
+                struct.pack_into("<Q", kf, 0, 4 << 20)
             blobs["kds_final"] = bytes(kf)
         return self._assemble(blobs, ngroups_estimate)
 

@@ -169,3 +169,69 @@ def test_batch_matches_single_chunk_path(device, kernel):
         device.free(base)
     truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
     assert F.compare_groups(F.decode_kds_final(final, sess), truth) == []
+
+
+@pytest.mark.parametrize("nrows,ppc", [(30_000, 40), (600_000, 1500)])
+def test_no_group_by_parity(device, kernel, nrows, ppc):
+    """count(*), count(b), sum(a), sum(c), avg(b), min(b), max(b) with no
+    GROUP BY keys: one KDS_FORMAT_ROW tuple, equal to the oracle's and to
+    the column arrays.  max(b) is the maximum (the reference's no-group
+    global path takes an atomic minimum there, cuda_gpupreagg.cu:524-526).
+    The float sum of b (N(0,1) terms, cancelling) is also within 1e-12
+    relative of the exactly rounded sum (math.fsum)."""
+    import math
+    import struct
+    tbl, sess, _, expect, meta = C.scan_nogroup(nrows=nrows)
+    chunks = tbl.block_chunks(pages_per_chunk=ppc)
+    final, st, res = run_gpu(device, sess, chunks, kernel=kernel)
+    assert st["nitems_in"] == meta["nitems_in"]
+    assert bytes(final)[24:25] == b"r" and struct.unpack_from("<I", bytes(final), 40)[0] == 0
+    got = F.decode_kds_final(final, sess)
+    assert F.compare_groups(got, expect) == []
+    ofinal, _ = run_oracle(sess, chunks)
+    want = F.decode_kds_final(ofinal, sess)
+    assert F.compare_groups(got, want) == []
+    g = got[()]
+    assert g[:4] == want[()][:4]                    # integer and numeric states exact
+    b, bnull, a = tbl.col("b").values, tbl.col("b").nulls, tbl.col("a").values
+    exact = math.fsum(b[(a < 300) & ~bnull].tolist())
+    assert abs(g[4][1] - exact) <= 1e-12 * abs(exact)
+    assert res["final_nitems"] == 1
+
+
+def test_no_group_by_no_rows(device, kernel):
+    tbl, sess, _, expect, meta = C.scan_nogroup(nrows=10_000, a_limit=0)
+    final, st, res = run_gpu(device, sess, tbl.block_chunks(), kernel=kernel)
+    assert st["nitems_in"] == 0
+    assert F.decode_kds_final(final, sess) == {}
+
+
+@pytest.mark.parametrize("nrows,ppc", [(40_000, 60), (300_000, 700)])
+def test_long_varlena_parity(device, kernel, nrows, ppc):
+    """Text group keys of 1..300 bytes (4-byte varlena headers above 126
+    bytes, aligned to 4 in the tuple) and numeric(18,4) values in the
+    short, NUMERIC_LONG and 4-byte-header long forms, summed and averaged:
+    equal to the oracle and to the column arrays."""
+    tbl, sess, _, expect, meta = C.long_varlena_groupby(nrows=nrows)
+    chunks = tbl.block_chunks(pages_per_chunk=ppc)
+    final, st, res = run_gpu(device, sess, chunks, kernel=kernel)
+    assert st["nitems_raw"] == meta["nitems_raw"] and st["nitems_in"] == meta["nitems_in"]
+    got = F.decode_kds_final(final, sess)
+    assert F.compare_groups(got, expect, rtol=0.0) == []
+    ofinal, _ = run_oracle(sess, chunks)
+    assert F.compare_groups(got, F.decode_kds_final(ofinal, sess), rtol=0.0) == []
+
+
+def test_join_long_text_keys_parity(device, kernel):
+    """GROUP BY an inner relation's text column whose values are up to 300
+    bytes (4-byte headers in the inner MinimalTuples)."""
+    fact, sess, km, expect, meta = C.join_groupby(nfact=300_000, ndim1=20_000, ndim2=2_000,
+                                                  regions=C.long_strings(40))
+    chunks = fact.block_chunks(pages_per_chunk=400)
+    final, st, res = run_gpu(device, sess, chunks, km, nrels=2, kernel=kernel)
+    assert st["nitems_out"] == meta["nitems_out"]
+    got = F.decode_kds_final(final, sess)
+    truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
+    assert F.compare_groups(got, truth) == []
+    ofinal, _ = run_oracle(sess, chunks, km)
+    assert F.compare_groups(got, F.decode_kds_final(ofinal, sess)) == []

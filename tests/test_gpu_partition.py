@@ -78,3 +78,61 @@ def test_partitioned_text_keys(device, monkeypatch):
     want = F.decode_kds_final(o.final(), sess)
     o.close()
     assert F.compare_groups(F.decode_kds_final(final, sess), want) == []
+
+
+@pytest.mark.parametrize("cap", ["1", "700"])
+def test_full_buckets_update_in_place(device, monkeypatch, cap):
+    # buckets clipped to a few records: most rows of a group are updated in
+    # place while others of the same group are deferred and replayed
+    monkeypatch.setenv("XPU_B200_PARTITION", "1")
+    monkeypatch.setenv("XPU_B200_PART_CAP", cap)
+    tbl, _, _, expect, meta = C.wide_groupby(nrows=300_000, ngroups=3000, seed_config=85)
+    sess = C.wide_groupby_session(ngroups=2_000_000)
+    final, info = _run(device, sess, tbl.block_chunks(pages_per_chunk=256))
+    assert info["partition_used"], info
+    assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
+
+
+def test_full_buckets_text_keys(device, monkeypatch):
+    import xb_oracle as O
+    from xb_producer import Agg, SessionBuilder, Var
+    monkeypatch.setenv("XPU_B200_PARTITION", "1")
+    monkeypatch.setenv("XPU_B200_PART_CAP", "300")
+    fact, _, km, _, meta = C.join_groupby(nfact=1000, ndim1=200_000, ndim2=70, seed_config=86)
+    dim1 = meta["dims"]["dim1"]
+    sess = SessionBuilder(0, C.DEVTASK_PREAGG | C.DEVKIND_GPU).build(
+        groupby_keys=[Var(0, 2, "text")], aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Var(0, 1, "int4"))],
+        ngroups_estimate=2_000_000.0)
+    chunks = dim1.block_chunks(pages_per_chunk=256)
+    final, info = _run(device, sess, chunks)
+    assert info["partition_used"], info
+    o = O.Oracle(sess)
+    for ch in chunks:
+        o.exec(ch)
+    want = F.decode_kds_final(o.final(), sess)
+    o.close()
+    assert F.compare_groups(F.decode_kds_final(final, sess), want) == []
+
+
+def test_staged_pages_do_not_defer_text_keys(device, monkeypatch):
+    # with heap pages staged in shared memory the text key registers point
+    # into the staging buffer, so partitioned aggregation stays off and the
+    # groups are updated in place
+    import xb_oracle as O
+    from xb_producer import Agg, SessionBuilder, Var
+    monkeypatch.setenv("XPU_B200_PARTITION", "1")
+    monkeypatch.setenv("XPU_B200_JIT_STAGE", "1")
+    fact, _, km, _, meta = C.join_groupby(nfact=1000, ndim1=200_000, ndim2=70, seed_config=87)
+    dim1 = meta["dims"]["dim1"]
+    sess = SessionBuilder(0, C.DEVTASK_PREAGG | C.DEVKIND_GPU).build(
+        groupby_keys=[Var(0, 2, "text")], aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Var(0, 1, "int4"))],
+        ngroups_estimate=2_000_000.0)
+    chunks = dim1.block_chunks(pages_per_chunk=256)
+    final, info = _run(device, sess, chunks)
+    assert not info["partition_used"], info
+    o = O.Oracle(sess)
+    for ch in chunks:
+        o.exec(ch)
+    want = F.decode_kds_final(o.final(), sess)
+    o.close()
+    assert F.compare_groups(F.decode_kds_final(final, sess), want) == []

@@ -56,3 +56,38 @@ def test_oracle_all_filtered_out():
     assert expect == {}
     assert F.decode_kds_final(o.final(), sess) == {}
     o.close()
+
+
+def _row_format(buf):
+    import struct
+    fmt = bytes(buf)[24:25]
+    nslots = struct.unpack_from("<I", bytes(buf), 40)[0]
+    return fmt, nslots
+
+
+def test_oracle_no_group_by():
+    # an aggregate without GROUP BY keys: one tuple in a KDS_FORMAT_ROW
+    # kds_final with no hash slots; max(float8) is the maximum
+    tbl, sess, _, expect, meta = C.scan_nogroup(nrows=120_000)
+    o = O.Oracle(sess)
+    for ch in tbl.block_chunks(pages_per_chunk=200):
+        o.exec(ch)
+    assert o.stats()["nitems_in"] == meta["nitems_in"]
+    out = o.final()
+    assert _row_format(out) == (b"r", 0)
+    got = F.decode_kds_final(out, sess)
+    assert list(got) == [()]
+    assert F.compare_groups(got, expect) == []
+    o.close()
+
+
+def test_oracle_no_group_by_no_rows():
+    # no qualifying row: no tuple (the reference creates the tuple only when
+    # rows reach the aggregation, cuda_gpupreagg.cu:2246-2247)
+    tbl, sess, _, expect, meta = C.scan_nogroup(nrows=5000, a_limit=0)
+    o = O.Oracle(sess)
+    for ch in tbl.block_chunks():
+        o.exec(ch)
+    assert expect == {}
+    assert F.decode_kds_final(o.final(), sess) == {}
+    o.close()

@@ -57,6 +57,8 @@ def _ref_groups(res, aggs, keytypes):
                 states.append(st)
             elif action in (503, 603):
                 states.append((st[0], float(st[1])))
+            elif action in (304, 404):
+                states.append((st[0], float(st[1]) if st[0] else None))
             elif action in (504, 604):
                 w = (((typmod - 4) & 0x7FF) ^ 1024) - 1024 if typmod >= 0 else 15
                 states.append((st[0], int(st[1]), max(0, min(15, w))))
@@ -66,11 +68,29 @@ def _ref_groups(res, aggs, keytypes):
     return out
 
 
-@pytest.mark.parametrize("which", ["scan", "join"])
+@pytest.mark.parametrize("which", ["scan", "join", "nogroup", "long_varlena", "join_long_text", "arrow"])
 def test_oracle_matches_reference_functions(which):
+    """The oracle's groups equal those the reference's functions compute
+    (rtol=0): heap scan and join, an aggregate without GROUP BY keys, text
+    and numeric varlenas with 4-byte headers and the NUMERIC_LONG format,
+    text group keys of inner rows longer than 126 bytes, and Arrow columns
+    read by ExecLoadVarsOuterArrow (int8 / int4 / float8 / date)."""
     if which == "scan":
         tbl, sess, km, expect, meta = C.scan_groupby(nrows=60_000)
         chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "nogroup":
+        tbl, sess, km, expect, meta = C.scan_nogroup(nrows=60_000)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "long_varlena":
+        tbl, sess, km, expect, meta = C.long_varlena_groupby(nrows=20_000)
+        chunks = tbl.block_chunks(pages_per_chunk=100)
+    elif which == "join_long_text":
+        tbl, sess, km, expect, meta = C.join_groupby(nfact=40_000, ndim1=3000, ndim2=500,
+                                                     regions=C.long_strings(40))
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "arrow":
+        chunks, sess, expect, meta = C.arrow_groupby(nrows=60_000, nkeys=5_000, rows_per_chunk=25_000)
+        km = None
     else:
         tbl, sess, km, expect, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
         chunks = tbl.block_chunks(pages_per_chunk=200)

@@ -12,6 +12,7 @@ array that the previous call left behind.
 The file is named so that pytest collects it after every other test file.
 """
 import ctypes
+import struct
 
 import numpy as np
 import pytest
@@ -51,6 +52,34 @@ def _no_alloc_final_bytes(sess):
     return out.cpu().numpy(), res
 
 
+def _layout(buf):
+    """(bytes with the hash-chain links blanked, {slot: set of item offsets}).
+    Items enter their slot's chain concurrently, so only the chains' order
+    may differ between two calls; every other byte must be the same."""
+    b = np.array(buf, dtype=np.uint8, copy=True)
+    length, _usage, nitems = struct.unpack_from("<QQI", b, 0)
+    nslots = struct.unpack_from("<I", b, 40)[0]
+    nr_colmeta = struct.unpack_from("<I", b, 68)[0]
+    head = (72 + 168 * nr_colmeta + 7) & ~7          # KDS_HEAD_LENGTH
+    slots = np.frombuffer(b[head:head + 8 * nslots].tobytes(), dtype=np.uint64)
+    chains = {}
+    for slot in np.flatnonzero(slots).tolist():
+        off = int(slots[slot])
+        seen = set()
+        while off:
+            item = length - off
+            assert item not in seen
+            seen.add(item)
+            off = struct.unpack_from("<Q", b, item)[0]
+        chains[slot] = seen
+    assert sum(len(v) for v in chains.values()) == nitems
+    b[head:head + 8 * nslots] = 0
+    for items in chains.values():
+        for item in items:
+            b[item:item + 8] = 0
+    return b.tobytes(), chains
+
+
 def _open(device, which):
     if which == "join":
         fact, sess, km, expect, _ = C.join_groupby(nfact=60_000, ndim1=3_000, ndim2=400)
@@ -83,10 +112,15 @@ def test_final_without_allocation_matches_final(device):
         first, res1 = _no_alloc_final_bytes(s_join)
         other, _ = _no_alloc_final_bytes(s_scan)
         second, res2 = _no_alloc_final_bytes(s_join)
+        want_bytes, want_chains = _layout(want)
         for got, res in ((first, res1), (second, res2)):
             assert got.nbytes == want.nbytes
             assert res["final_nitems"] == want_res["final_nitems"]
             assert F.compare_groups(F.decode_kds_final(got, sess_join), want_groups) == []
+            # byte for byte the same buffer, up to the order of hash chains
+            got_bytes, got_chains = _layout(got)
+            assert got_chains == want_chains
+            assert got_bytes == want_bytes
         assert F.compare_groups(F.decode_kds_final(other, sess_scan), truth_scan) == []
     finally:
         s_join.close()
