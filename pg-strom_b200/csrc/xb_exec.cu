@@ -117,7 +117,7 @@ xb_group_claim(const xb_plan *plan, char *e, XbRegs R, uint32_t hash,
     }
     xb_init_states(plan, e);
     if (gt) {
-        atomicAdd((unsigned long long *)&gt->nused, 1ULL);
+        xb_gt_count_new(gt);
         xb_st_release(&h->state, XB_GSTATE_READY);
     } else {
         xb_st_release_cta(&h->state, XB_GSTATE_READY);
@@ -621,6 +621,11 @@ xb_exec_body(const XbExecArgs &args, char *smem)
     for (;;) {
         const xb_prog *prog;
         if (stage == XB_ST_FETCH) {
+            if (args.left_out && __shfl_sync(XB_FULL, xb_grow_flag(args, lane), 0)) {
+                /* the table is to grow: leave the rest for the resume launch */
+                xb_src_leave(args, src, lane, src.item, src.nitems);
+                break;
+            }
             bool done = false, failed = false;
             mask = xb_fetch_batch(args, plan, meta, R, src, lane, ws, &done, &failed);
             if (done || failed)
@@ -706,6 +711,14 @@ xb_exec_body(const XbExecArgs &args, char *smem)
                         full = false;
                         e = xb_group_get<false>(plan, R, lane, gt->entries, gt->cap_mask, hash, gt, st, &full);
                         if (!e && full) {
+                            /* no room: an entry of the dump region */
+                            char *slot = xb_dump_slot(gt, plan->gent_size);
+                            if (slot) {
+                                full = false;
+                                e = xb_group_get<false>(plan, R, lane, slot, 0, hash, gt, st, &full);
+                            }
+                        }
+                        if (!e && full) {
                             XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
                             atomicOr(&gt->overflow, 1u);
                         }
@@ -753,14 +766,9 @@ xb_exec_body(const XbExecArgs &args, char *smem)
             if (h->state != XB_GSTATE_READY)
                 continue;
             const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
-            bool full = false;
-            char *g = xb_group_find(plan, gt->entries, gt->cap_mask, h->hash, img, gt, st, &full);
+            char *g = xb_group_find_or_dump(plan, gt, h->hash, img, st);
             if (g)
                 xb_merge_states(plan, g, e);
-            else if (full) {
-                XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
-                atomicOr(&gt->overflow, 1u);
-            }
         }
     }
 }
@@ -1823,13 +1831,103 @@ xb_merge_final(XbMergeArgs args)
             XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_TUPLE);
             continue;
         }
-        bool full = false;
-        char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, ti->hash, img, args.gt, args.st, &full);
+        char *g = xb_group_find_or_dump(plan, args.gt, ti->hash, img, args.st);
         if (g)
             xb_merge_states(plan, g, src);
+    }
+}
+
+/* ----------------------------------------------------------------
+ * group-table growth: the live entries of the old table rehashed into a
+ * larger one, then the dump entries (groups created while the table had
+ * no room) merged in.  Key bytes live in the key arena; when the arena is
+ * replaced by a larger copy, key pointers are moved with it.
+ * ---------------------------------------------------------------- */
+struct XbGrowArgs {
+    const xb_plan  *plan;
+    const char     *old_entries;
+    uint64_t        old_cap;
+    char           *dump;
+    uint64_t        ndump;
+    xb_gtable      *gt;             /* the new table (device) */
+    xb_status      *st;
+    const char     *arena_old;      /* key pointers in [arena_old, +arena_old_sz) move */
+    uint64_t        arena_old_sz;
+    char           *arena_new;
+};
+
+__device__ __forceinline__ void
+xb_gt_relocate_keys(const xb_plan *plan, char *e, const XbGrowArgs &a)
+{
+    if (a.arena_new == a.arena_old)
+        return;
+    xb_keyimg *img = (xb_keyimg *)(e + plan->gent_keys_off);
+    for (uint32_t k = 0; k < plan->nkeys; k++) {
+        if (img[k].isnull || (plan->keys[k].rk != XB_RK_TEXT && plan->keys[k].rk != XB_RK_NUM))
+            continue;
+        const uint64_t v = img[k].val, lo = (uint64_t)a.arena_old;
+        if (v >= lo && v < lo + a.arena_old_sz)
+            img[k].val = (uint64_t)a.arena_new + (v - lo);
+    }
+}
+
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_gt_rehash(XbGrowArgs a)
+{
+    const xb_plan *plan = a.plan;
+    const uint32_t gsz = plan->gent_size;
+    xb_gtable *gt = a.gt;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.old_cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const char *e = a.old_entries + i * gsz;
+        const xb_gent_head *h = (const xb_gent_head *)e;
+        if (h->state != XB_GSTATE_READY)
+            continue;
+        /* keys are distinct: the first EMPTY slot of the probe sequence */
+        uint64_t pos = h->hash & gt->cap_mask;
+        bool placed = false;
+        for (uint64_t probe = 0; probe <= gt->cap_mask; probe++) {
+            char *d = gt->entries + pos * gsz;
+            xb_gent_head *dh = (xb_gent_head *)d;
+            if (atomicCAS(&dh->state, XB_GSTATE_EMPTY, XB_GSTATE_BUSY) == XB_GSTATE_EMPTY) {
+                for (uint32_t w = 1; w < gsz / 8; w++)
+                    ((uint64_t *)d)[w] = ((const uint64_t *)e)[w];
+                dh->hash = h->hash;
+                xb_gt_relocate_keys(plan, d, a);
+                atomicAdd((unsigned long long *)&gt->nused, 1ULL);
+                xb_st_release(&dh->state, XB_GSTATE_READY);
+                placed = true;
+                break;
+            }
+            pos = (pos + 1) & gt->cap_mask;
+        }
+        if (!placed) {
+            XB_RAISE(a.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+            atomicOr(&gt->overflow, 1u);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(XB_BLOCK)
+xb_gt_merge_dump(XbGrowArgs a)
+{
+    const xb_plan *plan = a.plan;
+    const uint32_t gsz = plan->gent_size;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.ndump;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        char *e = a.dump + i * gsz;
+        const xb_gent_head *h = (const xb_gent_head *)e;
+        if (h->state != XB_GSTATE_READY)
+            continue;
+        xb_gt_relocate_keys(plan, e, a);
+        const xb_keyimg *img = (const xb_keyimg *)(e + plan->gent_keys_off);
+        bool full = false;
+        char *g = xb_group_find(plan, a.gt->entries, a.gt->cap_mask, h->hash, img, a.gt, a.st, &full);
+        if (g)
+            xb_merge_states(plan, g, e);
         else if (full) {
-            XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
-            atomicOr(&args.gt->overflow, 1u);
+            XB_RAISE(a.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+            atomicOr(&a.gt->overflow, 1u);
         }
     }
 }
@@ -2098,7 +2196,7 @@ struct xpuB200Session {
     std::vector<uint64_t> d_alloc_sz;
     xb_inner_entry *inner_entry = nullptr;  /* cached inner relations in use */
     bool            inner_hit = false;      /* found built by an earlier session */
-    xb_gtable       h_gt;
+    xb_gtable       h_gt = {};
     xb_gtable      *d_gt = nullptr;
     xb_status      *d_status = nullptr;
     xb_status      *h_status = nullptr;     /* pinned */
@@ -2150,6 +2248,18 @@ struct xpuB200Session {
     uint32_t        part_rec = 0;
     bool            part_used = false;
     bool            in_batch = false;       /* a prepared batch's launch is being issued */
+    /* group-table growth: where stopped warps record their leftover work
+     * (two lists: a resume launch reads one and records into the other),
+     * and the launch xb_run is issuing */
+    XbLeft         *d_left[2] = {nullptr, nullptr};
+    uint32_t        left_cap = 0;
+    bool            run_growth = false;
+    bool            run_resume = false;
+    uint32_t        run_left_sel = 0;
+    uint32_t        run_left_in_n = 0;
+    uint64_t        run_static_base0 = 0;
+    uint64_t        run_cursor0 = 0;
+    uint32_t        grow_count = 0;         /* times the group table grew */
 };
 
 /* shared group-table capacity 'cap' and the launch geometry that follows
@@ -2197,6 +2307,8 @@ static const char *xb_msg_text(uint32_t id)
     case XB_MSG_ARENA_FULL:       return "GpuPreAgg(GroupBy) - no space for variable-length keys";
     case XB_MSG_BAD_PAGE:         return "corrupted heap page";
     case XB_MSG_ARROW_TYPE:       return "Arrow column type does not match the device type";
+    case XB_MSG_NUMERIC_TYPE:     return "numeric key or argument of an unsupported form";
+    case XB_MSG_LEFT_FULL:        return "no room to record the work left for after the group table grows";
     default:                      return "device error";
     }
 }
@@ -2220,6 +2332,14 @@ static int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int
     return (int)code;
 }
 #define XB_ERR(err, code, ...) xb_set_error((err), (code), __func__, __LINE__, __VA_ARGS__)
+/* a CUDA call's result as 0 or a filled ERRCODE_DEVICE_FATAL */
+#define xb_set_cuda(call_rc, err) xb_cuda_rc((call_rc), (err), __func__, __LINE__)
+static int xb_cuda_rc(cudaError_t rc, kern_errorbuf *err, const char *func, int line)
+{
+    if (rc == cudaSuccess)
+        return 0;
+    return xb_set_error(err, ERRCODE_DEVICE_FATAL, func, line, "%s", cudaGetErrorString(rc));
+}
 #define XB_CUDA(call, err) do {                                               \
         cudaError_t __rc = (call);                                            \
         if (__rc != cudaSuccess)                                              \
@@ -2319,6 +2439,10 @@ static void xb_session_free(xpuB200Session *s)
     if (s->d_dst) cudaFreeAsync(s->d_dst, st);
     if (s->part_buf) cudaFreeAsync(s->part_buf, st);
     if (s->part_cnt) cudaFreeAsync(s->part_cnt, st);
+    for (int i = 0; i < 2; i++)
+        if (s->d_left[i]) cudaFreeAsync(s->d_left[i], st);
+    if (s->h_plan && s->h_plan->has_groupby && s->h_gt.dump)
+        cudaFreeAsync(s->h_gt.dump, st);
     cudaStreamSynchronize(st);
     if (s->inner_entry)
         xb_inner_cache_put(s->dev, s->inner_entry);
@@ -2476,6 +2600,11 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
         s->h_gt.arena_sz = arena;
         s->h_gt.arena_used = 0;
         s->h_gt.overflow = 0;
+        s->h_gt.grow = 0;
+        s->h_gt.soft_cap = cap / 2;
+        s->h_gt.dump = nullptr;
+        s->h_gt.dump_cap = 0;
+        s->h_gt.dump_used = 0;
         DALLOC(cap * plan->gent_size, &s->h_gt.entries);
         DALLOC(arena, &s->h_gt.arena);
         cudaMemsetAsync(s->h_gt.entries, 0, cap * plan->gent_size, st);
@@ -2906,6 +3035,200 @@ static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format,
     return true;
 }
 
+/* ----------------------------------------------------------------
+ * group-table growth (host side)
+ *
+ * The reference's service answers SUSPEND_NO_SPACE on kds_final by
+ * expanding the buffer and relaunching the suspended kernel
+ * (gpu_service.c:2418-2470, :3872-3879; resume at cuda_gpujoin.cu:
+ * 1098-1103).  Here the table asks to grow before it is full: once half of
+ * its slots are in use (or half of the key arena), every warp of a launch
+ * on the session's stream stops after its current 32-row batch and records
+ * the work it held (XbLeft ranges).  Groups that meanwhile find the table
+ * without room take an entry of the dump region.  The host then rehashes
+ * the live entries into a table at least twice as large, merges the dump
+ * entries in, and a resume launch processes the recorded ranges and the
+ * units nobody had claimed.  No row is applied twice or lost.
+ * ---------------------------------------------------------------- */
+
+static int xb_wait_status(xpuB200Session *s, kern_errorbuf *err);
+static int xb_gt_settle(xpuB200Session *s, kern_errorbuf *err);
+
+/* the dump region, sized for a launch of 'grid' CTAs: every CTA's shared
+ * table merged at exit, plus the rows in flight after the table asked to
+ * grow when its free half is smaller than twice those */
+static int xb_dump_ensure(xpuB200Session *s, int grid, uint32_t sm_cap, cudaStream_t st, kern_errorbuf *err)
+{
+    const uint64_t cap = s->h_gt.cap_mask + 1;
+    const uint64_t inflight = (uint64_t)grid * XB_WARPS * 32;
+    uint64_t need = (uint64_t)grid * sm_cap;
+    if (cap / 2 < 2 * inflight)
+        need += inflight;
+    if (need < 1024)
+        need = 1024;
+    if (s->h_gt.dump && s->h_gt.dump_cap >= need)
+        return 0;
+    if (s->h_gt.dump) {
+        /* entries a served or mixed launch left in the old region join the
+         * table before the region is replaced */
+        int rc = xb_gt_settle(s, err);
+        if (rc) return rc;
+    }
+    const uint64_t gsz = s->h_plan->gent_size;
+    char *d = nullptr;
+    if (cudaMallocAsync((void **)&d, need * gsz, st) != cudaSuccess) {
+        cudaGetLastError();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for the group dump (%llu entries)",
+                      (unsigned long long)need);
+    }
+    cudaMemsetAsync(d, 0, need * gsz, st);
+    if (s->h_gt.dump)
+        cudaFreeAsync(s->h_gt.dump, st);
+    s->h_gt.dump = d;
+    s->h_gt.dump_cap = need;
+    static_assert(offsetof(xb_gtable, dump_cap) == offsetof(xb_gtable, dump) + 8, "dump fields");
+    XB_CUDA(cudaMemcpyAsync(&s->d_gt->dump, &s->h_gt.dump, 16, cudaMemcpyHostToDevice, st), err);
+    return 0;
+}
+
+/* the device's copy of the group table header (synchronises the stream) */
+static int xb_gt_read(xpuB200Session *s, xb_gtable *g, kern_errorbuf *err)
+{
+    XB_CUDA(cudaMemcpyAsync(g, s->d_gt, sizeof(xb_gtable), cudaMemcpyDeviceToHost, s->stream), err);
+    XB_CUDA(cudaStreamSynchronize(s->stream), err);
+    return 0;
+}
+
+/* replace a tracked session allocation by another one */
+static void xb_swap_alloc(xpuB200Session *s, void *old_p, void *new_p, uint64_t new_sz)
+{
+    for (size_t i = 0; i < s->d_allocs.size(); i++) {
+        if (s->d_allocs[i] == old_p) {
+            s->d_allocs[i] = new_p;
+            s->d_alloc_sz[i] = new_sz;
+            return;
+        }
+    }
+    s->d_allocs.push_back(new_p);
+    s->d_alloc_sz.push_back(new_sz);
+}
+
+/* grow the group table: at least twice the slots, and room for
+ * min_entries groups at a load of 1/4 (1/2 above a million); the key
+ * arena doubles when more than half of it is used.  Session lock held;
+ * the stream is idle on entry and on return. */
+static int xb_gt_grow(xpuB200Session *s, uint64_t min_entries, kern_errorbuf *err)
+{
+    cudaStream_t st = s->stream;
+    const xb_plan *plan = s->h_plan;
+    xb_gtable g;
+    int rc = xb_gt_read(s, &g, err);
+    if (rc) return rc;
+    const uint64_t gsz = plan->gent_size;
+    const uint64_t cap = g.cap_mask + 1;
+    const uint64_t ndump = g.dump_used < g.dump_cap ? g.dump_used : g.dump_cap;
+    uint64_t want = g.nused > min_entries ? g.nused : min_entries;
+    uint64_t new_cap = xb_next_pow2(want * (want > 1000000 ? 2 : 4) + 1024);
+    if (new_cap < cap * 2)
+        new_cap = cap * 2;
+    const uint64_t max_cap = (s->dev->hbm_budget / 4) / gsz;
+    if (new_cap > max_cap) {
+        uint64_t c = xb_next_pow2(max_cap / 2 + 1);
+        if (c <= cap)
+            return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE,
+                          "GpuPreAgg(GroupBy) - the group table of %llu slots cannot grow within the "
+                          "device memory budget", (unsigned long long)cap);
+        new_cap = c;
+    }
+    /* the key arena: a larger copy when more than half of it is used */
+    char *arena_new = g.arena;
+    uint64_t arena_new_sz = g.arena_sz;
+    const uint64_t arena_used = g.arena_used < g.arena_sz ? g.arena_used : g.arena_sz;
+    if (plan->nkeys_text && g.arena_used > g.arena_sz / 2) {
+        arena_new_sz = g.arena_sz * 2 > g.arena_used * 4 ? g.arena_sz * 2 : g.arena_used * 4;
+        if (cudaMallocAsync((void **)&arena_new, arena_new_sz, st) != cudaSuccess) {
+            cudaGetLastError();
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory growing the key arena");
+        }
+        cudaMemcpyAsync(arena_new, g.arena, arena_used, cudaMemcpyDeviceToDevice, st);
+    }
+    char *entries_new = nullptr;
+    if (cudaMallocAsync((void **)&entries_new, new_cap * gsz, st) != cudaSuccess) {
+        cudaGetLastError();
+        if (arena_new != g.arena) cudaFreeAsync(arena_new, st);
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory growing the group table to %llu slots",
+                      (unsigned long long)new_cap);
+    }
+    cudaMemsetAsync(entries_new, 0, new_cap * gsz, st);
+    xb_gtable ng = g;
+    ng.cap_mask = new_cap - 1;
+    ng.nused = 0;
+    ng.entries = entries_new;
+    ng.arena = arena_new;
+    ng.arena_sz = arena_new_sz;
+    ng.arena_used = arena_used;
+    ng.overflow = 0;
+    ng.grow = 0;
+    ng.soft_cap = new_cap / 2;
+    ng.dump_used = 0;
+    XB_CUDA(cudaMemcpyAsync(s->d_gt, &ng, sizeof(xb_gtable), cudaMemcpyHostToDevice, st), err);
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
+    XbGrowArgs ga;
+    ga.plan = s->d_plan;
+    ga.old_entries = g.entries;
+    ga.old_cap = cap;
+    ga.dump = g.dump;
+    ga.ndump = ndump;
+    ga.gt = s->d_gt;
+    ga.st = s->d_status;
+    ga.arena_old = g.arena;
+    ga.arena_old_sz = g.arena_sz;
+    ga.arena_new = arena_new;
+    const int grid = s->dev->nsm * 8;
+    xb_gt_rehash<<<grid, XB_BLOCK, 0, st>>>(ga);
+    if (ndump) {
+        xb_gt_merge_dump<<<grid, XB_BLOCK, 0, st>>>(ga);
+        cudaMemsetAsync(g.dump, 0, ndump * gsz, st);
+    }
+    cudaError_t lrc = cudaGetLastError();
+    if (lrc != cudaSuccess)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "group table growth: %s", cudaGetErrorString(lrc));
+    rc = xb_wait_status(s, err);
+    cudaFreeAsync(g.entries, st);
+    xb_swap_alloc(s, g.entries, entries_new, new_cap * gsz);
+    if (arena_new != g.arena) {
+        cudaFreeAsync(g.arena, st);
+        xb_swap_alloc(s, g.arena, arena_new, arena_new_sz);
+    }
+    s->h_gt = ng;
+    s->grow_count++;
+    return rc;
+}
+
+/* pending dump entries (left by launches that do not stop for growth:
+ * served and mixed launches) merged into a grown table; session lock held */
+static int xb_gt_settle(xpuB200Session *s, kern_errorbuf *err)
+{
+    if (!s->h_plan->has_groupby || !s->h_gt.dump)
+        return 0;
+    xb_gtable g;
+    int rc = xb_gt_read(s, &g, err);
+    if (rc) return rc;
+    if (g.dump_used == 0)
+        return 0;
+    return xb_gt_grow(s, 0, err);
+}
+
+/* sum of two launches' statistics */
+static void xb_status_add(xb_status *t, const xb_status *h)
+{
+    t->nitems_raw += h->nitems_raw;
+    t->nitems_in += h->nitems_in;
+    t->nitems_out += h->nitems_out;
+    for (uint32_t d = 0; d <= XB_MAX_DEPTH; d++)
+        t->nitems_depth[d] += h->nitems_depth[d];
+}
+
 static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                         uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
                         kern_errorbuf *err)
@@ -2923,7 +3246,6 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     a.dst = s->launch_dst;
     a.dst_len = s->launch_dst_len;
     a.dyn_only = 0;
-    a.__pad = 0;
     a.gt = s->d_gt;
     a.st = d_status;
     void *fn = xb_session_jit(s, format);
@@ -2932,6 +3254,25 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     if ((uint64_t)grid * XB_WARPS > warps_needed)
         grid = (int)((warps_needed + XB_WARPS - 1) / XB_WARPS);
     if (grid < 1) grid = 1;
+    if (stream == s->stream && s->run_growth) {
+        /* group-table growth (xb_run): warps that see the table ask to
+         * grow record their leftover work here and stop */
+        a.left_out = s->d_left[s->run_left_sel];
+        a.left_cap = s->left_cap;
+        if (s->run_resume) {
+            a.resume = 1;
+            a.left_in = s->d_left[s->run_left_sel ^ 1];
+            a.left_in_n = s->run_left_in_n;
+            a.static_base0 = s->run_static_base0;
+            a.cursor0 = s->run_cursor0;
+        } else {
+            /* the static share each warp takes first (xb_src_start) */
+            const uint64_t warps = (uint64_t)grid * XB_WARPS;
+            s->run_static_base0 = format == KDS_FORMAT_BLOCK ? ((nunits * 3 / 5) / warps) * warps : 0;
+        }
+        if (xb_dump_ensure(s, grid, s->sm_cap, stream, err) != 0)
+            return err ? err->errcode : ERRCODE_DEVICE_FATAL;
+    }
     if (format < 256)
         s->ran_kind[format] = fn ? 'j' : 'v';
     const bool part = fn && s->jit_replay[format] && xb_part_prepare(s, nunits, format, stream);
@@ -2967,9 +3308,9 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     return 0;
 }
 
-/* single-chunk launch through the session's task buffer */
-static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
-                          const kern_data_store *h_kds_head, kern_errorbuf *err)
+/* a single chunk as the session's one-task work queue */
+static int xb_exec_task_of(xpuB200Session *s, const kern_data_store *d_kds,
+                           const kern_data_store *h_kds_head, xb_task *t, kern_errorbuf *err)
 {
     if (h_kds_head->format != KDS_FORMAT_BLOCK && h_kds_head->format != KDS_FORMAT_ARROW &&
         h_kds_head->format != KDS_FORMAT_ROW)
@@ -2978,12 +3319,21 @@ static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
         XB_CUDA(cudaMallocAsync((void **)&s->d_tasks, sizeof(xb_task) * 16, s->stream), err);
         s->d_tasks_cap = 16;
     }
+    t->kds = d_kds;
+    t->unit_base = 0;
+    t->nunits = xb_chunk_units(h_kds_head);
+    t->format = (uint32_t)h_kds_head->format;
+    XB_CUDA(cudaMemcpyAsync(s->d_tasks, t, sizeof(*t), cudaMemcpyHostToDevice, s->stream), err);
+    return 0;
+}
+
+/* single-chunk launch through the session's task buffer */
+static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
+                          const kern_data_store *h_kds_head, kern_errorbuf *err)
+{
     xb_task t;
-    t.kds = d_kds;
-    t.unit_base = 0;
-    t.nunits = xb_chunk_units(h_kds_head);
-    t.format = (uint32_t)h_kds_head->format;
-    XB_CUDA(cudaMemcpyAsync(s->d_tasks, &t, sizeof(t), cudaMemcpyHostToDevice, s->stream), err);
+    int rc = xb_exec_task_of(s, d_kds, h_kds_head, &t, err);
+    if (rc) return rc;
     return xb_launch_tasks(s, s->d_tasks, 1, t.nunits, t.format, err);
 }
 
@@ -3064,13 +3414,116 @@ static void xb_account(xpuB200Session *s, kern_exec_results *results)
     xb_account_status(s, s->h_status, results);
 }
 
-static int xb_finish_task(xpuB200Session *s, kern_exec_results *results, kern_errorbuf *err)
+
+/* the replay of partitioned aggregation again, for the records a full
+ * table left (after the table grew) */
+static int xb_replay_retry(xpuB200Session *s, uint32_t format, kern_errorbuf *err)
 {
-    int rc = xb_wait_status(s, err);
-    if (rc)
-        return rc;
-    xb_account(s, results);
-    return 0;
+    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
+    XbReplayArgs ra;
+    memset(&ra, 0, sizeof(ra));
+    ra.plan = s->d_plan;
+    ra.gt = s->d_gt;
+    ra.st = s->d_status;
+    ra.part_buf = s->part_buf;
+    ra.part_cnt = s->part_cnt;
+    ra.part_cap = s->part_cap;
+    ra.nparts = s->nparts;
+    ra.retry = 1;
+    if (!s->jit_replay[format] ||
+        xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK, 0, (void *)s->stream, &ra) != 0)
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "replay kernel launch failed");
+    return xb_wait_status(s, err);
+}
+
+/*
+ * Run a work queue on the session's stream to the end, growing the group
+ * table as often as it asks to: after each launch the host grows the
+ * table when asked (or when dump entries wait), replays the records a
+ * full table left, and issues a resume launch for the work the stopped
+ * warps recorded plus the units nobody claimed.  The statistics of all
+ * launches are added to the session and written to *results.  timed:
+ * ev0 / ev1 bracket every launch of the run.
+ */
+static int xb_run(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks, uint64_t nunits,
+                  uint32_t format, kern_exec_results *results, kern_errorbuf *err, bool timed = false)
+{
+    cudaStream_t st = s->stream;
+    const bool growth = s->h_plan->has_groupby != 0 && s->h_gt.entries != nullptr;
+    if (growth && !s->d_left[0]) {
+        /* two leftover records per warp of the largest grid (8 CTAs per SM) */
+        const uint32_t cap = 2u * (uint32_t)s->dev->nsm * 8u * XB_WARPS;
+        for (int i = 0; i < 2; i++)
+            if (cudaMallocAsync((void **)&s->d_left[i], sizeof(XbLeft) * cap, st) != cudaSuccess) {
+                cudaGetLastError();
+                return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for leftover ranges");
+            }
+        s->left_cap = cap;
+    }
+    xb_status total;
+    memset(&total, 0, sizeof(total));
+    s->run_growth = growth;
+    s->run_resume = false;
+    s->run_left_sel = 0;
+    s->run_cursor0 = 0;
+    int rc = 0;
+    for (uint32_t round = 0;; round++) {
+        if (round > 64) {
+            rc = XB_ERR(err, ERRCODE_DEVICE_ERROR, "the group table kept asking to grow (%u launches)", round);
+            break;
+        }
+        if ((rc = xb_set_cuda(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err)) != 0)
+            break;
+        if (timed && round == 0)
+            cudaEventRecord(s->ev0, st);
+        rc = xb_launch_tasks(s, d_tasks, ntasks, nunits, format, err);
+        if (rc) break;
+        if (timed)
+            cudaEventRecord(s->ev1, st);
+        rc = xb_wait_status(s, err);
+        if (rc) break;
+        const xb_status hs = *s->h_status;
+        xb_status_add(&total, &hs);
+        if (!growth)
+            break;
+        xb_gtable g;
+        if ((rc = xb_gt_read(s, &g, err)) != 0)
+            break;
+        if (g.grow || g.dump_used) {
+            if ((rc = xb_gt_grow(s, 0, err)) != 0)
+                break;
+        }
+        /* the replay's records that found the table full, after it grew */
+        bool left = hs.replay_left != 0;
+        for (uint32_t r = 0; left && r < 64; r++) {
+            if ((rc = xb_replay_retry(s, format, err)) != 0)
+                break;
+            left = s->h_status->replay_left != 0;
+            if ((rc = xb_gt_read(s, &g, err)) != 0)
+                break;
+            if (g.grow || g.dump_used)
+                if ((rc = xb_gt_grow(s, 0, err)) != 0)
+                    break;
+        }
+        if (rc) break;
+        if (left) {
+            rc = XB_ERR(err, ERRCODE_DEVICE_ERROR, "deferred group updates kept finding the table full");
+            break;
+        }
+        if (!hs.stopped)
+            break;
+        /* resume: the ranges the stopped warps recorded, then the units
+         * the stopped launch's cursor had not handed out */
+        s->run_resume = true;
+        s->run_left_in_n = hs.left_n;
+        s->run_cursor0 += hs.unit_cursor;
+        s->run_left_sel ^= 1;
+    }
+    s->run_growth = false;
+    s->run_resume = false;
+    if (rc == 0)
+        xb_account_status(s, &total, results);
+    return rc;
 }
 
 static int xb_place_src(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
@@ -3094,10 +3547,10 @@ xpuB200ExecTask(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_o
     std::vector<char> hbuf;
     int rc = xb_place_src(s, kds_src, kds_src_on_device, &head, &hbuf, &d_kds, err);
     if (rc) return rc;
-    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
-    rc = xb_launch_exec(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, err);
+    xb_task t;
+    rc = xb_exec_task_of(s, d_kds, kds_src_on_device ? (const kern_data_store *)hbuf.data() : &head, &t, err);
     if (rc) return rc;
-    return xb_finish_task(s, results, err);
+    return xb_run(s, s->d_tasks, 1, t.nunits, t.format, results, err);
 }
 
 /* validate a chunk and make it device-resident: host chunks are copied to
@@ -3236,7 +3689,6 @@ xpuB200TimeExecTask(xpuB200Session *s, const kern_data_store *kds_src_dev, int n
     xb_clear_error(err);
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->stream;
     kern_data_store head;
     if (((uintptr_t)kds_src_dev & 7) != 0)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
@@ -3246,13 +3698,11 @@ xpuB200TimeExecTask(xpuB200Session *s, const kern_data_store *kds_src_dev, int n
     int rc = xb_check_kds((const kern_data_store *)hbuf.data(), err);
     if (rc) return rc;
     float total = 0.0f;
+    xb_task t;
+    rc = xb_exec_task_of(s, kds_src_dev, (const kern_data_store *)hbuf.data(), &t, err);
+    if (rc) return rc;
     for (int i = 0; i < niters; i++) {
-        XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
-        cudaEventRecord(s->ev0, st);
-        rc = xb_launch_exec(s, kds_src_dev, (const kern_data_store *)hbuf.data(), err);
-        if (rc) return rc;
-        cudaEventRecord(s->ev1, st);
-        rc = xb_finish_task(s, nullptr, err);
+        rc = xb_run(s, s->d_tasks, 1, t.nunits, t.format, nullptr, err, true);
         if (rc) return rc;
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -3404,6 +3854,9 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
         if (p_required) *p_required = 0;
         return 0;
     }
+    /* groups waiting in the dump region join the table first */
+    int src = xb_gt_settle(s, err);
+    if (src) return src;
     const kern_session_info *session = (const kern_session_info *)s->h_session.data();
     const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
     const uint64_t head_len = KDS_HEAD_LENGTH(fh);
@@ -3502,7 +3955,9 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     kh->format = row_fmt ? KDS_FORMAT_ROW : KDS_FORMAT_HASH;
     kh->hash_nslots = (uint32_t)nslots;
     cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(d_out + head_len, 0, 8 * nslots + 8 * ngroups, st);
+    /* slots, row index and items: the padding between and after the
+     * tuples' attributes is zero, so equal results are equal bytes */
+    cudaMemsetAsync(d_out + head_len, 0, length - head_len, st);
     fa.kds_final = d_out;
     fa.items_base = items_base;
     fa.length = length;
@@ -3557,6 +4012,18 @@ xpuB200MergeFinal(xpuB200Session *s, const kern_data_store *kds_final, int kds_f
         XB_CUDA(cudaMemcpyAsync(d_copy, kds_final, h->length, cudaMemcpyHostToDevice, st), err);
         d_kds = (const kern_data_store *)d_copy;
     }
+    /* room for every incoming group before the merge (the table grows as
+     * for chunk launches when it would pass half of its slots) */
+    {
+        xb_gtable gh;
+        int rc = xb_gt_read(s, &gh, err);
+        if (!rc && (gh.dump_used || gh.nused + h->nitems > gh.soft_cap))
+            rc = xb_gt_grow(s, gh.nused + h->nitems, err);
+        if (rc) {
+            if (d_copy) cudaFreeAsync(d_copy, st);
+            return rc;
+        }
+    }
     XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
     XbMergeArgs ma;
     ma.plan = s->d_plan;
@@ -3568,7 +4035,9 @@ xpuB200MergeFinal(xpuB200Session *s, const kern_data_store *kds_final, int kds_f
     xb_merge_final<<<grid, XB_BLOCK, 0, st>>>(ma);
     if (d_copy)
         cudaFreeAsync(d_copy, st);
-    return xb_wait_status(s, err);
+    int mrc = xb_wait_status(s, err);
+    if (mrc) return mrc;
+    return xb_gt_settle(s, err);
 }
 
 /* ----------------------------------------------------------------
@@ -3644,6 +4113,17 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     if (!plan->has_groupby) {
         if (p_required) *p_required = 0;
         return 0;
+    }
+    if (s->h_gt.dump) {
+        /* groups in the dump region join the table only when it grows,
+         * which allocates: that is xpuB200Final's work */
+        xb_gtable gh;
+        int grc = xb_gt_read(s, &gh, err);
+        if (grc) return grc;
+        if (gh.dump_used)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR,
+                          "FinalNoAlloc: %llu groups wait for the group table to grow; use xpuB200Final",
+                          (unsigned long long)gh.dump_used);
     }
     const kern_session_info *session = (const kern_session_info *)s->h_session.data();
     const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
@@ -3737,7 +4217,9 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     kh->format = row_fmt ? KDS_FORMAT_ROW : KDS_FORMAT_HASH;
     kh->hash_nslots = (uint32_t)nslots;
     cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(d_out + head_len, 0, 8 * nslots + 8 * ngroups, st);
+    /* slots, row index and items: the padding between and after the
+     * tuples' attributes is zero, so equal results are equal bytes */
+    cudaMemsetAsync(d_out + head_len, 0, length - head_len, st);
     fa.kds_final = d_out;
     fa.items_base = items_base;
     fa.length = length;
@@ -3833,12 +4315,10 @@ xpuB200BatchExec(xpuB200Batch *b, kern_exec_results *results, kern_errorbuf *err
     xpuB200Session *s = b->sess;
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
     s->in_batch = true;
-    int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
+    int rc = xb_run(s, b->d_tasks, b->ntasks, b->nunits, b->format, results, err);
     s->in_batch = false;
-    if (rc) return rc;
-    return xb_finish_task(s, results, err);
+    return rc;
 }
 
 extern "C" int
@@ -3848,17 +4328,11 @@ xpuB200BatchTime(xpuB200Batch *b, int niters, double *p_msec, kern_errorbuf *err
     xpuB200Session *s = b->sess;
     std::lock_guard<std::mutex> g(s->lock);
     XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    cudaStream_t st = s->stream;
     float total = 0.0f;
     for (int i = 0; i < niters; i++) {
-        XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st), err);
-        cudaEventRecord(s->ev0, st);
         s->in_batch = true;
-        int rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, b->format, err);
+        int rc = xb_run(s, b->d_tasks, b->ntasks, b->nunits, b->format, nullptr, err, true);
         s->in_batch = false;
-        if (rc) return rc;
-        cudaEventRecord(s->ev1, st);
-        rc = xb_finish_task(s, nullptr, err);
         if (rc) return rc;
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -3875,9 +4349,14 @@ static void xb_reset_groups(xpuB200Session *s)
     cudaStream_t st = s->stream;
     if (s->h_plan->has_groupby) {
         cudaMemsetAsync(s->h_gt.entries, 0, (s->h_gt.cap_mask + 1) * s->h_plan->gent_size, st);
+        if (s->h_gt.dump)
+            cudaMemsetAsync(s->h_gt.dump, 0, s->h_gt.dump_cap * s->h_plan->gent_size, st);
         s->h_gt.nused = 0;
         s->h_gt.arena_used = 0;
         s->h_gt.overflow = 0;
+        s->h_gt.grow = 0;
+        s->h_gt.dump_used = 0;
+        s->h_gt.soft_cap = (s->h_gt.cap_mask + 1) / 2;
         cudaMemcpyAsync(s->d_gt, &s->h_gt, sizeof(xb_gtable), cudaMemcpyHostToDevice, st);
     }
     cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st);
@@ -3902,7 +4381,6 @@ xpuB200BatchTune(xpuB200Batch *b, uint32_t flags, char *report, size_t report_le
     s->tune_looked_up = true;               /* measured here, not adopted */
     const xb_plan *plan = s->h_plan;
     const uint32_t fmt = b->format;
-    cudaStream_t st = s->stream;
     bool gid = false;
     for (uint32_t d = 1; d <= plan->nrels; d++)
         gid |= plan->inner[d].gid_on != 0;
@@ -3929,13 +4407,9 @@ xpuB200BatchTune(xpuB200Batch *b, uint32_t flags, char *report, size_t report_le
         double best = 1e30;
         for (int r = 0; r < 3 && rc == 0; r++) {      /* the first run builds and warms */
             xb_reset_groups(s);
-            cudaEventRecord(s->ev0, st);
             s->in_batch = true;
-            rc = xb_launch_tasks(s, b->d_tasks, b->ntasks, b->nunits, fmt, err);
+            rc = xb_run(s, b->d_tasks, b->ntasks, b->nunits, fmt, nullptr, err, true);
             s->in_batch = false;
-            if (rc) break;
-            cudaEventRecord(s->ev1, st);
-            rc = xb_wait_status(s, err);
             if (rc) break;
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -5090,14 +5564,15 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
              "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u], "
              "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\", "
              "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u, \"inner_cache\": %s, "
-             "\"partitions\": %u, \"partition_used\": %s}",
+             "\"partitions\": %u, \"partition_used\": %s, \"gtable_grew\": %u, \"gtable_dump_cap\": %llu}",
              p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
              p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
              s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash,
              s->jit_enabled ? "true" : "false", kinds.c_str(), s->jit_compile_ms, msg.c_str(),
              s->jit_minb, s->sm_cap_default,
              s->inner_hit ? "\"hit\"" : s->inner_entry ? "\"built\"" : "\"none\"",
-             s->nparts, s->part_used ? "true" : "false");
+             s->nparts, s->part_used ? "true" : "false", s->grow_count,
+             (unsigned long long)(p->has_groupby ? s->h_gt.dump_cap : 0));
     return 0;
 }
 

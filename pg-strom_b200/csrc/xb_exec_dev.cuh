@@ -117,6 +117,42 @@ __device__ __forceinline__ void xb_st_release(uint32_t *p, uint32_t v)
     asm volatile("st.release.gpu.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
+__device__ __forceinline__ uint32_t xb_ld_relaxed(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+/* ================================================================
+ * group-table growth (the device half; the host rehashes the table)
+ * ================================================================ */
+__device__ __forceinline__ void xb_gt_want_grow(xb_gtable *gt)
+{
+    if (*(volatile uint32_t *)&gt->grow == 0)
+        atomicExch(&gt->grow, 1u);
+}
+
+/* count a new entry of the global table; once soft_cap entries are in
+ * use the table asks to grow */
+__device__ __forceinline__ void xb_gt_count_new(xb_gtable *gt)
+{
+    const unsigned long long n = atomicAdd((unsigned long long *)&gt->nused, 1ULL) + 1ULL;
+    if (n >= gt->soft_cap)
+        xb_gt_want_grow(gt);
+}
+
+/* a fresh (EMPTY) entry of the dump region for a group the table had no
+ * room for; nullptr when the session has none left */
+__device__ __forceinline__ char *xb_dump_slot(xb_gtable *gt, uint32_t gent_size)
+{
+    if (!gt->dump)
+        return nullptr;
+    xb_gt_want_grow(gt);
+    const unsigned long long i = atomicAdd((unsigned long long *)&gt->dump_used, 1ULL);
+    return i < gt->dump_cap ? gt->dump + i * (uint64_t)gent_size : nullptr;
+}
+
 /* L2 prefetch of a contiguous range by the TMA engine (sm_90+) */
 __device__ __forceinline__ void xb_prefetch_l2(const void *p, uint32_t bytes)
 {
@@ -458,6 +494,8 @@ xb_key_store(const xb_key &k, const xb_keyimg &src, xb_keyimg *dst,
                                                : xb_numeric_varsize((const uint8_t *)src.val);
         unsigned long long off = atomicAdd((unsigned long long *)&gt->arena_used,
                                            (unsigned long long)((nbytes + 7) & ~7u));
+        if (off + nbytes > gt->arena_sz / 2)
+            xb_gt_want_grow(gt);
         if (off + nbytes > gt->arena_sz) {
             XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_ARENA_FULL);
             return false;
@@ -498,7 +536,7 @@ xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t ha
                     ok &= xb_key_store(plan->keys[k], keys[k], &img[k], gt, st);
                 xb_init_states(plan, e);
                 if (gt)
-                    atomicAdd((unsigned long long *)&gt->nused, 1ULL);
+                    xb_gt_count_new(gt);
                 xb_st_release(&h->state, XB_GSTATE_READY);
                 return ok ? e : nullptr;
             }
@@ -527,9 +565,41 @@ xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t ha
     return nullptr;
 }
 
+/* xb_group_find on the global table; a group that finds it without room
+ * gets an entry of the dump region (merged into the grown table by the
+ * host), and only when that is used up is SUSPEND_NO_SPACE raised */
+__device__ __noinline__ char *
+xb_group_find_or_dump(const xb_plan *plan, xb_gtable *gt, uint32_t hash, const xb_keyimg *keys,
+                      xb_status *st)
+{
+    bool full = false;
+    char *g = xb_group_find(plan, gt->entries, gt->cap_mask, hash, keys, gt, st, &full);
+    if (!g && full) {
+        char *slot = xb_dump_slot(gt, plan->gent_size);
+        if (slot) {
+            full = false;
+            g = xb_group_find(plan, slot, 0, hash, keys, gt, st, &full);
+        }
+        if (!g && full) {
+            XB_RAISE(st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
+            atomicOr(&gt->overflow, 1u);
+        }
+    }
+    return g;
+}
+
 /* ================================================================
  * launch arguments and the source layout
  * ================================================================ */
+/* work a launch left when it stopped for its group table to grow: units
+ * [unit, unit_end), the first of them from item 'item' on */
+struct XbLeft {
+    uint64_t unit;
+    uint64_t unit_end;
+    uint32_t item;
+    uint32_t __pad;
+};
+
 struct XbExecArgs {
     const xb_plan  *plan;           /* device copy (copied into shared memory) */
     uint32_t        plan_bytes;     /* bytes of the plan copy: header + used code */
@@ -549,7 +619,15 @@ struct XbExecArgs {
     char           *part_buf;       /* bucket-major records, or nullptr (update in place) */
     uint32_t       *part_cnt;       /* records claimed per bucket */
     uint32_t        part_shift;     /* bucket = (hash & table mask) >> part_shift */
-    uint32_t        __pad;
+    uint32_t        resume;         /* a resume launch: left_in first, then claims that
+                                     * continue those of the stopped launch */
+    XbLeft         *left_out;       /* group-table growth on: where warps that stop
+                                     * record their leftover work (nullptr: growth off) */
+    uint32_t        left_cap;
+    uint32_t        left_in_n;
+    const XbLeft   *left_in;        /* resume: the stopped launch's leftover ranges */
+    uint64_t        static_base0;   /* resume: units below were handed out statically */
+    uint64_t        cursor0;        /* resume: dynamic claims the stopped launch made */
 };
 
 /* bucket counters of partitioned aggregation sit one per 128-byte line:
@@ -563,10 +641,12 @@ struct XbReplayArgs {
     const xb_plan  *plan;
     xb_gtable      *gt;
     xb_status      *st;
-    const char     *part_buf;
+    char           *part_buf;       /* records (a full table marks the ones it left) */
     const uint32_t *part_cnt;
     uint32_t        part_cap;
     uint32_t        nparts;
+    uint32_t        retry;          /* replay only the records marked left */
+    uint32_t        __pad;
 };
 
 /* largest existence bitmap of a direct depth (keys), 16 KB */
@@ -640,6 +720,7 @@ struct alignas(16) XbSrc {
     unsigned long long nx_l0;       /* BLOCK, lane 0: first unit of the claim taken ahead */
     unsigned long long sz_l0;       /* BLOCK, lane 0: its size */
     unsigned long long last_dyn;    /* BLOCK, lane 0: start of the last dynamic claim */
+    unsigned long long it_l0;       /* BLOCK, lane 0: first item of the claim taken ahead */
     uint64_t static_base;           /* BLOCK: units below are handed out statically */
     uint64_t task_base;             /* units [task_base, task_end) belong to kds */
     uint64_t task_end;
@@ -692,6 +773,39 @@ xb_prefetch_page(const XbExecArgs &args, const XbSrc &s, uint64_t unit, uint32_t
 }
 
 /*
+ * Lane 0: the heap-page claim a warp takes after its current one.  A
+ * resume launch hands out the stopped launch's leftover ranges first; then
+ * pages are claimed from the dynamic cursor with guided sizes (large
+ * claims while plenty is left, single pages near the end so that no warp
+ * is left with a long tail; one page for a warp's first claim).
+ */
+__device__ __forceinline__ void
+xb_claim_ahead(const XbExecArgs &args, XbSrc &s, bool first)
+{
+    if (args.resume && args.left_in) {
+        const uint32_t i = atomicAdd(&args.st->left_next, 1u);
+        if (i < args.left_in_n) {
+            const XbLeft L = args.left_in[i];
+            s.nx_l0 = L.unit;
+            s.sz_l0 = L.unit_end > L.unit ? L.unit_end - L.unit : 0;
+            s.it_l0 = L.item;
+            return;
+        }
+    }
+    unsigned long long sz = 1;
+    if (!first) {
+        const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
+        const unsigned long long left = s.last_dyn < args.nunits ? args.nunits - s.last_dyn : 0;
+        sz = left / (4 * warps);
+        sz = sz < 1 ? 1 : (sz > XB_CLAIM ? XB_CLAIM : sz);
+    }
+    s.sz_l0 = sz;
+    s.it_l0 = 0;
+    s.nx_l0 = s.static_base + args.cursor0 + atomicAdd((unsigned long long *)&args.st->unit_cursor, sz);
+    s.last_dyn = s.nx_l0;
+}
+
+/*
  * Set up a warp's first claim.  Heap pages: each warp first takes a static
  * share of 3/5 of the launch's pages (contiguous, no atomic), then claims
  * the rest dynamically; Arrow / row units are all claimed dynamically.
@@ -715,25 +829,25 @@ xb_src_start(const XbExecArgs &args, XbSrc &s, uint32_t lane)
             s.nx_l0 = 0;
             s.sz_l0 = 1;
             s.last_dyn = 0;
+            s.it_l0 = 0;
         }
         __syncwarp();
         return;
     }
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
     const uint64_t wid = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    const uint64_t share = args.dyn_only ? 0 : (args.nunits * 3 / 5) / warps;
-    s.static_base = share * warps;
+    const uint64_t share = (args.dyn_only || args.resume) ? 0 : (args.nunits * 3 / 5) / warps;
+    s.static_base = args.resume ? args.static_base0 : share * warps;
     /* the lane-0 fields are written by lane 0 only (the state may live in
      * shared memory, read back by every lane) */
     if (lane == 0) {
-        s.last_dyn = s.static_base;
+        s.last_dyn = s.static_base + args.cursor0;
+        s.it_l0 = 0;
         if (share > 0) {
             s.nx_l0 = wid * share;
             s.sz_l0 = share;
         } else {
-            s.nx_l0 = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
-            s.sz_l0 = 1;
-            s.last_dyn = s.nx_l0;
+            xb_claim_ahead(args, s, true);
         }
     }
     __syncwarp();
@@ -755,28 +869,20 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
 {
     if (args.format == KDS_FORMAT_BLOCK) {
         s.unit++;
+        uint32_t first_item = 0;
         if ((s.unit & 7) == 0 && *(volatile uint32_t *)&args.st->errcode != 0)
             return 0;                   /* another warp failed: stop early */
         if (s.unit >= s.claim_end) {
             /* the claim taken ahead (its atomic has long returned to lane 0) */
             s.unit = __shfl_sync(XB_FULL, s.nx_l0, 0);
-            const uint32_t size = (uint32_t)__shfl_sync(XB_FULL, s.sz_l0, 0);
+            const uint64_t size = __shfl_sync(XB_FULL, s.sz_l0, 0);
+            first_item = (uint32_t)__shfl_sync(XB_FULL, s.it_l0, 0);
             if (s.unit >= args.nunits || *(volatile uint32_t *)&args.st->errcode != 0)
                 return 0;
             s.claim_end = min(s.unit + size, args.nunits);
-            /* guided self-scheduling of the dynamic part: large claims while
-             * plenty of it is left, single pages near the end so no warp
-             * is left with a long tail; lane 0 keeps the result until the
-             * claim starts */
-            if (lane == 0) {
-                const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
-                const unsigned long long left = s.last_dyn < args.nunits ? args.nunits - s.last_dyn : 0;
-                unsigned long long sz = left / (4 * warps);
-                sz = sz < 1 ? 1 : (sz > XB_CLAIM ? XB_CLAIM : sz);
-                s.sz_l0 = sz;
-                s.nx_l0 = s.static_base + atomicAdd((unsigned long long *)&args.st->unit_cursor, sz);
-                s.last_dyn = s.nx_l0;
-            }
+            /* lane 0 keeps the next claim until this one is used up */
+            if (lane == 0)
+                xb_claim_ahead(args, s, false);
         }
         if (s.unit < s.task_base || s.unit >= s.task_end)
             xb_src_task(args, s, s.unit);
@@ -785,7 +891,7 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
         if (pf_next)
             xb_prefetch_page(args, s, xb_following_unit(s), lane);
         const uint32_t pd_lower = (uint32_t)xb_fetch_le(s.page + 12, 2);
-        s.item = 0;
+        s.item = first_item;
         s.nitems = 0;
         if (pd_lower > SizeOfPageHeaderData && pd_lower <= PGSTROM_BLCKSZ)
             s.nitems = (pd_lower - SizeOfPageHeaderData) / sizeof(ItemIdData);
@@ -796,9 +902,22 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
     if (*(volatile uint32_t *)&args.st->errcode != 0)
         return 0;
     unsigned long long u = 0;
-    if (lane == 0)
-        u = atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
+    uint32_t it = 0;
+    if (lane == 0) {
+        bool got = false;
+        if (args.resume && args.left_in) {
+            const uint32_t i = atomicAdd(&args.st->left_next, 1u);
+            if (i < args.left_in_n) {
+                u = args.left_in[i].unit;
+                it = args.left_in[i].item;
+                got = true;
+            }
+        }
+        if (!got)
+            u = args.cursor0 + atomicAdd((unsigned long long *)&args.st->unit_cursor, 1ULL);
+    }
     u = __shfl_sync(XB_FULL, u, 0);
+    it = __shfl_sync(XB_FULL, it, 0);
     if (u >= args.nunits)
         return 0;
     if (u < s.task_base || u >= s.task_end)
@@ -807,8 +926,62 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
     s.row0 = (uint32_t)(u - s.task_base) * XB_ROWS_UNIT;
     const uint32_t left = s.kds->nitems > s.row0 ? s.kds->nitems - s.row0 : 0;
     s.nitems = left < XB_ROWS_UNIT ? left : XB_ROWS_UNIT;
-    s.item = 0;
+    s.item = it;
     return 1;
+}
+
+/*
+ * The warp stops claiming work because the group table must grow: lane 0
+ * records what the warp still holds, for the resume launch after the host
+ * grew the table: the rest of the current unit from next_item on and the
+ * rest of the current claim (heap pages: one range), and the claim taken
+ * ahead.  Nothing is lost or done twice: every unit is either behind the
+ * warp, in these ranges, or not yet claimed from the cursor.
+ */
+__device__ __forceinline__ void
+xb_src_leave(const XbExecArgs &args, const XbSrc &s, uint32_t lane, uint32_t next_item, uint32_t nitems)
+{
+    if (lane == 0) {
+        XbLeft L[2];
+        uint32_t n = 0;
+        if (args.format == KDS_FORMAT_BLOCK) {
+            if (s.unit < s.claim_end) {
+                if (next_item < nitems) {
+                    L[n].unit = s.unit; L[n].unit_end = s.claim_end; L[n].item = next_item; n++;
+                } else if (s.unit + 1 < s.claim_end) {
+                    L[n].unit = s.unit + 1; L[n].unit_end = s.claim_end; L[n].item = 0; n++;
+                }
+            }
+            if (s.nx_l0 < args.nunits && s.sz_l0 > 0) {
+                L[n].unit = s.nx_l0;
+                L[n].unit_end = s.nx_l0 + s.sz_l0 < args.nunits ? s.nx_l0 + s.sz_l0 : args.nunits;
+                L[n].item = (uint32_t)s.it_l0;
+                n++;
+            }
+        } else if (s.kds && next_item < nitems) {
+            L[n].unit = s.unit; L[n].unit_end = s.unit + 1; L[n].item = next_item; n++;
+        }
+        atomicExch(&args.st->stopped, 1u);
+        if (n) {
+            const uint32_t at = atomicAdd(&args.st->left_n, n);
+            if (at + n > args.left_cap) {
+                XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_LEFT_FULL);
+            } else {
+                for (uint32_t i = 0; i < n; i++) {
+                    L[i].__pad = 0;
+                    args.left_out[at + i] = L[i];
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+/* the warp's view of the group table's growth request (lane 0 loads it:
+ * issue early, read after the batch) */
+__device__ __forceinline__ uint32_t xb_grow_flag(const XbExecArgs &args, uint32_t lane)
+{
+    return (args.left_out && lane == 0) ? xb_ld_relaxed(&args.gt->grow) : 0u;
 }
 
 /* Arrow column -> register (xpu_*_datum_arrow_read) */

@@ -42,6 +42,7 @@ struct XbjEnv {
     uint32_t       *part_cnt;
     uint32_t        part_cap;
     uint32_t        part_shift;
+    uint32_t        replay;         /* in the replay: a full table leaves the record for later */
 };
 
 /* per-thread counters, 32-bit to spare registers; flushed into the launch
@@ -111,9 +112,13 @@ __device__ __forceinline__ void
 xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
 
 #ifdef XBJ_PART
-/* generated: a deferred row's record, and the group update of one row */
+/* the record's NULL-mask word carries this bit while the record waits for
+ * the group table to grow (a replay that found the table without room) */
+#define XBJ_REC_LEFT    0x80000000u
+/* generated: a deferred row's record, and the group update of one row
+ * (returns true when, replaying, the table had no room for the group) */
 __device__ __forceinline__ void xbj_rec_load(const char *rec, XbjRegs &R, uint32_t &ghash);
-__device__ __forceinline__ void xbj_group_row(XbjRegs &R, const XbjEnv &E, const uint32_t ghash, bool &failed);
+__device__ __forceinline__ bool xbj_group_row(XbjRegs &R, const XbjEnv &E, const uint32_t ghash, bool &failed);
 #endif
 
 #ifdef XBJ_MERGE_SM
@@ -226,6 +231,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     E.part_cnt = args.part_cnt;
     E.part_cap = args.part_cap;
     E.part_shift = args.part_shift;
+    E.replay = 0;
     XbjCnt C;
     C.raw = C.in = C.out = 0;
     C.gready = 0;
@@ -268,7 +274,7 @@ xbj_body(const XbExecArgs &args, char *smem)
             page = src.page;
             kds = src.kds;
             row0 = src.row0;
-            item = 0;
+            item = src.item;            /* 0, or where a resumed range starts */
             nitems = src.nitems;
 #ifdef XBJ_STAGE
             staged = false;
@@ -291,12 +297,14 @@ xbj_body(const XbExecArgs &args, char *smem)
             }
 #endif
             if (args.format == KDS_FORMAT_BLOCK) {
-                lp_next = xbj_itemid(page, nitems, lane);
-                lp_after = xbj_itemid(page, nitems, lane + 32);
+                lp_next = xbj_itemid(page, nitems, item + lane);
+                lp_after = xbj_itemid(page, nitems, item + lane + 32);
             }
         }
         if (done)
             break;
+        /* the group table's growth request, read after the batch */
+        const uint32_t grow_ = xb_grow_flag(args, lane);
         const uint32_t idx = item + lane;
         uint32_t lp = 0;
         /* the warp's next heap page streams into L2 while the last
@@ -340,6 +348,11 @@ xbj_body(const XbExecArgs &args, char *smem)
             xbj_flush_cnt(C, args.st);
         if (__any_sync(XB_FULL, failed))
             break;
+        if (args.left_out && __shfl_sync(XB_FULL, grow_, 0)) {
+            /* the table is to grow: leave the rest for the resume launch */
+            xb_src_leave(args, src, lane, item, nitems);
+            break;
+        }
     }
 
 #ifdef XBJ_STAGE
@@ -377,19 +390,13 @@ xbj_body(const XbExecArgs &args, char *smem)
             if (h->state != XB_GSTATE_READY)
                 continue;
             const xb_keyimg *img = (const xb_keyimg *)(e + XBJ_KEYS_OFF);
-            bool full = false;
-            char *g = xb_group_find(plan, args.gt->entries, args.gt->cap_mask, h->hash,
-                                    img, args.gt, args.st, &full);
+            char *g = xb_group_find_or_dump(plan, args.gt, h->hash, img, args.st);
             if (g)
 #ifdef XBJ_MERGE_SM
                 xbj_merge_sm(g, e);
 #else
                 xb_merge_states(plan, g, e);
 #endif
-            else if (full) {
-                XB_RAISE(args.st, ERRCODE_SUSPEND_NO_SPACE, XB_MSG_GTABLE_FULL);
-                atomicOr(&args.gt->overflow, 1u);
-            }
         }
     }
 }
@@ -448,6 +455,7 @@ xbj_replay(const __grid_constant__ XbReplayArgs args)
     E.part_cnt = nullptr;
     E.part_cap = 0;
     E.part_shift = 0;
+    E.replay = 1;
     /* the records of every bucket, numbered in bucket order: pre[b] is the
      * number of records before bucket b (bucket counts clipped to the
      * bucket size; counts past it were updated in place) */
@@ -493,11 +501,22 @@ xbj_replay(const __grid_constant__ XbReplayArgs args)
             if (pre[mid] <= v) lo = mid; else hi = mid - 1;
         }
         const uint64_t i = (uint64_t)lo * args.part_cap + (v - pre[lo]);
+        char *rec = args.part_buf + i * XBJ_REC_SIZE;
+        /* a retry replays only the records a full table left behind */
+        if (args.retry && !(((const uint32_t *)rec)[1] & XBJ_REC_LEFT))
+            continue;
         XbjRegs R;
         uint32_t ghash;
-        xbj_rec_load(args.part_buf + i * XBJ_REC_SIZE, R, ghash);
+        xbj_rec_load(rec, R, ghash);
         bool failed = false;
-        xbj_group_row(R, E, ghash, failed);
+        const bool table_full = xbj_group_row(R, E, ghash, failed);
+        if (table_full) {
+            ((uint32_t *)rec)[1] |= XBJ_REC_LEFT;
+            if (!args.st->replay_left)
+                atomicExch(&args.st->replay_left, 1u);
+        } else if (args.retry) {
+            ((uint32_t *)rec)[1] &= ~XBJ_REC_LEFT;
+        }
     }
 }
 #endif

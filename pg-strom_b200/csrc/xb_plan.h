@@ -371,16 +371,28 @@ typedef struct xb_task {
     uint32_t    format;
 } xb_task;
 
-/* global group table */
+/* global group table.  It grows between launches (the host rehashes it
+ * into a larger one, as the reference's service expands kds_final on
+ * SUSPEND_NO_SPACE, gpu_service.c:2418-2470): a launch that sees 'grow'
+ * stops claiming work and records what it left (XbLeft ranges); groups
+ * that find the table without room meanwhile take an entry of the dump
+ * region, merged into the grown table before the work resumes */
 typedef struct xb_gtable {
     uint64_t    cap_mask;
-    uint64_t    nused;          /* number of claimed entries */
+    uint64_t    nused;          /* number of claimed entries (dump entries included) */
     char       *entries;        /* cap * gent_size bytes */
     char       *arena;          /* text/numeric key bytes */
     uint64_t    arena_sz;
     uint64_t    arena_used;
-    uint32_t    overflow;       /* set when the table or arena ran out */
-    uint32_t    __pad;
+    uint32_t    overflow;       /* set when the table, the dump or the arena ran out */
+    uint32_t    grow;           /* set when the table wants to grow: nused reached
+                                 * soft_cap, a dump entry was taken or the arena
+                                 * passed half of its bytes */
+    uint64_t    soft_cap;       /* entries at which growth is requested */
+    char       *dump;           /* entries (global form) of groups created while the
+                                 * table had no room, or nullptr */
+    uint64_t    dump_cap;
+    uint64_t    dump_used;
 } xb_gtable;
 
 /* execution statistics and error state, one per launch (device) */
@@ -393,7 +405,11 @@ typedef struct xb_status {
     uint64_t    nitems_in;
     uint64_t    nitems_out;
     uint64_t    nitems_depth[XB_MAX_DEPTH + 1];
-    uint64_t    __pad1[4];
+    uint32_t    stopped;        /* warps stopped claiming work for the group table to grow */
+    uint32_t    left_n;         /* leftover ranges they recorded */
+    uint32_t    left_next;      /* resume launch: next leftover range to take */
+    uint32_t    replay_left;    /* replay: records left for after the table grows */
+    uint64_t    __pad1[2];
     /* work distribution counter, alone in its 128-byte line: every warp's
      * claim lands here, away from the error word every warp polls */
     uint64_t    unit_cursor;
@@ -424,5 +440,6 @@ typedef struct xb_status {
 #define XB_MSG_BAD_PAGE         11
 #define XB_MSG_ARROW_TYPE       12
 #define XB_MSG_NUMERIC_TYPE     13
+#define XB_MSG_LEFT_FULL        14
 
 #endif  /* XB_PLAN_H */

@@ -197,10 +197,13 @@ def long_strings(n, seed=7, lo=20, hi=300):
     r = np.random.Generator(np.random.PCG64(seed))
     fixed = [1, 126, 127, 128, 300]
     lens = fixed[:n] + r.integers(lo, hi + 1, max(0, n - len(fixed))).tolist()
+    # letters stepping by 3 through the alphabet, from a per-string offset
+    pat = "".join(chr(97 + (3 * k) % 26) for k in range(26)) * (hi // 26 + 14)
     out = []
     for i, L in enumerate(lens):
         head = "%d:" % i
-        body = "".join(chr(97 + (i * 7 + 3 * j) % 26) for j in range(L))
+        off = (63 * i) % 26
+        body = pat[off:off + L]
         out.append((head + body)[:L] if L > len(head) else chr(65 + i % 26) * L)
     assert len(set(out)) == n
     return out
