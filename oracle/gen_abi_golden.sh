@@ -1,11 +1,11 @@
 #!/bin/sh
 # Regenerates the ABI pins under tests/golden/ from the reference headers.
-# Reads PG-Strom's src/ at $PGSTROM_SRC (default /root/reference/src); run it
+# Reads PG-Strom's src/ directory, given as $PGSTROM_SRC (required); run it
 # only where that tree exists.  Outputs:
 #   tests/golden/abi_layout.txt  sizeof/offsetof of every ABI field used
 #   tests/golden/opcodes.txt     TypeOpCode / FuncOpCode name -> value
 set -e
-SRC=${PGSTROM_SRC:-/root/reference/src}
+SRC=${PGSTROM_SRC:?set PGSTROM_SRC to the PG-Strom src/ directory}
 HERE=$(cd "$(dirname "$0")/.." && pwd)
 TMP=$(mktemp -d)
 gcc -std=gnu11 -DUSE_REFERENCE -I"$SRC" "$HERE/tests/abi_layout_probe.c" -o "$TMP/layout"

@@ -1329,6 +1329,7 @@ struct Compiler {
     {
         memset(plan, 0, sizeof(xb_plan));
         plan->magic = XB_PLAN_MAGIC;
+        plan->wait_limit = XB_WAIT_LIMIT;
         plan->plan_sz = sizeof(xb_plan);
         if (session_sz < sizeof(kern_session_info))
             return fail("session is shorter than kern_session_info");

@@ -15,7 +15,6 @@
 #include "xb_ops.cuh"
 
 #define XB_FULL         0xffffffffU
-#define XB_WAIT_LIMIT   (1u << 22)      /* bounded spin on a BUSY group entry */
 
 /* ---------------------------------------------------------------
  * per-warp register file in shared memory

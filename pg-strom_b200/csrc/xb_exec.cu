@@ -152,7 +152,7 @@ xb_group_get(const xb_plan *plan, const XbRegs &R, uint32_t lane, char *entries,
         }
         uint32_t spins = 0;
         while (s == XB_GSTATE_BUSY) {
-            if (++spins > XB_WAIT_LIMIT) {
+            if (++spins > plan->wait_limit) {
                 XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_WAIT_TIMEOUT);
                 return nullptr;
             }
@@ -2619,6 +2619,27 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
                 s->sm_cap = smc;
         }
     }
+    /* test hooks, inert unless set: XPU_B200_WAIT_LIMIT shortens the
+     * bounded wait on a BUSY group entry; XPU_B200_TEST_BUSY_GROUPS=1 marks
+     * every global entry BUSY, as if its creator never published it, so
+     * that every lookup runs its wait out and the launch reports
+     * XB_MSG_WAIT_TIMEOUT */
+    if (const char *wl = getenv("XPU_B200_WAIT_LIMIT")) {
+        const unsigned long v = strtoul(wl, nullptr, 10);
+        if (v > 0 && v < XB_WAIT_LIMIT)
+            plan->wait_limit = (uint32_t)v;
+    }
+    if (plan->has_groupby) {
+        const char *busy = getenv("XPU_B200_TEST_BUSY_GROUPS");
+        if (busy && busy[0] == '1') {
+            const uint64_t n = s->h_gt.cap_mask + 1, gsz = plan->gent_size;
+            std::vector<char> img(n * gsz, 0);
+            for (uint64_t i = 0; i < n; i++)
+                ((xb_gent_head *)(img.data() + i * gsz))->state = XB_GSTATE_BUSY;
+            cudaMemcpyAsync(s->h_gt.entries, img.data(), img.size(), cudaMemcpyHostToDevice, st);
+            cudaStreamSynchronize(st);
+        }
+    }
     DALLOC(sizeof(xb_plan), &s->d_plan);
     cudaMemcpyAsync(s->d_plan, plan, sizeof(xb_plan), cudaMemcpyHostToDevice, st);
 
@@ -3056,11 +3077,13 @@ static int xb_gt_settle(xpuB200Session *s, kern_errorbuf *err);
 
 /* the dump region, sized for a launch of 'grid' CTAs: every CTA's shared
  * table merged at exit, plus the rows in flight after the table asked to
- * grow when its free half is smaller than twice those */
+ * grow (two 32-row batches per warp: the one a warp is in when the request
+ * comes, and one more if its look at the flag came just before) when the
+ * table's free half is smaller than twice those */
 static int xb_dump_ensure(xpuB200Session *s, int grid, uint32_t sm_cap, cudaStream_t st, kern_errorbuf *err)
 {
     const uint64_t cap = s->h_gt.cap_mask + 1;
-    const uint64_t inflight = (uint64_t)grid * XB_WARPS * 32;
+    const uint64_t inflight = (uint64_t)grid * XB_WARPS * 64;
     uint64_t need = (uint64_t)grid * sm_cap;
     if (cap / 2 < 2 * inflight)
         need += inflight;

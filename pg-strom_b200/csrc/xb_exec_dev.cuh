@@ -544,7 +544,7 @@ xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t ha
         }
         uint32_t spins = 0;
         while (s == XB_GSTATE_BUSY) {
-            if (++spins > XB_WAIT_LIMIT) {
+            if (++spins > plan->wait_limit) {
                 XB_RAISE(st, ERRCODE_DEVICE_ERROR, XB_MSG_WAIT_TIMEOUT);
                 return nullptr;
             }
@@ -938,7 +938,7 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
  * ahead.  Nothing is lost or done twice: every unit is either behind the
  * warp, in these ranges, or not yet claimed from the cursor.
  */
-__device__ __forceinline__ void
+__device__ __noinline__ void
 xb_src_leave(const XbExecArgs &args, const XbSrc &s, uint32_t lane, uint32_t next_item, uint32_t nitems)
 {
     if (lane == 0) {
@@ -977,8 +977,7 @@ xb_src_leave(const XbExecArgs &args, const XbSrc &s, uint32_t lane, uint32_t nex
     __syncwarp();
 }
 
-/* the warp's view of the group table's growth request (lane 0 loads it:
- * issue early, read after the batch) */
+/* the warp's view of the group table's growth request (lane 0 loads it) */
 __device__ __forceinline__ uint32_t xb_grow_flag(const XbExecArgs &args, uint32_t lane)
 {
     return (args.left_out && lane == 0) ? xb_ld_relaxed(&args.gt->grow) : 0u;

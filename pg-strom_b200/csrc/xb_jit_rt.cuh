@@ -303,8 +303,6 @@ xbj_body(const XbExecArgs &args, char *smem)
         }
         if (done)
             break;
-        /* the group table's growth request, read after the batch */
-        const uint32_t grow_ = xb_grow_flag(args, lane);
         const uint32_t idx = item + lane;
         uint32_t lp = 0;
         /* the warp's next heap page streams into L2 while the last
@@ -348,7 +346,7 @@ xbj_body(const XbExecArgs &args, char *smem)
             xbj_flush_cnt(C, args.st);
         if (__any_sync(XB_FULL, failed))
             break;
-        if (args.left_out && __shfl_sync(XB_FULL, grow_, 0)) {
+        if (args.left_out && __shfl_sync(XB_FULL, xb_grow_flag(args, lane), 0)) {
             /* the table is to grow: leave the rest for the resume launch */
             xb_src_leave(args, src, lane, item, nitems);
             break;

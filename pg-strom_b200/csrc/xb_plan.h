@@ -296,12 +296,17 @@ typedef struct xb_plan {
     uint32_t    sort_rank_limit;
     int64_t     sort_limit;     /* LIMIT without a window function; 0: none */
 
+    /* spins a lane waits on a BUSY group entry before it gives up with
+     * XB_MSG_WAIT_TIMEOUT (XB_WAIT_LIMIT unless a test shortens it) */
+    uint32_t    wait_limit;
+
     /* VM code */
     uint32_t    ninsns;
     xb_insn     insns[XB_MAX_INSNS];
 } xb_plan;
 
 #define XB_PLAN_MAGIC   0x78623230U     /* 'xb20' */
+#define XB_WAIT_LIMIT   (1u << 22)      /* default bounded spin on a BUSY group entry */
 
 #ifdef __CUDACC__
 #define XB_PLAN_HD __host__ __device__ inline

@@ -56,3 +56,42 @@ def test_group_table_that_cannot_grow_suspends(kernel):
             s.close()
     finally:
         dev.close()
+
+
+@pytest.mark.parametrize("estimate", [64, 100_000])
+def test_bounded_wait_on_a_busy_entry_times_out(kernel, monkeypatch, estimate):
+    # every global group entry is left BUSY, as if its creator never
+    # published it, and the wait on such an entry is cut to 10,000 spins:
+    # the launch stops with the wait-timeout error (through the CTA's merge
+    # of its shared table when there is one, estimate 64, or on the rows'
+    # own lookups, estimate 100,000), promptly, the session closes, and the
+    # device runs the next session correctly
+    import time
+    import xb_final as F
+    monkeypatch.setenv("XPU_B200_WAIT_LIMIT", "10000")
+    monkeypatch.setenv("XPU_B200_TEST_BUSY_GROUPS", "1")
+    tbl, _, _, expect, meta = C.scan_groupby(nrows=60_000, seed_config=73)
+    chunks = tbl.block_chunks(pages_per_chunk=64)
+    dev = xpu_b200.Device(0)
+    try:
+        s = xpu_b200.Session(dev, C.scan_groupby_session(ngroups=estimate))
+        t0 = time.perf_counter()
+        try:
+            with pytest.raises(xpu_b200.XpuB200Error, match="wait timed out"):
+                for ch in chunks:
+                    s.exec(ch)
+        finally:
+            s.close()
+        assert time.perf_counter() - t0 < 20.0
+        monkeypatch.delenv("XPU_B200_TEST_BUSY_GROUPS")
+        s2 = xpu_b200.Session(dev, C.scan_groupby_session(ngroups=estimate))
+        try:
+            for ch in chunks:
+                s2.exec(ch)
+            final, _ = s2.final()
+        finally:
+            s2.close()
+        truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
+        assert F.compare_groups(F.decode_kds_final(final, C.scan_groupby_session(ngroups=estimate)), truth) == []
+    finally:
+        dev.close()
