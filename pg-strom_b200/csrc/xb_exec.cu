@@ -28,6 +28,8 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <thread>
+#include <chrono>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -1144,6 +1146,8 @@ struct XbFinalArgs {
     uint32_t        nslots;
     uint32_t        row_format;     /* KDS_FORMAT_ROW (no GROUP BY keys): kern_tupitems
                                      * without hash links, nslots 0 */
+    uint32_t        part_div;       /* >= 2: only the groups with hash % part_div == part_rem */
+    uint32_t        part_rem;
     const int64_t  *keep;           /* GPU-Sort: output position per entry, -1 dropped
                                      * (nullptr: every group, in table order) */
 };
@@ -1343,7 +1347,9 @@ __global__ void xb_final_sizes(XbFinalArgs args)
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < args.cap;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const char *e = args.gt->entries + i * plan->gent_size;
-        if (((const xb_gent_head *)e)->state == XB_GSTATE_READY && (!args.keep || args.keep[i] >= 0)) {
+        const xb_gent_head *h = (const xb_gent_head *)e;
+        if (h->state == XB_GSTATE_READY && (!args.keep || args.keep[i] >= 0) &&
+            (args.part_div < 2 || h->hash % args.part_div == args.part_rem)) {
             uint32_t t_len = xb_write_group_tuple(plan, e, nullptr, 0);
             args.sizes[i] = PGSTROM_MAXALIGN((args.row_format ? 0 : offsetof(kern_hashitem, t)) + t_len);
             args.flags[i] = 1;
@@ -2217,6 +2223,7 @@ struct xpuB200Session {
     bool            jit_tried[256] = {false};
     void           *jit_fn[256] = {nullptr};
     void           *jit_mixfn[256] = {nullptr};    /* its mixed-launch kernel */
+    void           *jit_job[256] = {nullptr};      /* a background build of it, pending */
     char            ran_kind[256] = {0};   /* 'j' / 'v': kernel last launched per format */
     uint32_t        sched_refs = 0;        /* submitted commands not yet finished */
     /* device projection: staging buffer for host kds_dst, and the buffer of
@@ -2314,6 +2321,11 @@ static const char *xb_msg_text(uint32_t id)
 }
 
 static_assert(XBJ_WARPS_PER_CTA == XB_WARPS, "specialised kernels assume the executor's CTA size");
+/* the specialised kernels fetch bytes 48..63 of the group table (16-byte
+ * aligned) for its 'grow' word, the second word there */
+static_assert(offsetof(xb_gtable, grow) == 52 && offsetof(xb_gtable, overflow) == 48,
+              "the group table's grow word moved");
+static_assert(offsetof(XbSrc, grow_buf) % 16 == 0, "XbSrc.grow_buf must be 16-byte aligned");
 
 static int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int line,
                         const char *fmt, ...)
@@ -2427,6 +2439,10 @@ xpuB200Shutdown(xpuB200Device *dev)
 static void xb_session_free(xpuB200Session *s)
 {
     cudaSetDevice(s->dev->dindex);
+    /* a background build goes on into the process-wide cache */
+    for (int f = 0; f < 256; f++)
+        if (s->jit_job[f])
+            xb_jit_job_release(s->jit_job[f]);
     /* session memory comes from the device's stream-ordered pool, on the
      * session's stream: freeing it waits for no other stream (a plain
      * cudaFree would wait for the whole device, i.e. every other session's
@@ -2925,7 +2941,16 @@ static bool xb_tune_lookup(xpuB200Session *s, uint32_t format, xb_tune_choice *c
 
 /* the session-specialised kernel of this format (nullptr: use the
  * interpreter), built on first use; session lock held */
-static void *xb_session_jit(xpuB200Session *s, uint32_t format)
+/*
+ * The session's specialised kernel for a source format, built at its first
+ * use.  wait == false (served launches): a kernel the process has not
+ * built yet is built on a background thread while this launch, and the
+ * next ones until it is there, run on the interpreting kernel, so that a
+ * request of a new plan shape does not wait seconds for NVRTC.
+ */
+static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, double ms, const char *msg);
+
+static void *xb_session_jit(xpuB200Session *s, uint32_t format, bool wait = true)
 {
     if (!s->jit_enabled || format >= 256)
         return nullptr;
@@ -2939,15 +2964,53 @@ static void *xb_session_jit(xpuB200Session *s, uint32_t format)
                 xb_set_sm_cap(s, s->sm_cap_default);
         }
     }
-    if (!s->jit_tried[format]) {
-        s->jit_tried[format] = true;
-        char msg[1024];
-        double ms = 0.0;
+    if (s->jit_tried[format])
+        return s->jit_fn[format];
+    char msg[1024] = {0};
+    double ms = 0.0;
+    if (!s->jit_job[format] && !wait) {
+        const int lrc = xb_jit_lookup_minb(s->h_plan, format, s->dev->dindex, s->jit_minb, &s->jit_fn[format],
+                                           &s->jit_mixfn[format], &s->jit_replay[format]);
+        if (lrc == 1) {
+            s->jit_job[format] = xb_jit_build_async(s->h_plan, format, s->dev->dindex, s->jit_minb);
+            if (s->jit_job[format]) {
+                s->jit_msg = "building in the background";
+                return nullptr;
+            }
+        } else {
+            xb_session_adopt_jit(s, format, lrc, 0.0, "not buildable");
+            return s->jit_fn[format];
+        }
+    }
+    if (s->jit_job[format]) {
+        int prc;
+        while ((prc = xb_jit_job_poll(s->jit_job[format], &s->jit_fn[format], &s->jit_mixfn[format],
+                                      &s->jit_replay[format], &ms, msg, sizeof(msg))) == 1) {
+            if (!wait)
+                return nullptr;
+            std::this_thread::sleep_for(std::chrono::milliseconds(2));
+        }
+        xb_jit_job_release(s->jit_job[format]);
+        s->jit_job[format] = nullptr;
+        xb_session_adopt_jit(s, format, prc, ms, msg);
+        return s->jit_fn[format];
+    }
+    const int crc = xb_jit_compile_minb(s->h_plan, format, s->dev->dindex, s->jit_minb, &s->jit_fn[format],
+                                        &s->jit_mixfn[format], &s->jit_replay[format], &ms, msg, sizeof(msg));
+    xb_session_adopt_jit(s, format, crc, ms, msg);
+    return s->jit_fn[format];
+}
+
+/* the kernels just found or built (rc 0), or the reason there are none */
+static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, double ms, const char *msg)
+{
+    s->jit_tried[format] = true;
+    {
         int per_sm = 0, mix_sm = 0;
-        if (xb_jit_compile_minb(s->h_plan, format, s->dev->dindex, s->jit_minb, &s->jit_fn[format],
-                                &s->jit_mixfn[format], &s->jit_replay[format], &ms, msg, sizeof(msg)) != 0) {
+        if (rc != 0) {
             s->jit_fn[format] = nullptr;
             s->jit_mixfn[format] = nullptr;
+            s->jit_replay[format] = nullptr;
             s->jit_msg = msg;
         } else if ((s->jit_smem_fmt[format] = s->jit_smem + xb_jit_stage_bytes(format)) == 0 ||
                    xb_jit_prepare(s->jit_fn[format], XB_BLOCK, s->jit_smem_fmt[format], &per_sm) != 0) {
@@ -2969,7 +3032,6 @@ static void *xb_session_jit(xpuB200Session *s, uint32_t format)
             s->jit_msg = "ok";
         }
     }
-    return s->jit_fn[format];
 }
 
 static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
@@ -3271,7 +3333,8 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
     a.dyn_only = 0;
     a.gt = s->d_gt;
     a.st = d_status;
-    void *fn = xb_session_jit(s, format);
+    /* served launches (pooled slot streams) do not wait for a kernel build */
+    void *fn = xb_session_jit(s, format, stream == s->stream);
     int grid = fn ? s->jit_grid[format] : s->grid;
     uint64_t warps_needed = (format == KDS_FORMAT_BLOCK) ? (nunits + XB_CLAIM - 1) / XB_CLAIM : nunits;
     if ((uint64_t)grid * XB_WARPS > warps_needed)
@@ -3312,6 +3375,7 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
         if (part) {
             XbReplayArgs ra;
+            memset(&ra, 0, sizeof(ra));
             ra.plan = s->d_plan;
             ra.gt = s->d_gt;
             ra.st = d_status;
@@ -4254,6 +4318,146 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
 }
 
 /* ----------------------------------------------------------------
+ * the session's groups as hash partitions, for the exchange step of a
+ * multi-GPU pre-aggregation: part p holds the groups whose hash % nparts
+ * is p, as a KDS_FORMAT_HASH kds_final of its own (the same layout as
+ * xpuB200Final's).  The parts lie back to back in one device buffer the
+ * caller owns, each at a 256-byte aligned offset, so that the buffer can
+ * be handed to the other GPUs whole (CUDA IPC, or NCCL all-to-all); each
+ * GPU then merges the parts destined for it with xpuB200MergeFinal,
+ * reading them in place from the peer's memory.
+ * ---------------------------------------------------------------- */
+extern "C" int
+xpuB200FinalParts(xpuB200Session *s, uint32_t nparts, void *parts_dev, uint64_t buf_sz,
+                  uint64_t *part_offsets, uint64_t *p_required, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!s || nparts < 1 || nparts > 4096 || !part_offsets)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid FinalParts arguments");
+    xb_sched_drain_session(s);
+    std::lock_guard<std::mutex> g(s->lock);
+    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
+    const xb_plan *plan = s->h_plan;
+    if (plan->has_groupby != 1)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "FinalParts needs a session with GROUP BY keys");
+    if (plan->nsort)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "GPU-Sort applies to the merged groups, not to their parts");
+    int rc = xb_gt_settle(s, err);
+    if (rc) return rc;
+    cudaStream_t st = s->stream;
+    const kern_session_info *session = (const kern_session_info *)s->h_session.data();
+    const kern_data_store *fh = (const kern_data_store *)(s->h_session.data() + session->groupby_kds_final);
+    const uint64_t head_len = KDS_HEAD_LENGTH(fh);
+    const uint64_t cap = s->h_gt.cap_mask + 1;
+    std::vector<void *> tmp;
+    auto cleanup = [&]() { for (void *p : tmp) cudaFreeAsync(p, st); };
+    auto alloc = [&](size_t sz, void **p) -> bool {
+        if (cudaMallocAsync(p, sz < 256 ? 256 : sz, st) != cudaSuccess) { cudaGetLastError(); return false; }
+        tmp.push_back(*p);
+        return true;
+    };
+    uint64_t *d_sizes, *d_size_scan;
+    uint32_t *d_flags, *d_flag_scan;
+    void *d_temp = nullptr;
+    if (!alloc(cap * 8, (void **)&d_sizes) || !alloc(cap * 8, (void **)&d_size_scan) ||
+        !alloc(cap * 4, (void **)&d_flags) || !alloc(cap * 4, (void **)&d_flag_scan)) {
+        cleanup();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in FinalParts");
+    }
+    size_t t1 = 0, t2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t1, d_sizes, d_size_scan, (int64_t)cap, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, t2, d_flags, d_flag_scan, (int64_t)cap, st);
+    const size_t tsz_max = t1 > t2 ? t1 : t2;
+    if (!alloc(tsz_max, &d_temp)) {
+        cleanup();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in FinalParts");
+    }
+    XbFinalArgs fa;
+    memset(&fa, 0, sizeof(fa));
+    fa.plan = s->d_plan;
+    fa.gt = s->d_gt;
+    fa.cap = cap;
+    fa.sizes = d_sizes;
+    fa.flags = d_flags;
+    fa.size_scan = d_size_scan;
+    fa.flag_scan = d_flag_scan;
+    fa.part_div = nparts;
+    const int grid = s->dev->nsm * 8;
+    /* sizes of part p (its items and groups) into the arrays */
+    auto size_part = [&](uint32_t p, uint64_t *p_items, uint64_t *p_groups) -> int {
+        fa.part_rem = p;
+        xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
+        size_t tsz = tsz_max;
+        cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_sizes, d_size_scan, (int64_t)cap, st);
+        tsz = tsz_max;
+        cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_flags, d_flag_scan, (int64_t)cap, st);
+        uint64_t last_size = 0, last_scan = 0;
+        uint32_t last_flag = 0, last_fscan = 0;
+        cudaMemcpyAsync(&last_size, d_sizes + cap - 1, 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last_scan, d_size_scan + cap - 1, 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last_flag, d_flags + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last_fscan, d_flag_scan + cap - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess)
+            return -1;
+        *p_items = last_scan + last_size;
+        *p_groups = (uint64_t)last_fscan + last_flag;
+        return 0;
+    };
+    std::vector<uint64_t> items(nparts), groups(nparts);
+    uint64_t total = 0;
+    for (uint32_t p = 0; p < nparts; p++) {
+        if (size_part(p, &items[p], &groups[p]) != 0) {
+            cleanup();
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalParts: %s", cudaGetErrorString(cudaGetLastError()));
+        }
+        const uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(groups[p]);
+        part_offsets[p] = total;
+        total += xb_align256(head_len + 8 * nslots + 8 * groups[p] + items[p]);
+    }
+    part_offsets[nparts] = total;
+    if (p_required) *p_required = total;
+    if (!parts_dev || buf_sz < total) {
+        cleanup();
+        if (!parts_dev && buf_sz == 0)
+            return 0;           /* size query only */
+        return XB_ERR(err, ERRCODE_SUSPEND_NO_SPACE, "the parts need %llu bytes (buffer %llu)",
+                      (unsigned long long)total, (unsigned long long)buf_sz);
+    }
+    std::vector<char> head((const char *)fh, (const char *)fh + head_len);
+    for (uint32_t p = 0; p < nparts; p++) {
+        uint64_t it, ng;
+        if (size_part(p, &it, &ng) != 0) {
+            cleanup();
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalParts: %s", cudaGetErrorString(cudaGetLastError()));
+        }
+        const uint64_t nslots = KDS_GET_HASHSLOT_WIDTH(ng);
+        const uint64_t items_base = head_len + 8 * nslots + 8 * ng;
+        const uint64_t length = items_base + it;
+        char *d_out = (char *)parts_dev + part_offsets[p];
+        kern_data_store *kh = (kern_data_store *)head.data();
+        kh->length = length;
+        kh->usage = it;
+        kh->nitems = (uint32_t)ng;
+        kh->format = KDS_FORMAT_HASH;
+        kh->hash_nslots = (uint32_t)nslots;
+        cudaMemcpyAsync(d_out, head.data(), head_len, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(d_out + head_len, 0, length - head_len, st);
+        fa.kds_final = d_out;
+        fa.items_base = items_base;
+        fa.length = length;
+        fa.nslots = (uint32_t)nslots;
+        xb_final_write<<<grid, XB_BLOCK, 0, st>>>(fa);
+        /* the host header copy must outlive the copy: wait per part */
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            cleanup();
+            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "FinalParts: %s", cudaGetErrorString(cudaGetLastError()));
+        }
+    }
+    cleanup();
+    return 0;
+}
+
+/* ----------------------------------------------------------------
  * prepared batches: many device-resident chunks in one persistent launch
  * ---------------------------------------------------------------- */
 struct xpuB200Batch {
@@ -4519,10 +4723,10 @@ struct xb_mix_group {
 };
 
 /* the mixed kernel a command of session s (chunk format) runs on */
-static void *xb_mix_kernel_of(xpuB200Session *s, uint32_t format)
+static void *xb_mix_kernel_of(xpuB200Session *s, uint32_t format, bool wait = true)
 {
     std::lock_guard<std::mutex> g(s->lock);
-    return xb_session_jit(s, format) ? s->jit_mixfn[format] : nullptr;
+    return xb_session_jit(s, format, wait) ? s->jit_mixfn[format] : nullptr;
 }
 
 /* split commands into launches by kernel and build each work queue:
@@ -4530,11 +4734,13 @@ static void *xb_mix_kernel_of(xpuB200Session *s, uint32_t format)
  * (at most once per CTA) */
 static int xb_mix_plan(xpuB200Device *dev, const std::vector<xpuB200Session *> &sess,
                        const std::vector<uint32_t> &formats, const std::vector<uint64_t> &units,
-                       std::vector<xb_mix_group> &groups, kern_errorbuf *err)
+                       std::vector<xb_mix_group> &groups, kern_errorbuf *err, bool wait = true)
 {
     groups.clear();
     for (uint32_t i = 0; i < sess.size(); i++) {
-        void *k = xb_mix_kernel_of(sess[i], formats[i]);
+        void *k = xb_mix_kernel_of(sess[i], formats[i], wait);
+        if (formats[i] < 256)
+            sess[i]->ran_kind[formats[i]] = k ? 'j' : 'v';
         size_t g = 0;
         while (g < groups.size() && groups[g].jfn != k)
             g++;
@@ -4877,6 +5083,21 @@ xpuB200MixDestroy(xpuB200Mix *m)
  * device.  A finished command's statistics are added to its session and
  * kept for xpuB200Poll; its groups are in the session's group table.
  */
+/* the device's free and total memory, and the reserve admission keeps */
+static void xb_mem_info(xpuB200Device *dev, uint64_t *p_free, uint64_t *p_total, uint64_t *p_reserve)
+{
+    size_t fr = 0, tot = 0;
+    cudaSetDevice(dev->dindex);
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        fr = tot = 0;
+    }
+    *p_free = fr;
+    *p_total = tot;
+    const uint64_t r = tot / 20;
+    *p_reserve = r > (1ULL << 30) ? r : (1ULL << 30);
+}
+
 #define XB_SLOTS            4       /* launches in flight per GPU */
 #define XB_SLOT_CMDS        256     /* commands of one mixed launch */
 #define XB_ALONE_UNITS      256     /* commands of this many units run alone */
@@ -4952,7 +5173,7 @@ static int xb_sched_init(xpuB200Device *dev, kern_errorbuf *err)
     if (dev->sched)
         return 0;
     xb_sched *q = new xb_sched();
-    q->admit_bytes = dev->hbm_budget / 4;
+    q->admit_bytes = XPU_B200_ADMIT_FREE_HBM;
     for (int i = 0; i < XB_SLOTS; i++) {
         xb_slot &sl = q->slot[i];
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -5043,17 +5264,27 @@ static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_er
 {
     std::vector<xb_cmd> take;
     uint64_t bytes = 0;
+    /* admission: by the device's free memory (the slot's staging buffer
+     * is reusable), or against a fixed budget for the bytes in flight */
+    uint64_t room;
+    if (q->admit_bytes == XPU_B200_ADMIT_FREE_HBM) {
+        uint64_t fr = 0, tot = 0, reserve = 0;
+        xb_mem_info(dev, &fr, &tot, &reserve);
+        room = (fr > reserve ? fr - reserve : 0) + sl.stage_cap;
+    } else {
+        room = q->admit_bytes > q->inflight_bytes ? q->admit_bytes - q->inflight_bytes : 0;
+    }
     const xb_cmd &f = q->pending.front();
     const bool alone = f.units >= q->alone_units && f.s->jit_enabled;
-    void *kern = alone ? nullptr : xb_mix_kernel_of(f.s, f.format);
+    void *kern = alone ? nullptr : xb_mix_kernel_of(f.s, f.format, false);
     while (!q->pending.empty() && take.size() < (alone ? 1u : (size_t)XB_SLOT_CMDS)) {
         const xb_cmd &c = q->pending.front();
         if (!alone && c.units >= q->alone_units && c.s->jit_enabled)
             break;                      /* a large one runs alone, in a later launch */
-        if (!alone && xb_mix_kernel_of(c.s, c.format) != kern)
+        if (!alone && xb_mix_kernel_of(c.s, c.format, false) != kern)
             break;                      /* another kernel: a launch of its own */
         const uint64_t b = c.on_device ? 0 : c.length + c.shift + 256;
-        if (q->inflight_bytes + bytes + b > q->admit_bytes && (!take.empty() || q->inflight_bytes > 0))
+        if (bytes + b > room && (!take.empty() || q->inflight_bytes > 0))
             break;                      /* admission: wait for memory to free up */
         bytes += b;
         take.push_back(c);
@@ -5095,7 +5326,7 @@ static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_er
             un[i] = sl.cmds[i].units;
         }
         std::vector<xb_mix_group> groups;
-        rc = xb_mix_plan(dev, ss, fm, un, groups, err);
+        rc = xb_mix_plan(dev, ss, fm, un, groups, err, false);
         const xb_mix_group *g = groups.empty() ? nullptr : &groups[0];
         if (!rc && g && g->items.size() > sl.items_cap) {
             cudaStreamSynchronize(sl.stream);
@@ -5229,6 +5460,19 @@ static void xb_sched_destroy(xpuB200Device *dev)
         xb_slot_free(q->slot[i]);
     delete q;
     dev->sched = nullptr;
+}
+
+extern "C" int
+xpuB200MemInfo(xpuB200Device *dev, uint64_t *p_free, uint64_t *p_total, uint64_t *p_reserve)
+{
+    if (!dev)
+        return ERRCODE_DEVICE_ERROR;
+    uint64_t fr, tot, res;
+    xb_mem_info(dev, &fr, &tot, &res);
+    if (p_free) *p_free = fr;
+    if (p_total) *p_total = tot;
+    if (p_reserve) *p_reserve = res;
+    return 0;
 }
 
 extern "C" int

@@ -730,6 +730,9 @@ struct alignas(16) XbSrc {
     uint32_t row0;                  /* ARROW / ROW: first row of the unit */
     uint32_t item;                  /* next item of the unit */
     uint32_t nitems;                /* items of the unit */
+    uint32_t __pad;
+    uint32_t grow_buf[4];           /* specialised kernels, lane 0: bytes 48..63 of the
+                                     * group table (its 'grow' word), fetched asynchronously */
 };
 
 /* chunk owning global unit 'unit' (tasks are sorted by unit_base) */

@@ -41,6 +41,20 @@ int xb_jit_compile_minb(const xb_plan *plan, uint32_t format, int dindex, int mi
                         void **p_func, void **p_mixfn, void **p_replay, double *p_compile_ms,
                         char *errbuf, size_t errlen);
 
+/* the kernels of plan + format if the process-wide cache has them
+ * already: 0 found, 1 not built yet, -1 not buildable */
+int xb_jit_lookup_minb(const xb_plan *plan, uint32_t format, int dindex, int min_blocks,
+                       void **p_func, void **p_mixfn, void **p_replay);
+
+/* build the kernels of plan + format on a background thread (the plan is
+ * copied); returns a job handle or NULL.  xb_jit_job_poll: 1 while
+ * building, 0 built (outputs filled), -1 failed (errbuf says why).  A job
+ * released before it finished still completes into the cache. */
+void *xb_jit_build_async(const xb_plan *plan, uint32_t format, int dindex, int min_blocks);
+int   xb_jit_job_poll(void *job, void **p_func, void **p_mixfn, void **p_replay, double *p_compile_ms,
+                      char *errbuf, size_t errlen);
+void  xb_jit_job_release(void *job);
+
 /* bytes of one deferred-row record of partitioned aggregation for plan
  * and source format (0: its kernel does not defer group updates); the replay kernel is
  * xbj_replay (parameter block XbReplayArgs), returned by

@@ -176,6 +176,24 @@ __device__ __forceinline__ bool xbj_stage_wait(uint64_t *mbar, uint32_t parity)
 }
 #endif
 
+/* 16 bytes of the group table holding its 'grow' word, copied into shared
+ * memory through L2 (cp.async.cg: no L1 copy that could be stale) */
+__device__ __forceinline__ void xbj_grow_fetch(uint32_t *buf, const xb_gtable *gt)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n\t"
+                 "cp.async.commit_group;"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(buf)), "l"((const char *)gt + 48) : "memory");
+}
+
+/* lane 0: the fetched 'grow' word, once its copy has landed */
+__device__ __forceinline__ uint32_t xbj_grow_seen(const uint32_t *buf, uint32_t lane)
+{
+    if (lane != 0)
+        return 0;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    return *(volatile const uint32_t *)&buf[1];
+}
+
 __device__ __forceinline__ unsigned long long xbj_warp_sum(unsigned long long v)
 {
 #pragma unroll
@@ -303,6 +321,11 @@ xbj_body(const XbExecArgs &args, char *smem)
         }
         if (done)
             break;
+        /* the group table's growth request: lane 0 fetches it into shared
+         * memory by an asynchronous copy now and looks at it after the
+         * batch, so no register is held and no latency is waited for */
+        if (args.left_out && lane == 0)
+            xbj_grow_fetch(src.grow_buf, args.gt);
         const uint32_t idx = item + lane;
         uint32_t lp = 0;
         /* the warp's next heap page streams into L2 while the last
@@ -346,7 +369,7 @@ xbj_body(const XbExecArgs &args, char *smem)
             xbj_flush_cnt(C, args.st);
         if (__any_sync(XB_FULL, failed))
             break;
-        if (args.left_out && __shfl_sync(XB_FULL, xb_grow_flag(args, lane), 0)) {
+        if (args.left_out && __shfl_sync(XB_FULL, xbj_grow_seen(src.grow_buf, lane), 0)) {
             /* the table is to grow: leave the rest for the resume launch */
             xb_src_leave(args, src, lane, item, nitems);
             break;

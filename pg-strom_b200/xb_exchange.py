@@ -1,14 +1,16 @@
 """
 Multi-GPU merge of partial-aggregation results by hash partitioning: each
-rank splits its kds_final into one KDS_FORMAT_HASH part per rank by
-hash % world on its GPU (xpuB200InnerRebuild), the parts are exchanged
-all-to-all through torch.distributed (NCCL over NVLink between GPUs, gloo
-between CPU processes), and each rank merges the parts it received into a
-fresh session of the same plan (xpuB200MergeFinal), so that every group
-ends on exactly one rank.  This is the exchange step of a multi-GPU
-GpuPreAgg whose groups are too many to gather on one GPU; the reference
-merges every GPU's kds_final into the first one instead
-(__gpuservHandleGpuPreAggFinal, gpu_service.c:5442-5518).
+rank splits its groups into one KDS_FORMAT_HASH part per rank by
+hash % world on its GPU (xpuB200FinalParts), the parts are exchanged
+all-to-all between the GPUs' memories (NCCL over NVLink; a C service would
+share the parts buffer by CUDA IPC instead), and each rank merges the parts
+it received into a fresh session of the same plan straight from device
+memory (xpuB200MergeFinal), so that every group ends on exactly one rank.
+alltoall_bytes / merge_parts move host bytes instead (gloo ranks on CPU).
+This is the exchange step of a multi-GPU GpuPreAgg whose groups are too
+many to gather on one GPU; the reference merges every GPU's kds_final into
+the first one instead (__gpuservHandleGpuPreAggFinal,
+gpu_service.c:5442-5518).
 """
 import struct
 
@@ -35,40 +37,19 @@ def empty_final_part(session: bytes, length: int, nslots: int) -> np.ndarray:
     return buf
 
 
-def split_final(dev, session: bytes, final: np.ndarray, nparts: int):
-    """The groups of one kds_final split into nparts KDS_FORMAT_HASH parts
-    by hash % nparts, on the device; returns host copies (None for an empty
-    part)."""
-    if final is None:
-        return [None] * nparts
-    length = int(struct.unpack_from("<Q", final, 0)[0])
-    nitems = int(struct.unpack_from("<I", final, 16)[0])
-    nslots = max(1024, 2 * (nitems // nparts + 1))
-    base, src = dev.upload(final, align_pages=False)
-    parts, bases = [], [base]
+def final_parts(dev, sess_obj, nparts):
+    """This session's groups split into nparts hash partitions on its GPU
+    (xpuB200FinalParts), back to back in one device buffer from dev.alloc;
+    returns (device address, offsets of the nparts parts + the total).
+    The caller frees the address."""
+    offs = sess_obj.final_parts(nparts)
+    base = dev.alloc(max(offs[-1], 256))
     try:
-        for r in range(nparts):
-            _, hl = _final_template(session)
-            plen = (hl + 8 * nslots + length + 7) & ~7      # every row could fall here
-            pb, pp = dev.upload(empty_final_part(session, plen, nslots), align_pages=False)
-            bases.append(pb)
-            used = dev.inner_rebuild(pp, src, divisor=nparts, remainder=r)
-            part = dev.download(pp, plen)
-            n = int(struct.unpack_from("<I", part, 16)[0])
-            if n == 0:
-                parts.append(None)
-                continue
-            # cut the unused middle: header, slots, row index, then the rows
-            usage = int(struct.unpack_from("<Q", part, 8)[0])
-            head = hl + 8 * nslots + 8 * n
-            out = np.concatenate([part[:head], part[plen - usage:]])
-            struct.pack_into("<Q", out, 0, len(out))
-            assert used == len(out)
-            parts.append(out)
-    finally:
-        for b in bases:
-            dev.free(b)
-    return parts
+        offs = sess_obj.final_parts(nparts, base, max(offs[-1], 256))
+    except Exception:
+        dev.free(base)
+        raise
+    return base, offs
 
 
 def alltoall_bytes(parts, rank, world, device=None):
@@ -111,8 +92,38 @@ def merge_parts(dev, session: bytes, parts, kmrels=None, nrels=0):
     return final
 
 
-def exchange_final(dev, session: bytes, final, rank, world, kmrels=None, nrels=0, device=None):
-    """This rank's share of the job's groups: split, exchange, merge."""
-    parts = split_final(dev, session, final, world)
-    got = alltoall_bytes(parts, rank, world, device)
-    return merge_parts(dev, session, got, kmrels, nrels)
+def exchange_final(dev, session: bytes, sess_obj, rank, world, kmrels=None, nrels=0, device=None):
+    """This rank's share of the job's groups, device to device: the
+    session's groups split by hash % world on its GPU (xpuB200FinalParts),
+    the parts exchanged between the GPUs' memories in one NCCL
+    all_to_all_single (sizes first), and the parts received merged into a
+    fresh session straight from device memory (xpuB200MergeFinal on
+    device).  No group crosses host memory; the returned kds_final (this
+    rank's share) is read back for the caller."""
+    import torch
+    import torch.distributed as dist
+    import xpu_b200
+    offs = sess_obj.final_parts(world)
+    send = torch.empty(max(offs[-1], 256), dtype=torch.uint8, device=device)
+    torch.cuda.synchronize(device)
+    offs = sess_obj.final_parts(world, send.data_ptr(), send.numel())
+    sizes = [offs[r + 1] - offs[r] for r in range(world)]
+    send_n = torch.tensor(sizes, dtype=torch.int64, device=device)
+    recv_n = torch.empty(world, dtype=torch.int64, device=device)
+    dist.all_to_all_single(recv_n, send_n)
+    recv_sizes = recv_n.cpu().tolist()
+    recv = torch.empty(max(sum(recv_sizes), 256), dtype=torch.uint8, device=device)
+    dist.all_to_all_single(recv[:sum(recv_sizes)], send[:offs[-1]],
+                           output_split_sizes=recv_sizes, input_split_sizes=sizes)
+    torch.cuda.synchronize(device)
+    s = xpu_b200.Session(dev, session, kmrels, nrels)
+    try:
+        pos = 0
+        for n in recv_sizes:
+            if n:
+                s.merge_final(recv.data_ptr() + pos, on_device=True)
+            pos += n
+        final, _ = s.final()
+    finally:
+        s.close()
+    return final

@@ -66,6 +66,8 @@ def lib():
         L.xpuB200Submit.argtypes = [P, P, I, ctypes.POINTER(U64), EB]
         L.xpuB200Poll.argtypes = [P, U64, I, ctypes.POINTER(I), P, EB]
         L.xpuB200ServeConfig.argtypes = [P, U64, ctypes.c_uint32, EB]
+        L.xpuB200MemInfo.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]
+        L.xpuB200FinalParts.argtypes = [P, ctypes.c_uint32, P, U64, ctypes.POINTER(U64), ctypes.POINTER(U64), EB]
         L.xpuB200MixCreate.argtypes = [P, ctypes.c_uint32, P, P, ctypes.POINTER(P), EB]
         L.xpuB200MixExec.argtypes = [P, P, P]
         L.xpuB200MixTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
@@ -99,6 +101,9 @@ def parse_results(buf):
     final_nitems, = struct.unpack_from("<I", b, 24)
     return {"nitems_raw": nraw, "nitems_in": nin, "nitems_out": nout, "num_rels": nrels,
             "depth_out": stats, "final_nitems": final_nitems}
+
+
+ADMIT_FREE_HBM = (1 << 64) - 1          # XPU_B200_ADMIT_FREE_HBM
 
 
 class Device:
@@ -162,7 +167,15 @@ class Device:
             raise RuntimeError("upload failed")
         return base, base + shift
 
+    def mem_info(self):
+        """(free, total, reserve) bytes of device memory (xpuB200MemInfo)."""
+        fr, tot, res = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        lib().xpuB200MemInfo(self.h, ctypes.byref(fr), ctypes.byref(tot), ctypes.byref(res))
+        return fr.value, tot.value, res.value
+
     def serve_config(self, admit_bytes=0, alone_units=0):
+        """Admission budget (ADMIT_FREE_HBM: by free device memory) and
+        the size at which a command runs alone (0 keeps a value)."""
         e = KernErrorbuf()
         rc = lib().xpuB200ServeConfig(self.h, admit_bytes, alone_units, ctypes.byref(e))
         if rc:
@@ -276,6 +289,20 @@ class Session:
         if rc:
             raise XpuB200Error(rc, e)
         return buf, parse_results(res)
+
+    def final_parts(self, nparts, out_dptr=None, out_size=0):
+        """xpuB200FinalParts: the groups split into nparts hash partitions,
+        written back to back into device memory at out_dptr (out_size
+        bytes).  Returns the nparts + 1 part offsets (the last: the bytes
+        needed); with out_dptr None only the offsets are computed."""
+        offs = (ctypes.c_uint64 * (nparts + 1))()
+        req = ctypes.c_uint64()
+        e = KernErrorbuf()
+        rc = lib().xpuB200FinalParts(self.h, nparts, ctypes.c_void_p(out_dptr) if out_dptr else None,
+                                     out_size if out_dptr else 0, offs, ctypes.byref(req), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return list(offs)
 
     def merge_final(self, kds, on_device=False):
         """Merge another session's kds_final (a uint8 array from final(), or

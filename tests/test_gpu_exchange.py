@@ -1,10 +1,11 @@
 """The device side of the hash-partitioned multi-GPU merge, with three
-ranks emulated on one GPU: each rank's kds_final is split by hash % 3
-(xb_exchange.split_final, xpuB200InnerRebuild on group tuples) and rank r
-merges part r of every rank (xpuB200MergeFinal).  Every group must end on
-exactly one rank with the states of one session over all chunks; the
-exchange of the bytes between processes is tested with gloo ranks in
-test_multirank.py."""
+ranks emulated on one GPU: each rank's groups are split by hash % 3 on the
+device (xpuB200FinalParts, one buffer of three KDS_FORMAT_HASH parts) and
+rank r merges part r of every rank straight from device memory
+(xpuB200MergeFinal on device), as it would from a peer's memory.  Every
+group must end on exactly one rank with the states of one session over all
+chunks; the exchange of the bytes between processes is tested with gloo
+ranks in test_multirank.py."""
 import struct
 
 import pytest
@@ -19,63 +20,70 @@ pytestmark = pytest.mark.gpu
 WORLD = 3
 
 
-def _finals(device, sess, chunks, km=None, nrels=0):
-    out = []
-    for r in range(WORLD):
-        s = xpu_b200.Session(device, sess, km, nrels)
-        try:
+def _exchange(device, sess, chunks, km=None, nrels=0):
+    """Three emulated ranks, each with its share of the chunks; every rank
+    splits its groups on the device and rank r merges part r of all."""
+    sessions, bufs = [], []
+    try:
+        for r in range(WORLD):
+            s = xpu_b200.Session(device, sess, km, nrels)
+            sessions.append(s)
             for ch in chunks[r::WORLD]:
                 s.exec(ch)
-            f, _ = s.final()
-        finally:
+            bufs.append(X.final_parts(device, s, WORLD))
+        for base, offs in bufs:
+            assert offs[0] == 0 and all(o % 256 == 0 for o in offs)
+            for r in range(WORLD):
+                p = device.download(base + offs[r], offs[r + 1] - offs[r])
+                length, = struct.unpack_from("<Q", p, 0)
+                assert bytes(p[24:25]) == b"h" and length <= len(p)
+                p = p[:length]
+                # every tuple of part r hashes to r
+                n, = struct.unpack_from("<I", p, 16)
+                ncol, = struct.unpack_from("<I", p, 68)
+                nslots, = struct.unpack_from("<I", p, 40)
+                hl = (72 + 168 * ncol + 7) & ~7
+                for i in range(n):
+                    off, = struct.unpack_from("<Q", p, hl + 8 * nslots + 8 * i)
+                    h, = struct.unpack_from("<I", p, length - off + 4)
+                    assert h % WORLD == r
+        merged = {}
+        for r in range(WORLD):
+            m = xpu_b200.Session(device, sess, km, nrels)
+            try:
+                for base, offs in bufs:
+                    m.merge_final(base + offs[r], on_device=True)
+                f, _ = m.final()
+            finally:
+                m.close()
+            d = F.decode_kds_final(f, sess) if f is not None else {}
+            assert not (set(d) & set(merged))              # a group lives on one rank only
+            merged.update(d)
+        return merged
+    finally:
+        for s in sessions:
             s.close()
-        out.append(f)
-    return out
-
-
-def _exchange(device, sess, finals, km=None, nrels=0):
-    parts = [X.split_final(device, sess, f, WORLD) for f in finals]
-    for s_, ps in enumerate(parts):
-        for r, p in enumerate(ps):
-            if p is None:
-                continue
-            # every tuple of part r hashes to r
-            n, = struct.unpack_from("<I", p, 16)
-            ncol, = struct.unpack_from("<I", p, 68)
-            nslots, = struct.unpack_from("<I", p, 40)
-            hl = (72 + 168 * ncol + 7) & ~7
-            length = len(p)
-            for i in range(n):
-                off, = struct.unpack_from("<Q", p, hl + 8 * nslots + 8 * i)
-                h, = struct.unpack_from("<I", p, length - off + 4)
-                assert h % WORLD == r
-    shares = [X.merge_parts(device, sess, [parts[s_][r] for s_ in range(WORLD)], km, nrels)
-              for r in range(WORLD)]
-    merged = {}
-    for f in shares:
-        d = F.decode_kds_final(f, sess) if f is not None else {}
-        assert not (set(d) & set(merged))              # a group lives on one rank only
-        merged.update(d)
-    return merged
+        for base, _ in bufs:
+            device.free(base)
 
 
 def test_exchange_wide_groupby(device):
     tbl, sess, _, expect, meta = C.wide_groupby(nrows=300_000, ngroups=5000, seed_config=61)
     chunks = tbl.block_chunks(pages_per_chunk=128)
-    merged = _exchange(device, sess, _finals(device, sess, chunks))
+    merged = _exchange(device, sess, chunks)
     assert F.compare_groups(merged, expect) == []
 
 
 def test_exchange_arrow_many_groups(device):
     chunks, sess, expect, meta = C.arrow_groupby(nrows=900_000, nkeys=300_000, rows_per_chunk=100_000,
                                                  seed_config=62)
-    merged = _exchange(device, sess, _finals(device, sess, chunks))
+    merged = _exchange(device, sess, chunks)
     assert F.compare_groups(merged, expect) == []
 
 
 def test_exchange_join_text_keys(device):
     fact, sess, km, expect, meta = C.join_groupby(nfact=150_000, ndim1=5000, ndim2=700, seed_config=63)
     chunks = fact.block_chunks(pages_per_chunk=100)
-    merged = _exchange(device, sess, _finals(device, sess, chunks, km, 2), km, 2)
+    merged = _exchange(device, sess, chunks, km, 2)
     truth = {k: [v["sum_amount"], v["nrows"]] for k, v in expect.items()}
     assert F.compare_groups(merged, truth) == []

@@ -84,7 +84,7 @@ def test_served_same_as_alone_with_large_commands(device):
             assert F.compare_groups(got, want) == []
             assert F.compare_groups(got, c["truth"]) == []
     finally:
-        device.serve_config(admit_bytes=1 << 36, alone_units=256)
+        device.serve_config(admit_bytes=xpu_b200.ADMIT_FREE_HBM, alone_units=256)
         js.close()
         for s in ss:
             s.close()
@@ -108,3 +108,57 @@ def test_poll_without_wait_and_final_drains(device):
     finally:
         for s in sessions:
             s.close()
+
+
+def _rare_shape_session(ngroups=64):
+    """A GROUP BY whose aggregate list no other test uses, so that no
+    specialised kernel exists for its plan shape when it is first served."""
+    from xb_producer import Agg, Const, Func, SessionBuilder, Var
+    va, vb, vg = Var(0, 2, "int4"), Var(0, 3, "float8"), Var(0, 5, "int4")
+    return SessionBuilder(0, C.DEVTASK_PREAGG | C.DEVKIND_GPU).build(
+        scan_quals=Func("int4lt", [va, Const("int4", 700)], "bool"),
+        groupby_keys=[vg],
+        aggs=[Agg("NROWS_ANY"), Agg("PMAX_INT32", va), Agg("PMIN_INT32", va), Agg("NROWS_COND", vb),
+              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")), Agg("PMAX_FP64", vb), Agg("NROWS_ANY")],
+        ngroups_estimate=float(ngroups))
+
+
+@pytest.mark.parametrize("alone", [True, False])
+def test_new_plan_shape_served_while_its_kernel_builds(device, alone):
+    """A served command of a plan shape without a kernel runs at once on
+    the interpreting kernel while the specialised kernel builds on a
+    background thread (NVRTC takes seconds); commands after the build run
+    on the specialised kernel.  Every result equals the oracle's."""
+    import time
+    import xb_oracle as O
+    tbl, _, _, _, _ = C.scan_groupby(nrows=300_000, seed_config=90 if alone else 91)
+    sess = _rare_shape_session()
+    # alone: commands of >= 256 heap pages run alone; else small ones, mixed
+    chunks = tbl.block_chunks(pages_per_chunk=400 if alone else 60)
+    device.serve_config(admit_bytes=xpu_b200.ADMIT_FREE_HBM, alone_units=256)
+    s = xpu_b200.Session(device, sess)
+    try:
+        t0 = time.perf_counter()
+        device.poll(device.submit(s, chunks[0]))
+        first_s = time.perf_counter() - t0
+        assert s.info()["kernels"] == {"b": "vm"}, s.info()
+        used = 1
+        deadline = time.perf_counter() + 120.0
+        while time.perf_counter() < deadline:
+            device.poll(device.submit(s, chunks[used % len(chunks)]))
+            used += 1
+            if s.info()["kernels"] == {"b": "jit"}:
+                break
+            time.sleep(0.2)
+        assert s.info()["kernels"] == {"b": "jit"}, s.info()
+        # the first command did not wait for the build
+        assert first_s < s.info()["jit_compile_ms"] / 1000.0 or first_s < 1.0, (first_s, s.info())
+        final, _ = s.final()
+    finally:
+        s.close()
+    o = O.Oracle(sess)
+    for i in range(used):
+        o.exec(chunks[i % len(chunks)])
+    want = F.decode_kds_final(o.final(), sess)
+    o.close()
+    assert F.compare_groups(F.decode_kds_final(final, sess), want) == []

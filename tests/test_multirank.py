@@ -136,3 +136,78 @@ def test_alltoall_of_final_parts_over_gloo():
                 assert g is None
             else:
                 assert g == (7 * (s_ + r + 1), 16 * s_ + r, True)
+
+
+def _exchange_worker(rank, world, port, q):
+    for sub in ("pg-strom_b200", os.path.join("pg-strom_b200", "producer"), "oracle", ""):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        import bench
+        import xb_configs as C
+        import xb_exchange as X
+        import xb_final as F
+        import xb_oracle as O
+        import xb_split as S
+        # every rank's shard through the oracle, its kds_final split by hash
+        # % world, the parts exchanged, the received parts merged
+        fact, sess, km, expect, meta = C.join_groupby(nfact=30_000, ndim1=2000, ndim2=300,
+                                                      regions=C.long_strings(200, lo=8, hi=40),
+                                                      seed_config=bench.shard_seed(rank))
+        o = O.Oracle(sess, km)
+        for ch in fact.block_chunks(pages_per_chunk=100):
+            o.exec(ch)
+        parts = S.split_kds_final(o.final(), world)
+        o.close()
+        got = X.alltoall_bytes(parts, rank, world)
+        actions = [a for a, _, _ in F.session_aggs(sess) if a != 101]
+        mine, hashes_ok = {}, True
+        for p in got:
+            if p is None:
+                continue
+            hashes_ok &= all(h % world == rank for h in S.tuple_hashes(p))
+            for k, v in F.decode_kds_final(p, sess).items():
+                mine[k] = S.merge_states(actions, mine[k], v) if k in mine else v
+        # the truth of every shard, for the union
+        truth = {}
+        for r in range(world):
+            _, _, _, ex, _ = C.join_groupby(nfact=30_000, ndim1=2000, ndim2=300,
+                                            regions=C.long_strings(200, lo=8, hi=40),
+                                            seed_config=bench.shard_seed(r))
+            for k, v in ex.items():
+                t = truth.setdefault(k, [(0, 0), 0])
+                truth[k] = [(t[0][0] + v["sum_amount"][0], t[0][1] + v["sum_amount"][1]), t[1] + v["nrows"]]
+        q.put((rank, hashes_ok, {k: v for k, v in mine.items()}, truth))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_exchange_split_merge_through_the_oracle():
+    """The whole exchange step on two gloo ranks: each rank's oracle
+    kds_final split by hash % 2 (the host restatement of FinalParts), the
+    parts exchanged all-to-all, the received parts merged.  Every group
+    ends on the rank its hash names, on exactly one rank, and the ranks'
+    merged groups are the union of both shards."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    world = 2
+    procs = [ctx.Process(target=_exchange_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict((r[0], r[1:]) for r in (q.get(timeout=180) for _ in procs))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    import xb_final as F
+    union = {}
+    for r in range(world):
+        ok, mine, truth = res[r]
+        assert ok
+        assert not (set(mine) & set(union))
+        union.update(mine)
+    assert F.compare_groups(union, res[0][2], rtol=0.0) == []
