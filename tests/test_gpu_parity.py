@@ -95,6 +95,31 @@ def test_every_partial_state_form_parity(device, kernel):
         assert got[k][:4] == want[k][:4] and got[k][7] == want[k][7], k
 
 
+def test_every_partial_state_form_in_shared_tables(device, kernel):
+    """The same partial-state forms with a group estimate small enough for
+    the per-CTA shared-memory group table (its own state form on the
+    specialised kernel: min/max, stddev and covariance updated with
+    shared-memory atomics, merged into the global table at CTA exit)."""
+    tbl, _, _, expect, meta = C.wide_groupby(nrows=300_000, ngroups=300, seed_config=9)
+    sess = C.wide_groupby_session(ngroups=300)
+    chunks = tbl.block_chunks(pages_per_chunk=256)
+    s = xpu_b200.Session(device, sess)
+    try:
+        assert s.info()["sm_cap"] > 0, s.info()
+        for ch in chunks:
+            s.exec(ch)
+        check_kernel(s, kernel)
+        final, _ = s.final()
+    finally:
+        s.close()
+    got = F.decode_kds_final(final, sess)
+    assert F.compare_groups(got, expect) == []
+    ofinal, _ = run_oracle(sess, chunks)
+    want = F.decode_kds_final(ofinal, sess)
+    for k in want:
+        assert got[k][:4] == want[k][:4] and got[k][7] == want[k][7], k
+
+
 def test_scan_groupby_device_resident(device, kernel):
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=100_000)
     chunks = tbl.block_chunks(pages_per_chunk=200)
