@@ -23,7 +23,6 @@
  * (cuda_gpupreagg.cu:18-223).
  */
 #include <cuda_runtime.h>
-#include <cub/cub.cuh>
 #include <algorithm>
 #include <deque>
 #include <map>
@@ -43,6 +42,7 @@
 #include "xb_exec_dev.cuh"
 #include "xb_compile.h"
 #include "xb_jit.h"
+#include "xb_sort.cuh"
 #include "xpu_b200.h"
 
 /* ================================================================
@@ -1644,10 +1644,6 @@ __global__ void xb_sort_keep(XbKeepArgs a, const uint32_t *keep_scan, int64_t *k
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x)
         keep[a.ents[a.idx[p]]] = a.keep_flag[p] ? (int64_t)keep_scan[p] : -1;
 }
-
-struct XbMaxOp {
-    __device__ __forceinline__ uint32_t operator()(uint32_t x, uint32_t y) const { return x > y ? x : y; }
-};
 
 __global__ void xb_iota_u32(uint32_t *out, uint32_t n)
 {
@@ -3811,11 +3807,9 @@ static int xb_final_sort(xpuB200Session *s, XbFinalArgs fa, cudaStream_t st, All
     const int grid = s->dev->nsm * 8;
     fa.keep = nullptr;
     xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);              /* flags of every group */
-    size_t tb = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, tb, fa.flags, fa.flag_scan, (int64_t)cap, st);
     void *d_t = nullptr;
-    if (!alloc(tb, &d_t)) return -1;
-    cub::DeviceScan::ExclusiveSum(d_t, tb, fa.flags, fa.flag_scan, (int64_t)cap, st);
+    if (!alloc(xb_scan_temp_bytes<uint32_t>(cap), &d_t)) return -1;
+    if (xb_scan<uint32_t, XbOpSum, true>(fa.flags, fa.flag_scan, cap, d_t, st) != cudaSuccess) return -1;
     uint32_t lf = 0, ls = 0;
     cudaMemcpyAsync(&lf, fa.flags + cap - 1, 4, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&ls, fa.flag_scan + cap - 1, 4, cudaMemcpyDeviceToHost, st);
@@ -3855,31 +3849,23 @@ static int xb_final_sort(xpuB200Session *s, XbFinalArgs fa, cudaStream_t st, All
     xb_sort_gather<<<grid, XB_BLOCK, 0, st>>>(sa);
     xb_sort_keys<<<g2, XB_BLOCK, 0, st>>>(sa);
     xb_iota_u32<<<g2, XB_BLOCK, 0, st>>>(idx, n);
-    /* temporary storage for the largest of the library passes */
-    size_t t64 = 0, t8 = 0, tmax = 0, tsum = 0, tex = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t64, k64a, k64b, idx, idx2, (int64_t)n, 0, 64, st);
-    cub::DeviceRadixSort::SortPairs(nullptr, t8, k8a, k8b, idx, idx2, (int64_t)n, 0, 1, st);
-    cub::DeviceScan::InclusiveScan(nullptr, tmax, part, part, XbMaxOp(), (int64_t)n, st);
-    cub::DeviceScan::InclusiveSum(nullptr, tsum, pflag, pcnt, (int64_t)n, st);
-    cub::DeviceScan::ExclusiveSum(nullptr, tex, kflag, kscan, (int64_t)n, st);
-    size_t tt = std::max(std::max(t64, t8), std::max(tmax, std::max(tsum, tex)));
+    /* temporary storage for the largest of the sort and scan passes */
+    const size_t tt = std::max(xb_radix_temp_bytes(n), xb_scan_temp_bytes<uint32_t>(n));
     void *d_tt = nullptr;
     if (!alloc(tt, &d_tt)) return -1;
     /* stable passes, least significant first: for each key from the last,
-     * its low word, its high word, then its NULL flag */
+     * its low word, its high word, then its NULL flag (each a stable radix
+     * sort of the word gathered in the current order, carrying the group
+     * indexes along) */
     for (int k = (int)nk - 1; k >= 0; k--) {
         for (int w = 1; w >= 0; w--) {
             if (w == 1 && plan->sort[k].words < 2)
                 continue;
             xb_sort_pass_key64<<<g2, XB_BLOCK, 0, st>>>(keyw + (2ULL * k + w) * n, idx, k64a, n);
-            size_t t = tt;
-            cub::DeviceRadixSort::SortPairs(d_tt, t, k64a, k64b, idx, idx2, (int64_t)n, 0, 64, st);
-            std::swap(idx, idx2);
+            if (xb_radix_sort<uint64_t>(k64a, k64b, idx, idx2, n, 64, d_tt, st) != cudaSuccess) return -1;
         }
         xb_sort_pass_key8<<<g2, XB_BLOCK, 0, st>>>(nul + (uint64_t)k * n, idx, k8a, n);
-        size_t t = tt;
-        cub::DeviceRadixSort::SortPairs(d_tt, t, k8a, k8b, idx, idx2, (int64_t)n, 0, 1, st);
-        std::swap(idx, idx2);
+        if (xb_radix_sort<uint8_t>(k8a, k8b, idx, idx2, n, 8, d_tt, st) != cudaSuccess) return -1;
     }
     XbRankArgs ra;
     ra.plan = s->d_plan;
@@ -3892,12 +3878,10 @@ static int xb_final_sort(xpuB200Session *s, XbFinalArgs fa, cudaStream_t st, All
     ra.peer_flag = pflag;
     if (plan->sort_window) {
         xb_sort_bounds<<<g2, XB_BLOCK, 0, st>>>(ra);
-        size_t t = tt;
-        cub::DeviceScan::InclusiveScan(d_tt, t, part, part, XbMaxOp(), (int64_t)n, st);
-        t = tt;
-        cub::DeviceScan::InclusiveScan(d_tt, t, peer, peer, XbMaxOp(), (int64_t)n, st);
-        t = tt;
-        cub::DeviceScan::InclusiveSum(d_tt, t, pflag, pcnt, (int64_t)n, st);
+        if (xb_scan<uint32_t, XbOpMax, false>(part, part, n, d_tt, st) != cudaSuccess ||
+            xb_scan<uint32_t, XbOpMax, false>(peer, peer, n, d_tt, st) != cudaSuccess ||
+            xb_scan<uint32_t, XbOpSum, false>(pflag, pcnt, n, d_tt, st) != cudaSuccess)
+            return -1;
     }
     XbKeepArgs ka;
     ka.plan = s->d_plan;
@@ -3909,8 +3893,7 @@ static int xb_final_sort(xpuB200Session *s, XbFinalArgs fa, cudaStream_t st, All
     ka.peer_cnt = pcnt;
     ka.keep_flag = kflag;
     xb_sort_keepflag<<<g2, XB_BLOCK, 0, st>>>(ka);
-    size_t t = tt;
-    cub::DeviceScan::ExclusiveSum(d_tt, t, kflag, kscan, (int64_t)n, st);
+    if (xb_scan<uint32_t, XbOpSum, true>(kflag, kscan, n, d_tt, st) != cudaSuccess) return -1;
     xb_sort_keep<<<g2, XB_BLOCK, 0, st>>>(ka, kscan, keep);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -3954,7 +3937,6 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     uint32_t *d_flags = nullptr, *d_flag_scan = nullptr;
     char *d_out = nullptr;
     void *d_temp = nullptr;
-    size_t temp1 = 0, temp2 = 0;
     int rc = 0;
     std::vector<void *> tmp;
     auto alloc = [&](size_t sz, void **p) -> bool {
@@ -3990,16 +3972,12 @@ xpuB200Final(xpuB200Session *s, void *kds_final_buf, uint64_t buf_sz, uint64_t *
     }
     /* the global table's entries pointer lives in h_gt */
     xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
-    cub::DeviceScan::ExclusiveSum(nullptr, temp1, d_sizes, d_size_scan, (int64_t)cap, st);
-    cub::DeviceScan::ExclusiveSum(nullptr, temp2, d_flags, d_flag_scan, (int64_t)cap, st);
-    if (!alloc(temp1 > temp2 ? temp1 : temp2, &d_temp)) {
+    if (!alloc(xb_scan_temp_bytes<uint64_t>(cap), &d_temp)) {
         cleanup();
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in Final");
     }
-    size_t tsz = temp1 > temp2 ? temp1 : temp2;
-    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_sizes, d_size_scan, (int64_t)cap, st);
-    tsz = temp1 > temp2 ? temp1 : temp2;
-    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_flags, d_flag_scan, (int64_t)cap, st);
+    xb_scan<uint64_t, XbOpSum, true>(d_sizes, d_size_scan, cap, d_temp, st);
+    xb_scan<uint32_t, XbOpSum, true>(d_flags, d_flag_scan, cap, d_temp, st);
     uint64_t last_size = 0, last_scan = 0;
     uint32_t last_flag = 0, last_fscan = 0;
     cudaMemcpyAsync(&last_size, d_sizes + cap - 1, 8, cudaMemcpyDeviceToHost, st);
@@ -4228,10 +4206,7 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     uint32_t *d_flags = (uint32_t *)(scratch + off_flags);
     uint32_t *d_flag_scan = (uint32_t *)(scratch + off_fscan);
     void *d_temp = scratch + off_temp;
-    size_t temp1 = 0, temp2 = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, temp1, d_sizes, d_size_scan, (int64_t)cap, st);
-    cub::DeviceScan::ExclusiveSum(nullptr, temp2, d_flags, d_flag_scan, (int64_t)cap, st);
-    const uint64_t tsz_max = temp1 > temp2 ? temp1 : temp2;
+    const uint64_t tsz_max = xb_scan_temp_bytes<uint64_t>(cap);
     if (off_temp + tsz_max > XB_FINAL_SCRATCH_BYTES)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR,
                       "FinalNoAlloc: the session's group table has %llu slots and needs %llu bytes of work "
@@ -4266,10 +4241,8 @@ xpuB200FinalNoAlloc(xpuB200Session *s, void *kds_final_dev, uint64_t buf_sz, uin
     fa.row_format = row_fmt ? 1 : 0;
     const int grid = s->dev->nsm * 8;
     xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
-    size_t tsz = tsz_max;
-    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_sizes, d_size_scan, (int64_t)cap, st);
-    tsz = tsz_max;
-    cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_flags, d_flag_scan, (int64_t)cap, st);
+    xb_scan<uint64_t, XbOpSum, true>(d_sizes, d_size_scan, cap, d_temp, st);
+    xb_scan<uint32_t, XbOpSum, true>(d_flags, d_flag_scan, cap, d_temp, st);
     uint64_t last_size = 0, last_scan = 0;
     uint32_t last_flag = 0, last_fscan = 0;
     cudaMemcpyAsync(&last_size, d_sizes + cap - 1, 8, cudaMemcpyDeviceToHost, st);
@@ -4364,10 +4337,7 @@ xpuB200FinalParts(xpuB200Session *s, uint32_t nparts, void *parts_dev, uint64_t 
         cleanup();
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in FinalParts");
     }
-    size_t t1 = 0, t2 = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, t1, d_sizes, d_size_scan, (int64_t)cap, st);
-    cub::DeviceScan::ExclusiveSum(nullptr, t2, d_flags, d_flag_scan, (int64_t)cap, st);
-    const size_t tsz_max = t1 > t2 ? t1 : t2;
+    const size_t tsz_max = xb_scan_temp_bytes<uint64_t>(cap);
     if (!alloc(tsz_max, &d_temp)) {
         cleanup();
         return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory in FinalParts");
@@ -4387,10 +4357,8 @@ xpuB200FinalParts(xpuB200Session *s, uint32_t nparts, void *parts_dev, uint64_t 
     auto size_part = [&](uint32_t p, uint64_t *p_items, uint64_t *p_groups) -> int {
         fa.part_rem = p;
         xb_final_sizes<<<grid, XB_BLOCK, 0, st>>>(fa);
-        size_t tsz = tsz_max;
-        cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_sizes, d_size_scan, (int64_t)cap, st);
-        tsz = tsz_max;
-        cub::DeviceScan::ExclusiveSum(d_temp, tsz, d_flags, d_flag_scan, (int64_t)cap, st);
+        xb_scan<uint64_t, XbOpSum, true>(d_sizes, d_size_scan, cap, d_temp, st);
+        xb_scan<uint32_t, XbOpSum, true>(d_flags, d_flag_scan, cap, d_temp, st);
         uint64_t last_size = 0, last_scan = 0;
         uint32_t last_flag = 0, last_fscan = 0;
         cudaMemcpyAsync(&last_size, d_sizes + cap - 1, 8, cudaMemcpyDeviceToHost, st);

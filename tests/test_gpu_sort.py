@@ -97,3 +97,29 @@ def test_sort_without_groups(device):
         s.close()
     assert res["final_nitems"] == 0
     assert final is None or F.decode_kds_final(final, sess) == {}
+
+
+@pytest.mark.parametrize("i", [1, 3, 6])
+def test_sorted_final_many_groups(device, i):
+    # 60,000 groups: the radix passes and scans span many 4096-element tiles
+    tbl, _, _, expect, meta = C.wide_groupby(nrows=400_000, ngroups=60_000, seed_config=44)
+    chunks = tbl.block_chunks(pages_per_chunk=512)
+    sort = SORTS[i]
+    sess = C.wide_groupby_session(ngroups=60_000, sort=sort)
+    o = O.Oracle(sess)
+    for ch in chunks:
+        o.exec(ch)
+    orows = list(F.decode_kds_final(o.final(), sess).items())
+    o.close()
+    s = xpu_b200.Session(device, sess)
+    try:
+        for ch in chunks:
+            s.exec(ch)
+        final, res = s.final()
+    finally:
+        s.close()
+    got = F.decode_kds_final(final, sess)
+    want = F.order_groups(orows, sess, sort["keys"], sort.get("window"), sort.get("limit", 0))
+    assert res["final_nitems"] == len(want)
+    _check(list(got.items()), want, sess, sort["keys"])
+    assert F.compare_groups(got, {k: expect[k] for k in got}) == []
