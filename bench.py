@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--keys", type=int, default=10_000_000)
     ap.add_argument("--requests", type=int, default=400)
     ap.add_argument("--qps", type=float, default=200.0)
+    ap.add_argument("--served-arrow-rows", type=int, default=500_000_000,
+                    help="served: rows of the Arrow template's table (queries take 1M..all of it)")
+    ap.add_argument("--no-served-leg", dest="served_leg", action="store_false",
+                    help="headline line: skip the short served-mix measurement")
     return ap.parse_args()
 
 
@@ -448,6 +452,14 @@ def run_b200(args, rank, world, local):
                "sample": f"{rows} fact rows of the same workload in {el:.1f} s on {threads} threads "
                          f"({'PG-Strom expression library host-compiled from the reference' if kind == 'reference' else 'C restatement'})"}
 
+    # ---- served mix (rank 0, N=1): continuous batching against the plain drop-in
+    served = None
+    if rank == 0 and world == 1 and args.served_leg:
+        try:
+            served = served_leg(dev)
+        except Exception as e:          # the headline stands without it
+            served = {"error": f"{type(e).__name__}: {e}"[:300]}
+
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -487,6 +499,8 @@ def run_b200(args, rank, world, local):
                 "gpu_launches": args.steps,
                 "parity": parity,
                 "cpu_baseline": cpu}
+        if served:
+            line["served"] = served
         if merge:
             line["final_merge"] = merge
         print(json.dumps(line), flush=True)
@@ -779,13 +793,54 @@ FINAL_THREADS = 4               # kds_final read-backs in flight
 FINAL_BUF_BYTES = 1536 << 20    # pinned response buffer per read-back
 
 
-def _pinned_buffers():
+def _pinned_buffers(nbytes=FINAL_BUF_BYTES):
     import queue
     import torch
     q = queue.Queue()
     for _ in range(FINAL_THREADS):
-        q.put(torch.empty(FINAL_BUF_BYTES, dtype=torch.uint8, pin_memory=True).numpy())
+        q.put(torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy())
     return q
+
+
+def _served_compare(dev, tables, requests, qps, bufs):
+    """The served and plain forms over the same requests: open-loop p50 /
+    p99 at the offered rate and saturation throughput (every query queued
+    at once), after a warm-up of both."""
+    reqs = _requests(tables, requests, qps)
+    warm = _requests(tables, 30, qps, seed=7)
+    served = lambda d, r, t: _serve_batched(d, r, t, bufs)
+    _serve_plain(dev, warm, time.perf_counter())      # kernel cache, pools
+    served(dev, warm, time.perf_counter())
+    res = {}
+    for mode, fn in (("plain", _serve_plain), ("served", served)):
+        lat, el = fn(dev, reqs, time.perf_counter())
+        sat = [dict(q, t=0.0) for q in reqs]
+        _, sat_el = fn(dev, sat, time.perf_counter())
+        res[mode] = {"qps": len(reqs) / el, "p50_ms": 1000 * float(np.percentile(lat, 50)),
+                     "p99_ms": 1000 * float(np.percentile(lat, 99)),
+                     "saturation_qps": len(reqs) / sat_el}
+    mix = {k: sum(1 for q in reqs if q["tpl"] == k) for k in range(3)}
+    return res, mix
+
+
+def served_leg(dev, requests=100, qps=200.0):
+    """A short served-mix measurement for the headline line: 100 Poisson
+    requests (mean 200 QPS) over resident tables of 8M (scan), 20M (join)
+    and 20M (Arrow) rows, served and plain."""
+    t0 = time.time()
+    tables = _Tables(dev, rows0=8_000_000, rows1=20_000_000, rows2=20_000_000)
+    gen_s = time.time() - t0
+    try:
+        res, mix = _served_compare(dev, tables, requests, qps, _pinned_buffers(512 << 20))
+    finally:
+        tables.free(dev)
+    return {"requests": requests, "offered_qps": qps, "template_counts": mix,
+            "tables_rows": [8_000_000, 20_000_000, 20_000_000], "generation_s": round(gen_s, 1),
+            "qps": res["served"]["qps"], "p50_ms": res["served"]["p50_ms"],
+            "p99_ms": res["served"]["p99_ms"], "saturation_qps": res["served"]["saturation_qps"],
+            "plain_qps": res["plain"]["qps"], "plain_p50_ms": res["plain"]["p50_ms"],
+            "plain_p99_ms": res["plain"]["p99_ms"], "plain_saturation_qps": res["plain"]["saturation_qps"],
+            "saturation_ratio": res["served"]["saturation_qps"] / res["plain"]["saturation_qps"]}
 
 
 def _serve_batched(dev, reqs, start, bufs):
@@ -840,30 +895,17 @@ def run_served(args):
     import xpu_b200
     dev = xpu_b200.Device(0)
     t0 = time.time()
-    tables = _Tables(dev, rows0=16_000_000, rows1=50_000_000, rows2=50_000_000)
+    tables = _Tables(dev, rows0=16_000_000, rows1=50_000_000, rows2=args.served_arrow_rows)
     gen_s = time.time() - t0
-    reqs = _requests(tables, args.requests, args.qps)
-    warm = _requests(tables, 30, args.qps, seed=7)
-    bufs = _pinned_buffers()
-    served = lambda d, r, t: _serve_batched(d, r, t, bufs)
-    _serve_plain(dev, warm, time.perf_counter())      # kernel cache, pools
-    served(dev, warm, time.perf_counter())
-    res = {}
-    for mode, fn in (("plain", _serve_plain), ("served", served)):
-        lat, el = fn(dev, reqs, time.perf_counter())
-        sat = [dict(q, t=0.0) for q in reqs]
-        _, sat_el = fn(dev, sat, time.perf_counter())
-        res[mode] = {"qps": len(reqs) / el, "p50_ms": 1000 * float(np.percentile(lat, 50)),
-                     "p99_ms": 1000 * float(np.percentile(lat, 99)),
-                     "saturation_qps": len(reqs) / sat_el}
-    mix = {k: sum(1 for q in reqs if q["tpl"] == k) for k in range(3)}
+    res, mix = _served_compare(dev, tables, args.requests, args.qps, _pinned_buffers())
     line = {"metric": "served QPS (p50/p99 latency)", "value": res["served"]["saturation_qps"],
             "unit": "queries/s", "n_gpus": 1, "higher_is_better": True, "vs_baseline": None,
             "dtype": "int64", "data": "synthetic (seeded)",
             "config": {"workload": "Poisson arrivals, templates 50/30/20 (scan+group-by 16M-row heap, "
-                                   "two-way join 50M-row heap, Arrow group-by 50M rows), rows log-uniform "
+                                   "two-way join 50M-row heap, Arrow group-by "
+                                   f"{args.served_arrow_rows // 1_000_000}M rows), rows log-uniform "
                                    "1M..table per query, randomized constants, tables resident in HBM",
-                       "requests": len(reqs), "offered_qps": args.qps, "template_counts": mix,
+                       "requests": args.requests, "offered_qps": args.qps, "template_counts": mix,
                        "resident_bytes": tables.bytes, "generation_s": round(gen_s, 1)},
             "served": res["served"], "plain": res["plain"],
             "served_inner_cache_bytes": dev.inner_cache(),

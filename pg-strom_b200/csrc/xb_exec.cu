@@ -3528,11 +3528,27 @@ static int xb_replay_retry(xpuB200Session *s, uint32_t format, kern_errorbuf *er
  * launches are added to the session and written to *results.  timed:
  * ev0 / ev1 bracket every launch of the run.
  */
+/* can the session's groups outnumber what its table holds below the
+ * growth threshold?  Not without GROUP BY keys (one group), nor when the
+ * keys come numbered from an inner relation (at most that many groups) */
+static bool xb_groups_may_grow(const xpuB200Session *s)
+{
+    const xb_plan *plan = s->h_plan;
+    if (plan->has_groupby != 1 || !s->h_gt.entries)
+        return false;
+    const uint32_t gd = plan->gid_depth;
+    if (gd >= 1 && gd <= plan->nrels && plan->inner[gd].gid_on &&
+        (uint64_t)plan->inner[gd].ngids < s->h_gt.soft_cap)
+        return false;
+    return true;
+}
+
 static int xb_run(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks, uint64_t nunits,
                   uint32_t format, kern_exec_results *results, kern_errorbuf *err, bool timed = false)
 {
     cudaStream_t st = s->stream;
-    const bool growth = s->h_plan->has_groupby != 0 && s->h_gt.entries != nullptr;
+    /* warps look for a growth request only where one can come */
+    const bool growth = xb_groups_may_grow(s);
     if (growth && !s->d_left[0]) {
         /* two leftover records per warp of the largest grid (8 CTAs per SM) */
         const uint32_t cap = 2u * (uint32_t)s->dev->nsm * 8u * XB_WARPS;

@@ -112,16 +112,18 @@ def test_poll_without_wait_and_final_drains(device):
             s.close()
 
 
-def _rare_shape_session(ngroups=64):
-    """A GROUP BY whose aggregate list no other test uses, so that no
-    specialised kernel exists for its plan shape when it is first served."""
+def _rare_shape_session(variant=0, ngroups=64):
+    """A GROUP BY whose aggregate list no other test uses (variant adds
+    count(*) columns), so that no specialised kernel exists for its plan
+    shape when it is first served."""
     from xb_producer import Agg, Const, Func, SessionBuilder, Var
     va, vb, vg = Var(0, 2, "int4"), Var(0, 3, "float8"), Var(0, 5, "int4")
     return SessionBuilder(0, C.DEVTASK_PREAGG | C.DEVKIND_GPU).build(
         scan_quals=Func("int4lt", [va, Const("int4", 700)], "bool"),
         groupby_keys=[vg],
         aggs=[Agg("NROWS_ANY"), Agg("PMAX_INT32", va), Agg("PMIN_INT32", va), Agg("NROWS_COND", vb),
-              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")), Agg("PMAX_FP64", vb), Agg("NROWS_ANY")],
+              Agg("PSUM_INT", Func("int4_to_int8", [va], "int8")), Agg("PMAX_FP64", vb)] +
+             [Agg("NROWS_ANY")] * (1 + variant),
         ngroups_estimate=float(ngroups))
 
 
@@ -134,7 +136,7 @@ def test_new_plan_shape_served_while_its_kernel_builds(device, alone):
     import time
     import xb_oracle as O
     tbl, _, _, _, _ = C.scan_groupby(nrows=300_000, seed_config=90 if alone else 91)
-    sess = _rare_shape_session()
+    sess = _rare_shape_session(variant=0 if alone else 1)
     # alone: commands of >= 256 heap pages run alone; else small ones, mixed
     chunks = tbl.block_chunks(pages_per_chunk=400 if alone else 60)
     device.serve_config(admit_bytes=xpu_b200.ADMIT_FREE_HBM, alone_units=256)
