@@ -703,15 +703,19 @@ def run_mixed(args):
 
 # ------------------------------------------------------------------ served mix
 class _Tables:
-    """Device-resident tables of the three query templates."""
+    """The three query templates' tables, resident in HBM through the
+    library's chunk cache (xpuB200ChunkCachePut), as a service keeps its
+    cached tables across requests."""
 
     def __init__(self, dev, rows0, rows1, rows2):
         import xb_configs as C
         self.bytes = 0
+        self.handle = 0x7AB0
 
         def up(chunks):
             self.bytes += sum(c.nbytes for c in chunks)
-            return [dev.upload(c) for c in chunks]
+            self.handle += 1
+            return [(None, dev.chunk_put(self.handle, i, c)) for i, c in enumerate(chunks)]
         tbl0, _, _, _, _ = C.scan_groupby(nrows=rows0, seed_config=20)
         self.t0 = up(tbl0.block_chunks(pages_per_chunk=8190))
         self.rows0 = rows0
@@ -728,8 +732,10 @@ class _Tables:
 
     def free(self, dev):
         for t in (self.t0, self.t1, self.t2):
-            for b, _ in t:
-                dev.free(b)
+            for _, p in t:
+                dev.chunk_release(p)
+        dev.chunk_cache(0)                  # the released chunks leave
+        dev.chunk_cache(64 << 30)           # the default budget again
 
 
 INNER_HANDLE_DIMS = 0xD1D2      # join_inner_handle of the join template's dimension tables

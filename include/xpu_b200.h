@@ -332,6 +332,30 @@ void xpuB200BatchDestroy(xpuB200Batch *batch);
 int  xpuB200InnerCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes,
                              kern_errorbuf *err);
 
+/*
+ * Outer-table chunks resident in HBM across sessions: the device-side
+ * copy of a table that GPU-Cache keeps (src/gpu_cache.c), and the chunks
+ * relscan.c / Arrow_Fdw would otherwise read and send for every query.
+ * xpuB200ChunkCachePut places chunk chunk_no of table table_handle on the
+ * device (from host memory, or device memory with kds_on_device; heap
+ * pages 16-byte aligned), or finds it there, and returns its device
+ * address in *p_kds_dev for ExecTask / Submit / batches with
+ * kds_src_on_device; xpuB200ChunkCacheGet only finds (1: not resident).
+ * Both pin the chunk until xpuB200ChunkCacheRelease; unpinned chunks stay
+ * while the cache holds at most max_bytes (xpuB200ChunkCacheConfig,
+ * default 64 GiB; least recently used first out; UINT64_MAX only reads
+ * *p_cached_bytes).  The caller guarantees that one (table_handle,
+ * chunk_no) always names the same contents.
+ */
+int  xpuB200ChunkCachePut(xpuB200Device *dev, uint64_t table_handle, uint32_t chunk_no,
+                          const kern_data_store *kds, int kds_on_device,
+                          const kern_data_store **p_kds_dev, kern_errorbuf *err);
+int  xpuB200ChunkCacheGet(xpuB200Device *dev, uint64_t table_handle, uint32_t chunk_no,
+                          const kern_data_store **p_kds_dev);
+int  xpuB200ChunkCacheRelease(xpuB200Device *dev, const kern_data_store *kds_dev);
+int  xpuB200ChunkCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes,
+                             kern_errorbuf *err);
+
 int  xpuB200InnerRebuild(xpuB200Device *dev, kern_data_store *kds_dst, const kern_data_store *kds_src,
                          uint32_t hash_divisor, uint32_t hash_remainder, uint64_t *p_required,
                          kern_errorbuf *err);

@@ -2042,6 +2042,22 @@ struct xpuB200Device {
     uint64_t        inner_budget = 16ULL << 30;
     uint64_t        inner_bytes = 0;
     uint64_t        inner_clock = 0;
+    /* outer-table chunks resident across sessions (xpuB200ChunkCache*) */
+    std::mutex      chunk_lock;
+    std::map<std::pair<uint64_t, uint32_t>, struct xb_chunk_entry> chunk_cache;
+    uint64_t        chunk_budget = 64ULL << 30;
+    uint64_t        chunk_bytes = 0;
+    uint64_t        chunk_clock = 0;
+};
+
+/* one resident chunk: the device copy of a caller's chunk, placed so that
+ * heap pages start 16-byte aligned; refs counts the callers using it */
+struct xb_chunk_entry {
+    char           *base = nullptr;
+    const kern_data_store *kds = nullptr;
+    uint64_t        bytes = 0;
+    uint32_t        refs = 0;
+    uint64_t        last_use = 0;
 };
 
 /* one cached set of inner relations: the built descriptors (with their
@@ -2423,6 +2439,9 @@ xpuB200Shutdown(xpuB200Device *dev)
     for (xb_inner_entry *e : dev->inner_cache)
         xb_inner_entry_free(dev, e);
     dev->inner_cache.clear();
+    for (auto &kv : dev->chunk_cache)
+        cudaFreeAsync(kv.second.base, dev->stream);
+    dev->chunk_cache.clear();
     cudaStreamSynchronize(dev->stream);
     cudaStreamDestroy(dev->stream);
     for (cudaStream_t st : dev->free_streams)
@@ -5704,6 +5723,134 @@ xpuB200InnerCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cach
     xb_inner_evict_locked(dev);
     if (p_cached_bytes)
         *p_cached_bytes = dev->inner_bytes;
+    return 0;
+}
+
+/* ----------------------------------------------------------------
+ * outer-table chunks resident in HBM across sessions
+ * ---------------------------------------------------------------- */
+/* drop unused chunks, least recently used first, while the cache holds
+ * more than its budget; chunk_lock held */
+static void xb_chunk_evict_locked(xpuB200Device *dev)
+{
+    while (dev->chunk_bytes > dev->chunk_budget) {
+        auto victim = dev->chunk_cache.end();
+        for (auto it = dev->chunk_cache.begin(); it != dev->chunk_cache.end(); ++it)
+            if (it->second.refs == 0 &&
+                (victim == dev->chunk_cache.end() || it->second.last_use < victim->second.last_use))
+                victim = it;
+        if (victim == dev->chunk_cache.end())
+            return;                     /* every chunk is in use */
+        cudaFreeAsync(victim->second.base, dev->stream);
+        dev->chunk_bytes -= victim->second.bytes;
+        dev->chunk_cache.erase(victim);
+    }
+}
+
+extern "C" int
+xpuB200ChunkCachePut(xpuB200Device *dev, uint64_t table_handle, uint32_t chunk_no,
+                     const kern_data_store *kds, int kds_on_device,
+                     const kern_data_store **p_kds_dev, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!dev || !kds || !p_kds_dev)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid ChunkCachePut arguments");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    std::lock_guard<std::mutex> g(dev->chunk_lock);
+    const auto key = std::make_pair(table_handle, chunk_no);
+    auto it = dev->chunk_cache.find(key);
+    if (it != dev->chunk_cache.end()) {
+        it->second.refs++;
+        it->second.last_use = ++dev->chunk_clock;
+        *p_kds_dev = it->second.kds;
+        return 0;
+    }
+    /* the header, to place the chunk and check it */
+    std::vector<char> hb(offsetof(kern_data_store, colmeta));
+    if (kds_on_device) {
+        XB_CUDA(cudaMemcpy(hb.data(), kds, hb.size(), cudaMemcpyDeviceToHost), err);
+        const kern_data_store *h = (const kern_data_store *)hb.data();
+        hb.resize(KDS_HEAD_LENGTH(h));
+        XB_CUDA(cudaMemcpy(hb.data(), kds, hb.size(), cudaMemcpyDeviceToHost), err);
+    } else {
+        hb.assign((const char *)kds, (const char *)kds + KDS_HEAD_LENGTH(kds));
+    }
+    const kern_data_store *h = (const kern_data_store *)hb.data();
+    int rc = xb_check_kds(h, err);
+    if (rc) return rc;
+    /* heap pages start 16-byte aligned on the device */
+    const uint64_t shift = h->format == KDS_FORMAT_BLOCK ? (16 - (h->block_offset & 15)) & 15 : 0;
+    const uint64_t bytes = h->length + shift;
+    char *base = nullptr;
+    if (cudaMallocAsync((void **)&base, bytes, dev->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for a resident chunk of %llu bytes",
+                      (unsigned long long)h->length);
+    }
+    XB_CUDA(cudaMemcpyAsync(base + shift, kds, h->length,
+                            kds_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, dev->stream), err);
+    /* the chunk is complete before any other stream reads it */
+    XB_CUDA(cudaStreamSynchronize(dev->stream), err);
+    xb_chunk_entry e;
+    e.base = base;
+    e.kds = (const kern_data_store *)(base + shift);
+    e.bytes = bytes;
+    e.refs = 1;
+    e.last_use = ++dev->chunk_clock;
+    dev->chunk_cache[key] = e;
+    dev->chunk_bytes += bytes;
+    xb_chunk_evict_locked(dev);
+    *p_kds_dev = e.kds;
+    return 0;
+}
+
+extern "C" int
+xpuB200ChunkCacheGet(xpuB200Device *dev, uint64_t table_handle, uint32_t chunk_no,
+                     const kern_data_store **p_kds_dev)
+{
+    if (!dev || !p_kds_dev)
+        return ERRCODE_DEVICE_ERROR;
+    std::lock_guard<std::mutex> g(dev->chunk_lock);
+    auto it = dev->chunk_cache.find(std::make_pair(table_handle, chunk_no));
+    if (it == dev->chunk_cache.end())
+        return 1;
+    it->second.refs++;
+    it->second.last_use = ++dev->chunk_clock;
+    *p_kds_dev = it->second.kds;
+    return 0;
+}
+
+extern "C" int
+xpuB200ChunkCacheRelease(xpuB200Device *dev, const kern_data_store *kds_dev)
+{
+    if (!dev)
+        return ERRCODE_DEVICE_ERROR;
+    cudaSetDevice(dev->dindex);
+    std::lock_guard<std::mutex> g(dev->chunk_lock);
+    for (auto &kv : dev->chunk_cache) {
+        if (kv.second.kds == kds_dev && kv.second.refs > 0) {
+            kv.second.refs--;
+            xb_chunk_evict_locked(dev);
+            return 0;
+        }
+    }
+    return ERRCODE_DEVICE_ERROR;
+}
+
+extern "C" int
+xpuB200ChunkCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    if (!dev)
+        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid device");
+    XB_CUDA(cudaSetDevice(dev->dindex), err);
+    std::lock_guard<std::mutex> g(dev->chunk_lock);
+    if (max_bytes != UINT64_MAX) {
+        dev->chunk_budget = max_bytes;
+        xb_chunk_evict_locked(dev);
+    }
+    if (p_cached_bytes)
+        *p_cached_bytes = dev->chunk_bytes;
     return 0;
 }
 

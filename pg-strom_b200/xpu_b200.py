@@ -68,6 +68,10 @@ def lib():
         L.xpuB200ServeConfig.argtypes = [P, U64, ctypes.c_uint32, EB]
         L.xpuB200MemInfo.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]
         L.xpuB200FinalParts.argtypes = [P, ctypes.c_uint32, P, U64, ctypes.POINTER(U64), ctypes.POINTER(U64), EB]
+        L.xpuB200ChunkCachePut.argtypes = [P, U64, ctypes.c_uint32, P, I, ctypes.POINTER(P), EB]
+        L.xpuB200ChunkCacheGet.argtypes = [P, U64, ctypes.c_uint32, ctypes.POINTER(P)]
+        L.xpuB200ChunkCacheRelease.argtypes = [P, P]
+        L.xpuB200ChunkCacheConfig.argtypes = [P, U64, ctypes.POINTER(U64), EB]
         L.xpuB200MixCreate.argtypes = [P, ctypes.c_uint32, P, P, ctypes.POINTER(P), EB]
         L.xpuB200MixExec.argtypes = [P, P, P]
         L.xpuB200MixTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
@@ -166,6 +170,36 @@ class Device:
         if lib().xpuB200CopyToDevice(self.h, ctypes.c_void_p(base + shift), _ptr(arr), arr.nbytes):
             raise RuntimeError("upload failed")
         return base, base + shift
+
+    def chunk_put(self, table, chunk_no, kds, on_device=False):
+        """xpuB200ChunkCachePut: the device address of chunk chunk_no of
+        table (placed now, or found resident), pinned until chunk_release."""
+        p = ctypes.c_void_p()
+        e = KernErrorbuf()
+        src = ctypes.c_void_p(kds) if on_device else _ptr(kds)
+        rc = lib().xpuB200ChunkCachePut(self.h, table, chunk_no, src, 1 if on_device else 0,
+                                        ctypes.byref(p), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return p.value
+
+    def chunk_get(self, table, chunk_no):
+        """The device address of a resident chunk (pinned), or None."""
+        p = ctypes.c_void_p()
+        return p.value if lib().xpuB200ChunkCacheGet(self.h, table, chunk_no, ctypes.byref(p)) == 0 else None
+
+    def chunk_release(self, dptr):
+        return lib().xpuB200ChunkCacheRelease(self.h, ctypes.c_void_p(dptr)) == 0
+
+    def chunk_cache(self, max_bytes=None):
+        """Set the chunk cache's budget; returns the bytes held now."""
+        got = ctypes.c_uint64()
+        e = KernErrorbuf()
+        rc = lib().xpuB200ChunkCacheConfig(self.h, (1 << 64) - 1 if max_bytes is None else max_bytes,
+                                           ctypes.byref(got), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return got.value
 
     def mem_info(self):
         """(free, total, reserve) bytes of device memory (xpuB200MemInfo)."""
