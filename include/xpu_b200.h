@@ -356,6 +356,38 @@ int  xpuB200ChunkCacheRelease(xpuB200Device *dev, const kern_data_store *kds_dev
 int  xpuB200ChunkCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes,
                              kern_errorbuf *err);
 
+/*
+ * Storage → HBM chunk ingest (GPUDirect Storage).  Replaces the file read
+ * of the GPU service before a KDS_FORMAT_BLOCK / KDS_FORMAT_ARROW chunk is
+ * run (__gpuservLoadKdsCommon, src/gpu_service.c:3415-3466, calling
+ * gpuDirectFileReadIOV, src/extra.c:569-630, with the I/O vector of
+ * strom_io_chunk entries, src/heterodb_extra.h:37-43).  The first
+ * base_offset bytes of kds_head (the KDS header and block numbers) are
+ * copied to kds_dev; then, for each I/O chunk, nr_pages pages of
+ * XPU_B200_IO_PAGE bytes starting at file page fchunk_id are read from
+ * 'pathname' into kds_dev + base_offset + m_offset (the reference places
+ * kds_dev so that kds_dev + base_offset is page aligned, the alignment
+ * direct DMA wants; any 16-byte alignment is accepted here).  With
+ * try_direct, pages are read by
+ * cuFileRead (libcufile, bound at run time); the pages cuFile does not
+ * read, and all pages without try_direct or without a working cuFile
+ * driver, go through a pinned bounce buffer.  *p_npages_direct and
+ * *p_npages_vfs count the two (the reference's npages_direct_read /
+ * npages_vfs_read).  Synchronous; kds_dev is device memory of 'dev'.
+ */
+#define XPU_B200_IO_PAGE            4096
+typedef struct {
+    uint64_t    m_offset;       /* destination offset from kds_dev + base_offset */
+    uint32_t    fchunk_id;      /* first file page (of XPU_B200_IO_PAGE bytes) */
+    uint32_t    nr_pages;       /* pages to read */
+} xpuB200IoChunk;
+
+int  xpuB200ChunkReadDirect(xpuB200Device *dev, const char *pathname,
+                            const kern_data_store *kds_head, uint64_t base_offset,
+                            const xpuB200IoChunk *ioc, uint32_t nr_chunks,
+                            void *kds_dev, uint64_t kds_dev_sz, int try_direct,
+                            uint32_t *p_npages_direct, uint32_t *p_npages_vfs, kern_errorbuf *err);
+
 int  xpuB200InnerRebuild(xpuB200Device *dev, kern_data_store *kds_dst, const kern_data_store *kds_src,
                          uint32_t hash_divisor, uint32_t hash_remainder, uint64_t *p_required,
                          kern_errorbuf *err);

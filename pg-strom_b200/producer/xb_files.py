@@ -67,6 +67,44 @@ def heap_file_chunks(table_def: Table, path: str, pages_per_chunk=8190, first_bl
     return chunks
 
 
+IO_PAGE = 4096                  # XPU_B200_IO_PAGE: the file page of an I/O chunk
+
+
+def heap_file_iovec(table_def: Table, path: str, pages_per_chunk=8190, first_blkno=0, io_pages=None):
+    """For reading a relation segment file straight into device memory
+    (xpuB200ChunkReadDirect): per chunk, its KDS header with the block
+    numbers (base_offset bytes, the part sent from host memory), its
+    length, and its I/O vector of (m_offset, fchunk_id, nr_pages) entries
+    in IO_PAGE units, as relscan.c builds them (relscan.c:630-663: file
+    pages of consecutive blocks merged into one entry)."""
+    size = os.path.getsize(path)
+    if size % BLCKSZ:
+        raise ValueError(f"{path}: {size} bytes is not a whole number of {BLCKSZ}-byte pages")
+    nblocks = size // BLCKSZ
+    head = bytes(table_def.kds_header("b"))
+    head_len = len(head)
+    per_block = BLCKSZ // IO_PAGE
+    out = []
+    blk = 0
+    while blk < nblocks:
+        n = min(pages_per_chunk, nblocks - blk)
+        block_offset = head_len + maxalign(4 * pages_per_chunk)
+        length = block_offset + BLCKSZ * n
+        hdr = np.zeros(block_offset, dtype=np.uint8)
+        hdr[:head_len] = np.frombuffer(head, dtype=np.uint8)
+        struct.pack_into("<Q", hdr, 0, length)
+        struct.pack_into("<I", hdr, 16, n)
+        struct.pack_into("<II", hdr, 44, block_offset, 0)
+        hdr[head_len:head_len + 4 * n] = np.arange(first_blkno + blk, first_blkno + blk + n,
+                                                   dtype=np.uint32).view(np.uint8)
+        total = n * per_block
+        step = io_pages or total
+        iov = [(IO_PAGE * p, blk * per_block + p, min(step, total - p)) for p in range(0, total, step)]
+        out.append({"head": hdr, "base_offset": block_offset, "length": length, "iov": iov})
+        blk += n
+    return out
+
+
 # --------------------------------------------------------------- Arrow files
 def write_arrow_ipc(path: str, columns: dict, dictionary=(), batch_rows=1 << 20):
     """An Arrow IPC file of the columns (name -> numpy array, or list of

@@ -72,6 +72,8 @@ def lib():
         L.xpuB200ChunkCacheGet.argtypes = [P, U64, ctypes.c_uint32, ctypes.POINTER(P)]
         L.xpuB200ChunkCacheRelease.argtypes = [P, P]
         L.xpuB200ChunkCacheConfig.argtypes = [P, U64, ctypes.POINTER(U64), EB]
+        L.xpuB200ChunkReadDirect.argtypes = [P, ctypes.c_char_p, P, U64, P, ctypes.c_uint32, P, U64, I,
+                                             ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32), EB]
         L.xpuB200MixCreate.argtypes = [P, ctypes.c_uint32, P, P, ctypes.POINTER(P), EB]
         L.xpuB200MixExec.argtypes = [P, P, P]
         L.xpuB200MixTime.argtypes = [P, I, ctypes.POINTER(ctypes.c_double), EB]
@@ -200,6 +202,23 @@ class Device:
         if rc:
             raise XpuB200Error(rc, e)
         return got.value
+
+    def read_direct(self, path, kds_head, base_offset, io_chunks, dptr, dsize, try_direct=True):
+        """xpuB200ChunkReadDirect: the first base_offset bytes of kds_head,
+        then the file pages of io_chunks ((m_offset, fchunk_id, nr_pages)
+        of XPU_B200_IO_PAGE-byte pages) into device memory at dptr.
+        Returns (pages read by cuFile, pages read through the bounce
+        buffer)."""
+        ioc = np.array(list(io_chunks), dtype=[("m_offset", "<u8"), ("fchunk_id", "<u4"), ("nr_pages", "<u4")])
+        nd, nv = ctypes.c_uint32(), ctypes.c_uint32()
+        e = KernErrorbuf()
+        rc = lib().xpuB200ChunkReadDirect(self.h, os.fsencode(path), _ptr(kds_head), base_offset,
+                                          _ptr(ioc) if len(ioc) else None, len(ioc),
+                                          ctypes.c_void_p(dptr), dsize, 1 if try_direct else 0,
+                                          ctypes.byref(nd), ctypes.byref(nv), ctypes.byref(e))
+        if rc:
+            raise XpuB200Error(rc, e)
+        return nd.value, nv.value
 
     def mem_info(self):
         """(free, total, reserve) bytes of device memory (xpuB200MemInfo)."""

@@ -83,3 +83,27 @@ def test_arrow_ipc_dictionary_column(tmp_path):
     assert o.stats()["nitems_in"] == nin
     assert F.compare_groups(F.decode_kds_final(o.final(), sess), expect) == []
     o.close()
+
+
+def test_heap_file_iovec_matches_chunks(tmp_path):
+    """the header plus the file pages an I/O vector names, laid out at
+    base_offset + m_offset, are the chunk heap_file_chunks builds"""
+    tbl, sess, _, expect, meta = C.scan_groupby(nrows=30_000, seed_config=34)
+    path = str(tmp_path / "16386")
+    XF.write_heap_relation(tbl, path)
+    want = XF.heap_file_chunks(tbl, path, pages_per_chunk=100)
+    got = XF.heap_file_iovec(tbl, path, pages_per_chunk=100, io_pages=7)
+    assert len(got) == len(want)
+    raw = open(path, "rb").read()
+    for g, w in zip(got, want):
+        buf = np.zeros(g["length"], dtype=np.uint8)
+        buf[:g["base_offset"]] = g["head"]
+        npages = 0
+        for m_off, fchunk, nr in g["iov"]:
+            assert nr <= 7
+            dst = g["base_offset"] + m_off
+            buf[dst:dst + nr * XF.IO_PAGE] = np.frombuffer(
+                raw[fchunk * XF.IO_PAGE:(fchunk + nr) * XF.IO_PAGE], dtype=np.uint8)
+            npages += nr
+        assert npages * XF.IO_PAGE == g["length"] - g["base_offset"]
+        assert buf.tobytes() == w.tobytes()

@@ -77,3 +77,53 @@ def test_arrow_ipc_dictionary_column_on_the_device(device, kernel, tmp_path):
         s.close()
     assert n == nin
     assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
+
+
+@pytest.mark.parametrize("try_direct", [True, False])
+def test_heap_file_read_direct_into_device(device, tmp_path, try_direct):
+    """xpuB200ChunkReadDirect: each chunk's header from host memory and its
+    heap pages straight from the relation file into device memory (cuFile
+    where it reads, else the bounce buffer; every page counted once), then
+    the chunks run from the device: the same bytes as heap_file_chunks and
+    the same groups as the truth."""
+    import numpy as np
+    tbl, sess, _, expect, meta = C.scan_groupby(nrows=300_000, seed_config=35)
+    path = str(tmp_path / "16387")
+    XF.write_heap_relation(tbl, path)
+    want = XF.heap_file_chunks(tbl, path, pages_per_chunk=512)
+    plan = XF.heap_file_iovec(tbl, path, pages_per_chunk=512, io_pages=96)
+    truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
+    bases, ptrs = [], []
+    try:
+        for ch, w in zip(plan, want):
+            size = ch["length"] + XF.IO_PAGE
+            base = device.alloc(size)
+            bases.append(base)
+            # the header ends on a page boundary of device memory
+            gap = (-(base + ch["base_offset"])) % XF.IO_PAGE
+            dptr = base + gap
+            nd, nv = device.read_direct(path, ch["head"], ch["base_offset"], ch["iov"], dptr,
+                                        size - gap, try_direct=try_direct)
+            assert nd + nv == (ch["length"] - ch["base_offset"]) // XF.IO_PAGE
+            if not try_direct:
+                assert nd == 0
+            got = np.frombuffer(device.download(dptr, ch["length"]), dtype=np.uint8)
+            assert got.tobytes() == w.tobytes()
+            ptrs.append(dptr)
+        assert F.compare_groups(_run_cached(device, sess, ptrs), truth) == []
+    finally:
+        for b in bases:
+            device.free(b)
+
+
+def test_read_direct_rejects_a_chunk_past_the_buffer(device, tmp_path):
+    tbl, sess, _, expect, meta = C.scan_groupby(nrows=20_000, seed_config=36)
+    path = str(tmp_path / "16388")
+    XF.write_heap_relation(tbl, path)
+    ch = XF.heap_file_iovec(tbl, path, pages_per_chunk=64)[0]
+    base = device.alloc(ch["length"])
+    try:
+        with pytest.raises(xpu_b200.XpuB200Error, match="past the device buffer"):
+            device.read_direct(path, ch["head"], ch["base_offset"], ch["iov"], base, ch["length"] - 1)
+    finally:
+        device.free(base)
