@@ -2867,11 +2867,27 @@ xpuB200CloseSession(xpuB200Session *sess)
  * its specialised kernel is built: the kernel reads the depth-0 columns at
  * these offsets (and checks each launch's layout against them); session
  * lock held */
+static void xb_note_walk(xb_plan *p, const kern_data_store *h);
+static void xb_note_layout_plan(xb_plan *p, const kern_data_store *h);
+
 static void xb_note_layout(xpuB200Session *s, const kern_data_store *h)
 {
-    xb_plan *p = s->h_plan;
-    if (h->format != KDS_FORMAT_BLOCK || p->lay_valid || s->jit_tried[KDS_FORMAT_BLOCK])
+    if (s->jit_tried[KDS_FORMAT_BLOCK])
         return;
+    xb_note_layout_plan(s->h_plan, h);
+}
+
+/* the same on a translated plan, for the generator's tests */
+extern "C" void xb_plan_note_layout(xb_plan *p, const kern_data_store *h)
+{
+    xb_note_layout_plan(p, h);
+}
+
+static void xb_note_layout_plan(xb_plan *p, const kern_data_store *h)
+{
+    if (h->format != KDS_FORMAT_BLOCK || p->lay_valid || p->walk_ncols)
+        return;
+    xb_note_walk(p, h);
     uint32_t end = 0;
     for (uint32_t i = 0; i < p->nload0; i++) {
         const xb_load &l = p->load0[i];
@@ -2894,6 +2910,46 @@ static void xb_note_layout(xpuB200Session *s, const kern_data_store *h)
     }
     p->lay_end = end;
     p->lay_valid = p->nload0 > 0 ? 1 : 0;
+}
+
+/* the column descriptors up to the last depth-0 column, when every one of
+ * them is fixed-width (1..8 bytes) or a varlena and every fixed-width
+ * load is naturally aligned by its column's attalign: the specialised
+ * kernel then walks tuples with NULLs, or with varlena columns before a
+ * loaded column, in straight-line code (checked against each launch's
+ * columns) */
+static void xb_note_walk(xb_plan *p, const kern_data_store *h)
+{
+    p->walk_ncols = 0;
+    const int n = p->max_resno0;
+    if (p->nload0 == 0 || n < 1 || n > XB_MAX_COLS || n > (int)h->ncols || n > (int)h->nr_colmeta)
+        return;
+    for (int j = 0; j < n; j++) {
+        const kern_colmeta &cm = h->colmeta[j];
+        const int al = cm.attalign;
+        if (!(cm.attlen == -1 || (cm.attlen >= 1 && cm.attlen <= 8)) || !(al == 1 || al == 2 || al == 4 || al == 8))
+            return;
+        p->walk_len[j] = cm.attlen;
+        p->walk_align[j] = (int8_t)al;
+    }
+    for (uint32_t i = 0; i < p->nload0; i++) {
+        const xb_load &l = p->load0[i];
+        if (l.resno < 1 || l.resno > n)
+            return;
+        const int len = p->walk_len[l.resno - 1], al = p->walk_align[l.resno - 1];
+        int w = 0;
+        switch (l.ld) {
+        case XB_LD_BOOL: w = 1; break;
+        case XB_LD_INT2: w = 2; break;
+        case XB_LD_INT4: case XB_LD_DATE: case XB_LD_FLT4: w = 4; break;
+        case XB_LD_INT8: case XB_LD_FLT8: w = 8; break;
+        case XB_LD_TEXT: case XB_LD_NUMERIC: w = -1; break;
+        default: return;
+        }
+        if (len != w || (w > 0 && al < w))
+            return;
+    }
+    p->walk_ncols = (uint32_t)n;
 }
 
 /* units of one chunk (pages, or 1024-row groups) */
@@ -5463,6 +5519,13 @@ static void xb_sched_destroy(xpuB200Device *dev)
         xb_slot_free(q->slot[i]);
     delete q;
     dev->sched = nullptr;
+}
+
+/* the CUDA device index of a device handle, for the storage reader (xb_direct.cpp) */
+extern "C" int
+xb_device_index(const xpuB200Device *dev)
+{
+    return dev->dindex;
 }
 
 extern "C" int

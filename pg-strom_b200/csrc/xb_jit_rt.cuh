@@ -340,7 +340,7 @@ xbj_body(const XbExecArgs &args, char *smem)
             lp_next = lp_after;
             /* (the fast decode of a known layout reads the tuple with two
              * wide loads; there the L1 prefetch only costs issue slots) */
-            if (!lay_ok
+            if (!(lay_ok && XBJ_LAY_FIXED)
 #ifdef XBJ_STAGE
                 && !staged
 #endif

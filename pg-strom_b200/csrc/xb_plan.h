@@ -250,6 +250,12 @@ typedef struct xb_plan {
     uint32_t    lay_valid;
     uint32_t    lay_end;
     int32_t     lay_off[XB_MAX_LOADS];
+    /* the column descriptors of columns 1..walk_ncols (attlen 1..8 or -1,
+     * attalign), for a generated walk over tuples with NULLs or varlena
+     * columns before a loaded one; walk_ncols 0: none */
+    uint32_t    walk_ncols;
+    int16_t     walk_len[XB_MAX_COLS];
+    int8_t      walk_align[XB_MAX_COLS];
     xb_load     load0[XB_MAX_LOADS];
     xb_prog     scan_quals;
 

@@ -55,6 +55,37 @@ def test_specialised_kernel_compiles(case):
     assert nbytes.value > 0
 
 
+def _walk_plan(L):
+    """the plain scan session's plan with the heap layout of its table
+    noted (numeric c before the group key g: no fixed offsets, a walk)"""
+    tbl, sess, _, _, _ = C.scan_groupby(nrows=1000)
+    plan = _translate(L, sess, None)
+    head = bytes(tbl.kds_header("b"))
+    L.xb_plan_note_layout(plan, head)
+    return plan
+
+
+def test_walk_kernel_compiles():
+    L = _lib()
+    plan = _walk_plan(L)
+    n = ctypes.c_size_t(0)
+    buf = ctypes.create_string_buffer(1 << 21)
+    assert L.xb_jit_source(plan, ctypes.c_uint32(ord("b")), buf, ctypes.c_size_t(len(buf)), ctypes.byref(n)) == 0
+    src = buf.value.decode()
+    # columns 1..5 walked; the numeric column's varlena header read, nullmap tested
+    assert "xbj_walk(" in src and "/* column 4: attlen -1, attalign 4 */" in src
+    assert "(nullmap[0] >> 2) & 1" in src and "#define XBJ_LAY_FIXED 0" in src
+    nbytes = ctypes.c_uint64(0)
+    ms = ctypes.c_double(0.0)
+    err = ctypes.create_string_buffer(2048)
+    rc = L.xb_jit_check(plan, ctypes.c_uint32(ord("b")), ctypes.byref(nbytes), ctypes.byref(ms), err,
+                        ctypes.c_size_t(len(err)))
+    msg = err.value.decode()
+    if rc != 0 and "libnvrtc" in msg:
+        pytest.skip(msg)
+    assert rc == 0, msg
+
+
 def test_generated_source_names_the_plan():
     L = _lib()
     _, sess, km, _, _ = C.join_groupby(nfact=1000, ndim1=100, ndim2=10)
