@@ -368,8 +368,10 @@ int  xpuB200ChunkCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p
  * 'pathname' into kds_dev + base_offset + m_offset (the reference places
  * kds_dev so that kds_dev + base_offset is page aligned, the alignment
  * direct DMA wants; any 16-byte alignment is accepted here).  With
- * try_direct, pages are read by
- * cuFileRead (libcufile, bound at run time); the pages cuFile does not
+ * try_direct, and with XPU_B200_CUFILE=1 in the environment (on hosts
+ * without the nvidia-fs driver a cuFile read was seen never to return, so
+ * the library does not enter libcufile unless the host says it may), pages
+ * are read by cuFileRead (libcufile, bound at run time); the pages cuFile does not
  * read, and all pages without try_direct or without a working cuFile
  * driver, go through a pinned bounce buffer.  *p_npages_direct and
  * *p_npages_vfs count the two (the reference's npages_direct_read /

@@ -17,6 +17,7 @@
 #include <fcntl.h>
 #include <unistd.h>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -49,6 +50,13 @@ void cufile_bind_locked()
     if (g_cf.tried)
         return;
     g_cf.tried = true;
+    /* libcufile is entered only where the host asks for it: on hosts without
+     * the nvidia-fs driver a cuFile read was seen not to return at all */
+    const char *on = getenv("XPU_B200_CUFILE");
+    if (!on || strcmp(on, "1") != 0) {
+        g_cf.why = "cuFile is not enabled (XPU_B200_CUFILE=1)";
+        return;
+    }
     void *h = nullptr;
     for (const char *l : {"libcufile.so.0", "libcufile.so", "/usr/local/cuda/lib64/libcufile.so.0"})
         if ((h = dlopen(l, RTLD_NOW | RTLD_LOCAL)) != nullptr)

@@ -4,6 +4,8 @@ serve two sessions (the second without any upload), pinned chunks survive
 eviction and unpinned ones go least recently used first; an Arrow IPC
 file with a dictionary-encoded text column is grouped by that column on
 both kernels, equal to the oracle and the arrays."""
+import os
+
 import pytest
 
 import xb_configs as C
@@ -82,10 +84,12 @@ def test_arrow_ipc_dictionary_column_on_the_device(device, kernel, tmp_path):
 @pytest.mark.parametrize("try_direct", [True, False])
 def test_heap_file_read_direct_into_device(device, tmp_path, try_direct):
     """xpuB200ChunkReadDirect: each chunk's header from host memory and its
-    heap pages straight from the relation file into device memory (cuFile
-    where it reads, else the bounce buffer; every page counted once), then
-    the chunks run from the device: the same bytes as heap_file_chunks and
-    the same groups as the truth."""
+    heap pages from the relation file into device memory, then the chunks
+    run from the device: the same bytes as heap_file_chunks and the same
+    groups as the truth.  try_direct without XPU_B200_CUFILE=1 leaves
+    libcufile alone and reads every page through the bounce buffer (every
+    page counted once)."""
+    assert os.environ.get("XPU_B200_CUFILE") != "1"
     import numpy as np
     tbl, sess, _, expect, meta = C.scan_groupby(nrows=300_000, seed_config=35)
     path = str(tmp_path / "16387")
@@ -105,8 +109,7 @@ def test_heap_file_read_direct_into_device(device, tmp_path, try_direct):
             nd, nv = device.read_direct(path, ch["head"], ch["base_offset"], ch["iov"], dptr,
                                         size - gap, try_direct=try_direct)
             assert nd + nv == (ch["length"] - ch["base_offset"]) // XF.IO_PAGE
-            if not try_direct:
-                assert nd == 0
+            assert nd == 0
             got = np.frombuffer(device.download(dptr, ch["length"]), dtype=np.uint8)
             assert got.tobytes() == w.tobytes()
             ptrs.append(dptr)
