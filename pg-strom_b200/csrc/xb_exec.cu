@@ -3020,6 +3020,7 @@ static bool xb_tune_lookup(xpuB200Session *s, uint32_t format, xb_tune_choice *c
  * request of a new plan shape does not wait seconds for NVRTC.
  */
 static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, double ms, const char *msg);
+static size_t xb_replay_smem(const xb_plan *plan);
 
 static void *xb_session_jit(xpuB200Session *s, uint32_t format, bool wait = true)
 {
@@ -3096,7 +3097,8 @@ static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, dou
                 s->jit_mixfn[format] = nullptr;
             s->jit_grid[format] = per_sm * s->dev->nsm;
             int rp = 0;
-            if (s->jit_replay[format] && xb_jit_prepare(s->jit_replay[format], XB_BLOCK, 0, &rp) != 0)
+            if (s->jit_replay[format] &&
+                xb_jit_prepare(s->jit_replay[format], XB_BLOCK, xb_replay_smem(s->h_plan), &rp) != 0)
                 s->jit_replay[format] = nullptr;
             s->jit_replay_grid[format] = rp * s->dev->nsm;
             s->jit_compile_ms += ms;
@@ -3113,9 +3115,10 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
 
 /* partitioned aggregation for this launch: a keyed GROUP BY whose groups
  * live in a global table larger than L2 defers each row's update into the
- * bucket of its table slot; the buckets cover slices of the table small
- * enough to stay in L2 while the replay works on them.  Rows past a full
- * bucket are updated in place, so any bucket size is correct.  Used by
+ * bucket of its table slot; a bucket covers the slots of one replay CTA's
+ * shared table, so the replay combines a bucket's rows in shared memory
+ * and merges each of its groups into the global table once.  Rows past a
+ * full bucket are updated in place, so any bucket size is correct.  Used by
  * prepared batches whose table is several times L2 (the records of a batch
  * take device memory in proportion to its rows, which the serving path's
  * admission does not budget); XPU_B200_PARTITION=1 uses it for every
@@ -3124,6 +3127,56 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
  * that rows past full buckets are updated in place while others of the
  * same groups are deferred.  Session lock held.  Returns whether it is
  * used. */
+/* table slots of one bucket of partitioned aggregation (xb_replay_slots).
+ * XPU_B200_REPLAY_KB=n gives each replay CTA a shared
+ * group table of n KB that covers its bucket's slots (the bucket's rows
+ * are combined there and each group merged into the global table once);
+ * the default, 0, updates the global table row by row, which measured
+ * faster at 2 and at 10 rows per group (the shared table's inserts and
+ * merges cost two group creations per group). */
+static uint32_t xb_replay_kb()
+{
+    static const int kb = [] {
+        const char *e = getenv("XPU_B200_REPLAY_KB");
+        const int v = e ? atoi(e) : -1;
+        return (v >= 0 && v <= 200) ? v : 0;
+    }();
+    return (uint32_t)kb;
+}
+
+static uint32_t xb_replay_slots(const xb_plan *plan)
+{
+    /* XPU_B200_PART_SLOTS=n (a power of two, 64..65536): n slots per bucket
+     * when the replay has no shared table */
+    static const uint32_t forced = [] {
+        const char *e = getenv("XPU_B200_PART_SLOTS");
+        const unsigned long v = e ? strtoul(e, nullptr, 10) : 0;
+        return (v >= 64 && v <= 65536 && (v & (v - 1)) == 0) ? (uint32_t)v : 0u;
+    }();
+    if (forced && !xb_replay_kb())
+        return forced;
+    /* with a shared table: the slots whose entries fit it; without: about
+     * 128 KB of global table per bucket (1024 of the Arrow group-by's
+     * 112-byte entries; measured against 512, 2048 and 4096 slots) */
+    const uint32_t stride = xb_replay_kb() ? xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16)
+                                           : (plan->gent_size ? plan->gent_size : 16);
+    const uint64_t target = (uint64_t)(xb_replay_kb() ? xb_replay_kb() : 128) << 10;
+    uint32_t c = 8192;
+    while (c > 64 && (uint64_t)c * stride > target)
+        c >>= 1;
+    return c;
+}
+
+static uint32_t xb_replay_sm_cap(const xb_plan *plan)
+{
+    return xb_replay_kb() ? xb_replay_slots(plan) : 0;
+}
+
+static size_t xb_replay_smem(const xb_plan *plan)
+{
+    return (size_t)xb_replay_sm_cap(plan) * xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16);
+}
+
 static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format, cudaStream_t stream)
 {
     const char *env = getenv("XPU_B200_PARTITION");
@@ -3143,23 +3196,23 @@ static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format,
     const uint64_t table = cap * plan->gent_size;
     if (rec == 0 || table <= (force ? (64ULL << 20) : (512ULL << 20)))
         return false;
-    /* buckets of about 16 MB of table, at most 4096 */
-    uint64_t np = 8;
-    while (np < 4096 && table / np > (16ULL << 20) && np * 2 <= cap)
-        np *= 2;
+    /* one bucket per slice of the table that a replay CTA's shared table
+     * covers: at the table's load its groups fit in shared memory */
+    uint64_t np = cap / xb_replay_slots(plan);
+    while (np > XB_PART_MAX)
+        np >>= 1;
+    if (np < 8 || np * 2 > cap)
+        return false;
     uint32_t lg_cap = 0, lg_np = 0;
     while ((1ULL << lg_cap) < cap) lg_cap++;
     while ((1ULL << lg_np) < np) lg_np++;
     const uint64_t rows = format == KDS_FORMAT_BLOCK ? nunits * 291ULL : nunits * (uint64_t)XB_ROWS_UNIT;
-    uint64_t per = (rows + rows / 4) / np + 1024;
+    uint64_t per = (rows + rows / 4) / np + 256;
     /* at most a quarter of the device budget for the records */
     const uint64_t limit = s->dev->hbm_budget / 4;
     if (per * np * rec > limit)
         per = limit / (np * rec);
-    /* the replay numbers records in 32 bits */
-    if (per * np > (1ULL << 31))
-        per = (1ULL << 31) / np;
-    if (per < 1024 || per > 0xffffffffULL)
+    if (per < 256 || per > 0xffffffffULL)
         return false;
     const char *cap_env = getenv("XPU_B200_PART_CAP");
     const uint64_t cap_force = cap_env ? strtoull(cap_env, nullptr, 10) : 0;
@@ -3171,7 +3224,9 @@ static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format,
         s->part_cnt = nullptr;
         s->part_bytes = 0;
         if (cudaMallocAsync((void **)&s->part_buf, bytes, stream) != cudaSuccess ||
-            cudaMallocAsync((void **)&s->part_cnt, sizeof(uint32_t) * XB_PART_CNT_STRIDE * np, stream) != cudaSuccess) {
+            /* the bucket counters, then the replay's bucket cursor */
+            cudaMallocAsync((void **)&s->part_cnt, sizeof(uint32_t) * XB_PART_CNT_STRIDE * (np + 1), stream) !=
+                cudaSuccess) {
             cudaGetLastError();
             if (s->part_buf) cudaFreeAsync(s->part_buf, stream);
             s->part_buf = nullptr;
@@ -3438,7 +3493,7 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
         a.part_cnt = s->part_cnt;
         a.part_cap = s->part_cap;
         a.part_shift = s->part_shift;
-        cudaMemsetAsync(s->part_cnt, 0, sizeof(uint32_t) * XB_PART_CNT_STRIDE * s->nparts, stream);
+        cudaMemsetAsync(s->part_cnt, 0, sizeof(uint32_t) * XB_PART_CNT_STRIDE * (s->nparts + 1), stream);
         s->part_used = true;
     }
     if (fn) {
@@ -3454,7 +3509,10 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
             ra.part_cnt = s->part_cnt;
             ra.part_cap = s->part_cap;
             ra.nparts = s->nparts;
-            if (xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK, 0, (void *)stream, &ra) != 0)
+            ra.cursor = s->part_cnt + (size_t)s->nparts * XB_PART_CNT_STRIDE;
+            ra.sm_cap = xb_replay_sm_cap(s->h_plan);
+            if (xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK,
+                              xb_replay_smem(s->h_plan), (void *)stream, &ra) != 0)
                 return XB_ERR(err, ERRCODE_DEVICE_FATAL, "replay kernel launch failed");
         }
     } else {
@@ -3578,6 +3636,8 @@ static void xb_account(xpuB200Session *s, kern_exec_results *results)
 static int xb_replay_retry(xpuB200Session *s, uint32_t format, kern_errorbuf *err)
 {
     XB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), s->stream), err);
+    uint32_t *cursor = s->part_cnt + (size_t)s->nparts * XB_PART_CNT_STRIDE;
+    XB_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), s->stream), err);
     XbReplayArgs ra;
     memset(&ra, 0, sizeof(ra));
     ra.plan = s->d_plan;
@@ -3585,8 +3645,10 @@ static int xb_replay_retry(xpuB200Session *s, uint32_t format, kern_errorbuf *er
     ra.st = s->d_status;
     ra.part_buf = s->part_buf;
     ra.part_cnt = s->part_cnt;
+    ra.cursor = cursor;
     ra.part_cap = s->part_cap;
     ra.nparts = s->nparts;
+    ra.sm_cap = 0;              /* the left records, row by row into the grown table */
     ra.retry = 1;
     if (!s->jit_replay[format] ||
         xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK, 0, (void *)s->stream, &ra) != 0)

@@ -634,7 +634,7 @@ struct XbExecArgs {
  * every aggregated row claims its slot with an atomic on its bucket's
  * counter, and counters sharing a line would serialise in one L2 slice */
 #define XB_PART_CNT_STRIDE  32
-#define XB_PART_MAX         4096    /* buckets of one partitioned launch */
+#define XB_PART_MAX         (1u << 18)  /* buckets of one partitioned launch */
 
 /* the replay launch of partitioned aggregation (xbj_replay) */
 struct XbReplayArgs {
@@ -643,10 +643,12 @@ struct XbReplayArgs {
     xb_status      *st;
     char           *part_buf;       /* records (a full table marks the ones it left) */
     const uint32_t *part_cnt;
+    uint32_t       *cursor;         /* next bucket to claim (zero at launch) */
     uint32_t        part_cap;
     uint32_t        nparts;
+    uint32_t        sm_cap;         /* shared group-table entries of a CTA, one bucket's
+                                     * slots (0: rows straight into the global table) */
     uint32_t        retry;          /* replay only the records marked left */
-    uint32_t        __pad;
 };
 
 /* largest existence bitmap of a direct depth (keys), 16 KB */
@@ -857,6 +859,110 @@ xb_src_start(const XbExecArgs &args, XbSrc &s, uint32_t lane)
     xb_prefetch_page(args, s, __shfl_sync(XB_FULL, s.nx_l0, 0), lane);
 }
 
+/* an Arrow column of the depth-0 loads, resolved once per 1024-row unit
+ * for the specialised kernel's fixed-width loads: the unit's first value,
+ * the chunk's NULL bitmap (nullptr: none) and how many of the unit's rows
+ * have a value inside the buffers (the rest read as NULL, as in
+ * xb_arrow_load); ok = 0 sends the column through xb_arrow_load (virtual
+ * columns, variable-width and mismatched types) */
+struct XbArrowCol {
+    const uint8_t *values;
+    const uint8_t *nullmap;
+    uint32_t nvalid;
+    uint32_t ok;
+    uint32_t width;                 /* bytes per value (ok columns) */
+    uint32_t __pad;
+};
+
+/* byte width of the values of an Arrow column read by loader ld when the
+ * column's type is the plain fixed-width one the loader expects, else 0 */
+__device__ __forceinline__ uint32_t
+xb_arrow_fixed_width(const kern_colmeta *cm, int ld)
+{
+    const int tag = cm->attopts.tag;
+    switch (ld) {
+    case XB_LD_INT2: case XB_LD_INT4: case XB_LD_INT8: {
+        const uint32_t w = ld == XB_LD_INT2 ? 2 : ld == XB_LD_INT4 ? 4 : 8;
+        return (tag == ArrowType__Int && cm->attopts.u.integer.bitWidth == w * 8) ? w : 0;
+    }
+    case XB_LD_FLT8:
+        return (tag == ArrowType__FloatingPoint &&
+                cm->attopts.u.floating_point.precision == ArrowPrecision__Double) ? 8 : 0;
+    case XB_LD_DATE:
+        return (tag == ArrowType__Date && cm->attopts.u.date.unit == ArrowDateUnit__Day) ? 4 : 0;
+    default:
+        return 0;
+    }
+}
+
+/* lane i resolves depth-0 load i for the unit of rows [row0, row0+nitems) */
+__device__ __forceinline__ void
+xb_arrow_resolve(const xb_plan *gp, const kern_data_store *kds, uint32_t row0, uint32_t nitems,
+                 XbArrowCol *acol, uint32_t lane)
+{
+    for (uint32_t i = lane; i < gp->nload0; i += 32) {
+        const xb_load &l = gp->load0[i];
+        XbArrowCol c;
+        c.values = nullptr;
+        c.nullmap = nullptr;
+        c.nvalid = 0;
+        c.ok = 0;
+        c.width = 0;
+        c.__pad = 0;
+        if (l.resno < 1 || l.resno > (int)kds->ncols) {
+            c.ok = 1;                   /* no such column: every row NULL */
+        } else {
+            const kern_colmeta *cm = &kds->colmeta[l.resno - 1];
+            const uint32_t w = xb_arrow_fixed_width(cm, l.ld);
+            if (cm->virtual_offset == 0 && w > 0) {
+                uint64_t nv = cm->values_length / w;
+                nv = nv > row0 ? nv - row0 : 0;
+                if (cm->nullmap_offset) {
+                    uint64_t nb = (uint64_t)cm->nullmap_length * 8;
+                    nb = nb > row0 ? nb - row0 : 0;
+                    nv = nv < nb ? nv : nb;
+                    c.nullmap = (const uint8_t *)kds + cm->nullmap_offset;
+                }
+                c.nvalid = (uint32_t)(nv < nitems ? nv : nitems);
+                c.values = (const uint8_t *)kds + cm->values_offset + (uint64_t)row0 * w;
+                c.ok = 1;
+                c.width = w;
+            }
+        }
+        acol[i] = c;
+    }
+}
+
+/* lane i: the first XB_ARROW_PF_ROWS rows of an Arrow unit in the column
+ * of depth-0 load i, pulled into L2 by the TMA engine (bulk prefetch)
+ * when the warp claims the unit (the interpreting kernel; the specialised
+ * kernel prefetches a window ahead of every batch instead).  A whole unit
+ * per warp would be too much: a launch's warps together would ask for
+ * about all of L2, and lines were evicted before their rows were read.
+ * Only whole 16-byte pieces inside each column's buffer are prefetched. */
+#define XB_ARROW_PF_ROWS    256
+__device__ __forceinline__ void
+xb_prefetch_arrow_unit(const XbExecArgs &args, const XbSrc &s, uint32_t lane)
+{
+    const xb_plan *gp = args.plan;
+    for (uint32_t i = lane; i < gp->nload0; i += 32) {
+        const xb_load &l = gp->load0[i];
+        const int w = xb_ld_width(l.ld);
+        if (w == 0 || l.ld == XB_LD_BOOL || l.resno < 1 || l.resno > (int)s.kds->ncols)
+            continue;
+        const kern_colmeta *cm = &s.kds->colmeta[l.resno - 1];
+        if (cm->virtual_offset != 0 || cm->values_offset == 0)
+            continue;
+        const uint32_t nr = s.nitems < XB_ARROW_PF_ROWS ? s.nitems : XB_ARROW_PF_ROWS;
+        const uint64_t lo = (uint64_t)s.row0 * w, hi = lo + (uint64_t)nr * w;
+        const uint64_t end = hi < cm->values_length ? hi : cm->values_length;
+        const uintptr_t a = ((uintptr_t)s.kds + cm->values_offset + lo + 15) & ~(uintptr_t)15;
+        const uintptr_t b = ((uintptr_t)s.kds + cm->values_offset + end) & ~(uintptr_t)15;
+        if (b > a)
+            xb_prefetch_l2((const void *)a, (uint32_t)(b - a));
+    }
+}
+
 /* the unit this warp takes after its current one (heap pages), or
  * args.nunits when its claims are exhausted */
 __device__ __forceinline__ uint64_t xb_following_unit(const XbSrc &s)
@@ -930,6 +1036,8 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
     const uint32_t left = s.kds->nitems > s.row0 ? s.kds->nitems - s.row0 : 0;
     s.nitems = left < XB_ROWS_UNIT ? left : XB_ROWS_UNIT;
     s.item = it;
+    if (pf_next && args.format == KDS_FORMAT_ARROW)
+        xb_prefetch_arrow_unit(args, s, lane);
     return 1;
 }
 

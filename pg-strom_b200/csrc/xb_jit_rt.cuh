@@ -22,6 +22,10 @@
 #ifndef XB_JIT_RT_CUH
 #define XB_JIT_RT_CUH
 
+#ifndef XBJ_ARROW_AHEAD
+#define XBJ_ARROW_AHEAD 4       /* 32-row batches an Arrow column's lines are prefetched ahead */
+#endif
+
 #ifndef XBJ_PF_LEAD
 #define XBJ_PF_LEAD     32      /* rows of a page left when the next page is prefetched (0: none) */
 #endif
@@ -68,11 +72,12 @@ __device__ __forceinline__ void xbj_flush_cnt(XbjCnt &C, xb_status *st)
 
 /* generated per session: decode item idx of the current unit (page: heap
  * page of a BLOCK chunk; kds / row0: chunk and first row of an ARROW or ROW
- * unit; lp: the heap item's line pointer) */
+ * unit; lp: the heap item's line pointer; acol: an ARROW unit's resolved
+ * columns) */
 __device__ __forceinline__ bool
 xbj_decode(XbjRegs &R, const XbExecArgs &args, const uint8_t *page, const kern_data_store *kds,
            uint32_t row0, const XbSrcMeta *meta, uint32_t idx, uint32_t lp, bool lay_ok, bool &exists,
-           xb_status *st);
+           xb_status *st, const XbArrowCol *acol);
 
 #ifdef XBJ_BITS
 /* generated: copy the filter depths' existence bitmaps into shared memory
@@ -119,6 +124,10 @@ xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
  * (returns true when, replaying, the table had no room for the group) */
 __device__ __forceinline__ void xbj_rec_load(const char *rec, XbjRegs &R, uint32_t &ghash);
 __device__ __forceinline__ bool xbj_group_row(XbjRegs &R, const XbjEnv &E, const uint32_t ghash, bool &failed);
+/* generated: find or create the group of R's keys in a table */
+template <bool SMEM>
+__device__ __forceinline__ char *
+xbj_group_get(const XbjRegs &R, const XbjEnv &E, char *entries, uint64_t cap_mask, uint32_t hash, bool *full);
 #endif
 
 #ifdef XBJ_MERGE_SM
@@ -258,6 +267,13 @@ xbj_body(const XbExecArgs &args, char *smem)
         C.depth[d] = 0;
 
     XbSrc &src = wsrc[threadIdx.x >> 5];
+#ifdef XBJ_ACOLS
+    /* the warp's Arrow columns, resolved for its current unit */
+    __shared__ XbArrowCol acol_all[XB_WARPS][XBJ_ACOLS];
+    XbArrowCol *acol = acol_all[threadIdx.x >> 5];
+#else
+    XbArrowCol *acol = nullptr;
+#endif
 #ifdef XBJ_STAGE
     /* this warp's page buffer and its mbarrier, after the group table */
     char *stage_base = (char *)(((uintptr_t)((char *)sbits + sbits_bytes) + 127) & ~(uintptr_t)127);
@@ -282,7 +298,7 @@ xbj_body(const XbExecArgs &args, char *smem)
     for (;;) {
         bool done = false;
         while (item >= nitems) {
-            const int rc = xb_next_unit(args, src, lane, args.format != KDS_FORMAT_BLOCK);
+            const int rc = xb_next_unit(args, src, lane, args.format == KDS_FORMAT_ROW);
             if (rc == 0) { done = true; break; }
             if (rc == 2) {
                 if (lane == 0) XB_RAISE(args.st, ERRCODE_DEVICE_ERROR, XB_MSG_BAD_PAGE);
@@ -318,6 +334,11 @@ xbj_body(const XbExecArgs &args, char *smem)
                 lp_next = xbj_itemid(page, nitems, item + lane);
                 lp_after = xbj_itemid(page, nitems, item + lane + 32);
             }
+#ifdef XBJ_ACOLS
+            __syncwarp();           /* every lane is done with the last unit's columns */
+            xb_arrow_resolve(args.plan, kds, row0, nitems, acol, lane);
+            __syncwarp();
+#endif
         }
         if (done)
             break;
@@ -328,6 +349,18 @@ xbj_body(const XbExecArgs &args, char *smem)
             xbj_grow_fetch(src.grow_buf, args.gt);
         const uint32_t idx = item + lane;
         uint32_t lp = 0;
+#ifdef XBJ_ACOLS
+        /* the columns' lines XBJ_ARROW_AHEAD batches ahead into L2: lane t
+         * takes line t % 2 of column t / 2 (32 values of at most 8 bytes) */
+        if (lane < 2 * XBJ_ACOLS) {
+            const XbArrowCol &c_ = acol[lane >> 1];
+            const uint32_t r_ = item + 32 * XBJ_ARROW_AHEAD;
+            /* the first row of the line: a row of the batch, inside the buffer */
+            const uint32_t rr_ = c_.width ? r_ + (lane & 1) * (128 / c_.width) : 0;
+            if (c_.ok && c_.width && rr_ < r_ + 32 && rr_ < c_.nvalid)
+                asm volatile("prefetch.global.L2 [%0];" :: "l"(c_.values + (size_t)rr_ * c_.width));
+        }
+#endif
         /* the warp's next heap page streams into L2 while the last
          * XBJ_PF_LEAD rows of this one are processed: early enough to
          * arrive, late enough not to be evicted by the pages streaming
@@ -353,7 +386,7 @@ xbj_body(const XbExecArgs &args, char *smem)
         if (idx < nitems) {
             XbjRegs R;
             bool exists = false;
-            const bool ok = xbj_decode(R, args, page, kds, row0, meta, idx, lp, lay_ok, exists, args.st);
+            const bool ok = xbj_decode(R, args, page, kds, row0, meta, idx, lp, lay_ok, exists, args.st, acol);
             if (exists)
                 C.raw++;
             if (exists && !ok)
@@ -453,21 +486,35 @@ xbj_mixed_kernel(const __grid_constant__ XbMixArgs m)
 }
 
 #ifdef XBJ_PART
-/* replay of the deferred rows, bucket after bucket: the grid sweeps the
- * bucket-major record array in order, so the CTAs work on neighbouring
- * buckets together and the slice of the group table they update (the
- * buckets are ranges of table slots) stays in L2 */
+/* a replay's shared entry that the global table (and the dump) had no room
+ * for: its rows are left for after the table grows */
+#define XBJ_SM_LEFT     3u
+
+/* replay of the deferred rows.  A bucket holds the rows whose groups have
+ * their home slot in one slice of the global table (sm_cap slots), so it
+ * holds no more groups than the CTA's shared table has room for at the
+ * global table's load.  Each CTA claims buckets in order: it combines the
+ * bucket's rows in its shared table (the specialised kernel's shared state
+ * form), then merges every group of the bucket into the global table once
+ * -- one probe and one state merge per group instead of one per row.
+ * Groups past a full shared table are updated in the global table
+ * directly.  A group that the global table and its dump have no room for
+ * (the table asked to grow meanwhile) is left: the re-sweep marks its rows
+ * for the retry replay after the growth, which updates the global table
+ * row by row (sm_cap 0). */
 extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
 xbj_replay(const __grid_constant__ XbReplayArgs args)
 {
+    extern __shared__ __align__(16) char sm_entries[];
+    __shared__ uint32_t cur[2];         /* the CTA's bucket; whether its merge left groups */
     XbjEnv E;
     E.plan = args.plan;
     E.st = args.st;
     E.gt = args.gt;
     E.gt_entries = args.gt->entries;
     E.gt_mask = args.gt->cap_mask;
-    E.sm_tab = nullptr;
-    E.sm_mask = 0;
+    E.sm_tab = args.sm_cap ? sm_entries : nullptr;
+    E.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
     E.lane = threadIdx.x & 31;
     E.dst = nullptr;
     E.dst_len = 0;
@@ -477,67 +524,86 @@ xbj_replay(const __grid_constant__ XbReplayArgs args)
     E.part_cap = 0;
     E.part_shift = 0;
     E.replay = 1;
-    /* the records of every bucket, numbered in bucket order: pre[b] is the
-     * number of records before bucket b (bucket counts clipped to the
-     * bucket size; counts past it were updated in place) */
-    __shared__ uint32_t pre[XB_PART_MAX + 1];
-    __shared__ uint32_t wsum[XB_WARPS];
-    const uint32_t np = args.nparts;
-    const uint32_t per_t = (np + blockDim.x - 1) / blockDim.x;
-    const uint32_t b0 = threadIdx.x * per_t;
-    uint32_t mine = 0;
-    for (uint32_t b = b0; b < b0 + per_t && b < np; b++) {
-        const uint32_t n = args.part_cnt[b * XB_PART_CNT_STRIDE];
-        mine += n < args.part_cap ? n : args.part_cap;
-    }
-    /* exclusive scan of the per-thread sums over the CTA */
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = mine;
-#pragma unroll
-    for (uint32_t o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(XB_FULL, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31)
-        wsum[warp] = incl;
-    __syncthreads();
-    uint32_t before = 0;
-    for (uint32_t w = 0; w < warp; w++)
-        before += wsum[w];
-    uint32_t run = before + incl - mine;
-    for (uint32_t b = b0; b < b0 + per_t && b < np; b++) {
-        pre[b] = run;
-        const uint32_t n = args.part_cnt[b * XB_PART_CNT_STRIDE];
-        run += n < args.part_cap ? n : args.part_cap;
-    }
-    if (threadIdx.x == blockDim.x - 1)
-        pre[np] = before + incl;
-    __syncthreads();
-    const uint32_t total = pre[np];
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
-        /* the bucket of record v: the last b with pre[b] <= v */
-        uint32_t lo = 0, hi = np - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (pre[mid] <= v) lo = mid; else hi = mid - 1;
+    const uint32_t sm_vec = (uint32_t)(((uint64_t)args.sm_cap * XBJ_SM_STRIDE) / 16);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            cur[0] = atomicAdd(args.cursor, 1u);
+            cur[1] = 0;
         }
-        const uint64_t i = (uint64_t)lo * args.part_cap + (v - pre[lo]);
-        char *rec = args.part_buf + i * XBJ_REC_SIZE;
-        /* a retry replays only the records a full table left behind */
-        if (args.retry && !(((const uint32_t *)rec)[1] & XBJ_REC_LEFT))
-            continue;
-        XbjRegs R;
-        uint32_t ghash;
-        xbj_rec_load(rec, R, ghash);
-        bool failed = false;
-        const bool table_full = xbj_group_row(R, E, ghash, failed);
-        if (table_full) {
-            ((uint32_t *)rec)[1] |= XBJ_REC_LEFT;
-            if (!args.st->replay_left)
-                atomicExch(&args.st->replay_left, 1u);
-        } else if (args.retry) {
-            ((uint32_t *)rec)[1] &= ~XBJ_REC_LEFT;
+        for (uint32_t i = threadIdx.x; i < sm_vec; i += blockDim.x)
+            ((uint4 *)sm_entries)[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        const uint32_t b = cur[0];
+        if (b >= args.nparts)
+            break;
+        const uint32_t cnt = args.part_cnt[(size_t)b * XB_PART_CNT_STRIDE];
+        const uint32_t n = cnt < args.part_cap ? cnt : args.part_cap;
+        char *base = args.part_buf + (uint64_t)b * args.part_cap * XBJ_REC_SIZE;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            char *rec = base + (uint64_t)i * XBJ_REC_SIZE;
+            /* a retry replays only the records a full table left behind */
+            if (args.retry && !(((const uint32_t *)rec)[1] & XBJ_REC_LEFT))
+                continue;
+            XbjRegs R;
+            uint32_t ghash;
+            xbj_rec_load(rec, R, ghash);
+            bool failed = false;
+            const bool table_full = xbj_group_row(R, E, ghash, failed);
+            if (table_full) {
+                ((uint32_t *)rec)[1] |= XBJ_REC_LEFT;
+                if (!args.st->replay_left)
+                    atomicExch(&args.st->replay_left, 1u);
+            } else if (args.retry) {
+                ((uint32_t *)rec)[1] &= ~XBJ_REC_LEFT;
+            }
         }
+        __syncthreads();
+        if (E.sm_tab) {
+            /* every group of the bucket into the global table, once */
+            for (uint32_t i = threadIdx.x; i < args.sm_cap; i += blockDim.x) {
+                char *e = sm_entries + (size_t)i * XBJ_SM_STRIDE;
+                xb_gent_head *h = (xb_gent_head *)e;
+                if (h->state != XB_GSTATE_READY)
+                    continue;
+                const xb_keyimg *img = (const xb_keyimg *)(e + XBJ_KEYS_OFF);
+                bool full = false;
+                char *g = xb_group_find(E.plan, E.gt_entries, E.gt_mask, h->hash, img, E.gt, E.st, &full);
+                if (!g && full) {
+                    char *slot = xb_dump_slot(E.gt, XBJ_GENT_SIZE);
+                    if (slot) {
+                        full = false;
+                        g = xb_group_find(E.plan, slot, 0, h->hash, img, E.gt, E.st, &full);
+                    }
+                }
+                if (g) {
+                    xbj_merge_sm(g, e);
+                } else if (full) {
+                    h->state = XBJ_SM_LEFT;
+                    cur[1] = 1;
+                }
+            }
+            __syncthreads();
+            if (cur[1]) {
+                /* the rows of the groups left: every row of the bucket finds
+                 * its group where it was combined (the shared table only
+                 * gains entries), or none when it went to the global table */
+                for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                    char *rec = base + (uint64_t)i * XBJ_REC_SIZE;
+                    XbjRegs R;
+                    uint32_t ghash;
+                    xbj_rec_load(rec, R, ghash);
+                    bool full = false;
+                    char *e = xbj_group_get<true>(R, E, E.sm_tab, E.sm_mask, ghash, &full);
+                    if (e && ((const xb_gent_head *)e)->state == XBJ_SM_LEFT) {
+                        ((uint32_t *)rec)[1] |= XBJ_REC_LEFT;
+                        if (!args.st->replay_left)
+                            atomicExch(&args.st->replay_left, 1u);
+                    }
+                }
+            }
+        }
+        /* every thread has read cur[] and is done with the shared table */
+        __syncthreads();
     }
 }
 #endif
