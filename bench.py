@@ -597,7 +597,10 @@ def run_config(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
             "config": {"workload": desc, "rows": args.rows, "chunks": len(chunks), "chunk_bytes": nbytes,
-                       "generation_s": round(gen_s, 1), "launch_shape": shape},
+                       "generation_s": round(gen_s, 1), "launch_shape": shape,
+                       **({"partitioned_pass_ms": {"scan": round(info["last_part_scan_ms"], 3),
+                                                   "replay": round(info["last_part_replay_ms"], 3)}}
+                          if info.get("partition_used") else {})},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "algorithmic_bytes": ref_bytes,
                          "kernel": ("xbj_kernel" if "jit" in info["kernels"].values() else "xb_exec_kernel"),

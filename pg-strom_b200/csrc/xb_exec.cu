@@ -2230,6 +2230,9 @@ struct xpuB200Session {
     uint64_t        total_raw = 0, total_in = 0, total_out = 0;
     uint64_t        total_depth[XB_MAX_DEPTH + 1] = {0};
     cudaEvent_t     ev0, ev1;
+    /* partitioned aggregation: the last such launch's scan and replay,
+     * bracketed on the session stream (diagnostics, xpuB200SessionInfo) */
+    cudaEvent_t     ev_part[3] = {nullptr, nullptr, nullptr};
     /* session-specialised kernels, per source format (index: KDS format) */
     bool            jit_enabled = true;
     bool            jit_tried[256] = {false};
@@ -2479,6 +2482,8 @@ static void xb_session_free(xpuB200Session *s)
         xb_inner_cache_put(s->dev, s->inner_entry);
     xb_put_status(s->dev, s->h_status);
     if (s->h_plan) free(s->h_plan);
+    for (cudaEvent_t e : s->ev_part)
+        if (e) cudaEventDestroy(e);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);
     xb_put_stream(s->dev, s->stream);
@@ -2526,6 +2531,8 @@ xpuB200OpenSession(xpuB200Device *dev, const kern_session_info *session, uint64_
     }
     cudaEventCreate(&s->ev0);
     cudaEventCreate(&s->ev1);
+    for (cudaEvent_t &e : s->ev_part)
+        cudaEventCreate(&e);
     int rc;
     char msg[256];
 #define FAIL(...) do { rc = XB_ERR(err, __VA_ARGS__); xb_session_free(s); return rc; } while (0)
@@ -3020,7 +3027,6 @@ static bool xb_tune_lookup(xpuB200Session *s, uint32_t format, xb_tune_choice *c
  * request of a new plan shape does not wait seconds for NVRTC.
  */
 static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, double ms, const char *msg);
-static size_t xb_replay_smem(const xb_plan *plan);
 
 static void *xb_session_jit(xpuB200Session *s, uint32_t format, bool wait = true)
 {
@@ -3097,8 +3103,7 @@ static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, dou
                 s->jit_mixfn[format] = nullptr;
             s->jit_grid[format] = per_sm * s->dev->nsm;
             int rp = 0;
-            if (s->jit_replay[format] &&
-                xb_jit_prepare(s->jit_replay[format], XB_BLOCK, xb_replay_smem(s->h_plan), &rp) != 0)
+            if (s->jit_replay[format] && xb_jit_prepare(s->jit_replay[format], XB_BLOCK, 0, &rp) != 0)
                 s->jit_replay[format] = nullptr;
             s->jit_replay_grid[format] = rp * s->dev->nsm;
             s->jit_compile_ms += ms;
@@ -3115,10 +3120,10 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
 
 /* partitioned aggregation for this launch: a keyed GROUP BY whose groups
  * live in a global table larger than L2 defers each row's update into the
- * bucket of its table slot; a bucket covers the slots of one replay CTA's
- * shared table, so the replay combines a bucket's rows in shared memory
- * and merges each of its groups into the global table once.  Rows past a
- * full bucket are updated in place, so any bucket size is correct.  Used by
+ * bucket of its table slot; a bucket covers a slice of the table small
+ * enough for the slices the replay's CTAs work on together to stay in L2.
+ * Rows past a full bucket are updated in place, so any bucket size is
+ * correct.  Used by
  * prepared batches whose table is several times L2 (the records of a batch
  * take device memory in proportion to its rows, which the serving path's
  * admission does not budget); XPU_B200_PARTITION=1 uses it for every
@@ -3127,54 +3132,24 @@ static int xb_launch_tasks(xpuB200Session *s, const xb_task *d_tasks, uint32_t n
  * that rows past full buckets are updated in place while others of the
  * same groups are deferred.  Session lock held.  Returns whether it is
  * used. */
-/* table slots of one bucket of partitioned aggregation (xb_replay_slots).
- * XPU_B200_REPLAY_KB=n gives each replay CTA a shared
- * group table of n KB that covers its bucket's slots (the bucket's rows
- * are combined there and each group merged into the global table once);
- * the default, 0, updates the global table row by row, which measured
- * faster at 2 and at 10 rows per group (the shared table's inserts and
- * merges cost two group creations per group). */
-static uint32_t xb_replay_kb()
-{
-    static const int kb = [] {
-        const char *e = getenv("XPU_B200_REPLAY_KB");
-        const int v = e ? atoi(e) : -1;
-        return (v >= 0 && v <= 200) ? v : 0;
-    }();
-    return (uint32_t)kb;
-}
-
+/* table slots of one bucket of partitioned aggregation: about 128 KB of
+ * global table (1024 of the Arrow group-by's 112-byte entries; measured
+ * against 512, 2048 and 4096 slots); XPU_B200_PART_SLOTS=n (a power of two,
+ * 64..65536) sets it */
 static uint32_t xb_replay_slots(const xb_plan *plan)
 {
-    /* XPU_B200_PART_SLOTS=n (a power of two, 64..65536): n slots per bucket
-     * when the replay has no shared table */
     static const uint32_t forced = [] {
         const char *e = getenv("XPU_B200_PART_SLOTS");
         const unsigned long v = e ? strtoul(e, nullptr, 10) : 0;
         return (v >= 64 && v <= 65536 && (v & (v - 1)) == 0) ? (uint32_t)v : 0u;
     }();
-    if (forced && !xb_replay_kb())
+    if (forced)
         return forced;
-    /* with a shared table: the slots whose entries fit it; without: about
-     * 128 KB of global table per bucket (1024 of the Arrow group-by's
-     * 112-byte entries; measured against 512, 2048 and 4096 slots) */
-    const uint32_t stride = xb_replay_kb() ? xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16)
-                                           : (plan->gent_size ? plan->gent_size : 16);
-    const uint64_t target = (uint64_t)(xb_replay_kb() ? xb_replay_kb() : 128) << 10;
+    const uint64_t gsz = plan->gent_size ? plan->gent_size : 16;
     uint32_t c = 8192;
-    while (c > 64 && (uint64_t)c * stride > target)
+    while (c > 64 && c * gsz > (128u << 10))
         c >>= 1;
     return c;
-}
-
-static uint32_t xb_replay_sm_cap(const xb_plan *plan)
-{
-    return xb_replay_kb() ? xb_replay_slots(plan) : 0;
-}
-
-static size_t xb_replay_smem(const xb_plan *plan)
-{
-    return (size_t)xb_replay_sm_cap(plan) * xb_jit_sm_stride(plan->gent_size ? plan->gent_size : 16);
 }
 
 static bool xb_part_prepare(xpuB200Session *s, uint64_t nunits, uint32_t format, cudaStream_t stream)
@@ -3497,9 +3472,12 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
         s->part_used = true;
     }
     if (fn) {
+        if (part)
+            cudaEventRecord(s->ev_part[0], stream);
         if (xb_jit_launch(fn, grid, XB_BLOCK, s->jit_smem_fmt[format], (void *)stream, &a) != 0)
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised kernel launch failed");
         if (part) {
+            cudaEventRecord(s->ev_part[1], stream);
             XbReplayArgs ra;
             memset(&ra, 0, sizeof(ra));
             ra.plan = s->d_plan;
@@ -3510,10 +3488,11 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
             ra.part_cap = s->part_cap;
             ra.nparts = s->nparts;
             ra.cursor = s->part_cnt + (size_t)s->nparts * XB_PART_CNT_STRIDE;
-            ra.sm_cap = xb_replay_sm_cap(s->h_plan);
-            if (xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK,
-                              xb_replay_smem(s->h_plan), (void *)stream, &ra) != 0)
+            ra.part_shift = s->part_shift;
+            if (xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK, 0, (void *)stream,
+                              &ra) != 0)
                 return XB_ERR(err, ERRCODE_DEVICE_FATAL, "replay kernel launch failed");
+            cudaEventRecord(s->ev_part[2], stream);
         }
     } else {
         xb_exec_kernel<<<grid, XB_BLOCK, s->smem_bytes, stream>>>(a);
@@ -3648,7 +3627,7 @@ static int xb_replay_retry(xpuB200Session *s, uint32_t format, kern_errorbuf *er
     ra.cursor = cursor;
     ra.part_cap = s->part_cap;
     ra.nparts = s->nparts;
-    ra.sm_cap = 0;              /* the left records, row by row into the grown table */
+    ra.part_shift = s->part_shift;
     ra.retry = 1;
     if (!s->jit_replay[format] ||
         xb_jit_launch(s->jit_replay[format], s->jit_replay_grid[format], XB_BLOCK, 0, (void *)s->stream, &ra) != 0)
@@ -6081,13 +6060,20 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
     }
     for (char c : s->jit_msg)
         msg += (c == '"' || c == '\\' || (unsigned char)c < 32) ? ' ' : c;
+    float scan_ms = 0.0f, replay_ms = 0.0f;
+    if (s->part_used && cudaEventQuery(s->ev_part[2]) == cudaSuccess) {
+        cudaEventElapsedTime(&scan_ms, s->ev_part[0], s->ev_part[1]);
+        cudaEventElapsedTime(&replay_ms, s->ev_part[1], s->ev_part[2]);
+    }
+    cudaGetLastError();
     snprintf(buf, buf_sz,
              "{\"nregs\": %u, \"nslots\": %u, \"nrels\": %u, \"ninsns\": %u, \"has_groupby\": %u, "
              "\"nkeys\": %u, \"naggs\": %u, \"gent_size\": %u, \"gtable_cap\": %llu, "
              "\"sm_cap\": %u, \"smem_bytes\": %zu, \"grid\": %d, \"unique_hash\": [%u, %u, %u], "
              "\"jit_enabled\": %s, \"kernels\": {%s}, \"jit_compile_ms\": %.1f, \"jit_msg\": \"%s\", "
              "\"jit_ctas_per_sm\": %d, \"sm_cap_default\": %u, \"inner_cache\": %s, "
-             "\"partitions\": %u, \"partition_used\": %s, \"gtable_grew\": %u, \"gtable_dump_cap\": %llu}",
+             "\"partitions\": %u, \"partition_used\": %s, \"gtable_grew\": %u, \"gtable_dump_cap\": %llu, "
+             "\"last_part_scan_ms\": %.3f, \"last_part_replay_ms\": %.3f}",
              p->nregs, p->nslots, p->nrels, p->ninsns, p->has_groupby, p->nkeys, p->naggs,
              p->gent_size, (unsigned long long)(s->h_gt.cap_mask + 1), s->sm_cap, s->smem_bytes,
              s->grid, p->inner[1].unique_hash, p->inner[2].unique_hash, p->inner[3].unique_hash,
@@ -6095,7 +6081,7 @@ xpuB200SessionInfo(xpuB200Session *s, char *buf, uint64_t buf_sz)
              s->jit_minb, s->sm_cap_default,
              s->inner_hit ? "\"hit\"" : s->inner_entry ? "\"built\"" : "\"none\"",
              s->nparts, s->part_used ? "true" : "false", s->grow_count,
-             (unsigned long long)(p->has_groupby ? s->h_gt.dump_cap : 0));
+             (unsigned long long)(p->has_groupby ? s->h_gt.dump_cap : 0), scan_ms, replay_ms);
     return 0;
 }
 

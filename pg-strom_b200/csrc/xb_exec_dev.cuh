@@ -646,9 +646,8 @@ struct XbReplayArgs {
     uint32_t       *cursor;         /* next bucket to claim (zero at launch) */
     uint32_t        part_cap;
     uint32_t        nparts;
-    uint32_t        sm_cap;         /* shared group-table entries of a CTA, one bucket's
-                                     * slots (0: rows straight into the global table) */
     uint32_t        retry;          /* replay only the records marked left */
+    uint32_t        part_shift;     /* a bucket holds 1 << part_shift table slots */
 };
 
 /* largest existence bitmap of a direct depth (keys), 16 KB */

@@ -19,6 +19,7 @@
  * exactly as in the interpreting kernel (xb_exec.cu), and the statistics,
  * shared-memory group table and error reporting are the same.
  */
+#ifndef XBJ_RT_TAIL
 #ifndef XB_JIT_RT_CUH
 #define XB_JIT_RT_CUH
 
@@ -124,10 +125,6 @@ xbj_pipeline(XbjRegs &R, const XbjEnv &E, XbjCnt &C, bool &failed);
  * (returns true when, replaying, the table had no room for the group) */
 __device__ __forceinline__ void xbj_rec_load(const char *rec, XbjRegs &R, uint32_t &ghash);
 __device__ __forceinline__ bool xbj_group_row(XbjRegs &R, const XbjEnv &E, const uint32_t ghash, bool &failed);
-/* generated: find or create the group of R's keys in a table */
-template <bool SMEM>
-__device__ __forceinline__ char *
-xbj_group_get(const XbjRegs &R, const XbjEnv &E, char *entries, uint64_t cap_mask, uint32_t hash, bool *full);
 #endif
 
 #ifdef XBJ_MERGE_SM
@@ -485,36 +482,35 @@ xbj_mixed_kernel(const __grid_constant__ XbMixArgs m)
     }
 }
 
-#ifdef XBJ_PART
-/* a replay's shared entry that the global table (and the dump) had no room
- * for: its rows are left for after the table grows */
-#define XBJ_SM_LEFT     3u
+#endif  /* XB_JIT_RT_CUH */
+#else   /* XBJ_RT_TAIL */
+#ifndef XB_JIT_RT_TAIL_DONE
+#define XB_JIT_RT_TAIL_DONE
+/* ---- the tail: included again at the end of the generated source (after
+ * XBJ_RT_TAIL is defined), where every generated definition is known ---- */
 
+#ifdef XBJ_PART
 /* replay of the deferred rows.  A bucket holds the rows whose groups have
- * their home slot in one slice of the global table (sm_cap slots), so it
- * holds no more groups than the CTA's shared table has room for at the
- * global table's load.  Each CTA claims buckets in order: it combines the
- * bucket's rows in its shared table (the specialised kernel's shared state
- * form), then merges every group of the bucket into the global table once
- * -- one probe and one state merge per group instead of one per row.
- * Groups past a full shared table are updated in the global table
- * directly.  A group that the global table and its dump have no room for
- * (the table asked to grow meanwhile) is left: the re-sweep marks its rows
- * for the retry replay after the growth, which updates the global table
- * row by row (sm_cap 0). */
+ * their home slot in one slice of the global table (1 << part_shift
+ * slots).  Each CTA claims buckets in order, so the CTAs work on
+ * neighbouring slices together and the slices stay in L2; the bucket's
+ * records and its slice are pulled into L2 by the TMA engine when it is
+ * claimed.  Every row updates its group in the global table (the same
+ * update as in place).  A row whose group the table and its dump have no
+ * room for (the table asked to grow meanwhile) is marked and replayed
+ * after the growth (retry). */
 extern "C" __global__ void __launch_bounds__(XB_BLOCK, XBJ_MIN_BLOCKS)
 xbj_replay(const __grid_constant__ XbReplayArgs args)
 {
-    extern __shared__ __align__(16) char sm_entries[];
-    __shared__ uint32_t cur[2];         /* the CTA's bucket; whether its merge left groups */
+    __shared__ uint32_t cur;            /* the CTA's bucket */
     XbjEnv E;
     E.plan = args.plan;
     E.st = args.st;
     E.gt = args.gt;
     E.gt_entries = args.gt->entries;
     E.gt_mask = args.gt->cap_mask;
-    E.sm_tab = args.sm_cap ? sm_entries : nullptr;
-    E.sm_mask = args.sm_cap ? args.sm_cap - 1 : 0;
+    E.sm_tab = nullptr;
+    E.sm_mask = 0;
     E.lane = threadIdx.x & 31;
     E.dst = nullptr;
     E.dst_len = 0;
@@ -524,21 +520,29 @@ xbj_replay(const __grid_constant__ XbReplayArgs args)
     E.part_cap = 0;
     E.part_shift = 0;
     E.replay = 1;
-    const uint32_t sm_vec = (uint32_t)(((uint64_t)args.sm_cap * XBJ_SM_STRIDE) / 16);
     for (;;) {
-        if (threadIdx.x == 0) {
-            cur[0] = atomicAdd(args.cursor, 1u);
-            cur[1] = 0;
-        }
-        for (uint32_t i = threadIdx.x; i < sm_vec; i += blockDim.x)
-            ((uint4 *)sm_entries)[i] = make_uint4(0u, 0u, 0u, 0u);
+        if (threadIdx.x == 0)
+            cur = atomicAdd(args.cursor, 1u);
         __syncthreads();
-        const uint32_t b = cur[0];
+        const uint32_t b = cur;
         if (b >= args.nparts)
             break;
         const uint32_t cnt = args.part_cnt[(size_t)b * XB_PART_CNT_STRIDE];
         const uint32_t n = cnt < args.part_cap ? cnt : args.part_cap;
         char *base = args.part_buf + (uint64_t)b * args.part_cap * XBJ_REC_SIZE;
+        if (threadIdx.x == 0 && !args.retry && n) {
+            const uint64_t rb = (uint64_t)n * XBJ_REC_SIZE;
+            /* (a bulk prefetch starts on a 16-byte boundary: a bucket of
+             * records of a size that is no multiple of 16 may not) */
+            if ((((uintptr_t)base) & 15) == 0 && rb >= 16)
+                xb_prefetch_l2(base, (uint32_t)(rb < (1u << 20) ? rb : (1u << 20)) & ~15u);
+            if (args.part_shift && ((uint64_t)b << args.part_shift) <= E.gt_mask) {
+                const uint64_t sb = ((uint64_t)XBJ_GENT_SIZE << args.part_shift);
+                const char *sl = E.gt_entries + ((uint64_t)b << args.part_shift) * XBJ_GENT_SIZE;
+                if ((((uintptr_t)sl) & 15) == 0 && sb <= (1u << 20))
+                    xb_prefetch_l2(sl, (uint32_t)sb & ~15u);
+            }
+        }
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             char *rec = base + (uint64_t)i * XBJ_REC_SIZE;
             /* a retry replays only the records a full table left behind */
@@ -557,55 +561,11 @@ xbj_replay(const __grid_constant__ XbReplayArgs args)
                 ((uint32_t *)rec)[1] &= ~XBJ_REC_LEFT;
             }
         }
-        __syncthreads();
-        if (E.sm_tab) {
-            /* every group of the bucket into the global table, once */
-            for (uint32_t i = threadIdx.x; i < args.sm_cap; i += blockDim.x) {
-                char *e = sm_entries + (size_t)i * XBJ_SM_STRIDE;
-                xb_gent_head *h = (xb_gent_head *)e;
-                if (h->state != XB_GSTATE_READY)
-                    continue;
-                const xb_keyimg *img = (const xb_keyimg *)(e + XBJ_KEYS_OFF);
-                bool full = false;
-                char *g = xb_group_find(E.plan, E.gt_entries, E.gt_mask, h->hash, img, E.gt, E.st, &full);
-                if (!g && full) {
-                    char *slot = xb_dump_slot(E.gt, XBJ_GENT_SIZE);
-                    if (slot) {
-                        full = false;
-                        g = xb_group_find(E.plan, slot, 0, h->hash, img, E.gt, E.st, &full);
-                    }
-                }
-                if (g) {
-                    xbj_merge_sm(g, e);
-                } else if (full) {
-                    h->state = XBJ_SM_LEFT;
-                    cur[1] = 1;
-                }
-            }
-            __syncthreads();
-            if (cur[1]) {
-                /* the rows of the groups left: every row of the bucket finds
-                 * its group where it was combined (the shared table only
-                 * gains entries), or none when it went to the global table */
-                for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-                    char *rec = base + (uint64_t)i * XBJ_REC_SIZE;
-                    XbjRegs R;
-                    uint32_t ghash;
-                    xbj_rec_load(rec, R, ghash);
-                    bool full = false;
-                    char *e = xbj_group_get<true>(R, E, E.sm_tab, E.sm_mask, ghash, &full);
-                    if (e && ((const xb_gent_head *)e)->state == XBJ_SM_LEFT) {
-                        ((uint32_t *)rec)[1] |= XBJ_REC_LEFT;
-                        if (!args.st->replay_left)
-                            atomicExch(&args.st->replay_left, 1u);
-                    }
-                }
-            }
-        }
-        /* every thread has read cur[] and is done with the shared table */
+        /* every thread has read cur */
         __syncthreads();
     }
 }
 #endif
 
-#endif  /* XB_JIT_RT_CUH */
+#endif  /* XB_JIT_RT_TAIL_DONE */
+#endif  /* XBJ_RT_TAIL */
