@@ -69,6 +69,8 @@ def parse():
                     help="served: rows of the Arrow template's table (queries take 1M..all of it)")
     ap.add_argument("--no-served-leg", dest="served_leg", action="store_false",
                     help="headline line: skip the short served-mix measurement")
+    ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
+                    help="skip the reference's own kernel (built for sm_100a) on the same GPU")
     return ap.parse_args()
 
 
@@ -287,6 +289,50 @@ def cpu_rows_per_sec(sess, km, chunks, seconds, threads, allow_ref=True):
     return state["rows"] / el, kind, state["rows"], el
 
 
+def reference_gpu_leg(sess, km, chunks, rows, truth, steps=3, warmup=1, rtol=None):
+    """PG-Strom's own device executor, kern_gpujoin_main, built for sm_100a
+    from the reference sources and launched as its GPU service launches it
+    (one task and one stream synchronisation per chunk), over its own
+    device copies of the same chunks on the same GPU.  Its groups are
+    checked against the truth; the timed passes reuse one session, as the
+    timed batches of this repository's path do."""
+    import ref_gpu
+    import xb_final as F
+    if not ref_gpu.available():
+        return {"unavailable": "the reference's sm_100a build (oracle/_ref) is not present"}
+    ref_gpu.open_device(0)
+    ptrs = [ref_gpu.upload(c) for c in chunks]
+    try:
+        rs = ref_gpu.RefSession(sess, km)
+        try:
+            rs.exec(ptrs)
+            final = rs.final()
+            got = F.decode_kds_final(final, sess)
+            errs = (F.compare_groups(got, truth) if rtol is None else F.compare_groups(got, truth, rtol=rtol)) \
+                if truth else []
+            for _ in range(warmup):
+                rs.exec(ptrs)
+            k0 = rs.info()["kernel_ms"]
+            times = [rs.exec(ptrs) for _ in range(steps)]
+            info = rs.info()
+        finally:
+            rs.close()
+    finally:
+        for p in ptrs:
+            ref_gpu.free(p)
+    ms = sum(times) / len(times)
+    kms = (info["kernel_ms"] - k0) / steps
+    return {"value": rows / (ms / 1000.0), "unit": UNIT, "ms_per_pass": ms,
+            "kernel_ms_per_pass": kms, "kernel_value": rows / (kms / 1000.0),
+            "kernel": "kern_gpujoin_main (PG-Strom sources, sm_100a, --maxrregcount=128)",
+            "tasks_per_pass": len(chunks),
+            "launch": {k: info[k] for k in ("grid", "block", "shmem", "prepfn_nbufs", "registers",
+                                            "stack_limit")},
+            "includes": "ms_per_pass: every chunk's launch and the stream synchronisation after it, as the "
+                        "reference's GPU service runs its tasks; kernel_ms_per_pass: the launches alone",
+            "parity": {"groups_equal_truth": errs == [], "errors": errs[:3]}}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -460,6 +506,15 @@ def run_b200(args, rank, world, local):
         except Exception as e:          # the headline stands without it
             served = {"error": f"{type(e).__name__}: {e}"[:300]}
 
+    # ---- the reference's own kernel on this GPU (rank 0, N=1), after
+    # every other measurement of the line
+    ref_gpu_line = None
+    if rank == 0 and world == 1 and args.reference_gpu:
+        try:
+            ref_gpu_line = reference_gpu_leg(sess, km, chunks, args.rows, meta["truth"], rtol=0.0)
+        except Exception as e:          # the headline stands without it
+            ref_gpu_line = {"error": f"{type(e).__name__}: {e}"[:300]}
+
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -501,6 +556,8 @@ def run_b200(args, rank, world, local):
                 "cpu_baseline": cpu}
         if served:
             line["served"] = served
+        if ref_gpu_line:
+            line["reference_gpu"] = ref_gpu_line
         if merge:
             line["final_merge"] = merge
         print(json.dumps(line), flush=True)
@@ -606,6 +663,11 @@ def run_config(args):
                          "kernel": ("xbj_kernel" if "jit" in info["kernels"].values() else "xb_exec_kernel"),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
             "clocks": clocks, "gpu_launches": args.steps}
+    if args.workload == "scan_groupby" and args.reference_gpu:
+        try:
+            line["reference_gpu"] = reference_gpu_leg(sess, None, chunks, args.rows, truth)
+        except Exception as e:
+            line["reference_gpu"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if args.cpu_seconds > 0:
         threads = os.cpu_count() or 1
         heap = args.workload == "scan_groupby"
