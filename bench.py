@@ -71,6 +71,8 @@ def parse():
                     help="headline line: skip the short served-mix measurement")
     ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
                     help="skip the reference's own kernel (built for sm_100a) on the same GPU")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="headline line: skip the C0 / C2 / C3 configuration runs")
     return ap.parse_args()
 
 
@@ -333,6 +335,55 @@ def reference_gpu_leg(sess, km, chunks, rows, truth, steps=3, warmup=1, rtol=Non
             "parity": {"groups_equal_truth": errs == [], "errors": errs[:3]}}
 
 
+CONFIG_RUNS = [
+    ("C0 scan_groupby 4M heap rows",
+     ["--workload", "scan_groupby", "--rows", "4000000", "--steps", "10", "--warmup", "3", "--cpu-seconds", "4"]),
+    ("C2 arrow_groupby 500M rows / 10M keys",
+     ["--workload", "arrow_groupby", "--rows", "500000000", "--steps", "5", "--warmup", "3", "--cpu-seconds", "0"]),
+    ("C3 mixed: 256 batched chunk commands",
+     ["--workload", "mixed", "--steps", "10", "--warmup", "3"]),
+]
+
+
+def config_lines(timeout_s=240):
+    """The other configurations of the benchmark, each in a process of its
+    own after every measurement of the headline (one at a time, so they
+    share the GPU with nothing): a short summary of each line."""
+    out = {}
+    for name, argv in CONFIG_RUNS:
+        t0 = time.time()
+        try:
+            p = subprocess.run([sys.executable, os.path.abspath(__file__)] + argv, capture_output=True,
+                               text=True, timeout=timeout_s)
+            lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+            if p.returncode != 0 or not lines:
+                out[name] = {"error": (p.stderr or "no output").strip().splitlines()[-1][:300]}
+                continue
+            d = json.loads(lines[-1])
+        except Exception as e:
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            continue
+        summ = {"metric": d.get("metric"), "value": d.get("value"), "unit": d.get("unit"),
+                "ms_per_step": d.get("ms_per_step"), "steps": d.get("steps"), "warmup": d.get("warmup"),
+                "wall_s": round(time.time() - t0, 1), "argv": " ".join(argv)}
+        rf = d.get("roofline")
+        if rf:
+            summ["roofline"] = {k: rf.get(k) for k in ("bound", "achieved", "peak", "unit", "frac", "kernel")}
+        cfg = d.get("config", {})
+        for k in ("partitioned_pass_ms", "launch_shape", "rows", "commands", "launches_per_run"):
+            if k in cfg:
+                summ[k] = cfg[k]
+        for k in ("plain", "clocks", "cpu_baseline"):
+            if k in d:
+                summ[k] = d[k]
+        rg = d.get("reference_gpu")
+        if rg:
+            summ["reference_gpu"] = {k: rg.get(k) for k in ("value", "ms_per_pass", "kernel_ms_per_pass",
+                                                           "parity", "unavailable", "error") if k in rg}
+        out[name] = summ
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -506,6 +557,11 @@ def run_b200(args, rank, world, local):
         except Exception as e:          # the headline stands without it
             served = {"error": f"{type(e).__name__}: {e}"[:300]}
 
+    # ---- the other configurations (rank 0, N=1), each in its own process
+    configs = None
+    if rank == 0 and world == 1 and args.configs:
+        configs = config_lines()
+
     # ---- the reference's own kernel on this GPU (rank 0, N=1), after
     # every other measurement of the line
     ref_gpu_line = None
@@ -558,6 +614,8 @@ def run_b200(args, rank, world, local):
             line["served"] = served
         if ref_gpu_line:
             line["reference_gpu"] = ref_gpu_line
+        if configs:
+            line["configs"] = configs
         if merge:
             line["final_merge"] = merge
         print(json.dumps(line), flush=True)
