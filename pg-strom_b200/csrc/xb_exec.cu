@@ -3097,9 +3097,11 @@ static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, dou
             s->jit_msg = "specialised kernel does not fit on an SM";
         } else {
             /* the mixed kernel is shared by sessions of one plan shape with
-             * their own table sizes: it opts in to all shared memory */
-            if (xb_jit_prepare(s->jit_mixfn[format], XB_BLOCK, s->dev->smem_optin - sizeof(XbExecArgs) - 16,
-                               &mix_sm) != 0)
+             * their own table sizes: it opts in to all shared memory that
+             * its static shared memory leaves */
+            if (s->jit_mixfn[format] &&
+                xb_jit_prepare(s->jit_mixfn[format], XB_BLOCK,
+                               s->dev->smem_optin - xb_jit_static_smem(s->jit_mixfn[format]) - 16, &mix_sm) != 0)
                 s->jit_mixfn[format] = nullptr;
             s->jit_grid[format] = per_sm * s->dev->nsm;
             int rp = 0;
@@ -4854,7 +4856,8 @@ static int xb_mix_plan(xpuB200Device *dev, const std::vector<xpuB200Session *> &
             groups[g].smem = sm;
     }
     for (xb_mix_group &g : groups) {
-        if (g.smem + sizeof(XbExecArgs) + 16 > dev->smem_optin)
+        const size_t st = g.jfn ? xb_jit_static_smem(g.jfn) : sizeof(XbExecArgs);
+        if (g.smem + st + 16 > dev->smem_optin)
             return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch needs %zu bytes of shared memory", g.smem);
         int per_sm = 0;
         if (g.jfn)

@@ -72,6 +72,9 @@ int xb_jit_check(const xb_plan *plan, uint32_t format, uint64_t *p_cubin_bytes, 
 /* allow 'smem' bytes of dynamic shared memory; resident CTAs per SM */
 int xb_jit_prepare(void *func, int block, size_t smem, int *p_per_sm);
 
+/* bytes of static shared memory of a kernel (0 when unknown) */
+size_t xb_jit_static_smem(void *func);
+
 /* resident CTAs per SM with 'smem' bytes (the limit already allowed) */
 int xb_jit_occupancy(void *func, int block, size_t smem, int *p_per_sm);
 
