@@ -255,7 +255,7 @@ xb_vm_exec(const xb_insn *__restrict__ code, uint32_t count, const XbRegs &R,
 }
 
 /* out-of-line entry for callers other than the executor's main loop */
-__device__ __noinline__ bool
+static __device__ __noinline__ bool
 xb_vm_run(const xb_insn *__restrict__ code, uint32_t count, XbRegs R,
           uint32_t active_in, xb_status *st)
 {

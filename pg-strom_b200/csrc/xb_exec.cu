@@ -44,6 +44,7 @@
 #include "xb_jit.h"
 #include "xb_sort.cuh"
 #include "xpu_b200.h"
+#include "xb_host.h"
 
 /* ================================================================
  * executor kernel
@@ -2022,57 +2023,6 @@ xb_inner_rebuild(XbRebuildArgs args)
 /* ================================================================
  * host side
  * ================================================================ */
-struct xpuB200Device {
-    int             dindex;
-    int             nsm;
-    uint64_t        hbm_budget;
-    size_t          smem_optin;     /* dynamic shared memory a CTA may opt in to */
-    cudaStream_t    stream;
-    struct xb_sched *sched = nullptr; /* asynchronous commands (created by the first submit) */
-    /* recycled per-session resources: creating a stream or pinning host
-     * memory costs far more than a query's own host work */
-    std::mutex      pool_lock;
-    std::vector<cudaStream_t> free_streams;
-    std::vector<xb_status *> free_status;
-    std::vector<xb_status *> status_blocks;
-    /* inner relations built for sessions with a join_inner_handle, kept
-     * while sessions use them and, within inner_budget bytes, after */
-    std::mutex      inner_lock;
-    std::vector<struct xb_inner_entry *> inner_cache;
-    uint64_t        inner_budget = 16ULL << 30;
-    uint64_t        inner_bytes = 0;
-    uint64_t        inner_clock = 0;
-    /* outer-table chunks resident across sessions (xpuB200ChunkCache*) */
-    std::mutex      chunk_lock;
-    std::map<std::pair<uint64_t, uint32_t>, struct xb_chunk_entry> chunk_cache;
-    uint64_t        chunk_budget = 64ULL << 30;
-    uint64_t        chunk_bytes = 0;
-    uint64_t        chunk_clock = 0;
-};
-
-/* one resident chunk: the device copy of a caller's chunk, placed so that
- * heap pages start 16-byte aligned; refs counts the callers using it */
-struct xb_chunk_entry {
-    char           *base = nullptr;
-    const kern_data_store *kds = nullptr;
-    uint64_t        bytes = 0;
-    uint32_t        refs = 0;
-    uint64_t        last_use = 0;
-};
-
-/* one cached set of inner relations: the built descriptors (with their
- * device memory) of every depth */
-struct xb_inner_entry {
-    uint64_t        key;
-    uint32_t        nrels;
-    xb_inner        inner[XB_MAX_DEPTH + 1];
-    uint32_t        gid_cap;        /* shared table slots the group ids need (0: none) */
-    std::vector<void *> allocs;
-    uint64_t        bytes = 0;
-    uint32_t        refs = 0;
-    uint64_t        last_use = 0;
-};
-
 static void xb_inner_entry_free(xpuB200Device *dev, xb_inner_entry *e)
 {
     for (void *p : e->allocs)
@@ -2083,7 +2033,7 @@ static void xb_inner_entry_free(xpuB200Device *dev, xb_inner_entry *e)
 
 /* drop unreferenced entries, least recently used first, while the cache
  * holds more than its budget; inner_lock held */
-static void xb_inner_evict_locked(xpuB200Device *dev)
+void xb_inner_evict_locked(xpuB200Device *dev)
 {
     while (dev->inner_bytes > dev->inner_budget) {
         int victim = -1;
@@ -2151,7 +2101,7 @@ static void xb_inner_cache_put(xpuB200Device *dev, xb_inner_entry *e)
     xb_inner_evict_locked(dev);
 }
 
-static cudaStream_t xb_get_stream(xpuB200Device *dev)
+cudaStream_t xb_get_stream(xpuB200Device *dev)
 {
     {
         std::lock_guard<std::mutex> g(dev->pool_lock);
@@ -2167,7 +2117,7 @@ static cudaStream_t xb_get_stream(xpuB200Device *dev)
     return st;
 }
 
-static void xb_put_stream(xpuB200Device *dev, cudaStream_t st)
+void xb_put_stream(xpuB200Device *dev, cudaStream_t st)
 {
     if (!st) return;
     std::lock_guard<std::mutex> g(dev->pool_lock);
@@ -2198,96 +2148,12 @@ static void xb_put_status(xpuB200Device *dev, xb_status *p)
     dev->free_status.push_back(p);
 }
 
-static void xb_sched_drain_session(xpuB200Session *s);
-static void xb_sched_destroy(xpuB200Device *dev);
 
-struct xpuB200Session {
-    xpuB200Device  *dev;
-    cudaStream_t    stream = nullptr;
-    std::mutex      lock;
-    std::vector<char> h_session;
-    char           *d_session = nullptr;
-    char           *d_kmrels = nullptr;
-    xb_plan        *h_plan = nullptr;
-    xb_plan        *d_plan = nullptr;
-    std::vector<void *> d_allocs;
-    std::vector<uint64_t> d_alloc_sz;
-    xb_inner_entry *inner_entry = nullptr;  /* cached inner relations in use */
-    bool            inner_hit = false;      /* found built by an earlier session */
-    xb_gtable       h_gt = {};
-    xb_gtable      *d_gt = nullptr;
-    xb_status      *d_status = nullptr;
-    xb_status      *h_status = nullptr;     /* pinned */
-    char           *d_src = nullptr;
-    uint64_t        d_src_cap = 0;
-    xb_task        *d_tasks = nullptr;      /* work queue of single-chunk launches */
-    uint32_t        d_tasks_cap = 0;
-    uint32_t        sm_cap = 0;
-    uint32_t        warp_bytes = 0;
-    uint32_t        plan_bytes = 0;
-    size_t          smem_bytes = 0;
-    int             grid = 0;
-    uint64_t        total_raw = 0, total_in = 0, total_out = 0;
-    uint64_t        total_depth[XB_MAX_DEPTH + 1] = {0};
-    cudaEvent_t     ev0, ev1;
-    /* partitioned aggregation: the last such launch's scan and replay,
-     * bracketed on the session stream (diagnostics, xpuB200SessionInfo) */
-    cudaEvent_t     ev_part[3] = {nullptr, nullptr, nullptr};
-    /* session-specialised kernels, per source format (index: KDS format) */
-    bool            jit_enabled = true;
-    bool            jit_tried[256] = {false};
-    void           *jit_fn[256] = {nullptr};
-    void           *jit_mixfn[256] = {nullptr};    /* its mixed-launch kernel */
-    void           *jit_job[256] = {nullptr};      /* a background build of it, pending */
-    char            ran_kind[256] = {0};   /* 'j' / 'v': kernel last launched per format */
-    uint32_t        sched_refs = 0;        /* submitted commands not yet finished */
-    /* device projection: staging buffer for host kds_dst, and the buffer of
-     * the launch in progress */
-    char           *d_dst = nullptr;
-    uint64_t        d_dst_cap = 0;
-    char           *launch_dst = nullptr;
-    uint64_t        launch_dst_len = 0;
-    int             jit_grid[256] = {0};
-    size_t          jit_smem = 0;           /* without page staging */
-    size_t          jit_smem_fmt[256] = {0}; /* per format, with its page staging */
-    double          jit_compile_ms = 0.0;
-    std::string     jit_msg;
-    /* launch shape: resident CTAs per SM the specialised kernels are built
-     * for (0: default) and the shared group table's default capacity, as
-     * tuned by xpuB200BatchTune or adopted from its process-wide cache */
-    int             jit_minb = 0;
-    uint32_t        sm_cap_default = 0;
-    bool            tune_looked_up = false;
-    /* partitioned aggregation: deferred rows bucketed by table slot */
-    void           *jit_replay[256] = {nullptr};
-    int             jit_replay_grid[256] = {0};
-    char           *part_buf = nullptr;
-    uint32_t       *part_cnt = nullptr;
-    uint64_t        part_bytes = 0;
-    uint32_t        part_cap = 0;
-    uint32_t        part_shift = 0;
-    uint32_t        nparts = 0;
-    uint32_t        part_rec = 0;
-    bool            part_used = false;
-    bool            in_batch = false;       /* a prepared batch's launch is being issued */
-    /* group-table growth: where stopped warps record their leftover work
-     * (two lists: a resume launch reads one and records into the other),
-     * and the launch xb_run is issuing */
-    XbLeft         *d_left[2] = {nullptr, nullptr};
-    uint32_t        left_cap = 0;
-    bool            run_growth = false;
-    bool            run_resume = false;
-    uint32_t        run_left_sel = 0;
-    uint32_t        run_left_in_n = 0;
-    uint64_t        run_static_base0 = 0;
-    uint64_t        run_cursor0 = 0;
-    uint32_t        grow_count = 0;         /* times the group table grew */
-};
 
 /* shared group-table capacity 'cap' and the launch geometry that follows
  * from it (shared memory of both kernels, the interpreter's grid); the
  * specialised kernels are prepared again at their next launch */
-static int xb_set_sm_cap(xpuB200Session *s, uint32_t cap)
+int xb_set_sm_cap(xpuB200Session *s, uint32_t cap)
 {
     const xb_plan *plan = s->h_plan;
     size_t smem = s->plan_bytes + PGSTROM_TYPEALIGN(16, sizeof(XbSrcMeta)) +
@@ -2314,7 +2180,7 @@ static int xb_set_sm_cap(xpuB200Session *s, uint32_t cap)
     return 0;
 }
 
-static const char *xb_msg_text(uint32_t id)
+const char *xb_msg_text(uint32_t id)
 {
     switch (id) {
     case XB_MSG_INT_RANGE:        return "integer value out of range";
@@ -2342,7 +2208,7 @@ static_assert(offsetof(xb_gtable, grow) == 52 && offsetof(xb_gtable, overflow) =
               "the group table's grow word moved");
 static_assert(offsetof(XbSrc, grow_buf) % 16 == 0, "XbSrc.grow_buf must be 16-byte aligned");
 
-static int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int line,
+int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int line,
                         const char *fmt, ...)
 {
     if (err) {
@@ -2358,26 +2224,13 @@ static int xb_set_error(kern_errorbuf *err, uint32_t code, const char *func, int
     }
     return (int)code;
 }
-#define XB_ERR(err, code, ...) xb_set_error((err), (code), __func__, __LINE__, __VA_ARGS__)
-/* a CUDA call's result as 0 or a filled ERRCODE_DEVICE_FATAL */
-#define xb_set_cuda(call_rc, err) xb_cuda_rc((call_rc), (err), __func__, __LINE__)
-static int xb_cuda_rc(cudaError_t rc, kern_errorbuf *err, const char *func, int line)
+int xb_cuda_rc(cudaError_t rc, kern_errorbuf *err, const char *func, int line)
 {
     if (rc == cudaSuccess)
         return 0;
     return xb_set_error(err, ERRCODE_DEVICE_FATAL, func, line, "%s", cudaGetErrorString(rc));
 }
-#define XB_CUDA(call, err) do {                                               \
-        cudaError_t __rc = (call);                                            \
-        if (__rc != cudaSuccess)                                              \
-            return XB_ERR((err), ERRCODE_DEVICE_FATAL, "%s: %s", #call,       \
-                          cudaGetErrorString(__rc));                          \
-    } while (0)
 
-static inline void xb_clear_error(kern_errorbuf *err)
-{
-    if (err) memset(err, 0, sizeof(*err));
-}
 
 extern "C" int
 xpuB200Init(int cuda_dindex, uint64_t hbm_budget, xpuB200Device **p_dev, kern_errorbuf *err)
@@ -2877,7 +2730,7 @@ xpuB200CloseSession(xpuB200Session *sess)
 static void xb_note_walk(xb_plan *p, const kern_data_store *h);
 static void xb_note_layout_plan(xb_plan *p, const kern_data_store *h);
 
-static void xb_note_layout(xpuB200Session *s, const kern_data_store *h)
+void xb_note_layout(xpuB200Session *s, const kern_data_store *h)
 {
     if (s->jit_tried[KDS_FORMAT_BLOCK])
         return;
@@ -2960,7 +2813,7 @@ static void xb_note_walk(xb_plan *p, const kern_data_store *h)
 }
 
 /* units of one chunk (pages, or 1024-row groups) */
-static uint32_t xb_chunk_units(const kern_data_store *head)
+uint32_t xb_chunk_units(const kern_data_store *head)
 {
     if (head->format == KDS_FORMAT_BLOCK)
         return head->nitems;
@@ -2969,7 +2822,7 @@ static uint32_t xb_chunk_units(const kern_data_store *head)
 
 /* launch the executor over a device-resident task table, on a stream
  * with a status of the caller's */
-static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
+int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                         uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
                         kern_errorbuf *err);
 
@@ -2979,18 +2832,11 @@ static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntas
  * remembered per GPU for every session of the same plan shape and default
  * table capacity (the caller's group-count estimate)
  * ---------------------------------------------------------------- */
-struct xb_tune_choice {
-    int         minb;
-    uint32_t    sm_cap;
-};
-static std::mutex g_tune_lock;
-static std::map<std::tuple<int, uint64_t, uint32_t>, xb_tune_choice> g_tune;
-/* per plan shape alone: the CTA bound last tuned for it, adopted by
- * sessions whose default table capacity was not tuned (another group-count
- * estimate) */
-static std::map<std::pair<int, uint64_t>, int> g_tune_minb;
+std::mutex g_tune_lock;
+std::map<std::tuple<int, uint64_t, uint32_t>, xb_tune_choice> g_tune;
+std::map<std::pair<int, uint64_t>, int> g_tune_minb;
 
-static std::tuple<int, uint64_t, uint32_t> xb_tune_key(xpuB200Session *s, uint32_t format)
+std::tuple<int, uint64_t, uint32_t> xb_tune_key(xpuB200Session *s, uint32_t format)
 {
     return std::make_tuple(s->dev->dindex, xb_jit_shape_key(s->h_plan, format), s->sm_cap_default);
 }
@@ -3028,7 +2874,7 @@ static bool xb_tune_lookup(xpuB200Session *s, uint32_t format, xb_tune_choice *c
  */
 static void xb_session_adopt_jit(xpuB200Session *s, uint32_t format, int rc, double ms, const char *msg);
 
-static void *xb_session_jit(xpuB200Session *s, uint32_t format, bool wait = true)
+void *xb_session_jit(xpuB200Session *s, uint32_t format, bool wait)
 {
     if (!s->jit_enabled || format >= 256)
         return nullptr;
@@ -3417,7 +3263,7 @@ static void xb_status_add(xb_status *t, const xb_status *h)
         t->nitems_depth[d] += h->nitems_depth[d];
 }
 
-static int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
+int xb_launch_on(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks,
                         uint64_t nunits, uint32_t format, cudaStream_t stream, xb_status *d_status,
                         kern_errorbuf *err)
 {
@@ -3534,7 +3380,7 @@ static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
     return xb_launch_tasks(s, s->d_tasks, 1, t.nunits, t.format, err);
 }
 
-static int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
+int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
 {
     if (kds->format == KDS_FORMAT_BLOCK) {
         if ((uint64_t)kds->block_offset + (uint64_t)PGSTROM_BLCKSZ * kds->nitems > kds->length ||
@@ -3578,7 +3424,7 @@ static int xb_wait_status(xpuB200Session *s, kern_errorbuf *err)
 }
 
 /* a finished launch's statistics (status hs) into *results */
-static void xb_fill_results(const xb_status *hs, uint32_t nrels, kern_exec_results *results)
+void xb_fill_results(const xb_status *hs, uint32_t nrels, kern_exec_results *results)
 {
     if (!results)
         return;
@@ -3596,7 +3442,7 @@ static void xb_fill_results(const xb_status *hs, uint32_t nrels, kern_exec_resul
 
 /* add a finished launch's statistics (status hs) to the session and to
  * *results */
-static void xb_account_status(xpuB200Session *s, const xb_status *hs, kern_exec_results *results)
+void xb_account_status(xpuB200Session *s, const xb_status *hs, kern_exec_results *results)
 {
     s->total_raw += hs->nitems_raw;
     s->total_in += hs->nitems_in;
@@ -3661,8 +3507,8 @@ static bool xb_groups_may_grow(const xpuB200Session *s)
     return true;
 }
 
-static int xb_run(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks, uint64_t nunits,
-                  uint32_t format, kern_exec_results *results, kern_errorbuf *err, bool timed = false)
+int xb_run(xpuB200Session *s, const xb_task *d_tasks, uint32_t ntasks, uint64_t nunits,
+                  uint32_t format, kern_exec_results *results, kern_errorbuf *err, bool timed)
 {
     cudaStream_t st = s->stream;
     /* warps look for a growth request only where one can come */
@@ -4556,1408 +4402,6 @@ xpuB200FinalParts(xpuB200Session *s, uint32_t nparts, void *parts_dev, uint64_t 
         }
     }
     cleanup();
-    return 0;
-}
-
-/* ----------------------------------------------------------------
- * prepared batches: many device-resident chunks in one persistent launch
- * ---------------------------------------------------------------- */
-struct xpuB200Batch {
-    xpuB200Session *sess;
-    xb_task        *d_tasks;
-    uint32_t        ntasks;
-    uint64_t        nunits;
-    uint32_t        format;
-    uint64_t        bytes;          /* sum of chunk lengths */
-    uint64_t        rows;           /* rows (ARROW/ROW) or pages (BLOCK) */
-};
-
-extern "C" int
-xpuB200BatchCreate(xpuB200Session *s, const kern_data_store *const *kds_dev, uint32_t nchunks,
-                   xpuB200Batch **p_batch, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    *p_batch = nullptr;
-    if (!s || !kds_dev || nchunks == 0)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid batch arguments");
-    std::lock_guard<std::mutex> g(s->lock);
-    if (s->h_plan->has_proj)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR,
-                      "the session projects rows into kds_dst: use xpuB200ExecTaskDst");
-    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    std::vector<xb_task> tasks(nchunks);
-    std::vector<char> first_head;
-    uint64_t base = 0, bytes = 0, rows = 0;
-    uint32_t format = 0;
-    for (uint32_t i = 0; i < nchunks; i++) {
-        kern_data_store head;
-        if (((uintptr_t)kds_dev[i] & 7) != 0)
-            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "chunk %u is not 8-byte aligned", i);
-        XB_CUDA(cudaMemcpy(&head, kds_dev[i], offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
-        std::vector<char> hb(KDS_HEAD_LENGTH(&head));
-        XB_CUDA(cudaMemcpy(hb.data(), kds_dev[i], hb.size(), cudaMemcpyDeviceToHost), err);
-        const kern_data_store *h = (const kern_data_store *)hb.data();
-        int rc = xb_check_kds(h, err);
-        if (rc) return rc;
-        if (i == 0) {
-            first_head = hb;
-            format = (uint32_t)h->format;
-            xb_note_layout(s, h);
-        } else {
-            /* one launch decodes every chunk with the same column layout */
-            const kern_data_store *f = (const kern_data_store *)first_head.data();
-            if ((uint32_t)h->format != format || h->ncols != f->ncols ||
-                (h->format != KDS_FORMAT_ARROW &&
-                 memcmp(h->colmeta, f->colmeta, sizeof(kern_colmeta) * h->ncols) != 0))
-                return XB_ERR(err, ERRCODE_DEVICE_ERROR, "chunk %u of the batch has another layout", i);
-        }
-        tasks[i].kds = kds_dev[i];
-        tasks[i].unit_base = base;
-        tasks[i].nunits = xb_chunk_units(h);
-        tasks[i].format = format;
-        base += tasks[i].nunits;
-        bytes += h->length;
-        rows += h->nitems;
-    }
-    xpuB200Batch *b = new xpuB200Batch();
-    b->sess = s;
-    b->ntasks = nchunks;
-    b->nunits = base;
-    b->format = format;
-    b->bytes = bytes;
-    b->rows = rows;
-    if (cudaMalloc((void **)&b->d_tasks, sizeof(xb_task) * nchunks) != cudaSuccess) {
-        delete b;
-        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for the batch");
-    }
-    cudaMemcpy(b->d_tasks, tasks.data(), sizeof(xb_task) * nchunks, cudaMemcpyHostToDevice);
-    *p_batch = b;
-    return 0;
-}
-
-extern "C" int
-xpuB200BatchExec(xpuB200Batch *b, kern_exec_results *results, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!b)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid batch");
-    xpuB200Session *s = b->sess;
-    std::lock_guard<std::mutex> g(s->lock);
-    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    s->in_batch = true;
-    int rc = xb_run(s, b->d_tasks, b->ntasks, b->nunits, b->format, results, err);
-    s->in_batch = false;
-    return rc;
-}
-
-extern "C" int
-xpuB200BatchTime(xpuB200Batch *b, int niters, double *p_msec, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    xpuB200Session *s = b->sess;
-    std::lock_guard<std::mutex> g(s->lock);
-    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    float total = 0.0f;
-    for (int i = 0; i < niters; i++) {
-        s->in_batch = true;
-        int rc = xb_run(s, b->d_tasks, b->ntasks, b->nunits, b->format, nullptr, err, true);
-        s->in_batch = false;
-        if (rc) return rc;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-        total += ms;
-    }
-    *p_msec = niters > 0 ? total / niters : 0.0;
-    return 0;
-}
-
-/* the session's group table and statistics back to their state after
- * OpenSession; session lock held */
-static void xb_reset_groups(xpuB200Session *s)
-{
-    cudaStream_t st = s->stream;
-    if (s->h_plan->has_groupby) {
-        cudaMemsetAsync(s->h_gt.entries, 0, (s->h_gt.cap_mask + 1) * s->h_plan->gent_size, st);
-        if (s->h_gt.dump)
-            cudaMemsetAsync(s->h_gt.dump, 0, s->h_gt.dump_cap * s->h_plan->gent_size, st);
-        s->h_gt.nused = 0;
-        s->h_gt.arena_used = 0;
-        s->h_gt.overflow = 0;
-        s->h_gt.grow = 0;
-        s->h_gt.dump_used = 0;
-        s->h_gt.soft_cap = (s->h_gt.cap_mask + 1) / 2;
-        cudaMemcpyAsync(s->d_gt, &s->h_gt, sizeof(xb_gtable), cudaMemcpyHostToDevice, st);
-    }
-    cudaMemsetAsync(s->d_status, 0, sizeof(xb_status), st);
-    cudaStreamSynchronize(st);
-    s->total_raw = s->total_in = s->total_out = 0;
-    for (uint32_t d = 0; d <= XB_MAX_DEPTH; d++)
-        s->total_depth[d] = 0;
-}
-
-extern "C" int
-xpuB200BatchTune(xpuB200Batch *b, uint32_t flags, char *report, size_t report_len, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!b || flags != 0)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid BatchTune arguments");
-    xpuB200Session *s = b->sess;
-    xb_sched_drain_session(s);
-    std::lock_guard<std::mutex> g(s->lock);
-    if (s->total_raw != 0)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "tune a session before it executes chunks");
-    XB_CUDA(cudaSetDevice(s->dev->dindex), err);
-    s->tune_looked_up = true;               /* measured here, not adopted */
-    const xb_plan *plan = s->h_plan;
-    const uint32_t fmt = b->format;
-    bool gid = false;
-    for (uint32_t d = 1; d <= plan->nrels; d++)
-        gid |= plan->inner[d].gid_on != 0;
-    const uint32_t sm0 = s->sm_cap_default;
-    /* group ids index the shared table directly: its size is then fixed */
-    std::vector<uint32_t> sms;
-    if (!gid && plan->has_groupby && sm0 > 0) {
-        if ((size_t)sm0 * 2 * plan->gent_size <= 48 * 1024)
-            sms.push_back(sm0 * 2);
-        sms.push_back(0);
-    }
-    std::vector<int> minbs;
-    if (s->jit_enabled)
-        minbs = {2, 3, 4, 6, 8};
-    else
-        minbs = {0};
-    struct cand { int minb; uint32_t sm; double ms; const char *kernel; };
-    std::vector<cand> done;
-    int rc = 0;
-    auto measure = [&](int minb, uint32_t smc) -> int {
-        s->jit_minb = minb;
-        if (xb_set_sm_cap(s, smc) != 0)
-            return 1;                       /* does not fit: skipped */
-        double best = 1e30;
-        for (int r = 0; r < 3 && rc == 0; r++) {      /* the first run builds and warms */
-            xb_reset_groups(s);
-            s->in_batch = true;
-            rc = xb_run(s, b->d_tasks, b->ntasks, b->nunits, fmt, nullptr, err, true);
-            s->in_batch = false;
-            if (rc) break;
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-            if (r > 0 && ms < best) best = ms;
-        }
-        if (rc)
-            return -1;
-        if (minb > 0 && !s->jit_fn[fmt])
-            return 1;                       /* the specialised kernel was not built */
-        done.push_back({minb, smc, best, s->jit_fn[fmt] ? "jit" : "vm"});
-        return 0;
-    };
-    /* coordinate search: CTAs per SM at the default table, then the table */
-    for (int m : minbs)
-        if (measure(m, sm0) < 0) break;
-    if (rc == 0 && !done.empty()) {
-        int bm = done[0].minb;
-        double bt = done[0].ms;
-        for (const cand &c : done)
-            if (c.ms < bt) { bt = c.ms; bm = c.minb; }
-        for (uint32_t c : sms)
-            if (measure(bm, c) < 0) break;
-    }
-    cand best = {0, sm0, 0.0, "none"};
-    if (rc == 0 && !done.empty()) {
-        best = done[0];
-        for (const cand &c : done)
-            if (c.ms < best.ms) best = c;
-    }
-    s->jit_minb = best.minb;
-    if (xb_set_sm_cap(s, best.sm) != 0)
-        xb_set_sm_cap(s, sm0);
-    xb_reset_groups(s);
-    s->tune_looked_up = true;
-    if (rc)
-        return rc;
-    if (done.empty())
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "no launch shape could be measured");
-    {
-        const auto key = xb_tune_key(s, fmt);
-        std::lock_guard<std::mutex> tg(g_tune_lock);
-        g_tune[key] = xb_tune_choice{best.minb, best.sm};
-        g_tune_minb[std::make_pair(std::get<0>(key), std::get<1>(key))] = best.minb;
-    }
-    if (report && report_len) {
-        std::string r = "{\"format\": \"" + std::string(1, (char)fmt) + "\", \"candidates\": [";
-        char buf[256];
-        for (size_t i = 0; i < done.size(); i++) {
-            snprintf(buf, sizeof(buf), "%s{\"ctas_per_sm\": %d, \"sm_groups\": %u, \"kernel\": \"%s\", \"ms\": %.4f}",
-                     i ? ", " : "", done[i].minb, done[i].sm, done[i].kernel, done[i].ms);
-            r += buf;
-        }
-        snprintf(buf, sizeof(buf), "], \"best\": {\"ctas_per_sm\": %d, \"sm_groups\": %u, \"ms\": %.4f}, "
-                 "\"default_sm_groups\": %u}", best.minb, best.sm, best.ms, sm0);
-        r += buf;
-        snprintf(report, report_len, "%s", r.c_str());
-    }
-    return 0;
-}
-
-extern "C" void
-xpuB200BatchDestroy(xpuB200Batch *b)
-{
-    if (!b) return;
-    cudaSetDevice(b->sess->dev->dindex);
-    cudaFree(b->d_tasks);
-    delete b;
-}
-
-/* ================================================================
- * mixed batches: chunk commands of many sessions in one launch
- * ================================================================ */
-/* units one CTA takes of a command before another CTA is sent to join it */
-#define XB_MIX_JOIN_UNITS   16
-
-/* one persistent launch of a mixed batch: the commands that share a kernel
- * (a specialised mixed kernel of one plan shape, or the interpreter) */
-struct xb_mix_group {
-    void           *jfn = nullptr;  /* xbj_mixed_kernel, or nullptr: xb_mixed_kernel */
-    std::vector<uint32_t> cmds;     /* command indexes */
-    std::vector<uint32_t> items;    /* work queue: command index per item */
-    size_t          smem = 0;
-    int             grid = 0;
-};
-
-/* the mixed kernel a command of session s (chunk format) runs on */
-static void *xb_mix_kernel_of(xpuB200Session *s, uint32_t format, bool wait = true)
-{
-    std::lock_guard<std::mutex> g(s->lock);
-    return xb_session_jit(s, format, wait) ? s->jit_mixfn[format] : nullptr;
-}
-
-/* split commands into launches by kernel and build each work queue:
- * largest command first, listed once per XB_MIX_JOIN_UNITS of its units
- * (at most once per CTA) */
-static int xb_mix_plan(xpuB200Device *dev, const std::vector<xpuB200Session *> &sess,
-                       const std::vector<uint32_t> &formats, const std::vector<uint64_t> &units,
-                       std::vector<xb_mix_group> &groups, kern_errorbuf *err, bool wait = true)
-{
-    groups.clear();
-    for (uint32_t i = 0; i < sess.size(); i++) {
-        void *k = xb_mix_kernel_of(sess[i], formats[i], wait);
-        if (formats[i] < 256)
-            sess[i]->ran_kind[formats[i]] = k ? 'j' : 'v';
-        size_t g = 0;
-        while (g < groups.size() && groups[g].jfn != k)
-            g++;
-        if (g == groups.size()) {
-            groups.emplace_back();
-            groups.back().jfn = k;
-        }
-        groups[g].cmds.push_back(i);
-        const size_t sm = k ? sess[i]->jit_smem_fmt[formats[i]] : sess[i]->smem_bytes;
-        if (sm > groups[g].smem)
-            groups[g].smem = sm;
-    }
-    for (xb_mix_group &g : groups) {
-        const size_t st = g.jfn ? xb_jit_static_smem(g.jfn) : sizeof(XbExecArgs);
-        if (g.smem + st + 16 > dev->smem_optin)
-            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch needs %zu bytes of shared memory", g.smem);
-        int per_sm = 0;
-        if (g.jfn)
-            xb_jit_occupancy(g.jfn, XB_BLOCK, g.smem, &per_sm);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xb_mixed_kernel, XB_BLOCK, g.smem);
-        if (per_sm < 1)
-            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed kernel does not fit on an SM (%zu bytes)", g.smem);
-        g.grid = per_sm * dev->nsm;
-        std::vector<uint32_t> order(g.cmds);
-        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return units[a] > units[b]; });
-        for (uint32_t i : order) {
-            uint64_t k = (units[i] + XB_MIX_JOIN_UNITS - 1) / XB_MIX_JOIN_UNITS;
-            k = k < 1 ? 1 : (k > (uint64_t)g.grid ? g.grid : k);
-            for (uint64_t j = 0; j < k; j++)
-                g.items.push_back(i);
-        }
-    }
-    return 0;
-}
-
-/* launch one group of a mixed batch on a stream */
-static int xb_mix_launch(const xb_mix_group &g, const XbMixArgs &ma, cudaStream_t stream, kern_errorbuf *err)
-{
-    if (g.jfn) {
-        XbMixArgs a = ma;
-        if (xb_jit_launch(g.jfn, g.grid, XB_BLOCK, g.smem, (void *)stream, &a) != 0)
-            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "specialised mixed kernel launch failed");
-    } else {
-        xb_mixed_kernel<<<g.grid, XB_BLOCK, g.smem, stream>>>(ma);
-    }
-    cudaError_t rc = cudaGetLastError();
-    if (rc != cudaSuccess)
-        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed launch: %s", cudaGetErrorString(rc));
-    return 0;
-}
-
-struct xpuB200Mix {
-    xpuB200Device  *dev;
-    uint32_t        ncmds = 0;
-    std::vector<xpuB200Session *> sess;
-    std::vector<xb_mix_group> groups;
-    xb_task        *d_tasks = nullptr;
-    XbExecArgs     *d_cmds = nullptr;
-    uint32_t       *d_items = nullptr;
-    uint32_t        nitems = 0;
-    uint32_t       *d_cursor = nullptr;     /* one per group, 32 bytes apart */
-    xb_status      *d_status = nullptr;
-    xb_status      *h_status = nullptr;     /* pinned */
-    cudaStream_t    stream = nullptr;
-    std::vector<cudaStream_t> aux;          /* a branch per further group */
-    std::vector<cudaEvent_t> forks, joins;
-    cudaGraph_t     graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    cudaEvent_t     ev0 = nullptr, ev1 = nullptr;
-    uint64_t        bytes = 0, units = 0;
-};
-
-static void xb_mix_free(xpuB200Mix *m)
-{
-    if (!m) return;
-    cudaSetDevice(m->dev->dindex);
-    if (m->gexec) cudaGraphExecDestroy(m->gexec);
-    if (m->graph) cudaGraphDestroy(m->graph);
-    if (m->ev0) cudaEventDestroy(m->ev0);
-    if (m->ev1) cudaEventDestroy(m->ev1);
-    for (cudaEvent_t e : m->forks) cudaEventDestroy(e);
-    for (cudaEvent_t e : m->joins) cudaEventDestroy(e);
-    for (cudaStream_t a : m->aux) cudaStreamDestroy(a);
-    if (m->stream) cudaStreamDestroy(m->stream);
-    cudaFree(m->d_tasks);
-    cudaFree(m->d_cmds);
-    cudaFree(m->d_items);
-    cudaFree(m->d_cursor);
-    cudaFree(m->d_status);
-    if (m->h_status) cudaFreeHost(m->h_status);
-    delete m;
-}
-
-extern "C" int
-xpuB200MixCreate(xpuB200Device *dev, uint32_t ncmds, xpuB200Session *const *sess,
-                 const kern_data_store *const *kds_dev, xpuB200Mix **p_mix, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    *p_mix = nullptr;
-    if (!dev || !sess || !kds_dev || ncmds == 0)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid mixed batch arguments");
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    std::vector<xb_task> tasks(ncmds);
-    std::vector<uint64_t> units(ncmds);
-    std::vector<uint32_t> formats(ncmds);
-    uint64_t bytes = 0, total_units = 0;
-    for (uint32_t i = 0; i < ncmds; i++) {
-        xpuB200Session *s = sess[i];
-        if (!s || s->dev != dev)
-            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "command %u: no session on this GPU", i);
-        if (s->h_plan->has_proj)
-            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "command %u: projection sessions run through xpuB200ExecTaskDst", i);
-        if (((uintptr_t)kds_dev[i] & 7) != 0)
-            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "command %u: chunk is not 8-byte aligned", i);
-        kern_data_store head;
-        XB_CUDA(cudaMemcpy(&head, kds_dev[i], offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
-        std::vector<char> hb(KDS_HEAD_LENGTH(&head));
-        XB_CUDA(cudaMemcpy(hb.data(), kds_dev[i], hb.size(), cudaMemcpyDeviceToHost), err);
-        const kern_data_store *h = (const kern_data_store *)hb.data();
-        int rc = xb_check_kds(h, err);
-        if (rc) return rc;
-        {
-            std::lock_guard<std::mutex> g(s->lock);
-            xb_note_layout(s, h);
-        }
-        tasks[i].kds = kds_dev[i];
-        tasks[i].unit_base = 0;
-        tasks[i].nunits = xb_chunk_units(h);
-        tasks[i].format = (uint32_t)h->format;
-        units[i] = tasks[i].nunits;
-        formats[i] = tasks[i].format;
-        total_units += units[i];
-        bytes += h->length;
-    }
-    xpuB200Mix *m = new xpuB200Mix();
-    m->dev = dev;
-    m->ncmds = ncmds;
-    m->sess.assign(sess, sess + ncmds);
-    m->bytes = bytes;
-    m->units = total_units;
-    int rc = xb_mix_plan(dev, m->sess, formats, units, m->groups, err);
-    if (rc) {
-        xb_mix_free(m);
-        return rc;
-    }
-    const size_t ng = m->groups.size();
-    std::vector<uint32_t> items;
-    std::vector<size_t> item_off;
-    for (const xb_mix_group &g : m->groups) {
-        item_off.push_back(items.size());
-        items.insert(items.end(), g.items.begin(), g.items.end());
-    }
-    m->nitems = (uint32_t)items.size();
-    auto fail = [&](const char *what) {
-        xb_mix_free(m);
-        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "mixed batch: %s", what);
-    };
-    if (cudaMalloc((void **)&m->d_tasks, sizeof(xb_task) * ncmds) != cudaSuccess ||
-        cudaMalloc((void **)&m->d_cmds, sizeof(XbExecArgs) * ncmds) != cudaSuccess ||
-        cudaMalloc((void **)&m->d_items, sizeof(uint32_t) * items.size()) != cudaSuccess ||
-        cudaMalloc((void **)&m->d_cursor, 32 * ng) != cudaSuccess ||
-        cudaMalloc((void **)&m->d_status, sizeof(xb_status) * ncmds) != cudaSuccess ||
-        cudaMallocHost((void **)&m->h_status, sizeof(xb_status) * ncmds) != cudaSuccess)
-        return fail("out of memory");
-    std::vector<XbExecArgs> cmds(ncmds);
-    for (uint32_t i = 0; i < ncmds; i++) {
-        xpuB200Session *s = sess[i];
-        XbExecArgs &a = cmds[i];
-        memset(&a, 0, sizeof(a));
-        a.plan = s->d_plan;
-        a.plan_bytes = s->plan_bytes;
-        a.tasks = m->d_tasks + i;
-        a.ntasks = 1;
-        a.nunits = tasks[i].nunits;
-        a.format = tasks[i].format;
-        a.sm_cap = s->sm_cap;
-        a.warp_bytes = s->warp_bytes;
-        a.gt = s->d_gt;
-        a.st = m->d_status + i;
-        a.dyn_only = 1;
-    }
-    if (cudaMemcpy(m->d_tasks, tasks.data(), sizeof(xb_task) * ncmds, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(m->d_cmds, cmds.data(), sizeof(XbExecArgs) * ncmds, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(m->d_items, items.data(), sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail("upload failed");
-    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&m->ev0) != cudaSuccess || cudaEventCreate(&m->ev1) != cudaSuccess)
-        return fail("stream setup failed");
-    for (size_t g = 1; g < ng; g++) {
-        cudaStream_t a;
-        cudaEvent_t f, j;
-        if (cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) != cudaSuccess)
-            return fail("stream setup failed");
-        m->aux.push_back(a);
-        if (cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess)
-            return fail("event setup failed");
-        m->forks.push_back(f);
-        if (cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess)
-            return fail("event setup failed");
-        m->joins.push_back(j);
-    }
-    /* one run = clear the statuses and the queue cursors, one persistent
-     * launch per kernel group (concurrent branches), the statuses back to
-     * the host: captured once, replayed */
-    if (cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return fail("stream capture failed");
-    kern_errorbuf lerr;
-    int lrc = 0;
-    cudaMemsetAsync(m->d_status, 0, sizeof(xb_status) * ncmds, m->stream);
-    cudaMemsetAsync(m->d_cursor, 0, 32 * ng, m->stream);
-    for (size_t g = 1; g < ng; g++) {
-        cudaEventRecord(m->forks[g - 1], m->stream);
-        cudaStreamWaitEvent(m->aux[g - 1], m->forks[g - 1], 0);
-    }
-    for (size_t g = 0; g < ng && !lrc; g++) {
-        XbMixArgs ma;
-        ma.cmds = m->d_cmds;
-        ma.items = m->d_items + item_off[g];
-        ma.nitems = (uint32_t)m->groups[g].items.size();
-        ma.cursor = m->d_cursor + 8 * g;
-        lrc = xb_mix_launch(m->groups[g], ma, g == 0 ? m->stream : m->aux[g - 1], &lerr);
-    }
-    for (size_t g = 1; g < ng; g++) {
-        cudaEventRecord(m->joins[g - 1], m->aux[g - 1]);
-        cudaStreamWaitEvent(m->stream, m->joins[g - 1], 0);
-    }
-    cudaMemcpyAsync(m->h_status, m->d_status, sizeof(xb_status) * ncmds, cudaMemcpyDeviceToHost, m->stream);
-    cudaError_t crc = cudaStreamEndCapture(m->stream, &m->graph);
-    if (lrc) {
-        if (err) *err = lerr;
-        xb_mix_free(m);
-        return lrc;
-    }
-    if (crc != cudaSuccess || cudaGraphInstantiate(&m->gexec, m->graph, 0) != cudaSuccess)
-        return fail("graph capture failed");
-    *p_mix = m;
-    return 0;
-}
-
-/* lock the distinct sessions of a mixed batch, in address order */
-static std::vector<std::unique_lock<std::mutex>> xb_mix_lock(xpuB200Mix *m)
-{
-    std::vector<xpuB200Session *> u(m->sess);
-    std::sort(u.begin(), u.end());
-    u.erase(std::unique(u.begin(), u.end()), u.end());
-    std::vector<std::unique_lock<std::mutex>> locks;
-    for (xpuB200Session *s : u)
-        locks.emplace_back(s->lock);
-    return locks;
-}
-
-extern "C" int
-xpuB200MixExec(xpuB200Mix *m, kern_exec_results *const *results, kern_errorbuf *errs)
-{
-    if (!m)
-        return ERRCODE_DEVICE_ERROR;
-    for (uint32_t i = 0; errs && i < m->ncmds; i++)
-        xb_clear_error(&errs[i]);
-    auto locks = xb_mix_lock(m);
-    kern_errorbuf *e0 = errs;
-    XB_CUDA(cudaSetDevice(m->dev->dindex), e0);
-    XB_CUDA(cudaGraphLaunch(m->gexec, m->stream), e0);
-    XB_CUDA(cudaStreamSynchronize(m->stream), e0);
-    int first = 0;
-    for (uint32_t i = 0; i < m->ncmds; i++) {
-        const xb_status *hs = &m->h_status[i];
-        if (hs->errcode) {
-            int rc = xb_set_error(errs ? &errs[i] : nullptr, hs->errcode, "xb_mixed_kernel", hs->lineno,
-                                  "%s", xb_msg_text(hs->msg_id));
-            if (!first) first = rc;
-            continue;
-        }
-        xb_account_status(m->sess[i], hs, results ? results[i] : nullptr);
-    }
-    return first;
-}
-
-extern "C" int
-xpuB200MixTime(xpuB200Mix *m, int niters, double *p_msec, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!m)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid mixed batch");
-    auto locks = xb_mix_lock(m);
-    XB_CUDA(cudaSetDevice(m->dev->dindex), err);
-    float total = 0.0f;
-    for (int it = 0; it < niters; it++) {
-        XB_CUDA(cudaEventRecord(m->ev0, m->stream), err);
-        XB_CUDA(cudaGraphLaunch(m->gexec, m->stream), err);
-        XB_CUDA(cudaEventRecord(m->ev1, m->stream), err);
-        XB_CUDA(cudaStreamSynchronize(m->stream), err);
-        for (uint32_t i = 0; i < m->ncmds; i++)
-            if (m->h_status[i].errcode)
-                return xb_set_error(err, m->h_status[i].errcode, "xb_mixed_kernel", m->h_status[i].lineno,
-                                    "command %u: %s", i, xb_msg_text(m->h_status[i].msg_id));
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, m->ev0, m->ev1);
-        total += ms;
-    }
-    *p_msec = niters > 0 ? total / niters : 0.0;
-    return 0;
-}
-
-extern "C" int
-xpuB200MixInfo(const xpuB200Mix *m, uint64_t *p_bytes, uint64_t *p_units, uint32_t *p_items,
-               uint32_t *p_launches, uint32_t *p_specialised)
-{
-    if (!m) return ERRCODE_DEVICE_ERROR;
-    if (p_bytes) *p_bytes = m->bytes;
-    if (p_units) *p_units = m->units;
-    if (p_items) *p_items = m->nitems;
-    if (p_launches) *p_launches = (uint32_t)m->groups.size();
-    if (p_specialised) {
-        uint32_t n = 0;
-        for (const xb_mix_group &g : m->groups)
-            if (g.jfn) n += (uint32_t)g.cmds.size();
-        *p_specialised = n;
-    }
-    return 0;
-}
-
-extern "C" void
-xpuB200MixDestroy(xpuB200Mix *m)
-{
-    xb_mix_free(m);
-}
-
-/* ================================================================
- * serving: asynchronous chunk commands with continuous batching
- * ================================================================
- *
- * xpuB200Submit queues a chunk command of any session; the scheduler keeps
- * up to XB_SLOTS launches in flight on their own streams.  Whenever a slot
- * is free (checked on every Submit and Poll), the queued commands are
- * admitted in arrival order while their staging bytes fit the admission
- * budget: a large command of a session with a specialised kernel runs
- * alone on it, the small ones go together into one mixed launch
- * (xb_mixed_kernel).  Commands that arrive while others are on the GPU are
- * admitted as slots and memory free up, so their work overlaps on the
- * device.  A finished command's statistics are added to its session and
- * kept for xpuB200Poll; its groups are in the session's group table.
- */
-/* the device's free and total memory, and the reserve admission keeps */
-static void xb_mem_info(xpuB200Device *dev, uint64_t *p_free, uint64_t *p_total, uint64_t *p_reserve)
-{
-    size_t fr = 0, tot = 0;
-    cudaSetDevice(dev->dindex);
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-        cudaGetLastError();
-        fr = tot = 0;
-    }
-    *p_free = fr;
-    *p_total = tot;
-    const uint64_t r = tot / 20;
-    *p_reserve = r > (1ULL << 30) ? r : (1ULL << 30);
-}
-
-#define XB_SLOTS            4       /* launches in flight per GPU */
-#define XB_SLOT_CMDS        256     /* commands of one mixed launch */
-#define XB_ALONE_UNITS      256     /* commands of this many units run alone */
-
-struct xb_cmd {
-    uint64_t        ticket;
-    xpuB200Session *s;
-    const kern_data_store *kds;     /* the caller's chunk */
-    int             on_device;
-    uint64_t        length;
-    uint64_t        shift;          /* staging offset that aligns heap pages */
-    uint64_t        units;
-    uint32_t        format;
-    const kern_data_store *d_kds;   /* the chunk on the device, once launched */
-};
-
-struct xb_done {
-    int             rc;             /* 0, or the command's error code */
-    kern_errorbuf   err;
-    xb_status       st;
-    uint32_t        nrels;
-};
-
-struct xb_slot {
-    cudaStream_t    stream = nullptr;
-    cudaEvent_t     done = nullptr;
-    bool            busy = false;
-    bool            alone = false;
-    std::vector<xb_cmd> cmds;
-    uint64_t        staged = 0;     /* admission bytes held by this launch */
-    char           *d_stage = nullptr;
-    uint64_t        stage_cap = 0;
-    xb_status      *d_status = nullptr;
-    xb_status      *h_status = nullptr;     /* pinned */
-    xb_task        *d_tasks = nullptr, *h_tasks = nullptr;
-    XbExecArgs     *d_cmds = nullptr, *h_cmds = nullptr;
-    uint32_t       *d_items = nullptr, *h_items = nullptr;
-    uint32_t        items_cap = 0;
-    uint32_t       *d_cursor = nullptr;
-};
-
-struct xb_sched {
-    std::mutex      lock;
-    uint64_t        next_ticket = 1;
-    std::deque<xb_cmd> pending;
-    xb_slot         slot[XB_SLOTS];
-    std::unordered_map<uint64_t, xb_done> done;
-    uint64_t        admit_bytes = 0;
-    uint64_t        inflight_bytes = 0;
-    uint32_t        alone_units = XB_ALONE_UNITS;
-    int             mix_grid_per_sm[2] = {0, 0};
-};
-
-static void xb_slot_free(xb_slot &sl)
-{
-    if (sl.stream) { cudaStreamSynchronize(sl.stream); cudaStreamDestroy(sl.stream); }
-    if (sl.done) cudaEventDestroy(sl.done);
-    cudaFree(sl.d_stage);
-    cudaFree(sl.d_status);
-    cudaFree(sl.d_tasks);
-    cudaFree(sl.d_cmds);
-    cudaFree(sl.d_items);
-    cudaFree(sl.d_cursor);
-    if (sl.h_status) cudaFreeHost(sl.h_status);
-    if (sl.h_tasks) cudaFreeHost(sl.h_tasks);
-    if (sl.h_cmds) cudaFreeHost(sl.h_cmds);
-    if (sl.h_items) cudaFreeHost(sl.h_items);
-    sl = xb_slot();
-}
-
-static int xb_sched_init(xpuB200Device *dev, kern_errorbuf *err)
-{
-    if (dev->sched)
-        return 0;
-    xb_sched *q = new xb_sched();
-    q->admit_bytes = XPU_B200_ADMIT_FREE_HBM;
-    for (int i = 0; i < XB_SLOTS; i++) {
-        xb_slot &sl = q->slot[i];
-        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_status, sizeof(xb_status) * XB_SLOT_CMDS) != cudaSuccess ||
-            cudaMallocHost((void **)&sl.h_status, sizeof(xb_status) * XB_SLOT_CMDS) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_tasks, sizeof(xb_task) * XB_SLOT_CMDS) != cudaSuccess ||
-            cudaMallocHost((void **)&sl.h_tasks, sizeof(xb_task) * XB_SLOT_CMDS) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_cmds, sizeof(XbExecArgs) * XB_SLOT_CMDS) != cudaSuccess ||
-            cudaMallocHost((void **)&sl.h_cmds, sizeof(XbExecArgs) * XB_SLOT_CMDS) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_cursor, 16) != cudaSuccess) {
-            for (int j = 0; j <= i; j++)
-                xb_slot_free(q->slot[j]);
-            delete q;
-            return XB_ERR(err, ERRCODE_DEVICE_FATAL, "cannot set up the command scheduler");
-        }
-    }
-    dev->sched = q;
-    return 0;
-}
-
-/* finish the launch of slot sl if its work is done; sched lock held */
-static void xb_sched_retire(xb_sched *q, xb_slot &sl, bool wait)
-{
-    if (!sl.busy)
-        return;
-    cudaError_t rc = wait ? cudaEventSynchronize(sl.done) : cudaEventQuery(sl.done);
-    if (rc == cudaErrorNotReady)
-        return;
-    for (size_t i = 0; i < sl.cmds.size(); i++) {
-        const xb_cmd &c = sl.cmds[i];
-        xb_done d;
-        memset(&d, 0, sizeof(d));
-        d.nrels = c.s->h_plan->nrels;
-        if (rc != cudaSuccess) {
-            d.rc = xb_set_error(&d.err, ERRCODE_DEVICE_FATAL, "xpuB200Poll", __LINE__, "%s",
-                                cudaGetErrorString(rc));
-        } else {
-            d.st = sl.h_status[i];
-            if (d.st.errcode) {
-                d.rc = xb_set_error(&d.err, d.st.errcode, sl.alone ? "xb_exec_kernel" : "xb_mixed_kernel",
-                                    d.st.lineno, "%s", xb_msg_text(d.st.msg_id));
-            } else {
-                std::lock_guard<std::mutex> g(c.s->lock);
-                xb_account_status(c.s, &d.st, nullptr);
-            }
-        }
-        c.s->sched_refs--;
-        q->done[c.ticket] = d;
-    }
-    q->inflight_bytes -= sl.staged;
-    sl.staged = 0;
-    sl.cmds.clear();
-    sl.busy = false;
-}
-
-/* copy the host chunks of cmds into the slot's staging buffer; sched lock held */
-static int xb_sched_stage(xb_slot &sl, std::vector<xb_cmd> &cmds, kern_errorbuf *err)
-{
-    uint64_t need = 0;
-    for (const xb_cmd &c : cmds)
-        if (!c.on_device)
-            need += PGSTROM_TYPEALIGN(256, c.length + c.shift);
-    if (need > sl.stage_cap) {
-        cudaStreamSynchronize(sl.stream);
-        cudaFree(sl.d_stage);
-        sl.d_stage = nullptr;
-        sl.stage_cap = 0;
-        uint64_t cap = need < (64ULL << 20) ? (64ULL << 20) : need;
-        XB_CUDA(cudaMalloc((void **)&sl.d_stage, cap), err);
-        sl.stage_cap = cap;
-    }
-    uint64_t off = 0;
-    for (xb_cmd &c : cmds) {
-        if (c.on_device) {
-            c.d_kds = c.kds;
-            continue;
-        }
-        XB_CUDA(cudaMemcpyAsync(sl.d_stage + off + c.shift, c.kds, c.length, cudaMemcpyHostToDevice, sl.stream), err);
-        c.d_kds = (const kern_data_store *)(sl.d_stage + off + c.shift);
-        off += PGSTROM_TYPEALIGN(256, c.length + c.shift);
-    }
-    return 0;
-}
-
-/* launch the next admitted commands on slot sl; sched lock held */
-static int xb_sched_launch(xpuB200Device *dev, xb_sched *q, xb_slot &sl, kern_errorbuf *err)
-{
-    std::vector<xb_cmd> take;
-    uint64_t bytes = 0;
-    /* admission: by the device's free memory (the slot's staging buffer
-     * is reusable), or against a fixed budget for the bytes in flight */
-    uint64_t room;
-    if (q->admit_bytes == XPU_B200_ADMIT_FREE_HBM) {
-        uint64_t fr = 0, tot = 0, reserve = 0;
-        xb_mem_info(dev, &fr, &tot, &reserve);
-        room = (fr > reserve ? fr - reserve : 0) + sl.stage_cap;
-    } else {
-        room = q->admit_bytes > q->inflight_bytes ? q->admit_bytes - q->inflight_bytes : 0;
-    }
-    const xb_cmd &f = q->pending.front();
-    const bool alone = f.units >= q->alone_units && f.s->jit_enabled;
-    void *kern = alone ? nullptr : xb_mix_kernel_of(f.s, f.format, false);
-    while (!q->pending.empty() && take.size() < (alone ? 1u : (size_t)XB_SLOT_CMDS)) {
-        const xb_cmd &c = q->pending.front();
-        if (!alone && c.units >= q->alone_units && c.s->jit_enabled)
-            break;                      /* a large one runs alone, in a later launch */
-        if (!alone && xb_mix_kernel_of(c.s, c.format, false) != kern)
-            break;                      /* another kernel: a launch of its own */
-        const uint64_t b = c.on_device ? 0 : c.length + c.shift + 256;
-        if (bytes + b > room && (!take.empty() || q->inflight_bytes > 0))
-            break;                      /* admission: wait for memory to free up */
-        bytes += b;
-        take.push_back(c);
-        q->pending.pop_front();
-    }
-    if (take.empty())
-        return 0;
-    sl.busy = true;
-    sl.alone = alone;
-    sl.staged = bytes;
-    q->inflight_bytes += bytes;
-    sl.cmds = take;
-    int rc = xb_sched_stage(sl, sl.cmds, err);
-    const uint32_t n = (uint32_t)sl.cmds.size();
-    if (!rc) {
-        for (uint32_t i = 0; i < n; i++) {
-            const xb_cmd &c = sl.cmds[i];
-            sl.h_tasks[i].kds = c.d_kds;
-            sl.h_tasks[i].unit_base = 0;
-            sl.h_tasks[i].nunits = c.units;
-            sl.h_tasks[i].format = c.format;
-        }
-        if (cudaMemcpyAsync(sl.d_tasks, sl.h_tasks, sizeof(xb_task) * n, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
-            cudaMemsetAsync(sl.d_status, 0, sizeof(xb_status) * n, sl.stream) != cudaSuccess)
-            rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler upload failed");
-    }
-    if (!rc && alone) {
-        xpuB200Session *s = sl.cmds[0].s;
-        std::lock_guard<std::mutex> g(s->lock);
-        rc = xb_launch_on(s, sl.d_tasks, 1, sl.cmds[0].units, sl.cmds[0].format, sl.stream, sl.d_status, err);
-    } else if (!rc) {
-        /* one mixed launch of commands that share a kernel */
-        std::vector<xpuB200Session *> ss(n);
-        std::vector<uint32_t> fm(n);
-        std::vector<uint64_t> un(n);
-        for (uint32_t i = 0; i < n; i++) {
-            ss[i] = sl.cmds[i].s;
-            fm[i] = sl.cmds[i].format;
-            un[i] = sl.cmds[i].units;
-        }
-        std::vector<xb_mix_group> groups;
-        rc = xb_mix_plan(dev, ss, fm, un, groups, err, false);
-        const xb_mix_group *g = groups.empty() ? nullptr : &groups[0];
-        if (!rc && g && g->items.size() > sl.items_cap) {
-            cudaStreamSynchronize(sl.stream);
-            cudaFree(sl.d_items);
-            if (sl.h_items) cudaFreeHost(sl.h_items);
-            sl.d_items = nullptr;
-            sl.h_items = nullptr;
-            sl.items_cap = 0;
-            const uint32_t cap = (uint32_t)g->items.size() * 2;
-            if (cudaMalloc((void **)&sl.d_items, sizeof(uint32_t) * cap) != cudaSuccess ||
-                cudaMallocHost((void **)&sl.h_items, sizeof(uint32_t) * cap) != cudaSuccess)
-                rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler: out of memory for the work queue");
-            else
-                sl.items_cap = cap;
-        }
-        if (!rc && g) {
-            memcpy(sl.h_items, g->items.data(), sizeof(uint32_t) * g->items.size());
-            for (uint32_t i = 0; i < n; i++) {
-                xpuB200Session *s = sl.cmds[i].s;
-                XbExecArgs &a = sl.h_cmds[i];
-                memset(&a, 0, sizeof(a));
-                a.plan = s->d_plan;
-                a.plan_bytes = s->plan_bytes;
-                a.tasks = sl.d_tasks + i;
-                a.ntasks = 1;
-                a.nunits = sl.cmds[i].units;
-                a.format = sl.cmds[i].format;
-                a.sm_cap = s->sm_cap;
-                a.warp_bytes = s->warp_bytes;
-                a.gt = s->d_gt;
-                a.st = sl.d_status + i;
-                a.dyn_only = 1;
-            }
-            XbMixArgs ma;
-            ma.cmds = sl.d_cmds;
-            ma.items = sl.d_items;
-            ma.nitems = (uint32_t)g->items.size();
-            ma.cursor = sl.d_cursor;
-            cudaMemcpyAsync(sl.d_cmds, sl.h_cmds, sizeof(XbExecArgs) * n, cudaMemcpyHostToDevice, sl.stream);
-            cudaMemcpyAsync(sl.d_items, sl.h_items, sizeof(uint32_t) * g->items.size(), cudaMemcpyHostToDevice, sl.stream);
-            cudaMemsetAsync(sl.d_cursor, 0, 16, sl.stream);
-            rc = xb_mix_launch(*g, ma, sl.stream, err);
-        }
-    }
-    if (!rc) {
-        if (cudaMemcpyAsync(sl.h_status, sl.d_status, sizeof(xb_status) * n, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
-            cudaEventRecord(sl.done, sl.stream) != cudaSuccess)
-            rc = XB_ERR(err, ERRCODE_DEVICE_FATAL, "scheduler: status read-back failed");
-    }
-    if (rc) {
-        /* the launch did not happen: its commands finish with the error */
-        cudaStreamSynchronize(sl.stream);
-        for (const xb_cmd &c : sl.cmds) {
-            xb_done d;
-            memset(&d, 0, sizeof(d));
-            d.rc = rc;
-            if (err) d.err = *err;
-            d.nrels = c.s->h_plan->nrels;
-            c.s->sched_refs--;
-            q->done[c.ticket] = d;
-        }
-        q->inflight_bytes -= sl.staged;
-        sl.staged = 0;
-        sl.cmds.clear();
-        sl.busy = false;
-    }
-    return rc;
-}
-
-/* retire finished launches and launch admitted commands; sched lock held */
-static void xb_sched_progress(xpuB200Device *dev, xb_sched *q)
-{
-    for (int i = 0; i < XB_SLOTS; i++)
-        xb_sched_retire(q, q->slot[i], false);
-    for (int i = 0; i < XB_SLOTS && !q->pending.empty(); i++) {
-        xb_slot &sl = q->slot[i];
-        if (sl.busy)
-            continue;
-        kern_errorbuf e;
-        xb_sched_launch(dev, q, sl, &e);    /* errors are recorded per command */
-    }
-}
-
-/* block until one in-flight launch finishes (one holding 'who' if given);
- * called with the lock held through lk, which is released while waiting */
-static void xb_sched_wait_one(xb_sched *q, std::unique_lock<std::mutex> &lk, const xpuB200Session *who)
-{
-    int pick = -1;
-    for (int i = 0; i < XB_SLOTS && pick < 0; i++) {
-        if (!q->slot[i].busy)
-            continue;
-        if (!who)
-            pick = i;
-        for (const xb_cmd &c : q->slot[i].cmds)
-            if (c.s == who)
-                pick = i;
-    }
-    for (int i = 0; i < XB_SLOTS && pick < 0; i++)
-        if (q->slot[i].busy)
-            pick = i;
-    if (pick < 0)
-        return;
-    cudaEvent_t ev = q->slot[pick].done;
-    lk.unlock();
-    cudaEventSynchronize(ev);
-    lk.lock();
-}
-
-static void xb_sched_drain_session(xpuB200Session *s)
-{
-    xpuB200Device *dev = s->dev;
-    xb_sched *q = dev->sched;
-    if (!q)
-        return;
-    cudaSetDevice(dev->dindex);
-    std::unique_lock<std::mutex> lk(q->lock);
-    for (;;) {
-        xb_sched_progress(dev, q);
-        if (s->sched_refs == 0)
-            break;
-        xb_sched_wait_one(q, lk, s);
-    }
-}
-
-static void xb_sched_destroy(xpuB200Device *dev)
-{
-    xb_sched *q = dev->sched;
-    if (!q)
-        return;
-    for (int i = 0; i < XB_SLOTS; i++)
-        xb_slot_free(q->slot[i]);
-    delete q;
-    dev->sched = nullptr;
-}
-
-/* the CUDA device index of a device handle, for the storage reader (xb_direct.cpp) */
-extern "C" int
-xb_device_index(const xpuB200Device *dev)
-{
-    return dev->dindex;
-}
-
-extern "C" int
-xpuB200MemInfo(xpuB200Device *dev, uint64_t *p_free, uint64_t *p_total, uint64_t *p_reserve)
-{
-    if (!dev)
-        return ERRCODE_DEVICE_ERROR;
-    uint64_t fr, tot, res;
-    xb_mem_info(dev, &fr, &tot, &res);
-    if (p_free) *p_free = fr;
-    if (p_total) *p_total = tot;
-    if (p_reserve) *p_reserve = res;
-    return 0;
-}
-
-extern "C" int
-xpuB200ServeConfig(xpuB200Device *dev, uint64_t admit_bytes, uint32_t alone_units, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!dev)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid device");
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    int rc = xb_sched_init(dev, err);
-    if (rc) return rc;
-    std::lock_guard<std::mutex> g(dev->sched->lock);
-    if (admit_bytes)
-        dev->sched->admit_bytes = admit_bytes;
-    if (alone_units)
-        dev->sched->alone_units = alone_units;
-    return 0;
-}
-
-extern "C" int
-xpuB200Submit(xpuB200Session *s, const kern_data_store *kds_src, int kds_src_on_device,
-              uint64_t *p_ticket, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!s || !kds_src || !p_ticket)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid Submit arguments");
-    if (s->h_plan->has_proj)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "projection sessions run through xpuB200ExecTaskDst");
-    xpuB200Device *dev = s->dev;
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    int rc = xb_sched_init(dev, err);
-    if (rc) return rc;
-    /* the chunk header, checked now */
-    xb_cmd c;
-    memset(&c, 0, sizeof(c));
-    std::vector<char> hb;
-    kern_data_store head;
-    if (kds_src_on_device) {
-        if (((uintptr_t)kds_src & 7) != 0)
-            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "device chunk is not 8-byte aligned");
-        XB_CUDA(cudaMemcpy(&head, kds_src, offsetof(kern_data_store, colmeta), cudaMemcpyDeviceToHost), err);
-        hb.resize(KDS_HEAD_LENGTH(&head));
-        XB_CUDA(cudaMemcpy(hb.data(), kds_src, hb.size(), cudaMemcpyDeviceToHost), err);
-    } else {
-        hb.assign((const char *)kds_src, (const char *)kds_src + KDS_HEAD_LENGTH(kds_src));
-    }
-    const kern_data_store *h = (const kern_data_store *)hb.data();
-    rc = xb_check_kds(h, err);
-    if (rc) return rc;
-    if (kds_src_on_device && h->format == KDS_FORMAT_BLOCK &&
-        (((uintptr_t)kds_src + h->block_offset) & 15) != 0)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "heap pages of a device chunk must start 16-byte aligned");
-    {
-        std::lock_guard<std::mutex> g(s->lock);
-        xb_note_layout(s, h);
-    }
-    c.s = s;
-    c.kds = kds_src;
-    c.on_device = kds_src_on_device;
-    c.length = h->length;
-    c.shift = (!kds_src_on_device && h->format == KDS_FORMAT_BLOCK) ? ((16 - (h->block_offset & 15)) & 15) : 0;
-    c.units = xb_chunk_units(h);
-    c.format = (uint32_t)h->format;
-    xb_sched *q = dev->sched;
-    std::lock_guard<std::mutex> g(q->lock);
-    c.ticket = q->next_ticket++;
-    s->sched_refs++;
-    q->pending.push_back(c);
-    xb_sched_progress(dev, q);
-    *p_ticket = c.ticket;
-    return 0;
-}
-
-extern "C" int
-xpuB200Poll(xpuB200Device *dev, uint64_t ticket, int wait, int *p_done,
-            kern_exec_results *results, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (p_done) *p_done = 0;
-    if (!dev || !dev->sched)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "no command was submitted on this device");
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    xb_sched *q = dev->sched;
-    std::unique_lock<std::mutex> lk(q->lock);
-    for (;;) {
-        xb_sched_progress(dev, q);
-        auto it = q->done.find(ticket);
-        if (it != q->done.end()) {
-            const xb_done d = it->second;
-            q->done.erase(it);
-            if (p_done) *p_done = 1;
-            if (d.rc) {
-                if (err) *err = d.err;
-                return d.rc;
-            }
-            xb_fill_results(&d.st, d.nrels, results);
-            return 0;
-        }
-        bool known = ticket > 0 && ticket < q->next_ticket;
-        if (known) {
-            known = false;
-            for (const xb_cmd &c : q->pending)
-                if (c.ticket == ticket) known = true;
-            for (int i = 0; i < XB_SLOTS && !known; i++)
-                for (const xb_cmd &c : q->slot[i].cmds)
-                    if (c.ticket == ticket) known = true;
-        }
-        if (!known)
-            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unknown ticket %llu", (unsigned long long)ticket);
-        if (!wait)
-            return 0;
-        xb_sched_wait_one(q, lk, nullptr);
-    }
-}
-
-extern "C" int
-xpuB200HandleCommand(xpuB200Device *dev, xpuB200Session **p_sess, const XpuCommand *xcmd,
-                     const kern_multirels *kmrels, uint64_t kmrels_sz,
-                     XpuCommand *resp, uint64_t resp_sz)
-{
-    kern_errorbuf ebuf;
-    int rc = 0;
-    if (!xcmd || xcmd->magic != XpuCommandMagicNumber || !resp ||
-        resp_sz < offsetof(XpuCommand, u) + sizeof(kern_errorbuf))
-        return ERRCODE_DEVICE_ERROR;
-    memset(resp, 0, offsetof(XpuCommand, u));
-    resp->magic = XpuCommandMagicNumber;
-    const uint64_t head = offsetof(XpuCommand, u);
-    switch (xcmd->tag) {
-    case XpuCommandTag__OpenSession:
-        rc = xpuB200OpenSession(dev, &xcmd->u.session, xcmd->length - head, kmrels, kmrels_sz,
-                                p_sess, &ebuf);
-        if (!rc) {
-            resp->tag = XpuCommandTag__Success;
-            resp->length = head;
-        }
-        break;
-    case XpuCommandTag__XpuTaskExec: {
-        const kern_data_store *kds = (const kern_data_store *)((const char *)xcmd + xcmd->u.task.kds_src_offset);
-        if (!*p_sess || xcmd->u.task.kds_src_offset == 0 ||
-            xcmd->u.task.kds_src_offset + sizeof(kern_data_store) > xcmd->length ||
-            xcmd->u.task.kds_src_offset + kds->length > xcmd->length) {
-            rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "malformed XpuTaskExec command");
-            break;
-        }
-        uint32_t nrels = (*p_sess)->h_plan->nrels;
-        uint64_t rsz = head + offsetof(kern_exec_results, stats) + sizeof(resp->u.results.stats[0]) * (nrels + 1);
-        if (resp_sz < rsz) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
-        memset(&resp->u.results, 0, rsz - head);
-        resp->u.results.num_rels = nrels;
-        if ((*p_sess)->h_plan->has_proj) {
-            /* the projected rows follow the results as one KDS_FORMAT_ROW
-             * chunk, cut down to header + row index + tuples like
-             * __gpuClientWriteBackOneChunk (gpu_service.c:2818-2846) */
-            const uint64_t rhead = PGSTROM_MAXALIGN(rsz);
-            if (resp_sz < rhead + 64) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
-            char *dst = (char *)resp + rhead;
-            const uint64_t len = (resp_sz - rhead) & ~7ULL;
-            uint64_t required = 0;
-            rc = xpuB200ExecTaskDst(*p_sess, kds, 0, dst, len, 0, &required, &resp->u.results, &ebuf);
-            if (rc == ERRCODE_SUSPEND_NO_SPACE) {
-                rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR,
-                            "response buffer too small for the projected rows (%llu bytes needed)",
-                            (unsigned long long)(rhead + required));
-                break;
-            }
-            if (rc) break;
-            kern_data_store *kd = (kern_data_store *)dst;
-            /* offsets from the end (row index, hash chains) stay valid */
-            const uint64_t hsz = KDS_HEAD_LENGTH(kd) + 8 * (uint64_t)kd->hash_nslots +
-                                 PGSTROM_MAXALIGN(8 * (uint64_t)kd->nitems);
-            if (kd->usage)
-                memmove(dst + hsz, dst + len - kd->usage, kd->usage);
-            kd->length = hsz + kd->usage;
-            resp->u.results.chunks_offset = (uint32_t)rhead;
-            resp->u.results.chunks_nitems = 1;
-            resp->tag = XpuCommandTag__Success;
-            resp->length = rhead + kd->length;
-            break;
-        }
-        rc = xpuB200ExecTask(*p_sess, kds, 0, &resp->u.results, &ebuf);
-        if (!rc) {
-            resp->tag = XpuCommandTag__Success;
-            resp->length = rsz;
-        }
-        break;
-    }
-    case XpuCommandTag__XpuTaskFinal: {
-        if (!*p_sess) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "XpuTaskFinal without a session"); break; }
-        uint32_t nrels = (*p_sess)->h_plan->nrels;
-        uint64_t rhead = head + PGSTROM_MAXALIGN(offsetof(kern_exec_results, stats) +
-                                                 sizeof(resp->u.results.stats[0]) * (nrels + 1));
-        if (resp_sz < rhead) { rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "response buffer too small"); break; }
-        memset(&resp->u.results, 0, rhead - head);
-        resp->u.results.num_rels = nrels;
-        uint64_t required = 0;
-        rc = xpuB200Final(*p_sess, (char *)resp + rhead, resp_sz - rhead, &required,
-                          &resp->u.results, &ebuf);
-        if (!rc) {
-            resp->tag = XpuCommandTag__Success;
-            resp->u.results.chunks_offset = (uint32_t)rhead;
-            resp->u.results.chunks_nitems = required > 0 ? 1 : 0;
-            resp->u.results.final_plan_task = true;
-            resp->length = rhead + required;
-        }
-        break;
-    }
-    default:
-        rc = XB_ERR(&ebuf, ERRCODE_DEVICE_ERROR, "unknown XpuCommand tag %u", xcmd->tag);
-        break;
-    }
-    if (rc) {
-        resp->tag = XpuCommandTag__Error;
-        resp->length = head + sizeof(kern_errorbuf);
-        memcpy(&resp->u.error, &ebuf, sizeof(kern_errorbuf));
-    }
-    return rc;
-}
-
-extern "C" int
-xpuB200DeviceAlloc(xpuB200Device *dev, uint64_t sz, void **p_dptr)
-{
-    cudaSetDevice(dev->dindex);
-    if (cudaMalloc(p_dptr, sz) != cudaSuccess) { cudaGetLastError(); return ERRCODE_DEVICE_FATAL; }
-    return 0;
-}
-
-extern "C" int
-xpuB200DeviceFree(xpuB200Device *dev, void *dptr)
-{
-    cudaSetDevice(dev->dindex);
-    return cudaFree(dptr) == cudaSuccess ? 0 : ERRCODE_DEVICE_FATAL;
-}
-
-extern "C" int
-xpuB200InnerCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!dev)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid InnerCacheConfig arguments");
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    std::lock_guard<std::mutex> g(dev->inner_lock);
-    if (max_bytes != UINT64_MAX)
-        dev->inner_budget = max_bytes;
-    xb_inner_evict_locked(dev);
-    if (p_cached_bytes)
-        *p_cached_bytes = dev->inner_bytes;
-    return 0;
-}
-
-/* ----------------------------------------------------------------
- * outer-table chunks resident in HBM across sessions
- * ---------------------------------------------------------------- */
-/* drop unused chunks, least recently used first, while the cache holds
- * more than its budget; chunk_lock held */
-static void xb_chunk_evict_locked(xpuB200Device *dev)
-{
-    while (dev->chunk_bytes > dev->chunk_budget) {
-        auto victim = dev->chunk_cache.end();
-        for (auto it = dev->chunk_cache.begin(); it != dev->chunk_cache.end(); ++it)
-            if (it->second.refs == 0 &&
-                (victim == dev->chunk_cache.end() || it->second.last_use < victim->second.last_use))
-                victim = it;
-        if (victim == dev->chunk_cache.end())
-            return;                     /* every chunk is in use */
-        cudaFreeAsync(victim->second.base, dev->stream);
-        dev->chunk_bytes -= victim->second.bytes;
-        dev->chunk_cache.erase(victim);
-    }
-}
-
-extern "C" int
-xpuB200ChunkCachePut(xpuB200Device *dev, uint64_t table_handle, uint32_t chunk_no,
-                     const kern_data_store *kds, int kds_on_device,
-                     const kern_data_store **p_kds_dev, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!dev || !kds || !p_kds_dev)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid ChunkCachePut arguments");
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    std::lock_guard<std::mutex> g(dev->chunk_lock);
-    const auto key = std::make_pair(table_handle, chunk_no);
-    auto it = dev->chunk_cache.find(key);
-    if (it != dev->chunk_cache.end()) {
-        it->second.refs++;
-        it->second.last_use = ++dev->chunk_clock;
-        *p_kds_dev = it->second.kds;
-        return 0;
-    }
-    /* the header, to place the chunk and check it */
-    std::vector<char> hb(offsetof(kern_data_store, colmeta));
-    if (kds_on_device) {
-        XB_CUDA(cudaMemcpy(hb.data(), kds, hb.size(), cudaMemcpyDeviceToHost), err);
-        const kern_data_store *h = (const kern_data_store *)hb.data();
-        hb.resize(KDS_HEAD_LENGTH(h));
-        XB_CUDA(cudaMemcpy(hb.data(), kds, hb.size(), cudaMemcpyDeviceToHost), err);
-    } else {
-        hb.assign((const char *)kds, (const char *)kds + KDS_HEAD_LENGTH(kds));
-    }
-    const kern_data_store *h = (const kern_data_store *)hb.data();
-    int rc = xb_check_kds(h, err);
-    if (rc) return rc;
-    /* heap pages start 16-byte aligned on the device */
-    const uint64_t shift = h->format == KDS_FORMAT_BLOCK ? (16 - (h->block_offset & 15)) & 15 : 0;
-    const uint64_t bytes = h->length + shift;
-    char *base = nullptr;
-    if (cudaMallocAsync((void **)&base, bytes, dev->stream) != cudaSuccess) {
-        cudaGetLastError();
-        return XB_ERR(err, ERRCODE_DEVICE_FATAL, "out of device memory for a resident chunk of %llu bytes",
-                      (unsigned long long)h->length);
-    }
-    XB_CUDA(cudaMemcpyAsync(base + shift, kds, h->length,
-                            kds_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, dev->stream), err);
-    /* the chunk is complete before any other stream reads it */
-    XB_CUDA(cudaStreamSynchronize(dev->stream), err);
-    xb_chunk_entry e;
-    e.base = base;
-    e.kds = (const kern_data_store *)(base + shift);
-    e.bytes = bytes;
-    e.refs = 1;
-    e.last_use = ++dev->chunk_clock;
-    dev->chunk_cache[key] = e;
-    dev->chunk_bytes += bytes;
-    xb_chunk_evict_locked(dev);
-    *p_kds_dev = e.kds;
-    return 0;
-}
-
-extern "C" int
-xpuB200ChunkCacheGet(xpuB200Device *dev, uint64_t table_handle, uint32_t chunk_no,
-                     const kern_data_store **p_kds_dev)
-{
-    if (!dev || !p_kds_dev)
-        return ERRCODE_DEVICE_ERROR;
-    std::lock_guard<std::mutex> g(dev->chunk_lock);
-    auto it = dev->chunk_cache.find(std::make_pair(table_handle, chunk_no));
-    if (it == dev->chunk_cache.end())
-        return 1;
-    it->second.refs++;
-    it->second.last_use = ++dev->chunk_clock;
-    *p_kds_dev = it->second.kds;
-    return 0;
-}
-
-extern "C" int
-xpuB200ChunkCacheRelease(xpuB200Device *dev, const kern_data_store *kds_dev)
-{
-    if (!dev)
-        return ERRCODE_DEVICE_ERROR;
-    cudaSetDevice(dev->dindex);
-    std::lock_guard<std::mutex> g(dev->chunk_lock);
-    for (auto &kv : dev->chunk_cache) {
-        if (kv.second.kds == kds_dev && kv.second.refs > 0) {
-            kv.second.refs--;
-            xb_chunk_evict_locked(dev);
-            return 0;
-        }
-    }
-    return ERRCODE_DEVICE_ERROR;
-}
-
-extern "C" int
-xpuB200ChunkCacheConfig(xpuB200Device *dev, uint64_t max_bytes, uint64_t *p_cached_bytes, kern_errorbuf *err)
-{
-    xb_clear_error(err);
-    if (!dev)
-        return XB_ERR(err, ERRCODE_DEVICE_ERROR, "invalid device");
-    XB_CUDA(cudaSetDevice(dev->dindex), err);
-    std::lock_guard<std::mutex> g(dev->chunk_lock);
-    if (max_bytes != UINT64_MAX) {
-        dev->chunk_budget = max_bytes;
-        xb_chunk_evict_locked(dev);
-    }
-    if (p_cached_bytes)
-        *p_cached_bytes = dev->chunk_bytes;
     return 0;
 }
 

@@ -350,7 +350,7 @@ __device__ __forceinline__ void xb_agg_covar_add(char *s, double x, double y)
     xb_atomic_add_f64c((double *)(s + 72), (double *)(s + 80), x * y);
 }
 
-__device__ __noinline__ void xb_init_states(const xb_plan *plan, char *e)
+static __device__ __noinline__ void xb_init_states(const xb_plan *plan, char *e)
 {
     for (uint32_t i = 0; i < plan->naggs; i++) {
         const xb_agg &a = plan->aggs[i];
@@ -377,7 +377,7 @@ __device__ __noinline__ void xb_init_states(const xb_plan *plan, char *e)
 }
 
 /* merge a shared-memory group entry's states into a global entry */
-__device__ __noinline__ void xb_merge_states(const xb_plan *plan, char *dst, const char *src)
+static __device__ __noinline__ void xb_merge_states(const xb_plan *plan, char *dst, const char *src)
 {
     for (uint32_t i = 0; i < plan->naggs; i++) {
         const xb_agg &a = plan->aggs[i];
@@ -516,7 +516,7 @@ xb_key_store(const xb_key &k, const xb_keyimg &src, xb_keyimg *dst,
  * release store; readers wait (bounded) on BUSY entries.
  * Returns nullptr when the table is full (*full) or on error.
  */
-__device__ __noinline__ char *
+static __device__ __noinline__ char *
 xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t hash,
               const xb_keyimg *keys, xb_gtable *gt, xb_status *st, bool *full)
 {
@@ -568,7 +568,7 @@ xb_group_find(const xb_plan *plan, char *entries, uint64_t cap_mask, uint32_t ha
 /* xb_group_find on the global table; a group that finds it without room
  * gets an entry of the dump region (merged into the grown table by the
  * host), and only when that is used up is SUSPEND_NO_SPACE raised */
-__device__ __noinline__ char *
+static __device__ __noinline__ char *
 xb_group_find_or_dump(const xb_plan *plan, xb_gtable *gt, uint32_t hash, const xb_keyimg *keys,
                       xb_status *st)
 {
@@ -1048,7 +1048,7 @@ xb_next_unit(const XbExecArgs &args, XbSrc &s, uint32_t lane, bool pf_next = tru
  * ahead.  Nothing is lost or done twice: every unit is either behind the
  * warp, in these ranges, or not yet claimed from the cursor.
  */
-__device__ __noinline__ void
+static __device__ __noinline__ void
 xb_src_leave(const XbExecArgs &args, const XbSrc &s, uint32_t lane, uint32_t next_item, uint32_t nitems)
 {
     if (lane == 0) {

@@ -59,13 +59,13 @@ __device__ __forceinline__ bool xb_bytes_eq(const uint8_t *a, const uint8_t *b, 
     return diff == 0;
 }
 
-__device__ __noinline__ bool xb_bytes_eq_ool(const uint8_t *a, const uint8_t *b, uint32_t n)
+static __device__ __noinline__ bool xb_bytes_eq_ool(const uint8_t *a, const uint8_t *b, uint32_t n)
 {
     return xb_bytes_eq(a, b, n);
 }
 
 /* numeric comparison (numeric_cmp); *err on a corrupt varlena */
-__device__ __noinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, int *err)
+static __device__ __noinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, int *err)
 {
     uint8_t ka, kb; int16_t wa, wb; xb_i128 va, vb;
     if (xb_numeric_decode(a, &ka, &wa, &va) || xb_numeric_decode(b, &kb, &wb, &vb)) {
@@ -83,13 +83,13 @@ __device__ __noinline__ int xb_numeric_cmp(const uint8_t *a, const uint8_t *b, i
     return va < vb ? -1 : (va > vb ? 1 : 0);
 }
 
-__device__ __noinline__ uint32_t xb_hash_text_ool(const uint8_t *p, uint32_t len)
+static __device__ __noinline__ uint32_t xb_hash_text_ool(const uint8_t *p, uint32_t len)
 {
     return xb_hash_bytes(p, len);
 }
 
 /* returns the hash, or sets *bad on a corrupt numeric */
-__device__ __noinline__ uint32_t xb_hash_numeric_ool(const uint8_t *vl, bool *bad)
+static __device__ __noinline__ uint32_t xb_hash_numeric_ool(const uint8_t *vl, bool *bad)
 {
     uint8_t k; int16_t w; xb_i128 v;
     if (xb_numeric_decode(vl, &k, &w, &v)) {
