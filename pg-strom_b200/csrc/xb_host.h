@@ -167,11 +167,12 @@ struct xb_tune_choice {
     int         minb;
     uint32_t    sm_cap;
 };
+extern std::mutex g_tune_lock;
+/* per (GPU, plan shape, default table capacity) */
+extern std::map<std::tuple<int, uint64_t, uint32_t>, xb_tune_choice> g_tune;
 /* per plan shape alone: the CTA bound last tuned for it, adopted by
  * sessions whose default table capacity was not tuned (another group-count
  * estimate) */
-extern std::mutex g_tune_lock;
-extern std::map<std::tuple<int, uint64_t, uint32_t>, xb_tune_choice> g_tune;
 extern std::map<std::pair<int, uint64_t>, int> g_tune_minb;
 
 /* errors: the reference's ERRCODE_* with a filled kern_errorbuf */
