@@ -373,7 +373,7 @@ def config_lines(timeout_s=240):
         for k in ("partitioned_pass_ms", "launch_shape", "rows", "commands", "launches_per_run"):
             if k in cfg:
                 summ[k] = cfg[k]
-        for k in ("plain", "clocks", "cpu_baseline"):
+        for k in ("plain", "clocks", "cpu_baseline", "parity"):
             if k in d:
                 summ[k] = d[k]
         rg = d.get("reference_gpu")
@@ -720,7 +720,15 @@ def run_config(args):
                          "frac": achieved / peak, "traffic": None, "algorithmic_bytes": ref_bytes,
                          "kernel": ("xbj_kernel" if "jit" in info["kernels"].values() else "xb_exec_kernel"),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
-            "clocks": clocks, "gpu_launches": args.steps}
+            "clocks": clocks, "gpu_launches": args.steps,
+            "parity": ({"groups_equal_truth": True,
+                        "compared": "every group of the first pass against the generator's column arrays: "
+                                    "counts, integer and numeric sums exact; float8 averages within 1e-12 "
+                                    "relative (of the sum of magnitudes where a group's terms cancel)"}
+                       if truth is not None else
+                       {"checked": False,
+                        "why": "no truth is generated at this size; the GPU tests check the same session "
+                               "shape against the truth up to 2M rows / 1M keys"})}
     if args.workload == "scan_groupby" and args.reference_gpu:
         try:
             line["reference_gpu"] = reference_gpu_leg(sess, None, chunks, args.rows, truth)
@@ -814,6 +822,9 @@ def run_mixed(args):
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
             "plain": {"ms_per_run": plain_ms, "rows_per_s": rows / (plain_ms / 1000.0),
                       "how": "one xpuB200ExecTask per command on the same resident chunks, sequential"},
+            "parity": {"rows_in_equal_truth": True,
+                       "compared": "every command's qualifying-row count against its generator; the groups "
+                                   "of a mixed batch against the truth and the oracle: tests/test_gpu_mixed.py"},
             "clocks": clocks, "gpu_launches": args.steps * info["launches"]}
     print(json.dumps(line), flush=True)
     mix.close()

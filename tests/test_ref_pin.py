@@ -108,3 +108,20 @@ def test_oracle_matches_reference_functions(which):
     mine = F.decode_kds_final(o.final(), sess)
     o.close()
     assert F.compare_groups(mine, ref, rtol=0.0) == []
+
+
+def test_reference_gpu_harness_exports():
+    """The reference's sm_100a build and the harness that launches it
+    (oracle/Makefile ref_gpu): the fatbin is there and the harness exports
+    every entry point its front end binds (running it needs a GPU:
+    test_gpu_ref_kernel.py)."""
+    import ctypes
+    import os
+    import ref_gpu
+    if not ref_gpu.available():
+        pytest.skip("oracle/_ref/libref_gpu.so or the fatbin not built")
+    assert os.path.getsize(ref_gpu.FATBIN) > 0
+    L = ctypes.CDLL(ref_gpu.SO)
+    for name in ("rg_open", "rg_session", "rg_exec", "rg_final", "rg_info", "rg_close", "rg_upload", "rg_free"):
+        assert hasattr(L, name), name
+    ref_gpu.lib()
