@@ -968,6 +968,21 @@ int xo_exec(xo_sess *s, const kern_data_store *kds, char *errmsg, int errlen)
                 }
                 const uint8_t *vals = (const uint8_t *)kds + cm->values_offset;
                 int tc = s->slot_type[vl->vl_slot_id];
+                /* a row past the values buffer reads as NULL, as the
+                 * reference's readers have it (KDS_ARROW_REF_SIMPLE_DATUM,
+                 * KDS_ARROW_REF_VARLENA32_DATUM, xpu_common.h:1557-1605) */
+                {
+                    const uint64_t unitsz = tc == TypeOpCode__int2 ? 2 :
+                                            (tc == TypeOpCode__int4 || tc == TypeOpCode__date ||
+                                             tc == TypeOpCode__text) ? 4 : 8;
+                    if (unitsz * ((uint64_t)row + 1) > cm->values_length)
+                        continue;
+                }
+                if (tc == TypeOpCode__text) {
+                    const uint32_t *o = (const uint32_t *)vals;
+                    if (o[row] > o[row + 1] || o[row + 1] > cm->extra_length || o[row + 1] - o[row] > 0x4ffffff8U)
+                        continue;
+                }
                 d->type_code = tc;
                 switch (tc) {
                 case TypeOpCode__int2: d->kind = DK_INT; d->i = ((const int16_t *)vals)[row]; break;

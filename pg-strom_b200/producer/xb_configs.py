@@ -513,6 +513,75 @@ def arrow_groupby(nrows=500_000_000, nkeys=10_000_000, seed_config=2, rows_per_c
     return chunks, session, expect, meta
 
 
+def _validity(valid: np.ndarray) -> np.ndarray:
+    """Arrow validity bitmap (bit i set: row i has a value, least significant
+    bit first)"""
+    return np.packbits(valid.astype(np.uint8), bitorder="little")
+
+
+def arrow_nulls(nrows=200_000, nkeys=2_000, seed_config=37, rows_per_chunk=50_000, null_frac=0.1,
+                short_rows=100):
+    """The Arrow group-by's session over columns with NULLs: every
+    referenced column carries a validity bitmap with null_frac of its rows
+    NULL (k NULL: one group of its own; d NULL: the filter drops the row;
+    v1 / v2 NULL: the aggregates skip it), and in every chunk the v2 values
+    buffer ends short_rows rows before the chunk does, so those rows read as
+    NULL (the readers' bound on values_length, KDS_ARROW_REF_SIMPLE_DATUM,
+    xpu_common.h:1557-1574; the reference asserts that a row marked valid has
+    a value, xpu_common.cu:273, so short_rows > 0 is for this library's
+    readers and the oracle only).  Returns (chunks, session, expect, meta)."""
+    r = rng_for(seed_config, 0)
+    d0 = 16436
+    lo_day, hi_day = 17532, 18262
+    typs = [("k", "int8"), ("v1", "int4"), ("v2", "float8"), ("d", "date")]
+    session = arrow_groupby_session(lo_day, hi_day, float(nkeys))
+    chunks = []
+    rows = {nm: [] for nm in ("k", "v1", "v2", "d", "kn", "v1n", "v2n", "dn")}
+    done = 0
+    while done < nrows:
+        n = min(rows_per_chunk, nrows - done)
+        k = r.integers(0, nkeys, n, dtype=np.int64)
+        v1 = r.integers(-1_000_000, 1_000_001, n, dtype=np.int32)
+        v2 = r.lognormal(0.0, 1.0, n)
+        d = r.integers(d0, d0 + 3652, n, dtype=np.int32)
+        nulls = {nm: r.random(n) < null_frac for nm in ("k", "v1", "v2", "d")}
+        short = np.zeros(n, dtype=bool)
+        short[max(0, n - short_rows):] = True
+        t = Table("t2n", [Column(nm, ty) for nm, ty in typs], n)
+        chunks.append(t.arrow_kds({
+            "k": {"tag": 2, "bitwidth": 64, "values": k, "validity": _validity(~nulls["k"])},
+            "v1": {"tag": 2, "bitwidth": 32, "values": v1, "validity": _validity(~nulls["v1"])},
+            "v2": {"tag": 3, "precision": 2, "values": v2[:n - short_rows], "validity": _validity(~nulls["v2"])},
+            "d": {"tag": 8, "unit": 0, "values": d, "validity": _validity(~nulls["d"])},
+        }))
+        for nm, arr in (("k", k), ("v1", v1), ("v2", v2), ("d", d)):
+            rows[nm].append(arr)
+        rows["kn"].append(nulls["k"])
+        rows["v1n"].append(nulls["v1"])
+        rows["v2n"].append(nulls["v2"] | short)
+        rows["dn"].append(nulls["d"])
+        done += n
+    c = {nm: np.concatenate(v) for nm, v in rows.items()}
+    m = ~c["dn"] & (c["d"] >= lo_day) & (c["d"] < hi_day)
+    expect = {}
+    for i in np.flatnonzero(m).tolist():        # row order: the FP64 sums are row-ordered
+        key = (None,) if c["kn"][i] else (int(c["k"][i]),)
+        g = expect.setdefault(key, [0, [0, 0], [0, None], [0, None], [0, 0.0]])
+        g[0] += 1
+        if not c["v1n"][i]:
+            g[1][0] += 1
+            g[1][1] += int(c["v1"][i])
+        if not c["v2n"][i]:
+            x = float(c["v2"][i])
+            g[2] = [1, x if g[2][1] is None else min(g[2][1], x)]
+            g[3] = [1, x if g[3][1] is None else max(g[3][1], x)]
+            g[4][0] += 1
+            g[4][1] += x
+    expect = {k: [v[0], tuple(v[1]), tuple(v[2]), tuple(v[3]), tuple(v[4])] for k, v in expect.items()}
+    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum())}
+    return chunks, session, expect, meta
+
+
 # ---------------------------------------------------------------------------
 def scan_projection(nrows=200_000, seed_config=0, null_frac=0.05, a_limit=300, htup_margin=0):
     """The scan_groupby table and filter, rows projected into kds_dst:

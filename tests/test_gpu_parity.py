@@ -194,6 +194,24 @@ def test_arrow_groupby_parity(device, kernel, nrows, nkeys, rpc):
     assert F.compare_groups(got, expect) == []
 
 
+@pytest.mark.parametrize("short_rows", [0, 100])
+def test_arrow_nulls_parity(device, kernel, short_rows):
+    """Arrow columns with validity bitmaps (NULL group keys, NULL dates in
+    the filter, NULL arguments) and, with short_rows, a values buffer that
+    ends before its chunk (those rows read as NULL): the groups of the
+    oracle and of the arrays, on both kernels."""
+    chunks, sess, expect, meta = C.arrow_nulls(nrows=300_000, nkeys=3_000, rows_per_chunk=100_000,
+                                               short_rows=short_rows)
+    final, st, res = run_gpu(device, sess, chunks, kernel=kernel)
+    assert st["nitems_raw"] == meta["nitems_raw"]
+    assert st["nitems_in"] == meta["nitems_in"]
+    got = F.decode_kds_final(final, sess)
+    assert (None,) in got
+    assert F.compare_groups(got, expect) == []
+    ofinal, _ = run_oracle(sess, chunks)
+    assert F.compare_groups(got, F.decode_kds_final(ofinal, sess)) == []
+
+
 def test_batch_matches_single_chunk_path(device, kernel):
     fact, sess, km, expect, meta = C.join_groupby(nfact=300_000, ndim1=20_000, ndim2=2_000)
     chunks = fact.block_chunks(pages_per_chunk=300)

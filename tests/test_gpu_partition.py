@@ -49,6 +49,19 @@ def test_partitioned_every_state_form(device, monkeypatch):
     assert F.compare_groups(F.decode_kds_final(final, sess), expect) == []
 
 
+def test_partitioned_arrow_nulls(device, monkeypatch):
+    # NULL group keys and NULL arguments travel through the deferred
+    # records' NULL masks and the replay
+    monkeypatch.delenv("XPU_B200_PARTITION", raising=False)
+    chunks, _, expect, meta = C.arrow_nulls(nrows=600_000, nkeys=200_000, rows_per_chunk=200_000, seed_config=84)
+    sess = C.arrow_groupby_session(ngroups_estimate=10_000_000.0)
+    final, info = _run(device, sess, chunks)
+    assert info["partition_used"], info
+    got = F.decode_kds_final(final, sess)
+    assert (None,) in got
+    assert F.compare_groups(got, expect) == []
+
+
 def test_in_place_without_the_switch(device, monkeypatch):
     monkeypatch.setenv("XPU_B200_PARTITION", "0")
     chunks, sess, expect, meta = C.arrow_groupby(nrows=1_000_000, nkeys=300_000, rows_per_chunk=500_000,

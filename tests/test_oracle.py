@@ -91,3 +91,19 @@ def test_oracle_no_group_by_no_rows():
     assert expect == {}
     assert F.decode_kds_final(o.final(), sess) == {}
     o.close()
+
+
+def test_oracle_arrow_nulls_and_short_buffers():
+    # validity bitmaps on every column (NULL group keys form a group of their
+    # own, NULL dates fail the filter, NULL arguments are skipped) and a v2
+    # values buffer that ends before its chunk (those rows read as NULL)
+    chunks, sess, expect, meta = C.arrow_nulls(nrows=80_000, nkeys=700, rows_per_chunk=30_000)
+    o = O.Oracle(sess)
+    for ch in chunks:
+        o.exec(ch)
+    got = F.decode_kds_final(o.final(), sess)
+    st = o.stats()
+    o.close()
+    assert st["nitems_in"] == meta["nitems_in"]
+    assert (None,) in got
+    assert F.compare_groups(got, expect) == []

@@ -68,13 +68,16 @@ def _ref_groups(res, aggs, keytypes):
     return out
 
 
-@pytest.mark.parametrize("which", ["scan", "join", "nogroup", "long_varlena", "join_long_text", "arrow"])
+@pytest.mark.parametrize("which", ["scan", "join", "nogroup", "long_varlena", "join_long_text", "arrow",
+                                   "arrow_nulls"])
 def test_oracle_matches_reference_functions(which):
     """The oracle's groups equal those the reference's functions compute
     (rtol=0): heap scan and join, an aggregate without GROUP BY keys, text
     and numeric varlenas with 4-byte headers and the NUMERIC_LONG format,
     text group keys of inner rows longer than 126 bytes, and Arrow columns
-    read by ExecLoadVarsOuterArrow (int8 / int4 / float8 / date)."""
+    read by ExecLoadVarsOuterArrow (int8 / int4 / float8 / date), also with
+    validity bitmaps on every column (NULL keys, NULL filter inputs, NULL
+    arguments)."""
     if which == "scan":
         tbl, sess, km, expect, meta = C.scan_groupby(nrows=60_000)
         chunks = tbl.block_chunks(pages_per_chunk=200)
@@ -90,6 +93,11 @@ def test_oracle_matches_reference_functions(which):
         chunks = tbl.block_chunks(pages_per_chunk=200)
     elif which == "arrow":
         chunks, sess, expect, meta = C.arrow_groupby(nrows=60_000, nkeys=5_000, rows_per_chunk=25_000)
+        km = None
+    elif which == "arrow_nulls":
+        # (validity NULLs only: the reference asserts that a row its bitmap
+        # marks valid has a value, xpu_common.cu:273)
+        chunks, sess, expect, meta = C.arrow_nulls(nrows=60_000, nkeys=500, rows_per_chunk=20_000, short_rows=0)
         km = None
     else:
         tbl, sess, km, expect, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
