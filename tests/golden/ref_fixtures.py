@@ -1,0 +1,177 @@
+"""
+Golden vectors computed by PG-Strom's own functions, committed so that the
+oracle's pin travels without the reference sources.
+
+Run as a script where oracle/_ref/libref_xpu.so is built (oracle/Makefile
+"ref": PG-Strom's expression library host-compiled from its sources, driven by
+oracle/ref_harness.cpp):
+
+    python tests/golden/ref_fixtures.py
+
+It writes, next to this file:
+
+* ref_scalars.json -- pg_hash_any (src/xpu_common.cu:2921) of seeded byte
+  strings, and the reference's decode of numerics as xb_producer encodes
+  them (__decimal_from_varlena, src/xpu_numeric.h:217);
+* ref_pin_<case>.json -- per configuration, the row counters and every group
+  (keys and partial states) that ExecLoadVarsOuterHeap / ExecLoadVarsOuterArrow,
+  the quals, the hash joins and the aggregate functions of the reference
+  compute over the chunks and bytecode that xb_configs produces, with the
+  SHA-256 of those inputs so a drift of the generators is told apart from a
+  drift of the oracle.
+
+tests/test_golden_ref.py checks the C oracle against these files on any host.
+TEST INFRASTRUCTURE ONLY.
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+for _sub in ("pg-strom_b200", os.path.join("pg-strom_b200", "producer"), "oracle"):
+    _p = os.path.join(ROOT, _sub)
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import xb_configs as C  # noqa: E402
+import xb_final as F  # noqa: E402
+
+# small enough that the oracle finishes each in about a second and each file
+# stays a few tens of KB
+CASES = ("scan", "nogroup", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls")
+
+HASH_LENGTHS = list(range(0, 48)) + [63, 64, 65, 100, 255, 1000]
+NUMERIC_SCALES = (0, 2, 4)
+
+
+def case_inputs(which):
+    """(session, chunks, kmrels or None, meta) of one configuration."""
+    if which == "scan":
+        tbl, sess, km, _, meta = C.scan_groupby(nrows=60_000)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "nogroup":
+        tbl, sess, km, _, meta = C.scan_nogroup(nrows=60_000)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "join":
+        tbl, sess, km, _, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "long_varlena":
+        tbl, sess, km, _, meta = C.long_varlena_groupby(nrows=20_000)
+        chunks = tbl.block_chunks(pages_per_chunk=100)
+    elif which == "join_long_text":
+        tbl, sess, km, _, meta = C.join_groupby(nfact=40_000, ndim1=3000, ndim2=500,
+                                                regions=C.long_strings(40))
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "arrow":
+        chunks, sess, _, meta = C.arrow_groupby(nrows=30_000, nkeys=400, rows_per_chunk=12_000)
+        km = None
+    elif which == "arrow_nulls":
+        # validity-bitmap NULLs only: the reference asserts that a row its
+        # bitmap marks valid has a value (src/xpu_common.cu:273)
+        chunks, sess, _, meta = C.arrow_nulls(nrows=30_000, nkeys=300, rows_per_chunk=10_000, short_rows=0)
+        km = None
+    else:
+        raise ValueError(which)
+    return sess, chunks, km, meta
+
+
+def input_digest(sess, chunks, km):
+    h = hashlib.sha256()
+    h.update(bytes(sess))
+    for ch in chunks:
+        h.update(np.ascontiguousarray(ch).tobytes())
+    if km is not None:
+        h.update(np.ascontiguousarray(km).tobytes())
+    return h.hexdigest()
+
+
+def hash_inputs():
+    r = np.random.default_rng(11)
+    return [r.integers(0, 256, n, dtype=np.uint8).tobytes() for n in HASH_LENGTHS]
+
+
+def numeric_inputs():
+    r = np.random.default_rng(12)
+    vals = [0, 1, -1, 5, 10, 100, 9999, 10000, 123456, 999999, -999999, 1000000, 12300]
+    vals += [int(v) for v in r.integers(-10**9, 10**9, 60)]
+    return [(v, s) for s in NUMERIC_SCALES for v in vals]
+
+
+def decode_groups(res, sess):
+    """The harness's groups as {keys: states} in xb_final's decoded form:
+    text keys without their 4-byte header, integers as Python ints, float
+    states exact (the harness prints them with 17 significant digits)."""
+    aggs = F.session_aggs(sess)
+    stypes = F.slot_types(sess)
+    keytypes = [stypes[a0] for (act, a0, _) in aggs if act == 101]
+    out = {}
+    for g in res["groups"]:
+        keys = []
+        for hexv, tc in zip(g["keys"], keytypes):
+            if hexv is None:
+                keys.append(None)
+                continue
+            b = bytes.fromhex(hexv)
+            keys.append(b[4:] if tc == 11 else int.from_bytes(b, "little", signed=True))
+        states = []
+        for st, (action, _, typmod) in zip(g["states"], [a for a in aggs if a[0] != 101]):
+            if action in (201, 202):
+                states.append(st)
+            elif action in (503, 603):
+                states.append((st[0], float(st[1])))
+            elif action in (304, 404):
+                states.append((st[0], float(st[1]) if st[0] else None))
+            elif action in (504, 604):
+                w = (((typmod - 4) & 0x7FF) ^ 1024) - 1024 if typmod >= 0 else 15
+                states.append((st[0], int(st[1]), max(0, min(15, w))))
+            else:
+                states.append((st[0], int(st[1])))
+        out[tuple(keys)] = states
+    return out
+
+
+def fixture_path(name):
+    return os.path.join(HERE, name)
+
+
+def load(name):
+    with open(fixture_path(name)) as f:
+        return json.load(f)
+
+
+def generate():
+    import ref_pin
+    import xb_producer as P
+    if not ref_pin.available():
+        raise SystemExit("oracle/_ref/libref_xpu.so is not built (make -C oracle ref PGSTROM_SRC=...)")
+    scal = {
+        "hash_any": [[d.hex(), ref_pin.hash_any(d)] for d in hash_inputs()],
+        "numeric": [],
+    }
+    for v, s in numeric_inputs():
+        kind, w, iv = ref_pin.numeric_decode(P.encode_numeric(v, s))
+        scal["numeric"].append([v, s, kind, w, str(iv)])
+    with open(fixture_path("ref_scalars.json"), "w") as f:
+        json.dump(scal, f, separators=(",", ":"))
+    for which in CASES:
+        sess, chunks, km, meta = case_inputs(which)
+        res = ref_pin.run(sess, chunks, km)
+        out = {
+            "case": which,
+            "inputs_sha256": input_digest(sess, chunks, km),
+            "nitems_raw": res["nitems_raw"],
+            "nitems_in": res["nitems_in"],
+            "nitems_out": res["nitems_out"],
+            "groups": res["groups"],
+        }
+        with open(fixture_path(f"ref_pin_{which}.json"), "w") as f:
+            json.dump(out, f, separators=(",", ":"))
+        print(f"{which}: {len(res['groups'])} groups, {res['nitems_raw']} rows")
+
+
+if __name__ == "__main__":
+    generate()

@@ -2,6 +2,9 @@
 full scan/join/group-by pass evaluated by the reference's host-compiled
 expression library over the same chunks and bytecode.  Skipped where
 oracle/_ref was not built (it needs the reference sources)."""
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -10,6 +13,9 @@ import xb_configs as C
 import xb_final as F
 import xb_oracle as O
 import xb_producer as P
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+import ref_fixtures as G  # noqa: E402
 
 pytestmark = pytest.mark.skipif(not ref_pin.available(), reason="oracle/_ref not built")
 
@@ -36,36 +42,6 @@ def test_numeric_encoding_matches_reference():
         blob, offs = P.encode_numeric_array(np.array(vals[:50], dtype=np.int64) % 10**7, scale)
         for i in range(50):
             assert bytes(blob[offs[i]:offs[i + 1]]) == P.encode_numeric(int(vals[i] % 10**7), scale)
-
-
-def _ref_groups(res, aggs, keytypes):
-    out = {}
-    for g in res["groups"]:
-        keys = []
-        for hexv, tc in zip(g["keys"], keytypes):
-            if hexv is None:
-                keys.append(None)
-                continue
-            b = bytes.fromhex(hexv)
-            if tc == 11:
-                keys.append(b[4:])
-            else:
-                keys.append(int.from_bytes(b, "little", signed=True))
-        states = []
-        for st, (action, _, typmod) in zip(g["states"], [a for a in aggs if a[0] != 101]):
-            if action in (201, 202):
-                states.append(st)
-            elif action in (503, 603):
-                states.append((st[0], float(st[1])))
-            elif action in (304, 404):
-                states.append((st[0], float(st[1]) if st[0] else None))
-            elif action in (504, 604):
-                w = (((typmod - 4) & 0x7FF) ^ 1024) - 1024 if typmod >= 0 else 15
-                states.append((st[0], int(st[1]), max(0, min(15, w))))
-            else:
-                states.append((st[0], int(st[1])))
-        out[tuple(keys)] = states
-    return out
 
 
 @pytest.mark.parametrize("which", ["scan", "join", "nogroup", "long_varlena", "join_long_text", "arrow",
@@ -106,10 +82,7 @@ def test_oracle_matches_reference_functions(which):
     assert res["nitems_raw"] == meta["nitems_raw"]
     assert res["nitems_in"] == meta["nitems_in"]
     assert res["nitems_out"] == meta["nitems_out"]
-    aggs = F.session_aggs(sess)
-    stypes = F.slot_types(sess)
-    keytypes = [stypes[a0] for (act, a0, _) in aggs if act == 101]
-    ref = _ref_groups(res, aggs, keytypes)
+    ref = G.decode_groups(res, sess)
     o = O.Oracle(sess, km)
     for ch in chunks:
         o.exec(ch)
@@ -124,7 +97,6 @@ def test_reference_gpu_harness_exports():
     every entry point its front end binds (running it needs a GPU:
     test_gpu_ref_kernel.py)."""
     import ctypes
-    import os
     import ref_gpu
     if not ref_gpu.available():
         pytest.skip("oracle/_ref/libref_gpu.so or the fatbin not built")
@@ -133,3 +105,25 @@ def test_reference_gpu_harness_exports():
     for name in ("rg_open", "rg_session", "rg_exec", "rg_final", "rg_info", "rg_close", "rg_upload", "rg_free"):
         assert hasattr(L, name), name
     ref_gpu.lib()
+
+
+@pytest.mark.parametrize("which", G.CASES)
+def test_golden_vectors_are_current(which):
+    """The committed golden vectors (tests/golden/ref_pin_*.json, checked
+    against the oracle by test_golden_ref.py on hosts without the reference)
+    are what the reference's functions compute today over the same inputs."""
+    fx = G.load(f"ref_pin_{which}.json")
+    sess, chunks, km, _ = G.case_inputs(which)
+    assert G.input_digest(sess, chunks, km) == fx["inputs_sha256"]
+    res = ref_pin.run(sess, chunks, km)
+    for k in ("nitems_raw", "nitems_in", "nitems_out"):
+        assert res[k] == fx[k], k
+    assert G.decode_groups(res, sess) == G.decode_groups(fx, sess)
+
+
+def test_golden_scalars_are_current():
+    scal = G.load("ref_scalars.json")
+    assert [[d.hex(), ref_pin.hash_any(d)] for d in G.hash_inputs()] == scal["hash_any"]
+    for (v, s), row in zip(G.numeric_inputs(), scal["numeric"]):
+        kind, w, iv = ref_pin.numeric_decode(P.encode_numeric(v, s))
+        assert [v, s, kind, w, str(iv)] == row
