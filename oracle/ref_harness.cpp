@@ -18,6 +18,7 @@
  *
  * Compiled against the reference headers; never part of the product.
  */
+#include <array>
 #include <string>
 #include <vector>
 #include <map>
@@ -73,6 +74,7 @@ struct Group {
     std::vector<__int128> isum;
     std::vector<double> fsum, fsum2, fext;
     std::vector<int> valid;
+    std::vector<std::array<double, 5>> fm;  /* stddev: sx, sxx; covar: sx, sxx, sy, syy, sxy */
 };
 
 struct RefSess {
@@ -183,6 +185,7 @@ static void group_row(RefSess *s, kern_context *kcxt)
         g.n.assign(nattrs, 0); g.isum.assign(nattrs, 0);
         g.fsum.assign(nattrs, 0.0); g.fsum2.assign(nattrs, 0.0); g.fext.assign(nattrs, 0.0);
         g.valid.assign(nattrs, 0);
+        g.fm.assign(nattrs, std::array<double, 5>{0.0, 0.0, 0.0, 0.0, 0.0});
         it = s->groups.emplace(gk, g).first;
         s->order.push_back(gk);
     }
@@ -223,6 +226,44 @@ static void group_row(RefSess *s, kern_context *kcxt)
                 bool take = !g.valid[j] || (d->action == KAGG_ACTION__PMIN_FP64 ? v < g.fext[j] : v > g.fext[j]);
                 if (take) g.fext[j] = v;
                 g.valid[j] = 1;
+            }
+            break;
+        case KAGG_ACTION__STDDEV:
+            /* __update_groupby__pstddev (cuda_gpupreagg.cu:1448-1466):
+             * count, sum of x, sum of x*x in FP64; the argument fetched by
+             * the reference's __preagg_fetch_xdatum_as_float64 */
+            if (x) {
+                float8_t v;
+                if (__preagg_fetch_xdatum_as_float64(&v, x)) {
+                    g.n[j]++; g.fm[j][0] += v; g.fm[j][1] += v * v;
+                }
+            }
+            break;
+        case KAGG_ACTION__COVAR: {
+            /* __update_groupby__pcovar (cuda_gpupreagg.cu:1470-1492): both
+             * arguments fetched, then the five sums */
+            xpu_datum_t *y = d->arg1_slot_id >= 0 ? kcxt->kvars_slot[d->arg1_slot_id] : NULL;
+            float8_t xv, yv;
+            if (x && y && __preagg_fetch_xdatum_as_float64(&xv, x) &&
+                __preagg_fetch_xdatum_as_float64(&yv, y)) {
+                g.n[j]++;
+                g.fm[j][0] += xv; g.fm[j][1] += xv * xv;
+                g.fm[j][2] += yv; g.fm[j][3] += yv * yv;
+                g.fm[j][4] += xv * yv;
+            }
+            break;
+        }
+        case KAGG_ACTION__PMIN_INT32: case KAGG_ACTION__PMIN_INT64:
+        case KAGG_ACTION__PMAX_INT32: case KAGG_ACTION__PMAX_INT64:
+            /* state printed as [valid, value]: n holds the valid flag */
+            if (!xn) {
+                int64_t v = (x->expr_ops == &xpu_int8_ops) ? ((xpu_int8_t *)x)->value
+                          : (x->expr_ops == &xpu_int4_ops) ? ((xpu_int4_t *)x)->value
+                          : ((xpu_int2_t *)x)->value;
+                bool is_min = (d->action == KAGG_ACTION__PMIN_INT32 || d->action == KAGG_ACTION__PMIN_INT64);
+                bool take = !g.n[j] || (is_min ? v < g.isum[j] : v > g.isum[j]);
+                if (take) g.isum[j] = v;
+                g.n[j] = 1;
             }
             break;
         default:
@@ -391,6 +432,15 @@ extern "C" uint64_t ref_result(void *handle, char *buf, uint64_t bufsz)
             case KAGG_ACTION__PMIN_FP64: case KAGG_ACTION__PMAX_FP64:
                 snprintf(tmp, sizeof(tmp), "[%d,%.17g]", g.valid[j], g.fext[j]);
                 out += tmp; break;
+            case KAGG_ACTION__STDDEV:
+                snprintf(tmp, sizeof(tmp), "[%lld,%.17g,%.17g]", (long long)g.n[j], g.fm[j][0], g.fm[j][1]);
+                out += tmp; break;
+            case KAGG_ACTION__COVAR: {
+                char big[256];
+                snprintf(big, sizeof(big), "[%lld,%.17g,%.17g,%.17g,%.17g,%.17g]", (long long)g.n[j],
+                         g.fm[j][0], g.fm[j][1], g.fm[j][2], g.fm[j][3], g.fm[j][4]);
+                out += big; break;
+            }
             default:
                 out += "[" + std::to_string(g.n[j]) + ",\"" + i128str(g.isum[j]) + "\"]"; break;
             }

@@ -183,17 +183,25 @@ def _buffers(arr):
     return ent
 
 
-def arrow_ipc_chunks(path: str):
+def arrow_ipc_chunks(path: str, columns=None):
     """KDS_FORMAT_ARROW chunks, one per record batch of an Arrow IPC file,
     and the Table describing their columns.  Dictionary columns come out
-    decoded."""
+    decoded.  'columns' names the fields to load, in the order they become
+    the chunk's attributes (default: every field); the others are not
+    read, as Arrow_Fdw sets up I/O only for the referenced columns of a
+    record batch (src/arrow_fdw.c:3750-3768)."""
     import pyarrow as pa
     reader = pa.ipc.open_file(pa.memory_map(path, "r"))
     schema = reader.schema
-    cols = [Column(f.name, _column_type(f.type)) for f in schema]
+    names = list(columns) if columns is not None else [f.name for f in schema]
+    index = {f.name: j for j, f in enumerate(schema)}
+    missing = [n for n in names if n not in index]
+    if missing:
+        raise ValueError(f"{path}: no field named {', '.join(missing)}")
+    cols = [Column(n, _column_type(schema.field(index[n]).type)) for n in names]
     chunks = []
     for i in range(reader.num_record_batches):
         batch = reader.get_batch(i)
         t = Table(os.path.basename(path), cols, batch.num_rows)
-        chunks.append(t.arrow_kds({f.name: _buffers(batch.column(j)) for j, f in enumerate(schema)}))
+        chunks.append(t.arrow_kds({n: _buffers(batch.column(index[n])) for n in names}))
     return chunks, Table(os.path.basename(path), cols, 0)

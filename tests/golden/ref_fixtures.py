@@ -42,7 +42,7 @@ import xb_final as F  # noqa: E402
 
 # small enough that the oracle finishes each in about a second and each file
 # stays a few tens of KB
-CASES = ("scan", "nogroup", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls")
+CASES = ("scan", "nogroup", "wide", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls")
 
 HASH_LENGTHS = list(range(0, 48)) + [63, 64, 65, 100, 255, 1000]
 NUMERIC_SCALES = (0, 2, 4)
@@ -56,6 +56,11 @@ def case_inputs(which):
     elif which == "nogroup":
         tbl, sess, km, _, meta = C.scan_nogroup(nrows=60_000)
         chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "wide":
+        # every partial-state form: count, count(x), int and float min/max,
+        # float sum, numeric avg, stddev, covar
+        tbl, sess, km, _, meta = C.wide_groupby(nrows=40_000, ngroups=300)
+        chunks = tbl.block_chunks(pages_per_chunk=100)
     elif which == "join":
         tbl, sess, km, _, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
         chunks = tbl.block_chunks(pages_per_chunk=200)
@@ -125,6 +130,10 @@ def decode_groups(res, sess):
                 states.append((st[0], float(st[1])))
             elif action in (304, 404):
                 states.append((st[0], float(st[1]) if st[0] else None))
+            elif action == 701:
+                states.append((st[0], float(st[1]), float(st[2])))
+            elif action == 801:
+                states.append((st[0],) + tuple(float(v) for v in st[1:]))
             elif action in (504, 604):
                 w = (((typmod - 4) & 0x7FF) ^ 1024) - 1024 if typmod >= 0 else 15
                 states.append((st[0], int(st[1]), max(0, min(15, w))))

@@ -44,11 +44,13 @@ def test_numeric_encoding_matches_reference():
             assert bytes(blob[offs[i]:offs[i + 1]]) == P.encode_numeric(int(vals[i] % 10**7), scale)
 
 
-@pytest.mark.parametrize("which", ["scan", "join", "nogroup", "long_varlena", "join_long_text", "arrow",
+@pytest.mark.parametrize("which", ["scan", "join", "nogroup", "wide", "long_varlena", "join_long_text", "arrow",
                                    "arrow_nulls"])
 def test_oracle_matches_reference_functions(which):
     """The oracle's groups equal those the reference's functions compute
-    (rtol=0): heap scan and join, an aggregate without GROUP BY keys, text
+    (rtol=0): heap scan and join, an aggregate without GROUP BY keys, every
+    partial-state form (count(x), int and float min/max, float sum, numeric
+    avg, stddev, covar), text
     and numeric varlenas with 4-byte headers and the NUMERIC_LONG format,
     text group keys of inner rows longer than 126 bytes, and Arrow columns
     read by ExecLoadVarsOuterArrow (int8 / int4 / float8 / date), also with
@@ -59,6 +61,9 @@ def test_oracle_matches_reference_functions(which):
         chunks = tbl.block_chunks(pages_per_chunk=200)
     elif which == "nogroup":
         tbl, sess, km, expect, meta = C.scan_nogroup(nrows=60_000)
+        chunks = tbl.block_chunks(pages_per_chunk=200)
+    elif which == "wide":
+        tbl, sess, km, expect, meta = C.wide_groupby(nrows=60_000, ngroups=800)
         chunks = tbl.block_chunks(pages_per_chunk=200)
     elif which == "long_varlena":
         tbl, sess, km, expect, meta = C.long_varlena_groupby(nrows=20_000)
