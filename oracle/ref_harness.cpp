@@ -12,7 +12,9 @@
  * reference's functions (ExecLoadVarsOuterHeap, ExecLoadVarsOuterArrow,
  * ExecLoadVarsMinimalTuple,
  * ExecMoveKernelVariables, EXEC_KERN_EXPRESSION, ExecGpuJoinQuals,
- * pg_hash_any, xpu_*_datum_write).  Only the group accumulation itself is
+ * pg_hash_any, xpu_*_datum_write, and for projection sessions
+ * kern_estimate_minimal_tuple / kern_form_minimal_tuple, whose tuples are
+ * returned as they are).  Only the group accumulation itself is
  * restated (its reference form is device-only code), with exact int128
  * and row-ordered FP64 sums.  Results are returned as JSON text.
  *
@@ -86,6 +88,7 @@ struct RefSess {
     std::vector<std::pair<uint32_t, std::string>> order;
     uint64_t nraw = 0, nin = 0, nout = 0;
     std::string err;
+    std::vector<std::string> proj;      /* projected tuples (hex), row id cut off */
 };
 
 static std::string hexof(const char *p, int n)
@@ -123,7 +126,7 @@ extern "C" void *ref_open(const void *session, uint64_t sz, void *kmrels, char *
                         s->session->xpucode_scan_quals, s->session->xpucode_join_quals_packed,
                         s->session->xpucode_hash_values_packed, s->session->xpucode_groupby_keyhash,
                         s->session->xpucode_groupby_keyload, s->session->xpucode_groupby_keycomp,
-                        s->session->xpucode_groupby_actions };
+                        s->session->xpucode_groupby_actions, s->session->xpucode_projection };
     for (uint32_t off : offs) {
         if (off && !resolve((kern_expression *)((char *)s->session + off), s->err)) {
             snprintf(errbuf, errlen, "%s", s->err.c_str());
@@ -272,6 +275,24 @@ static void group_row(RefSess *s, kern_context *kcxt)
     }
 }
 
+/* a projection session's row: its tuple as the reference's own
+ * kern_estimate_minimal_tuple / kern_form_minimal_tuple write it into a
+ * KDS_FORMAT_ROW kds_dst (execGpuJoinProjection, cuda_gpujoin.cu:754-936) */
+static void project_row(RefSess *s, kern_context *kcxt)
+{
+    kern_session_info *session = s->session;
+    const kern_expression *kproj = SESSION_KEXP_PROJECTION(session);
+    const kern_data_store *kds_dst = SESSION_KDS_DST_HEAD(session);
+    if (!kds_dst) { s->err = "projection without a kds_dst head"; return; }
+    int sz = kern_estimate_minimal_tuple(kcxt, kproj, kds_dst);
+    if (sz < 0) { s->err = "kern_estimate_minimal_tuple failed"; return; }
+    std::vector<uint64_t> buf((sz + 64) / 8 + 1, 0);
+    kern_tupitem *titem = (kern_tupitem *)buf.data();
+    int len = kern_form_minimal_tuple(kcxt, kproj, kds_dst, titem, (uint32_t)s->proj.size());
+    if (len < ROWID_SIZE || len > sz + 8) { s->err = "kern_form_minimal_tuple failed"; return; }
+    s->proj.push_back(hexof((const char *)titem, len - ROWID_SIZE));
+}
+
 static void process_depth(RefSess *s, kern_context *kcxt, int depth,
                           std::vector<std::vector<char>> &kvecs)
 {
@@ -282,7 +303,10 @@ static void process_depth(RefSess *s, kern_context *kcxt, int depth,
             kcxt->kvecs_curr_buffer = kvecs[depth - 1].data();
             kcxt->kvecs_curr_id = 0;
         }
-        group_row(s, kcxt);
+        if (session->xpucode_projection)
+            project_row(s, kcxt);
+        if (session->xpucode_groupby_actions)
+            group_row(s, kcxt);
         return;
     }
     /* expressions of this depth read outer values from the previous depth's kvec */
@@ -404,7 +428,10 @@ extern "C" uint64_t ref_result(void *handle, char *buf, uint64_t bufsz)
     RefSess *s = (RefSess *)handle;
     kern_expression *kact = SESSION_KEXP_GROUPBY_ACTIONS(s->session);
     std::string out = "{\"nitems_raw\":" + std::to_string(s->nraw) + ",\"nitems_in\":" +
-                      std::to_string(s->nin) + ",\"nitems_out\":" + std::to_string(s->nout) + ",\"groups\":[";
+                      std::to_string(s->nin) + ",\"nitems_out\":" + std::to_string(s->nout) + ",\"rows\":[";
+    for (size_t i = 0; i < s->proj.size(); i++)
+        out += (i ? ",\"" : "\"") + s->proj[i] + "\"";
+    out += "],\"groups\":[";
     bool first = true;
     for (auto &gk : s->order) {
         Group &g = s->groups[gk];

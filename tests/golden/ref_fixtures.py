@@ -18,7 +18,10 @@ It writes, next to this file:
   the quals, the hash joins and the aggregate functions of the reference
   compute over the chunks and bytecode that xb_configs produces, with the
   SHA-256 of those inputs so a drift of the generators is told apart from a
-  drift of the oracle.
+  drift of the oracle;
+* ref_proj_<case>.json -- per projection configuration, the row counters,
+  the number and SHA-256 of the tuples the reference forms, and the first
+  few of them.
 
 tests/test_golden_ref.py checks the C oracle against these files on any host.
 TEST INFRASTRUCTURE ONLY.
@@ -43,6 +46,13 @@ import xb_final as F  # noqa: E402
 # small enough that the oracle finishes each in about a second and each file
 # stays a few tens of KB
 CASES = ("scan", "nogroup", "wide", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls")
+
+# projection sessions: rows formed into a KDS_FORMAT_ROW kds_dst by the
+# reference's kern_estimate_minimal_tuple / kern_form_minimal_tuple
+# (src/xpu_common.cu:1097-1300); the vectors keep the SHA-256 of the sorted
+# tuple images (row id cut off) and the first few images in full
+PROJ_CASES = ("scan_proj", "scan_proj_nulls", "join_proj", "join_proj_multi")
+PROJ_SAMPLE = 8
 
 HASH_LENGTHS = list(range(0, 48)) + [63, 64, 65, 100, 255, 1000]
 NUMERIC_SCALES = (0, 2, 4)
@@ -79,9 +89,31 @@ def case_inputs(which):
         # bitmap marks valid has a value (src/xpu_common.cu:273)
         chunks, sess, _, meta = C.arrow_nulls(nrows=30_000, nkeys=300, rows_per_chunk=10_000, short_rows=0)
         km = None
+    elif which == "scan_proj":
+        tbl, sess, _, meta = C.scan_projection(nrows=20_000)
+        chunks, km = tbl.block_chunks(pages_per_chunk=64), None
+    elif which == "scan_proj_nulls":
+        tbl, sess, _, meta = C.scan_projection(nrows=12_000, null_frac=0.5, htup_margin=24)
+        chunks, km = tbl.block_chunks(pages_per_chunk=64), None
+    elif which == "join_proj":
+        tbl, sess, km, meta = C.join_projection(nfact=20_000)
+        chunks = tbl.block_chunks(pages_per_chunk=64)
+    elif which == "join_proj_multi":
+        # several dim1 rows per key and fact keys without a match
+        tbl, sess, km, meta = C.join_projection(nfact=12_000, dim1_copies=3, miss_frac=0.2, key_stride=2)
+        chunks = tbl.block_chunks(pages_per_chunk=64)
     else:
         raise ValueError(which)
     return sess, chunks, km, meta
+
+
+def rows_digest(images):
+    """SHA-256 of the sorted tuple images, each preceded by its length."""
+    h = hashlib.sha256()
+    for img in sorted(images):
+        h.update(len(img).to_bytes(4, "little"))
+        h.update(img)
+    return h.hexdigest()
 
 
 def input_digest(sess, chunks, km):
@@ -180,6 +212,23 @@ def generate():
         with open(fixture_path(f"ref_pin_{which}.json"), "w") as f:
             json.dump(out, f, separators=(",", ":"))
         print(f"{which}: {len(res['groups'])} groups, {res['nitems_raw']} rows")
+    for which in PROJ_CASES:
+        sess, chunks, km, meta = case_inputs(which)
+        res = ref_pin.run(sess, chunks, km)
+        images = sorted(bytes.fromhex(h) for h in res["rows"])
+        out = {
+            "case": which,
+            "inputs_sha256": input_digest(sess, chunks, km),
+            "nitems_raw": res["nitems_raw"],
+            "nitems_in": res["nitems_in"],
+            "nitems_out": res["nitems_out"],
+            "nrows": len(images),
+            "rows_sha256": rows_digest(images),
+            "first_rows": [img.hex() for img in images[:PROJ_SAMPLE]],
+        }
+        with open(fixture_path(f"ref_proj_{which}.json"), "w") as f:
+            json.dump(out, f, separators=(",", ":"))
+        print(f"{which}: {len(images)} projected rows")
 
 
 if __name__ == "__main__":

@@ -60,3 +60,26 @@ def test_oracle_matches_reference_golden(which):
     o.close()
     assert st["nitems_out"] == fx["nitems_out"]
     assert F.compare_groups(mine, ref, rtol=0.0) == []
+
+
+@pytest.mark.parametrize("which", G.PROJ_CASES)
+def test_oracle_projection_matches_reference_golden(which):
+    """Projected rows: the oracle's tuple images (kern_tupitem, row id cut
+    off) are, as a multiset, byte for byte those the reference's
+    kern_form_minimal_tuple formed: same count, same SHA-256 of the sorted
+    images, same first images."""
+    fx = G.load(f"ref_proj_{which}.json")
+    sess, chunks, km, meta = G.case_inputs(which)
+    assert G.input_digest(sess, chunks, km) == fx["inputs_sha256"], \
+        "the generator's inputs drifted from those the vectors were made from: rerun tests/golden/ref_fixtures.py"
+    o = O.Oracle(sess, km)
+    for ch in chunks:
+        o.exec(ch)
+    rows, _ = o.proj_rows()
+    st = o.stats()
+    o.close()
+    assert (st["nitems_raw"], st["nitems_in"], st["nitems_out"]) == \
+        (fx["nitems_raw"], fx["nitems_in"], fx["nitems_out"])
+    assert len(rows) == fx["nrows"]
+    assert [r.hex() for r in sorted(rows)[:G.PROJ_SAMPLE]] == fx["first_rows"]
+    assert G.rows_digest(rows) == fx["rows_sha256"]

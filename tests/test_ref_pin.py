@@ -132,3 +132,25 @@ def test_golden_scalars_are_current():
     for (v, s), row in zip(G.numeric_inputs(), scal["numeric"]):
         kind, w, iv = ref_pin.numeric_decode(P.encode_numeric(v, s))
         assert [v, s, kind, w, str(iv)] == row
+
+
+@pytest.mark.parametrize("which", G.PROJ_CASES)
+def test_projection_matches_reference_functions(which):
+    """Projection sessions: every row the oracle forms into kds_dst is, byte
+    for byte (row id cut off), a row the reference's kern_estimate_minimal_tuple
+    / kern_form_minimal_tuple form for the same scan or join result, with
+    NULL bitmaps, varlenas and alignment padding; the committed vectors are
+    current."""
+    sess, chunks, km, _ = G.case_inputs(which)
+    res = ref_pin.run(sess, chunks, km)
+    ref = sorted(bytes.fromhex(h) for h in res["rows"])
+    o = O.Oracle(sess, km)
+    for ch in chunks:
+        o.exec(ch)
+    mine, _ = o.proj_rows()
+    st = o.stats()
+    o.close()
+    assert res["nitems_out"] == st["nitems_out"] == len(ref)
+    assert sorted(mine) == ref
+    fx = G.load(f"ref_proj_{which}.json")
+    assert G.rows_digest(ref) == fx["rows_sha256"]
