@@ -28,7 +28,7 @@ import struct
 import numpy as np
 
 from xb_final import Approx
-from xb_producer import (Table, Column, Var, Const, Func, Agg, SessionBuilder,
+from xb_producer import (BLCKSZ, Table, Column, Var, Const, Func, Agg, SessionBuilder,
                          encode_numeric, encode_varlena_list, encode_numeric_array, encode_text_array, encode_text_from_dict,
                          hash_u32_array, hash_merge_array, kern_multirels, numeric_typmod)
 
@@ -93,8 +93,17 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ng
     g (64 in the benchmark configuration)."""
     tbl, a, b, bnull, c_unscaled, g = _scan_table(nrows, seed_config, null_frac, ngroups)
     session = scan_groupby_session(a_limit, ngroups)
-    # expected partial states per group, straight from the arrays
+    expect, meta = _scan_expect(a, b, bnull, c_unscaled, g, a_limit, ngroups)
+    return tbl, session, None, expect, meta
+
+
+def _scan_expect(a, b, bnull, c_unscaled, g, a_limit, ngroups, visible=None):
+    """expected partial states per group of scan_groupby_session, straight
+    from the arrays; visible masks the rows the chunks still hold"""
+    nrows = len(a)
     m = a < a_limit
+    if visible is not None:
+        m &= visible
     gm = g[m]
     cnt = np.bincount(gm, minlength=ngroups)
     sa = np.zeros(ngroups, dtype=np.int64)
@@ -112,9 +121,69 @@ def scan_groupby(nrows=4_000_000, seed_config=0, null_frac=0.05, a_limit=300, ng
         expect[(k,)] = {"nrows": int(cnt[k]), "sum_a": (int(cnt[k]), int(sa[k])),
                         "sum_c": (int(cnt[k]), int(sc[k]), 2),
                         "avg_b": (int(nb[k]), Approx(float(sb_[k]), float(sab[k])))}
-    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()),
+    meta = {"nitems_raw": nrows if visible is None else int(visible.sum()),
+            "nitems_in": int(m.sum()), "nitems_out": int(m.sum()),
             "agg_names": ["nrows", "sum_a", "sum_c", "avg_b"], "nkeys": 1}
-    return tbl, session, None, expect, meta
+    return expect, meta
+
+
+LP_UNUSED, LP_NORMAL, LP_REDIRECT, LP_DEAD = 0, 1, 2, 3
+
+
+def invalidate_lines(chunks, frac, seed=41):
+    """Copies of KDS_FORMAT_BLOCK chunks in which a share 'frac' of the line
+    pointers no longer point at a visible tuple, the pages the reference's
+    relscan.c hands the GPU when they are not all-visible (it sets the line
+    pointers of invisible tuples unused, src/relscan.c:462-494), and pages
+    after HOT pruning (dead items keeping their storage, redirects).  Each
+    chosen line pointer becomes LP_UNUSED (offset and length cleared),
+    LP_DEAD (storage kept) or LP_REDIRECT (offset = another line number,
+    length 0), in turn.  Returns the chunks and the mask of rows, in the
+    order the chunks hold them, that stay visible."""
+    r = np.random.default_rng(seed)
+    out, keep = [], []
+    kind = 0
+    for ch in chunks:
+        ch = ch.copy()
+        nblocks, = struct.unpack_from("<I", ch, 16)
+        block_offset, = struct.unpack_from("<I", ch, 44)
+        for b in range(nblocks):
+            base = block_offset + b * BLCKSZ
+            lower, = struct.unpack_from("<H", ch, base + 12)
+            nlp = (lower - 24) // 4
+            for i in range(nlp):
+                pos = base + 24 + 4 * i
+                lp, = struct.unpack_from("<I", ch, pos)
+                if ((lp >> 15) & 3) != LP_NORMAL:
+                    continue
+                if r.random() >= frac:
+                    keep.append(True)
+                    continue
+                keep.append(False)
+                if kind == 0:
+                    lp = 0
+                elif kind == 1:
+                    lp = (lp & ~(3 << 15)) | (LP_DEAD << 15)
+                else:
+                    lp = (((i + 1) % nlp) + 1) | (LP_REDIRECT << 15)
+                kind = (kind + 1) % 3
+                struct.pack_into("<I", ch, pos, lp)
+        out.append(ch)
+    return out, np.array(keep, dtype=bool)
+
+
+def scan_groupby_filtered(nrows=200_000, seed_config=40, null_frac=0.05, a_limit=300, ngroups=64,
+                          pages_per_chunk=200, frac=0.15):
+    """scan_groupby over pages whose line pointers are partly invalidated
+    (invalidate_lines).  Returns (chunks, session, expect, meta) with the
+    expected groups over the rows left visible."""
+    tbl, a, b, bnull, c_unscaled, g = _scan_table(nrows, seed_config, null_frac, ngroups)
+    session = scan_groupby_session(a_limit, ngroups)
+    chunks, keep = invalidate_lines(tbl.block_chunks(pages_per_chunk=pages_per_chunk), frac,
+                                    seed=seed_config + 1)
+    assert len(keep) == nrows
+    expect, meta = _scan_expect(a, b, bnull, c_unscaled, g, a_limit, ngroups, visible=keep)
+    return chunks, session, expect, meta
 
 
 def wide_groupby_session(a_limit=600, ngroups=3000, sort=None):

@@ -45,7 +45,8 @@ import xb_final as F  # noqa: E402
 
 # small enough that the oracle finishes each in about a second and each file
 # stays a few tens of KB
-CASES = ("scan", "nogroup", "wide", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls")
+CASES = ("scan", "nogroup", "wide", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls",
+         "filtered")
 
 # projection sessions: rows formed into a KDS_FORMAT_ROW kds_dst by the
 # reference's kern_estimate_minimal_tuple / kern_form_minimal_tuple
@@ -88,6 +89,10 @@ def case_inputs(which):
         # validity-bitmap NULLs only: the reference asserts that a row its
         # bitmap marks valid has a value (src/xpu_common.cu:273)
         chunks, sess, _, meta = C.arrow_nulls(nrows=30_000, nkeys=300, rows_per_chunk=10_000, short_rows=0)
+        km = None
+    elif which == "filtered":
+        # line pointers partly LP_UNUSED / LP_DEAD / LP_REDIRECT
+        chunks, sess, _, meta = C.scan_groupby_filtered(nrows=40_000, frac=0.2)
         km = None
     elif which == "scan_proj":
         tbl, sess, _, meta = C.scan_projection(nrows=20_000)

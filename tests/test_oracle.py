@@ -107,3 +107,19 @@ def test_oracle_arrow_nulls_and_short_buffers():
     assert st["nitems_in"] == meta["nitems_in"]
     assert (None,) in got
     assert F.compare_groups(got, expect) == []
+
+
+def test_oracle_skips_invalidated_line_pointers():
+    """Pages whose line pointers are partly LP_UNUSED, LP_DEAD or
+    LP_REDIRECT (as relscan.c leaves pages that are not all-visible, and as
+    HOT pruning leaves them): only LP_NORMAL items are rows, as the
+    reference's page walkers read them."""
+    chunks, sess, expect, meta = C.scan_groupby_filtered(nrows=80_000, frac=0.2)
+    assert meta["nitems_raw"] < 80_000 * 0.85
+    o = O.Oracle(sess)
+    for ch in chunks:
+        o.exec(ch)
+    st = o.stats()
+    assert st["nitems_raw"] == meta["nitems_raw"] and st["nitems_in"] == meta["nitems_in"]
+    assert F.compare_groups(F.decode_kds_final(o.final(), sess), _want_c0(expect)) == []
+    o.close()

@@ -45,7 +45,7 @@ def test_numeric_encoding_matches_reference():
 
 
 @pytest.mark.parametrize("which", ["scan", "join", "nogroup", "wide", "long_varlena", "join_long_text", "arrow",
-                                   "arrow_nulls"])
+                                   "arrow_nulls", "filtered"])
 def test_oracle_matches_reference_functions(which):
     """The oracle's groups equal those the reference's functions compute
     (rtol=0): heap scan and join, an aggregate without GROUP BY keys, every
@@ -55,7 +55,8 @@ def test_oracle_matches_reference_functions(which):
     text group keys of inner rows longer than 126 bytes, and Arrow columns
     read by ExecLoadVarsOuterArrow (int8 / int4 / float8 / date), also with
     validity bitmaps on every column (NULL keys, NULL filter inputs, NULL
-    arguments)."""
+    arguments), and heap pages whose line pointers are partly unused, dead
+    or redirected."""
     if which == "scan":
         tbl, sess, km, expect, meta = C.scan_groupby(nrows=60_000)
         chunks = tbl.block_chunks(pages_per_chunk=200)
@@ -79,6 +80,9 @@ def test_oracle_matches_reference_functions(which):
         # (validity NULLs only: the reference asserts that a row its bitmap
         # marks valid has a value, xpu_common.cu:273)
         chunks, sess, expect, meta = C.arrow_nulls(nrows=60_000, nkeys=500, rows_per_chunk=20_000, short_rows=0)
+        km = None
+    elif which == "filtered":
+        chunks, sess, expect, meta = C.scan_groupby_filtered(nrows=60_000, frac=0.2)
         km = None
     else:
         tbl, sess, km, expect, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
