@@ -30,18 +30,45 @@ def _translate(L, sess, km):
     return plan
 
 
-def _sessions():
-    _, s0, _, _, _ = C.scan_groupby(nrows=1000)
-    _, s1, k1, _, _ = C.join_groupby(nfact=1000, ndim1=100, ndim2=10)
-    _, s2, _, _ = C.arrow_groupby(nrows=1000, nkeys=100, rows_per_chunk=1000, with_expect=False)
-    return [("scan_groupby", s0, None, ord("b")), ("join_groupby", s1, k1, ord("b")),
-            ("arrow_groupby", s2, None, ord("a")), ("join_groupby_row", s1, k1, ord("r"))]
+def _session(case):
+    if case == "scan_groupby":
+        _, s, _, _, _ = C.scan_groupby(nrows=1000)
+        return s, None, ord("b")
+    if case in ("join_groupby", "join_groupby_row"):
+        _, s, k, _, _ = C.join_groupby(nfact=1000, ndim1=100, ndim2=10)
+        return s, k, ord("b" if case == "join_groupby" else "r")
+    if case == "arrow_groupby":
+        _, s, _, _ = C.arrow_groupby(nrows=1000, nkeys=100, rows_per_chunk=1000, with_expect=False)
+        return s, None, ord("a")
+    if case == "wide_groupby":
+        _, s, _, _, _ = C.wide_groupby(nrows=1000, ngroups=50)
+        return s, None, ord("b")
+    if case == "scan_nogroup":
+        _, s, _, _, _ = C.scan_nogroup(nrows=1000)
+        return s, None, ord("b")
+    if case == "long_varlena":
+        _, s, _, _, _ = C.long_varlena_groupby(nrows=1000)
+        return s, None, ord("b")
+    if case == "arrow_nulls":
+        _, s, _, _ = C.arrow_nulls(nrows=1000, nkeys=50, rows_per_chunk=1000)
+        return s, None, ord("a")
+    if case == "scan_projection":
+        _, s, _, _ = C.scan_projection(nrows=1000)
+        return s, None, ord("b")
+    if case == "join_projection":
+        _, s, k, _ = C.join_projection(nfact=1000, ndim1=100, ndim2=10)
+        return s, k, ord("b")
+    raise ValueError(case)
 
 
-@pytest.mark.parametrize("case", range(4))
-def test_specialised_kernel_compiles(case):
+CASES = ["scan_groupby", "join_groupby", "arrow_groupby", "join_groupby_row", "wide_groupby",
+         "scan_nogroup", "long_varlena", "arrow_nulls", "scan_projection", "join_projection"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_specialised_kernel_compiles(name):
     L = _lib()
-    name, sess, km, fmt = _sessions()[case]
+    sess, km, fmt = _session(name)
     plan = _translate(L, sess, km)
     nbytes = ctypes.c_uint64(0)
     ms = ctypes.c_double(0.0)
