@@ -3380,6 +3380,12 @@ static int xb_launch_exec(xpuB200Session *s, const kern_data_store *d_kds,
     return xb_launch_tasks(s, s->d_tasks, 1, t.nunits, t.format, err);
 }
 
+/* [off, off + len) lies inside [0, total), without a wrapping sum */
+static inline bool xb_within(uint64_t off, uint64_t len, uint64_t total)
+{
+    return off <= total && len <= total - off;
+}
+
 int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
 {
     if (kds->format == KDS_FORMAT_BLOCK) {
@@ -3393,13 +3399,17 @@ int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", kds->format);
     }
     if (kds->format == KDS_FORMAT_ARROW) {
-        for (uint32_t j = 0; j < kds->ncols && j < kds->nr_colmeta; j++) {
+        /* the kernels read colmeta[] up to ncols */
+        if (kds->ncols > kds->nr_colmeta)
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "Arrow chunk has %u columns but %u column descriptors",
+                          (unsigned)kds->ncols, (unsigned)kds->nr_colmeta);
+        for (uint32_t j = 0; j < kds->ncols; j++) {
             const kern_colmeta *cm = &kds->colmeta[j];
             if (cm->virtual_offset != 0)
                 continue;
-            if (cm->nullmap_offset + cm->nullmap_length > kds->length ||
-                cm->values_offset + cm->values_length > kds->length ||
-                cm->extra_offset + cm->extra_length > kds->length)
+            if (!xb_within(cm->nullmap_offset, cm->nullmap_length, kds->length) ||
+                !xb_within(cm->values_offset, cm->values_length, kds->length) ||
+                !xb_within(cm->extra_offset, cm->extra_length, kds->length))
                 return XB_ERR(err, ERRCODE_DEVICE_ERROR, "Arrow column %u is out of the chunk", j);
             /* value arrays are read with their natural width */
             if ((cm->values_offset & 7) != 0)
@@ -3407,6 +3417,14 @@ int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
         }
     }
     return 0;
+}
+
+/* the chunk checks ExecTask applies before a launch, for the host-side
+ * tests (no device needed) */
+extern "C" int xb_kds_check(const kern_data_store *kds, kern_errorbuf *err)
+{
+    xb_clear_error(err);
+    return xb_check_kds(kds, err);
 }
 
 /* wait for the launch and read its status (errors reported by the kernel) */

@@ -2,6 +2,9 @@
 import ctypes
 import os
 import re
+import struct
+
+import numpy as np
 
 import xpu_b200
 
@@ -29,3 +32,61 @@ def test_library_exports_declared_symbols():
 def test_library_is_sm100a_build():
     data = open(xpu_b200.LIB_PATH, "rb").read()
     assert b"sm_100a" in data
+
+
+def _kds_check(buf):
+    L = xpu_b200.lib()
+    L.xb_kds_check.argtypes = [ctypes.c_void_p, ctypes.POINTER(xpu_b200.KernErrorbuf)]
+    L.xb_kds_check.restype = ctypes.c_int
+    a = np.ascontiguousarray(buf)
+    eb = xpu_b200.KernErrorbuf()
+    rc = L.xb_kds_check(ctypes.c_void_p(a.ctypes.data), ctypes.byref(eb))
+    return rc, eb.message.decode()
+
+
+COLMETA, COLMETA_SZ = 72, 168
+
+
+def test_chunk_checks_reject_broken_chunks():
+    """The checks ExecTask applies to a chunk before any launch (no device
+    needed): well-formed heap and Arrow chunks pass; a chunk whose pages or
+    Arrow buffers lie outside its length, whose Arrow ranges wrap around
+    2^64, whose columns outnumber their descriptors, or whose format is
+    unknown is rejected with ERRCODE_DEVICE_ERROR and a message, so no
+    kernel reads outside the chunk."""
+    import xb_configs as C
+    tbl, _, _, _, _ = C.scan_groupby(nrows=2_000)
+    blk = tbl.block_chunks(pages_per_chunk=16)[0]
+    assert _kds_check(blk) == (0, "")
+
+    bad = blk.copy()
+    struct.pack_into("<I", bad, 16, 10_000)                       # nitems: pages past the length
+    rc, msg = _kds_check(bad)
+    assert rc == ord("E") and "broken" in msg
+    bad = blk.copy()
+    struct.pack_into("<I", bad, 44, 64)                           # block_offset inside the header
+    assert _kds_check(bad)[0] == ord("E")
+    bad = blk.copy()
+    bad[24] = ord("x")
+    rc, msg = _kds_check(bad)
+    assert rc == ord("E") and "unsupported KDS format" in msg
+
+    chunks, _, _, _ = C.arrow_groupby(nrows=2_000, nkeys=100, rows_per_chunk=2_000, with_expect=False)
+    arw = chunks[0]
+    assert _kds_check(arw) == (0, "")
+    ncols, = struct.unpack_from("<I", arw, 20)
+    for field in (120, 136, 152):                                 # nullmap, values, extra
+        bad = arw.copy()
+        off = COLMETA + COLMETA_SZ * (ncols - 1) + field
+        struct.pack_into("<QQ", bad, off, (1 << 64) - 8, 16)      # offset + length wraps to 8
+        rc, msg = _kds_check(bad)
+        assert rc == ord("E") and "out of the chunk" in msg, field
+    bad = arw.copy()
+    struct.pack_into("<I", bad, 68, ncols - 1)                    # nr_colmeta < ncols
+    rc, msg = _kds_check(bad)
+    assert rc == ord("E") and "column descriptors" in msg
+    bad = arw.copy()
+    values_offset, = struct.unpack_from("<Q", arw, COLMETA + 136)
+    struct.pack_into("<Q", bad, COLMETA + 136, values_offset + 4)
+    rc, msg = _kds_check(bad)
+    assert rc == ord("E") and "aligned" in msg
