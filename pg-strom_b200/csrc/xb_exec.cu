@@ -3392,9 +3392,13 @@ int xb_check_kds(const kern_data_store *kds, kern_errorbuf *err)
         if ((uint64_t)kds->block_offset + (uint64_t)PGSTROM_BLCKSZ * kds->nitems > kds->length ||
             kds->block_offset < KDS_HEAD_LENGTH(kds))
             return XB_ERR(err, ERRCODE_DEVICE_ERROR, "KDS_FORMAT_BLOCK chunk is broken");
-    } else if (kds->format == KDS_FORMAT_ARROW || kds->format == KDS_FORMAT_ROW) {
+    } else if (kds->format == KDS_FORMAT_ARROW) {
         if (KDS_HEAD_LENGTH(kds) > kds->length)
             return XB_ERR(err, ERRCODE_DEVICE_ERROR, "chunk header is broken");
+    } else if (kds->format == KDS_FORMAT_ROW) {
+        /* the kernels read the row index (after the hash slots) up to nitems */
+        if (!xb_within(KDS_HEAD_LENGTH(kds), 8ULL * ((uint64_t)kds->hash_nslots + kds->nitems), kds->length))
+            return XB_ERR(err, ERRCODE_DEVICE_ERROR, "KDS_FORMAT_ROW chunk is broken");
     } else {
         return XB_ERR(err, ERRCODE_DEVICE_ERROR, "unsupported KDS format '%c'", kds->format);
     }

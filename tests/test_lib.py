@@ -90,3 +90,22 @@ def test_chunk_checks_reject_broken_chunks():
     struct.pack_into("<Q", bad, COLMETA + 136, values_offset + 4)
     rc, msg = _kds_check(bad)
     assert rc == ord("E") and "aligned" in msg
+
+
+def test_chunk_checks_row_index_inside_the_chunk():
+    """A KDS_FORMAT_ROW source chunk: its row index (after the hash slots)
+    must fit in the chunk's length for every one of its nitems rows."""
+    import xb_configs as C
+    tbl, _, _, _, _ = C.scan_groupby(nrows=100)
+    head = bytes(tbl.kds_header("r", 10))
+    buf = np.zeros(len(head) + 8 * 10 + 64, dtype=np.uint8)
+    buf[:len(head)] = np.frombuffer(head, dtype=np.uint8)
+    struct.pack_into("<Q", buf, 0, buf.nbytes)
+    assert _kds_check(buf) == (0, "")
+    struct.pack_into("<I", buf, 16, 19)                           # 19 rows: the index runs 8 bytes past
+    rc, msg = _kds_check(buf)
+    assert rc == ord("E") and "ROW chunk is broken" in msg
+    struct.pack_into("<I", buf, 16, 10)
+    assert _kds_check(buf) == (0, "")
+    struct.pack_into("<I", buf, 40, 9)                            # 9 hash slots before the index
+    assert _kds_check(buf)[0] == ord("E")
