@@ -211,6 +211,14 @@ int xb_cuda_rc(cudaError_t rc, kern_errorbuf *err, const char *func, int line);
 int xb_set_sm_cap(xpuB200Session *s, uint32_t cap);
 std::tuple<int, uint64_t, uint32_t> xb_tune_key(xpuB200Session *s, uint32_t format);
 
+/* the group table's host side (xb_exec.cu), which the final stage
+ * (xb_final.cu) also drives: read its header, grow it, settle the groups
+ * waiting in its dump, wait for the session's launch and read its status */
+int xb_gt_read(xpuB200Session *s, xb_gtable *g, kern_errorbuf *err);
+int xb_gt_grow(xpuB200Session *s, uint64_t min_entries, kern_errorbuf *err);
+int xb_gt_settle(xpuB200Session *s, kern_errorbuf *err);
+int xb_wait_status(xpuB200Session *s, kern_errorbuf *err);
+
 /* mixed launches (xb_batch.cu), which the serving scheduler also issues:
  * the commands grouped by the kernel they run on, one launch per group */
 struct xb_mix_group {
