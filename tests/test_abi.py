@@ -37,3 +37,28 @@ def test_opcodes_match_reference():
                 # structural opcodes defined before the generated ones
                 assert name.startswith("FuncOpCode__"), name
     assert n > 100
+
+
+def test_c_client_of_the_abi(tmp_path):
+    """include/xpu_b200.h compiles as strict C99 and the library links into
+    a C program (PG-Strom's GPU service is C); from C, xpuB200HashBytes
+    equals the reference's pg_hash_any on its committed vectors, and
+    xpuB200Init attaches GPU 0 or, without one, fails with an error code
+    and a message rather than crashing."""
+    import json
+    lib_dir = os.path.join(ROOT, "pg-strom_b200")
+    if not os.path.exists(os.path.join(lib_dir, "libxpu_b200.so")):
+        import pytest
+        pytest.skip("library not built")
+    exe = tmp_path / "abi_c_client"
+    subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror",
+                    "-I" + os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "abi_c_client.c"),
+                    "-L" + lib_dir, "-lxpu_b200", "-Wl,-rpath," + lib_dir, "-o", str(exe)], check=True)
+    with open(os.path.join(GOLDEN, "ref_scalars.json")) as f:
+        vec = json.load(f)["hash_any"]
+    stdin = "\n".join(f"{h or '-'} {v}" for h, v in vec) + "\n"
+    r = subprocess.run([str(exe)], input=stdin, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    lines, bad, init = r.stdout.split()
+    assert (int(lines), int(bad)) == (len(vec), 0)
+    assert init in ("ok", "error")
