@@ -26,6 +26,15 @@
  *                       (execGpuJoinProjection, __kern_form_minimal_tuple)
  * Floating-point sums are accumulated in row order in plain FP64: this is
  * the "FP64 sequentially ordered sum" the GPU results are compared with.
+ *
+ * Parity pinned: against PG-Strom's own functions host-compiled from its
+ * sources (oracle/ref_harness.cpp: tuple and Arrow decode, quals, hash
+ * joins and aggregate arguments computed by the reference, groups equal
+ * with rtol=0; projected tuples byte for byte against its
+ * kern_form_minimal_tuple), against the golden vectors those functions
+ * produced (tests/golden/ref_*.json), against the reference's own Arrow
+ * test file and its CSV, and against the reference's device kernel built
+ * for sm_100a (oracle/ref_gpu.cpp).
  */
 #include <stdint.h>
 #include <stdlib.h>
