@@ -18,6 +18,17 @@ def available():
     return os.path.exists(SO)
 
 
+def source_dir():
+    """PG-Strom's src/ directory the library was built from (recorded by
+    oracle/Makefile "ref"), or None."""
+    rec = os.path.join(HERE, "_ref", "pgstrom_src.txt")
+    if not os.path.exists(rec):
+        return None
+    with open(rec) as f:
+        path = f.read().strip()
+    return path if os.path.isdir(path) else None
+
+
 def lib():
     global _LIB
     if _LIB is None:

@@ -129,9 +129,12 @@ PY_DATA_COLS = ["a_int32", "b_int64", "e_double", "f_string", "g_enum", "i_date"
 
 
 def _reference_test_data(name):
-    src = os.environ.get("PGSTROM_SRC", "/root/reference/src")
-    path = os.path.join(os.path.dirname(os.path.abspath(src)), "test", "data", name)
-    if not os.path.exists(path):
+    """The reference tree's test/data/<name>, next to the src/ directory
+    PGSTROM_SRC names or oracle/_ref was built from."""
+    import ref_pin
+    src = os.environ.get("PGSTROM_SRC") or ref_pin.source_dir()
+    path = os.path.join(os.path.dirname(os.path.abspath(src)), "test", "data", name) if src else None
+    if not path or not os.path.exists(path):
         pytest.skip(f"the reference's test/data/{name} is not present")
     return path
 
