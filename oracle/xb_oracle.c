@@ -980,7 +980,15 @@ int xo_exec(xo_sess *s, const kern_data_store *kds, char *errmsg, int errlen)
                 /* a row past the values buffer reads as NULL, as the
                  * reference's readers have it (KDS_ARROW_REF_SIMPLE_DATUM,
                  * KDS_ARROW_REF_VARLENA32_DATUM, xpu_common.h:1557-1605) */
-                {
+                if (tc == TypeOpCode__bool) {
+                    /* bit-packed values (xpu_bool_datum_arrow_read,
+                     * xpu_basetype.cu:37-57).  That reader does not bound
+                     * the bitmap; a row past it reads as NULL here, as the
+                     * reference's other fixed-width readers have it and as
+                     * the device's reader does */
+                    if (((uint64_t)row >> 3) >= cm->values_length)
+                        continue;
+                } else {
                     const uint64_t unitsz = tc == TypeOpCode__int2 ? 2 :
                                             (tc == TypeOpCode__int4 || tc == TypeOpCode__date ||
                                              tc == TypeOpCode__text) ? 4 : 8;
@@ -994,6 +1002,7 @@ int xo_exec(xo_sess *s, const kern_data_store *kds, char *errmsg, int errlen)
                 }
                 d->type_code = tc;
                 switch (tc) {
+                case TypeOpCode__bool: d->kind = DK_INT; d->i = (vals[row >> 3] >> (row & 7)) & 1; break;
                 case TypeOpCode__int2: d->kind = DK_INT; d->i = ((const int16_t *)vals)[row]; break;
                 case TypeOpCode__int4: d->kind = DK_INT; d->i = ((const int32_t *)vals)[row]; break;
                 case TypeOpCode__int8: d->kind = DK_INT; d->i = ((const int64_t *)vals)[row]; break;

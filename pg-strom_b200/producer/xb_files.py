@@ -18,7 +18,7 @@ import numpy as np
 from xb_producer import BLCKSZ, Column, Table, maxalign
 
 # ArrowType tags of the KDS_FORMAT_ARROW column options (arrow_defs.h)
-_TAG_INT, _TAG_FLOAT, _TAG_UTF8, _TAG_DATE = 2, 3, 5, 8
+_TAG_INT, _TAG_FLOAT, _TAG_UTF8, _TAG_BOOL, _TAG_DATE = 2, 3, 5, 6, 8
 
 
 # ---------------------------------------------------------------- heap files
@@ -140,6 +140,8 @@ def _column_type(t):
         return "int4"
     if pa.types.is_int16(t):
         return "int2"
+    if pa.types.is_boolean(t):
+        return "bool"
     if pa.types.is_float64(t):
         return "float8"
     if pa.types.is_date32(t):
@@ -170,6 +172,12 @@ def _buffers(arr):
         base = int(offs[0])
         ent.update({"tag": _TAG_UTF8, "values": (offs - base).astype(np.int32),
                     "data": data[base:int(offs[-1])].copy()})
+        return ent
+    if pa.types.is_boolean(t):
+        # bit-packed values, re-based so that row 0 is bit 0
+        bits = np.unpackbits(np.frombuffer(bufs[1], dtype=np.uint8), bitorder="little")
+        vals = np.packbits(bits[arr.offset:arr.offset + n], bitorder="little")
+        ent.update({"tag": _TAG_BOOL, "values": vals})
         return ent
     width = {"int8": 8, "int4": 4, "int2": 2, "float8": 8, "date": 4}[_column_type(t)]
     vals = np.frombuffer(bufs[1], dtype=np.uint8)[arr.offset * width:(arr.offset + n) * width].copy()

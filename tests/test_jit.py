@@ -58,11 +58,18 @@ def _session(case):
     if case == "join_projection":
         _, s, k, _ = C.join_projection(nfact=1000, ndim1=100, ndim2=10)
         return s, k, ord("b")
+    if case == "arrow_int2_bool":
+        import pathlib
+        import tempfile
+        from test_files import arrow_int2_bool_case
+        with tempfile.TemporaryDirectory() as d:
+            _, s, _, _ = arrow_int2_bool_case(pathlib.Path(d), nrows=1000)
+        return s, None, ord("a")
     raise ValueError(case)
 
 
 CASES = ["scan_groupby", "join_groupby", "arrow_groupby", "join_groupby_row", "wide_groupby",
-         "scan_nogroup", "long_varlena", "arrow_nulls", "scan_projection", "join_projection"]
+         "scan_nogroup", "long_varlena", "arrow_nulls", "scan_projection", "join_projection", "arrow_int2_bool"]
 
 
 @pytest.mark.parametrize("name", CASES)
