@@ -374,8 +374,52 @@ extern "C" int ref_exec(void *handle, const kern_data_store *kds, char *errbuf, 
         }
         return 0;
     }
+    if (kds->format == KDS_FORMAT_ROW) {
+        /* rows by index as __gpuscan_load_source_row reads them
+         * (cuda_gpuscan.cu:646-700): KDS_GET_TUPITEM, the depth-0 load by
+         * ExecLoadVarsMinimalTuple, then the scan quals; the rows carry no
+         * transaction attributes (the visibility check is device code) */
+        kern_expression *kquals = SESSION_KEXP_SCAN_QUALS(session);
+        for (uint32_t i = 0; i < kds->nitems; i++) {
+            kern_tupitem *titem = KDS_GET_TUPITEM(kds, i);
+            if (!titem) continue;
+            if (titem->has_xact_attrs) {
+                snprintf(errbuf, errlen, "ref harness: row %u carries transaction attributes", i);
+                return -1;
+            }
+            s->nraw++;
+            kcxt_reset(kcxt);
+            kcxt->kvecs_curr_buffer = NULL;
+            kcxt->kvecs_curr_id = 0;
+            if (!ExecLoadVarsMinimalTuple(kcxt, SESSION_KEXP_LOAD_VARS(session, 0), 0, kds, titem)) {
+                snprintf(errbuf, errlen, "%s", kcxt->errcode ? kcxt->error_message : "row load failed");
+                return -1;
+            }
+            if (kquals) {
+                xpu_bool_t ok;
+                if (!EXEC_KERN_EXPRESSION(kcxt, kquals, &ok)) {
+                    snprintf(errbuf, errlen, "%s", kcxt->error_message ? kcxt->error_message : "quals failed");
+                    return -1;
+                }
+                if (XPU_DATUM_ISNULL(&ok) || !ok.value)
+                    continue;
+            }
+            s->nin++;
+            if (!ExecMoveKernelVariables(kcxt, SESSION_KEXP_MOVE_VARS(session, 0), kvecs[0].data(), 0)) {
+                snprintf(errbuf, errlen, "move vars at depth 0 failed");
+                return -1;
+            }
+            process_depth(s, kcxt, 1, kvecs);
+            if (!s->err.empty() || kcxt->errcode) {
+                snprintf(errbuf, errlen, "%s %s", s->err.c_str(),
+                         kcxt->error_message ? kcxt->error_message : "");
+                return -1;
+            }
+        }
+        return 0;
+    }
     if (kds->format != KDS_FORMAT_BLOCK) {
-        snprintf(errbuf, errlen, "ref harness handles KDS_FORMAT_BLOCK and KDS_FORMAT_ARROW");
+        snprintf(errbuf, errlen, "ref harness handles KDS_FORMAT_BLOCK, KDS_FORMAT_ARROW and KDS_FORMAT_ROW");
         return -1;
     }
     for (uint32_t b = 0; b < kds->nitems; b++) {

@@ -1024,6 +1024,41 @@ int xo_exec(xo_sess *s, const kern_data_store *kds, char *errmsg, int errlen)
             }
             if (!process_row(s)) { snprintf(errmsg, errlen, "%s", s->err.msg); return -1; }
         }
+    } else if (kds->format == KDS_FORMAT_ROW) {
+        /* rows by index (__gpuscan_load_source_row, cuda_gpuscan.cu:646-700):
+         * the row index after the hash slots holds each kern_tupitem's
+         * offset back from the chunk's end (KDS_GET_TUPITEM,
+         * xpu_common.h:1337-1345); the tuple's header and data follow the
+         * heap tuple's from t_infomask2 on, MINIMAL_TUPLE_OFFSET bytes
+         * later (kern_extract_minimal_tuple, xpu_common.cu:132-191).  Rows
+         * carry no transaction attributes here (they would be checked for
+         * visibility); an empty slot is no row */
+        const uint64_t *rowindex = (const uint64_t *)((const char *)kds + KDS_HEAD_LENGTH(kds)) + kds->hash_nslots;
+        for (uint32_t row = 0; row < kds->nitems; row++) {
+            const uint64_t off = rowindex[row];
+            if (off == 0) continue;
+            if (off > kds->length || off < 16 || ((kds->length - off) & 7) != 0) {
+                snprintf(errmsg, errlen, "KDS_FORMAT_ROW row %u is out of the chunk", row);
+                return -1;
+            }
+            const uint8_t *ti = (const uint8_t *)kds + kds->length - off;
+            uint32_t t_len; memcpy(&t_len, ti, 4);
+            uint16_t im2, im; memcpy(&im2, ti + 10, 2); memcpy(&im, ti + 12, 2);
+            const uint32_t t_hoff = ti[14];
+            if (ti[8] != 0 || t_hoff < MINIMAL_TUPLE_OFFSET + 15 || t_hoff - MINIMAL_TUPLE_OFFSET > t_len ||
+                t_len > off) {
+                snprintf(errmsg, errlen, "KDS_FORMAT_ROW row %u is broken", row);
+                return -1;
+            }
+            int natts = im2 & HEAP_NATTS_MASK;
+            if (natts > (int)kds->ncols) natts = kds->ncols;
+            s->nitems_raw++;
+            if (!decode_tuple(s, kds, natts, (im & HEAP_HASNULL) ? ti + 15 : NULL,
+                              ti + t_hoff - MINIMAL_TUPLE_OFFSET, s->load[0]) || !process_row(s)) {
+                snprintf(errmsg, errlen, "%s", s->err.msg);
+                return -1;
+            }
+        }
     } else {
         snprintf(errmsg, errlen, "unsupported KDS format");
         return -1;

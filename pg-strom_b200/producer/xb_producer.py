@@ -477,6 +477,52 @@ class Table:
             blk += np_
         return chunks
 
+    def row_chunks(self, rows_per_chunk=20_000):
+        """KDS_FORMAT_ROW chunks of the table's rows in table order, the
+        outer-chunk form the reference's __gpuscan_load_source_row reads
+        (cuda_gpuscan.cu:646-700): the header, the row index of nitems
+        offsets counted back from the chunk's end (KDS_GET_TUPITEM,
+        xpu_common.h:1337-1345), and the rows as kern_tupitems from the end,
+        8-byte aligned.  A kern_tupitem is its length and hash words, no
+        transaction attributes, the heap tuple's header from t_infomask2 on
+        with t_hoff kept relative to the heap tuple (MINIMAL_TUPLE_OFFSET
+        bytes before the item), its data, and the row id at its tail."""
+        images = []
+        for ch in self.block_chunks():
+            nblocks, = struct.unpack_from("<I", ch, 16)
+            block_offset, = struct.unpack_from("<I", ch, 44)
+            for b in range(nblocks):
+                base = block_offset + b * BLCKSZ
+                lower, = struct.unpack_from("<H", ch, base + 12)
+                for i in range((lower - 24) // 4):
+                    lp, = struct.unpack_from("<I", ch, base + 24 + 4 * i)
+                    off, flags, ln = lp & 0x7fff, (lp >> 15) & 3, lp >> 17
+                    if flags != 1:
+                        continue
+                    images.append(bytes(ch[base + off + 18:base + off + ln]))
+        chunks = []
+        for c0 in range(0, len(images), rows_per_chunk):
+            part = images[c0:c0 + rows_per_chunk]
+            head = self.kds_header("r", len(part))
+            head_len = len(head)
+            items = []
+            for rowid, tail in enumerate(part):
+                t_len = 10 + len(tail) + 4
+                items.append(struct.pack("<IIBB", t_len, 0, 0, 0) + tail + struct.pack("<I", rowid))
+            sizes = [maxalign(len(t)) for t in items]
+            usage = sum(sizes)
+            length = head_len + 8 * len(part) + usage
+            buf = np.zeros(length, dtype=np.uint8)
+            buf[:head_len] = np.frombuffer(bytes(head), dtype=np.uint8)
+            struct.pack_into("<QQ", buf, 0, length, usage)
+            back = 0
+            for j, (t, sz) in enumerate(zip(items, sizes)):
+                back += sz
+                struct.pack_into("<Q", buf, head_len + 8 * j, back)
+                buf[length - back:length - back + len(t)] = np.frombuffer(t, dtype=np.uint8)
+            chunks.append(buf)
+        return chunks
+
     def hash_kds(self, hashes: np.ndarray) -> np.ndarray:
         """KDS_FORMAT_HASH inner buffer with host-computed hash per row."""
         hg = _heapgen()

@@ -109,3 +109,5 @@ def test_chunk_checks_row_index_inside_the_chunk():
     assert _kds_check(buf) == (0, "")
     struct.pack_into("<I", buf, 40, 9)                            # 9 hash slots before the index
     assert _kds_check(buf)[0] == ord("E")
+    for ch in tbl.row_chunks(rows_per_chunk=30):                  # chunks of the ROW producer
+        assert _kds_check(ch) == (0, "")

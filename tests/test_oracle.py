@@ -123,3 +123,27 @@ def test_oracle_skips_invalidated_line_pointers():
     assert st["nitems_raw"] == meta["nitems_raw"] and st["nitems_in"] == meta["nitems_in"]
     assert F.compare_groups(F.decode_kds_final(o.final(), sess), _want_c0(expect)) == []
     o.close()
+
+
+def test_oracle_row_chunks():
+    """KDS_FORMAT_ROW outer chunks (kern_tupitems, row index from the
+    chunk's end) of the same tables: the oracle's groups equal the arrays'
+    and those of the heap chunks, with NULLs, 4-byte varlena headers and
+    long numerics."""
+    tbl, sess, _, expect, meta = C.scan_groupby(nrows=50_000)
+    o = O.Oracle(sess)
+    for ch in tbl.row_chunks(rows_per_chunk=12_000):
+        o.exec(ch)
+    st = o.stats()
+    assert st["nitems_raw"] == meta["nitems_raw"] and st["nitems_in"] == meta["nitems_in"]
+    assert F.compare_groups(F.decode_kds_final(o.final(), sess), _want_c0(expect)) == []
+    o.close()
+    tbl, sess, _, _, _ = C.long_varlena_groupby(nrows=10_000)
+    got = []
+    for chunks in (tbl.row_chunks(rows_per_chunk=3_000), tbl.block_chunks(pages_per_chunk=50)):
+        o = O.Oracle(sess)
+        for ch in chunks:
+            o.exec(ch)
+        got.append(F.decode_kds_final(o.final(), sess))
+        o.close()
+    assert F.compare_groups(got[0], got[1], rtol=0.0) == []

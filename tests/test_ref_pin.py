@@ -45,7 +45,7 @@ def test_numeric_encoding_matches_reference():
 
 
 @pytest.mark.parametrize("which", ["scan", "join", "nogroup", "wide", "long_varlena", "join_long_text", "arrow",
-                                   "arrow_nulls", "filtered"])
+                                   "arrow_nulls", "filtered", "row_scan", "row_wide"])
 def test_oracle_matches_reference_functions(which):
     """The oracle's groups equal those the reference's functions compute
     (rtol=0): heap scan and join, an aggregate without GROUP BY keys, every
@@ -55,8 +55,9 @@ def test_oracle_matches_reference_functions(which):
     text group keys of inner rows longer than 126 bytes, and Arrow columns
     read by ExecLoadVarsOuterArrow (int8 / int4 / float8 / date), also with
     validity bitmaps on every column (NULL keys, NULL filter inputs, NULL
-    arguments), and heap pages whose line pointers are partly unused, dead
-    or redirected."""
+    arguments), heap pages whose line pointers are partly unused, dead
+    or redirected, and KDS_FORMAT_ROW outer chunks read by
+    ExecLoadVarsMinimalTuple."""
     if which == "scan":
         tbl, sess, km, expect, meta = C.scan_groupby(nrows=60_000)
         chunks = tbl.block_chunks(pages_per_chunk=200)
@@ -84,6 +85,12 @@ def test_oracle_matches_reference_functions(which):
     elif which == "filtered":
         chunks, sess, expect, meta = C.scan_groupby_filtered(nrows=60_000, frac=0.2)
         km = None
+    elif which == "row_scan":
+        tbl, sess, km, expect, meta = C.scan_groupby(nrows=40_000)
+        chunks = tbl.row_chunks(rows_per_chunk=9_000)
+    elif which == "row_wide":
+        tbl, sess, km, expect, meta = C.wide_groupby(nrows=40_000, ngroups=500)
+        chunks = tbl.row_chunks(rows_per_chunk=9_000)
     else:
         tbl, sess, km, expect, meta = C.join_groupby(nfact=60_000, ndim1=3000, ndim2=500)
         chunks = tbl.block_chunks(pages_per_chunk=200)
