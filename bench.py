@@ -251,9 +251,10 @@ def build_workload(nrows, rank):
 
 # ------------------------------------------------------------------ CPU arms
 def cpu_rows_per_sec(sess, km, chunks, seconds, threads, allow_ref=True):
-    """Runs the reference's host-compiled functions (or the C oracle) over
-    chunks on 'threads' threads until 'seconds' of wall time; rows/s.  The
-    reference harness reads heap chunks only (allow_ref=False for Arrow)."""
+    """Runs the reference's host-compiled functions (or, where oracle/_ref
+    was not built, the C oracle) over chunks on 'threads' threads until
+    'seconds' of wall time; rows/s.  The reference harness reads heap,
+    Arrow and ROW chunks and counts rows without writing its groups out."""
     import ref_pin
     import xb_oracle as O
     use_ref = allow_ref and ref_pin.available()
@@ -270,8 +271,7 @@ def cpu_rows_per_sec(sess, km, chunks, seconds, threads, allow_ref=True):
                 state["next"] += 1
             ch = chunks[i]
             if use_ref:
-                res = ref_pin.run(sess, [ch], km)
-                n = res["nitems_raw"]
+                n = ref_pin.run_counts(sess, [ch], km)["nitems_raw"]
             else:
                 before = o.stats()["nitems_raw"]
                 o.exec(ch)
@@ -644,19 +644,17 @@ def _config_workload(args, nrows):
 
 def run_reference_config(args):
     """The reference arm of the scan and Arrow configurations: the
-    reference's host-compiled functions (heap) or the C restatement (Arrow,
-    which the reference harness does not read) on every host thread, over
-    a bounded sample of the same workload per step."""
+    reference's host-compiled functions on every host thread, over a
+    bounded sample of the same workload per step."""
     nrows = min(args.rows, 20_000_000)
     chunks, sess, _, meta, desc, _ = _config_workload(args, nrows)
     threads = os.cpu_count() or 1
-    heap = args.workload == "scan_groupby"
     per_step = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_rows_per_sec(sess, None, chunks, per_step / 2, threads, allow_ref=heap)
+        cpu_rows_per_sec(sess, None, chunks, per_step / 2, threads)
     total_rows, total_s, kind = 0, 0.0, "port"
     for _ in range(args.steps):
-        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks, per_step, threads, allow_ref=heap)
+        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks, per_step, threads)
         total_rows += rows
         total_s += el
     value = total_rows / total_s
@@ -736,8 +734,7 @@ def run_config(args):
             line["reference_gpu"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if args.cpu_seconds > 0:
         threads = os.cpu_count() or 1
-        heap = args.workload == "scan_groupby"
-        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks[:8], args.cpu_seconds, threads, allow_ref=heap)
+        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks[:8], args.cpu_seconds, threads)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"{rows} rows of the same workload in {el:.1f} s on {threads} threads "
                                           f"({'PG-Strom expression library host-compiled from the reference' if kind == 'reference' else 'C restatement'})"}

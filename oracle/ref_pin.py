@@ -44,6 +44,7 @@ def lib():
         L.ref_result.argtypes = [P, ctypes.c_char_p, ctypes.c_uint64]
         L.ref_result.restype = ctypes.c_uint64
         L.ref_close.argtypes = [P]
+        L.ref_counts.argtypes = [P, ctypes.POINTER(ctypes.c_uint64)]
         _LIB = L
     return _LIB
 
@@ -64,6 +65,27 @@ def numeric_decode(vl: bytes):
     if v >= 1 << 127:
         v -= 1 << 128
     return k.value, w.value, v
+
+
+def run_counts(session: bytes, chunks, kmrels=None):
+    """Runs the reference functions over the chunks; returns the row
+    counters only (no groups written out)."""
+    sess = np.frombuffer(session + b"\0" * 64, dtype=np.uint8).copy()
+    km = kmrels.copy() if kmrels is not None else None
+    err = ctypes.create_string_buffer(256)
+    h = lib().ref_open(ctypes.c_void_p(sess.ctypes.data), len(session),
+                       ctypes.c_void_p(km.ctypes.data) if km is not None else None, err, 256)
+    if not h:
+        raise RuntimeError("ref_open: " + err.value.decode())
+    try:
+        for ch in chunks:
+            if lib().ref_exec(h, ctypes.c_void_p(ch.ctypes.data), err, 256):
+                raise RuntimeError("ref_exec: " + err.value.decode())
+        out = (ctypes.c_uint64 * 3)()
+        lib().ref_counts(h, out)
+        return {"nitems_raw": out[0], "nitems_in": out[1], "nitems_out": out[2]}
+    finally:
+        lib().ref_close(h)
 
 
 def run(session: bytes, chunks, kmrels=None):

@@ -165,3 +165,15 @@ def test_projection_matches_reference_functions(which):
     assert sorted(mine) == ref
     fx = G.load(f"ref_proj_{which}.json")
     assert G.rows_digest(ref) == fx["rows_sha256"]
+
+
+def test_counts_only_run_matches():
+    """ref_pin.run_counts (the bench's reference arm: no groups written
+    out) counts the same rows as the full run, on heap and Arrow chunks."""
+    tbl, sess, km, _, _ = C.join_groupby(nfact=30_000, ndim1=2000, ndim2=300)
+    chunks = tbl.block_chunks(pages_per_chunk=100)
+    full = ref_pin.run(sess, chunks, km)
+    assert ref_pin.run_counts(sess, chunks, km) == {k: full[k] for k in ("nitems_raw", "nitems_in", "nitems_out")}
+    achunks, asess, _, _ = C.arrow_groupby(nrows=30_000, nkeys=3_000, rows_per_chunk=10_000)
+    full = ref_pin.run(asess, achunks)
+    assert ref_pin.run_counts(asess, achunks) == {k: full[k] for k in ("nitems_raw", "nitems_in", "nitems_out")}
