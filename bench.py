@@ -625,9 +625,17 @@ def run_b200(args, rank, world, local):
 
 
 # ------------------------------------------------------------------ other configurations
-def _config_workload(args, nrows):
+# The reference's functions keep one session's groups per host thread: the
+# CPU arms read the Arrow configuration in chunks of this many rows, so that
+# a thread holds tens of thousands of groups rather than the half million of
+# a 2.5M-row chunk (about 50 MB against 460 MB per thread)
+CPU_ARROW_CHUNK_ROWS = 250_000
+
+
+def _config_workload(args, nrows, rows_per_chunk=None):
     """(chunks, session, truth or None, meta, description, referenced bytes)
-    of the scan or Arrow configuration at nrows"""
+    of the scan or Arrow configuration at nrows (rows_per_chunk: Arrow
+    chunks of that many rows instead of the configuration's)"""
     import xb_configs as C
     if args.workload == "scan_groupby":
         tbl, sess, _, expect, meta = C.scan_groupby(nrows=nrows)
@@ -636,7 +644,8 @@ def _config_workload(args, nrows):
                 "GROUP BY g (64 groups) -> count, sum(a), sum(c numeric), avg(b)")
         truth = {k: [v["nrows"], v["sum_a"], v["sum_c"], v["avg_b"]] for k, v in expect.items()}
         return chunks, sess, truth, meta, desc, sum(c.nbytes for c in chunks)
-    chunks, sess, _, meta = C.arrow_groupby(nrows=nrows, nkeys=args.keys, with_expect=False)
+    kw = {"rows_per_chunk": rows_per_chunk} if rows_per_chunk else {}
+    chunks, sess, _, meta = C.arrow_groupby(nrows=nrows, nkeys=args.keys, with_expect=False, **kw)
     desc = (f"Arrow high-cardinality pre-aggregation: {nrows} rows, {args.keys} keys, 2-year date "
             "window -> GROUP BY k: count, sum(v1), min/max/sum(v2)")
     return chunks, sess, None, meta, desc, 24 * nrows
@@ -647,7 +656,9 @@ def run_reference_config(args):
     reference's host-compiled functions on every host thread, over a
     bounded sample of the same workload per step."""
     nrows = min(args.rows, 20_000_000)
-    chunks, sess, _, meta, desc, _ = _config_workload(args, nrows)
+    arrow = args.workload != "scan_groupby"
+    chunks, sess, _, meta, desc, _ = _config_workload(args, nrows,
+                                                      CPU_ARROW_CHUNK_ROWS if arrow else None)
     threads = os.cpu_count() or 1
     per_step = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
@@ -664,7 +675,8 @@ def run_reference_config(args):
             "data": "synthetic", "config": {"workload": desc + " (bounded sample per step)",
                                             "rows_generated": nrows, "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{total_rows} rows over {total_s:.1f} s ({per_step:.1f} s per step)"},
+                             "sample": f"{total_rows} rows over {total_s:.1f} s ({per_step:.1f} s per step)"
+                                       + (f", in {CPU_ARROW_CHUNK_ROWS}-row chunks" if arrow else "")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -734,10 +746,15 @@ def run_config(args):
             line["reference_gpu"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if args.cpu_seconds > 0:
         threads = os.cpu_count() or 1
-        v, kind, rows, el = cpu_rows_per_sec(sess, None, chunks[:8], args.cpu_seconds, threads)
+        cchunks = chunks[:8]
+        if args.workload != "scan_groupby":
+            cchunks = _config_workload(args, 8 * CPU_ARROW_CHUNK_ROWS, CPU_ARROW_CHUNK_ROWS)[0]
+        v, kind, rows, el = cpu_rows_per_sec(sess, None, cchunks, args.cpu_seconds, threads)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"{rows} rows of the same workload in {el:.1f} s on {threads} threads "
-                                          f"({'PG-Strom expression library host-compiled from the reference' if kind == 'reference' else 'C restatement'})"}
+                                          + (f"in {CPU_ARROW_CHUNK_ROWS}-row chunks "
+                                             if args.workload != "scan_groupby" else "")
+                                          + f"({'PG-Strom expression library host-compiled from the reference' if kind == 'reference' else 'C restatement'})"}
     print(json.dumps(line), flush=True)
     batch.close()
     s.close()
