@@ -749,3 +749,45 @@ def mixed_commands(ncmds=256, min_bytes=64 << 10, max_bytes=64 << 20, min_sel=0.
         out.append({"chunk": chunk, "session": sess, "truth": truth, "meta": meta,
                     "params": {"rows": nrows, "a_limit": a_limit, "groups": groups}})
     return out
+
+
+def arrow_int2_bool(workdir, nrows=30_000, seed=33, null_frac=0.1, batch_rows=7_001):
+    """An Arrow IPC file written into workdir (k int16, flag bool with NULLs,
+    v int32, w int64; record batches of batch_rows rows, each batch's last
+    bitmap byte partly used) read back by the chunk producer, and
+    WHERE flag GROUP BY k -> count(*), sum(v::int8), min(w), max(w).
+    Returns (chunks, session, expect, meta)."""
+    import os
+    import pyarrow as pa
+    import xb_files as XF
+    r = np.random.default_rng(seed)
+    k = r.integers(-300, 300, nrows).astype(np.int16)
+    flag = r.random(nrows) < 0.6
+    fnull = r.random(nrows) < null_frac
+    v = r.integers(-10**6, 10**6, nrows, dtype=np.int32)
+    w = r.integers(-10**15, 10**15, nrows, dtype=np.int64)
+    tbl = pa.table({"k": pa.array(k), "flag": pa.array(flag, mask=fnull), "v": pa.array(v),
+                    "w": pa.array(w)})
+    path = os.path.join(workdir, "int2_bool.arrow")
+    with pa.OSFile(path, "wb") as sink:
+        with pa.ipc.new_file(sink, tbl.schema) as wr:
+            for b in tbl.to_batches(max_chunksize=batch_rows):
+                wr.write_batch(b)
+    chunks, tdef = XF.arrow_ipc_chunks(path)
+    vk, vf, vv, vw = Var(0, 1, "int2"), Var(0, 2, "bool"), Var(0, 3, "int4"), Var(0, 4, "int8")
+    session = SessionBuilder(0, DEVTASK_PREAGG | DEVKIND_GPU).build(
+        scan_quals=vf,
+        groupby_keys=[vk],
+        aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Func("int4_to_int8", [vv], "int8")),
+              Agg("PMIN_INT64", vw), Agg("PMAX_INT64", vw)],
+        ngroups_estimate=600.0)
+    m = flag & ~fnull
+    expect = {}
+    for key in np.unique(k[m]).tolist():
+        sel = m & (k == key)
+        n = int(sel.sum())
+        expect[(key,)] = [n, (n, int(v[sel].astype(np.int64).sum())), (1, int(w[sel].min())),
+                          (1, int(w[sel].max()))]
+    meta = {"nitems_raw": nrows, "nitems_in": int(m.sum()), "nitems_out": int(m.sum()),
+            "types": [c.typ for c in tdef.columns]}
+    return chunks, session, expect, meta

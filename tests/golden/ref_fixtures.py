@@ -46,7 +46,7 @@ import xb_final as F  # noqa: E402
 # small enough that the oracle finishes each in about a second and each file
 # stays a few tens of KB
 CASES = ("scan", "nogroup", "wide", "join", "long_varlena", "join_long_text", "arrow", "arrow_nulls",
-         "filtered", "row_long_varlena")
+         "filtered", "row_long_varlena", "arrow_int2_bool")
 
 # projection sessions: rows formed into a KDS_FORMAT_ROW kds_dst by the
 # reference's kern_estimate_minimal_tuple / kern_form_minimal_tuple
@@ -98,6 +98,12 @@ def case_inputs(which):
         # KDS_FORMAT_ROW outer chunks (kern_tupitems) of the long-varlena table
         tbl, sess, km, _, meta = C.long_varlena_groupby(nrows=12_000)
         chunks = tbl.row_chunks(rows_per_chunk=5_000)
+    elif which == "arrow_int2_bool":
+        # Arrow Int16 keys and a bit-packed Bool filter with NULLs, through an IPC file
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            chunks, sess, _, meta = C.arrow_int2_bool(d)
+        km = None
     elif which == "scan_proj":
         tbl, sess, _, meta = C.scan_projection(nrows=20_000)
         chunks, km = tbl.block_chunks(pages_per_chunk=64), None

@@ -230,50 +230,15 @@ def test_reference_arrow_fixture_groups():
         assert F.compare_groups(G.decode_groups(res, sess), want, rtol=0.0) == []
 
 
-def arrow_int2_bool_case(tmp_path, nrows=30_000, seed=33, null_frac=0.1):
-    """An Arrow IPC file (k int16, flag bool with NULLs, v int32, w int64)
-    and WHERE flag GROUP BY k -> count(*), sum(v::int8), min(w), max(w),
-    with its expected groups."""
-    import pyarrow as pa
-    r = np.random.default_rng(seed)
-    k = r.integers(-300, 300, nrows).astype(np.int16)
-    flag = r.random(nrows) < 0.6
-    fnull = r.random(nrows) < null_frac
-    v = r.integers(-10**6, 10**6, nrows, dtype=np.int32)
-    w = r.integers(-10**15, 10**15, nrows, dtype=np.int64)
-    tbl = pa.table({"k": pa.array(k), "flag": pa.array(flag, mask=fnull), "v": pa.array(v),
-                    "w": pa.array(w)})
-    path = str(tmp_path / "int2_bool.arrow")
-    with pa.OSFile(path, "wb") as sink:
-        with pa.ipc.new_file(sink, tbl.schema) as wr:
-            for b in tbl.to_batches(max_chunksize=7_001):     # batches of a row count not a multiple of 8
-                wr.write_batch(b)
-    vk, vf, vv, vw = Var(0, 1, "int2"), Var(0, 2, "bool"), Var(0, 3, "int4"), Var(0, 4, "int8")
-    sess = SessionBuilder(0, C.DEVTASK_PREAGG | C.DEVKIND_GPU).build(
-        scan_quals=vf,
-        groupby_keys=[vk],
-        aggs=[Agg("NROWS_ANY"), Agg("PSUM_INT", Func("int4_to_int8", [vv], "int8")),
-              Agg("PMIN_INT64", vw), Agg("PMAX_INT64", vw)],
-        ngroups_estimate=600.0)
-    m = flag & ~fnull
-    expect = {}
-    for key in np.unique(k[m]).tolist():
-        sel = m & (k == key)
-        n = int(sel.sum())
-        expect[(key,)] = [n, (n, int(v[sel].astype(np.int64).sum())), (1, int(w[sel].min())),
-                          (1, int(w[sel].max()))]
-    return path, sess, expect, int(m.sum())
-
-
 def test_arrow_int16_and_bool_columns(tmp_path):
     """Arrow Int16 keys and a bit-packed Bool filter with NULLs, in record
     batches of 7,001 rows (each batch's last bitmap byte partly used): the
     oracle against the arrays, and, where oracle/_ref is built, the
     reference's own readers (xpu_int2 / xpu_bool_datum_arrow_read) against
     the same groups."""
-    path, sess, expect, nin = arrow_int2_bool_case(tmp_path)
-    chunks, tdef = XF.arrow_ipc_chunks(path)
-    assert [c.typ for c in tdef.columns] == ["int2", "bool", "int4", "int8"]
+    chunks, sess, expect, meta = C.arrow_int2_bool(str(tmp_path))
+    nin = meta["nitems_in"]
+    assert meta["types"] == ["int2", "bool", "int4", "int8"]
     got, st = _groups_of(sess, chunks)
     assert st["nitems_in"] == nin
     assert F.compare_groups(got, expect, rtol=0.0) == []

@@ -59,11 +59,9 @@ def _session(case):
         _, s, k, _ = C.join_projection(nfact=1000, ndim1=100, ndim2=10)
         return s, k, ord("b")
     if case == "arrow_int2_bool":
-        import pathlib
         import tempfile
-        from test_files import arrow_int2_bool_case
         with tempfile.TemporaryDirectory() as d:
-            _, s, _, _ = arrow_int2_bool_case(pathlib.Path(d), nrows=1000)
+            _, s, _, _ = C.arrow_int2_bool(d, nrows=1000)
         return s, None, ord("a")
     raise ValueError(case)
 
